@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Time to a 1e-8 relative residual on the 256^3 variable-coefficient Poisson
+system (-div(k grad p) = f, k = exp(g), g a Gaussian random field with
+correlation length 8 cells and sigma = 1; RHS i.i.d. U[-1, 1]) with FP32 AMG-PCG
+inside FP64 iterative refinement on one B200, beside the plain FP64 AMG-PCG on
+the same hierarchy, and the SpMV HBM bandwidth.
+
+One step = one complete solve from x = 0 to ||b - A x|| <= 1e-8 ||b||, with
+the matrix and the AMG hierarchy resident (the hierarchy is built once, as the
+reference caches it per sparsity pattern). `value` times it with inputs in
+HBM; `e2e` times the same solve through the C ABI with host buffers (pinned b
+and x copied in, x copied out inside the timed region).
+
+--impl reference times the CPU restatement of the reference algorithm (FP64
+AMG-PCG, same problem, same hierarchy algorithm) on the host cores.
+
+Multi-GPU: the solve does not shard here; `--gpus N` under torchrun runs N
+independent replicas and reports the slowest.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms to 1e-8 rel-residual (FP32 AMG-PCG + FP64 refinement), 256^3 variable-k Poisson"
+RTOL = 1e-8
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=256, help="grid edge (cells per side)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(n, stats=None):
+    cfg = {
+        "workload": f"3-D variable-coefficient Poisson {n}^3, 7-point FV, harmonic-mean faces, "
+                    "k=exp(GRF l=8 sigma=1), Dirichlet x=0,1; AMG-PCG V(1,1) damped Jacobi w=2/3, "
+                    "Ruge-Stueben + modified classical interpolation, dense FP64 coarsest <= 4096; "
+                    "FP32 inner tol 1e-4 inside FP64 refinement to rel-res 1e-8",
+        "unknowns": n ** 3,
+        "l2": "inputs larger than L2 (fine matrix alone > 1 GB)",
+        "seed": 0,
+    }
+    if stats is not None:
+        cfg["nnz"] = int(stats.level_nnz[0])
+        cfg["amg_levels"] = int(stats.num_levels)
+        cfg["operator_complexity"] = round(stats.operator_complexity, 3)
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """dram bytes per launch recorded from an ncu capture (profiles/<name>)."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        for ln in open(path):
+            if ln.startswith("dram_bytes_per_launch_256:"):
+                return float(ln.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, world, rank):
+    """CPU restatement of the reference algorithm (oracle/), all host threads."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from cfdrs_b200 import problems as P
+    O.build()
+    cores = O.get_threads()
+    A, b, _ = P.poisson_3d_variable(args.n, 8.0, 1.0, seed=0)
+    Ao = O.Csr.from_matrix(A)
+    t0 = time.perf_counter()
+    amg = O.Amg(Ao, O.AmgConfig(max_levels=16, min_coarse_size=4096, smoother=O.SMOOTH_JACOBI, pre_smooth=1,
+                                post_smooth=1, relaxation=2 / 3, coarse_solve=O.COARSE_DENSE, interpolation=2))
+    setup_s = time.perf_counter() - t0
+    times, iters = [], None
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        x, rep = O.pcg(Ao, b, precond=O.PRE_AMG, amg=amg, rtol=RTOL, max_it=1000)
+        dt = (time.perf_counter() - t0) * 1e3
+        iters = rep.iterations
+        if s >= args.warmup:
+            times.append(dt)
+    ms = sum(times) / len(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args.n),
+        "iterations": iters, "termination": rep.termination, "setup_s": setup_s,
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "port",
+                         "sample": f"full FP64 AMG-PCG solve phase to 1e-8 on the {args.n}^3 system "
+                                   "(hierarchy built once by the oracle, setup excluded)"},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import _lib, problems as P
+    from cfdrs_b200.device import context, device_matrix
+
+    n = args.n
+    A, b, _ = P.poisson_3d_variable(n, 8.0, 1.0, seed=0)
+    N = A.nrows
+    ctx = context(local)
+    dA = device_matrix(A, ctx)
+    t0 = time.perf_counter()
+    amg = cf.AlgebraicMultigrid(A, cf.AMGConfig.pressure_poisson(), ctx=ctx)
+    setup_s = time.perf_counter() - t0
+    st = amg.statistics()
+
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    bd = torch.as_tensor(b, device="cuda")
+    cfg = cf.IterativeSolverConfig(0.0, RTOL, 1000)
+
+    def solve(x, precision):
+        x.zero_()
+        return cf.cg_preconditioned(A, bd, amg, x, cfg, precision=precision)
+
+    # Plain FP64 AMG-PCG (same hierarchy): reference point of the mixed-precision claim.
+    x64 = torch.zeros_like(bd)
+    solve(x64, cf.Precision.FP64)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fp64_ms = []
+    for _ in range(2):
+        ev0.record(stream)
+        rep64 = solve(x64, cf.Precision.FP64)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        fp64_ms.append(ev0.elapsed_time(ev1))
+
+    # FP32 inner + FP64 refinement: the timed step.
+    x32 = torch.zeros_like(bd)
+    for _ in range(args.warmup):
+        solve(x32, cf.Precision.FP32_REFINE)
+    launches = ctx.kernel_stats()["launches"]
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            rep32 = solve(x32, cf.Precision.FP32_REFINE)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    elapsed = max_over_ranks(ev0.elapsed_time(ev1), world)
+    ms = elapsed / args.steps
+
+    xs, x6 = x32.double().cpu().numpy(), x64.cpu().numpy()
+    diff_at_1e8 = float(np.linalg.norm(xs - x6) / np.linalg.norm(x6))
+    true_rel = float(np.linalg.norm(b - A.matvec(xs)) / np.linalg.norm(b))
+    # Accuracy statement (untimed): the mixed solve driven to 1e-10 against the
+    # FP64 AMG-PCG solution driven to 1e-12 on the same device.
+    xa, xr = torch.zeros_like(bd), torch.zeros_like(bd)
+    cf.cg_preconditioned(A, bd, amg, xa, cf.IterativeSolverConfig(0.0, 1e-10, 1000),
+                         precision=cf.Precision.FP32_REFINE)
+    cf.cg_preconditioned(A, bd, amg, xr, cf.IterativeSolverConfig(0.0, 1e-12, 1000))
+    err_vs_fp64 = float(torch.linalg.norm(xa - xr) / torch.linalg.norm(xr))
+
+    # End to end through the C ABI with host buffers (pinned).
+    ctx.set_stream(None)
+    b_pin = torch.from_numpy(b).pin_memory()
+    x_pin = torch.zeros(N, dtype=torch.float64).pin_memory()
+    bh, xh = b_pin.numpy(), x_pin.numpy()
+    e2e = []
+    for s in range(args.warmup + args.steps):
+        xh[:] = 0.0
+        t0 = time.perf_counter()
+        cf.cg_preconditioned(A, bh, amg, xh, cfg, precision=cf.Precision.FP32_REFINE)
+        dt = (time.perf_counter() - t0) * 1e3
+        if s >= args.warmup:
+            e2e.append(dt)
+    e2e_ms = max_over_ranks(sum(e2e) / len(e2e), world)
+
+    # SpMV roofline: FP32 fine-level operator (the inner solve's dominant kernel) and FP64.
+    ctx.set_stream(stream.cuda_stream)
+    peak, peak_kind = measured_peak()
+    nnz = A.nnz
+    spmv = {}
+    for label, dt, vs in (("f32", torch.float32, 4), ("f64", torch.float64, 8)):
+        xv = torch.rand(N, device="cuda", dtype=dt)
+        yv = torch.empty(N, device="cuda", dtype=dt)
+        for _ in range(3):
+            dA.spmv(xv.data_ptr(), yv.data_ptr(), fp32=(label == "f32"))
+        reps = 20
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(reps):
+            dA.spmv(xv.data_ptr(), yv.data_ptr(), fp32=(label == "f32"))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        t = ev0.elapsed_time(ev1) / reps
+        bytes_ = nnz * (vs + 4) + 4 * (N + 1) + 2 * N * vs
+        spmv[label] = {"ms": t, "bytes": bytes_, "gbs": bytes_ / t / 1e6}
+    ctx.set_stream(None)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_from_hierarchy(amg, A, b, rep64.iterations)
+
+    if rank == 0:
+        f32 = spmv["f32"]
+        traffic = profile_traffic("spmv_f32_256.txt")
+        line = {
+            "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded GRF coefficient, U[-1,1] RHS)",
+            "config": workload_config(n, st),
+            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": N * 8},
+            "gpu_launches": int(launches * args.steps),
+            "roofline": {"bound": "hbm", "achieved": f32["gbs"], "peak": peak, "unit": "GB/s",
+                         "frac": f32["gbs"] / peak, "traffic": traffic,
+                         "kernel": "k_spmv FP32 fine operator (256^3, 117M nnz), timed alone",
+                         "peak_kind": peak_kind},
+            "spmv_gbs": {"f32": f32["gbs"], "f64": spmv["f64"]["gbs"],
+                         "frac_f32": f32["gbs"] / peak, "frac_f64": spmv["f64"]["gbs"] / peak},
+            "fp64_pcg_ms": min(fp64_ms), "speedup_vs_fp64_pcg": min(fp64_ms) / ms,
+            "iterations": {"fp32_inner": rep32.iterations, "outer": rep32.outer_iterations,
+                           "fp64_pcg": rep64.iterations},
+            "error_vs_fp64_pcg": err_vs_fp64,
+            "error_note": "FP32+refinement solved to 1e-10 vs FP64 AMG-PCG solved to 1e-12, same device",
+            "diff_vs_fp64_at_1e-8": diff_at_1e8, "true_rel_residual": true_rel,
+            "amg_setup_s": setup_s, "clocks": clk.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline_from_hierarchy(amg, A, b, iterations):
+    """FP64 AMG-PCG of the CPU oracle on the same hierarchy (exported from the
+    device handle): a bounded sample of 2 iterations, extrapolated to the
+    iteration count of the FP64 solve."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    levels = []
+    for l in range(amg.num_levels):
+        mats = [amg.level(l, 0)]
+        if l + 1 < amg.num_levels:
+            mats += [amg.level(l, 1), amg.level(l, 2)]
+        levels.append([O.Csr.from_matrix(m) for m in mats])
+    oamg = O.Amg.from_levels(levels, O.AmgConfig(max_levels=16, min_coarse_size=4096, smoother=O.SMOOTH_JACOBI,
+                                                 pre_smooth=1, post_smooth=1, relaxation=2 / 3,
+                                                 coarse_solve=O.COARSE_DENSE, interpolation=2))
+    Ao = levels[0][0]
+    sample = 2
+    O.pcg(Ao, b, precond=O.PRE_AMG, amg=oamg, rtol=0.0, tol=0.0, max_it=1)  # warm caches
+    t0 = time.perf_counter()
+    O.pcg(Ao, b, precond=O.PRE_AMG, amg=oamg, rtol=0.0, tol=0.0, max_it=sample)
+    per_it = (time.perf_counter() - t0) * 1e3 / sample
+    return {"value": per_it * iterations, "unit": "ms", "cores": O.get_threads(), "kind": "port",
+            "sample": f"{sample} FP64 AMG-PCG iterations of the full system on the oracle, same hierarchy, "
+                      f"scaled to the {iterations} iterations of the FP64 solve (setup excluded)"}
+
+
+if __name__ == "__main__":
+    main()

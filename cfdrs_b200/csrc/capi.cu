@@ -1,0 +1,704 @@
+// C ABI of libcfdgpu: handles, uploads and dispatch. See include/cfdgpu.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "amg_device.h"
+#include "amg_setup.h"
+#include "internal.h"
+
+namespace cfd {
+
+cfd_status solve_fp64(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg, const double* b, double* x,
+                      const cfd_solver_config& cfg, cfd_solve_report& rep);
+cfd_status solve_refine(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg, const double* b, double* x,
+                        const cfd_solver_config& cfg, cfd_solve_report& rep);
+cfd_status check_precond(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg);
+cfd_status amg_apply_fp64(cfd_amg* amg, const double* r, double* z);
+cfd_status spmv_fp64(cfd_csr* a, const double* x, double* y);
+cfd_status spmv_fp32(cfd_csr* a, const float* x, float* y);
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+namespace {
+
+__global__ void k_f64_to_f32(int64_t n, const double* __restrict__ s, float* __restrict__ d) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    d[i] = (float)s[i];
+}
+
+cfd_status cast_to_f32(const double* s, float* d, int64_t n, cudaStream_t st) {
+  if (n == 0) return CFD_OK;
+  int g = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+  k_f64_to_f32<<<g, 256, 0, st>>>(n, s, d);
+  CFD_TRY_CUDA(cudaGetLastError());
+  return CFD_OK;
+}
+
+template <typename T>
+cfd_status dmalloc(T** p, int64_t n) {
+  // +16 elements of slack keeps vectorised loads of a row-block tail inside the allocation.
+  cudaError_t e = cudaMalloc((void**)p, (size_t)(n + 16) * sizeof(T));
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc(%lld bytes): %s", (long long)((n + 16) * sizeof(T)), cudaGetErrorString(e));
+    *p = nullptr;
+    return CFD_ERR_ALLOC;
+  }
+  return CFD_OK;
+}
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+}  // namespace
+
+// Threads per row: rows of ~6 or fewer nonzeros get a thread each; longer
+// rows (Galerkin coarse operators) a power-of-two group of up to 32 threads.
+int threads_per_row(int64_t nnz, int64_t nrows) {
+  const double avg = nrows > 0 ? (double)nnz / (double)nrows : 0.0;
+  int t = 1;
+  while (t < 32 && 2.0 * t * 6.0 <= avg) t <<= 1;
+  return t;
+}
+
+// Greedy row-block partition: up to kRowsPerBlock / tpr rows and kNnzCap
+// nonzeros per block; a row with more nonzeros than the cap becomes a block
+// of its own.
+std::vector<int> row_partition(const int64_t* rp, int64_t nrows, int tpr) {
+  const int64_t max_rows = kRowsPerBlock / tpr;
+  std::vector<int> blk;
+  blk.reserve(nrows / max_rows + 2);
+  int64_t r = 0;
+  blk.push_back(0);
+  while (r < nrows) {
+    int64_t start = r;
+    int64_t nnz = rp[r + 1] - rp[r];
+    ++r;
+    if (nnz <= kNnzCap) {
+      while (r < nrows && r - start < max_rows) {
+        const int64_t rn = rp[r + 1] - rp[r];
+        if (nnz + rn > kNnzCap) break;
+        nnz += rn;
+        ++r;
+      }
+    }
+    blk.push_back((int)r);
+  }
+  return blk;
+}
+
+cfd_status devmat_upload(DevMat& m, const HostCsr& h, bool want32, cudaStream_t s) {
+  devmat_free(m);
+  m.nrows = h.nrows;
+  m.ncols = h.ncols;
+  m.nnz = h.nnz();
+  if (m.nnz >= INT32_MAX || m.nrows >= INT32_MAX || m.ncols >= INT32_MAX) {
+    set_error("matrix too large for int32 indices (nnz %lld)", (long long)m.nnz);
+    return CFD_ERR_DIM;
+  }
+  std::vector<int> rp32(h.nrows + 1);
+  for (int64_t i = 0; i <= h.nrows; ++i) rp32[i] = (int)h.rp[i];
+  m.tpr = threads_per_row(m.nnz, m.nrows);
+  std::vector<int> blk = row_partition(h.rp.data(), h.nrows, m.tpr);
+  m.nblk = (int)blk.size() - 1;
+  CFD_TRY(dmalloc(&m.rp, h.nrows + 1));
+  CFD_TRY(dmalloc(&m.col, m.nnz));
+  CFD_TRY(dmalloc(&m.v64, m.nnz));
+  CFD_TRY(dmalloc(&m.blk, (int64_t)blk.size()));
+  std::vector<int4> desc(m.nblk);
+  for (int b = 0; b < m.nblk; ++b)
+    desc[b] = make_int4(blk[b], blk[b + 1], (int)h.rp[blk[b]], (int)h.rp[blk[b + 1]]);
+  CFD_TRY(dmalloc(&m.desc, (int64_t)m.nblk));
+  CFD_TRY_CUDA(cudaMemcpyAsync(m.desc, desc.data(), desc.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+  CFD_TRY_CUDA(cudaMemcpyAsync(m.rp, rp32.data(), rp32.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  CFD_TRY_CUDA(cudaMemcpyAsync(m.col, h.ci.data(), m.nnz * sizeof(int), cudaMemcpyHostToDevice, s));
+  CFD_TRY_CUDA(cudaMemcpyAsync(m.v64, h.v.data(), m.nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+  CFD_TRY_CUDA(cudaMemcpyAsync(m.blk, blk.data(), blk.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  if (want32) CFD_TRY(devmat_ensure32(m, s));
+  CFD_TRY_CUDA(cudaStreamSynchronize(s));
+  return CFD_OK;
+}
+
+cfd_status devmat_ensure32(DevMat& m, cudaStream_t s) {
+  if (m.v32 || m.nnz == 0) return CFD_OK;
+  CFD_TRY(dmalloc(&m.v32, m.nnz));
+  return cast_to_f32(m.v64, m.v32, m.nnz, s);
+}
+
+cfd_status devmat_update_values(DevMat& m, const double* v, int64_t nnz, bool want32, cudaStream_t s) {
+  if (nnz != m.nnz) {
+    set_error("value array length %lld does not match nnz %lld", (long long)nnz, (long long)m.nnz);
+    return CFD_ERR_DIM;
+  }
+  CFD_TRY_CUDA(cudaMemcpyAsync(m.v64, v, nnz * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (m.v32 || want32) {
+    if (!m.v32) CFD_TRY(dmalloc(&m.v32, m.nnz));
+    CFD_TRY(cast_to_f32(m.v64, m.v32, m.nnz, s));
+  }
+  CFD_TRY_CUDA(cudaStreamSynchronize(s));
+  return CFD_OK;
+}
+
+void devmat_free(DevMat& m) {
+  dfree(m.rp);
+  dfree(m.col);
+  dfree(m.v64);
+  dfree(m.v32);
+  dfree(m.blk);
+  dfree(m.desc);
+  m.nblk = 0;
+}
+
+cfd_status ensure_partials(cfd_context* ctx, int blocks) {
+  if (blocks <= ctx->partial_capacity) return CFD_OK;
+  dfree(ctx->partials);
+  int cap = std::max(blocks, kVecGrid);
+  CFD_TRY(dmalloc(&ctx->partials, (int64_t)cap * kMaxRed));
+  ctx->partial_capacity = cap;
+  return CFD_OK;
+}
+
+cfd_status check_device_flag(cfd_context* ctx) {
+  CFD_TRY_CUDA(cudaMemcpyAsync(ctx->h_err, ctx->err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CFD_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (*ctx->h_err != 0) {
+    cudaMemsetAsync(ctx->err, 0, sizeof(int), ctx->stream);
+    cudaMemsetAsync(ctx->counter, 0, sizeof(unsigned), ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    *ctx->h_err = 0;
+    set_error("a device-side bounded wait ran out (bulk-copy pipeline); results are invalid");
+    return CFD_ERR_TIMEOUT;
+  }
+  return CFD_OK;
+}
+
+// Diagonal of A (FP64/FP32) and the DiagJacobi inverse: 1/a_ii, or 1 where
+// |a_ii| <= f64::EPSILON (linear_system.rs:286-295); a non-finite diagonal
+// entry makes the Jacobi preconditioner unavailable (linear_system.rs:281-285).
+cfd_status ensure_diagonals(cfd_csr* a) {
+  if (a->diag64) return CFD_OK;
+  const HostCsr& h = a->host;
+  const int64_t n = h.nrows;
+  std::vector<double> d(n, 0.0), inv(n, 1.0);
+  bool finite = true;
+  for (int64_t i = 0; i < n; ++i) {
+    for (int64_t k = h.rp[i]; k < h.rp[i + 1]; ++k)
+      if (h.ci[k] == i) d[i] = h.v[k];
+    if (!std::isfinite(d[i])) finite = false;
+    inv[i] = std::fabs(d[i]) <= DBL_EPSILON ? 1.0 : 1.0 / d[i];
+  }
+  a->jacobi_status = finite ? 0 : 1;
+  cudaStream_t s = a->ctx->stream;
+  CFD_TRY(dmalloc(&a->diag64, n));
+  CFD_TRY(dmalloc(&a->diag32, n));
+  CFD_TRY(dmalloc(&a->jinv64, n));
+  CFD_TRY(dmalloc(&a->jinv32, n));
+  CFD_TRY_CUDA(cudaMemcpyAsync(a->diag64, d.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CFD_TRY_CUDA(cudaMemcpyAsync(a->jinv64, inv.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CFD_TRY(cast_to_f32(a->diag64, a->diag32, n, s));
+  CFD_TRY(cast_to_f32(a->jinv64, a->jinv32, n, s));
+  CFD_TRY_CUDA(cudaStreamSynchronize(s));
+  return CFD_OK;
+}
+
+// ---- AMG device hierarchy -------------------------------------------------------
+template <typename XT>
+static cfd_status alloc_level_vecs(LevelVecs<XT>& v, int64_t n) {
+  CFD_TRY(dmalloc(&v.b, n));
+  CFD_TRY(dmalloc(&v.xa, n));
+  CFD_TRY(dmalloc(&v.xb, n));
+  CFD_TRY(dmalloc(&v.r, n));
+  CFD_TRY(dmalloc(&v.e, n));
+  return CFD_OK;
+}
+
+template <typename XT>
+static void free_level_vecs(LevelVecs<XT>& v) {
+  dfree(v.b);
+  dfree(v.xa);
+  dfree(v.xb);
+  dfree(v.r);
+  dfree(v.e);
+}
+
+void amg_free_device(cfd_amg* amg) {
+  for (DevLevel& L : amg->dev) {
+    devmat_free(L.A);
+    devmat_free(L.P);
+    devmat_free(L.R);
+    dfree(L.d64);
+    dfree(L.d32);
+    free_level_vecs(L.v64);
+    free_level_vecs(L.v32);
+  }
+  amg->dev.clear();
+  dfree(amg->coarse_inv);
+  amg->have32 = false;
+}
+
+cfd_status amg_upload(cfd_amg* amg, bool want32) {
+  cudaStream_t s = amg->ctx->stream;
+  amg_free_device(amg);
+  amg->dev.resize(amg->host.size());
+  int maxblk = 0;
+  for (size_t l = 0; l < amg->host.size(); ++l) {
+    const HostLevel& H = amg->host[l];
+    DevLevel& D = amg->dev[l];
+    CFD_TRY(devmat_upload(D.A, H.A, false, s));
+    maxblk = std::max(maxblk, D.A.nblk);
+    if (l + 1 < amg->host.size()) {
+      CFD_TRY(devmat_upload(D.P, H.P, false, s));
+      CFD_TRY(devmat_upload(D.R, H.R, false, s));
+      maxblk = std::max({maxblk, D.P.nblk, D.R.nblk});
+    }
+    const int64_t n = H.A.nrows;
+    std::vector<double> d(n, 0.0);
+    for (int64_t i = 0; i < n; ++i)
+      for (int64_t k = H.A.rp[i]; k < H.A.rp[i + 1]; ++k)
+        if (H.A.ci[k] == i) d[i] = H.A.v[k];
+    CFD_TRY(dmalloc(&D.d64, n));
+    CFD_TRY(dmalloc(&D.d32, n));
+    CFD_TRY_CUDA(cudaMemcpyAsync(D.d64, d.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CFD_TRY(cast_to_f32(D.d64, D.d32, n, s));
+    CFD_TRY(alloc_level_vecs(D.v64, n));
+  }
+  CFD_TRY(ensure_partials(amg->ctx, maxblk));
+  if (amg->cfg.coarse_solve == CFD_COARSE_DENSE) {
+    const HostCsr& Ac = amg->host.back().A;
+    std::vector<double> inv;
+    if (!dense_inverse(Ac, inv)) {
+      set_error("AMG coarsest operator (%lld rows) is singular", (long long)Ac.nrows);
+      return CFD_ERR_CONFIG;
+    }
+    amg->coarse_n = Ac.nrows;
+    CFD_TRY(dmalloc(&amg->coarse_inv, (int64_t)inv.size()));
+    CFD_TRY_CUDA(cudaMemcpyAsync(amg->coarse_inv, inv.data(), inv.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
+  CFD_TRY_CUDA(cudaStreamSynchronize(s));
+  if (want32) CFD_TRY(amg_ensure32(amg));
+  return CFD_OK;
+}
+
+cfd_status amg_ensure32(cfd_amg* amg) {
+  if (amg->have32) return CFD_OK;
+  cudaStream_t s = amg->ctx->stream;
+  for (size_t l = 0; l < amg->dev.size(); ++l) {
+    DevLevel& D = amg->dev[l];
+    CFD_TRY(devmat_ensure32(D.A, s));
+    if (l + 1 < amg->dev.size()) {
+      CFD_TRY(devmat_ensure32(D.P, s));
+      CFD_TRY(devmat_ensure32(D.R, s));
+    }
+    CFD_TRY(alloc_level_vecs(D.v32, D.A.nrows));
+  }
+  CFD_TRY_CUDA(cudaStreamSynchronize(s));
+  amg->have32 = true;
+  return CFD_OK;
+}
+
+static HostCsr host_from(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* rp, const int32_t* c32,
+                         const int64_t* c64, const double* v) {
+  HostCsr h;
+  h.nrows = nrows;
+  h.ncols = ncols;
+  h.rp.assign(rp, rp + nrows + 1);
+  h.ci.resize(nnz);
+  if (c32)
+    std::memcpy(h.ci.data(), c32, nnz * sizeof(int32_t));
+  else
+    for (int64_t k = 0; k < nnz; ++k) h.ci[k] = (int32_t)c64[k];
+  h.v.assign(v, v + nnz);
+  return h;
+}
+
+static cfd_status validate_csr(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* rp, const int32_t* c32,
+                               const int64_t* c64) {
+  if (nrows < 0 || ncols < 0 || nnz < 0 || !rp || (nnz > 0 && !c32 && !c64)) {
+    set_error("invalid CSR arguments");
+    return CFD_ERR_DIM;
+  }
+  if (nrows >= INT32_MAX || ncols >= INT32_MAX || nnz >= INT32_MAX) {
+    set_error("matrix too large for int32 indices");
+    return CFD_ERR_DIM;
+  }
+  if (rp[0] != 0 || rp[nrows] != nnz) {
+    set_error("row_ptr must start at 0 and end at nnz (%lld != %lld)", (long long)rp[nrows], (long long)nnz);
+    return CFD_ERR_DIM;
+  }
+  for (int64_t i = 0; i < nrows; ++i) {
+    if (rp[i + 1] < rp[i]) {
+      set_error("row_ptr decreases at row %lld", (long long)i);
+      return CFD_ERR_DIM;
+    }
+    for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {
+      const int64_t c = c32 ? c32[k] : c64[k];
+      if (c < 0 || c >= ncols) {
+        set_error("column index %lld out of range in row %lld", (long long)c, (long long)i);
+        return CFD_ERR_DIM;
+      }
+      if (k > rp[i]) {
+        const int64_t cp = c32 ? c32[k - 1] : c64[k - 1];
+        if (cp >= c) {
+          set_error("column indices must be strictly increasing within row %lld", (long long)i);
+          return CFD_ERR_DIM;
+        }
+      }
+    }
+  }
+  return CFD_OK;
+}
+
+}  // namespace cfd
+
+using namespace cfd;
+
+extern "C" {
+
+const char* cfd_last_error(void) { return g_err; }
+const char* cfd_version(void) { return "cfdgpu 0.1.0 (sm_100a)"; }
+
+cfd_status cfd_context_create(int device, cfd_context** out) {
+  if (!out) return CFD_ERR_CONFIG;
+  *out = nullptr;
+  int count = 0;
+  CFD_TRY_CUDA(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count) {
+    set_error("device %d not present (%d devices)", device, count);
+    return CFD_ERR_CONFIG;
+  }
+  CFD_TRY_CUDA(cudaSetDevice(device));
+  cfd_context* c = new cfd_context;
+  c->device = device;
+  CFD_TRY_CUDA(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+  c->stream = c->own;
+  CFD_TRY(dmalloc(&c->counter, 1));
+  CFD_TRY_CUDA(cudaMemset(c->counter, 0, sizeof(unsigned)));
+  CFD_TRY(dmalloc(&c->state, 2));
+  CFD_TRY_CUDA(cudaMallocHost((void**)&c->h_state, 2 * sizeof(DevState)));
+  CFD_TRY_CUDA(cudaEventCreate(&c->ev0));
+  CFD_TRY_CUDA(cudaEventCreate(&c->ev1));
+  CFD_TRY(ensure_partials(c, kVecGrid));
+  CFD_TRY(dmalloc(&c->err, 1));
+  CFD_TRY_CUDA(cudaMemset(c->err, 0, sizeof(int)));
+  CFD_TRY_CUDA(cudaMallocHost((void**)&c->h_err, sizeof(int)));
+  *c->h_err = 0;
+  CFD_TRY_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+  // Keep freed stream-ordered workspace in the pool for the next solve.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  *out = c;
+  return CFD_OK;
+}
+
+cfd_status cfd_context_set_stream(cfd_context* ctx, void* stream) {
+  if (!ctx) return CFD_ERR_STATE;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+  return CFD_OK;
+}
+
+cfd_status cfd_context_synchronize(cfd_context* ctx) {
+  if (!ctx) return CFD_ERR_STATE;
+  CFD_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+  return CFD_OK;
+}
+
+cfd_status cfd_context_destroy(cfd_context* ctx) {
+  if (!ctx) return CFD_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  dfree(ctx->partials);
+  dfree(ctx->counter);
+  dfree(ctx->state);
+  dfree(ctx->err);
+  if (ctx->h_state) cudaFreeHost(ctx->h_state);
+  if (ctx->h_err) cudaFreeHost(ctx->h_err);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->own) cudaStreamDestroy(ctx->own);
+  delete ctx;
+  return CFD_OK;
+}
+
+static cfd_status csr_create_common(cfd_context* ctx, int64_t nrows, int64_t ncols, int64_t nnz,
+                                    const int64_t* rp, const int32_t* c32, const int64_t* c64, const double* val,
+                                    cfd_csr** out) {
+  if (!ctx || !out) {
+    set_error("null context or output handle");
+    return CFD_ERR_STATE;
+  }
+  *out = nullptr;
+  CFD_TRY(validate_csr(nrows, ncols, nnz, rp, c32, c64));
+  if (nnz > 0 && !val) {
+    set_error("null value array");
+    return CFD_ERR_DIM;
+  }
+  CFD_TRY_CUDA(cudaSetDevice(ctx->device));
+  std::lock_guard<std::mutex> g(ctx->mu);
+  cfd_csr* a = new cfd_csr;
+  a->ctx = ctx;
+  a->host = host_from(nrows, ncols, nnz, rp, c32, c64, val);
+  cfd_status s = devmat_upload(a->dev, a->host, false, ctx->stream);
+  if (s == CFD_OK) s = ensure_partials(ctx, a->dev.nblk);
+  if (s != CFD_OK) {
+    devmat_free(a->dev);
+    delete a;
+    return s;
+  }
+  *out = a;
+  return CFD_OK;
+}
+
+cfd_status cfd_csr_create(cfd_context* ctx, int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* row_ptr,
+                          const int64_t* col, const double* val, cfd_csr** out) {
+  return csr_create_common(ctx, nrows, ncols, nnz, row_ptr, nullptr, col, val, out);
+}
+
+cfd_status cfd_csr_create_i32(cfd_context* ctx, int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* row_ptr,
+                              const int32_t* col, const double* val, cfd_csr** out) {
+  return csr_create_common(ctx, nrows, ncols, nnz, row_ptr, col, nullptr, val, out);
+}
+
+cfd_status cfd_csr_update_values(cfd_csr* a, const double* val) {
+  if (!a || !val) return CFD_ERR_STATE;
+  std::lock_guard<std::mutex> g(a->ctx->mu);
+  std::copy(val, val + a->host.nnz(), a->host.v.begin());
+  CFD_TRY(devmat_update_values(a->dev, val, a->host.nnz(), false, a->ctx->stream));
+  dfree(a->diag64);
+  dfree(a->diag32);
+  dfree(a->jinv64);
+  dfree(a->jinv32);
+  a->jacobi_status = -1;
+  return CFD_OK;
+}
+
+cfd_status cfd_csr_info(const cfd_csr* a, int64_t* nrows, int64_t* ncols, int64_t* nnz) {
+  if (!a) return CFD_ERR_STATE;
+  if (nrows) *nrows = a->host.nrows;
+  if (ncols) *ncols = a->host.ncols;
+  if (nnz) *nnz = a->host.nnz();
+  return CFD_OK;
+}
+
+cfd_status cfd_csr_destroy(cfd_csr* a) {
+  if (!a) return CFD_OK;
+  cudaSetDevice(a->ctx->device);
+  cudaStreamSynchronize(a->ctx->stream);
+  devmat_free(a->dev);
+  dfree(a->diag64);
+  dfree(a->diag32);
+  dfree(a->jinv64);
+  dfree(a->jinv32);
+  delete a;
+  return CFD_OK;
+}
+
+cfd_status cfd_spmv(cfd_csr* a, const double* x, double* y) {
+  if (!a || !x || !y) return CFD_ERR_STATE;
+  std::lock_guard<std::mutex> g(a->ctx->mu);
+  CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+  CFD_TRY(spmv_fp64(a, x, y));
+  return check_device_flag(a->ctx);
+}
+
+cfd_status cfd_spmv_f32(cfd_csr* a, const float* x, float* y) {
+  if (!a || !x || !y) return CFD_ERR_STATE;
+  std::lock_guard<std::mutex> g(a->ctx->mu);
+  CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+  CFD_TRY(spmv_fp32(a, x, y));
+  return check_device_flag(a->ctx);
+}
+
+void cfd_amg_config_default(cfd_amg_config* c) {
+  // AMGConfig::default, multigrid/mod.rs:244-259 (smoother: damped Jacobi is the
+  // device smoother; the reference default is Gauss-Seidel).
+  c->max_levels = 10;
+  c->coarsening = CFD_COARSEN_RUGE_STUEBEN;
+  c->min_coarse_size = 50;
+  c->interpolation = CFD_INTERP_CLASSICAL;
+  c->smoother = CFD_SMOOTH_JACOBI;
+  c->pre_smooth = 2;
+  c->post_smooth = 2;
+  c->relaxation = 1.0;
+  c->strength_threshold = 0.25;
+  c->coarse_solve = CFD_COARSE_SWEEPS;
+  c->coarse_sweeps = 10;
+  c->aggregate_size = 8;
+  c->seed = 0;
+}
+
+cfd_status cfd_amg_setup(cfd_csr* a, const cfd_amg_config* cfg, cfd_amg** out) {
+  if (!a || !cfg || !out) return CFD_ERR_STATE;
+  *out = nullptr;
+  if (cfg->max_levels < 1 || cfg->max_levels > 16 || cfg->smoother != CFD_SMOOTH_JACOBI ||
+      cfg->pre_smooth < 0 || cfg->post_smooth < 0 || !(cfg->strength_threshold >= 0.0) ||
+      !std::isfinite(cfg->relaxation) || cfg->coarsening < 0 || cfg->coarsening > 2 || cfg->interpolation < 0 ||
+      cfg->interpolation > 2) {
+    set_error("invalid AMG configuration");
+    return CFD_ERR_CONFIG;
+  }
+  if (a->host.nrows != a->host.ncols) {
+    set_error("AMG needs a square matrix");
+    return CFD_ERR_DIM;
+  }
+  std::lock_guard<std::mutex> g(a->ctx->mu);
+  CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+  auto t0 = std::chrono::steady_clock::now();
+  cfd_amg* amg = new cfd_amg;
+  amg->ctx = a->ctx;
+  amg->cfg = *cfg;
+  amg->host = build_hierarchy(a->host, *cfg);
+  cfd_status s = amg_upload(amg, false);
+  if (s != CFD_OK) {
+    amg_free_device(amg);
+    delete amg;
+    return s;
+  }
+  amg->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  *out = amg;
+  return CFD_OK;
+}
+
+cfd_status cfd_amg_recompute(cfd_amg* amg, cfd_csr* a) {
+  if (!amg || !a) return CFD_ERR_STATE;
+  if (amg->host.empty()) return CFD_ERR_STATE;
+  if (a->host.nrows != amg->host[0].A.nrows || a->host.nnz() != amg->host[0].A.nnz()) {
+    set_error("recompute needs the hierarchy's sparsity pattern");
+    return CFD_ERR_DIM;
+  }
+  std::lock_guard<std::mutex> g(a->ctx->mu);
+  CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+  const bool want32 = amg->have32;
+  recompute_hierarchy(amg->host, a->host);
+  return amg_upload(amg, want32);
+}
+
+cfd_status cfd_amg_apply(cfd_amg* amg, const double* r, double* z) {
+  if (!amg || !r || !z) return CFD_ERR_STATE;
+  std::lock_guard<std::mutex> g(amg->ctx->mu);
+  CFD_TRY_CUDA(cudaSetDevice(amg->ctx->device));
+  CFD_TRY(amg_apply_fp64(amg, r, z));
+  return check_device_flag(amg->ctx);
+}
+
+cfd_status cfd_amg_stats(const cfd_amg* amg, cfd_amg_stats_t* out) {
+  if (!amg || !out) return CFD_ERR_STATE;
+  std::memset(out, 0, sizeof(*out));
+  out->num_levels = (int32_t)amg->host.size();
+  double tot_nnz = 0, tot_rows = 0;
+  for (size_t l = 0; l < amg->host.size(); ++l) {
+    if (l < 16) {
+      out->level_rows[l] = amg->host[l].A.nrows;
+      out->level_nnz[l] = amg->host[l].A.nnz();
+    }
+    tot_nnz += (double)amg->host[l].A.nnz();
+    tot_rows += (double)amg->host[l].A.nrows;
+  }
+  out->operator_complexity = tot_nnz / std::max<double>(1.0, (double)amg->host[0].A.nnz());
+  out->grid_complexity = tot_rows / std::max<double>(1.0, (double)amg->host[0].A.nrows);
+  out->setup_seconds = amg->setup_seconds;
+  return CFD_OK;
+}
+
+cfd_status cfd_amg_level(const cfd_amg* amg, int level, int which, int64_t* nrows, int64_t* ncols, int64_t* nnz,
+                         int64_t* row_ptr, int64_t* col, double* val) {
+  if (!amg || level < 0 || level >= (int)amg->host.size() || which < 0 || which > 2) return CFD_ERR_DIM;
+  const HostLevel& L = amg->host[level];
+  if (which > 0 && level + 1 == (int)amg->host.size()) return CFD_ERR_DIM;
+  const HostCsr& m = which == 0 ? L.A : (which == 1 ? L.P : L.R);
+  if (nrows) *nrows = m.nrows;
+  if (ncols) *ncols = m.ncols;
+  if (nnz) *nnz = m.nnz();
+  if (row_ptr) std::copy(m.rp.begin(), m.rp.end(), row_ptr);
+  if (col)
+    for (int64_t k = 0; k < m.nnz(); ++k) col[k] = m.ci[k];
+  if (val) std::copy(m.v.begin(), m.v.end(), val);
+  return CFD_OK;
+}
+
+cfd_status cfd_amg_destroy(cfd_amg* amg) {
+  if (!amg) return CFD_OK;
+  cudaSetDevice(amg->ctx->device);
+  cudaStreamSynchronize(amg->ctx->stream);
+  amg_free_device(amg);
+  delete amg;
+  return CFD_OK;
+}
+
+void cfd_solve_options_default(cfd_solve_options* o) {
+  o->solver = CFD_SOLVER_CG;
+  o->precond = CFD_PRECOND_JACOBI;
+  o->precision = CFD_PRECISION_FP64;
+  o->memory = CFD_MEMORY_HOST;
+  o->inner_tolerance = 1e-4;
+  o->max_outer = 20;
+  o->check_every = 0;
+}
+
+cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, const double* b, double* x,
+                     const cfd_solver_config* cfg, cfd_solve_report* rep) {
+  if (!a || !opt || !b || !x || !cfg || !rep) {
+    set_error("null argument to cfd_solve");
+    return CFD_ERR_STATE;
+  }
+  // convergence_policy (krylov.rs:123-139) rejects non-finite or negative
+  // tolerances and a zero iteration budget at construction.
+  if (!(cfg->tolerance >= 0.0) || !(cfg->relative_tolerance >= 0.0) || !std::isfinite(cfg->tolerance) ||
+      !std::isfinite(cfg->relative_tolerance) || cfg->max_iterations <= 0) {
+    set_error("invalid iterative solver configuration: tolerance %g, relative %g, max_iterations %lld",
+              cfg->tolerance, cfg->relative_tolerance, (long long)cfg->max_iterations);
+    return CFD_ERR_CONFIG;
+  }
+  if (opt->solver < 0 || opt->solver > 1 || opt->precond < 0 || opt->precond > 2 || opt->precision < 0 ||
+      opt->precision > 1 || opt->memory < 0 || opt->memory > 1) {
+    set_error("invalid solve options");
+    return CFD_ERR_CONFIG;
+  }
+  if (a->host.nrows != a->host.ncols) {
+    set_error("Krylov solve needs a square matrix (%lld x %lld)", (long long)a->host.nrows,
+              (long long)a->host.ncols);
+    return CFD_ERR_DIM;
+  }
+  std::lock_guard<std::mutex> g(a->ctx->mu);
+  CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+  CFD_TRY(check_precond(a, *opt, amg));
+  a->ctx->stats.reset();
+  std::memset(rep, 0, sizeof(*rep));
+  if (a->host.nrows == 0) {
+    rep->termination = CFD_TERM_INITIAL_RESIDUAL;
+    return CFD_OK;
+  }
+  if (opt->precision == CFD_PRECISION_FP32_REFINE)
+    CFD_TRY(solve_refine(a, *opt, amg, b, x, *cfg, *rep));
+  else
+    CFD_TRY(solve_fp64(a, *opt, amg, b, x, *cfg, *rep));
+  return check_device_flag(a->ctx);
+}
+
+cfd_status cfd_last_kernel_stats(cfd_context* ctx, cfd_kernel_stats* out) {
+  if (!ctx || !out) return CFD_ERR_STATE;
+  out->launches = ctx->stats.launches;
+  out->spmv_launches = ctx->stats.spmv_launches;
+  out->spmv_bytes = ctx->stats.spmv_bytes;
+  return CFD_OK;
+}
+
+}  // extern "C"

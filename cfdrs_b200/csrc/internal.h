@@ -1,0 +1,129 @@
+// Internal declarations of libcfdgpu (host + device). Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cfdgpu.h"
+
+namespace cfd {
+
+// Error message of the last failure on this thread (cfd_last_error()).
+void set_error(const char* fmt, ...);
+
+#define CFD_TRY_CUDA(...)                                                                           \
+  do {                                                                                              \
+    cudaError_t e_ = (__VA_ARGS__);                                                                 \
+    if (e_ != cudaSuccess) {                                                                        \
+      ::cfd::set_error("%s: %s (%s:%d)", #__VA_ARGS__, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return CFD_ERR_CUDA;                                                                          \
+    }                                                                                               \
+  } while (0)
+
+#define CFD_TRY(...)                  \
+  do {                                \
+    cfd_status s_ = (__VA_ARGS__);    \
+    if (s_ != CFD_OK) return s_;      \
+  } while (0)
+
+// Row-blocked CSR SpMV geometry: 256 consumer threads per CTA, row blocks of
+// at most kRowsPerBlock rows (two per consumer thread or row group) and
+// kNnzCap nonzeros staged in shared memory; a row with more than kNnzCap
+// nonzeros is a block of its own (block-stride reduction).
+constexpr int kThreads = 256;
+constexpr int kRowsPerThread = 2;
+constexpr int kRowsPerBlock = kThreads * kRowsPerThread;
+constexpr int kNnzCap = 4096;
+// Grid of the streaming vector kernels: 148 SMs x 8 resident CTAs.
+constexpr int kVecGrid = 148 * 8;
+// Device-side scratch for two-stage reductions (per-CTA partials, up to 4 values).
+constexpr int kMaxRed = 4;
+
+// Host CSR (int64 offsets, int32 columns), the form AMG setup works on.
+struct HostCsr {
+  int64_t nrows = 0, ncols = 0;
+  std::vector<int64_t> rp;
+  std::vector<int32_t> ci;
+  std::vector<double> v;
+  int64_t nnz() const { return (int64_t)ci.size(); }
+};
+
+// Device CSR. Indices are int32 (nnz < 2^31); values are kept in FP64 and,
+// once asked for, an FP32 copy sharing the same index arrays.
+struct DevMat {
+  int64_t nrows = 0, ncols = 0, nnz = 0;
+  int* rp = nullptr;
+  int* col = nullptr;
+  double* v64 = nullptr;
+  float* v32 = nullptr;
+  int* blk = nullptr;  // row-block partition, nblk + 1 entries
+  int4* desc = nullptr;  // per row block {r0, r1, k0, k1}
+  int nblk = 0;
+  int tpr = 1;         // threads cooperating on one row (power of two, <= 32)
+};
+
+cfd_status devmat_upload(DevMat& m, const HostCsr& h, bool want32, cudaStream_t s);
+cfd_status devmat_update_values(DevMat& m, const double* v, int64_t nnz, bool want32, cudaStream_t s);
+cfd_status devmat_ensure32(DevMat& m, cudaStream_t s);
+void devmat_free(DevMat& m);
+std::vector<int> row_partition(const int64_t* rp, int64_t nrows, int tpr);
+int threads_per_row(int64_t nnz, int64_t nrows);
+
+// Scalars of one Krylov recurrence, resident on the device so that the
+// iteration runs without host round trips; the host polls `done`.
+struct DevState {
+  double rho, alpha, beta, omega;
+  double pq, rr, rnorm, threshold;
+  double rnorm0, rhat_v, ts, tt;
+  double tol_abs, tol_rel, spare0, spare1;
+  int32_t iter, max_iter, done, term;
+};
+
+struct KernelStats {
+  int64_t launches = 0;
+  int64_t spmv_launches = 0;
+  double spmv_bytes = 0.0;
+  void reset() { *this = KernelStats(); }
+};
+
+}  // namespace cfd
+
+struct cfd_context {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  double* partials = nullptr;      // kMaxRed * max grid
+  unsigned* counter = nullptr;     // last-CTA ticket of the two-stage reduction
+  int partial_capacity = 0;        // CTAs covered by `partials`
+  cfd::DevState* state = nullptr;  // two states: [0] outer/FP64, [1] inner
+  cfd::DevState* h_state = nullptr;  // pinned mirror
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int* err = nullptr;    // set by a kernel whose bounded wait ran out
+  int* h_err = nullptr;  // pinned mirror
+  int num_sms = 148;
+  cfd::KernelStats stats;
+  std::mutex mu;
+};
+
+struct cfd_csr {
+  cfd_context* ctx = nullptr;
+  cfd::HostCsr host;
+  cfd::DevMat dev;
+  double* diag64 = nullptr;
+  float* diag32 = nullptr;
+  double* jinv64 = nullptr;  // DiagJacobi inverse diagonal (identity for |d| <= eps)
+  float* jinv32 = nullptr;
+  int jacobi_status = -1;    // -1 unknown, 0 ok, 1 non-finite diagonal
+};
+
+namespace cfd {
+cfd_status ensure_partials(cfd_context* ctx, int blocks);
+// Reads the device error flag; a set flag (a bounded wait ran out) is reported
+// as CFD_ERR_TIMEOUT and the flag and reduction ticket are reset.
+cfd_status check_device_flag(cfd_context* ctx);
+cfd_status ensure_diagonals(cfd_csr* a);
+}  // namespace cfd

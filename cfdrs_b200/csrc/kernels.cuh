@@ -1,0 +1,603 @@
+// Device kernels of the sparse solve path (sm_100a). All are HBM-bound.
+//
+//  * k_spmv_pipe: persistent, warp-specialized CSR SpMV. A producer warp walks
+//    the CTA's row blocks (b = blockIdx.x + k * gridDim.x) and moves each
+//    block's value, column and row-offset streams into a ring of shared-memory
+//    stages with 1-D bulk copies (cp.async.bulk, the TMA engine); full/empty
+//    mbarrier pairs hand stages between the producer and 8 consumer warps.
+//    Consumers never touch global metadata: they read offsets and entries from
+//    shared memory, gather x through the read-only path, and pass the row
+//    result to a fused epilogue whose own operands were loaded before the
+//    gathers. Row groups of 2^k threads serve operators with long rows.
+//  * k_spmv: the same computation with one row block per CTA and plain
+//    coalesced staging, for matrices of only a few row blocks.
+//  * Epilogue functors (plain store, residual, damped Jacobi, PCG / BiCGSTAB
+//    dots, prolongation-correction) consume the row result so no kernel
+//    re-reads what another just wrote.
+//  * Reductions are two-stage and deterministic: per-CTA partials in fixed
+//    slots, and the last CTA to arrive (atomic ticket) sums them in a fixed
+//    order and applies the Krylov scalar update on the device.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+
+#include "internal.h"
+
+namespace cfd {
+
+template <typename VT>
+struct MatView {
+  const int* __restrict__ rp;
+  const int* __restrict__ col;
+  const VT* __restrict__ val;
+  const int* __restrict__ blk;
+  const int4* __restrict__ desc;  // per row block {r0, r1, k0, k1}
+  int tpr_log2;                   // log2 of the threads cooperating on one row
+};
+
+inline int ilog2(int v) {
+  int l = 0;
+  while ((1 << (l + 1)) <= v) ++l;
+  return l;
+}
+
+template <typename VT>
+inline MatView<VT> mat_view(const DevMat& m);
+template <>
+inline MatView<double> mat_view<double>(const DevMat& m) {
+  return {m.rp, m.col, m.v64, m.blk, m.desc, ilog2(m.tpr)};
+}
+template <>
+inline MatView<float> mat_view<float>(const DevMat& m) {
+  return {m.rp, m.col, m.v32, m.blk, m.desc, ilog2(m.tpr)};
+}
+
+// Scratch of one two-stage reduction.
+struct Red {
+  double* partials;
+  unsigned* counter;
+};
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum over the CTA; the result is valid in thread 0.
+template <typename T>
+__device__ __forceinline__ T block_sum(T v) {
+  __shared__ T sm[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) sm[w] = v;
+  __syncthreads();
+  T t = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : T(0);
+  if (w == 0) t = warp_sum(t);
+  return t;
+}
+
+// Sum over the kThreads consumer threads only (named barrier 1); valid in thread 0.
+template <typename T>
+__device__ __forceinline__ T consumer_sum(T v) {
+  __shared__ T sm[kThreads / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = warp_sum(v);
+  asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory");
+  if (lane == 0) sm[w] = v;
+  asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory");
+  T t = threadIdx.x < kThreads / 32 ? sm[threadIdx.x] : T(0);
+  if (w == 0) t = warp_sum(t);
+  return t;
+}
+
+// Two-stage grid reduction of NV doubles. Every thread of every CTA must call
+// it. Returns true in the last CTA, whose thread 0 then holds the totals.
+template <int NV>
+__device__ __forceinline__ bool grid_reduce(double (&v)[NV], Red red, double (&tot)[NV]) {
+  __shared__ bool s_last;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    const double b = block_sum(v[q]);
+    if (threadIdx.x == 0) red.partials[(size_t)blockIdx.x * NV + q] = b;
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned t = atomicAdd(red.counter, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += __ldcg(red.partials + (size_t)b * NV + q);
+    tot[q] = block_sum(s);
+  }
+  if (threadIdx.x == 0) *red.counter = 0u;
+  return true;
+}
+
+__device__ __forceinline__ bool flag_set(const int* done) { return done != nullptr && *done != 0; }
+
+template <typename T>
+__device__ __forceinline__ bool diag_ok(T d);
+template <>
+__device__ __forceinline__ bool diag_ok<double>(double d) {
+  return fabs(d) > 1e-15;
+}
+template <>
+__device__ __forceinline__ bool diag_ok<float>(float d) {
+  return fabsf(d) > 1e-15f;
+}
+
+// ---------------------------------------------------------------------------
+// Epilogues. load(i) fetches the row's own operands (issued before the x
+// gathers so the latencies overlap); row(i, sum, diag, pre, acc) finishes it.
+
+struct NoPre {};
+
+// y = A x
+template <typename XT>
+struct EpiStore {
+  static constexpr int NRED = 0;
+  using Pre = NoPre;
+  XT* __restrict__ y;
+  const int* done;
+  Red red;
+  __device__ bool skip() const { return flag_set(done); }
+  __device__ Pre load(int) const { return {}; }
+  template <typename S>
+  __device__ void row(int i, S s, S, const Pre&, double*) const {
+    y[i] = (XT)s;
+  }
+  __device__ void finish(const double*) const {}
+};
+
+// y = base + A x (prolongation with correction, amg.rs:475-489; y may alias base)
+template <typename XT>
+struct EpiAddTo {
+  static constexpr int NRED = 0;
+  using Pre = XT;
+  XT* y;
+  const XT* base;
+  const int* done;
+  Red red;
+  __device__ bool skip() const { return flag_set(done); }
+  __device__ Pre load(int i) const { return base[i]; }
+  template <typename S>
+  __device__ void row(int i, S s, S, const Pre& bi, double*) const {
+    y[i] = bi + (XT)s;
+  }
+  __device__ void finish(const double*) const {}
+};
+
+// r = b - A x. MODE 0: plain. MODE 1: Krylov start (||r0||, threshold, the
+// InitialResidual test). MODE 2: refinement outer residual (||r|| into rnorm).
+template <typename XT, int MODE>
+struct EpiResidual {
+  static constexpr int NRED = MODE ? 1 : 0;
+  using Pre = XT;
+  XT* __restrict__ r;
+  const XT* __restrict__ b;
+  DevState* st;
+  const int* done;
+  Red red;
+  __device__ bool skip() const { return flag_set(done); }
+  __device__ Pre load(int i) const { return b[i]; }
+  template <typename S>
+  __device__ void row(int i, S s, S, const Pre& bi, double* acc) const {
+    const XT ri = bi - (XT)s;
+    r[i] = ri;
+    if (MODE) acc[0] += (double)ri * (double)ri;
+  }
+  __device__ void finish(const double* tot) const {
+    const double rn = sqrt(tot[0]);
+    st->rr = tot[0];
+    st->rnorm = rn;
+    if (MODE == 1) {
+      st->rnorm0 = rn;
+      st->threshold = fmax(st->tol_abs, st->tol_rel * rn);
+      st->iter = 0;
+      st->done = 0;
+      st->term = CFD_TERM_MAX_ITERATIONS;
+      if (!isfinite(rn)) {
+        st->term = CFD_TERM_BREAKDOWN;
+        st->done = 1;
+      } else if (rn <= st->threshold) {
+        st->term = CFD_TERM_INITIAL_RESIDUAL;
+        st->done = 1;
+      }
+    }
+  }
+};
+
+__device__ __forceinline__ void pcg_rho_update(DevState* st, double rho_new) {
+  if (rho_new == 0.0 || !isfinite(rho_new)) {
+    st->term = CFD_TERM_BREAKDOWN;
+    st->done = 1;
+    return;
+  }
+  st->beta = rho_new / st->rho;
+  st->rho = rho_new;
+}
+
+// One damped-Jacobi sweep, JacobiSmoother::apply (smoothers.rs:160-194):
+//   xn_i = xo_i + w ((b_i - sum_{j != i} a_ij xo_j) / a_ii - xo_i),  xn_i = xo_i if |a_ii| <= 1e-15.
+// DOT 1: also accumulate b.xn and store it as rho (PCG start, z = M r).
+// DOT 2: b.xn is rho_new of the PCG recurrence: breakdown test, beta, rho.
+template <typename XT, int DOT>
+struct EpiJacobi {
+  static constexpr int NRED = DOT ? 1 : 0;
+  struct Pre {
+    XT xo, b;
+  };
+  XT* __restrict__ xn;
+  const XT* __restrict__ xo;
+  const XT* __restrict__ b;
+  XT omega;
+  DevState* st;
+  const int* done;
+  Red red;
+  __device__ bool skip() const { return flag_set(done); }
+  __device__ Pre load(int i) const { return {xo[i], b[i]}; }
+  template <typename S>
+  __device__ void row(int i, S s, S d, const Pre& p, double* acc) const {
+    XT out = p.xo;
+    if (diag_ok<XT>((XT)d)) {
+      const XT nv = (p.b - (XT)s) / (XT)d;
+      out = p.xo + omega * (nv - p.xo);
+    }
+    xn[i] = out;
+    if (DOT) acc[0] += (double)p.b * (double)out;
+  }
+  __device__ void finish(const double* tot) const {
+    if (DOT == 1) st->rho = tot[0];
+    if (DOT == 2) pcg_rho_update(st, tot[0]);
+  }
+};
+
+// PCG q = A p with p.q: alpha = rho / p.q, or NonPositiveCurvature.
+template <typename XT>
+struct EpiCgDot {
+  static constexpr int NRED = 1;
+  using Pre = XT;
+  XT* __restrict__ q;
+  const XT* __restrict__ p;
+  DevState* st;
+  Red red;
+  __device__ bool skip() const { return st->done != 0; }
+  __device__ Pre load(int i) const { return p[i]; }
+  template <typename S>
+  __device__ void row(int i, S s, S, const Pre& pi, double* acc) const {
+    const XT qi = (XT)s;
+    q[i] = qi;
+    acc[0] += (double)pi * (double)qi;
+  }
+  __device__ void finish(const double* tot) const {
+    st->pq = tot[0];
+    if (!(tot[0] > 0.0)) {
+      st->term = CFD_TERM_NON_POSITIVE_CURVATURE;
+      st->done = 1;
+    } else {
+      st->alpha = st->rho / tot[0];
+    }
+  }
+};
+
+// BiCGSTAB v = A p_hat with r_hat.v: alpha = rho / r_hat.v, or Breakdown.
+template <typename XT>
+struct EpiBicgV {
+  static constexpr int NRED = 1;
+  using Pre = XT;
+  XT* __restrict__ v;
+  const XT* __restrict__ rhat;
+  DevState* st;
+  Red red;
+  __device__ bool skip() const { return st->done != 0; }
+  __device__ Pre load(int i) const { return rhat[i]; }
+  template <typename S>
+  __device__ void row(int i, S s, S, const Pre& ri, double* acc) const {
+    const XT vi = (XT)s;
+    v[i] = vi;
+    acc[0] += (double)ri * (double)vi;
+  }
+  __device__ void finish(const double* tot) const {
+    if (tot[0] == 0.0 || !isfinite(tot[0])) {
+      st->term = CFD_TERM_BREAKDOWN;
+      st->done = 1;
+    } else {
+      st->alpha = st->rho / tot[0];
+    }
+  }
+};
+
+// BiCGSTAB t = A s_hat with (t.s, t.t): omega = t.s / t.t, or Breakdown.
+template <typename XT>
+struct EpiBicgT {
+  static constexpr int NRED = 2;
+  using Pre = XT;
+  XT* __restrict__ t;
+  const XT* __restrict__ s;
+  DevState* st;
+  Red red;
+  __device__ bool skip() const { return st->done != 0; }
+  __device__ Pre load(int i) const { return s[i]; }
+  template <typename S>
+  __device__ void row(int i, S sum, S, const Pre& si, double* acc) const {
+    const XT ti = (XT)sum;
+    t[i] = ti;
+    acc[0] += (double)ti * (double)si;
+    acc[1] += (double)ti * (double)ti;
+  }
+  __device__ void finish(const double* tot) const {
+    if (tot[1] == 0.0 || !isfinite(tot[1])) {
+      st->term = CFD_TERM_BREAKDOWN;
+      st->done = 1;
+    } else {
+      st->omega = tot[0] / tot[1];
+      st->ts = tot[0];
+      st->tt = tot[1];
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Row-group dot products over staged entries. A group of 2^tl threads owns
+// kRowsPerThread rows of the block (g and g + 256 >> tl, ...); the groups read
+// strided shares of both rows in one interleaved loop so their x gathers are in
+// flight together, then reduce with a butterfly. OFFDIAG=true forms
+// sum_{j != i} a_ij x_j and returns a_ii separately (the Jacobi smoother's
+// split, smoothers.rs:177-186). srp/sc/sv index rows and nonzeros directly.
+template <typename VT, typename XT, bool OFFDIAG, class Epi>
+__device__ __forceinline__ void rows_from_stage(const Epi& epi, const int* srp, const int* sc, const VT* sv, int r0,
+                                                int r1, int tl, int tid, const XT* __restrict__ x, double* red) {
+  const int lane = tid & ((1 << tl) - 1);
+  const int step = 1 << tl;
+  const int g = tid >> tl;
+  const int ngroups = kThreads >> tl;
+  int row[kRowsPerThread], ra[kRowsPerThread], re[kRowsPerThread];
+  typename Epi::Pre pre[kRowsPerThread];
+  VT sum[kRowsPerThread], diag[kRowsPerThread];
+#pragma unroll
+  for (int q = 0; q < kRowsPerThread; ++q) {
+    row[q] = r0 + g + q * ngroups;
+    const bool live = row[q] < r1;
+    ra[q] = live ? srp[row[q]] + lane : 0;
+    re[q] = live ? srp[row[q] + 1] : 0;
+    pre[q] = typename Epi::Pre{};
+    if (live && lane == 0) pre[q] = epi.load(row[q]);
+    sum[q] = VT(0);
+    diag[q] = VT(0);
+  }
+  int len = 0;
+#pragma unroll
+  for (int q = 0; q < kRowsPerThread; ++q) len = max(len, re[q] - ra[q]);
+#pragma unroll 4
+  for (int j = 0; j < len; j += step) {
+#pragma unroll
+    for (int q = 0; q < kRowsPerThread; ++q) {
+      const int k = ra[q] + j;
+      if (k < re[q]) {
+        const int c = sc[k];
+        const VT v = sv[k];
+        if (OFFDIAG && c == row[q])
+          diag[q] = v;
+        else
+          sum[q] += v * (VT)__ldg(x + c);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kRowsPerThread; ++q) {
+    for (int o = step >> 1; o > 0; o >>= 1) {
+      sum[q] += __shfl_xor_sync(0xffffffffu, sum[q], o);
+      if (OFFDIAG) diag[q] += __shfl_xor_sync(0xffffffffu, diag[q], o);
+    }
+    if (row[q] < r1 && lane == 0) epi.row(row[q], sum[q], diag[q], pre[q], red);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent warp-specialized pipeline. Every wait is bounded: when one runs
+// out the CTA records the failure in *err, drains the copies it issued (again
+// bounded) and leaves without joining the reduction.
+constexpr int kPipeThreads = kThreads + 32;  // 8 consumer warps + 1 producer warp
+constexpr unsigned kWaitLimit = 1u << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+  for (unsigned i = 0; i < kWaitLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+template <typename VT>
+struct PipeLayout {
+  static constexpr int kStages = 2;
+  static constexpr int kValSlack = 16 / (int)sizeof(VT);
+  static constexpr int kValBytes = ((kNnzCap + 2 * kValSlack) * (int)sizeof(VT) + 127) / 128 * 128;
+  static constexpr int kColBytes = ((kNnzCap + 8) * 4 + 127) / 128 * 128;
+  static constexpr int kRpBytes = ((kRowsPerBlock + 1 + 8) * 4 + 127) / 128 * 128;
+  static constexpr int kStageBytes = kValBytes + kColBytes + kRpBytes;
+  static constexpr int kSmemBytes = kStages * kStageBytes;
+};
+
+template <typename VT, typename XT, bool OFFDIAG, class Epi>
+__global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, int nblk, const XT* __restrict__ x,
+                                                                Epi epi, int* err) {
+  if (epi.skip()) return;
+  using L = PipeLayout<VT>;
+  constexpr int kStages = L::kStages;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full[kStages];
+  __shared__ __align__(8) uint64_t empty[kStages];
+  __shared__ int4 meta[kStages];  // r0, r1, k0, k1 of the staged block
+  __shared__ int s_ok[kStages];
+  __shared__ volatile int s_abort;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  constexpr int mv = L::kValSlack;
+  auto stage_val = [&](int s) { return reinterpret_cast<VT*>(smem + s * L::kStageBytes); };
+  auto stage_col = [&](int s) { return reinterpret_cast<int*>(smem + s * L::kStageBytes + L::kValBytes); };
+  auto stage_rp = [&](int s) {
+    return reinterpret_cast<int*>(smem + s * L::kStageBytes + L::kValBytes + L::kColBytes);
+  };
+
+  if (tid == kThreads) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kThreads / 32);
+    }
+    s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  double red[Epi::NRED > 0 ? Epi::NRED : 1];
+#pragma unroll
+  for (int q = 0; q < (Epi::NRED > 0 ? Epi::NRED : 1); ++q) red[q] = 0.0;
+
+  if (warp == kThreads / 32) {
+    // ---- producer warp: descriptors of 32 blocks are fetched at once (one per
+    // lane); lane 0 waits for free stages and issues the copies.
+    const int lane = tid & 31;
+    int it = 0;
+    bool stop = false;
+    for (int base = blockIdx.x; base < nblk && !stop; base += 32 * gridDim.x) {
+      const int bl = base + lane * gridDim.x;
+      const int4 dl = bl < nblk ? A.desc[bl] : make_int4(0, 0, 0, 0);
+      for (int j = 0; j < 32; ++j, ++it) {
+        const int b = base + j * gridDim.x;
+        if (b >= nblk) {
+          stop = true;
+          break;
+        }
+        int4 m;
+        m.x = __shfl_sync(0xffffffffu, dl.x, j);
+        m.y = __shfl_sync(0xffffffffu, dl.y, j);
+        m.z = __shfl_sync(0xffffffffu, dl.z, j);
+        m.w = __shfl_sync(0xffffffffu, dl.w, j);
+        int ok = 1;
+        if (lane == 0) {
+          const int s = it % kStages;
+          if (it >= kStages && !mbar_wait_bounded(&empty[s], (unsigned)((it / kStages) - 1) & 1u)) {
+            s_abort = 1;
+            atomicExch(err, 1);
+          }
+          if (s_abort) {
+            ok = 0;
+          } else {
+            meta[s] = m;
+            const int p0 = m.x & ~3, p1 = (m.y + 1 + 3) & ~3;
+            const unsigned brp = (unsigned)(p1 - p0) * 4u;
+            if (m.w - m.z > kNnzCap || m.w == m.z) {
+              mbar_expect_tx(&full[s], brp);
+              bulk_g2s(stage_rp(s), A.rp + p0, brp, &full[s]);
+            } else {
+              const int v0 = m.z & ~(mv - 1), v1 = (m.w + mv - 1) & ~(mv - 1);
+              const int c0 = m.z & ~3, c1 = (m.w + 3) & ~3;
+              const unsigned bv = (unsigned)(v1 - v0) * sizeof(VT), bc = (unsigned)(c1 - c0) * 4u;
+              mbar_expect_tx(&full[s], bv + bc + brp);
+              bulk_g2s(stage_val(s), A.val + v0, bv, &full[s]);
+              bulk_g2s(stage_col(s), A.col + c0, bc, &full[s]);
+              bulk_g2s(stage_rp(s), A.rp + p0, brp, &full[s]);
+            }
+          }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) {
+          stop = true;
+          break;
+        }
+      }
+    }
+    if (lane == 0 && s_abort) {
+      // Drain what was issued before leaving (bounded).
+      for (int j = (it > kStages ? it - kStages : 0); j < it; ++j)
+        mbar_wait_bounded(&full[j % kStages], (unsigned)(j / kStages) & 1u);
+    }
+  } else {
+    // ---- consumers ----
+    const int tl = A.tpr_log2;
+    int it = 0;
+    for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++it) {
+      const int s = it % kStages;
+      const unsigned parity = (unsigned)(it / kStages) & 1u;
+      if (tid == 0) s_ok[s] = (!s_abort && mbar_wait_bounded(&full[s], parity)) ? 1 : 0;
+      asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory");
+      if (!s_ok[s]) {
+        if (tid == 0) {
+          s_abort = 1;
+          atomicExch(err, 1);
+        }
+        break;
+      }
+      mbar_wait_bounded(&full[s], parity);  // completes at once; acquires the stage for this thread
+      const int4 m = meta[s];
+      const int* srp = stage_rp(s) - (m.x & ~3);
+      if (m.w - m.z <= kNnzCap) {
+        rows_from_stage<VT, XT, OFFDIAG>(epi, srp, stage_col(s) - (m.z & ~3), stage_val(s) - (m.z & ~(mv - 1)), m.x,
+                                         m.y, tl, tid, x, red);
+      } else {
+        const int row = m.x;
+        typename Epi::Pre pre{};
+        if (tid == 0) pre = epi.load(row);
+        VT sum = VT(0), diag = VT(0);
+        for (int k = m.z + tid; k < m.w; k += kThreads) {
+          const int c = __ldcs(A.col + k);
+          const VT v = __ldcs(A.val + k);
+          if (OFFDIAG && c == row)
+            diag += v;
+          else
+            sum += v * (VT)__ldg(x + c);
+        }
+        sum = consumer_sum(sum);
+        diag = consumer_sum(diag);
+        if (tid == 0) epi.row(row, sum, diag, pre, red);
+      }
+      __syncwarp();
+      if ((tid & 31) == 0) mbar_arrive(&empty[s]);
+    }
+  }
+  __syncthreads();
+  if (s_abort) return;
+  if constexpr (Epi::NRED > 0) {
+    double tot[Epi::NRED];
+    if (grid_reduce<Epi::NRED>(red, epi.red, tot) && tid == 0) epi.finish(tot);
+  }
+}
+
+}  // namespace cfd

@@ -1,0 +1,825 @@
+// Device orchestration: SpMV launch helpers, the AMG V-cycle, preconditioned
+// CG and BiCGSTAB, and FP32-inner / FP64-refinement solves.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "amg_device.h"
+#include "internal.h"
+#include "kernels.cuh"
+
+namespace cfd {
+
+namespace {
+
+constexpr int kPreNone = 0, kPreJacobi = 1, kPreAmg = 2;
+
+inline int vec_grid(int64_t n) {
+  int64_t g = (n + kThreads - 1) / kThreads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, kVecGrid));
+}
+
+#define GRID_STRIDE(i, n) for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < (n); i += (int64_t)gridDim.x * kThreads)
+
+// ---------------------------------------------------------------------------
+// Vector kernels.
+
+// First damped-Jacobi sweep from a zero iterate: x = w (b / a_ii).
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_smooth0(int64_t n, const XT* __restrict__ b, const XT* __restrict__ d,
+                                                      XT omega, XT* __restrict__ x, const int* done) {
+  if (flag_set(done)) return;
+  GRID_STRIDE(i, n) {
+    const XT di = d[i];
+    x[i] = diag_ok<XT>(di) ? omega * (b[i] / di) : XT(0);
+  }
+}
+
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_fill(int64_t n, XT* __restrict__ x, XT v, const int* done) {
+  if (flag_set(done)) return;
+  GRID_STRIDE(i, n) x[i] = v;
+}
+
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_copy(int64_t n, const XT* __restrict__ s, XT* __restrict__ d, const int* done) {
+  if (flag_set(done)) return;
+  GRID_STRIDE(i, n) d[i] = s[i];
+}
+
+// Dense coarsest-level solve x = A_c^{-1} b with the FP64 inverse; one warp per row.
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_dense_gemv(int n, const double* __restrict__ inv, const XT* __restrict__ b,
+                                                         XT* __restrict__ x, const int* done) {
+  if (flag_set(done)) return;
+  const int lane = threadIdx.x & 31;
+  const int row = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+  if (row >= n) return;
+  const double* a = inv + (size_t)row * n;
+  double s = 0.0;
+  for (int k = lane; k < n; k += 32) s += a[k] * (double)b[k];
+  s = warp_sum(s);
+  if (lane == 0) x[row] = (XT)s;
+}
+
+// PCG: x += alpha p; r -= alpha q; ||r||; with Jacobi also rho_new = r.(D^-1 r).
+// The last CTA applies the termination tests (converged / non-finite / budget)
+// and, for Jacobi or no preconditioner, beta = rho_new / rho.
+template <typename XT, int PRE>
+__global__ void __launch_bounds__(kThreads) k_cg_update(int64_t n, XT* __restrict__ x, const XT* __restrict__ p,
+                                                        XT* __restrict__ r, const XT* __restrict__ q,
+                                                        const XT* __restrict__ jinv, DevState* st, Red red) {
+  if (st->done) return;
+  const XT a = (XT)st->alpha;
+  double acc[2] = {0.0, 0.0};
+  GRID_STRIDE(i, n) {
+    x[i] = x[i] + a * p[i];
+    const XT ri = r[i] - a * q[i];
+    r[i] = ri;
+    acc[0] += (double)ri * (double)ri;
+    if (PRE == kPreJacobi) acc[1] += (double)ri * (double)(ri * jinv[i]);
+  }
+  double tot[2];
+  if (grid_reduce<2>(acc, red, tot) && threadIdx.x == 0) {
+    const double rn = sqrt(tot[0]);
+    st->rr = tot[0];
+    st->rnorm = rn;
+    st->iter += 1;
+    if (!isfinite(rn)) {
+      st->term = CFD_TERM_BREAKDOWN;
+      st->done = 1;
+    } else if (rn <= st->threshold) {
+      st->term = CFD_TERM_CONVERGED;
+      st->done = 1;
+    } else if (st->iter >= st->max_iter) {
+      st->term = CFD_TERM_MAX_ITERATIONS;
+      st->done = 1;
+    } else if (PRE == kPreJacobi) {
+      pcg_rho_update(st, tot[1]);
+    } else if (PRE == kPreNone) {
+      pcg_rho_update(st, tot[0]);
+    }
+  }
+}
+
+// PCG start: p = M r and rho = r.p.
+template <typename XT, int PRE>
+__global__ void __launch_bounds__(kThreads) k_pcg_init(int64_t n, XT* __restrict__ p, const XT* __restrict__ r,
+                                                       const XT* __restrict__ z, const XT* __restrict__ jinv,
+                                                       DevState* st, Red red) {
+  if (st->done) return;
+  double acc[1] = {0.0};
+  GRID_STRIDE(i, n) {
+    const XT ri = r[i];
+    const XT zi = PRE == kPreAmg ? z[i] : (PRE == kPreJacobi ? ri * jinv[i] : ri);
+    p[i] = zi;
+    acc[0] += (double)ri * (double)zi;
+  }
+  double tot[1];
+  if (grid_reduce<1>(acc, red, tot) && threadIdx.x == 0) st->rho = tot[0];
+}
+
+// PCG direction: p = z + beta p (z = D^-1 r, r or the V-cycle output).
+template <typename XT, int PRE>
+__global__ void __launch_bounds__(kThreads) k_p_update(int64_t n, XT* __restrict__ p, const XT* __restrict__ r,
+                                                       const XT* __restrict__ z, const XT* __restrict__ jinv,
+                                                       const DevState* st) {
+  if (st->done) return;
+  const XT beta = (XT)st->beta;
+  GRID_STRIDE(i, n) {
+    const XT zi = PRE == kPreAmg ? z[i] : (PRE == kPreJacobi ? r[i] * jinv[i] : r[i]);
+    p[i] = zi + beta * p[i];
+  }
+}
+
+// rho_new = r.z after a preconditioner whose last kernel could not fuse it.
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_rz(int64_t n, const XT* __restrict__ r, const XT* __restrict__ z,
+                                                 DevState* st, int mode, Red red) {
+  if (st->done) return;
+  double acc[1] = {0.0};
+  GRID_STRIDE(i, n) acc[0] += (double)r[i] * (double)z[i];
+  double tot[1];
+  if (grid_reduce<1>(acc, red, tot) && threadIdx.x == 0) {
+    if (mode == 1)
+      st->rho = tot[0];
+    else
+      pcg_rho_update(st, tot[0]);
+  }
+}
+
+// ---- BiCGSTAB (Saad 2003, Alg. 7.7, right preconditioning) --------------------
+// rho_new = r_hat.r; beta = (rho_new / rho)(alpha / omega).
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_bicg_rho(int64_t n, const XT* __restrict__ rhat, const XT* __restrict__ r,
+                                                       DevState* st, Red red) {
+  if (st->done) return;
+  double acc[1] = {0.0};
+  GRID_STRIDE(i, n) acc[0] += (double)rhat[i] * (double)r[i];
+  double tot[1];
+  if (grid_reduce<1>(acc, red, tot) && threadIdx.x == 0) {
+    const double rho_new = tot[0];
+    if (rho_new == 0.0 || !isfinite(rho_new)) {
+      st->term = CFD_TERM_BREAKDOWN;
+      st->done = 1;
+      return;
+    }
+    st->beta = (rho_new / st->rho) * (st->alpha / st->omega);
+    st->rho = rho_new;
+  }
+}
+
+// p = r + beta (p - omega v) (first: p = r); with Jacobi also p_hat = D^-1 p.
+template <typename XT, int PRE>
+__global__ void __launch_bounds__(kThreads) k_bicg_p(int64_t n, XT* __restrict__ p, XT* __restrict__ ph,
+                                                     const XT* __restrict__ r, const XT* __restrict__ v,
+                                                     const XT* __restrict__ jinv, const DevState* st, int first) {
+  if (st->done) return;
+  const XT beta = (XT)st->beta, om = (XT)st->omega;
+  GRID_STRIDE(i, n) {
+    const XT pi = first ? r[i] : r[i] + beta * (p[i] - om * v[i]);
+    p[i] = pi;
+    if (PRE == kPreJacobi) ph[i] = pi * jinv[i];
+    if (PRE == kPreNone) ph[i] = pi;
+  }
+}
+
+// s = r - alpha v; ||s|| (early exit: the host then adds alpha p_hat to x);
+// with Jacobi also s_hat = D^-1 s.
+template <typename XT, int PRE>
+__global__ void __launch_bounds__(kThreads) k_bicg_s(int64_t n, XT* __restrict__ s, XT* __restrict__ sh,
+                                                     const XT* __restrict__ r, const XT* __restrict__ v,
+                                                     const XT* __restrict__ jinv, DevState* st, Red red) {
+  if (st->done) return;
+  const XT a = (XT)st->alpha;
+  double acc[1] = {0.0};
+  GRID_STRIDE(i, n) {
+    const XT si = r[i] - a * v[i];
+    s[i] = si;
+    if (PRE == kPreJacobi) sh[i] = si * jinv[i];
+    if (PRE == kPreNone) sh[i] = si;
+    acc[0] += (double)si * (double)si;
+  }
+  double tot[1];
+  if (grid_reduce<1>(acc, red, tot) && threadIdx.x == 0) {
+    const double sn = sqrt(tot[0]);
+    st->iter += 1;
+    if (sn <= st->threshold) {
+      st->rnorm = sn;
+      st->term = CFD_TERM_CONVERGED;
+      st->spare0 = 1.0;  // x still needs alpha p_hat
+      st->done = 1;
+    }
+  }
+}
+
+// x += alpha p_hat + omega s_hat; r = s - omega t; ||r|| and termination tests.
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_bicg_x(int64_t n, XT* __restrict__ x, XT* __restrict__ r,
+                                                     const XT* __restrict__ ph, const XT* __restrict__ sh,
+                                                     const XT* __restrict__ s, const XT* __restrict__ t,
+                                                     DevState* st, Red red) {
+  if (st->done) return;
+  const XT a = (XT)st->alpha, om = (XT)st->omega;
+  double acc[1] = {0.0};
+  GRID_STRIDE(i, n) {
+    x[i] = x[i] + (a * ph[i] + om * sh[i]);
+    const XT ri = s[i] - om * t[i];
+    r[i] = ri;
+    acc[0] += (double)ri * (double)ri;
+  }
+  double tot[1];
+  if (grid_reduce<1>(acc, red, tot) && threadIdx.x == 0) {
+    const double rn = sqrt(tot[0]);
+    st->rnorm = rn;
+    if (!isfinite(rn)) {
+      st->term = CFD_TERM_BREAKDOWN;
+      st->done = 1;
+    } else if (rn <= st->threshold) {
+      st->term = CFD_TERM_CONVERGED;
+      st->done = 1;
+    } else if (st->omega == 0.0) {
+      st->term = CFD_TERM_BREAKDOWN;
+      st->done = 1;
+    } else if (st->iter >= st->max_iter) {
+      st->term = CFD_TERM_MAX_ITERATIONS;
+      st->done = 1;
+    }
+  }
+}
+
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_axpy_state(int64_t n, XT* __restrict__ x, const XT* __restrict__ y,
+                                                         const DevState* st) {
+  const XT a = (XT)st->alpha;
+  GRID_STRIDE(i, n) x[i] = x[i] + a * y[i];
+}
+
+// ---- refinement ----------------------------------------------------------------
+// Inner right-hand side r32 = r64 / ||r64||, inner iterate zeroed; sets up the
+// inner state (threshold = inner_tol * ||r32||).
+__global__ void __launch_bounds__(kThreads) k_refine_start(int64_t n, const double* __restrict__ r64,
+                                                           float* __restrict__ r32, float* __restrict__ x32,
+                                                           const DevState* outer, DevState* inner, Red red) {
+  const double sc = 1.0 / outer->rnorm;
+  double acc[1] = {0.0};
+  GRID_STRIDE(i, n) {
+    const float ri = (float)(r64[i] * sc);
+    r32[i] = ri;
+    x32[i] = 0.0f;
+    acc[0] += (double)ri * (double)ri;
+  }
+  double tot[1];
+  if (grid_reduce<1>(acc, red, tot) && threadIdx.x == 0) {
+    const double rn = sqrt(tot[0]);
+    inner->rnorm0 = rn;
+    inner->rnorm = rn;
+    inner->rr = tot[0];
+    inner->threshold = fmax(inner->tol_abs, inner->tol_rel * rn);
+    inner->iter = 0;
+    inner->done = 0;
+    inner->spare0 = 0.0;
+    inner->term = CFD_TERM_MAX_ITERATIONS;
+    inner->rho = inner->alpha = inner->omega = 1.0;
+    inner->beta = 0.0;
+    if (!(rn > inner->threshold)) {
+      inner->term = CFD_TERM_INITIAL_RESIDUAL;
+      inner->done = 1;
+    }
+  }
+}
+
+// x64 += ||r64|| * d32 (the FP64 solution accumulation).
+__global__ void __launch_bounds__(kThreads) k_refine_accumulate(int64_t n, double* __restrict__ x64,
+                                                                const float* __restrict__ d32, const DevState* outer) {
+  const double sc = outer->rnorm;
+  GRID_STRIDE(i, n) x64[i] += sc * (double)d32[i];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launch helpers.
+
+struct Launcher {
+  cfd_context* ctx;
+  cudaStream_t s;
+  Red red() const { return Red{ctx->partials, ctx->counter}; }
+  // Every SpMV runs the persistent bulk-copy pipeline, one CTA per row block
+  // up to num_sms * (resident CTAs per SM).
+  template <typename VT, typename XT, bool OFF, class Epi>
+  cfd_status spmv(const DevMat& m, const XT* x, Epi epi) {
+    if (m.nrows == 0) return CFD_OK;
+    epi.red = red();
+    auto kern = k_spmv_pipe<VT, XT, OFF, Epi>;
+    constexpr int smem = PipeLayout<VT>::kSmemBytes;
+    static int occ = -1;
+    if (occ < 0) {
+      CFD_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      int o = 0;
+      CFD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kPipeThreads, smem));
+      occ = std::max(1, o);
+    }
+    const int grid = std::min(m.nblk, ctx->num_sms * occ);
+    kern<<<grid, kPipeThreads, smem, s>>>(mat_view<VT>(m), m.nblk, x, epi, ctx->err);
+    ctx->stats.launches++;
+    ctx->stats.spmv_launches++;
+    ctx->stats.spmv_bytes += (double)m.nnz * (sizeof(VT) + 4) + 4.0 * (m.nrows + 1) +
+                             (double)sizeof(XT) * (m.nrows + m.ncols);
+    return check();
+  }
+  cfd_status check() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      set_error("kernel launch failed: %s", cudaGetErrorString(e));
+      return CFD_ERR_CUDA;
+    }
+    return CFD_OK;
+  }
+  template <typename K, typename... Args>
+  cfd_status vec(int64_t n, K kernel, Args... args) {
+    kernel<<<vec_grid(n), kThreads, 0, s>>>(n, args...);
+    ctx->stats.launches++;
+    return check();
+  }
+};
+
+// ---------------------------------------------------------------------------
+// V-cycle, AlgebraicMultigrid::v_cycle (amg.rs:423-503) from a zero iterate
+// (amg.rs:464-466, :553-554). `out` receives the level result; at level 0 with
+// dot != 0 the last kernel also forms b.out (PCG rho).
+
+template <typename XT>
+LevelVecs<XT>& vecs(DevLevel& L);
+template <>
+LevelVecs<double>& vecs<double>(DevLevel& L) {
+  return L.v64;
+}
+template <>
+LevelVecs<float>& vecs<float>(DevLevel& L) {
+  return L.v32;
+}
+template <typename XT>
+const XT* diag_of(const DevLevel& L);
+template <>
+const double* diag_of<double>(const DevLevel& L) {
+  return L.d64;
+}
+template <>
+const float* diag_of<float>(const DevLevel& L) {
+  return L.d32;
+}
+
+template <typename XT>
+static cfd_status jacobi_sweep(Launcher& lc, const DevLevel& L, const XT* xo, XT* xn, const XT* b, XT omega,
+                               int dot, DevState* st, const int* done) {
+  if (dot == 1) return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 1>{xn, xo, b, omega, st, done, {}});
+  if (dot == 2) return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 2>{xn, xo, b, omega, st, done, {}});
+  return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 0>{xn, xo, b, omega, st, done, {}});
+}
+
+template <typename XT>
+static cfd_status vcycle(Launcher& lc, cfd_amg* amg, size_t l, const XT* b, XT* out, int dot, DevState* st,
+                         const int* done) {
+  DevLevel& L = amg->dev[l];
+  LevelVecs<XT>& V = vecs<XT>(L);
+  const int64_t n = L.A.nrows;
+  const cfd_amg_config& c = amg->cfg;
+  const XT omega = (XT)c.relaxation;
+  const bool coarsest = (l + 1 == amg->dev.size());
+  if (coarsest) {
+    if (c.coarse_solve == CFD_COARSE_DENSE && amg->coarse_inv) {
+      k_dense_gemv<XT><<<(int)((n + 7) / 8), kThreads, 0, lc.s>>>((int)n, amg->coarse_inv, b, out, done);
+      lc.ctx->stats.launches++;
+      CFD_TRY(lc.check());
+      if (dot) CFD_TRY(lc.vec(n, k_rz<XT>, b, (const XT*)out, st, dot, lc.red()));
+      return CFD_OK;
+    }
+    const int sweeps = std::max(0, (int)c.coarse_sweeps);
+    if (sweeps == 0) {
+      CFD_TRY(lc.vec(n, k_fill<XT>, out, XT(0), done));
+      if (dot) CFD_TRY(lc.vec(n, k_rz<XT>, b, (const XT*)out, st, dot, lc.red()));
+      return CFD_OK;
+    }
+    XT* cur = V.xa;
+    XT* nxt = V.xb;
+    CFD_TRY(lc.vec(n, k_smooth0<XT>, b, diag_of<XT>(L), omega, sweeps == 1 ? out : cur, done));
+    if (sweeps == 1) {
+      if (dot) CFD_TRY(lc.vec(n, k_rz<XT>, b, (const XT*)out, st, dot, lc.red()));
+      return CFD_OK;
+    }
+    for (int s = 1; s < sweeps; ++s) {
+      XT* dst = (s == sweeps - 1) ? out : nxt;
+      CFD_TRY(jacobi_sweep<XT>(lc, L, cur, dst, b, omega, s == sweeps - 1 ? dot : 0, st, done));
+      std::swap(cur, nxt);
+    }
+    return CFD_OK;
+  }
+  // 1. pre-smoothing from x = 0
+  XT* x = V.xa;
+  XT* y = V.xb;
+  if (c.pre_smooth >= 1) {
+    CFD_TRY(lc.vec(n, k_smooth0<XT>, b, diag_of<XT>(L), omega, x, done));
+    for (int s = 1; s < c.pre_smooth; ++s) {
+      CFD_TRY(jacobi_sweep<XT>(lc, L, x, y, b, omega, 0, st, done));
+      std::swap(x, y);
+    }
+  } else {
+    CFD_TRY(lc.vec(n, k_fill<XT>, x, XT(0), done));
+  }
+  // 2. residual r = b - A x
+  CFD_TRY(lc.spmv<XT, XT, false>(L.A, x, EpiResidual<XT, 0>{V.r, b, nullptr, done, {}}));
+  // 3. restriction to the next level's right-hand side
+  DevLevel& Lc = amg->dev[l + 1];
+  LevelVecs<XT>& Vc = vecs<XT>(Lc);
+  CFD_TRY(lc.spmv<XT, XT, false>(L.R, V.r, EpiStore<XT>{Vc.b, done, {}}));
+  // 4. coarse solve from zero
+  CFD_TRY(vcycle<XT>(lc, amg, l + 1, Vc.b, Vc.e, 0, st, done));
+  // 5-6. x += P e_c
+  CFD_TRY(lc.spmv<XT, XT, false>(L.P, Vc.e, EpiAddTo<XT>{x, x, done, {}}));
+  // 7. post-smoothing
+  if (c.post_smooth <= 0) {
+    CFD_TRY(lc.vec(n, k_copy<XT>, (const XT*)x, out, done));
+    if (dot) CFD_TRY(lc.vec(n, k_rz<XT>, b, (const XT*)out, st, dot, lc.red()));
+    return CFD_OK;
+  }
+  for (int s = 0; s < c.post_smooth; ++s) {
+    const bool last = (s == c.post_smooth - 1);
+    XT* dst = last ? out : y;
+    CFD_TRY(jacobi_sweep<XT>(lc, L, x, dst, b, omega, last ? dot : 0, st, done));
+    if (!last) std::swap(x, y);
+  }
+  return CFD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Krylov drivers. The recurrences run on device-resident scalars; the host
+// only polls the state to stop launching, choosing how many iterations to
+// enqueue from the observed convergence rate.
+
+struct Poller {
+  cfd_context* ctx;
+  DevState* dev;
+  DevState* host;  // pinned slot
+  int64_t last_iter = 0;
+  double last_rn = 0.0;
+  int chunk = 1;
+  int fixed = 0;
+  cfd_status poll() {
+    CFD_TRY_CUDA(cudaMemcpyAsync(host, dev, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+    CFD_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+    return CFD_OK;
+  }
+  void next_chunk() {
+    if (fixed > 0) {
+      chunk = fixed;
+      return;
+    }
+    const DevState& h = *host;
+    int c = std::min(2 * chunk, 64);
+    if (h.iter > last_iter && last_rn > 0.0 && h.rnorm > 0.0 && h.rnorm < last_rn) {
+      const double rate = std::pow(h.rnorm / last_rn, 1.0 / (double)(h.iter - last_iter));
+      if (rate < 1.0 && rate > 0.0) {
+        const double rem = std::log(h.threshold / h.rnorm) / std::log(rate);
+        c = (int)std::ceil(std::max(1.0, std::min(64.0, rem)));
+      }
+    }
+    last_iter = h.iter;
+    last_rn = h.rnorm;
+    chunk = std::max(1, c);
+  }
+};
+
+template <typename XT>
+struct KrylovBufs {
+  XT *x, *b, *r, *p, *q, *z, *rh, *v, *s, *sh, *t;
+};
+
+template <typename XT>
+static const XT* jinv_of(cfd_csr* a);
+template <>
+const double* jinv_of<double>(cfd_csr* a) {
+  return a->jinv64;
+}
+template <>
+const float* jinv_of<float>(cfd_csr* a) {
+  return a->jinv32;
+}
+
+// Preconditioned CG. Expects the state's start (rnorm0, threshold, done, iter)
+// already set and r holding the initial residual.
+template <typename XT, int PRE>
+static cfd_status pcg_loop(Launcher& lc, cfd_csr* a, cfd_amg* amg, KrylovBufs<XT>& B, DevState* st, Poller& pl) {
+  const int64_t n = a->dev.nrows;
+  const XT* jinv = jinv_of<XT>(a);
+  const int* done = &st->done;
+  if (PRE == kPreAmg) CFD_TRY(vcycle<XT>(lc, amg, 0, B.r, B.z, 0, st, done));
+  CFD_TRY(lc.vec(n, k_pcg_init<XT, PRE>, B.p, (const XT*)B.r, (const XT*)B.z, jinv, st, lc.red()));
+  const int64_t max_launch = std::max<int64_t>(1, st ? (int64_t)1 << 40 : 1);
+  (void)max_launch;
+  int64_t launched = 0;
+  for (;;) {
+    for (int k = 0; k < pl.chunk; ++k) {
+      CFD_TRY(lc.spmv<XT, XT, false>(a->dev, B.p, EpiCgDot<XT>{B.q, B.p, st, {}}));
+      CFD_TRY(lc.vec(n, k_cg_update<XT, PRE>, B.x, (const XT*)B.p, B.r, (const XT*)B.q, jinv, st, lc.red()));
+      if (PRE == kPreAmg) CFD_TRY(vcycle<XT>(lc, amg, 0, B.r, B.z, 2, st, done));
+      CFD_TRY(lc.vec(n, k_p_update<XT, PRE>, B.p, (const XT*)B.r, (const XT*)B.z, jinv, (const DevState*)st));
+      ++launched;
+    }
+    CFD_TRY(pl.poll());
+    if (pl.host->done) break;
+    if (launched > pl.host->max_iter + 64) {
+      set_error("PCG did not terminate within its iteration budget");
+      return CFD_ERR_TIMEOUT;
+    }
+    pl.next_chunk();
+  }
+  return CFD_OK;
+}
+
+template <typename XT, int PRE>
+static cfd_status bicgstab_loop(Launcher& lc, cfd_csr* a, cfd_amg* amg, KrylovBufs<XT>& B, DevState* st,
+                                Poller& pl) {
+  const int64_t n = a->dev.nrows;
+  const XT* jinv = jinv_of<XT>(a);
+  const int* done = &st->done;
+  CFD_TRY(lc.vec(n, k_copy<XT>, (const XT*)B.r, B.rh, (const int*)nullptr));
+  int64_t launched = 0;
+  bool first = true;
+  for (;;) {
+    for (int k = 0; k < pl.chunk; ++k) {
+      CFD_TRY(lc.vec(n, k_bicg_rho<XT>, (const XT*)B.rh, (const XT*)B.r, st, lc.red()));
+      CFD_TRY(lc.vec(n, k_bicg_p<XT, PRE>, B.p, B.z, (const XT*)B.r, (const XT*)B.v, jinv, (const DevState*)st,
+                     first ? 1 : 0));
+      if (PRE == kPreAmg) CFD_TRY(vcycle<XT>(lc, amg, 0, B.p, B.z, 0, st, done));
+      CFD_TRY(lc.spmv<XT, XT, false>(a->dev, B.z, EpiBicgV<XT>{B.v, B.rh, st, {}}));
+      CFD_TRY(lc.vec(n, k_bicg_s<XT, PRE>, B.s, B.sh, (const XT*)B.r, (const XT*)B.v, jinv, st, lc.red()));
+      if (PRE == kPreAmg) CFD_TRY(vcycle<XT>(lc, amg, 0, B.s, B.sh, 0, st, done));
+      CFD_TRY(lc.spmv<XT, XT, false>(a->dev, B.sh, EpiBicgT<XT>{B.t, B.s, st, {}}));
+      CFD_TRY(lc.vec(n, k_bicg_x<XT>, B.x, B.r, (const XT*)B.z, (const XT*)B.sh, (const XT*)B.s, (const XT*)B.t, st,
+                     lc.red()));
+      first = false;
+      ++launched;
+    }
+    CFD_TRY(pl.poll());
+    if (pl.host->done) break;
+    if (launched > pl.host->max_iter + 64) {
+      set_error("BiCGSTAB did not terminate within its iteration budget");
+      return CFD_ERR_TIMEOUT;
+    }
+    pl.next_chunk();
+  }
+  if (pl.host->spare0 != 0.0) {
+    // Converged on ||s||: x += alpha p_hat (the Krylov loop stopped before k_bicg_x).
+    CFD_TRY(lc.vec(n, k_axpy_state<XT>, B.x, (const XT*)B.z, (const DevState*)st));
+  }
+  return CFD_OK;
+}
+
+template <typename XT>
+static cfd_status krylov_loop(Launcher& lc, int solver, int pre, cfd_csr* a, cfd_amg* amg, KrylovBufs<XT>& B,
+                              DevState* st, Poller& pl) {
+  if (solver == CFD_SOLVER_BICGSTAB) {
+    if (pre == kPreJacobi) return bicgstab_loop<XT, kPreJacobi>(lc, a, amg, B, st, pl);
+    if (pre == kPreAmg) return bicgstab_loop<XT, kPreAmg>(lc, a, amg, B, st, pl);
+    return bicgstab_loop<XT, kPreNone>(lc, a, amg, B, st, pl);
+  }
+  if (pre == kPreJacobi) return pcg_loop<XT, kPreJacobi>(lc, a, amg, B, st, pl);
+  if (pre == kPreAmg) return pcg_loop<XT, kPreAmg>(lc, a, amg, B, st, pl);
+  return pcg_loop<XT, kPreNone>(lc, a, amg, B, st, pl);
+}
+
+// Stream-ordered workspace (the default memory pool keeps freed blocks for reuse).
+template <typename XT>
+struct Alloc {
+  cudaStream_t s;
+  std::vector<void*> ptrs;
+  XT* get(int64_t n) {
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, (size_t)std::max<int64_t>(n, 1) * sizeof(XT), s) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return (XT*)p;
+  }
+  ~Alloc() {
+    for (void* p : ptrs) cudaFreeAsync(p, s);
+  }
+};
+
+static void init_state(DevState& h, const cfd_solver_config& cfg) {
+  std::memset(&h, 0, sizeof(h));
+  h.tol_abs = cfg.tolerance;
+  h.tol_rel = cfg.relative_tolerance;
+  h.max_iter = (int32_t)std::min<int64_t>(cfg.max_iterations, INT32_MAX);
+  h.rho = h.alpha = h.omega = 1.0;
+  h.term = CFD_TERM_MAX_ITERATIONS;
+}
+
+cfd_status check_precond(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg) {
+  if (opt.precond == CFD_PRECOND_AMG) {
+    if (!amg) {
+      set_error("AMG preconditioner requested without an AMG handle");
+      return CFD_ERR_CONFIG;
+    }
+    if (amg->dev.empty() || amg->dev[0].A.nrows != a->dev.nrows) {
+      set_error("AMG hierarchy does not match the matrix (%lld rows)", (long long)a->dev.nrows);
+      return CFD_ERR_DIM;
+    }
+  }
+  if (opt.precond == CFD_PRECOND_JACOBI) {
+    CFD_TRY(ensure_diagonals(a));
+    if (a->jacobi_status != 0) {
+      set_error("Jacobi preconditioner: non-finite diagonal entry");
+      return CFD_ERR_NONFINITE;
+    }
+  }
+  return CFD_OK;
+}
+
+// Plain FP64 solve.
+cfd_status solve_fp64(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg, const double* b, double* x,
+                      const cfd_solver_config& cfg, cfd_solve_report& rep) {
+  cfd_context* ctx = a->ctx;
+  Launcher lc{ctx, ctx->stream};
+  const int64_t n = a->dev.nrows;
+  Alloc<double> al{ctx->stream, {}};
+  KrylovBufs<double> B{};
+  const bool host_mem = opt.memory == CFD_MEMORY_HOST;
+  B.x = host_mem ? al.get(n) : x;
+  B.b = host_mem ? al.get(n) : const_cast<double*>(b);
+  B.r = al.get(n);
+  B.p = al.get(n);
+  B.q = al.get(n);
+  B.z = al.get(n);
+  if (opt.solver == CFD_SOLVER_BICGSTAB) {
+    B.rh = al.get(n);
+    B.v = al.get(n);
+    B.s = al.get(n);
+    B.sh = al.get(n);
+    B.t = al.get(n);
+  }
+  if (!B.x || !B.b || !B.r || !B.p || !B.q || !B.z || (opt.solver == CFD_SOLVER_BICGSTAB && !B.t)) {
+    set_error("device workspace allocation failed (%lld unknowns)", (long long)n);
+    return CFD_ERR_ALLOC;
+  }
+  DevState* st = ctx->state;
+  DevState* hs = ctx->h_state;
+  init_state(*hs, cfg);
+  CFD_TRY_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  if (host_mem) {
+    CFD_TRY_CUDA(cudaMemcpyAsync(B.b, b, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CFD_TRY_CUDA(cudaMemcpyAsync(B.x, x, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  CFD_TRY_CUDA(cudaMemcpyAsync(st, hs, sizeof(DevState), cudaMemcpyHostToDevice, ctx->stream));
+  if (opt.solver == CFD_SOLVER_BICGSTAB) {
+    CFD_TRY_CUDA(cudaMemsetAsync(B.v, 0, n * sizeof(double), ctx->stream));
+    CFD_TRY_CUDA(cudaMemsetAsync(B.p, 0, n * sizeof(double), ctx->stream));
+  }
+  // r0 = b - A x0, ||r0||, threshold, InitialResidual test.
+  CFD_TRY(lc.spmv<double, double, false>(a->dev, B.x, EpiResidual<double, 1>{B.r, B.b, st, nullptr, {}}));
+  Poller pl{ctx, st, hs};
+  pl.fixed = opt.check_every;
+  CFD_TRY(krylov_loop<double>(lc, opt.solver, opt.precond, a, amg, B, st, pl));
+  if (host_mem) CFD_TRY_CUDA(cudaMemcpyAsync(x, B.x, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CFD_TRY_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  CFD_TRY(pl.poll());
+  float ms = 0.f;
+  CFD_TRY_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  rep.termination = hs->term;
+  rep.outer_iterations = 0;
+  rep.iterations = hs->iter;
+  rep.initial_residual = hs->rnorm0;
+  rep.final_residual = hs->rnorm;
+  rep.threshold = hs->threshold;
+  rep.device_ms = ms;
+  return CFD_OK;
+}
+
+// FP32 inner Krylov/AMG solves inside FP64 iterative refinement. FP64 is kept
+// for the outer residual r = b - A x, the solution accumulation, the reduction
+// accumulators and the coarsest-level solve.
+cfd_status solve_refine(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg, const double* b, double* x,
+                        const cfd_solver_config& cfg, cfd_solve_report& rep) {
+  cfd_context* ctx = a->ctx;
+  Launcher lc{ctx, ctx->stream};
+  const int64_t n = a->dev.nrows;
+  CFD_TRY(devmat_ensure32(a->dev, ctx->stream));
+  if (opt.precond == CFD_PRECOND_AMG) CFD_TRY(amg_ensure32(amg));
+  Alloc<double> ad{ctx->stream, {}};
+  Alloc<float> af{ctx->stream, {}};
+  const bool host_mem = opt.memory == CFD_MEMORY_HOST;
+  double* x64 = host_mem ? ad.get(n) : x;
+  double* b64 = host_mem ? ad.get(n) : const_cast<double*>(b);
+  double* r64 = ad.get(n);
+  KrylovBufs<float> B{};
+  B.x = af.get(n);
+  B.r = af.get(n);
+  B.p = af.get(n);
+  B.q = af.get(n);
+  B.z = af.get(n);
+  if (opt.solver == CFD_SOLVER_BICGSTAB) {
+    B.rh = af.get(n);
+    B.v = af.get(n);
+    B.s = af.get(n);
+    B.sh = af.get(n);
+    B.t = af.get(n);
+  }
+  if (!x64 || !b64 || !r64 || !B.x || !B.r || !B.p || !B.q || !B.z ||
+      (opt.solver == CFD_SOLVER_BICGSTAB && !B.t)) {
+    set_error("device workspace allocation failed (%lld unknowns)", (long long)n);
+    return CFD_ERR_ALLOC;
+  }
+  DevState* outer = ctx->state;
+  DevState* inner = ctx->state + 1;
+  DevState* hs = ctx->h_state;
+  init_state(hs[0], cfg);
+  cfd_solver_config icfg = cfg;
+  icfg.tolerance = 0.0;
+  icfg.relative_tolerance = opt.inner_tolerance > 0 ? opt.inner_tolerance : 1e-4;
+  init_state(hs[1], icfg);
+  CFD_TRY_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  if (host_mem) {
+    CFD_TRY_CUDA(cudaMemcpyAsync(b64, b, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CFD_TRY_CUDA(cudaMemcpyAsync(x64, x, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  CFD_TRY_CUDA(cudaMemcpyAsync(ctx->state, hs, 2 * sizeof(DevState), cudaMemcpyHostToDevice, ctx->stream));
+  CFD_TRY(lc.spmv<double, double, false>(a->dev, x64, EpiResidual<double, 1>{r64, b64, outer, nullptr, {}}));
+  Poller pl_out{ctx, outer, hs};
+  CFD_TRY(pl_out.poll());
+  const double r0 = hs[0].rnorm0, thr = hs[0].threshold;
+  int term = hs[0].term;
+  double rn = hs[0].rnorm;
+  int64_t inner_iters = 0;
+  int outer_steps = 0;
+  const int max_outer = opt.max_outer > 0 ? opt.max_outer : 20;
+  while (!hs[0].done) {
+    if (outer_steps >= max_outer || inner_iters >= cfg.max_iterations) {
+      term = CFD_TERM_MAX_ITERATIONS;
+      break;
+    }
+    // inner budget: what is left of the outer one
+    hs[1].max_iter = (int32_t)std::min<int64_t>(cfg.max_iterations - inner_iters, INT32_MAX);
+    CFD_TRY_CUDA(cudaMemcpyAsync(&inner->max_iter, &hs[1].max_iter, sizeof(int32_t), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    CFD_TRY(lc.vec(n, k_refine_start, (const double*)r64, B.r, B.x, (const DevState*)outer, inner, lc.red()));
+    Poller pl{ctx, inner, hs + 1};
+    pl.fixed = opt.check_every;
+    pl.poll();
+    CFD_TRY(krylov_loop<float>(lc, opt.solver, opt.precond, a, amg, B, inner, pl));
+    inner_iters += hs[1].iter;
+    ++outer_steps;
+    const int iterm = hs[1].term;
+    CFD_TRY(lc.vec(n, k_refine_accumulate, x64, (const float*)B.x, (const DevState*)outer));
+    // outer FP64 residual and convergence test
+    CFD_TRY(lc.spmv<double, double, false>(a->dev, x64, EpiResidual<double, 2>{r64, b64, outer, nullptr, {}}));
+    CFD_TRY(pl_out.poll());
+    rn = hs[0].rnorm;
+    if (!std::isfinite(rn)) {
+      term = CFD_TERM_BREAKDOWN;
+      break;
+    }
+    if (rn <= thr) {
+      term = CFD_TERM_CONVERGED;
+      break;
+    }
+    if (iterm == CFD_TERM_BREAKDOWN || iterm == CFD_TERM_NON_POSITIVE_CURVATURE) {
+      term = iterm;
+      break;
+    }
+  }
+  if (host_mem) CFD_TRY_CUDA(cudaMemcpyAsync(x, x64, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CFD_TRY_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  CFD_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+  float ms = 0.f;
+  CFD_TRY_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  rep.termination = term;
+  rep.outer_iterations = outer_steps;
+  rep.iterations = inner_iters;
+  rep.initial_residual = r0;
+  rep.final_residual = rn;
+  rep.threshold = thr;
+  rep.device_ms = ms;
+  return CFD_OK;
+}
+
+// Standalone preconditioner application z = M^-1 r (FP64).
+cfd_status amg_apply_fp64(cfd_amg* amg, const double* r, double* z) {
+  cfd_context* ctx = amg->ctx;
+  Launcher lc{ctx, ctx->stream};
+  return vcycle<double>(lc, amg, 0, r, z, 0, nullptr, nullptr);
+}
+
+cfd_status spmv_fp64(cfd_csr* a, const double* x, double* y) {
+  Launcher lc{a->ctx, a->ctx->stream};
+  return lc.spmv<double, double, false>(a->dev, x, EpiStore<double>{y, nullptr, {}});
+}
+
+cfd_status spmv_fp32(cfd_csr* a, const float* x, float* y) {
+  CFD_TRY(devmat_ensure32(a->dev, a->ctx->stream));
+  Launcher lc{a->ctx, a->ctx->stream};
+  return lc.spmv<float, float, false>(a->dev, x, EpiStore<float>{y, nullptr, {}});
+}
+
+}  // namespace cfd

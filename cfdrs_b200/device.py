@@ -1,0 +1,119 @@
+"""Device handles: the CUDA context/stream (``cfd_context``) and device CSR
+matrices (``cfd_csr``), with the upload cached per host matrix so repeated
+solves on one pattern pay it once (the reference borrows the matrix per call,
+``krylov.rs:330``)."""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+import weakref
+
+import numpy as np
+
+from . import _lib
+from .sparse import CsrMatrix
+
+_contexts: dict[int, "Context"] = {}
+# cudaStreamLegacy: the handle value CUDA reserves for the legacy default stream.
+LEGACY_STREAM = 0x1
+_ctx_lock = threading.Lock()
+
+
+class Context:
+    """One device and one CUDA stream (``cfd_context``)."""
+
+    def __init__(self, device: int = 0):
+        L = _lib.load()
+        h = C.c_void_p()
+        _lib.check(L.cfd_context_create(device, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        """Run this context's work on an existing CUDA stream (e.g. torch's);
+        ``None`` returns to the context's own stream. Handle 0 is CUDA's legacy
+        default stream (torch's default stream) and is passed on as such."""
+        if stream_ptr is None:
+            arg = None
+        elif stream_ptr == 0:
+            arg = LEGACY_STREAM
+        else:
+            arg = stream_ptr
+        _lib.check(_lib.load().cfd_context_set_stream(self.h, C.c_void_p(arg)))
+
+    def synchronize(self) -> None:
+        _lib.check(_lib.load().cfd_context_synchronize(self.h))
+
+    def kernel_stats(self) -> dict:
+        s = _lib.KernelStatsC()
+        _lib.check(_lib.load().cfd_last_kernel_stats(self.h, C.byref(s)))
+        return {"launches": s.launches, "spmv_launches": s.spmv_launches, "spmv_bytes": s.spmv_bytes}
+
+    def close(self) -> None:
+        if self.h:
+            _lib.load().cfd_context_destroy(self.h)
+            self.h = None
+
+
+def context(device: int = 0) -> Context:
+    """The process-wide context of ``device`` (created on first use)."""
+    with _ctx_lock:
+        ctx = _contexts.get(device)
+        if ctx is None:
+            ctx = Context(device)
+            _contexts[device] = ctx
+        return ctx
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class DeviceCsr:
+    """A CSR matrix resident on the device (``cfd_csr``)."""
+
+    def __init__(self, m: CsrMatrix, ctx: Context | None = None):
+        self.ctx = ctx or context()
+        self.shape = m.shape
+        self.nnz = m.nnz
+        h = C.c_void_p()
+        rp = np.ascontiguousarray(m.row_ptr, dtype=np.int64)
+        col = np.ascontiguousarray(m.col, dtype=np.int32)
+        val = np.ascontiguousarray(m.val, dtype=np.float64)
+        _lib.check(_lib.load().cfd_csr_create_i32(self.ctx.h, m.nrows, m.ncols, m.nnz, _ptr(rp), _ptr(col),
+                                                  _ptr(val), C.byref(h)))
+        self.h = h
+
+    def update_values(self, values) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        if v.shape[0] != self.nnz:
+            raise ValueError("value array must match nnz")
+        _lib.check(_lib.load().cfd_csr_update_values(self.h, _ptr(v)))
+
+    def spmv(self, x_dev_ptr: int, y_dev_ptr: int, fp32: bool = False) -> None:
+        """y = A x on device pointers."""
+        fn = _lib.load().cfd_spmv_f32 if fp32 else _lib.load().cfd_spmv
+        _lib.check(fn(self.h, C.c_void_p(x_dev_ptr), C.c_void_p(y_dev_ptr)))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            try:
+                _lib.load().cfd_csr_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+
+_uploads: "weakref.WeakKeyDictionary[CsrMatrix, DeviceCsr]" = weakref.WeakKeyDictionary()
+
+
+def device_matrix(m, ctx: Context | None = None) -> DeviceCsr:
+    """Upload ``m`` once and reuse the device copy while ``m`` is alive."""
+    if isinstance(m, DeviceCsr):
+        return m
+    d = _uploads.get(m)
+    if d is None or (ctx is not None and d.ctx is not ctx):
+        d = DeviceCsr(m, ctx)
+        _uploads[m] = d
+    return d

@@ -1,0 +1,271 @@
+"""Seeded host-side CSR assembly for the pressure / Kirchhoff systems the
+CFDrs callers hand to cfd-math's Krylov solvers.
+
+Every generator returns a :class:`~cfdrs_b200.sparse.CsrMatrix` (int64 row
+offsets, int32 column indices sorted within each row, float64 values) plus the
+right-hand side. The matrices are scaled so their entries are O(1); relative
+residuals are invariant under that scaling.
+
+Reference semantics restated here:
+
+* 2-D pressure Poisson (``poisson_2d_dirichlet``): the 5-point assembly of
+  ``crates/cfd-2d/src/pressure_velocity/correction.rs:273-330`` -- off-diagonal
+  ``-1/h^2`` toward each interior neighbour, and a Dirichlet wall adds ``1/h^2``
+  to the diagonal (``:295-311``). Rows are ``x``-major,
+  ``idx = (i-1)*(ny-2) + (j-1)`` (``:281``).
+* 3-D / 2-D variable-coefficient finite-volume Poisson ``-div(k grad p) = f``:
+  face coefficient is the harmonic mean ``2 k_P k_E / (k_P + k_E)``
+  (``crates/cfd-2d/src/pressure_velocity/rhie_chow.rs:155``); a Dirichlet face
+  at half a cell from the centre contributes ``2 k_P`` to the diagonal.
+* Kirchhoff networks (``kirchhoff_network``): the grounded conductance
+  Laplacian of ``crates/cfd-1d/src/solver/core/matrix_assembly.rs:163-250``
+  (Dirichlet column elimination into the RHS, identity rows for fixed nodes),
+  with Hagen-Poiseuille conductance ``g = pi d^4 / (128 mu L)``
+  (``crates/cfd-1d/src/physics/resistance/models/bahrami_universal.rs:64``).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .sparse import CsrMatrix
+
+
+def _uniform_rhs(n: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return rng.uniform(-1.0, 1.0, size=n)
+
+
+def _stencil_csr(n_rows: int, offsets: list[int], vals: np.ndarray, mask: np.ndarray) -> CsrMatrix:
+    """Assemble CSR from per-row stencil columns ``row + offsets[q]`` (ascending)."""
+    counts = mask.sum(axis=1, dtype=np.int64)
+    row_ptr = np.zeros(n_rows + 1, dtype=np.int64)
+    np.cumsum(counts, out=row_ptr[1:])
+    rows = np.arange(n_rows, dtype=np.int64)
+    cols = np.empty(mask.shape, dtype=np.int32)
+    for q, off in enumerate(offsets):
+        cols[:, q] = (rows + off).astype(np.int32, copy=False) if n_rows < 2**31 else rows + off
+    col = cols[mask]
+    val = vals[mask]
+    return CsrMatrix(row_ptr, col, val, (n_rows, n_rows))
+
+
+def poisson_2d_dirichlet(nx: int, ny: int | None = None, seed: int = 0):
+    """2-D pressure Poisson on an ``nx x ny`` cell grid, homogeneous Dirichlet on
+    all four walls, scaled by ``h^2`` (diagonal 4, off-diagonals -1).
+
+    Returns ``(A, b)`` with ``b ~ U[-1, 1]`` i.i.d. from ``seed``.
+    """
+    ny = nx if ny is None else ny
+    n = nx * ny
+    i = np.arange(n, dtype=np.int64) // ny  # x index
+    j = np.arange(n, dtype=np.int64) % ny   # y index
+    offsets = [-ny, -1, 0, 1, ny]
+    mask = np.ones((n, 5), dtype=bool)
+    vals = np.full((n, 5), -1.0)
+    mask[:, 0] = i > 0
+    mask[:, 1] = j > 0
+    mask[:, 3] = j < ny - 1
+    mask[:, 4] = i < nx - 1
+    # Diagonal: interior neighbours plus 1 per Dirichlet wall (correction.rs:295-311)
+    # gives 4 in every row on a uniform grid.
+    vals[:, 2] = 4.0
+    return _stencil_csr(n, offsets, vals, mask), _uniform_rhs(n, seed)
+
+
+def poisson_3d_fv(n: int, k: np.ndarray | None = None, seed: int = 0,
+                  dirichlet_x: bool = True):
+    """Cell-centred 7-point finite-volume ``-div(k grad p) = f`` on an ``n^3``
+    grid (row index ``i + n*j + n^2*l``, ``i`` along x), scaled by ``1/h``.
+
+    Faces carry the harmonic mean of the two cell coefficients. Dirichlet
+    (``p = 0``) on the x = 0 and x = 1 faces contributes ``2 k_P``; all other
+    faces are Neumann (no flux). ``k=None`` means ``k = 1``.
+    """
+    N = n ** 3
+    if k is None:
+        kk = np.ones((n, n, n))
+    else:
+        kk = np.asarray(k, dtype=np.float64).reshape(n, n, n)  # [l, j, i]
+    def hmean(a, b):
+        return 2.0 * a * b / (a + b)
+    # Face coefficients along each axis, stored on the lower cell.
+    fx = hmean(kk[:, :, :-1], kk[:, :, 1:])   # (n, n, n-1) faces between i and i+1
+    fy = hmean(kk[:, :-1, :], kk[:, 1:, :])
+    fz = hmean(kk[:-1, :, :], kk[1:, :, :])
+    offsets = [-n * n, -n, -1, 0, 1, n, n * n]
+    vals = np.zeros((n, n, n, 7))
+    mask = np.zeros((n, n, n, 7), dtype=bool)
+    vals[1:, :, :, 0] = -fz
+    mask[1:, :, :, 0] = True
+    vals[:, 1:, :, 1] = -fy
+    mask[:, 1:, :, 1] = True
+    vals[:, :, 1:, 2] = -fx
+    mask[:, :, 1:, 2] = True
+    vals[:, :, :-1, 4] = -fx
+    mask[:, :, :-1, 4] = True
+    vals[:, :-1, :, 5] = -fy
+    mask[:, :-1, :, 5] = True
+    vals[:-1, :, :, 6] = -fz
+    mask[:-1, :, :, 6] = True
+    diag = -(vals[..., 0] + vals[..., 1] + vals[..., 2] + vals[..., 4] + vals[..., 5] + vals[..., 6])
+    if dirichlet_x:
+        diag[:, :, 0] += 2.0 * kk[:, :, 0]
+        diag[:, :, -1] += 2.0 * kk[:, :, -1]
+    vals[..., 3] = diag
+    mask[..., 3] = True
+    A = _stencil_csr(N, offsets, vals.reshape(N, 7), mask.reshape(N, 7))
+    return A, _uniform_rhs(N, seed)
+
+
+def gaussian_random_field(shape: tuple[int, ...], corr_len: float, sigma: float,
+                          seed: int) -> np.ndarray:
+    """Seeded stationary Gaussian random field with squared-exponential
+    covariance ``sigma^2 exp(-r^2 / (2 corr_len^2))`` (lengths in cells), by
+    spectral synthesis on the periodic box: white noise filtered by the square
+    root of the spectral density ``exp(-|kappa|^2 corr_len^2 / 2)``, then
+    normalised to zero mean and standard deviation ``sigma``.
+    """
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal(shape)
+    W = np.fft.rfftn(w)
+    k2 = np.zeros(W.shape)
+    for ax, m in enumerate(shape):
+        if ax == len(shape) - 1:
+            f = np.fft.rfftfreq(m)
+        else:
+            f = np.fft.fftfreq(m)
+        kap = 2.0 * np.pi * f
+        sh = [1] * len(shape)
+        sh[ax] = W.shape[ax]
+        k2 = k2 + (kap ** 2).reshape(sh)
+    W *= np.exp(-0.25 * k2 * corr_len ** 2)
+    g = np.fft.irfftn(W, s=shape, axes=tuple(range(len(shape))))
+    g -= g.mean()
+    g *= sigma / g.std()
+    return g
+
+
+def poisson_3d_variable(n: int, corr_len: float = 8.0, sigma: float = 1.0, seed: int = 0):
+    """3-D variable-coefficient Poisson with ``k = exp(g)``, ``g`` a seeded GRF.
+
+    Returns ``(A, b, k)``.
+    """
+    g = gaussian_random_field((n, n, n), corr_len, sigma, seed + 1)
+    k = np.exp(g)
+    A, b = poisson_3d_fv(n, k, seed=seed)
+    return A, b, k
+
+
+def darcy_2d(theta: np.ndarray):
+    """2-D ``-div(exp(theta) grad p) = 0`` on an ``n x n`` cell grid (row index
+    ``i + n*j``, ``i`` along x): Dirichlet ``p = 1`` on the left wall and ``p = 0``
+    on the right wall (half-cell faces, ``2 k_P``), no flux top and bottom.
+
+    Returns ``(A, b)``; ``b`` carries the left-wall Dirichlet flux ``2 k_P * 1``.
+    """
+    n = theta.shape[0]
+    kk = np.exp(np.asarray(theta, dtype=np.float64)).reshape(n, n)  # [j, i]
+    N = n * n
+    def hmean(a, b):
+        return 2.0 * a * b / (a + b)
+    fx = hmean(kk[:, :-1], kk[:, 1:])
+    fy = hmean(kk[:-1, :], kk[1:, :])
+    offsets = [-n, -1, 0, 1, n]
+    vals = np.zeros((n, n, 5))
+    mask = np.zeros((n, n, 5), dtype=bool)
+    vals[1:, :, 0] = -fy
+    mask[1:, :, 0] = True
+    vals[:, 1:, 1] = -fx
+    mask[:, 1:, 1] = True
+    vals[:, :-1, 3] = -fx
+    mask[:, :-1, 3] = True
+    vals[:-1, :, 4] = -fy
+    mask[:-1, :, 4] = True
+    diag = -(vals[..., 0] + vals[..., 1] + vals[..., 3] + vals[..., 4])
+    diag[:, 0] += 2.0 * kk[:, 0]
+    diag[:, -1] += 2.0 * kk[:, -1]
+    vals[..., 2] = diag
+    mask[..., 2] = True
+    b = np.zeros((n, n))
+    b[:, 0] = 2.0 * kk[:, 0] * 1.0
+    A = _stencil_csr(N, offsets, vals.reshape(N, 5), mask.reshape(N, 5))
+    return A, b.reshape(N)
+
+
+def kirchhoff_assemble(n_nodes: int, edges_i, edges_j, conductance, dirichlet: dict, neumann: dict | None = None):
+    """Grounded conductance Laplacian, ``MatrixAssembler::assemble_into``
+    (``crates/cfd-1d/src/solver/core/matrix_assembly.rs:163-250``): a free-free
+    edge adds the symmetric 2x2 Laplacian block; an edge to a Dirichlet node
+    adds to the free node's diagonal and moves ``g p_D`` to its RHS; Neumann
+    sources add to the RHS; Dirichlet nodes get identity rows with RHS ``p_D``.
+
+    Raises ``ValueError`` on self loops and non-finite or non-positive
+    conductances (``:184-203``). Returns ``(A, b)``.
+    """
+    import scipy.sparse as sp
+    ei = np.asarray(edges_i, dtype=np.int64)
+    ej = np.asarray(edges_j, dtype=np.int64)
+    g = np.asarray(conductance, dtype=np.float64)
+    if np.any(ei == ej):
+        raise ValueError("Self-loop edge detected in network assembly")
+    if not np.all(np.isfinite(g)):
+        raise ValueError("Non-finite conductance encountered in network assembly")
+    if np.any(g <= 0):
+        raise ValueError("Non-positive conductance encountered in network assembly")
+    is_dir = np.zeros(n_nodes, dtype=bool)
+    pval = np.zeros(n_nodes)
+    for node, p in dirichlet.items():
+        is_dir[int(node)] = True
+        pval[int(node)] = p
+    di, dj = is_dir[ei], is_dir[ej]
+    ff = ~di & ~dj
+    rows = [ei[ff], ej[ff], ei[ff], ej[ff], ej[di & ~dj], ei[~di & dj], np.flatnonzero(is_dir)]
+    cols = [ei[ff], ej[ff], ej[ff], ei[ff], ej[di & ~dj], ei[~di & dj], np.flatnonzero(is_dir)]
+    vals = [g[ff], g[ff], -g[ff], -g[ff], g[di & ~dj], g[~di & dj], np.ones(int(is_dir.sum()))]
+    b = np.zeros(n_nodes)
+    np.add.at(b, ej[di & ~dj], g[di & ~dj] * pval[ei[di & ~dj]])
+    np.add.at(b, ei[~di & dj], g[~di & dj] * pval[ej[~di & dj]])
+    for node, q in (neumann or {}).items():
+        b[int(node)] += q
+    b[is_dir] = pval[is_dir]
+    m = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(n_nodes, n_nodes)).tocsr()
+    m.sum_duplicates()
+    m.sort_indices()
+    return CsrMatrix(m.indptr, m.indices, m.data, m.shape), b
+
+
+def hagen_poiseuille_conductance(d, length, mu=1.0e-3):
+    """``g = pi d^4 / (128 mu L)``, the inverse of the Hagen-Poiseuille
+    resistance ``R = 128 mu L / (pi d^4)`` (``bahrami_universal.rs:64``)."""
+    return np.pi * np.asarray(d) ** 4 / (128.0 * mu * np.asarray(length))
+
+
+def random_network(n_nodes: int, rng: np.random.Generator, loop_fraction: float = 0.1,
+                   p_in: float = 1000.0, p_out: float = 0.0):
+    """Seeded pipe network: a random spanning tree (node i attaches to a uniform
+    j < i) plus ``floor(loop_fraction * n)`` extra distinct edges; diameters
+    U[50, 500] um, lengths U[1, 20] mm, mu = 1e-3 Pa s; node 0 fixed at ``p_in``,
+    node n-1 at ``p_out``. Returns ``(A, b)`` from :func:`kirchhoff_assemble`."""
+    n = int(n_nodes)
+    parent = np.array([rng.integers(0, i) for i in range(1, n)], dtype=np.int64)
+    ei = list(parent)
+    ej = list(range(1, n))
+    seen = set(zip(np.minimum(ei, ej).tolist(), np.maximum(ei, ej).tolist()))
+    extra = int(np.floor(loop_fraction * n))
+    while extra > 0:
+        a, c = (int(v) for v in rng.integers(0, n, size=2))
+        if a == c:
+            continue
+        key = (min(a, c), max(a, c))
+        if key in seen:
+            continue
+        seen.add(key)
+        ei.append(key[0])
+        ej.append(key[1])
+        extra -= 1
+    m = len(ei)
+    d = rng.uniform(50e-6, 500e-6, size=m)
+    length = rng.uniform(1e-3, 20e-3, size=m)
+    g = hagen_poiseuille_conductance(d, length)
+    return kirchhoff_assemble(n, ei, ej, g, {0: p_in, n - 1: p_out})

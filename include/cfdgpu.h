@@ -1,0 +1,199 @@
+/*
+ * cfdgpu.h -- C ABI of the B200 (sm_100a) sparse linear-solve library that
+ * stands in for cfd-math's Krylov / preconditioner surface of CFDrs.
+ *
+ * Plain pointers and sizes only. Every entry point returns a cfd_status; a
+ * human-readable message for the last failure on the calling thread is
+ * available from cfd_last_error(). Numerical end states (converged, stalled,
+ * broken down) are NOT errors: they are reported in cfd_solve_report, as the
+ * reference reports them value-semantically (krylov.rs:362-401).
+ *
+ * Reference interfaces replaced (paths relative to the CFDrs repository):
+ *   cfd_solve                krylov::cg_preconditioned       crates/cfd-math/src/linear_solver/krylov.rs:318-343
+ *                            krylov::bicgstab_preconditioned  krylov.rs:253-278
+ *                            krylov::cg / krylov::bicgstab    krylov.rs:350-360 / :285-308
+ *                            SolverKind::solve[_preconditioned] krylov.rs:562-612
+ *   cfd_solver_config        IterativeSolverConfig -> convergence_policy, krylov.rs:123-139
+ *   cfd_solve_report         athena SolveReport{termination, iterations, initial_residual_norm,
+ *                            final_residual_norm, threshold} (fields read at krylov.rs:486, 509-512)
+ *   cfd_termination          athena Termination as mapped by krylov::interpret, krylov.rs:385-399
+ *   cfd_csr_create           leto_ops::CsrMatrix::from_parts (e.g. krylov.rs:467), the borrowed
+ *                            BorrowedCsrOperator of krylov.rs:330
+ *   cfd_csr_update_values    same pattern, new values (the input of AlgebraicMultigrid::recompute)
+ *   cfd_spmv                 leto_ops::spmv_into, wrapped at crates/cfd-math/src/sparse/operations.rs:50-79
+ *   cfd_amg_config           AMGConfig, crates/cfd-math/src/linear_solver/preconditioners/multigrid/mod.rs:219-259
+ *   cfd_amg_setup            AlgebraicMultigrid::new, .../multigrid/amg.rs:133-146
+ *   cfd_amg_recompute        AlgebraicMultigrid::recompute, amg.rs:179-214
+ *   cfd_amg_apply            Preconditioner::apply_to (z = 0, one V-cycle), amg.rs:507-557
+ *   cfd_amg_stats            AMGStatistics, multigrid/mod.rs:366-395
+ *   cfd_jacobi_*             DiagJacobi, crates/cfd-1d/src/solver/core/linear_system.rs:270-332
+ *   cfd_batch_solve          LinearSystemSolver::solve_with_initial_guess called once per network
+ *                            (crates/cfd-1d/src/solver/core/linear_system.rs:114-155) by the
+ *                            cfd-optim candidate fold (crates/cfd-optim/src/metrics/blueprint_graph.rs:48-135)
+ *   cfd_adjoint_*            no reference counterpart (new differentiable-solve layer; see each entry)
+ */
+#ifndef CFDGPU_H
+#define CFDGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status / termination -------------------------------------------- */
+typedef enum {
+  CFD_OK = 0,
+  CFD_ERR_DIM = 1,       /* dimension / structure mismatch (Error::InvalidConfiguration) */
+  CFD_ERR_CONFIG = 2,    /* invalid solver / AMG configuration (convergence_policy rejection) */
+  CFD_ERR_CUDA = 3,      /* CUDA runtime failure */
+  CFD_ERR_TIMEOUT = 4,   /* a bounded device wait ran out */
+  CFD_ERR_NONFINITE = 5, /* non-finite input (e.g. DiagJacobi::new on a non-finite diagonal) */
+  CFD_ERR_ALLOC = 6,     /* device or host allocation failed */
+  CFD_ERR_STATE = 7      /* handle used in the wrong state (e.g. recompute before setup) */
+} cfd_status;
+
+typedef enum {
+  CFD_TERM_CONVERGED = 0,
+  CFD_TERM_INITIAL_RESIDUAL = 1,
+  CFD_TERM_MAX_ITERATIONS = 2,        /* SolveOutcome::Stalled */
+  CFD_TERM_BREAKDOWN = 3,             /* SolveOutcome::BrokenDown */
+  CFD_TERM_NON_POSITIVE_CURVATURE = 4 /* SolveOutcome::BrokenDown */
+} cfd_termination;
+
+const char* cfd_last_error(void);
+const char* cfd_version(void);
+
+/* ---- context: one device + one stream ---------------------------------- */
+typedef struct cfd_context cfd_context;
+cfd_status cfd_context_create(int device, cfd_context** out);
+/* Run subsequent work of this context on an existing stream (e.g. torch's
+ * current stream); NULL restores the context's own stream. To run on CUDA's
+ * legacy default stream pass cudaStreamLegacy ((void*)0x1). */
+cfd_status cfd_context_set_stream(cfd_context* ctx, void* cuda_stream);
+cfd_status cfd_context_synchronize(cfd_context* ctx);
+cfd_status cfd_context_destroy(cfd_context* ctx);
+
+/* ---- device CSR -------------------------------------------------------- */
+typedef struct cfd_csr cfd_csr;
+/* Host arrays (row_ptr[nrows+1], col[nnz] sorted per row, val[nnz]); copied to
+ * the device. Indices must fit int32. */
+cfd_status cfd_csr_create(cfd_context* ctx, int64_t nrows, int64_t ncols, int64_t nnz,
+                          const int64_t* row_ptr, const int64_t* col, const double* val,
+                          cfd_csr** out);
+cfd_status cfd_csr_create_i32(cfd_context* ctx, int64_t nrows, int64_t ncols, int64_t nnz,
+                              const int64_t* row_ptr, const int32_t* col, const double* val,
+                              cfd_csr** out);
+cfd_status cfd_csr_update_values(cfd_csr* a, const double* val_host);
+cfd_status cfd_csr_info(const cfd_csr* a, int64_t* nrows, int64_t* ncols, int64_t* nnz);
+cfd_status cfd_csr_destroy(cfd_csr* a);
+
+/* y = A x on device pointers (FP64), or FP32 values/vectors (values cast once). */
+cfd_status cfd_spmv(cfd_csr* a, const double* x_dev, double* y_dev);
+cfd_status cfd_spmv_f32(cfd_csr* a, const float* x_dev, float* y_dev);
+
+/* ---- AMG preconditioner ------------------------------------------------ */
+typedef enum { CFD_COARSEN_RUGE_STUEBEN = 0, CFD_COARSEN_AGGREGATION = 1, CFD_COARSEN_PMIS = 2 } cfd_coarsening;
+/* CLASSICAL: the reference formula (interpolation.rs:38-188). MODIFIED_CLASSICAL:
+ * sign-restricted distribution with lumping of F-neighbours that share no
+ * C-point (robust on deep hierarchies). DIRECT: piecewise constant (:191-217). */
+typedef enum {
+  CFD_INTERP_CLASSICAL = 0,
+  CFD_INTERP_DIRECT = 1,
+  CFD_INTERP_MODIFIED_CLASSICAL = 2
+} cfd_interpolation;
+typedef enum { CFD_SMOOTH_JACOBI = 0 } cfd_smoother;
+typedef enum { CFD_COARSE_SWEEPS = 0, CFD_COARSE_DENSE = 1 } cfd_coarse_solve;
+
+typedef struct {
+  int32_t max_levels;          /* AMGConfig::max_levels (default 10) */
+  int32_t coarsening;          /* cfd_coarsening */
+  int64_t min_coarse_size;     /* AMGConfig::min_coarse_size (default 50) */
+  int32_t interpolation;       /* cfd_interpolation */
+  int32_t smoother;            /* cfd_smoother (damped Jacobi only on the device) */
+  int32_t pre_smooth;          /* AMGConfig::pre_smooth_iterations */
+  int32_t post_smooth;         /* AMGConfig::post_smooth_iterations */
+  double relaxation;           /* AMGConfig::relaxation_factor (omega) */
+  double strength_threshold;   /* AMGConfig::strength_threshold (theta) */
+  int32_t coarse_solve;        /* cfd_coarse_solve: reference sweeps (amg.rs:499-501) or dense FP64 */
+  int32_t coarse_sweeps;       /* sweeps for CFD_COARSE_SWEEPS (reference: 10) */
+  int64_t aggregate_size;      /* aggregation coarsening (reference passes 8, amg.rs:304) */
+  uint64_t seed;               /* PMIS priorities (the reference draws them unseeded) */
+} cfd_amg_config;
+
+void cfd_amg_config_default(cfd_amg_config* cfg);
+
+typedef struct {
+  int32_t num_levels;
+  int32_t pad;
+  int64_t level_rows[16];
+  int64_t level_nnz[16];
+  double operator_complexity;
+  double grid_complexity;
+  double setup_seconds;
+} cfd_amg_stats_t;
+
+typedef struct cfd_amg cfd_amg;
+cfd_status cfd_amg_setup(cfd_csr* a, const cfd_amg_config* cfg, cfd_amg** out);
+cfd_status cfd_amg_recompute(cfd_amg* amg, cfd_csr* a);
+/* z = M^-1 r (one V-cycle from z = 0), device pointers, FP64. */
+cfd_status cfd_amg_apply(cfd_amg* amg, const double* r_dev, double* z_dev);
+cfd_status cfd_amg_stats(const cfd_amg* amg, cfd_amg_stats_t* out);
+/* Copy level `level`'s operator (which: 0 = A_l, 1 = P_l, 2 = R_l) to host
+ * arrays; pass NULL arrays to query sizes only. */
+cfd_status cfd_amg_level(const cfd_amg* amg, int level, int which, int64_t* nrows, int64_t* ncols,
+                         int64_t* nnz, int64_t* row_ptr, int64_t* col, double* val);
+cfd_status cfd_amg_destroy(cfd_amg* amg);
+
+/* ---- Krylov solve ------------------------------------------------------ */
+typedef enum { CFD_SOLVER_CG = 0, CFD_SOLVER_BICGSTAB = 1 } cfd_solver_kind;
+typedef enum { CFD_PRECOND_NONE = 0, CFD_PRECOND_JACOBI = 1, CFD_PRECOND_AMG = 2 } cfd_precond_kind;
+typedef enum { CFD_PRECISION_FP64 = 0, CFD_PRECISION_FP32_REFINE = 1 } cfd_precision;
+typedef enum { CFD_MEMORY_HOST = 0, CFD_MEMORY_DEVICE = 1 } cfd_memory;
+
+typedef struct {
+  double tolerance;           /* IterativeSolverConfig::tolerance (absolute) */
+  double relative_tolerance;  /* IterativeSolverConfig::relative_tolerance (vs ||r0||) */
+  int64_t max_iterations;     /* IterativeSolverConfig::max_iterations */
+} cfd_solver_config;
+
+typedef struct {
+  int32_t solver;           /* cfd_solver_kind */
+  int32_t precond;          /* cfd_precond_kind */
+  int32_t precision;        /* cfd_precision */
+  int32_t memory;           /* cfd_memory: b and x are host or device pointers */
+  double inner_tolerance;   /* FP32 inner relative tolerance (refinement), e.g. 1e-4 */
+  int32_t max_outer;        /* refinement steps cap */
+  int32_t check_every;      /* device iterations between host convergence polls (0 = auto) */
+} cfd_solve_options;
+
+void cfd_solve_options_default(cfd_solve_options* opt);
+
+typedef struct {
+  int32_t termination;      /* cfd_termination */
+  int32_t outer_iterations; /* refinement steps (0 for plain FP64) */
+  int64_t iterations;       /* Krylov iterations (summed over refinement steps) */
+  double initial_residual;  /* ||b - A x0||_2 */
+  double final_residual;    /* FP64: recurrence residual; FP32_REFINE: true FP64 residual */
+  double threshold;         /* max(tolerance, relative_tolerance * ||r0||) */
+  double device_ms;         /* device time of the solve (CUDA events) */
+} cfd_solve_report;
+
+/* Solve A x = b; x carries the initial guess in and the solution out.
+ * amg must be non-NULL when opt->precond == CFD_PRECOND_AMG. */
+cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, const double* b,
+                     double* x, const cfd_solver_config* cfg, cfd_solve_report* rep);
+
+/* ---- per-kernel statistics of the last solve --------------------------- */
+typedef struct {
+  int64_t launches;         /* kernels launched by the library in the last cfd_solve */
+  int64_t spmv_launches;
+  double spmv_bytes;        /* algorithmic bytes moved by SpMV kernels in the last solve */
+} cfd_kernel_stats;
+cfd_status cfd_last_kernel_stats(cfd_context* ctx, cfd_kernel_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFDGPU_H */

@@ -1,0 +1,1010 @@
+// CPU oracle: plain restatement of the CFDrs FP64 sparse-solve path.
+// Test infrastructure only -- see oracle.h for scope and the reference map.
+#include "oracle.h"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+struct or_csr {
+  int64_t nrows = 0, ncols = 0;
+  std::vector<int64_t> rp, ci;
+  std::vector<double> v;
+  int64_t nnz() const { return (int64_t)ci.size(); }
+};
+
+namespace {
+
+// diagonal_epsilon() in multigrid/amg.rs:58-61 and smoothers.rs (|diag| > 1e-15).
+constexpr double kDiagEps = 1e-15;
+
+double dot(int64_t n, const double* a, const double* b) {
+  double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+  for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+  return s;
+}
+
+void spmv_raw(const or_csr& a, const double* x, double* y) {
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < a.nrows; ++i) {
+    double s = 0.0;
+    for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k) s += a.v[k] * x[a.ci[k]];
+    y[i] = s;
+  }
+}
+
+// csr_value (multigrid/mod.rs:205-215): binary search of column col in row.
+double csr_value(const or_csr& a, int64_t row, int64_t col) {
+  const int64_t* b = a.ci.data() + a.rp[row];
+  const int64_t* e = a.ci.data() + a.rp[row + 1];
+  const int64_t* it = std::lower_bound(b, e, col);
+  if (it != e && *it == col) return a.v[a.rp[row] + (it - b)];
+  return 0.0;
+}
+
+[[maybe_unused]] bool row_has(const or_csr& a, int64_t row, int64_t col) {
+  const int64_t* b = a.ci.data() + a.rp[row];
+  const int64_t* e = a.ci.data() + a.rp[row + 1];
+  return std::binary_search(b, e, col);
+}
+
+or_csr transpose(const or_csr& a) {
+  or_csr t;
+  t.nrows = a.ncols;
+  t.ncols = a.nrows;
+  t.rp.assign(t.nrows + 1, 0);
+  for (int64_t k = 0; k < a.nnz(); ++k) t.rp[a.ci[k] + 1]++;
+  for (int64_t i = 0; i < t.nrows; ++i) t.rp[i + 1] += t.rp[i];
+  t.ci.resize(a.nnz());
+  t.v.resize(a.nnz());
+  std::vector<int64_t> pos(t.rp.begin(), t.rp.end() - 1);
+  for (int64_t i = 0; i < a.nrows; ++i)
+    for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k) {
+      int64_t p = pos[a.ci[k]]++;
+      t.ci[p] = i;
+      t.v[p] = a.v[k];
+    }
+  return t;
+}
+
+// Gustavson row-by-row product; columns of each output row sorted, structural
+// zeros kept (the product pattern is the symbolic pattern).
+or_csr spgemm(const or_csr& a, const or_csr& b) {
+  or_csr c;
+  c.nrows = a.nrows;
+  c.ncols = b.ncols;
+  c.rp.assign(a.nrows + 1, 0);
+  int nt = omp_get_max_threads();
+  std::vector<std::vector<int64_t>> rows_ci(a.nrows);
+  std::vector<std::vector<double>> rows_v(a.nrows);
+#pragma omp parallel num_threads(nt)
+  {
+    std::vector<int64_t> marker(b.ncols, -1);
+    std::vector<double> acc(b.ncols, 0.0);
+    std::vector<int64_t> cols;
+#pragma omp for schedule(dynamic, 1024)
+    for (int64_t i = 0; i < a.nrows; ++i) {
+      cols.clear();
+      for (int64_t ka = a.rp[i]; ka < a.rp[i + 1]; ++ka) {
+        int64_t k = a.ci[ka];
+        double av = a.v[ka];
+        for (int64_t kb = b.rp[k]; kb < b.rp[k + 1]; ++kb) {
+          int64_t j = b.ci[kb];
+          if (marker[j] != i) {
+            marker[j] = i;
+            acc[j] = av * b.v[kb];
+            cols.push_back(j);
+          } else {
+            acc[j] += av * b.v[kb];
+          }
+        }
+      }
+      std::sort(cols.begin(), cols.end());
+      rows_ci[i] = cols;
+      rows_v[i].resize(cols.size());
+      for (size_t q = 0; q < cols.size(); ++q) rows_v[i][q] = acc[cols[q]];
+    }
+  }
+  for (int64_t i = 0; i < a.nrows; ++i) c.rp[i + 1] = c.rp[i] + (int64_t)rows_ci[i].size();
+  c.ci.resize(c.rp[a.nrows]);
+  c.v.resize(c.rp[a.nrows]);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < a.nrows; ++i) {
+    std::copy(rows_ci[i].begin(), rows_ci[i].end(), c.ci.begin() + c.rp[i]);
+    std::copy(rows_v[i].begin(), rows_v[i].end(), c.v.begin() + c.rp[i]);
+  }
+  return c;
+}
+
+// compute_strength_matrix, coarsening/algorithms.rs:395-436.
+or_csr strength(const or_csr& a, double theta) {
+  or_csr s;
+  s.nrows = a.nrows;
+  s.ncols = a.nrows;
+  s.rp.assign(a.nrows + 1, 0);
+  for (int64_t i = 0; i < a.nrows; ++i) {
+    double mx = 0.0;
+    for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k)
+      if (a.ci[k] != i) {
+        double val = std::fabs(a.v[k]);
+        mx = mx > val ? mx : val;
+      }
+    for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k)
+      if (a.ci[k] != i) {
+        double st = std::fabs(a.v[k]);
+        if (st >= theta * mx) {
+          s.ci.push_back(a.ci[k]);
+          s.v.push_back(st);
+        }
+      }
+    s.rp[i + 1] = (int64_t)s.ci.size();
+  }
+  return s;
+}
+
+// assign_closest_coarse_points, coarsening/algorithms.rs:199-230.
+void assign_closest(std::vector<int64_t>& f2c, const std::vector<int>& status, const or_csr& s) {
+  for (int64_t i = 0; i < s.nrows; ++i) {
+    if (f2c[i] >= 0) continue;
+    double best = 0.0;
+    int64_t best_idx = -1;
+    bool have = false;
+    for (int64_t k = s.rp[i]; k < s.rp[i + 1]; ++k) {
+      int64_t j = s.ci[k];
+      if (status[j] == 1) {
+        double st = s.v[k];
+        if (!have || st > best) {
+          best = st;
+          best_idx = f2c[j];
+          have = true;
+        }
+      }
+    }
+    if (best_idx >= 0) f2c[i] = best_idx;
+  }
+}
+
+// Leftmost-maximum tournament tree over lambda (undecided points only);
+// reproduces the reference's first-index-of-maximum linear scan exactly.
+struct MaxTree {
+  int64_t size = 1;
+  std::vector<int64_t> key;   // per leaf, -1 when decided
+  std::vector<int64_t> best;  // per node, leaf index of its leftmost maximum
+  explicit MaxTree(const std::vector<int64_t>& k) {
+    int64_t n = (int64_t)k.size();
+    while (size < n) size <<= 1;
+    key.assign(size, -2);
+    for (int64_t i = 0; i < n; ++i) key[i] = k[i];
+    best.assign(2 * size, 0);
+    for (int64_t i = 0; i < size; ++i) best[size + i] = i;
+    for (int64_t p = size - 1; p >= 1; --p) best[p] = pick(best[2 * p], best[2 * p + 1]);
+  }
+  int64_t pick(int64_t l, int64_t r) const { return key[r] > key[l] ? r : l; }
+  void set(int64_t i, int64_t k) {
+    key[i] = k;
+    for (int64_t p = (i + size) >> 1; p >= 1; p >>= 1) best[p] = pick(best[2 * p], best[2 * p + 1]);
+  }
+  int64_t top() const { return best[1]; }
+};
+
+// ruge_stueben_coarsening, coarsening/algorithms.rs:34-126.
+int64_t ruge_stueben(const or_csr& a, double theta, bool literal, std::vector<int64_t>& cpts,
+                     std::vector<int64_t>& f2c, or_csr* s_out) {
+  const int64_t n = a.nrows;
+  or_csr s = strength(a, theta);
+  or_csr st = transpose(s);
+  std::vector<int64_t> lambda(n);
+  for (int64_t i = 0; i < n; ++i) lambda[i] = st.rp[i + 1] - st.rp[i];
+  std::vector<int> status(n, 0);
+  f2c.assign(n, -1);
+  cpts.clear();
+  int64_t undecided = n;
+  MaxTree* tree = literal ? nullptr : new MaxTree(lambda);
+  auto decide = [&](int64_t j) {
+    if (tree) tree->set(j, -1);
+  };
+  while (undecided > 0) {
+    int64_t i_opt = -1;
+    int64_t max_lambda = -1;
+    if (literal) {
+      for (int64_t k = 0; k < n; ++k)
+        if (status[k] == 0 && lambda[k] > max_lambda) {
+          max_lambda = lambda[k];
+          i_opt = k;
+        }
+    } else {
+      int64_t t = tree->top();
+      if (t < n && tree->key[t] >= 0) {
+        i_opt = t;
+        max_lambda = lambda[t];
+      }
+    }
+    if (i_opt < 0) break;
+    if (max_lambda <= 0) break;
+    int64_t i = i_opt;
+    status[i] = 1;
+    decide(i);
+    undecided--;
+    cpts.push_back(i);
+    f2c[i] = (int64_t)cpts.size() - 1;
+    for (int64_t k = st.rp[i]; k < st.rp[i + 1]; ++k) {
+      int64_t j = st.ci[k];
+      if (status[j] == 0) {
+        status[j] = 2;
+        decide(j);
+        undecided--;
+        for (int64_t m = s.rp[j]; m < s.rp[j + 1]; ++m) {
+          int64_t kk = s.ci[m];
+          if (status[kk] == 0) {
+            lambda[kk] += 1;
+            if (tree) tree->set(kk, lambda[kk]);
+          }
+        }
+      }
+    }
+  }
+  delete tree;
+  for (int64_t i = 0; i < n; ++i)
+    if (status[i] == 0) {
+      status[i] = 1;
+      cpts.push_back(i);
+      f2c[i] = (int64_t)cpts.size() - 1;
+    }
+  assign_closest(f2c, status, s);
+  if (s_out) *s_out = std::move(s);
+  return (int64_t)cpts.size();
+}
+
+// aggregation_coarsening, coarsening/algorithms.rs:129-172 (strength theta fixed at 0.5).
+int64_t aggregation(const or_csr& a, int64_t max_size, std::vector<int64_t>& cpts,
+                    std::vector<int64_t>& f2c, or_csr* s_out) {
+  const int64_t n = a.nrows;
+  or_csr s = strength(a, 0.5);
+  std::vector<char> agg(n, 0);
+  f2c.assign(n, -1);
+  cpts.clear();
+  int64_t id = 0;
+  std::vector<int64_t> members;
+  for (int64_t i = 0; i < n; ++i) {
+    if (agg[i]) continue;
+    members.assign(1, i);
+    agg[i] = 1;
+    for (int64_t k = s.rp[i]; k < s.rp[i + 1]; ++k) {
+      int64_t j = s.ci[k];
+      if (!agg[j] && (int64_t)members.size() < max_size) {
+        members.push_back(j);
+        agg[j] = 1;
+      }
+    }
+    cpts.push_back(members[0]);
+    for (int64_t p : members) f2c[p] = id;
+    id++;
+  }
+  if (s_out) *s_out = std::move(s);
+  return (int64_t)cpts.size();
+}
+
+uint64_t splitmix64(uint64_t& state) {
+  uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// pmis_coarsening, coarsening/algorithms.rs:310-354; the reference draws the
+// priorities from an unseeded thread_rng (:324) -- here a seeded SplitMix64.
+int64_t pmis(const or_csr& a, double theta, uint64_t seed, std::vector<int64_t>& cpts,
+             std::vector<int64_t>& f2c, or_csr* s_out) {
+  const int64_t n = a.nrows;
+  or_csr s = strength(a, theta);
+  std::vector<double> prio(n);
+  uint64_t state = seed;
+  for (int64_t i = 0; i < n; ++i) prio[i] = (double)(splitmix64(state) >> 11) * 0x1.0p-53;
+  std::vector<int64_t> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int64_t x, int64_t y) { return prio[x] > prio[y]; });
+  std::vector<int> status(n, 0);
+  f2c.assign(n, -1);
+  cpts.clear();
+  for (int64_t i : order) {
+    if (status[i] != 0) continue;
+    status[i] = 1;
+    cpts.push_back(i);
+    f2c[i] = (int64_t)cpts.size() - 1;
+    for (int64_t k = s.rp[i]; k < s.rp[i + 1]; ++k)
+      if (status[s.ci[k]] == 0) status[s.ci[k]] = 2;
+  }
+  assign_closest(f2c, status, s);
+  if (s_out) *s_out = std::move(s);
+  return (int64_t)cpts.size();
+}
+
+// create_classical_interpolation, interpolation.rs:38-188.
+or_csr classical_interp(const or_csr& a, const std::vector<int64_t>& cpts, const or_csr& s) {
+  const int64_t n = a.nrows;
+  const int64_t nc = (int64_t)cpts.size();
+  std::vector<int64_t> cmap(n, -1);
+  for (int64_t l = 0; l < nc; ++l)
+    if (cpts[l] < n) cmap[cpts[l]] = l;
+  std::vector<std::vector<std::pair<int64_t, double>>> rows(n);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t i = 0; i < n; ++i) {
+    auto& out = rows[i];
+    if (cmap[i] >= 0) {
+      out.emplace_back(cmap[i], 1.0);
+      continue;
+    }
+    const int64_t* scols = s.ci.data() + s.rp[i];
+    const int64_t ns = s.rp[i + 1] - s.rp[i];
+    std::vector<int64_t> c_i, f_i;
+    for (int64_t q = 0; q < ns; ++q) {
+      int64_t nb = scols[q];
+      if (cmap[nb] >= 0)
+        c_i.push_back(nb);
+      else if (nb != i)
+        f_i.push_back(nb);
+    }
+    if (c_i.empty()) continue;
+    double a_ii = 0.0, sum_weak = 0.0;
+    for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k) {
+      int64_t nb = a.ci[k];
+      if (nb == i)
+        a_ii = a.v[k];
+      else if (!std::binary_search(scols, scols + ns, nb))
+        sum_weak += a.v[k];
+    }
+    double diagonal = a_ii + sum_weak;
+    if (!(std::fabs(diagonal) > DBL_EPSILON)) continue;
+    std::vector<double> denoms(f_i.size());
+    for (size_t q = 0; q < f_i.size(); ++q) {
+      double d = 0.0;
+      for (int64_t m : c_i) d += csr_value(a, f_i[q], m);
+      denoms[q] = d;
+    }
+    double neg_diag_inv = 1.0 / -diagonal;
+    for (int64_t j : c_i) {
+      double a_ij = csr_value(a, i, j);
+      double indirect = 0.0;
+      for (size_t q = 0; q < f_i.size(); ++q) {
+        double den = denoms[q];
+        if (std::fabs(den) > DBL_EPSILON) {
+          double a_ik = csr_value(a, i, f_i[q]);
+          double a_kj = csr_value(a, f_i[q], j);
+          indirect += a_ik * a_kj / den;
+        }
+      }
+      out.emplace_back(cmap[j], (a_ij + indirect) * neg_diag_inv);
+    }
+    std::stable_sort(out.begin(), out.end(),
+                     [](const std::pair<int64_t, double>& x, const std::pair<int64_t, double>& y) {
+                       return x.first < y.first;
+                     });
+  }
+  or_csr p;
+  p.nrows = n;
+  p.ncols = nc;
+  p.rp.assign(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i) p.rp[i + 1] = p.rp[i] + (int64_t)rows[i].size();
+  p.ci.resize(p.rp[n]);
+  p.v.resize(p.rp[n]);
+  for (int64_t i = 0; i < n; ++i)
+    for (size_t q = 0; q < rows[i].size(); ++q) {
+      p.ci[p.rp[i] + q] = rows[i][q].first;
+      p.v[p.rp[i] + q] = rows[i][q].second;
+    }
+  return p;
+}
+
+// Modified classical interpolation (Stueben 2001, "Algebraic multigrid (AMG):
+// an introduction with applications", App. A.7.2; the sign-restricted form used by
+// hypre BoomerAMG's classical-modified interpolation). Same sets C_i / F_i as
+// classical_interp above, but for each strong F-neighbour k only the entries
+// a_km whose sign is opposite to a_kk take part in the distribution, and an F
+// neighbour with no such entry to C_i is lumped into the diagonal instead of
+// being dropped, so row sums are preserved and no denominator can cancel.
+or_csr modified_classical_interp(const or_csr& a, const std::vector<int64_t>& cpts, const or_csr& s) {
+  const int64_t n = a.nrows;
+  const int64_t nc = (int64_t)cpts.size();
+  std::vector<int64_t> cmap(n, -1);
+  for (int64_t l = 0; l < nc; ++l)
+    if (cpts[l] < n) cmap[cpts[l]] = l;
+  std::vector<std::vector<std::pair<int64_t, double>>> rows(n);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t i = 0; i < n; ++i) {
+    auto& out = rows[i];
+    if (cmap[i] >= 0) {
+      out.emplace_back(cmap[i], 1.0);
+      continue;
+    }
+    const int64_t* scols = s.ci.data() + s.rp[i];
+    const int64_t ns = s.rp[i + 1] - s.rp[i];
+    std::vector<int64_t> c_i, f_i;
+    for (int64_t q = 0; q < ns; ++q) {
+      int64_t nb = scols[q];
+      if (cmap[nb] >= 0)
+        c_i.push_back(nb);
+      else if (nb != i)
+        f_i.push_back(nb);
+    }
+    if (c_i.empty()) continue;
+    double diagonal = 0.0;
+    for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k) {
+      int64_t nb = a.ci[k];
+      if (nb == i || !std::binary_search(scols, scols + ns, nb)) diagonal += a.v[k];
+    }
+    std::vector<double> num(c_i.size(), 0.0);
+    for (size_t q = 0; q < c_i.size(); ++q) num[q] = csr_value(a, i, c_i[q]);
+    for (int64_t k : f_i) {
+      const double a_ik = csr_value(a, i, k);
+      const double a_kk = csr_value(a, k, k);
+      double den = 0.0;
+      for (int64_t m : c_i) {
+        const double v = csr_value(a, k, m);
+        if (v * a_kk < 0.0) den += v;
+      }
+      if (den == 0.0) {
+        diagonal += a_ik;
+        continue;
+      }
+      for (size_t q = 0; q < c_i.size(); ++q) {
+        const double v = csr_value(a, k, c_i[q]);
+        if (v * a_kk < 0.0) num[q] += a_ik * v / den;
+      }
+    }
+    if (!(std::fabs(diagonal) > DBL_EPSILON)) continue;
+    const double neg_diag_inv = 1.0 / -diagonal;
+    for (size_t q = 0; q < c_i.size(); ++q) out.emplace_back(cmap[c_i[q]], num[q] * neg_diag_inv);
+    std::stable_sort(out.begin(), out.end(),
+                     [](const std::pair<int64_t, double>& x, const std::pair<int64_t, double>& y) {
+                       return x.first < y.first;
+                     });
+  }
+  or_csr p;
+  p.nrows = n;
+  p.ncols = nc;
+  p.rp.assign(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i) p.rp[i + 1] = p.rp[i] + (int64_t)rows[i].size();
+  p.ci.resize(p.rp[n]);
+  p.v.resize(p.rp[n]);
+  for (int64_t i = 0; i < n; ++i)
+    for (size_t q = 0; q < rows[i].size(); ++q) {
+      p.ci[p.rp[i] + q] = rows[i][q].first;
+      p.v[p.rp[i] + q] = rows[i][q].second;
+    }
+  return p;
+}
+
+// create_direct_interpolation, interpolation.rs:191-217.
+or_csr direct_interp(const std::vector<int64_t>& f2c, int64_t n, int64_t nc) {
+  or_csr p;
+  p.nrows = n;
+  p.ncols = nc;
+  p.rp.assign(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i) {
+    if (f2c[i] >= 0) {
+      p.ci.push_back(f2c[i]);
+      p.v.push_back(1.0);
+    }
+    p.rp[i + 1] = (int64_t)p.ci.size();
+  }
+  return p;
+}
+
+// JacobiSmoother::apply, smoothers.rs:160-194.
+void jacobi_sweeps(const or_csr& a, double* x, const double* b, double omega, int iters) {
+  std::vector<double> xo(a.nrows);
+  for (int it = 0; it < iters; ++it) {
+    std::copy(x, x + a.nrows, xo.begin());
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < a.nrows; ++i) {
+      double sum = 0.0, diag = 0.0;
+      for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k) {
+        if (a.ci[k] == i)
+          diag = a.v[k];
+        else
+          sum += a.v[k] * xo[a.ci[k]];
+      }
+      if (std::fabs(diag) > kDiagEps) {
+        double nv = (b[i] - sum) / diag;
+        x[i] = xo[i] + omega * (nv - xo[i]);
+      }
+    }
+  }
+}
+
+// GaussSeidelSmoother::apply, smoothers.rs:45-82 (forward) and the backward
+// half of SymmetricGaussSeidelSmoother, smoothers.rs:84-138.
+void gs_sweep(const or_csr& a, double* x, const double* b, double omega, bool backward) {
+  for (int64_t q = 0; q < a.nrows; ++q) {
+    int64_t i = backward ? a.nrows - 1 - q : q;
+    double sum = 0.0, diag = 0.0;
+    for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k) {
+      if (a.ci[k] == i)
+        diag = a.v[k];
+      else
+        sum += a.v[k] * x[a.ci[k]];
+    }
+    if (std::fabs(diag) > kDiagEps) {
+      double nv = (b[i] - sum) / diag;
+      x[i] = x[i] + omega * (nv - x[i]);
+    }
+  }
+}
+
+void smooth(const or_csr& a, double* x, const double* b, int kind, double omega, int iters) {
+  if (kind == OR_SMOOTH_JACOBI) {
+    jacobi_sweeps(a, x, b, omega, iters);
+  } else if (kind == OR_SMOOTH_GS) {
+    for (int it = 0; it < iters; ++it) gs_sweep(a, x, b, omega, false);
+  } else {
+    for (int it = 0; it < iters; ++it) gs_sweep(a, x, b, omega, false);
+    for (int it = 0; it < iters; ++it) gs_sweep(a, x, b, omega, true);
+  }
+}
+
+// Dense LU with partial pivoting (coarsest-level direct solve).
+int dense_solve(const or_csr& a, const double* b, double* x) {
+  const int64_t n = a.nrows;
+  std::vector<double> m((size_t)n * n, 0.0);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k) m[(size_t)i * n + a.ci[k]] += a.v[k];
+  std::vector<double> rhs(b, b + n);
+  for (int64_t c = 0; c < n; ++c) {
+    int64_t piv = c;
+    for (int64_t r = c + 1; r < n; ++r)
+      if (std::fabs(m[(size_t)r * n + c]) > std::fabs(m[(size_t)piv * n + c])) piv = r;
+    if (m[(size_t)piv * n + c] == 0.0) return -1;
+    if (piv != c) {
+      for (int64_t k = 0; k < n; ++k) std::swap(m[(size_t)c * n + k], m[(size_t)piv * n + k]);
+      std::swap(rhs[c], rhs[piv]);
+    }
+    double d = m[(size_t)c * n + c];
+#pragma omp parallel for schedule(static) if (n > 512)
+    for (int64_t r = c + 1; r < n; ++r) {
+      double f = m[(size_t)r * n + c] / d;
+      if (f == 0.0) continue;
+      for (int64_t k = c; k < n; ++k) m[(size_t)r * n + k] -= f * m[(size_t)c * n + k];
+      rhs[r] -= f * rhs[c];
+    }
+  }
+  for (int64_t r = n - 1; r >= 0; --r) {
+    double s = rhs[r];
+    for (int64_t k = r + 1; k < n; ++k) s -= m[(size_t)r * n + k] * x[k];
+    x[r] = s / m[(size_t)r * n + r];
+  }
+  return 0;
+}
+
+}  // namespace
+
+struct or_amg {
+  or_amg_config cfg;
+  std::vector<or_csr> A, P, R;
+  // Dense LU factor of the coarsest level (row-major, with pivots), when used.
+  std::vector<double> lu;
+  std::vector<int64_t> piv;
+  mutable std::vector<std::vector<double>> ws_r, ws_rc, ws_xc, ws_e, ws_ax;
+};
+
+namespace {
+
+void lu_factor(const or_csr& a, std::vector<double>& m, std::vector<int64_t>& piv) {
+  const int64_t n = a.nrows;
+  m.assign((size_t)n * n, 0.0);
+  piv.resize(n);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k) m[(size_t)i * n + a.ci[k]] += a.v[k];
+  for (int64_t c = 0; c < n; ++c) {
+    int64_t p = c;
+    for (int64_t r = c + 1; r < n; ++r)
+      if (std::fabs(m[(size_t)r * n + c]) > std::fabs(m[(size_t)p * n + c])) p = r;
+    piv[c] = p;
+    if (p != c)
+      for (int64_t k = 0; k < n; ++k) std::swap(m[(size_t)c * n + k], m[(size_t)p * n + k]);
+    double d = m[(size_t)c * n + c];
+    if (d == 0.0) continue;
+#pragma omp parallel for schedule(static) if (n > 256)
+    for (int64_t r = c + 1; r < n; ++r) {
+      double f = m[(size_t)r * n + c] / d;
+      m[(size_t)r * n + c] = f;
+      if (f == 0.0) continue;
+      for (int64_t k = c + 1; k < n; ++k) m[(size_t)r * n + k] -= f * m[(size_t)c * n + k];
+    }
+  }
+}
+
+void lu_solve(const std::vector<double>& m, const std::vector<int64_t>& piv, int64_t n,
+              const double* b, double* x) {
+  std::vector<double> y(b, b + n);
+  for (int64_t c = 0; c < n; ++c) {
+    if (piv[c] != c) std::swap(y[c], y[piv[c]]);
+    for (int64_t r = c + 1; r < n; ++r) y[r] -= m[(size_t)r * n + c] * y[c];
+  }
+  for (int64_t r = n - 1; r >= 0; --r) {
+    double s = y[r];
+    for (int64_t k = r + 1; k < n; ++k) s -= m[(size_t)r * n + k] * x[k];
+    x[r] = s / m[(size_t)r * n + r];
+  }
+}
+
+// AlgebraicMultigrid::v_cycle, amg.rs:423-503.
+void v_cycle(const or_amg& h, size_t l, const double* b, double* x) {
+  const or_csr& a = h.A[l];
+  const int64_t n = a.nrows;
+  const or_amg_config& c = h.cfg;
+  if (l + 1 < h.A.size()) {
+    smooth(a, x, b, c.smoother, c.relaxation, c.pre_smooth);
+    std::vector<double>& ax = h.ws_ax[l];
+    std::vector<double>& r = h.ws_r[l];
+    spmv_raw(a, x, ax.data());
+    for (int64_t i = 0; i < n; ++i) r[i] = b[i] - ax[i];
+    std::vector<double>& rc = h.ws_rc[l];
+    spmv_raw(h.R[l], r.data(), rc.data());
+    std::vector<double>& xc = h.ws_xc[l];
+    std::fill(xc.begin(), xc.end(), 0.0);
+    v_cycle(h, l + 1, rc.data(), xc.data());
+    std::vector<double>& e = h.ws_e[l];
+    spmv_raw(h.P[l], xc.data(), e.data());
+    for (int64_t i = 0; i < n; ++i) x[i] += e[i];
+    smooth(a, x, b, c.smoother, c.relaxation, c.post_smooth);
+  } else if (c.coarse_solve == OR_COARSE_DENSE) {
+    lu_solve(h.lu, h.piv, n, b, x);
+  } else {
+    smooth(a, x, b, c.smoother, c.relaxation, c.coarse_sweeps);
+  }
+}
+
+// DiagJacobi::new, cfd-1d/src/solver/core/linear_system.rs:270-299.
+int jacobi_inverse(const or_csr& a, std::vector<double>& inv) {
+  inv.assign(a.nrows, 1.0);
+  for (int64_t i = 0; i < a.nrows; ++i) {
+    double d = csr_value(a, i, i);
+    if (!std::isfinite(d)) return -1;
+    inv[i] = std::fabs(d) <= DBL_EPSILON ? 1.0 : 1.0 / d;
+  }
+  return 0;
+}
+
+struct Precond {
+  int kind;
+  const or_amg* amg;
+  std::vector<double> inv;
+  void apply(const double* r, double* z, int64_t n) const {
+    if (kind == OR_PRE_JACOBI) {
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < n; ++i) z[i] = r[i] * inv[i];
+    } else if (kind == OR_PRE_AMG) {
+      or_amg_apply(amg, r, z);
+    } else {
+      std::copy(r, r + n, z);
+    }
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+or_csr* or_csr_new(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* row_ptr,
+                   const int64_t* col, const double* val) {
+  or_csr* a = new or_csr;
+  a->nrows = nrows;
+  a->ncols = ncols;
+  a->rp.assign(row_ptr, row_ptr + nrows + 1);
+  a->ci.assign(col, col + nnz);
+  a->v.assign(val, val + nnz);
+  return a;
+}
+
+void or_csr_info(const or_csr* a, int64_t* nrows, int64_t* ncols, int64_t* nnz) {
+  *nrows = a->nrows;
+  *ncols = a->ncols;
+  *nnz = a->nnz();
+}
+
+void or_csr_export(const or_csr* a, int64_t* row_ptr, int64_t* col, double* val) {
+  std::copy(a->rp.begin(), a->rp.end(), row_ptr);
+  std::copy(a->ci.begin(), a->ci.end(), col);
+  std::copy(a->v.begin(), a->v.end(), val);
+}
+
+void or_csr_free(or_csr* a) { delete a; }
+
+void or_set_threads(int n) {
+  if (n > 0) omp_set_num_threads(n);
+}
+int or_get_threads(void) { return omp_get_max_threads(); }
+
+void or_spmv(const or_csr* a, const double* x, double* y) { spmv_raw(*a, x, y); }
+or_csr* or_strength(const or_csr* a, double theta) { return new or_csr(strength(*a, theta)); }
+or_csr* or_transpose(const or_csr* a) { return new or_csr(transpose(*a)); }
+or_csr* or_spgemm(const or_csr* a, const or_csr* b) { return new or_csr(spgemm(*a, *b)); }
+
+int64_t or_coarsen(const or_csr* a, int kind, double theta, int64_t param, uint64_t seed,
+                   int literal_scan, int64_t* coarse_points, int64_t* f2c) {
+  std::vector<int64_t> cp, map;
+  int64_t nc;
+  if (kind == OR_RUGE_STUEBEN)
+    nc = ruge_stueben(*a, theta, literal_scan != 0, cp, map, nullptr);
+  else if (kind == OR_AGGREGATION)
+    nc = aggregation(*a, param, cp, map, nullptr);
+  else
+    nc = pmis(*a, theta, seed, cp, map, nullptr);
+  std::copy(cp.begin(), cp.end(), coarse_points);
+  std::copy(map.begin(), map.end(), f2c);
+  return nc;
+}
+
+or_csr* or_classical_interp(const or_csr* a, const int64_t* coarse_points, int64_t nc,
+                            const or_csr* s) {
+  std::vector<int64_t> cp(coarse_points, coarse_points + nc);
+  return new or_csr(classical_interp(*a, cp, *s));
+}
+
+or_csr* or_direct_interp(const int64_t* f2c, int64_t n, int64_t nc) {
+  std::vector<int64_t> m(f2c, f2c + n);
+  return new or_csr(direct_interp(m, n, nc));
+}
+
+void or_smooth(const or_csr* a, double* x, const double* b, int kind, double omega, int iters) {
+  smooth(*a, x, b, kind, omega, iters);
+}
+
+int or_dense_solve(const or_csr* a, const double* b, double* x) { return dense_solve(*a, b, x); }
+
+// AlgebraicMultigrid::setup / build_next_level, amg.rs:217-380.
+or_amg* or_amg_setup(const or_csr* a, const or_amg_config* cfg) {
+  or_amg* h = new or_amg;
+  h->cfg = *cfg;
+  h->A.push_back(*a);
+  while ((int)h->A.size() < cfg->max_levels && h->A.back().nrows > cfg->min_coarse_size) {
+    const or_csr& cur = h->A.back();
+    std::vector<int64_t> cp, map;
+    or_csr s;
+    int64_t nc;
+    if (cfg->coarsening == OR_RUGE_STUEBEN)
+      nc = ruge_stueben(cur, cfg->strength_threshold, false, cp, map, &s);
+    else if (cfg->coarsening == OR_AGGREGATION)
+      nc = aggregation(cur, cfg->aggregate_size, cp, map, &s);
+    else
+      nc = pmis(cur, cfg->strength_threshold, cfg->seed, cp, map, &s);
+    or_csr p = cfg->interpolation == 0   ? classical_interp(cur, cp, s)
+               : cfg->interpolation == 2 ? modified_classical_interp(cur, cp, s)
+                                         : direct_interp(map, cur.nrows, nc);
+    or_csr r = transpose(p);
+    or_csr ra = spgemm(r, cur);
+    or_csr ac = spgemm(ra, p);
+    h->P.push_back(std::move(p));
+    h->R.push_back(std::move(r));
+    h->A.push_back(std::move(ac));
+    if (nc == 0 || nc >= cur.nrows) break;  // no progress: stop coarsening
+  }
+  if (cfg->coarse_solve == OR_COARSE_DENSE) lu_factor(h->A.back(), h->lu, h->piv);
+  size_t L = h->A.size();
+  h->ws_r.resize(L);
+  h->ws_rc.resize(L);
+  h->ws_xc.resize(L);
+  h->ws_e.resize(L);
+  h->ws_ax.resize(L);
+  for (size_t l = 0; l + 1 < L; ++l) {
+    h->ws_r[l].assign(h->A[l].nrows, 0.0);
+    h->ws_ax[l].assign(h->A[l].nrows, 0.0);
+    h->ws_e[l].assign(h->A[l].nrows, 0.0);
+    h->ws_rc[l].assign(h->A[l + 1].nrows, 0.0);
+    h->ws_xc[l].assign(h->A[l + 1].nrows, 0.0);
+  }
+  return h;
+}
+
+// A hierarchy given level by level (e.g. exported from another setup), for
+// timing the solve phase on an identical hierarchy.
+or_amg* or_amg_from_levels(int nlev, const or_csr* const* a, const or_csr* const* p, const or_csr* const* r,
+                           const or_amg_config* cfg) {
+  or_amg* h = new or_amg;
+  h->cfg = *cfg;
+  for (int l = 0; l < nlev; ++l) {
+    h->A.push_back(*a[l]);
+    if (l + 1 < nlev) {
+      h->P.push_back(*p[l]);
+      h->R.push_back(*r[l]);
+    }
+  }
+  if (cfg->coarse_solve == OR_COARSE_DENSE) lu_factor(h->A.back(), h->lu, h->piv);
+  size_t L = h->A.size();
+  h->ws_r.resize(L);
+  h->ws_rc.resize(L);
+  h->ws_xc.resize(L);
+  h->ws_e.resize(L);
+  h->ws_ax.resize(L);
+  for (size_t l = 0; l + 1 < L; ++l) {
+    h->ws_r[l].assign(h->A[l].nrows, 0.0);
+    h->ws_ax[l].assign(h->A[l].nrows, 0.0);
+    h->ws_e[l].assign(h->A[l].nrows, 0.0);
+    h->ws_rc[l].assign(h->A[l + 1].nrows, 0.0);
+    h->ws_xc[l].assign(h->A[l + 1].nrows, 0.0);
+  }
+  return h;
+}
+
+int or_amg_num_levels(const or_amg* h) { return (int)h->A.size(); }
+
+const or_csr* or_amg_level(const or_amg* h, int level, int which) {
+  if (level < 0 || level >= (int)h->A.size()) return nullptr;
+  if (which == 0) return &h->A[level];
+  if (level >= (int)h->P.size()) return nullptr;
+  return which == 1 ? &h->P[level] : &h->R[level];
+}
+
+// Preconditioner::apply_to, amg.rs:507-557: z = 0, then one V-cycle.
+void or_amg_apply(const or_amg* h, const double* r, double* z) {
+  std::fill(z, z + h->A[0].nrows, 0.0);
+  v_cycle(*h, 0, r, z);
+}
+
+void or_amg_free(or_amg* h) { delete h; }
+
+// Preconditioned CG (Saad 2003, Alg. 9.1) with the termination mapping of
+// krylov.rs:375-401. threshold = max(tolerance, relative_tolerance * ||r0||)
+// (the absolute-or-relative test of cfd-core compute/solver/convergence.rs:26-30).
+int or_pcg(const or_csr* a, int precond, const or_amg* amg, const double* b, double* x,
+           const or_solver_config* cfg, or_report* rep, double* history) {
+  const int64_t n = a->nrows;
+  if (a->ncols != n) return -1;
+  Precond M{precond, amg, {}};
+  if (precond == OR_PRE_JACOBI && jacobi_inverse(*a, M.inv) != 0) return -2;
+  std::vector<double> r(n), z(n), p(n), q(n);
+  spmv_raw(*a, x, q.data());
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+  double rn = std::sqrt(dot(n, r.data(), r.data()));
+  rep->initial_residual = rn;
+  rep->threshold = std::max(cfg->tolerance, cfg->relative_tolerance * rn);
+  rep->final_residual = rn;
+  rep->iterations = 0;
+  if (history) history[0] = rn;
+  if (rn <= rep->threshold) {
+    rep->termination = OR_TERM_INITIAL_RESIDUAL;
+    return 0;
+  }
+  M.apply(r.data(), z.data(), n);
+  double rho = dot(n, r.data(), z.data());
+  std::copy(z.begin(), z.end(), p.begin());
+  for (int64_t it = 1; it <= cfg->max_iterations; ++it) {
+    spmv_raw(*a, p.data(), q.data());
+    double pq = dot(n, p.data(), q.data());
+    if (!(pq > 0.0)) {
+      rep->termination = OR_TERM_NON_POSITIVE_CURVATURE;
+      return 0;
+    }
+    double alpha = rho / pq;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+      x[i] += alpha * p[i];
+      r[i] -= alpha * q[i];
+    }
+    rn = std::sqrt(dot(n, r.data(), r.data()));
+    rep->iterations = it;
+    rep->final_residual = rn;
+    if (history) history[it] = rn;
+    if (!std::isfinite(rn)) {
+      rep->termination = OR_TERM_BREAKDOWN;
+      return 0;
+    }
+    if (rn <= rep->threshold) {
+      rep->termination = OR_TERM_CONVERGED;
+      return 0;
+    }
+    M.apply(r.data(), z.data(), n);
+    double rho_new = dot(n, r.data(), z.data());
+    if (rho_new == 0.0 || !std::isfinite(rho_new)) {
+      rep->termination = OR_TERM_BREAKDOWN;
+      return 0;
+    }
+    double beta = rho_new / rho;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+    rho = rho_new;
+  }
+  rep->termination = OR_TERM_MAX_ITERATIONS;
+  return 0;
+}
+
+// Right-preconditioned BiCGSTAB (Saad 2003, Alg. 7.7 with M^-1 applied to p and s).
+int or_bicgstab(const or_csr* a, int precond, const or_amg* amg, const double* b, double* x,
+                const or_solver_config* cfg, or_report* rep, double* history) {
+  const int64_t n = a->nrows;
+  if (a->ncols != n) return -1;
+  Precond M{precond, amg, {}};
+  if (precond == OR_PRE_JACOBI && jacobi_inverse(*a, M.inv) != 0) return -2;
+  std::vector<double> r(n), rh(n), p(n, 0.0), v(n, 0.0), ph(n), s(n), sh(n), t(n);
+  spmv_raw(*a, x, t.data());
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) r[i] = b[i] - t[i];
+  std::copy(r.begin(), r.end(), rh.begin());
+  double rn = std::sqrt(dot(n, r.data(), r.data()));
+  rep->initial_residual = rn;
+  rep->threshold = std::max(cfg->tolerance, cfg->relative_tolerance * rn);
+  rep->final_residual = rn;
+  rep->iterations = 0;
+  if (history) history[0] = rn;
+  if (rn <= rep->threshold) {
+    rep->termination = OR_TERM_INITIAL_RESIDUAL;
+    return 0;
+  }
+  double rho = 1.0, alpha = 1.0, omega = 1.0;
+  for (int64_t it = 1; it <= cfg->max_iterations; ++it) {
+    double rho_new = dot(n, rh.data(), r.data());
+    if (rho_new == 0.0 || !std::isfinite(rho_new)) {
+      rep->termination = OR_TERM_BREAKDOWN;
+      return 0;
+    }
+    if (it == 1) {
+      std::copy(r.begin(), r.end(), p.begin());
+    } else {
+      double beta = (rho_new / rho) * (alpha / omega);
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < n; ++i) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+    }
+    M.apply(p.data(), ph.data(), n);
+    spmv_raw(*a, ph.data(), v.data());
+    double rv = dot(n, rh.data(), v.data());
+    if (rv == 0.0 || !std::isfinite(rv)) {
+      rep->termination = OR_TERM_BREAKDOWN;
+      return 0;
+    }
+    alpha = rho_new / rv;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) s[i] = r[i] - alpha * v[i];
+    double sn = std::sqrt(dot(n, s.data(), s.data()));
+    rep->iterations = it;
+    if (sn <= rep->threshold) {
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < n; ++i) x[i] += alpha * ph[i];
+      rep->final_residual = sn;
+      if (history) history[it] = sn;
+      rep->termination = OR_TERM_CONVERGED;
+      return 0;
+    }
+    M.apply(s.data(), sh.data(), n);
+    spmv_raw(*a, sh.data(), t.data());
+    double tt = dot(n, t.data(), t.data());
+    if (tt == 0.0 || !std::isfinite(tt)) {
+      rep->termination = OR_TERM_BREAKDOWN;
+      return 0;
+    }
+    omega = dot(n, t.data(), s.data()) / tt;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+      x[i] += alpha * ph[i] + omega * sh[i];
+      r[i] = s[i] - omega * t[i];
+    }
+    rn = std::sqrt(dot(n, r.data(), r.data()));
+    rep->final_residual = rn;
+    if (history) history[it] = rn;
+    if (!std::isfinite(rn)) {
+      rep->termination = OR_TERM_BREAKDOWN;
+      return 0;
+    }
+    if (rn <= rep->threshold) {
+      rep->termination = OR_TERM_CONVERGED;
+      return 0;
+    }
+    if (omega == 0.0) {
+      rep->termination = OR_TERM_BREAKDOWN;
+      return 0;
+    }
+    rho = rho_new;
+  }
+  rep->termination = OR_TERM_MAX_ITERATIONS;
+  return 0;
+}
+
+}  // extern "C"

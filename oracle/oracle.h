@@ -1,0 +1,128 @@
+/*
+ * CPU oracle for the CFDrs preconditioned sparse linear-solve path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is the checker used by tests/,
+ * __graft_entry__.smoke() and the CPU-baseline leg of bench.py. The product
+ * library (cfdrs_b200/libcfdgpu.so) never links, loads or calls it.
+ *
+ * It restates, in plain C++17/OpenMP, the FP64 algorithms of the reference
+ * (ryancinsight/CFDrs, Rust) for this path:
+ *   - CSR SpMV                      leto_ops::spmv_into via crates/cfd-math/src/sparse/operations.rs:50-79
+ *   - strength of connection        crates/cfd-math/src/linear_solver/preconditioners/multigrid/coarsening/algorithms.rs:395-436
+ *   - Ruge-Stueben C/F split        .../coarsening/algorithms.rs:34-126 (+ assign_closest_coarse_points :199-230)
+ *   - aggregation / PMIS            .../coarsening/algorithms.rs:129-172, :310-354 (PMIS priorities seeded)
+ *   - classical / direct interp.    .../multigrid/interpolation.rs:38-188, :191-217
+ *   - Galerkin RAP, R = P^T         .../multigrid/amg.rs:290-380
+ *   - V-cycle                       .../multigrid/amg.rs:423-503, entry with z = 0 at :553-554
+ *   - Jacobi / GS / SGS smoothers   .../multigrid/smoothers.rs:45-199
+ *   - Jacobi preconditioner         crates/cfd-1d/src/solver/core/linear_system.rs:270-332
+ *   - PCG / BiCGSTAB + termination  crates/cfd-math/src/linear_solver/krylov.rs:253-360, :375-428
+ *     (the recurrences themselves live in the un-vendored athena-core 0.1.1 @ f6608bef;
+ *      they are restated from Saad 2003, Alg. 9.1 / 7.7, which the reference cites).
+ *
+ * Parity is pinned by the golden vectors transcribed from the reference's own
+ * unit tests (tests/golden/make_golden.py lists each with its file:line).
+ */
+#ifndef CFD_ORACLE_H
+#define CFD_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or_csr or_csr;
+typedef struct or_amg or_amg;
+
+/* CSR matrices (int64 indices mirror the reference's usize). */
+or_csr* or_csr_new(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* row_ptr,
+                   const int64_t* col, const double* val);
+void or_csr_info(const or_csr* a, int64_t* nrows, int64_t* ncols, int64_t* nnz);
+void or_csr_export(const or_csr* a, int64_t* row_ptr, int64_t* col, double* val);
+void or_csr_free(or_csr* a);
+
+void or_set_threads(int n);
+int or_get_threads(void);
+
+void or_spmv(const or_csr* a, const double* x, double* y);
+or_csr* or_strength(const or_csr* a, double theta);
+or_csr* or_transpose(const or_csr* a);
+or_csr* or_spgemm(const or_csr* a, const or_csr* b);
+
+/* Coarsening kinds. */
+enum { OR_RUGE_STUEBEN = 0, OR_AGGREGATION = 1, OR_PMIS = 2 };
+/* Returns the number of coarse points; coarse_points[0..nc) in selection order,
+ * f2c[i] = coarse index or -1. literal_scan=1 uses the reference's O(n^2) scan
+ * for the Ruge-Stueben maximum (for pinning the fast path on small inputs). */
+int64_t or_coarsen(const or_csr* a, int kind, double theta, int64_t param, uint64_t seed,
+                   int literal_scan, int64_t* coarse_points, int64_t* f2c);
+or_csr* or_classical_interp(const or_csr* a, const int64_t* coarse_points, int64_t nc,
+                            const or_csr* strength);
+or_csr* or_direct_interp(const int64_t* f2c, int64_t n, int64_t nc);
+
+enum { OR_SMOOTH_JACOBI = 0, OR_SMOOTH_GS = 1, OR_SMOOTH_SGS = 2 };
+void or_smooth(const or_csr* a, double* x, const double* b, int kind, double omega, int iters);
+
+/* Dense LU with partial pivoting solve of a small CSR system (coarsest level). */
+int or_dense_solve(const or_csr* a, const double* b, double* x);
+
+enum { OR_COARSE_SWEEPS = 0, OR_COARSE_DENSE = 1 };
+typedef struct {
+  int32_t max_levels;
+  int32_t coarsening;      /* OR_RUGE_STUEBEN ... */
+  int64_t min_coarse_size;
+  int32_t interpolation;   /* 0 classical (reference), 1 direct, 2 modified classical */
+  int32_t smoother;        /* OR_SMOOTH_* */
+  int32_t pre_smooth;
+  int32_t post_smooth;
+  double relaxation;
+  double strength_threshold;
+  int32_t coarse_solve;    /* OR_COARSE_* */
+  int32_t coarse_sweeps;   /* reference: 10 */
+  int64_t aggregate_size;  /* reference: 8 */
+  uint64_t seed;           /* PMIS priorities */
+} or_amg_config;
+
+or_amg* or_amg_setup(const or_csr* a, const or_amg_config* cfg);
+or_amg* or_amg_from_levels(int nlev, const or_csr* const* a, const or_csr* const* p,
+                           const or_csr* const* r, const or_amg_config* cfg);
+int or_amg_num_levels(const or_amg* h);
+/* which: 0 = A_l, 1 = P_l (interpolation), 2 = R_l (restriction). NULL when absent. */
+const or_csr* or_amg_level(const or_amg* h, int level, int which);
+void or_amg_apply(const or_amg* h, const double* r, double* z);
+void or_amg_free(or_amg* h);
+
+/* Krylov. */
+enum { OR_PRE_NONE = 0, OR_PRE_JACOBI = 1, OR_PRE_AMG = 2 };
+enum {
+  OR_TERM_CONVERGED = 0,
+  OR_TERM_INITIAL_RESIDUAL = 1,
+  OR_TERM_MAX_ITERATIONS = 2,
+  OR_TERM_BREAKDOWN = 3,
+  OR_TERM_NON_POSITIVE_CURVATURE = 4
+};
+typedef struct {
+  double tolerance;           /* absolute */
+  double relative_tolerance;  /* relative to ||r0|| */
+  int64_t max_iterations;
+} or_solver_config;
+typedef struct {
+  int32_t termination;
+  int32_t pad;
+  int64_t iterations;
+  double initial_residual;
+  double final_residual;
+  double threshold;
+} or_report;
+
+/* Return 0 on success, <0 on a setup/dimension error (e.g. non-finite diagonal). */
+int or_pcg(const or_csr* a, int precond, const or_amg* amg, const double* b, double* x,
+           const or_solver_config* cfg, or_report* rep, double* history);
+int or_bicgstab(const or_csr* a, int precond, const or_amg* amg, const double* b, double* x,
+                const or_solver_config* cfg, or_report* rep, double* history);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

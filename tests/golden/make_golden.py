@@ -1,0 +1,103 @@
+"""Writes tests/golden/reference_golden.json: the known-answer vectors of the
+CFDrs unit tests for this path, transcribed from the reference's test sources
+(paths relative to the CFDrs repository). The reference is Rust and cannot be
+built here, so these vectors -- not a run of the reference -- pin the oracle.
+
+Run: python tests/golden/make_golden.py
+"""
+import json
+import os
+
+GOLDEN = {
+    "smoother_tridiagonal_5": {
+        "source": "crates/cfd-math/src/linear_solver/preconditioners/multigrid/smoothers.rs:395-492",
+        "matrix": "5x5 tridiagonal [-1, 2, -1]",
+        "b": [1.0, 2.0, 3.0, 4.0, 5.0],
+        "x0": [0.0, 0.0, 0.0, 0.0, 0.0],
+        "relaxation": 1.0,
+        "sweeps": 1,
+        "jacobi": [0.5, 1.0, 1.5, 2.0, 2.5],
+        "gauss_seidel": [0.5, 1.25, 2.125, 3.0625, 4.03125],
+        "symmetric_gauss_seidel": [2.291015625, 3.58203125, 4.6640625, 5.078125, 4.03125],
+        "sor_1": [0.5, 1.25, 2.125, 3.0625, 4.03125],
+    },
+    "strength_grid_4x4": {
+        "source": "crates/cfd-math/src/linear_solver/preconditioners/multigrid/coarsening/mod.rs:30-66,108-122",
+        "matrix": "4x4 grid Laplacian, 4 on the diagonal, -1 to grid neighbours, row-major",
+        "theta": 0.5,
+        "nnz": 48,
+        "row0_cols": [1, 4],
+        "row0_vals": [1.0, 1.0],
+        "row5_cols": [1, 4, 6, 9],
+        "row5_vals": [1.0, 1.0, 1.0, 1.0],
+    },
+    "spmv_3x3": {
+        "source": "crates/cfd-math/src/sparse/tests.rs:195-221",
+        "row_ptr": [0, 2, 3, 5],
+        "col": [0, 2, 1, 0, 2],
+        "val": [2.0, 1.0, 3.0, 1.0, 2.0],
+        "x": [1.0, 2.0, 3.0],
+        "y": [5.0, 6.0, 7.0],
+        "tol": 1e-10,
+    },
+    "coarsest_solve_3x3": {
+        "source": "crates/cfd-math/src/linear_solver/preconditioners/multigrid/cycles.rs:513-534",
+        "row_ptr": [0, 2, 4, 5],
+        "col": [0, 1, 1, 2, 2],
+        "val": [1.0, 1.0, 1.0, 1.0, 1.0],
+        "b": [1.0, 2.0, 3.0],
+        "x": [2.0, -1.0, 3.0],
+        "tol": 1e-12,
+    },
+    "diagonal_solve_2": {
+        "source": "crates/cfd-math/src/linear_solver/krylov.rs:466-492",
+        "row_ptr": [0, 1, 2],
+        "col": [0, 1],
+        "val": [2.0, 3.0],
+        "b": [2.0, 6.0],
+        "x": [1.0, 2.0],
+        "tolerance": 1e-12,
+        "max_iterations": 20,
+        "tol": 1e-10,
+    },
+    "jacobi_tiny_diagonal": {
+        "source": "crates/cfd-1d/src/solver/core/linear_system.rs:339-349",
+        "row_ptr": [0, 1, 2],
+        "col": [0, 1],
+        "val": [1.0e-18, 2.0],
+        "inv_diag": [1.0, 0.5],
+        "tol": 1e-12,
+    },
+    "amg_poisson_2d_16": {
+        "source": "crates/cfd-math/tests/amg_integration_test.rs:17-122,212-268",
+        "matrix": "poisson_2d(16): 4 on the diagonal, -1 to grid neighbours",
+        "n": 16,
+        "manufactured": "x*_k = sin(pi t) + 0.5 t, t = k / n^2; b = A x*",
+        "tolerance": 1e-10,
+        "max_iterations": 200,
+        "max_abs_error": 1e-6,
+        "contraction_sizes": [8, 16],
+        "contraction_steps": 5,
+        "contraction_bound": 1.0,
+    },
+    "kirchhoff_abc": {
+        "source": "crates/cfd-1d/src/solver/core/matrix_assembly.rs:270-410",
+        "edges": [[0, 1, 1.0], [1, 2, 2.0]],
+        "dirichlet": {"0": 100.0, "2": 0.0},
+        "diag_b": 3.0,
+        "rhs_b": 100.0,
+        "rhs_b_with_neumann_5": 105.0,
+        "tol": 1e-12,
+    },
+}
+
+
+def main():
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
+    with open(out, "w") as f:
+        json.dump(GOLDEN, f, indent=1, sort_keys=True)
+    print(out)
+
+
+if __name__ == "__main__":
+    main()

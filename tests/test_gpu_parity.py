@@ -1,0 +1,296 @@
+"""GPU parity: the sm_100a path through the C ABI against the CPU oracle.
+
+Tolerances (FP64 path): SpMV 1e-13 relative; hierarchy operators 1e-13;
+V-cycle output 1e-11; Krylov solutions 1e-10 relative difference at an equal
+residual tolerance with the same iteration count. FP32+refinement: solution
+error <= 1e-8 against the FP64 oracle solution.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from helpers import csr_from_lists, grid_laplacian, manufactured, tridiag
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def dev(torch, a, dtype=None):
+    return torch.as_tensor(np.ascontiguousarray(a), device="cuda", dtype=dtype or torch.float64)
+
+
+def random_csr(rng, n, ncols, lens):
+    rp, col, val = [0], [], []
+    for i in range(n):
+        k = int(lens[i])
+        cols = np.sort(rng.choice(ncols, size=min(k, ncols), replace=False))
+        col += cols.tolist()
+        val += rng.uniform(-1, 1, cols.size).tolist()
+        rp.append(len(col))
+    return csr_from_lists(rp, col, val, ncols)
+
+
+def test_spmv_golden(cuda, golden):
+    from cfdrs_b200.device import DeviceCsr
+    g = golden["spmv_3x3"]
+    A = DeviceCsr(csr_from_lists(g["row_ptr"], g["col"], g["val"]))
+    x = dev(cuda, g["x"])
+    y = cuda.zeros(3, device="cuda", dtype=cuda.float64)
+    A.spmv(x.data_ptr(), y.data_ptr())
+    cuda.cuda.synchronize()
+    np.testing.assert_allclose(y.cpu().numpy(), g["y"], atol=g["tol"])
+
+
+@pytest.mark.parametrize("shape", ["stencil", "ragged", "long_rows", "rectangular"])
+def test_spmv_vs_oracle(cuda, oracle, shape):
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.device import DeviceCsr
+    rng = np.random.default_rng(7)
+    if shape == "stencil":
+        A = P.poisson_3d_variable(20, 4.0, 1.0, seed=2)[0]
+    elif shape == "ragged":  # empty rows and short rows of uneven length
+        A = random_csr(rng, 3000, 3000, rng.integers(0, 12, 3000))
+    elif shape == "long_rows":  # rows beyond the 2048-nonzero staging capacity
+        lens = rng.integers(1, 20, 600)
+        lens[[5, 300, 599]] = [2500, 4096, 3001]
+        A = random_csr(rng, 600, 5000, lens)
+    else:
+        A = random_csr(rng, 700, 1900, rng.integers(0, 30, 700))
+    x = rng.uniform(-1, 1, A.ncols)
+    ref = oracle.Csr.from_matrix(A).spmv(x)
+    d = DeviceCsr(A)
+    y = cuda.zeros(A.nrows, device="cuda", dtype=cuda.float64)
+    d.spmv(dev(cuda, x).data_ptr(), y.data_ptr())
+    cuda.cuda.synchronize()
+    np.testing.assert_allclose(y.cpu().numpy(), ref, rtol=1e-13, atol=1e-13 * np.abs(ref).max())
+    y32 = cuda.zeros(A.nrows, device="cuda", dtype=cuda.float32)
+    d.spmv(dev(cuda, x, cuda.float32).data_ptr(), y32.data_ptr(), fp32=True)
+    cuda.cuda.synchronize()
+    assert rel(y32.cpu().numpy().astype(np.float64), ref) < 1e-5
+
+
+@pytest.mark.parametrize("interp", [0, 2])
+def test_amg_hierarchy_matches_oracle(cuda, oracle, interp):
+    """Reference classical (0) and modified classical (2) hierarchies, level by level."""
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.multigrid import AlgebraicMultigrid, AMGConfig, InterpolationStrategy
+    A = P.poisson_3d_variable(16, 4.0, 1.0, seed=5)[0]
+    cfg = AMGConfig.pressure_poisson()
+    cfg.min_coarse_size = 100
+    cfg.interpolation_strategy = InterpolationStrategy(interp)
+    amg = AlgebraicMultigrid(A, cfg)
+    ocfg = oracle.AmgConfig(max_levels=16, min_coarse_size=100, smoother=oracle.SMOOTH_JACOBI, pre_smooth=1,
+                            post_smooth=1, relaxation=2 / 3, coarse_solve=oracle.COARSE_DENSE,
+                            interpolation=interp)
+    oamg = oracle.Amg(oracle.Csr.from_matrix(A), ocfg)
+    assert amg.num_levels == oamg.num_levels >= 3
+    for l in range(amg.num_levels):
+        for which in (0, 1, 2):
+            if which and l == amg.num_levels - 1:
+                continue
+            mine = amg.level(l, which)
+            rp, ci, v, shape = oamg.level(l, which).arrays()
+            assert mine.shape == shape
+            np.testing.assert_array_equal(mine.row_ptr, rp)
+            np.testing.assert_array_equal(mine.col, ci)
+            np.testing.assert_allclose(mine.val, v, rtol=1e-13, atol=1e-13 * np.abs(v).max())
+
+
+@pytest.mark.parametrize("coarse", ["dense", "sweeps"])
+def test_vcycle_matches_oracle(cuda, oracle, coarse):
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.multigrid import AlgebraicMultigrid, AMGConfig, CoarseSolve
+    A = P.poisson_3d_variable(16, 4.0, 1.0, seed=6)[0]
+    cfg = AMGConfig.pressure_poisson()
+    cfg.min_coarse_size = 100
+    cfg.coarse_solve = CoarseSolve.DENSE if coarse == "dense" else CoarseSolve.SWEEPS
+    amg = AlgebraicMultigrid(A, cfg)
+    oamg = oracle.Amg(oracle.Csr.from_matrix(A), oracle.AmgConfig(
+        max_levels=16, min_coarse_size=100, smoother=oracle.SMOOTH_JACOBI, pre_smooth=1, post_smooth=1,
+        relaxation=2 / 3, coarse_solve=oracle.COARSE_DENSE if coarse == "dense" else oracle.COARSE_SWEEPS,
+        interpolation=2))
+    r = np.random.default_rng(1).uniform(-1, 1, A.nrows)
+    z = amg.apply_to(r)
+    assert rel(z, oamg.apply(r)) < 1e-11
+
+
+def _oracle_solve(oracle, A, b, pre, solver="pcg", amg=None, rtol=1e-8, max_it=5000):
+    Ao = oracle.Csr.from_matrix(A)
+    return getattr(oracle, solver)(Ao, b, precond=pre, amg=amg, rtol=rtol, max_it=max_it)
+
+
+def test_pcg_jacobi_c1_parity(cuda, oracle):
+    """2-D pressure Poisson 128x128, Jacobi-PCG to 1e-8 (the CPU-runnable case)."""
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    A, b = P.poisson_2d_dirichlet(128, seed=0)
+    xo, ro = _oracle_solve(oracle, A, b, oracle.PRE_JACOBI)
+    x = np.zeros_like(b)
+    rep = cf.cg_preconditioned(A, b, cf.JacobiPreconditioner(A), x,
+                               cf.IterativeSolverConfig(0.0, 1e-8, 5000))
+    assert rep.termination == cf.Termination.CONVERGED and ro.termination == "Converged"
+    assert abs(rep.iterations - ro.iterations) <= 1
+    assert rel(x, xo) < 1e-10
+    assert np.linalg.norm(b - A.matvec(x)) <= 1.0000001e-8 * np.linalg.norm(b)
+
+
+def test_amg_pcg_parity(cuda, oracle):
+    """3-D Poisson (constant k), AMG-PCG V(1,1) Jacobi w=2/3, dense coarsest, to 1e-8."""
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    A, b = P.poisson_3d_fv(32, seed=1)
+    cfg = cf.AMGConfig.pressure_poisson()
+    cfg.min_coarse_size = 512
+    amg = cf.AlgebraicMultigrid(A, cfg)
+    oamg = oracle.Amg(oracle.Csr.from_matrix(A), oracle.AmgConfig(
+        max_levels=16, min_coarse_size=512, smoother=oracle.SMOOTH_JACOBI, pre_smooth=1, post_smooth=1,
+        relaxation=2 / 3, coarse_solve=oracle.COARSE_DENSE, interpolation=2))
+    xo, ro = _oracle_solve(oracle, A, b, oracle.PRE_AMG, amg=oamg)
+    x = np.zeros_like(b)
+    rep = cf.cg_preconditioned(A, b, amg, x, cf.IterativeSolverConfig(0.0, 1e-8, 500))
+    assert rep.termination == cf.Termination.CONVERGED
+    assert rep.iterations == ro.iterations
+    assert rel(x, xo) < 1e-10
+
+
+@pytest.mark.parametrize("pre", ["none", "jacobi", "amg"])
+def test_bicgstab_parity(cuda, oracle, pre):
+    import cfdrs_b200 as cf
+    if pre == "amg":
+        A = grid_laplacian(24)
+        b = A.matvec(manufactured(A.nrows))
+    else:
+        A = tridiag(400, lo=-1.3, d=3.0, hi=-0.7)
+        b = np.random.default_rng(3).uniform(-1, 1, 400)
+    amg = oamg = None
+    if pre == "amg":
+        cfg = cf.AMGConfig(pre_smooth_iterations=1, post_smooth_iterations=1, relaxation_factor=2 / 3)
+        amg = cf.AlgebraicMultigrid(A, cfg)
+        oamg = oracle.Amg(oracle.Csr.from_matrix(A), oracle.AmgConfig(
+            smoother=oracle.SMOOTH_JACOBI, pre_smooth=1, post_smooth=1, relaxation=2 / 3))
+        P_ = amg
+    else:
+        P_ = cf.JacobiPreconditioner(A) if pre == "jacobi" else None
+    opre = {"none": oracle.PRE_NONE, "jacobi": oracle.PRE_JACOBI, "amg": oracle.PRE_AMG}[pre]
+    xo, ro = _oracle_solve(oracle, A, b, opre, solver="bicgstab", amg=oamg, rtol=1e-10)
+    x = np.zeros_like(b)
+    cfgs = cf.IterativeSolverConfig(0.0, 1e-10, 500)
+    rep = (cf.bicgstab_preconditioned(A, b, P_, x, cfgs) if P_ is not None else cf.bicgstab(A, b, x, cfgs))
+    assert rep.termination == cf.Termination.CONVERGED and ro.termination == "Converged"
+    assert abs(rep.iterations - ro.iterations) <= 1
+    assert rel(x, xo) < 1e-9
+
+
+@pytest.mark.parametrize("solver", ["cg", "bicgstab"])
+def test_diagonal_golden_gpu(cuda, golden, solver):
+    import cfdrs_b200 as cf
+    g = golden["diagonal_solve_2"]
+    A = csr_from_lists(g["row_ptr"], g["col"], g["val"])
+    for _ in range(2):
+        x = np.zeros(2)
+        fn = cf.cg if solver == "cg" else cf.bicgstab
+        rep = fn(A, np.array(g["b"]), x, cf.IterativeSolverConfig(g["tolerance"], 0.0, g["max_iterations"]))
+        assert rep.final_residual_norm <= rep.threshold
+        np.testing.assert_allclose(x, g["x"], atol=g["tol"])
+
+
+def test_amg_integration_gpu(cuda, golden):
+    """amg_integration_test.rs:97-122 on the device V-cycle (damped Jacobi smoother)."""
+    import cfdrs_b200 as cf
+    g = golden["amg_poisson_2d_16"]
+    A = grid_laplacian(g["n"])
+    xs = manufactured(A.nrows)
+    b = A.matvec(xs)
+    amg = cf.AlgebraicMultigrid(A, cf.AMGConfig(relaxation_factor=2 / 3))
+    for fn in (cf.bicgstab_preconditioned, cf.cg_preconditioned):
+        x = np.zeros_like(b)
+        rep = fn(A, b, amg, x, cf.IterativeSolverConfig(g["tolerance"], 0.0, g["max_iterations"]))
+        assert rep.termination == cf.Termination.CONVERGED
+        assert np.max(np.abs(x - xs)) < g["max_abs_error"]
+
+
+@pytest.mark.parametrize("solver", ["cg", "bicgstab"])
+def test_fp32_refinement_error(cuda, oracle, solver):
+    """FP32 inner AMG Krylov + FP64 refinement to 1e-10: error vs the FP64 oracle <= 1e-8."""
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    A, b, _ = P.poisson_3d_variable(32, 8.0, 1.0, seed=0)
+    cfg = cf.AMGConfig.pressure_poisson()
+    cfg.min_coarse_size = 512
+    amg = cf.AlgebraicMultigrid(A, cfg)
+    oamg = oracle.Amg(oracle.Csr.from_matrix(A), oracle.AmgConfig(
+        max_levels=16, min_coarse_size=512, smoother=oracle.SMOOTH_JACOBI, pre_smooth=1, post_smooth=1,
+        relaxation=2 / 3, coarse_solve=oracle.COARSE_DENSE, interpolation=2))
+    xo, ro = _oracle_solve(oracle, A, b, oracle.PRE_AMG, amg=oamg, rtol=1e-13, max_it=500)
+    x = np.zeros_like(b)
+    fn = cf.cg_preconditioned if solver == "cg" else cf.bicgstab_preconditioned
+    rep = fn(A, b, amg, x, cf.IterativeSolverConfig(0.0, 1e-10, 500), precision=cf.Precision.FP32_REFINE)
+    assert rep.termination == cf.Termination.CONVERGED
+    assert rep.outer_iterations >= 2
+    true_res = np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b)
+    assert true_res <= 1e-10 * 1.0001
+    assert rel(x, xo) <= 1e-8
+
+
+def test_device_pointer_solve_matches_host(cuda):
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    A, b = P.poisson_2d_dirichlet(48, seed=9)
+    x_host = np.zeros_like(b)
+    cfgs = cf.IterativeSolverConfig(0.0, 1e-9, 2000)
+    r1 = cf.cg_preconditioned(A, b, cf.JacobiPreconditioner(A), x_host, cfgs)
+    bd = dev(cuda, b)
+    xd = cuda.zeros_like(bd)
+    r2 = cf.cg_preconditioned(A, bd, cf.JacobiPreconditioner(A), xd, cfgs)
+    assert r1.iterations == r2.iterations
+    np.testing.assert_array_equal(xd.cpu().numpy(), x_host)
+
+
+def test_termination_and_errors(cuda):
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    A, b = P.poisson_2d_dirichlet(16, seed=1)
+    J = cf.JacobiPreconditioner(A)
+    rep = cf.cg_preconditioned(A, b, J, np.zeros_like(b), cf.IterativeSolverConfig(0.0, 1e-12, 1))
+    assert rep.termination == cf.Termination.MAX_ITERATIONS and rep.iterations == 1
+    assert cf.interpret("t", rep).kind == cf.SolveOutcome.STALLED
+    rep = cf.cg_preconditioned(A, np.zeros_like(b), J, np.zeros_like(b), cf.IterativeSolverConfig(0.0, 1e-8, 10))
+    assert rep.termination == cf.Termination.INITIAL_RESIDUAL and rep.iterations == 0
+    neg = csr_from_lists([0, 1, 2], [0, 1], [-1.0, -2.0])
+    rep = cf.cg(neg, np.ones(2), np.zeros(2), cf.IterativeSolverConfig(0.0, 1e-8, 10))
+    assert rep.termination == cf.Termination.NON_POSITIVE_CURVATURE
+    assert cf.interpret("t", rep).kind == cf.SolveOutcome.BROKEN_DOWN
+    with pytest.raises(cf.SolveError):
+        cf.cg(A, b[:-1], np.zeros(A.nrows), cf.IterativeSolverConfig(0.0, 1e-8, 10))
+    with pytest.raises(cf.SolveError):
+        cf.cg(A, b, np.zeros_like(b), cf.IterativeSolverConfig(0.0, 1e-8, 0))
+    bad = csr_from_lists([0, 1, 2], [0, 1], [np.inf, 1.0])
+    with pytest.raises(cf.SolveError, match="NONFINITE"):
+        cf.cg_preconditioned(bad, np.ones(2), cf.JacobiPreconditioner(bad), np.zeros(2),
+                             cf.IterativeSolverConfig(0.0, 1e-8, 10))
+    x = np.zeros(2)
+    rep = cf.cg(csr_from_lists([0, 1, 2], [0, 1], [1.0, 1.0]), np.array([np.nan, 1.0]), x,
+                cf.IterativeSolverConfig(0.0, 1e-8, 10))
+    assert rep.termination == cf.Termination.BREAKDOWN
+
+
+def test_recompute_matches_fresh_setup(cuda):
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    A1 = P.poisson_3d_variable(12, 3.0, 1.0, seed=1)[0]
+    A2 = P.poisson_3d_variable(12, 3.0, 1.0, seed=2)[0]
+    cfg = cf.AMGConfig.pressure_poisson()
+    cfg.min_coarse_size = 64
+    amg = cf.AlgebraicMultigrid(A1, cfg)
+    amg.recompute(A2)
+    fresh_P = cf.AlgebraicMultigrid(A1.with_values(A1.val), cfg)
+    r = np.random.default_rng(0).uniform(-1, 1, A1.nrows)
+    z = amg.apply_to(r)
+    # recompute keeps the transfer operators of A1 and re-forms the Galerkin chain of A2
+    np.testing.assert_array_equal(amg.level(0, 1).val, fresh_P.level(0, 1).val)
+    np.testing.assert_allclose(amg.level(0, 0).val, A2.val)
+    assert np.all(np.isfinite(z))

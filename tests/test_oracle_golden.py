@@ -1,0 +1,171 @@
+"""Pins the CPU oracle against the reference's own known-answer tests
+(tests/golden/reference_golden.json) and against scipy as an independent referee."""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+
+from helpers import csr_from_lists, grid_laplacian, manufactured, tridiag
+
+
+def test_smoother_golden_vectors(oracle, golden):
+    g = golden["smoother_tridiagonal_5"]
+    A = oracle.Csr.from_matrix(tridiag(5))
+    x0, b = np.array(g["x0"]), np.array(g["b"])
+    for kind, key in [(oracle.SMOOTH_JACOBI, "jacobi"), (oracle.SMOOTH_GS, "gauss_seidel"),
+                      (oracle.SMOOTH_SGS, "symmetric_gauss_seidel"), (oracle.SMOOTH_GS, "sor_1")]:
+        x = oracle.smooth(A, x0, b, kind, g["relaxation"], g["sweeps"])
+        np.testing.assert_array_equal(x, np.array(g[key]), err_msg=key)
+
+
+def test_strength_golden(oracle, golden):
+    g = golden["strength_grid_4x4"]
+    S = oracle.strength(oracle.Csr.from_matrix(grid_laplacian(4)), g["theta"])
+    rp, ci, v, _ = S.arrays()
+    assert rp[-1] == g["nnz"]
+    assert list(ci[rp[0]:rp[1]]) == g["row0_cols"] and list(v[rp[0]:rp[1]]) == g["row0_vals"]
+    assert list(ci[rp[5]:rp[6]]) == g["row5_cols"] and list(v[rp[5]:rp[6]]) == g["row5_vals"]
+
+
+def test_spmv_golden(oracle, golden):
+    g = golden["spmv_3x3"]
+    A = oracle.Csr.from_matrix(csr_from_lists(g["row_ptr"], g["col"], g["val"]))
+    np.testing.assert_allclose(A.spmv(np.array(g["x"])), g["y"], atol=g["tol"])
+
+
+def test_coarsest_dense_golden(oracle, golden):
+    g = golden["coarsest_solve_3x3"]
+    A = oracle.Csr.from_matrix(csr_from_lists(g["row_ptr"], g["col"], g["val"]))
+    np.testing.assert_allclose(oracle.dense_solve(A, np.array(g["b"])), g["x"], atol=g["tol"])
+
+
+@pytest.mark.parametrize("solver", ["pcg", "bicgstab"])
+def test_diagonal_solve_golden(oracle, golden, solver):
+    g = golden["diagonal_solve_2"]
+    A = oracle.Csr.from_matrix(csr_from_lists(g["row_ptr"], g["col"], g["val"]))
+    fn = getattr(oracle, solver)
+    for _ in range(2):  # reusable-workspace test runs the solve twice
+        x, rep = fn(A, np.array(g["b"]), tol=g["tolerance"], rtol=0.0, max_it=g["max_iterations"])
+        assert rep.final_residual <= rep.threshold
+        np.testing.assert_allclose(x, g["x"], atol=g["tol"])
+
+
+def test_amg_integration_bicgstab(oracle, golden):
+    """amg_integration_test.rs:97-122 with AMGConfig::default (RS, classical, GS 2/2)."""
+    g = golden["amg_poisson_2d_16"]
+    n = g["n"]
+    A = grid_laplacian(n)
+    xs = manufactured(n * n)
+    b = A.matvec(xs)
+    Ao = oracle.Csr.from_matrix(A)
+    amg = oracle.Amg(Ao, oracle.AmgConfig())
+    x, rep = oracle.bicgstab(Ao, b, precond=oracle.PRE_AMG, amg=amg, tol=g["tolerance"], rtol=0.0,
+                             max_it=g["max_iterations"])
+    assert rep.termination == "Converged"
+    assert np.max(np.abs(x - xs)) < g["max_abs_error"]
+    x, rep = oracle.pcg(Ao, b, precond=oracle.PRE_AMG, amg=oracle.Amg(Ao, oracle.AmgConfig(
+        smoother=oracle.SMOOTH_JACOBI, relaxation=2 / 3, pre_smooth=1, post_smooth=1)),
+        tol=g["tolerance"], rtol=0.0, max_it=g["max_iterations"])
+    assert rep.termination == "Converged" and np.max(np.abs(x - xs)) < g["max_abs_error"]
+
+
+def test_amg_contraction(oracle, golden):
+    """amg_integration_test.rs:212-268: stationary AMG iteration contracts in the A-norm."""
+    g = golden["amg_poisson_2d_16"]
+    for n in g["contraction_sizes"]:
+        A = grid_laplacian(n)
+        S = A.to_scipy()
+        xs = manufactured(n * n)
+        b = S @ xs
+        Ao = oracle.Csr.from_matrix(A)
+        amg = oracle.Amg(Ao, oracle.AmgConfig())
+        x = np.zeros(n * n)
+        en = lambda v: np.sqrt(max(v @ (S @ v), 0.0))  # noqa: E731
+        prev, worst = en(xs - x), 0.0
+        for _ in range(g["contraction_steps"]):
+            x = x + amg.apply(b - S @ x)
+            e = en(xs - x)
+            worst = max(worst, e / prev)
+            prev = e
+            if e == 0:
+                break
+        assert worst < g["contraction_bound"]
+
+
+def test_amg_single_level_and_depth_cap(oracle):
+    """amg_integration_test.rs:170-209: tiny matrix -> one level, still nonzero z; max_levels=1 honoured."""
+    A = oracle.Csr.from_matrix(grid_laplacian(4))
+    amg = oracle.Amg(A, oracle.AmgConfig())
+    assert amg.num_levels == 1
+    assert np.any(amg.apply(manufactured(16)) != 0)
+    deep = oracle.Amg(oracle.Csr.from_matrix(grid_laplacian(16)), oracle.AmgConfig(max_levels=1))
+    assert deep.num_levels == 1
+
+
+def test_ruge_stueben_tree_matches_reference_scan(oracle):
+    """The O(log n) tournament pick equals the reference's first-maximum scan (algorithms.rs:64-74)."""
+    from cfdrs_b200 import problems as P
+    for A in [grid_laplacian(9), P.poisson_3d_fv(6)[0], P.poisson_3d_variable(8, 2.0, 1.0, seed=3)[0]]:
+        Ao = oracle.Csr.from_matrix(A)
+        cp_fast, f_fast = oracle.coarsen(Ao, oracle.RUGE_STUEBEN, 0.25, literal_scan=False)
+        cp_lit, f_lit = oracle.coarsen(Ao, oracle.RUGE_STUEBEN, 0.25, literal_scan=True)
+        np.testing.assert_array_equal(cp_fast, cp_lit)
+        np.testing.assert_array_equal(f_fast, f_lit)
+
+
+def test_pcg_against_scipy(oracle):
+    from cfdrs_b200 import problems as P
+    A, b = P.poisson_2d_dirichlet(32, seed=4)
+    Ao = oracle.Csr.from_matrix(A)
+    x, rep = oracle.pcg(Ao, b, precond=oracle.PRE_JACOBI, rtol=1e-12, max_it=2000)
+    assert rep.termination == "Converged"
+    xs = spla.spsolve(A.to_scipy().tocsc(), b)
+    np.testing.assert_allclose(x, xs, rtol=1e-9, atol=1e-10)
+
+
+def test_bicgstab_nonsymmetric_against_scipy(oracle):
+    n = 200
+    rng = np.random.default_rng(0)
+    A = tridiag(n, lo=-1.3, d=3.0, hi=-0.7)
+    b = rng.uniform(-1, 1, n)
+    x, rep = oracle.bicgstab(oracle.Csr.from_matrix(A), b, precond=oracle.PRE_JACOBI, rtol=1e-12, max_it=500)
+    assert rep.termination == "Converged"
+    np.testing.assert_allclose(x, spla.spsolve(A.to_scipy().tocsc(), b), rtol=1e-9, atol=1e-10)
+
+
+def test_termination_mapping(oracle):
+    from cfdrs_b200 import problems as P
+    A, b = P.poisson_2d_dirichlet(16, seed=1)
+    Ao = oracle.Csr.from_matrix(A)
+    _, rep = oracle.pcg(Ao, b, precond=oracle.PRE_JACOBI, rtol=1e-12, max_it=1)
+    assert rep.termination == "MaxIterations" and rep.iterations == 1
+    _, rep = oracle.pcg(Ao, np.zeros_like(b), precond=oracle.PRE_JACOBI, rtol=1e-8, max_it=10)
+    assert rep.termination == "InitialResidual" and rep.iterations == 0
+    neg = csr_from_lists([0, 1, 2], [0, 1], [-1.0, -2.0])
+    _, rep = oracle.pcg(oracle.Csr.from_matrix(neg), np.array([1.0, 1.0]), precond=oracle.PRE_NONE, rtol=1e-8)
+    assert rep.termination == "NonPositiveCurvature"
+
+
+def test_jacobi_tiny_diagonal(oracle, golden):
+    """linear_system.rs:339-349: |d| <= eps gives identity for that row."""
+    g = golden["jacobi_tiny_diagonal"]
+    A = oracle.Csr.from_matrix(csr_from_lists(g["row_ptr"], g["col"], g["val"]))
+    b = np.array([3.0, 4.0])
+    x, rep = oracle.pcg(A, b, precond=oracle.PRE_JACOBI, rtol=0.0, tol=1e-30, max_it=1)
+    # one PCG step with z = inv_diag * r from x = 0: x = alpha * z
+    z = np.array(g["inv_diag"]) * b
+    alpha = (b @ z) / (z @ np.array([1e-18 * z[0], 2.0 * z[1]]))
+    np.testing.assert_allclose(x, alpha * z, rtol=1e-12)
+
+
+def test_kirchhoff_abc_golden(golden):
+    from cfdrs_b200 import problems as P
+    g = golden["kirchhoff_abc"]
+    e = np.array(g["edges"])
+    dirichlet = {int(k): v for k, v in g["dirichlet"].items()}
+    A, b = P.kirchhoff_assemble(3, e[:, 0].astype(int), e[:, 1].astype(int), e[:, 2], dirichlet)
+    D = A.to_scipy().toarray()
+    assert abs(D[1, 1] - g["diag_b"]) < g["tol"] and abs(b[1] - g["rhs_b"]) < g["tol"]
+    assert D[0, 0] == 1.0 and D[2, 2] == 1.0 and b[0] == 100.0 and b[2] == 0.0
+    assert D[1, 0] == 0.0 and D[1, 2] == 0.0
+    _, b5 = P.kirchhoff_assemble(3, e[:, 0].astype(int), e[:, 1].astype(int), e[:, 2], dirichlet, {1: 5.0})
+    assert abs(b5[1] - g["rhs_b_with_neumann_5"]) < g["tol"]
