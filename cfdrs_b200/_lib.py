@@ -25,6 +25,7 @@ EXPORTS = [
     "cfd_amg_config_default", "cfd_amg_setup", "cfd_amg_recompute", "cfd_amg_apply", "cfd_amg_stats",
     "cfd_amg_level", "cfd_amg_destroy",
     "cfd_solve_options_default", "cfd_solve", "cfd_last_kernel_stats",
+    "cfd_residual_norm_noalloc",
 ]
 
 
@@ -109,6 +110,7 @@ def load():
         "cfd_solve_options_default": (None, [P]),
         "cfd_solve": (C.c_int, [P, P, P, P, P, P, P]),
         "cfd_last_kernel_stats": (C.c_int, [P, P]),
+        "cfd_residual_norm_noalloc": (C.c_int, [I64, I64, P, P, P, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

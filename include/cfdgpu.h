@@ -185,6 +185,28 @@ typedef struct {
 cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, const double* b,
                      double* x, const cfd_solver_config* cfg, cfd_solve_report* rep);
 
+/* ---- residual without device allocation ---------------------------------
+ * No counterpart in the reference: an addition for callers that cannot
+ * allocate device memory -- a solver embedded in a host application whose
+ * memory manager has already reserved the device memory, or a latency-critical
+ * loop (a per-time-step convergence monitor, network solves issued from
+ * parallel design-search workers) where cudaMalloc/cudaFree would synchronize
+ * the device and serialize threads.
+ * Computes r = b - A x and *norm2 = ||r||_2^2 (FP64) on device arrays the
+ * caller owns: CSR (int32 row_ptr[nrows+1], int32 col[nnz], double val[nnz]),
+ * x[ncols], b[nrows], outputs r[nrows] and one double at norm2, enqueued on
+ * cuda_stream (NULL: the legacy default stream). It calls no cudaMalloc,
+ * cudaFree or allocating library routine: the reduction scratch is a 1 MiB
+ * array compiled into the library, held on every GPU that loads it until the
+ * process exits. Limit: nrows <= 33 546 240 (one partial sum per 256 rows);
+ * larger inputs return CFD_ERR_DIM. The first call on a device looks up the
+ * array's device address (set-up) and should come before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU (other streams,
+ * other threads) race; serialize them. */
+cfd_status cfd_residual_norm_noalloc(int64_t nrows, int64_t ncols, const int32_t* row_ptr,
+                                     const int32_t* col, const double* val, const double* x,
+                                     const double* b, double* r, double* norm2, void* cuda_stream);
+
 /* ---- per-kernel statistics of the last solve --------------------------- */
 typedef struct {
   int64_t launches;         /* kernels launched by the library in the last cfd_solve */
