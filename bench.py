@@ -178,7 +178,7 @@ def run_reference(args, world, rank):
     Ao = O.Csr.from_matrix(A)
     t0 = time.perf_counter()
     amg = O.Amg(Ao, O.AmgConfig(max_levels=16, min_coarse_size=4096, smoother=O.SMOOTH_JACOBI, pre_smooth=1,
-                                post_smooth=1, relaxation=2 / 3, coarse_solve=O.COARSE_DENSE, interpolation=2))
+                                post_smooth=1, relaxation=2 / 3, coarse_solve=O.COARSE_DENSE, interpolation=2, coarse_order=1))
     setup_s = time.perf_counter() - t0
     times, iters = [], None
     for s in range(args.warmup + args.steps):
@@ -370,7 +370,7 @@ def cpu_baseline_from_hierarchy(amg, A, b, iterations):
         levels.append([O.Csr.from_matrix(m) for m in mats])
     oamg = O.Amg.from_levels(levels, O.AmgConfig(max_levels=16, min_coarse_size=4096, smoother=O.SMOOTH_JACOBI,
                                                  pre_smooth=1, post_smooth=1, relaxation=2 / 3,
-                                                 coarse_solve=O.COARSE_DENSE, interpolation=2))
+                                                 coarse_solve=O.COARSE_DENSE, interpolation=2, coarse_order=1))
     Ao = levels[0][0]
     sample = 2
     O.pcg(Ao, b, precond=O.PRE_AMG, amg=oamg, rtol=0.0, tol=0.0, max_it=1)  # warm caches

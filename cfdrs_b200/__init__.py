@@ -12,7 +12,7 @@ from .krylov import (  # noqa: F401
     bicgstab, bicgstab_preconditioned, cg, cg_preconditioned, converged_or_none, interpret,
 )
 from .multigrid import (  # noqa: F401
-    AMGConfig, AMGStatistics, AlgebraicMultigrid, CoarseSolve, CoarseningStrategy, IdentityPreconditioner,
+    AMGConfig, AMGStatistics, AlgebraicMultigrid, CoarseOrder, CoarseSolve, CoarseningStrategy, IdentityPreconditioner,
     InterpolationStrategy, JacobiPreconditioner, SmootherType,
 )
 

@@ -536,6 +536,17 @@ bool dense_inverse(const HostCsr& a, std::vector<double>& inv) {
   return true;
 }
 
+// Renumber the coarse points by ascending fine index (f2c follows).
+void renumber_ascending(Coarsening& c) {
+  std::vector<int32_t> sorted(c.coarse_points);
+  std::sort(sorted.begin(), sorted.end());
+  std::vector<int32_t> newid(c.f2c.size(), -1);
+  for (size_t q = 0; q < sorted.size(); ++q) newid[sorted[q]] = (int32_t)q;
+  for (size_t i = 0; i < c.f2c.size(); ++i)
+    if (c.f2c[i] >= 0) c.f2c[i] = newid[c.coarse_points[c.f2c[i]]];
+  c.coarse_points.swap(sorted);
+}
+
 // AlgebraicMultigrid::setup (amg.rs:217-288) and build_next_level (:290-380):
 // coarsen while levels < max_levels and n > min_coarse_size; R = P^T; the
 // Galerkin operator is (R A) P.
@@ -552,6 +563,7 @@ std::vector<HostLevel> build_hierarchy(const HostCsr& a, const cfd_amg_config& c
     else
       c = ruge_stueben(cur, cfg.strength_threshold);
     const int64_t nc = (int64_t)c.coarse_points.size();
+    if (cfg.coarse_order == CFD_COARSE_ORDER_ASCENDING) renumber_ascending(c);
     HostCsr p = cfg.interpolation == CFD_INTERP_DIRECT               ? direct_interpolation(c, cur.nrows)
                 : cfg.interpolation == CFD_INTERP_MODIFIED_CLASSICAL ? modified_classical_interpolation(cur, c)
                                                                      : classical_interpolation(cur, c);

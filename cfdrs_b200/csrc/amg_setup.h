@@ -24,6 +24,7 @@ Coarsening ruge_stueben(const HostCsr& a, double theta);
 Coarsening aggregation(const HostCsr& a, int64_t max_size);
 Coarsening pmis(const HostCsr& a, double theta, uint64_t seed);
 
+void renumber_ascending(Coarsening& c);
 HostCsr classical_interpolation(const HostCsr& a, const Coarsening& c);
 HostCsr modified_classical_interpolation(const HostCsr& a, const Coarsening& c);
 HostCsr direct_interpolation(const Coarsening& c, int64_t n);

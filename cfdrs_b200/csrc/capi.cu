@@ -543,6 +543,8 @@ void cfd_amg_config_default(cfd_amg_config* c) {
   c->coarse_sweeps = 10;
   c->aggregate_size = 8;
   c->seed = 0;
+  c->coarse_order = CFD_COARSE_ORDER_SELECTION;
+  c->reserved = 0;
 }
 
 cfd_status cfd_amg_setup(cfd_csr* a, const cfd_amg_config* cfg, cfd_amg** out) {
@@ -551,7 +553,7 @@ cfd_status cfd_amg_setup(cfd_csr* a, const cfd_amg_config* cfg, cfd_amg** out) {
   if (cfg->max_levels < 1 || cfg->max_levels > 16 || cfg->smoother != CFD_SMOOTH_JACOBI ||
       cfg->pre_smooth < 0 || cfg->post_smooth < 0 || !(cfg->strength_threshold >= 0.0) ||
       !std::isfinite(cfg->relaxation) || cfg->coarsening < 0 || cfg->coarsening > 2 || cfg->interpolation < 0 ||
-      cfg->interpolation > 2) {
+      cfg->interpolation > 2 || cfg->coarse_order < 0 || cfg->coarse_order > 1) {
     set_error("invalid AMG configuration");
     return CFD_ERR_CONFIG;
   }

@@ -35,6 +35,11 @@ class SmootherType(enum.IntEnum):
     JACOBI = 0
 
 
+class CoarseOrder(enum.IntEnum):
+    SELECTION = 0  # coarse index = selection order (the reference)
+    ASCENDING = 1  # coarse points numbered by ascending fine index (local P/R gathers)
+
+
 class CoarseSolve(enum.IntEnum):
     SWEEPS = 0  # smoother sweeps at the coarsest level (amg.rs:499-501)
     DENSE = 1   # exact FP64 solve with the dense inverse
@@ -56,22 +61,25 @@ class AMGConfig:
     coarse_sweeps: int = 10
     aggregate_size: int = 8
     seed: int = 0
+    coarse_order: CoarseOrder = CoarseOrder.SELECTION
 
     @classmethod
     def pressure_poisson(cls) -> "AMGConfig":
         """V(1,1), damped Jacobi w = 2/3, coarsening to <= 4096 unknowns, exact
         FP64 coarsest solve, Ruge-Stueben coarsening with modified classical
-        interpolation: the configuration of the 3-D Poisson workloads."""
+        interpolation and ascending coarse numbering: the configuration of the
+        3-D Poisson workloads."""
         return cls(max_levels=16, min_coarse_size=4096, pre_smooth_iterations=1, post_smooth_iterations=1,
                    relaxation_factor=2.0 / 3.0, coarse_solve=CoarseSolve.DENSE,
-                   interpolation_strategy=InterpolationStrategy.MODIFIED_CLASSICAL)
+                   interpolation_strategy=InterpolationStrategy.MODIFIED_CLASSICAL,
+                   coarse_order=CoarseOrder.ASCENDING)
 
     def to_c(self) -> _lib.AmgConfigC:
         return _lib.AmgConfigC(self.max_levels, int(self.coarsening_strategy), self.min_coarse_size,
                                int(self.interpolation_strategy), int(self.smoother_type),
                                self.pre_smooth_iterations, self.post_smooth_iterations, self.relaxation_factor,
                                self.strength_threshold, int(self.coarse_solve), self.coarse_sweeps,
-                               self.aggregate_size, self.seed)
+                               self.aggregate_size, self.seed, int(self.coarse_order), 0)
 
 
 @dataclass

@@ -105,6 +105,11 @@ typedef enum {
 } cfd_interpolation;
 typedef enum { CFD_SMOOTH_JACOBI = 0 } cfd_smoother;
 typedef enum { CFD_COARSE_SWEEPS = 0, CFD_COARSE_DENSE = 1 } cfd_coarse_solve;
+/* SELECTION: coarse index = order of selection (the reference, algorithms.rs:81-85).
+ * ASCENDING: coarse points numbered by ascending fine index -- the same
+ * hierarchy up to a symmetric permutation per level (from level 2 on the
+ * coarsening sees the permuted operator), with local P/R gathers. */
+typedef enum { CFD_COARSE_ORDER_SELECTION = 0, CFD_COARSE_ORDER_ASCENDING = 1 } cfd_coarse_order;
 
 typedef struct {
   int32_t max_levels;          /* AMGConfig::max_levels (default 10) */
@@ -120,6 +125,8 @@ typedef struct {
   int32_t coarse_sweeps;       /* sweeps for CFD_COARSE_SWEEPS (reference: 10) */
   int64_t aggregate_size;      /* aggregation coarsening (reference passes 8, amg.rs:304) */
   uint64_t seed;               /* PMIS priorities (the reference draws them unseeded) */
+  int32_t coarse_order;        /* cfd_coarse_order: numbering of each level's coarse points */
+  int32_t reserved;
 } cfd_amg_config;
 
 void cfd_amg_config_default(cfd_amg_config* cfg);

@@ -776,6 +776,16 @@ or_amg* or_amg_setup(const or_csr* a, const or_amg_config* cfg) {
       nc = aggregation(cur, cfg->aggregate_size, cp, map, &s);
     else
       nc = pmis(cur, cfg->strength_threshold, cfg->seed, cp, map, &s);
+    if (cfg->coarse_order == 1) {
+      // Number coarse points in ascending fine index instead of selection order.
+      std::vector<int64_t> sorted(cp);
+      std::sort(sorted.begin(), sorted.end());
+      std::vector<int64_t> newid(cur.nrows, -1);
+      for (size_t q = 0; q < sorted.size(); ++q) newid[sorted[q]] = (int64_t)q;
+      for (int64_t i = 0; i < cur.nrows; ++i)
+        if (map[i] >= 0) map[i] = newid[cp[map[i]]];
+      cp.swap(sorted);
+    }
     or_csr p = cfg->interpolation == 0   ? classical_interp(cur, cp, s)
                : cfg->interpolation == 2 ? modified_classical_interp(cur, cp, s)
                                          : direct_interp(map, cur.nrows, nc);

@@ -82,6 +82,8 @@ typedef struct {
   int32_t coarse_sweeps;   /* reference: 10 */
   int64_t aggregate_size;  /* reference: 8 */
   uint64_t seed;           /* PMIS priorities */
+  int32_t coarse_order;    /* 0 selection order (reference), 1 ascending fine index */
+  int32_t pad;
 } or_amg_config;
 
 or_amg* or_amg_setup(const or_csr* a, const or_amg_config* cfg);

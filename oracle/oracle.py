@@ -35,7 +35,8 @@ class _AmgConfig(C.Structure):
                 ("smoother", C.c_int32), ("pre_smooth", C.c_int32), ("post_smooth", C.c_int32),
                 ("relaxation", C.c_double), ("strength_threshold", C.c_double),
                 ("coarse_solve", C.c_int32), ("coarse_sweeps", C.c_int32),
-                ("aggregate_size", C.c_int64), ("seed", C.c_uint64)]
+                ("aggregate_size", C.c_int64), ("seed", C.c_uint64), ("coarse_order", C.c_int32),
+                ("pad", C.c_int32)]
 
 
 class _SolverConfig(C.Structure):
@@ -213,12 +214,13 @@ class AmgConfig:
     coarse_sweeps: int = 10
     aggregate_size: int = 8
     seed: int = 0
+    coarse_order: int = 0  # 0 selection order (reference), 1 ascending fine index
 
     def _c(self):
         return _AmgConfig(self.max_levels, self.coarsening, self.min_coarse_size, self.interpolation,
                           self.smoother, self.pre_smooth, self.post_smooth, self.relaxation,
                           self.strength_threshold, self.coarse_solve, self.coarse_sweeps,
-                          self.aggregate_size, self.seed)
+                          self.aggregate_size, self.seed, self.coarse_order, 0)
 
 
 class Amg:

@@ -73,19 +73,21 @@ def test_spmv_vs_oracle(cuda, oracle, shape):
     assert rel(y32.cpu().numpy().astype(np.float64), ref) < 1e-5
 
 
-@pytest.mark.parametrize("interp", [0, 2])
-def test_amg_hierarchy_matches_oracle(cuda, oracle, interp):
-    """Reference classical (0) and modified classical (2) hierarchies, level by level."""
+@pytest.mark.parametrize("interp,order", [(0, 0), (2, 0), (2, 1)])
+def test_amg_hierarchy_matches_oracle(cuda, oracle, interp, order):
+    """Reference classical (0) / modified classical (2) interpolation, selection (0) /
+    ascending (1) coarse numbering: the hierarchies agree level by level."""
     from cfdrs_b200 import problems as P
     from cfdrs_b200.multigrid import AlgebraicMultigrid, AMGConfig, InterpolationStrategy
     A = P.poisson_3d_variable(16, 4.0, 1.0, seed=5)[0]
     cfg = AMGConfig.pressure_poisson()
     cfg.min_coarse_size = 100
     cfg.interpolation_strategy = InterpolationStrategy(interp)
+    cfg.coarse_order = order
     amg = AlgebraicMultigrid(A, cfg)
     ocfg = oracle.AmgConfig(max_levels=16, min_coarse_size=100, smoother=oracle.SMOOTH_JACOBI, pre_smooth=1,
                             post_smooth=1, relaxation=2 / 3, coarse_solve=oracle.COARSE_DENSE,
-                            interpolation=interp)
+                            interpolation=interp, coarse_order=order)
     oamg = oracle.Amg(oracle.Csr.from_matrix(A), ocfg)
     assert amg.num_levels == oamg.num_levels >= 3
     for l in range(amg.num_levels):
@@ -112,7 +114,7 @@ def test_vcycle_matches_oracle(cuda, oracle, coarse):
     oamg = oracle.Amg(oracle.Csr.from_matrix(A), oracle.AmgConfig(
         max_levels=16, min_coarse_size=100, smoother=oracle.SMOOTH_JACOBI, pre_smooth=1, post_smooth=1,
         relaxation=2 / 3, coarse_solve=oracle.COARSE_DENSE if coarse == "dense" else oracle.COARSE_SWEEPS,
-        interpolation=2))
+        interpolation=2, coarse_order=1))
     r = np.random.default_rng(1).uniform(-1, 1, A.nrows)
     z = amg.apply_to(r)
     assert rel(z, oamg.apply(r)) < 1e-11
@@ -148,7 +150,7 @@ def test_amg_pcg_parity(cuda, oracle):
     amg = cf.AlgebraicMultigrid(A, cfg)
     oamg = oracle.Amg(oracle.Csr.from_matrix(A), oracle.AmgConfig(
         max_levels=16, min_coarse_size=512, smoother=oracle.SMOOTH_JACOBI, pre_smooth=1, post_smooth=1,
-        relaxation=2 / 3, coarse_solve=oracle.COARSE_DENSE, interpolation=2))
+        relaxation=2 / 3, coarse_solve=oracle.COARSE_DENSE, interpolation=2, coarse_order=1))
     xo, ro = _oracle_solve(oracle, A, b, oracle.PRE_AMG, amg=oamg)
     x = np.zeros_like(b)
     rep = cf.cg_preconditioned(A, b, amg, x, cf.IterativeSolverConfig(0.0, 1e-8, 500))
@@ -224,7 +226,7 @@ def test_fp32_refinement_error(cuda, oracle, solver):
     amg = cf.AlgebraicMultigrid(A, cfg)
     oamg = oracle.Amg(oracle.Csr.from_matrix(A), oracle.AmgConfig(
         max_levels=16, min_coarse_size=512, smoother=oracle.SMOOTH_JACOBI, pre_smooth=1, post_smooth=1,
-        relaxation=2 / 3, coarse_solve=oracle.COARSE_DENSE, interpolation=2))
+        relaxation=2 / 3, coarse_solve=oracle.COARSE_DENSE, interpolation=2, coarse_order=1))
     xo, ro = _oracle_solve(oracle, A, b, oracle.PRE_AMG, amg=oamg, rtol=1e-13, max_it=500)
     x = np.zeros_like(b)
     fn = cf.cg_preconditioned if solver == "cg" else cf.bicgstab_preconditioned
