@@ -25,6 +25,8 @@ EXPORTS = [
     "cfd_amg_config_default", "cfd_amg_setup", "cfd_amg_recompute", "cfd_amg_apply", "cfd_amg_stats",
     "cfd_amg_level", "cfd_amg_destroy",
     "cfd_solve_options_default", "cfd_solve", "cfd_last_kernel_stats",
+    "cfd_batch_create", "cfd_batch_update_values", "cfd_batch_solve", "cfd_batch_autotune", "cfd_batch_config",
+    "cfd_batch_destroy",
     "cfd_residual_norm_noalloc",
 ]
 
@@ -57,6 +59,12 @@ class SolveReportC(C.Structure):
     _fields_ = [("termination", C.c_int32), ("outer_iterations", C.c_int32), ("iterations", C.c_int64),
                 ("initial_residual", C.c_double), ("final_residual", C.c_double),
                 ("threshold", C.c_double), ("device_ms", C.c_double)]
+
+
+class BatchReportC(C.Structure):
+    _fields_ = [("num_systems", C.c_int32), ("converged_systems", C.c_int32), ("total_iterations", C.c_int64),
+                ("max_iterations", C.c_int32), ("pad", C.c_int32), ("max_rel_residual", C.c_double),
+                ("device_ms", C.c_double)]
 
 
 class KernelStatsC(C.Structure):
@@ -110,6 +118,12 @@ def load():
         "cfd_solve_options_default": (None, [P]),
         "cfd_solve": (C.c_int, [P, P, P, P, P, P, P]),
         "cfd_last_kernel_stats": (C.c_int, [P, P]),
+        "cfd_batch_create": (C.c_int, [P, I32, P, P, P, P, PP]),
+        "cfd_batch_update_values": (C.c_int, [P, P]),
+        "cfd_batch_solve": (C.c_int, [P, P, P, P, P, P, P, P, P]),
+        "cfd_batch_autotune": (C.c_int, [P, I32, I32]),
+        "cfd_batch_config": (C.c_int, [P, I32, P, P, P]),
+        "cfd_batch_destroy": (C.c_int, [P]),
         "cfd_residual_norm_noalloc": (C.c_int, [I64, I64, P, P, P, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():

@@ -248,9 +248,10 @@ def random_network(n_nodes: int, rng: np.random.Generator, loop_fraction: float 
     U[50, 500] um, lengths U[1, 20] mm, mu = 1e-3 Pa s; node 0 fixed at ``p_in``,
     node n-1 at ``p_out``. Returns ``(A, b)`` from :func:`kirchhoff_assemble`."""
     n = int(n_nodes)
-    parent = np.array([rng.integers(0, i) for i in range(1, n)], dtype=np.int64)
-    ei = list(parent)
-    ej = list(range(1, n))
+    child = np.arange(1, n, dtype=np.int64)
+    parent = np.minimum((rng.random(n - 1) * child).astype(np.int64), child - 1)
+    ei = parent.tolist()
+    ej = child.tolist()
     seen = set(zip(np.minimum(ei, ej).tolist(), np.maximum(ei, ej).tolist()))
     extra = int(np.floor(loop_fraction * n))
     while extra > 0:
@@ -269,3 +270,11 @@ def random_network(n_nodes: int, rng: np.random.Generator, loop_fraction: float 
     length = rng.uniform(1e-3, 20e-3, size=m)
     g = hagen_poiseuille_conductance(d, length)
     return kirchhoff_assemble(n, ei, ej, g, {0: p_in, n - 1: p_out})
+
+
+def network_batch(num: int, seed: int = 0, n_min: int = 20, n_max: int = 2000, loop_fraction: float = 0.1):
+    """``num`` seeded networks with node counts uniform in [n_min, n_max]
+    (:func:`random_network` each). Returns a list of ``(A, b)``."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(n_min, n_max + 1, size=num)
+    return [random_network(int(n), rng, loop_fraction) for n in sizes]

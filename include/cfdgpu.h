@@ -192,6 +192,47 @@ typedef struct {
 cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, const double* b,
                      double* x, const cfd_solver_config* cfg, cfd_solve_report* rep);
 
+/* ---- batched small systems --------------------------------------------
+ * Many independent systems (e.g. the Kirchhoff networks of many design
+ * candidates) solved by Jacobi-PCG in one persistent launch per size bucket,
+ * replayed from a captured CUDA graph. Replaces calling
+ * LinearSystemSolver::solve_with_initial_guess once per network
+ * (crates/cfd-1d/src/solver/core/linear_system.rs:114-155) from the cfd-optim
+ * candidate fold (crates/cfd-optim/src/metrics/blueprint_graph.rs:48-135).
+ * Layout: system s owns global rows [sys_row_offsets[s], sys_row_offsets[s+1]);
+ * row_ptr holds global nonzero offsets (total_rows + 1 entries); col holds the
+ * column index LOCAL to the row's system. At most 2048 rows and 8192 nonzeros
+ * per system. Convergence per system: the row-equilibrated residual
+ * ||D(b - A x)|| <= max(tolerance, relative_tolerance * ||D(b - A x0)||),
+ * D = 1 / max_j |a_ij| (linear_system.rs:157-204). */
+typedef struct cfd_batch cfd_batch;
+typedef struct {
+  int32_t num_systems;
+  int32_t converged_systems;
+  int64_t total_iterations;   /* summed over systems (inner iterations for FP32_REFINE) */
+  int32_t max_iterations;     /* largest per-system count */
+  int32_t pad;
+  double max_rel_residual;    /* largest final equilibrated relative residual */
+  double device_ms;           /* copies in, graph, copies out (CUDA events) */
+} cfd_batch_report;
+cfd_status cfd_batch_create(cfd_context* ctx, int32_t num_systems, const int64_t* sys_row_offsets,
+                            const int64_t* row_ptr, const int32_t* col, const double* val,
+                            cfd_batch** out);
+cfd_status cfd_batch_update_values(cfd_batch* batch, const double* val_host);
+/* opt: solver CG, precond JACOBI, precision FP64 or FP32_REFINE, memory of b/x.
+ * x carries the initial guesses in and the solutions out. Per-system outputs
+ * (host arrays of num_systems entries) may be NULL. */
+cfd_status cfd_batch_solve(cfd_batch* batch, const cfd_solve_options* opt, const double* b, double* x,
+                           const cfd_solver_config* cfg, int32_t* termination, int32_t* iterations,
+                           double* rel_residual, cfd_batch_report* rep);
+/* Time each CTA width (32..512 threads) per size bucket on this batch with a
+ * fixed iteration budget and keep the fastest (per precision). */
+cfd_status cfd_batch_autotune(cfd_batch* batch, int32_t precision, int32_t sample_iterations);
+/* Bucket row limits, chosen CTA widths and systems per bucket (4 entries each). */
+cfd_status cfd_batch_config(const cfd_batch* batch, int32_t precision, int32_t* bucket_rows,
+                            int32_t* threads, int32_t* systems);
+cfd_status cfd_batch_destroy(cfd_batch* batch);
+
 /* ---- residual without device allocation ---------------------------------
  * No counterpart in the reference: an addition for callers that cannot
  * allocate device memory -- a solver embedded in a host application whose

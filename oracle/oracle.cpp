@@ -927,6 +927,86 @@ int or_pcg(const or_csr* a, int precond, const or_amg* amg, const double* b, dou
   return 0;
 }
 
+// Jacobi-PCG with the convergence test of the 1-D network solver: the
+// row-equilibrated residual ||D (b - A x)||_2 with D = 1 / max_j |a_ij|
+// (identity where the row maximum is not above f64::EPSILON or not finite),
+// crates/cfd-1d/src/solver/core/linear_system.rs:157-204; threshold
+// max(tolerance, relative_tolerance * ||D r0||).
+int or_pcg_equilibrated(const or_csr* a, const double* b, double* x, const or_solver_config* cfg, or_report* rep) {
+  const int64_t n = a->nrows;
+  if (a->ncols != n) return -1;
+  Precond M{OR_PRE_JACOBI, nullptr, {}};
+  if (jacobi_inverse(*a, M.inv) != 0) return -2;
+  std::vector<double> s(n, 1.0);
+  for (int64_t i = 0; i < n; ++i) {
+    double mx = 0.0;
+    for (int64_t k = a->rp[i]; k < a->rp[i + 1]; ++k) mx = std::max(mx, std::fabs(a->v[k]));
+    if (mx > DBL_EPSILON && std::isfinite(mx)) s[i] = 1.0 / mx;
+  }
+  auto enorm = [&](const std::vector<double>& r) {
+    double t = 0.0;
+    for (int64_t i = 0; i < n; ++i) t += (s[i] * r[i]) * (s[i] * r[i]);
+    return std::sqrt(t);
+  };
+  std::vector<double> r(n), z(n), p(n), q(n);
+  spmv_raw(*a, x, q.data());
+  for (int64_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+  double e = enorm(r);
+  rep->initial_residual = e;
+  rep->threshold = std::max(cfg->tolerance, cfg->relative_tolerance * e);
+  rep->final_residual = e;
+  rep->iterations = 0;
+  if (!std::isfinite(e)) {
+    rep->termination = OR_TERM_BREAKDOWN;
+    return 0;
+  }
+  if (e <= rep->threshold) {
+    rep->termination = OR_TERM_INITIAL_RESIDUAL;
+    return 0;
+  }
+  M.apply(r.data(), z.data(), n);
+  double rho = 0.0;
+  for (int64_t i = 0; i < n; ++i) rho += r[i] * z[i];
+  p = z;
+  for (int64_t it = 1; it <= cfg->max_iterations; ++it) {
+    spmv_raw(*a, p.data(), q.data());
+    double pq = 0.0;
+    for (int64_t i = 0; i < n; ++i) pq += p[i] * q[i];
+    if (!(pq > 0.0)) {
+      rep->termination = OR_TERM_NON_POSITIVE_CURVATURE;
+      return 0;
+    }
+    const double alpha = rho / pq;
+    for (int64_t i = 0; i < n; ++i) {
+      x[i] += alpha * p[i];
+      r[i] -= alpha * q[i];
+    }
+    e = enorm(r);
+    rep->iterations = it;
+    rep->final_residual = e;
+    if (!std::isfinite(e)) {
+      rep->termination = OR_TERM_BREAKDOWN;
+      return 0;
+    }
+    if (e <= rep->threshold) {
+      rep->termination = OR_TERM_CONVERGED;
+      return 0;
+    }
+    M.apply(r.data(), z.data(), n);
+    double rn = 0.0;
+    for (int64_t i = 0; i < n; ++i) rn += r[i] * z[i];
+    if (rn == 0.0 || !std::isfinite(rn)) {
+      rep->termination = OR_TERM_BREAKDOWN;
+      return 0;
+    }
+    const double beta = rn / rho;
+    for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+    rho = rn;
+  }
+  rep->termination = OR_TERM_MAX_ITERATIONS;
+  return 0;
+}
+
 // Right-preconditioned BiCGSTAB (Saad 2003, Alg. 7.7 with M^-1 applied to p and s).
 int or_bicgstab(const or_csr* a, int precond, const or_amg* amg, const double* b, double* x,
                 const or_solver_config* cfg, or_report* rep, double* history) {

@@ -121,6 +121,8 @@ typedef struct {
 /* Return 0 on success, <0 on a setup/dimension error (e.g. non-finite diagonal). */
 int or_pcg(const or_csr* a, int precond, const or_amg* amg, const double* b, double* x,
            const or_solver_config* cfg, or_report* rep, double* history);
+int or_pcg_equilibrated(const or_csr* a, const double* b, double* x, const or_solver_config* cfg,
+                        or_report* rep);
 int or_bicgstab(const or_csr* a, int precond, const or_amg* amg, const double* b, double* x,
                 const or_solver_config* cfg, or_report* rep, double* history);
 

@@ -93,6 +93,8 @@ def lib():
         L.or_amg_level.argtypes = [P, C.c_int, C.c_int]
         L.or_amg_apply.argtypes = [P, P, P]
         L.or_amg_free.argtypes = [P]
+        L.or_pcg_equilibrated.restype = C.c_int
+        L.or_pcg_equilibrated.argtypes = [P, P, P, P, P]
         for fn in (L.or_pcg, L.or_bicgstab):
             fn.restype = C.c_int
             fn.argtypes = [P, C.c_int, P, P, P, P, P, P]
@@ -300,6 +302,19 @@ def pcg(a, b, **kw):
 
 def bicgstab(a, b, **kw):
     return _krylov(lib().or_bicgstab, a, b, **kw)
+
+
+def pcg_equilibrated(a: Csr, b, x0=None, tol=0.0, rtol=1e-10, max_it=20000):
+    """Jacobi-PCG with the 1-D solver's row-equilibrated residual test."""
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+    cfg = _SolverConfig(tol, rtol, max_it)
+    rep = _Report()
+    rc = lib().or_pcg_equilibrated(a.h, _ptr(b), _ptr(x), C.byref(cfg), C.byref(rep))
+    if rc != 0:
+        raise ValueError(f"oracle solve setup failed ({rc})")
+    return x, Report(TERMINATIONS[rep.termination], rep.iterations, rep.initial_residual, rep.final_residual,
+                     rep.threshold, np.zeros(0))
 
 
 def set_threads(n: int):

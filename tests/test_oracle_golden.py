@@ -169,3 +169,14 @@ def test_kirchhoff_abc_golden(golden):
     assert D[1, 0] == 0.0 and D[1, 2] == 0.0
     _, b5 = P.kirchhoff_assemble(3, e[:, 0].astype(int), e[:, 1].astype(int), e[:, 2], dirichlet, {1: 5.0})
     assert abs(b5[1] - g["rhs_b_with_neumann_5"]) < g["tol"]
+
+
+def test_equilibrated_pcg_networks(oracle):
+    """Jacobi-PCG with the 1-D solver's equilibrated residual test reaches the
+    direct solution on seeded networks (linear_system.rs:157-204)."""
+    from cfdrs_b200 import problems as P
+    for A, b in P.network_batch(6, seed=2, n_min=20, n_max=400):
+        x, rep = oracle.pcg_equilibrated(oracle.Csr.from_matrix(A), b, rtol=1e-12)
+        assert rep.termination == "Converged"
+        xs = spla.spsolve(A.to_scipy().tocsc(), b)
+        assert np.linalg.norm(x - xs) <= 1e-6 * np.linalg.norm(xs)
