@@ -25,6 +25,7 @@ EXPORTS = [
     "cfd_amg_config_default", "cfd_amg_setup", "cfd_amg_recompute", "cfd_amg_apply", "cfd_amg_stats",
     "cfd_amg_level", "cfd_amg_destroy",
     "cfd_solve_options_default", "cfd_solve", "cfd_last_kernel_stats",
+    "cfd_pattern_outer", "cfd_csr_set_values_device",
     "cfd_batch_create", "cfd_batch_update_values", "cfd_batch_solve", "cfd_batch_autotune", "cfd_batch_config",
     "cfd_batch_destroy",
     "cfd_residual_norm_noalloc",
@@ -118,6 +119,8 @@ def load():
         "cfd_solve_options_default": (None, [P]),
         "cfd_solve": (C.c_int, [P, P, P, P, P, P, P]),
         "cfd_last_kernel_stats": (C.c_int, [P, P]),
+        "cfd_pattern_outer": (C.c_int, [P, P, P, D, P]),
+        "cfd_csr_set_values_device": (C.c_int, [P, P]),
         "cfd_batch_create": (C.c_int, [P, I32, P, P, P, P, PP]),
         "cfd_batch_update_values": (C.c_int, [P, P]),
         "cfd_batch_solve": (C.c_int, [P, P, P, P, P, P, P, P, P]),

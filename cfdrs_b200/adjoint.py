@@ -1,0 +1,181 @@
+"""Differentiable sparse solve: ``x = A^{-1} b`` as a ``torch.autograd.Function``
+whose backward is hand-written on the device.
+
+Backward of x = A^{-1} b for an upstream gradient g = dL/dx:
+    lambda = A^{-T} g        (a second solve with the same preconditioner; A symmetric)
+    dL/db  = lambda
+    dL/dA  = -lambda x^T on A's sparsity pattern (cfd_pattern_outer)
+
+Any differentiable assembly of A's values and b in torch (e.g.
+:func:`darcy_2d_torch`, k = exp(theta) with harmonic-mean faces) then carries
+the chain rule to its parameters. CFDrs has no differentiable solve; its Python
+layer (``crates/cfd-python/src/lib.rs:85-158``) exposes physics solvers only, so
+this module is new surface rather than a mirror.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from .device import device_matrix
+from .krylov import IterativeSolverConfig, Precision, SolveError, Termination, cg_preconditioned
+from .multigrid import AlgebraicMultigrid, AMGConfig, JacobiPreconditioner
+from .sparse import CsrMatrix
+
+
+class SparseSolver:
+    """Device solver for a fixed sparsity pattern whose values come from torch.
+
+    ``preconditioner``: "amg" (AMG-PCG) or "jacobi". With AMG, :meth:`set_values`
+    rebuilds the hierarchy when asked (``rebuild=True``) and otherwise follows
+    ``refresh``: "recompute" re-forms the Galerkin operators for the new values
+    with the cached transfer operators (``AlgebraicMultigrid::recompute``),
+    "keep" leaves the hierarchy as it is (still an SPD preconditioner; only its
+    quality for the new values changes, not the solution's accuracy).
+    """
+
+    def __init__(self, pattern: CsrMatrix, preconditioner: str = "amg", amg_config: AMGConfig | None = None,
+                 precision: Precision = Precision.FP32_REFINE,
+                 config: IterativeSolverConfig | None = None):
+        self.pattern = CsrMatrix(pattern.row_ptr, pattern.col, pattern.val.copy(), pattern.shape)
+        if self.pattern.nrows != self.pattern.ncols:
+            raise SolveError("SparseSolver needs a square matrix")
+        self.dm = device_matrix(self.pattern)
+        self.kind = preconditioner
+        self.amg_config = amg_config or AMGConfig.pressure_poisson()
+        self.precision = precision
+        self.config = config or IterativeSolverConfig(0.0, 1e-10, 2000)
+        self.amg = None
+        self.refresh = "recompute"
+        # position of the transpose of every entry (symmetry check of the pattern)
+        S = self.pattern.to_scipy().tocoo()
+        key = S.row.astype(np.int64) * self.pattern.ncols + S.col
+        keyT = S.col.astype(np.int64) * self.pattern.ncols + S.row
+        order = np.argsort(key)
+        pos = np.searchsorted(key[order], keyT)
+        ok = (pos < key.size) & (key[order][np.minimum(pos, key.size - 1)] == keyT)
+        self.pattern_symmetric = bool(ok.all())
+        self._transpose_pos = order[np.minimum(pos, key.size - 1)] if self.pattern_symmetric else None
+        self.symmetric = False
+
+    def set_values(self, values: torch.Tensor, rebuild: bool = False) -> None:
+        """New values (device float64, A's CSR order) for the fixed pattern."""
+        v = values.detach().to(dtype=torch.float64).contiguous()
+        if v.numel() != self.pattern.nnz or not v.is_cuda:
+            raise SolveError("values must be a CUDA float64 tensor with one entry per stored nonzero")
+        _lib.check(_lib.load().cfd_csr_set_values_device(self.dm.h, C.c_void_p(v.data_ptr())))
+        host = v.cpu().numpy()
+        self.pattern.val[:] = host
+        self.symmetric = self.pattern_symmetric and bool(
+            np.allclose(host, host[self._transpose_pos], rtol=1e-13, atol=0.0))
+        if self.kind == "amg":
+            if self.amg is None or rebuild:
+                self.amg = AlgebraicMultigrid(self.dm, self.amg_config, ctx=self.dm.ctx)
+            elif self.refresh == "recompute":
+                self.amg.recompute(self.dm)
+
+    def solve(self, b: torch.Tensor, precision: Precision | None = None,
+              config: IterativeSolverConfig | None = None) -> torch.Tensor:
+        x = torch.zeros_like(b, dtype=torch.float64)
+        pre = self.amg if self.kind == "amg" else JacobiPreconditioner(self.dm)
+        rep = cg_preconditioned(self.dm, b.to(torch.float64).contiguous(), pre, x, config or self.config,
+                                precision=self.precision if precision is None else precision)
+        if rep.termination not in (Termination.CONVERGED, Termination.INITIAL_RESIDUAL):
+            raise SolveError(f"sparse solve did not converge: {rep}")
+        self.last_report = rep
+        return x
+
+    def pattern_outer(self, lam: torch.Tensor, x: torch.Tensor, scale: float = 1.0) -> torch.Tensor:
+        """g_e = -scale * lam[row(e)] * x[col(e)] on A's pattern (device)."""
+        g = torch.empty(self.pattern.nnz, dtype=torch.float64, device=lam.device)
+        lam = lam.contiguous()
+        x = x.contiguous()
+        self.dm.ctx.set_stream(torch.cuda.current_stream(lam.device).cuda_stream)
+        try:
+            _lib.check(_lib.load().cfd_pattern_outer(self.dm.h, C.c_void_p(lam.data_ptr()),
+                                                     C.c_void_p(x.data_ptr()), scale, C.c_void_p(g.data_ptr())))
+        finally:
+            self.dm.ctx.set_stream(None)
+        return g
+
+
+class SparseSolveFunction(torch.autograd.Function):
+    """x = A(values)^{-1} b; gradients to ``values`` (on A's pattern) and ``b``."""
+
+    @staticmethod
+    def forward(ctx, values, b, solver: SparseSolver, rebuild: bool = False):
+        solver.set_values(values, rebuild=rebuild)
+        x = solver.solve(b)
+        ctx.solver = solver
+        ctx.save_for_backward(x)
+        return x
+
+    @staticmethod
+    def backward(ctx, gx):
+        solver: SparseSolver = ctx.solver
+        (x,) = ctx.saved_tensors
+        if not solver.symmetric:
+            raise SolveError("the adjoint solve reuses A and its preconditioner, so A must be symmetric")
+        lam = solver.solve(gx.contiguous())  # A^T lambda = dL/dx with A^T = A
+        gvals = solver.pattern_outer(lam, x)
+        return gvals, lam, None, None
+
+
+def sparse_solve(values, b, solver: SparseSolver, rebuild: bool = False):
+    return SparseSolveFunction.apply(values, b, solver, rebuild)
+
+
+# ---------------------------------------------------------------------------
+# 2-D Darcy assembly in torch (the same system as problems.darcy_2d).
+
+def darcy_2d_pattern(n: int):
+    """Pattern (CsrMatrix) and the (n, n, 5) mask of problems.darcy_2d."""
+    from .problems import darcy_2d
+    A, _ = darcy_2d(np.zeros((n, n)))
+    mask = np.zeros((n, n, 5), dtype=bool)
+    mask[1:, :, 0] = True
+    mask[:, 1:, 1] = True
+    mask[:, :, 2] = True
+    mask[:, :-1, 3] = True
+    mask[:-1, :, 4] = True
+    return A, mask
+
+
+def darcy_2d_torch(theta: torch.Tensor, mask: torch.Tensor):
+    """CSR values and right-hand side of -div(exp(theta) grad p) = 0 on an n x n
+    cell grid (row i + n*j), harmonic-mean faces, Dirichlet p = 1 (left) and
+    p = 0 (right) at half a cell, no flux top/bottom; differentiable in theta."""
+    n = theta.shape[0]
+    k = torch.exp(theta)
+
+    def hmean(a, b):
+        return 2.0 * a * b / (a + b)
+
+    fx = hmean(k[:, :-1], k[:, 1:])
+    fy = hmean(k[:-1, :], k[1:, :])
+    z = torch.zeros((n, n), dtype=theta.dtype, device=theta.device)
+    south = torch.cat([torch.zeros((1, n), dtype=theta.dtype, device=theta.device), -fy], dim=0)
+    north = torch.cat([-fy, torch.zeros((1, n), dtype=theta.dtype, device=theta.device)], dim=0)
+    west = torch.cat([torch.zeros((n, 1), dtype=theta.dtype, device=theta.device), -fx], dim=1)
+    east = torch.cat([-fx, torch.zeros((n, 1), dtype=theta.dtype, device=theta.device)], dim=1)
+    wall = z.clone()
+    wall = wall + torch.nn.functional.pad(2.0 * k[:, :1], (0, n - 1))
+    wall = wall + torch.nn.functional.pad(2.0 * k[:, -1:], (n - 1, 0))
+    diag = -(south + west + east + north) + wall
+    vals = torch.stack([south, west, diag, east, north], dim=-1)
+    values = vals[mask]
+    b = torch.nn.functional.pad(2.0 * k[:, :1], (0, n - 1)).reshape(-1)
+    return values, b
+
+
+def column_loss(p: torch.Tensor, n: int, column: int) -> torch.Tensor:
+    """Sum of p^2 over the n cells of grid column ``column`` (row index i + n*j)."""
+    return (p.reshape(n, n)[:, column] ** 2).sum()
+
+
+def loss_column_index(n: int, x: float = 0.75) -> int:
+    """First cell column whose centre (i + 1/2)/n is at or beyond ``x``."""
+    return int(np.ceil(x * n - 0.5))

@@ -192,6 +192,19 @@ typedef struct {
 cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, const double* b,
                      double* x, const cfd_solver_config* cfg, cfd_solve_report* rep);
 
+/* ---- adjoint building blocks ------------------------------------------
+ * No reference counterpart (CFDrs has no differentiable solve; its Python
+ * layer crates/cfd-python/src/lib.rs:85-158 exposes physics solvers only).
+ * For x = A^{-1} b and a loss L(x): lambda = A^{-T} dL/dx (for symmetric A a
+ * second cfd_solve with the same preconditioner), dL/db = lambda and
+ *   g[e] = dL/da_ij = -scale * lambda_i * x_j  for every stored entry e = (i, j).
+ * All pointers are device pointers; g has nnz entries in A's CSR order. */
+cfd_status cfd_pattern_outer(cfd_csr* a, const double* lambda_dev, const double* x_dev, double scale,
+                             double* g_dev);
+/* Replace A's values from device memory (same pattern); the host copy used by
+ * AMG setup/recompute is refreshed too. */
+cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev);
+
 /* ---- batched small systems --------------------------------------------
  * Many independent systems (e.g. the Kirchhoff networks of many design
  * candidates) solved by Jacobi-PCG in one persistent launch per size bucket,

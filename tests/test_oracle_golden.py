@@ -180,3 +180,26 @@ def test_equilibrated_pcg_networks(oracle):
         assert rep.termination == "Converged"
         xs = spla.spsolve(A.to_scipy().tocsc(), b)
         assert np.linalg.norm(x - xs) <= 1e-6 * np.linalg.norm(xs)
+
+
+def test_cpu_adjoint_against_fd_and_assembly():
+    """The CPU adjoint checker: its assembly equals problems.darcy_2d and the
+    torch assembly, and its hand-derived gradient matches central differences."""
+    import adjoint_cpu as AC
+    import torch
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.adjoint import darcy_2d_pattern, darcy_2d_torch, loss_column_index
+    n = 20
+    theta = P.gaussian_random_field((n, n), 3.0, 0.5, seed=3)
+    A1, b1 = P.darcy_2d(theta)
+    A2, b2 = AC.assemble(theta)
+    assert abs(A1.to_scipy() - A2).max() <= 1e-14 and np.array_equal(b1, b2)
+    _, mask = darcy_2d_pattern(n)
+    vals, bt = darcy_2d_torch(torch.as_tensor(theta), torch.as_tensor(mask))
+    assert np.array_equal(vals.numpy(), A1.val) and np.array_equal(bt.numpy(), b1)
+    col = loss_column_index(n)
+    _, g, _ = AC.loss_and_grad(theta, col)
+    cells = [(1, 2), (5, col), (n - 1, n - 1), (7, 0), (10, 13)]
+    fd = AC.central_fd(theta, col, cells)
+    ga = np.array([g[j, i] for j, i in cells])
+    assert np.abs(ga - fd).max() <= 1e-6 * np.abs(g).max()
