@@ -103,6 +103,63 @@ std::vector<int> row_partition(const int64_t* rp, int64_t nrows, int tpr) {
   return blk;
 }
 
+// Per-block offset dictionaries (see DevMat::code). Blocks with more than 256
+// distinct offsets, and the single-row blocks beyond the staging capacity,
+// keep int32 columns.
+static cfd_status encode_columns(DevMat& m, const HostCsr& h, const std::vector<int>& blk, cudaStream_t s) {
+  const int nb = m.nblk;
+  const uint64_t mult = h.nrows ? (((uint64_t)h.ncols << 20) / (uint64_t)h.nrows) : (1u << 20);
+  m.base_mult = mult;
+  auto row_base = [mult](int r) { return (int)(((uint64_t)r * mult) >> 20); };
+  int raw_blocks = 0;
+  std::vector<std::vector<int>> dicts(nb);
+  std::vector<int2> dd(nb);
+  std::vector<uint8_t> code(h.nnz() + 16, 0);
+  int64_t comp = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : comp)
+  for (int b = 0; b < nb; ++b) {
+    const int r0 = blk[b], r1 = blk[b + 1];
+    const int64_t k0 = h.rp[r0], k1 = h.rp[r1];
+    if (k1 - k0 > kNnzCap || k1 == k0) continue;
+    std::vector<int>& d = dicts[b];
+    d.reserve(64);
+    for (int r = r0; r < r1; ++r) {
+      const int base = row_base(r);
+      for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k) d.push_back(h.ci[k] - base);
+    }
+    std::sort(d.begin(), d.end());
+    d.erase(std::unique(d.begin(), d.end()), d.end());
+    if (d.size() > 256) {
+      d.clear();
+#pragma omp atomic
+      ++raw_blocks;
+      continue;
+    }
+    for (int r = r0; r < r1; ++r) {
+      const int base = row_base(r);
+      for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k)
+        code[k] = (uint8_t)(std::lower_bound(d.begin(), d.end(), h.ci[k] - base) - d.begin());
+    }
+    comp += k1 - k0;
+  }
+  std::vector<int> flat;
+  for (int b = 0; b < nb; ++b) {
+    dd[b] = make_int2((int)flat.size(), (int)dicts[b].size());
+    flat.insert(flat.end(), dicts[b].begin(), dicts[b].end());
+  }
+  m.compressed_nnz = comp;
+  m.all_compressed = comp > 0 && raw_blocks == 0;
+  if (comp == 0) return CFD_OK;
+  CFD_TRY(dmalloc(&m.code, h.nnz() + 16));
+  CFD_TRY(dmalloc(&m.dict, (int64_t)flat.size() + 16));
+  CFD_TRY(dmalloc(&m.dict_desc, (int64_t)nb));
+  CFD_TRY_CUDA(cudaMemcpyAsync(m.code, code.data(), code.size(), cudaMemcpyHostToDevice, s));
+  CFD_TRY_CUDA(cudaMemcpyAsync(m.dict, flat.data(), flat.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  CFD_TRY_CUDA(cudaMemcpyAsync(m.dict_desc, dd.data(), dd.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+  CFD_TRY_CUDA(cudaStreamSynchronize(s));  // host staging buffers go out of scope
+  return CFD_OK;
+}
+
 cfd_status devmat_upload(DevMat& m, const HostCsr& h, bool want32, cudaStream_t s) {
   devmat_free(m);
   m.nrows = h.nrows;
@@ -126,6 +183,7 @@ cfd_status devmat_upload(DevMat& m, const HostCsr& h, bool want32, cudaStream_t 
     desc[b] = make_int4(blk[b], blk[b + 1], (int)h.rp[blk[b]], (int)h.rp[blk[b + 1]]);
   CFD_TRY(dmalloc(&m.desc, (int64_t)m.nblk));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.desc, desc.data(), desc.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+  CFD_TRY(encode_columns(m, h, blk, s));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.rp, rp32.data(), rp32.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.col, h.ci.data(), m.nnz * sizeof(int), cudaMemcpyHostToDevice, s));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.v64, h.v.data(), m.nnz * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -162,6 +220,11 @@ void devmat_free(DevMat& m) {
   dfree(m.v32);
   dfree(m.blk);
   dfree(m.desc);
+  dfree(m.code);
+  dfree(m.dict);
+  dfree(m.dict_desc);
+  m.compressed_nnz = 0;
+  m.all_compressed = false;
   m.nblk = 0;
 }
 
@@ -178,11 +241,13 @@ cfd_status check_device_flag(cfd_context* ctx) {
   CFD_TRY_CUDA(cudaMemcpyAsync(ctx->h_err, ctx->err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CFD_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
   if (*ctx->h_err != 0) {
+    const int code = *ctx->h_err;
     cudaMemsetAsync(ctx->err, 0, sizeof(int), ctx->stream);
     cudaMemsetAsync(ctx->counter, 0, sizeof(unsigned), ctx->stream);
     cudaStreamSynchronize(ctx->stream);
     *ctx->h_err = 0;
-    set_error("a device-side bounded wait ran out (bulk-copy pipeline); results are invalid");
+    set_error(code == 2 ? "device-side layout check failed (int32 block in a codes-only SpMV); results are invalid"
+                               : "a device-side bounded wait ran out (bulk-copy pipeline); results are invalid");
     return CFD_ERR_TIMEOUT;
   }
   return CFD_OK;

@@ -62,6 +62,17 @@ struct DevMat {
   float* v32 = nullptr;
   int* blk = nullptr;  // row-block partition, nblk + 1 entries
   int4* desc = nullptr;  // per row block {r0, r1, k0, k1}
+  // Column compression: a block whose column offsets (col - base(row), base =
+  // row * ncols / nrows) take at most 256 distinct values stores one byte per
+  // nonzero indexing the block's offset dictionary; other blocks stay int32.
+  uint8_t* code = nullptr;  // per-nonzero dictionary index (compressed blocks)
+  int* dict = nullptr;      // concatenated per-block offset dictionaries
+  int2* dict_desc = nullptr;  // per block {first entry, entries}; 0 entries = int32 columns
+  int64_t compressed_nnz = 0;
+  bool all_compressed = false;  // every staged block is dictionary-coded
+  // base(row) = (row * base_mult) >> 20 with base_mult = (ncols << 20) / nrows:
+  // the reference point of the column offsets (row itself for square matrices).
+  uint64_t base_mult = 1u << 20;
   int nblk = 0;
   int tpr = 1;         // threads cooperating on one row (power of two, <= 32)
 };

@@ -35,7 +35,11 @@ struct MatView {
   const VT* __restrict__ val;
   const int* __restrict__ blk;
   const int4* __restrict__ desc;  // per row block {r0, r1, k0, k1}
-  int tpr_log2;                   // log2 of the threads cooperating on one row
+  const uint8_t* __restrict__ code;    // dictionary codes (nullptr: no compressed block)
+  const int* __restrict__ dict;        // concatenated offset dictionaries
+  const int2* __restrict__ dict_desc;  // per block {first entry, entries}
+  unsigned long long base_mult;        // base(row) = (row * base_mult) >> 20
+  int tpr_log2;  // log2 of the threads cooperating on one row
 };
 
 inline int ilog2(int v) {
@@ -48,11 +52,11 @@ template <typename VT>
 inline MatView<VT> mat_view(const DevMat& m);
 template <>
 inline MatView<double> mat_view<double>(const DevMat& m) {
-  return {m.rp, m.col, m.v64, m.blk, m.desc, ilog2(m.tpr)};
+  return {m.rp, m.col, m.v64, m.blk, m.desc, m.code, m.dict, m.dict_desc, (unsigned long long)m.base_mult, ilog2(m.tpr)};
 }
 template <>
 inline MatView<float> mat_view<float>(const DevMat& m) {
-  return {m.rp, m.col, m.v32, m.blk, m.desc, ilog2(m.tpr)};
+  return {m.rp, m.col, m.v32, m.blk, m.desc, m.code, m.dict, m.dict_desc, (unsigned long long)m.base_mult, ilog2(m.tpr)};
 }
 
 // Scratch of one two-stage reduction.
@@ -355,14 +359,30 @@ struct EpiBicgT {
 // flight together, then reduce with a butterfly. OFFDIAG=true forms
 // sum_{j != i} a_ij x_j and returns a_ii separately (the Jacobi smoother's
 // split, smoothers.rs:177-186). srp/sc/sv index rows and nonzeros directly.
-template <typename VT, typename XT, bool OFFDIAG, class Epi>
-__device__ __forceinline__ void rows_from_stage(const Epi& epi, const int* srp, const int* sc, const VT* sv, int r0,
+// Column of staged entry k: int32 as stored, or base(row) + dict[code[k]]
+// with base(row) = (row * mult) >> 20, mult = (ncols << 20) / nrows (row
+// itself for square matrices), computed identically by the host encoder.
+struct ColRaw {
+  const int* sc;
+  __device__ __forceinline__ int base(int) const { return 0; }
+  __device__ __forceinline__ int at(int k, int) const { return sc[k]; }
+};
+struct ColDict {
+  const uint8_t* scode;
+  const int* sdict;
+  unsigned long long mult;
+  __device__ __forceinline__ int base(int row) const { return (int)(((unsigned long long)row * mult) >> 20); }
+  __device__ __forceinline__ int at(int k, int rowbase) const { return rowbase + sdict[scode[k]]; }
+};
+
+template <typename VT, typename XT, bool OFFDIAG, class Epi, class Col>
+__device__ __forceinline__ void rows_from_stage(const Epi& epi, const int* srp, const Col& sc, const VT* sv, int r0,
                                                 int r1, int tl, int tid, const XT* __restrict__ x, double* red) {
   const int lane = tid & ((1 << tl) - 1);
   const int step = 1 << tl;
   const int g = tid >> tl;
   const int ngroups = kThreads >> tl;
-  int row[kRowsPerThread], ra[kRowsPerThread], re[kRowsPerThread];
+  int row[kRowsPerThread], ra[kRowsPerThread], re[kRowsPerThread], rb[kRowsPerThread];
   typename Epi::Pre pre[kRowsPerThread];
   VT sum[kRowsPerThread], diag[kRowsPerThread];
 #pragma unroll
@@ -371,6 +391,7 @@ __device__ __forceinline__ void rows_from_stage(const Epi& epi, const int* srp, 
     const bool live = row[q] < r1;
     ra[q] = live ? srp[row[q]] + lane : 0;
     re[q] = live ? srp[row[q] + 1] : 0;
+    rb[q] = live ? sc.base(row[q]) : 0;
     pre[q] = typename Epi::Pre{};
     if (live && lane == 0) pre[q] = epi.load(row[q]);
     sum[q] = VT(0);
@@ -385,7 +406,7 @@ __device__ __forceinline__ void rows_from_stage(const Epi& epi, const int* srp, 
     for (int q = 0; q < kRowsPerThread; ++q) {
       const int k = ra[q] + j;
       if (k < re[q]) {
-        const int c = sc[k];
+        const int c = sc.at(k, rb[q]);
         const VT v = sv[k];
         if (OFFDIAG && c == row[q])
           diag[q] = v;
@@ -444,27 +465,31 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                : "memory");
 }
 
-template <typename VT>
+// Stage layout. CODES: every staged block is dictionary-coded, so the column
+// region holds one byte per nonzero instead of four and the ring gets deeper.
+template <typename VT, bool CODES>
 struct PipeLayout {
-  static constexpr int kStages = 2;
+  static constexpr int kStages = (CODES && sizeof(VT) == 4) ? 3 : 2;
   static constexpr int kValSlack = 16 / (int)sizeof(VT);
   static constexpr int kValBytes = ((kNnzCap + 2 * kValSlack) * (int)sizeof(VT) + 127) / 128 * 128;
-  static constexpr int kColBytes = ((kNnzCap + 8) * 4 + 127) / 128 * 128;
+  static constexpr int kColBytes = CODES ? ((kNnzCap + 32) + 127) / 128 * 128 : ((kNnzCap + 8) * 4 + 127) / 128 * 128;
   static constexpr int kRpBytes = ((kRowsPerBlock + 1 + 8) * 4 + 127) / 128 * 128;
-  static constexpr int kStageBytes = kValBytes + kColBytes + kRpBytes;
+  static constexpr int kDictBytes = ((256 + 8) * 4 + 127) / 128 * 128;
+  static constexpr int kStageBytes = kValBytes + kColBytes + kRpBytes + kDictBytes;
   static constexpr int kSmemBytes = kStages * kStageBytes;
 };
 
-template <typename VT, typename XT, bool OFFDIAG, class Epi>
+template <typename VT, typename XT, bool OFFDIAG, class Epi, bool CODES>
 __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, int nblk, const XT* __restrict__ x,
                                                                 Epi epi, int* err) {
   if (epi.skip()) return;
-  using L = PipeLayout<VT>;
+  using L = PipeLayout<VT, CODES>;
   constexpr int kStages = L::kStages;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t full[kStages];
   __shared__ __align__(8) uint64_t empty[kStages];
   __shared__ int4 meta[kStages];  // r0, r1, k0, k1 of the staged block
+  __shared__ int2 dmeta[kStages];  // dictionary {first entry, entries} of the staged block
   __shared__ int s_ok[kStages];
   __shared__ volatile int s_abort;
   const int tid = threadIdx.x;
@@ -474,6 +499,9 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
   auto stage_col = [&](int s) { return reinterpret_cast<int*>(smem + s * L::kStageBytes + L::kValBytes); };
   auto stage_rp = [&](int s) {
     return reinterpret_cast<int*>(smem + s * L::kStageBytes + L::kValBytes + L::kColBytes);
+  };
+  auto stage_dict = [&](int s) {
+    return reinterpret_cast<int*>(smem + s * L::kStageBytes + L::kValBytes + L::kColBytes + L::kRpBytes);
   };
 
   if (tid == kThreads) {
@@ -499,6 +527,7 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
     for (int base = blockIdx.x; base < nblk && !stop; base += 32 * gridDim.x) {
       const int bl = base + lane * gridDim.x;
       const int4 dl = bl < nblk ? A.desc[bl] : make_int4(0, 0, 0, 0);
+      const int2 ddl = (bl < nblk && A.dict_desc) ? A.dict_desc[bl] : make_int2(0, 0);
       for (int j = 0; j < 32; ++j, ++it) {
         const int b = base + j * gridDim.x;
         if (b >= nblk) {
@@ -510,6 +539,9 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
         m.y = __shfl_sync(0xffffffffu, dl.y, j);
         m.z = __shfl_sync(0xffffffffu, dl.z, j);
         m.w = __shfl_sync(0xffffffffu, dl.w, j);
+        int2 md;
+        md.x = __shfl_sync(0xffffffffu, ddl.x, j);
+        md.y = __shfl_sync(0xffffffffu, ddl.y, j);
         int ok = 1;
         if (lane == 0) {
           const int s = it % kStages;
@@ -521,12 +553,25 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
             ok = 0;
           } else {
             meta[s] = m;
+            dmeta[s] = md;
             const int p0 = m.x & ~3, p1 = (m.y + 1 + 3) & ~3;
             const unsigned brp = (unsigned)(p1 - p0) * 4u;
             if (m.w - m.z > kNnzCap || m.w == m.z) {
               mbar_expect_tx(&full[s], brp);
               bulk_g2s(stage_rp(s), A.rp + p0, brp, &full[s]);
-            } else {
+            } else if (md.y > 0) {
+              // dictionary-coded columns: values, one-byte codes, offsets, dictionary
+              const int v0 = m.z & ~(mv - 1), v1 = (m.w + mv - 1) & ~(mv - 1);
+              const int c0 = m.z & ~15, c1 = (m.w + 15) & ~15;
+              const int d0 = md.x & ~3, d1 = (md.x + md.y + 3) & ~3;
+              const unsigned bv = (unsigned)(v1 - v0) * sizeof(VT), bc = (unsigned)(c1 - c0);
+              const unsigned bd = (unsigned)(d1 - d0) * 4u;
+              mbar_expect_tx(&full[s], bv + bc + brp + bd);
+              bulk_g2s(stage_val(s), A.val + v0, bv, &full[s]);
+              bulk_g2s(stage_col(s), A.code + c0, bc, &full[s]);
+              bulk_g2s(stage_rp(s), A.rp + p0, brp, &full[s]);
+              bulk_g2s(stage_dict(s), A.dict + d0, bd, &full[s]);
+            } else if (!CODES) {
               const int v0 = m.z & ~(mv - 1), v1 = (m.w + mv - 1) & ~(mv - 1);
               const int c0 = m.z & ~3, c1 = (m.w + 3) & ~3;
               const unsigned bv = (unsigned)(v1 - v0) * sizeof(VT), bc = (unsigned)(c1 - c0) * 4u;
@@ -534,6 +579,11 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
               bulk_g2s(stage_val(s), A.val + v0, bv, &full[s]);
               bulk_g2s(stage_col(s), A.col + c0, bc, &full[s]);
               bulk_g2s(stage_rp(s), A.rp + p0, brp, &full[s]);
+            } else {
+              // An int32 block in the codes-only layout breaks the launch
+              // invariant: complete the phase without data and flag it.
+              atomicExch(err, 2);
+              mbar_arrive(&full[s]);
             }
           }
         }
@@ -567,10 +617,21 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
       }
       mbar_wait_bounded(&full[s], parity);  // completes at once; acquires the stage for this thread
       const int4 m = meta[s];
+      const int2 md = dmeta[s];
       const int* srp = stage_rp(s) - (m.x & ~3);
-      if (m.w - m.z <= kNnzCap) {
-        rows_from_stage<VT, XT, OFFDIAG>(epi, srp, stage_col(s) - (m.z & ~3), stage_val(s) - (m.z & ~(mv - 1)), m.x,
-                                         m.y, tl, tid, x, red);
+      if (m.w - m.z <= kNnzCap && md.y > 0) {
+        // codes index the block's own dictionary, staged from entry md.x & ~3
+        const ColDict cd{reinterpret_cast<const uint8_t*>(stage_col(s)) - (m.z & ~15), stage_dict(s) + (md.x & 3),
+                         A.base_mult};
+        rows_from_stage<VT, XT, OFFDIAG>(epi, srp, cd, stage_val(s) - (m.z & ~(mv - 1)), m.x, m.y, tl, tid, x, red);
+      } else if (m.w - m.z <= kNnzCap) {
+        if (CODES) {  // no int32 columns were staged (flagged by the producer)
+          __syncwarp();
+          if ((tid & 31) == 0) mbar_arrive(&empty[s]);
+          continue;
+        }
+        const ColRaw cr{stage_col(s) - (m.z & ~3)};
+        rows_from_stage<VT, XT, OFFDIAG>(epi, srp, cr, stage_val(s) - (m.z & ~(mv - 1)), m.x, m.y, tl, tid, x, red);
       } else {
         const int row = m.x;
         typename Epi::Pre pre{};

@@ -310,12 +310,10 @@ struct Launcher {
   Red red() const { return Red{ctx->partials, ctx->counter}; }
   // Every SpMV runs the persistent bulk-copy pipeline, one CTA per row block
   // up to num_sms * (resident CTAs per SM).
-  template <typename VT, typename XT, bool OFF, class Epi>
-  cfd_status spmv(const DevMat& m, const XT* x, Epi epi) {
-    if (m.nrows == 0) return CFD_OK;
-    epi.red = red();
-    auto kern = k_spmv_pipe<VT, XT, OFF, Epi>;
-    constexpr int smem = PipeLayout<VT>::kSmemBytes;
+  template <typename VT, typename XT, bool OFF, class Epi, bool CODES>
+  cfd_status spmv_launch(const DevMat& m, const XT* x, Epi epi) {
+    auto kern = k_spmv_pipe<VT, XT, OFF, Epi, CODES>;
+    constexpr int smem = PipeLayout<VT, CODES>::kSmemBytes;
     static int occ = -1;
     if (occ < 0) {
       CFD_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -325,6 +323,19 @@ struct Launcher {
     }
     const int grid = std::min(m.nblk, ctx->num_sms * occ);
     kern<<<grid, kPipeThreads, smem, s>>>(mat_view<VT>(m), m.nblk, x, epi, ctx->err);
+    return CFD_OK;
+  }
+  // Every SpMV runs the persistent bulk-copy pipeline, one CTA per row block
+  // up to num_sms * (resident CTAs per SM); fully dictionary-coded matrices use
+  // the deeper codes-only stage ring.
+  template <typename VT, typename XT, bool OFF, class Epi>
+  cfd_status spmv(const DevMat& m, const XT* x, Epi epi) {
+    if (m.nrows == 0) return CFD_OK;
+    epi.red = red();
+    if (m.all_compressed)
+      CFD_TRY((spmv_launch<VT, XT, OFF, Epi, true>(m, x, epi)));
+    else
+      CFD_TRY((spmv_launch<VT, XT, OFF, Epi, false>(m, x, epi)));
     ctx->stats.launches++;
     ctx->stats.spmv_launches++;
     ctx->stats.spmv_bytes += (double)m.nnz * (sizeof(VT) + 4) + 4.0 * (m.nrows + 1) +

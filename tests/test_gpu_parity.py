@@ -45,7 +45,7 @@ def test_spmv_golden(cuda, golden):
     np.testing.assert_allclose(y.cpu().numpy(), g["y"], atol=g["tol"])
 
 
-@pytest.mark.parametrize("shape", ["stencil", "ragged", "long_rows", "rectangular"])
+@pytest.mark.parametrize("shape", ["stencil", "ragged", "long_rows", "rectangular", "mixed", "prolongation"])
 def test_spmv_vs_oracle(cuda, oracle, shape):
     from cfdrs_b200 import problems as P
     from cfdrs_b200.device import DeviceCsr
@@ -58,8 +58,21 @@ def test_spmv_vs_oracle(cuda, oracle, shape):
         lens = rng.integers(1, 20, 600)
         lens[[5, 300, 599]] = [2500, 4096, 3001]
         A = random_csr(rng, 600, 5000, lens)
-    else:
+    elif shape == "rectangular":
         A = random_csr(rng, 700, 1900, rng.integers(0, 30, 700))
+    elif shape == "mixed":  # dictionary-coded stencil blocks followed by int32 random blocks
+        import scipy.sparse as sp
+        S1 = P.poisson_3d_fv(12)[0].to_scipy()
+        S2 = random_csr(rng, 1500, S1.shape[1], rng.integers(0, 40, 1500)).to_scipy()
+        from cfdrs_b200.sparse import CsrMatrix
+        A = CsrMatrix.from_scipy(sp.vstack([S1, S2]).tocsr())
+    else:  # a structured rectangular operator: AMG interpolation (dictionary-coded)
+        import cfdrs_b200 as cf
+        B = P.poisson_3d_variable(16, 4.0, 1.0, seed=2)[0]
+        cfg = cf.AMGConfig.pressure_poisson()
+        cfg.min_coarse_size = 100
+        amg = cf.AlgebraicMultigrid(B, cfg)
+        A = amg.level(0, 1 if rng.random() < 2 else 2)
     x = rng.uniform(-1, 1, A.ncols)
     ref = oracle.Csr.from_matrix(A).spmv(x)
     d = DeviceCsr(A)
