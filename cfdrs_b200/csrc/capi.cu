@@ -103,59 +103,31 @@ std::vector<int> row_partition(const int64_t* rp, int64_t nrows, int tpr) {
   return blk;
 }
 
-// Per-block offset dictionaries (see DevMat::code). Blocks with more than 256
-// distinct offsets, and the single-row blocks beyond the staging capacity,
-// keep int32 columns.
-static cfd_status encode_columns(DevMat& m, const HostCsr& h, const std::vector<int>& blk, cudaStream_t s) {
-  const int nb = m.nblk;
-  const uint64_t mult = h.nrows ? (((uint64_t)h.ncols << 20) / (uint64_t)h.nrows) : (1u << 20);
-  m.base_mult = mult;
-  auto row_base = [mult](int r) { return (int)(((uint64_t)r * mult) >> 20); };
-  int raw_blocks = 0;
-  std::vector<std::vector<int>> dicts(nb);
-  std::vector<int2> dd(nb);
-  std::vector<uint8_t> code(h.nnz() + 16, 0);
-  int64_t comp = 0;
-#pragma omp parallel for schedule(dynamic, 64) reduction(+ : comp)
-  for (int b = 0; b < nb; ++b) {
-    const int r0 = blk[b], r1 = blk[b + 1];
-    const int64_t k0 = h.rp[r0], k1 = h.rp[r1];
-    if (k1 - k0 > kNnzCap || k1 == k0) continue;
-    std::vector<int>& d = dicts[b];
-    d.reserve(64);
-    for (int r = r0; r < r1; ++r) {
-      const int base = row_base(r);
-      for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k) d.push_back(h.ci[k] - base);
-    }
-    std::sort(d.begin(), d.end());
-    d.erase(std::unique(d.begin(), d.end()), d.end());
-    if (d.size() > 256) {
-      d.clear();
-#pragma omp atomic
-      ++raw_blocks;
-      continue;
-    }
-    for (int r = r0; r < r1; ++r) {
-      const int base = row_base(r);
-      for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k)
-        code[k] = (uint8_t)(std::lower_bound(d.begin(), d.end(), h.ci[k] - base) - d.begin());
-    }
-    comp += k1 - k0;
-  }
-  std::vector<int> flat;
-  for (int b = 0; b < nb; ++b) {
-    dd[b] = make_int2((int)flat.size(), (int)dicts[b].size());
-    flat.insert(flat.end(), dicts[b].begin(), dicts[b].end());
-  }
-  m.compressed_nnz = comp;
-  m.all_compressed = comp > 0 && raw_blocks == 0;
-  if (comp == 0) return CFD_OK;
+// Uploads the column dictionaries and, when every block qualifies, the x
+// windows and index records (encode_layout in layout.cpp).
+static cfd_status upload_layout(DevMat& m, const HostCsr& h, const std::vector<int>& blk, cudaStream_t s) {
+  HostLayout L;
+  encode_layout(h, blk, L);
+  m.base_mult = L.base_mult;
+  m.compressed_nnz = L.compressed_nnz;
+  m.all_compressed = L.all_compressed;
+  if (L.compressed_nnz == 0) return CFD_OK;
   CFD_TRY(dmalloc(&m.code, h.nnz() + 16));
-  CFD_TRY(dmalloc(&m.dict, (int64_t)flat.size() + 16));
-  CFD_TRY(dmalloc(&m.dict_desc, (int64_t)nb));
-  CFD_TRY_CUDA(cudaMemcpyAsync(m.code, code.data(), code.size(), cudaMemcpyHostToDevice, s));
-  CFD_TRY_CUDA(cudaMemcpyAsync(m.dict, flat.data(), flat.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-  CFD_TRY_CUDA(cudaMemcpyAsync(m.dict_desc, dd.data(), dd.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+  CFD_TRY(dmalloc(&m.dict, (int64_t)L.dict.size() + 16));
+  CFD_TRY(dmalloc(&m.dict_desc, (int64_t)L.dict_desc.size()));
+  CFD_TRY_CUDA(cudaMemcpyAsync(m.code, L.code.data(), L.code.size(), cudaMemcpyHostToDevice, s));
+  CFD_TRY_CUDA(cudaMemcpyAsync(m.dict, L.dict.data(), L.dict.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  CFD_TRY_CUDA(cudaMemcpyAsync(m.dict_desc, L.dict_desc.data(), L.dict_desc.size() * sizeof(int2),
+                               cudaMemcpyHostToDevice, s));
+  if (L.xs) {
+    CFD_TRY(dmalloc(&m.xrec, (int64_t)L.xrec.size()));
+    CFD_TRY(dmalloc(&m.xwin, (int64_t)L.xwin.size()));
+    CFD_TRY(dmalloc(&m.xdesc, (int64_t)L.xdesc.size()));
+    CFD_TRY_CUDA(cudaMemcpyAsync(m.xrec, L.xrec.data(), L.xrec.size(), cudaMemcpyHostToDevice, s));
+    CFD_TRY_CUDA(cudaMemcpyAsync(m.xwin, L.xwin.data(), L.xwin.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+    CFD_TRY_CUDA(cudaMemcpyAsync(m.xdesc, L.xdesc.data(), L.xdesc.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+    m.xs = true;
+  }
   CFD_TRY_CUDA(cudaStreamSynchronize(s));  // host staging buffers go out of scope
   return CFD_OK;
 }
@@ -183,7 +155,7 @@ cfd_status devmat_upload(DevMat& m, const HostCsr& h, bool want32, cudaStream_t 
     desc[b] = make_int4(blk[b], blk[b + 1], (int)h.rp[blk[b]], (int)h.rp[blk[b + 1]]);
   CFD_TRY(dmalloc(&m.desc, (int64_t)m.nblk));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.desc, desc.data(), desc.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
-  CFD_TRY(encode_columns(m, h, blk, s));
+  CFD_TRY(upload_layout(m, h, blk, s));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.rp, rp32.data(), rp32.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.col, h.ci.data(), m.nnz * sizeof(int), cudaMemcpyHostToDevice, s));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.v64, h.v.data(), m.nnz * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -223,8 +195,12 @@ void devmat_free(DevMat& m) {
   dfree(m.code);
   dfree(m.dict);
   dfree(m.dict_desc);
+  dfree(m.xrec);
+  dfree(m.xwin);
+  dfree(m.xdesc);
   m.compressed_nnz = 0;
   m.all_compressed = false;
+  m.xs = false;
   m.nblk = 0;
 }
 
@@ -560,6 +536,53 @@ cfd_status cfd_csr_info(const cfd_csr* a, int64_t* nrows, int64_t* ncols, int64_
   if (nrows) *nrows = a->host.nrows;
   if (ncols) *ncols = a->host.ncols;
   if (nnz) *nnz = a->host.nnz();
+  return CFD_OK;
+}
+
+cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out) {
+  if (!a || !out) {
+    set_error("cfd_csr_layout: null argument");
+    return CFD_ERR_STATE;
+  }
+  const DevMat& m = a->dev;
+  *out = cfd_layout_info{};
+  out->blocks = m.nblk;
+  out->compressed_nnz = m.compressed_nnz;
+  out->all_compressed = m.all_compressed ? 1 : 0;
+  out->x_staged = m.xs ? 1 : 0;
+  out->threads_per_row = m.tpr;
+  return CFD_OK;
+}
+
+cfd_status cfd_layout_check(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* row_ptr, const int32_t* col,
+                            const double* val, const double* x, double* y, cfd_layout_info* out) {
+  CFD_TRY(validate_csr(nrows, ncols, nnz, row_ptr, col, nullptr));
+  if ((nnz > 0 && !val) || (ncols > 0 && !x) || (nrows > 0 && !y)) {
+    set_error("cfd_layout_check: null array");
+    return CFD_ERR_DIM;
+  }
+  const HostCsr h = host_from(nrows, ncols, nnz, row_ptr, col, nullptr, val);
+  const int tpr = threads_per_row(h.nnz(), h.nrows);
+  const std::vector<int> blk = row_partition(h.rp.data(), h.nrows, tpr);
+  HostLayout L;
+  encode_layout(h, blk, L);
+  std::string why;
+  int64_t staged = 0;
+  int maxw = 0;
+  if (!check_layout(h, blk, L, x, y, &why, &staged, &maxw)) {
+    set_error("layout check: %s", why.c_str());
+    return CFD_ERR_STATE;
+  }
+  if (out) {
+    *out = cfd_layout_info{};
+    out->blocks = (int64_t)blk.size() - 1;
+    out->compressed_nnz = L.compressed_nnz;
+    out->all_compressed = L.all_compressed ? 1 : 0;
+    out->x_staged = L.xs ? 1 : 0;
+    out->threads_per_row = tpr;
+    out->max_windows = maxw;
+    out->staged_x_entries = staged;
+  }
   return CFD_OK;
 }
 

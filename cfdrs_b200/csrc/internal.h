@@ -38,10 +38,28 @@ constexpr int kThreads = 256;
 constexpr int kRowsPerThread = 2;
 constexpr int kRowsPerBlock = kThreads * kRowsPerThread;
 constexpr int kNnzCap = 4096;
+// x staging: a dictionary-coded block whose columns fall in at most kXsMaxWin
+// windows of kXsCap entries in total reads x from shared memory (the windows
+// are bulk-copied with the block) instead of gathering it from global memory.
+constexpr int kXsCap = 4096;
+constexpr int kXsMaxWin = 8;
+// Index record of an x-staged block (one bulk copy): row offsets relative to
+// the block's first nonzero (uint16, rows + 1 of them), the one-byte codes and
+// the code -> staged-x displacement table (int32), each part 16-byte aligned.
+struct XsRecord {
+  int rp_bytes, code_bytes, e_bytes;
+  __host__ __device__ static XsRecord of(int rows, int nnz, int nd) {
+    return {(2 * (rows + 1) + 15) & ~15, (nnz + 15) & ~15, (4 * nd + 15) & ~15};
+  }
+  __host__ __device__ int bytes() const { return rp_bytes + code_bytes + e_bytes; }
+};
+constexpr int kXsRecordCap = ((2 * (kRowsPerBlock + 1) + 15) & ~15) + kNnzCap + 4 * 256;
 // Grid of the streaming vector kernels: 148 SMs x 8 resident CTAs.
 constexpr int kVecGrid = 148 * 8;
 // Device-side scratch for two-stage reductions (per-CTA partials, up to 4 values).
 constexpr int kMaxRed = 4;
+// Device ordinals covered by the per-device launch-attribute caches.
+constexpr int kLaunchCacheDevices = 64;
 
 // Host CSR (int64 offsets, int32 columns), the form AMG setup works on.
 struct HostCsr {
@@ -73,9 +91,37 @@ struct DevMat {
   // base(row) = (row * base_mult) >> 20 with base_mult = (ncols << 20) / nrows:
   // the reference point of the column offsets (row itself for square matrices).
   uint64_t base_mult = 1u << 20;
+  // x staging (all blocks dictionary-coded and within kXsCap / kXsMaxWin).
+  // Windows are 4-entry aligned column ranges [src, src + len) placed one after
+  // another in shared memory; a window that would run past ncols copies up to
+  // the last full 4-entry group and its `tail` (< 4) entries are read one by
+  // one. The x entry of a nonzero with code q in row r sits at shared entry
+  // base(r) - base(r0) + E[q], E being the block's table in its XsRecord.
+  uint8_t* xrec = nullptr;  // concatenated 16-byte aligned XsRecords
+  int4* xwin = nullptr;     // per block kXsMaxWin slots of {src, len}, two per int4
+  // per block {windows | tail << 16, zero-offset code or -1, record offset / 16, entries copied}
+  int4* xdesc = nullptr;
+  bool xs = false;
   int nblk = 0;
   int tpr = 1;         // threads cooperating on one row (power of two, <= 32)
 };
+
+// Host image of DevMat's compression and x-staging arrays (layout.cpp).
+struct HostLayout {
+  uint64_t base_mult = 1u << 20;
+  std::vector<uint8_t> code;  // nnz + 16
+  std::vector<int> dict;
+  std::vector<int2> dict_desc;
+  int64_t compressed_nnz = 0;
+  bool all_compressed = false;
+  std::vector<int> xe;        // code -> staged-x displacement (dictionary layout)
+  std::vector<uint8_t> xrec;  // XsRecords
+  std::vector<int4> xwin, xdesc;
+  bool xs = false;
+};
+void encode_layout(const HostCsr& h, const std::vector<int>& blk, HostLayout& L);
+bool check_layout(const HostCsr& h, const std::vector<int>& blk, const HostLayout& L, const double* x, double* y,
+                  std::string* why, int64_t* staged_entries, int* max_windows);
 
 cfd_status devmat_upload(DevMat& m, const HostCsr& h, bool want32, cudaStream_t s);
 cfd_status devmat_update_values(DevMat& m, const double* v, int64_t nnz, bool want32, cudaStream_t s);
@@ -97,6 +143,7 @@ struct DevState {
 struct KernelStats {
   int64_t launches = 0;
   int64_t spmv_launches = 0;
+  int64_t xs_launches = 0;  // SpMV launches on the x-staged pipeline
   double spmv_bytes = 0.0;
   void reset() { *this = KernelStats(); }
 };

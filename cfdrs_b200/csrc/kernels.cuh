@@ -9,8 +9,9 @@
 //    shared memory, gather x through the read-only path, and pass the row
 //    result to a fused epilogue whose own operands were loaded before the
 //    gathers. Row groups of 2^k threads serve operators with long rows.
-//  * k_spmv: the same computation with one row block per CTA and plain
-//    coalesced staging, for matrices of only a few row blocks.
+//  * k_spmv_xs: the same pipeline for matrices whose blocks all have compact
+//    column windows: x is staged in shared memory with the block, so no
+//    gather leaves the SM.
 //  * Epilogue functors (plain store, residual, damped Jacobi, PCG / BiCGSTAB
 //    dots, prolongation-correction) consume the row result so no kernel
 //    re-reads what another just wrote.
@@ -619,8 +620,9 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
       const int4 m = meta[s];
       const int2 md = dmeta[s];
       const int* srp = stage_rp(s) - (m.x & ~3);
-      if (m.w - m.z <= kNnzCap && md.y > 0) {
+      if (m.w - m.z <= kNnzCap && (md.y > 0 || m.w == m.z)) {
         // codes index the block's own dictionary, staged from entry md.x & ~3
+        // (a block of empty rows reads no entry and still runs its epilogue)
         const ColDict cd{reinterpret_cast<const uint8_t*>(stage_col(s)) - (m.z & ~15), stage_dict(s) + (md.x & 3),
                          A.base_mult};
         rows_from_stage<VT, XT, OFFDIAG>(epi, srp, cd, stage_val(s) - (m.z & ~(mv - 1)), m.x, m.y, tl, tid, x, red);
@@ -648,6 +650,266 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
         sum = consumer_sum(sum);
         diag = consumer_sum(diag);
         if (tid == 0) epi.row(row, sum, diag, pre, red);
+      }
+      __syncwarp();
+      if ((tid & 31) == 0) mbar_arrive(&empty[s]);
+    }
+  }
+  __syncthreads();
+  if (s_abort) return;
+  if constexpr (Epi::NRED > 0) {
+    double tot[Epi::NRED];
+    if (grid_reduce<Epi::NRED>(red, epi.red, tot) && tid == 0) epi.finish(tot);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// x-staged pipeline (DevMat::xs): each stage receives the block's values, its
+// index record (row offsets, codes, displacement table) and its x windows by
+// bulk copy, so the consumers read every operand from shared memory and no
+// gather leaves the SM. One CTA per SM with 16 consumer warps (one row or row
+// group per thread) on a ring sized to fill the SM's shared memory; the
+// consumers take the stages in order, so a parity wait always names the phase
+// it means. Entry addresses are 32-bit shared-window offsets. Summation order
+// per row equals k_spmv_pipe's, so both paths give bit-identical results.
+struct XsView {
+  const int4* __restrict__ xdesc;    // per block {windows | tail << 16, zero code, record offset / 16, entries copied}
+  const int4* __restrict__ xwin;     // per block 4 x int4 = 8 windows {src, len, src, len}
+  const uint8_t* __restrict__ xrec;  // XsRecords
+  int ncols;
+};
+
+constexpr int kXsConsumers = 2 * kThreads;  // one thread per row of a full block
+constexpr int kXsThreads = kXsConsumers + 32;
+
+template <typename VT>
+struct XsLayout {
+  static constexpr int kValSlack = 16 / (int)sizeof(VT);
+  static constexpr int kValBytes = ((kNnzCap + 2 * kValSlack) * (int)sizeof(VT) + 127) / 128 * 128;
+  static constexpr int kRecBytes = (kXsRecordCap + 127) / 128 * 128;
+  static constexpr int kXBytes = (kXsCap * (int)sizeof(VT) + 127) / 128 * 128;
+  static constexpr int kStageBytes = kValBytes + kRecBytes + kXBytes;
+  // 227 KB per CTA less 2 KB for the static barriers and reduction scratch
+  static constexpr int kStages = (227 * 1024 - 2048) / kStageBytes;
+  static constexpr int kSmemBytes = kStages * kStageBytes;
+  static_assert(kStages >= 2, "x-staged ring needs two stages");
+};
+
+__device__ __forceinline__ unsigned lds_u8(uint32_t a) {
+  unsigned v;
+  asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ int lds_u16(uint32_t a) {
+  unsigned v;
+  asm volatile("ld.shared.u16 %0, [%1];" : "=r"(v) : "r"(a));
+  return (int)v;
+}
+__device__ __forceinline__ int lds_s32(uint32_t a) {
+  int v;
+  asm volatile("ld.shared.s32 %0, [%1];" : "=r"(v) : "r"(a));
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T lds(uint32_t a);
+template <>
+__device__ __forceinline__ float lds<float>(uint32_t a) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+  return v;
+}
+template <>
+__device__ __forceinline__ double lds<double>(uint32_t a) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
+  return v;
+}
+
+// Rows of one staged block (ctid in [0, kXsConsumers)): row group g of 2^tl
+// threads owns row r0 + g; the strided loop and butterfly per row are those of
+// rows_from_stage, so every row is summed in the same order.
+template <typename VT, bool OFFDIAG, class Epi>
+__device__ __forceinline__ void rows_from_stage_xs(const Epi& epi, uint32_t a_rp16, uint32_t a_code, uint32_t a_val,
+                                                   uint32_t a_e, uint32_t a_x, int zq, int r0, int r1,
+                                                   unsigned long long mult, int tl, int ctid, double* red) {
+  constexpr int vs = (int)sizeof(VT);
+  const int lane = ctid & ((1 << tl) - 1);
+  const int step = 1 << tl;
+  const int i = ctid >> tl;
+  const int row = r0 + i;
+  const bool live = row < r1;
+  int ka = 0, ke = 0;
+  uint32_t xr = a_x;
+  typename Epi::Pre pre{};
+  if (live) {
+    ka = lds_u16(a_rp16 + 2u * (uint32_t)i) + lane;  // offsets from the block's first nonzero
+    ke = lds_u16(a_rp16 + 2u * (uint32_t)i + 2u);
+    const int b0 = (int)(((unsigned long long)r0 * mult) >> 20);
+    xr += (uint32_t)(((int)(((unsigned long long)row * mult) >> 20) - b0) * vs);
+    if (lane == 0) pre = epi.load(row);
+  }
+  VT sum = VT(0), diag = VT(0);
+#pragma unroll 4
+  for (int k = ka; k < ke; k += step) {
+    const unsigned c = lds_u8(a_code + (uint32_t)k);
+    const int e = lds_s32(a_e + 4u * c);
+    const VT xv = lds<VT>(xr + (uint32_t)(e * vs));
+    const VT v = lds<VT>(a_val + (uint32_t)(k * vs));
+    if (OFFDIAG && (int)c == zq)
+      diag = v;
+    else
+      sum += v * xv;
+  }
+  for (int o = step >> 1; o > 0; o >>= 1) {
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (OFFDIAG) diag += __shfl_xor_sync(0xffffffffu, diag, o);
+  }
+  if (live && lane == 0) epi.row(row, sum, diag, pre, red);
+}
+
+template <typename VT, bool OFFDIAG, class Epi>
+__global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView X, int nblk,
+                                                            const VT* __restrict__ x, Epi epi, int* err) {
+  if (epi.skip()) return;
+  using L = XsLayout<VT>;
+  constexpr int kStages = L::kStages;
+  constexpr int vs = (int)sizeof(VT);
+  constexpr int mv = L::kValSlack;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t full[kStages];
+  __shared__ __align__(8) uint64_t empty[kStages];
+  __shared__ int4 meta[kStages];   // r0, r1, k0, k1
+  __shared__ int4 xmeta[kStages];  // dictionary entries, zero code, tail entries, entries copied
+  __shared__ int s_ok[kStages];
+  __shared__ volatile int s_abort;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const uint32_t sbase = smem_u32(smem);
+  auto a_val = [&](int s) { return sbase + (uint32_t)(s * L::kStageBytes); };
+  auto a_rec = [&](int s) { return a_val(s) + (uint32_t)L::kValBytes; };
+  auto a_x = [&](int s) { return a_rec(s) + (uint32_t)L::kRecBytes; };
+  auto p_of = [&](uint32_t a) { return (void*)(smem + (a - sbase)); };
+
+  if (tid == kXsConsumers) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kXsConsumers / 32);
+    }
+    s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  double red[Epi::NRED > 0 ? Epi::NRED : 1];
+#pragma unroll
+  for (int q = 0; q < (Epi::NRED > 0 ? Epi::NRED : 1); ++q) red[q] = 0.0;
+
+  if (warp == kXsConsumers / 32) {
+    // ---- producer warp: lane j holds the descriptors of the j-th of the next
+    // 32 blocks and issues that block's copies itself.
+    const int lane = tid & 31;
+    int it = 0;
+    bool stop = false;
+    for (int base = blockIdx.x; base < nblk && !stop; base += 32 * gridDim.x) {
+      const int bl = base + lane * gridDim.x;
+      const bool have = bl < nblk;
+      const int4 m = have ? A.desc[bl] : make_int4(0, 0, 0, 0);
+      const int2 md = have ? A.dict_desc[bl] : make_int2(0, 0);
+      const int4 xd = have ? X.xdesc[bl] : make_int4(0, -1, 0, 0);
+      int4 w[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) w[i] = have ? X.xwin[(size_t)bl * 4 + i] : make_int4(0, 0, 0, 0);
+      const int nj = min(32, (nblk - base + (int)gridDim.x - 1) / (int)gridDim.x);
+      for (int j = 0; j < nj; ++j, ++it) {
+        int ok = 1;
+        if (lane == j) {
+          const int s = it % kStages;
+          if (it >= kStages && !mbar_wait_bounded(&empty[s], (unsigned)((it / kStages) - 1) & 1u)) {
+            s_abort = 1;
+            atomicExch(err, 1);
+          }
+          if (s_abort) {
+            ok = 0;
+          } else {
+            meta[s] = m;
+            const int nwin = xd.x & 0xffff;
+            xmeta[s] = make_int4(md.y, xd.y, xd.x >> 16, xd.w);
+            const XsRecord R = XsRecord::of(m.y - m.x, m.w - m.z, md.y);
+            const uint8_t* rec = X.xrec + (size_t)xd.z * 16;
+            if (m.w - m.z > kNnzCap || m.y - m.x > kRowsPerBlock) {
+              // outside the x-staged invariant: complete the phase and flag it
+              atomicExch(err, 2);
+              mbar_arrive(&full[s]);
+            } else if (m.w == m.z) {
+              mbar_expect_tx(&full[s], (unsigned)R.bytes());
+              bulk_g2s(p_of(a_rec(s)), rec, (unsigned)R.bytes(), &full[s]);
+            } else {
+              const int v0 = m.z & ~(mv - 1), v1 = (m.w + mv - 1) & ~(mv - 1);
+              const unsigned bv = (unsigned)(v1 - v0) * vs, bx = (unsigned)xd.w * vs;
+              mbar_expect_tx(&full[s], bv + (unsigned)R.bytes() + bx);
+              bulk_g2s(p_of(a_val(s)), A.val + v0, bv, &full[s]);
+              bulk_g2s(p_of(a_rec(s)), rec, (unsigned)R.bytes(), &full[s]);
+              uint32_t soff = a_x(s);
+#pragma unroll
+              for (int i = 0; i < 8; ++i) {
+                const int src = (i & 1) ? w[i >> 1].z : w[i >> 1].x;
+                const int len = (i & 1) ? w[i >> 1].w : w[i >> 1].y;
+                if (i < nwin && len > 0) {
+                  bulk_g2s(p_of(soff), x + src, (unsigned)len * vs, &full[s]);
+                  soff += (uint32_t)(len * vs);
+                }
+              }
+            }
+          }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, j);
+        if (!ok) {
+          stop = true;
+          break;
+        }
+      }
+    }
+    if (lane == 0 && s_abort) {
+      // Drain what was issued before leaving (bounded).
+      for (int j = (it > kStages ? it - kStages : 0); j < it; ++j)
+        mbar_wait_bounded(&full[j % kStages], (unsigned)(j / kStages) & 1u);
+    }
+  } else {
+    // ---- consumers: every block of this CTA in order
+    const int tl = A.tpr_log2;
+    const int ncols4 = X.ncols & ~3;
+    int it = 0;
+    for (int b = blockIdx.x; b < nblk; b += (int)gridDim.x, ++it) {
+      const int s = it % kStages;
+      const unsigned parity = (unsigned)(it / kStages) & 1u;
+      if (tid == 0) {
+        const int ok = (!s_abort && mbar_wait_bounded(&full[s], parity)) ? 1 : 0;
+        s_ok[s] = ok;
+        const int4 xm = xmeta[s];
+        if (ok && xm.z > 0) {
+          // the 1-3 entries past the last 16-byte boundary of x
+          const uint32_t at = a_x(s) + (uint32_t)(xm.w * vs);
+          for (int t = 0; t < xm.z; ++t) *reinterpret_cast<VT*>(p_of(at + (uint32_t)(t * vs))) = x[ncols4 + t];
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        }
+      }
+      asm volatile("bar.sync 1, %0;" ::"n"(kXsConsumers) : "memory");
+      if (!s_ok[s]) {
+        if (tid == 0) {
+          s_abort = 1;
+          atomicExch(err, 1);
+        }
+        break;
+      }
+      mbar_wait_bounded(&full[s], parity);  // completes at once; acquires the stage for this thread
+      const int4 m = meta[s];
+      const int4 xm = xmeta[s];
+      if (m.w - m.z <= kNnzCap && m.y - m.x <= kRowsPerBlock) {
+        const XsRecord R = XsRecord::of(m.y - m.x, m.w - m.z, xm.x);
+        rows_from_stage_xs<VT, OFFDIAG>(epi, a_rec(s), a_rec(s) + (uint32_t)R.rp_bytes,
+                                        a_val(s) + (uint32_t)((m.z & (mv - 1)) * vs),
+                                        a_rec(s) + (uint32_t)(R.rp_bytes + R.code_bytes), a_x(s), xm.y, m.x, m.y,
+                                        A.base_mult, tl, tid, red);
       }
       __syncwarp();
       if ((tid & 31) == 0) mbar_arrive(&empty[s]);

@@ -6,6 +6,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "amg_device.h"
 #include "internal.h"
@@ -314,28 +315,63 @@ struct Launcher {
   cfd_status spmv_launch(const DevMat& m, const XT* x, Epi epi) {
     auto kern = k_spmv_pipe<VT, XT, OFF, Epi, CODES>;
     constexpr int smem = PipeLayout<VT, CODES>::kSmemBytes;
-    static int occ = -1;
-    if (occ < 0) {
+    static int occ[kLaunchCacheDevices] = {};
+    if (ctx->device >= kLaunchCacheDevices) {
+      set_error("device ordinal %d beyond %d", ctx->device, kLaunchCacheDevices);
+      return CFD_ERR_CUDA;
+    }
+    if (occ[ctx->device] <= 0) {
       CFD_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
       int o = 0;
       CFD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kPipeThreads, smem));
-      occ = std::max(1, o);
+      occ[ctx->device] = std::max(1, o);
     }
-    const int grid = std::min(m.nblk, ctx->num_sms * occ);
+    const int grid = std::min(m.nblk, ctx->num_sms * occ[ctx->device]);
     kern<<<grid, kPipeThreads, smem, s>>>(mat_view<VT>(m), m.nblk, x, epi, ctx->err);
     return CFD_OK;
   }
-  // Every SpMV runs the persistent bulk-copy pipeline, one CTA per row block
-  // up to num_sms * (resident CTAs per SM); fully dictionary-coded matrices use
-  // the deeper codes-only stage ring.
+  // x-staged pipeline: one CTA per SM.
+  template <typename VT, bool OFF, class Epi>
+  cfd_status spmv_xs_launch(const DevMat& m, const VT* x, Epi epi) {
+    auto kern = k_spmv_xs<VT, OFF, Epi>;
+    constexpr int smem = XsLayout<VT>::kSmemBytes;
+    static bool attr[kLaunchCacheDevices] = {};
+    if (ctx->device >= kLaunchCacheDevices) {
+      set_error("device ordinal %d beyond %d", ctx->device, kLaunchCacheDevices);
+      return CFD_ERR_CUDA;
+    }
+    if (!attr[ctx->device]) {
+      CFD_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      attr[ctx->device] = true;
+    }
+    const int grid = std::min(m.nblk, ctx->num_sms);
+    const XsView xv{m.xdesc, m.xwin, m.xrec, (int)m.ncols};
+    kern<<<grid, kXsThreads, smem, s>>>(mat_view<VT>(m), xv, m.nblk, x, epi, ctx->err);
+    ctx->stats.xs_launches++;
+    return CFD_OK;
+  }
+  // Every SpMV runs a persistent bulk-copy pipeline. Matrices whose blocks all
+  // have dictionary codes and compact x windows stage x with the block (when x
+  // is 16-byte aligned); other fully coded matrices use the codes-only ring,
+  // the rest the int32-column ring.
   template <typename VT, typename XT, bool OFF, class Epi>
   cfd_status spmv(const DevMat& m, const XT* x, Epi epi) {
     if (m.nrows == 0) return CFD_OK;
     epi.red = red();
+    if constexpr (std::is_same<VT, XT>::value) {
+      if (m.xs && ((uintptr_t)x & 15) == 0) {
+        CFD_TRY((spmv_xs_launch<VT, OFF, Epi>(m, x, epi)));
+        return finish_spmv<VT, XT>(m);
+      }
+    }
     if (m.all_compressed)
       CFD_TRY((spmv_launch<VT, XT, OFF, Epi, true>(m, x, epi)));
     else
       CFD_TRY((spmv_launch<VT, XT, OFF, Epi, false>(m, x, epi)));
+    return finish_spmv<VT, XT>(m);
+  }
+  template <typename VT, typename XT>
+  cfd_status finish_spmv(const DevMat& m) {
     ctx->stats.launches++;
     ctx->stats.spmv_launches++;
     ctx->stats.spmv_bytes += (double)m.nnz * (sizeof(VT) + 4) + 4.0 * (m.nrows + 1) +

@@ -90,6 +90,12 @@ class DeviceCsr:
             raise ValueError("value array must match nnz")
         _lib.check(_lib.load().cfd_csr_update_values(self.h, _ptr(v)))
 
+    def layout(self) -> dict:
+        """Device layout of this matrix (row blocks, column codes, x staging)."""
+        info = _lib.LayoutInfoC()
+        _lib.check(_lib.load().cfd_csr_layout(self.h, C.byref(info)))
+        return {f: getattr(info, f) for f, _ in info._fields_}
+
     def spmv(self, x_dev_ptr: int, y_dev_ptr: int, fp32: bool = False) -> None:
         """y = A x on device pointers."""
         fn = _lib.load().cfd_spmv_f32 if fp32 else _lib.load().cfd_spmv
@@ -103,6 +109,23 @@ class DeviceCsr:
             except Exception:
                 pass
             self.h = None
+
+
+def layout_check(m: CsrMatrix, x: np.ndarray):
+    """Host-only walk of the SpMV device layout (``cfd_layout_check``): returns
+    y = A x evaluated through the kernels' index arithmetic and the layout
+    statistics; raises CfdError if any staged index leaves its region."""
+    rp = np.ascontiguousarray(m.row_ptr, dtype=np.int64)
+    col = np.ascontiguousarray(m.col, dtype=np.int32)
+    val = np.ascontiguousarray(m.val, dtype=np.float64)
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    if xx.shape[0] != m.ncols:
+        raise ValueError("x must have ncols entries")
+    y = np.zeros(m.nrows)
+    info = _lib.LayoutInfoC()
+    _lib.check(_lib.load().cfd_layout_check(m.nrows, m.ncols, m.nnz, _ptr(rp), _ptr(col), _ptr(val), _ptr(xx),
+                                            _ptr(y), C.byref(info)))
+    return y, {f: getattr(info, f) for f, _ in info._fields_}
 
 
 _uploads: "weakref.WeakKeyDictionary[CsrMatrix, DeviceCsr]" = weakref.WeakKeyDictionary()

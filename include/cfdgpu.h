@@ -89,6 +89,30 @@ cfd_status cfd_csr_update_values(cfd_csr* a, const double* val_host);
 cfd_status cfd_csr_info(const cfd_csr* a, int64_t* nrows, int64_t* ncols, int64_t* nnz);
 cfd_status cfd_csr_destroy(cfd_csr* a);
 
+/* ---- SpMV device layout (no reference counterpart: CFDrs multiplies plain
+ * CSR, crates/cfd-math/src/sparse/operations.rs:14-30) -------------------
+ * Row blocks of <= 512 rows / 4096 nonzeros. A block whose column offsets from
+ * base(row) = row * ncols / nrows take <= 256 values stores one-byte codes;
+ * when every block is coded and its columns fall in <= 8 windows of <= 4096
+ * entries in total, SpMV stages those x windows in shared memory ("x staged"). */
+typedef struct {
+  int64_t blocks;
+  int64_t compressed_nnz;    /* nonzeros stored as one-byte codes */
+  int32_t all_compressed;
+  int32_t x_staged;
+  int32_t threads_per_row;
+  int32_t max_windows;       /* cfd_layout_check only */
+  int64_t staged_x_entries;  /* cfd_layout_check only: x entries staged over all blocks */
+} cfd_layout_info;
+cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out);
+/* Host only, no GPU: builds the layout of a CSR matrix and evaluates y = A x by
+ * walking the device kernels' index arithmetic (staged x image, index record,
+ * codes, tables), failing with CFD_ERR_STATE and a message on any index
+ * outside its region. */
+cfd_status cfd_layout_check(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* row_ptr,
+                            const int32_t* col, const double* val, const double* x, double* y,
+                            cfd_layout_info* out);
+
 /* y = A x on device pointers (FP64), or FP32 values/vectors (values cast once). */
 cfd_status cfd_spmv(cfd_csr* a, const double* x_dev, double* y_dev);
 cfd_status cfd_spmv_f32(cfd_csr* a, const float* x_dev, float* y_dev);

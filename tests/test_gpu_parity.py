@@ -45,13 +45,22 @@ def test_spmv_golden(cuda, golden):
     np.testing.assert_allclose(y.cpu().numpy(), g["y"], atol=g["tol"])
 
 
-@pytest.mark.parametrize("shape", ["stencil", "ragged", "long_rows", "rectangular", "mixed", "prolongation"])
-def test_spmv_vs_oracle(cuda, oracle, shape):
+def spmv_case(shape):
+    """Matrices of the SpMV parity tests; x-staged ones are marked True."""
     from cfdrs_b200 import problems as P
-    from cfdrs_b200.device import DeviceCsr
     rng = np.random.default_rng(7)
+    staged = False
     if shape == "stencil":
-        A = P.poisson_3d_variable(20, 4.0, 1.0, seed=2)[0]
+        A, staged = P.poisson_3d_variable(20, 4.0, 1.0, seed=2)[0], True
+    elif shape == "stencil_tail":  # 33^3 columns: the last x window ends in a 1-entry tail
+        A, staged = P.poisson_3d_variable(33, 4.0, 1.0, seed=3)[0], True
+    elif shape == "empty_blocks":  # > 2 blocks of empty rows between two stencils
+        import scipy.sparse as sp
+        from cfdrs_b200.sparse import CsrMatrix
+        S = P.poisson_3d_fv(10)[0].to_scipy()
+        A, staged = CsrMatrix.from_scipy(sp.block_diag([S, sp.csr_matrix((1300, 1300)), S]).tocsr()), True
+    elif shape == "narrow":  # three columns: no bulk-copied window, all tail
+        A, staged = random_csr(rng, 2000, 3, rng.integers(0, 4, 2000)), True
     elif shape == "ragged":  # empty rows and short rows of uneven length
         A = random_csr(rng, 3000, 3000, rng.integers(0, 12, 3000))
     elif shape == "long_rows":  # rows beyond the 2048-nonzero staging capacity
@@ -66,13 +75,23 @@ def test_spmv_vs_oracle(cuda, oracle, shape):
         S2 = random_csr(rng, 1500, S1.shape[1], rng.integers(0, 40, 1500)).to_scipy()
         from cfdrs_b200.sparse import CsrMatrix
         A = CsrMatrix.from_scipy(sp.vstack([S1, S2]).tocsr())
-    else:  # a structured rectangular operator: AMG interpolation (dictionary-coded)
+    else:  # AMG operators of the 3-D solve: interpolation, restriction, coarse A (2 threads per row)
         import cfdrs_b200 as cf
         B = P.poisson_3d_variable(16, 4.0, 1.0, seed=2)[0]
         cfg = cf.AMGConfig.pressure_poisson()
         cfg.min_coarse_size = 100
         amg = cf.AlgebraicMultigrid(B, cfg)
-        A = amg.level(0, 1 if rng.random() < 2 else 2)
+        which = {"prolongation": (0, 1), "restriction": (0, 2), "coarse_operator": (1, 0)}[shape]
+        A, staged = amg.level(*which), shape != "coarse_operator"
+    return A, staged
+
+
+@pytest.mark.parametrize("shape", ["stencil", "stencil_tail", "empty_blocks", "narrow", "ragged", "long_rows",
+                                   "rectangular", "mixed", "prolongation", "restriction", "coarse_operator"])
+def test_spmv_vs_oracle(cuda, oracle, shape):
+    from cfdrs_b200.device import DeviceCsr
+    A, staged = spmv_case(shape)
+    rng = np.random.default_rng(11)
     x = rng.uniform(-1, 1, A.ncols)
     ref = oracle.Csr.from_matrix(A).spmv(x)
     d = DeviceCsr(A)
@@ -84,6 +103,34 @@ def test_spmv_vs_oracle(cuda, oracle, shape):
     d.spmv(dev(cuda, x, cuda.float32).data_ptr(), y32.data_ptr(), fp32=True)
     cuda.cuda.synchronize()
     assert rel(y32.cpu().numpy().astype(np.float64), ref) < 1e-5
+    if staged:
+        assert d.layout()["x_staged"] == 1
+
+
+@pytest.mark.parametrize("shape", ["stencil", "stencil_tail", "empty_blocks", "narrow", "prolongation",
+                                   "restriction"])
+def test_x_staged_equals_gather_path(cuda, shape):
+    """The x-staged kernel (x 16-byte aligned) and the gather kernel (the same x
+    one element into a buffer, so not 16-byte aligned) sum every row in the same
+    order: FP64 and FP32 results are bit-identical."""
+    from cfdrs_b200.device import DeviceCsr
+    A, staged = spmv_case(shape)
+    assert staged
+    d = DeviceCsr(A)
+    assert d.layout()["x_staged"] == 1
+    x = np.random.default_rng(5).uniform(-1, 1, A.ncols)
+    for dt in (cuda.float64, cuda.float32):
+        xa = dev(cuda, x, dt)
+        buf = cuda.zeros(A.ncols + 1, device="cuda", dtype=dt)
+        buf[1:] = xa
+        ya = cuda.zeros(A.nrows, device="cuda", dtype=dt)
+        yb = cuda.full((A.nrows,), float("nan"), device="cuda", dtype=dt)
+        fp32 = dt == cuda.float32
+        d.spmv(xa.data_ptr(), ya.data_ptr(), fp32=fp32)
+        d.spmv(buf[1:].data_ptr(), yb.data_ptr(), fp32=fp32)
+        cuda.cuda.synchronize()
+        assert buf[1:].data_ptr() % 16 != 0
+        assert cuda.equal(ya, yb), f"{shape} {dt}"
 
 
 @pytest.mark.parametrize("interp,order", [(0, 0), (2, 0), (2, 1)])

@@ -1,0 +1,108 @@
+"""The SpMV device layout on the host: column codes, x windows, tails, index
+records and code tables are walked with the kernels' own index arithmetic
+(cfd_layout_check), every staged index is checked against its region and
+against the column it must hold, and y = A x from that walk must equal the
+CSR product."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from cfdrs_b200 import problems as P
+from cfdrs_b200.device import layout_check
+from cfdrs_b200.sparse import CsrMatrix
+from helpers import csr_from_lists, grid_laplacian
+
+
+def random_csr(rng, n, ncols, lens):
+    rp, col, val = [0], [], []
+    for i in range(n):
+        cols = np.sort(rng.choice(ncols, size=min(int(lens[i]), ncols), replace=False))
+        col += cols.tolist()
+        val += rng.uniform(-1, 1, cols.size).tolist()
+        rp.append(len(col))
+    return csr_from_lists(rp, col, val, ncols)
+
+
+def check(A, seed=0):
+    x = np.random.default_rng(seed).standard_normal(A.ncols)
+    y, info = layout_check(A, x)
+    ref = A.to_scipy() @ x
+    np.testing.assert_allclose(y, ref, rtol=1e-14, atol=1e-14 * max(np.abs(ref).max(initial=0.0), 1.0))
+    return info
+
+
+@pytest.mark.parametrize("n", [5, 16, 33, 41])
+def test_stencils_are_x_staged(n):
+    """3-D 7-point operators, including sizes whose column count is not a
+    multiple of 4 (the last window ends in a tail of 1-3 entries)."""
+    info = check(P.poisson_3d_variable(n, 4.0, 1.0, seed=n)[0])
+    assert info["all_compressed"] == 1 and info["x_staged"] == 1
+    assert 1 <= info["max_windows"] <= 3
+
+
+def test_2d_operators():
+    assert check(grid_laplacian(37))["x_staged"] == 1
+    A, _ = P.darcy_2d(P.gaussian_random_field((45, 45), 5.0, 0.5, seed=1))
+    assert check(A)["x_staged"] == 1
+
+
+def test_amg_levels(oracle):
+    """Every operator of a modified-classical hierarchy (A, P, R per level), in
+    both coarse numberings; each is checked whether or not it is x-staged."""
+    A = P.poisson_3d_variable(24, 8.0, 1.0, seed=0)[0]
+    staged = []
+    for order in (0, 1):
+        amg = oracle.Amg(oracle.Csr.from_matrix(A), oracle.AmgConfig(
+            smoother=oracle.SMOOTH_JACOBI, relaxation=2 / 3, pre_smooth=1, post_smooth=1, interpolation=2,
+            coarse_order=order, min_coarse_size=50, coarse_solve=oracle.COARSE_DENSE))
+        for l in range(amg.num_levels):
+            for which in ((0, 1, 2) if l < amg.num_levels - 1 else (0,)):
+                rp, ci, v, shape = amg.level(l, which).arrays()
+                staged.append(check(CsrMatrix(rp, ci, v, shape), seed=l)["x_staged"])
+    assert staged[0] == 1 and sum(staged) >= 3
+
+
+def test_ragged_rectangular_and_mixed():
+    rng = np.random.default_rng(3)
+    check(random_csr(rng, 3000, 3000, rng.integers(0, 12, 3000)))
+    check(random_csr(rng, 700, 1900, rng.integers(0, 30, 700)))
+    lens = rng.integers(1, 20, 600)
+    lens[[5, 300, 599]] = [2500, 4096, 3001]
+    info = check(random_csr(rng, 600, 5000, lens))  # rows beyond the staging capacity
+    assert info["x_staged"] == 0
+    S1 = P.poisson_3d_fv(12)[0].to_scipy()
+    S2 = random_csr(rng, 1500, S1.shape[1], rng.integers(0, 40, 1500)).to_scipy()
+    info = check(CsrMatrix.from_scipy(sp.vstack([S1, S2]).tocsr()))
+    assert info["all_compressed"] == 0 and info["x_staged"] == 0
+
+
+def test_empty_row_blocks():
+    """A run of more than two blocks of empty rows between two stencils: the
+    empty blocks stage only their row offsets and still produce y = 0."""
+    S = P.poisson_3d_fv(10)[0].to_scipy()
+    n = S.shape[0]
+    A = CsrMatrix.from_scipy(sp.block_diag([S, sp.csr_matrix((1300, 1300)), S]).tocsr())
+    info = check(A)
+    assert info["x_staged"] == 1
+    y, _ = layout_check(A, np.ones(A.ncols))
+    assert np.all(y[n:n + 1300] == 0.0)
+
+
+@pytest.mark.parametrize("ncols", [1, 2, 3, 5, 7])
+def test_narrow_column_ranges(ncols):
+    """Fewer than 4 columns (nothing to bulk-copy, the whole window is tail)
+    and other column counts just past a 4-entry boundary."""
+    rng = np.random.default_rng(ncols)
+    A = random_csr(rng, 900, ncols, rng.integers(0, ncols + 1, 900))
+    assert check(A)["x_staged"] == 1
+
+
+def test_degenerate_shapes():
+    check(csr_from_lists([0, 0, 0], [], [], 4))
+    check(csr_from_lists([0, 1], [0], [2.0], 1))
+    assert check(P.poisson_2d_dirichlet(64, seed=0)[0])["threads_per_row"] == 1
+
+
+def test_networks():
+    for A, _ in P.network_batch(4, seed=5, n_min=200, n_max=900):
+        check(A)
