@@ -103,8 +103,8 @@ std::vector<int> row_partition(const int64_t* rp, int64_t nrows, int tpr) {
   return blk;
 }
 
-// Uploads the column dictionaries and, when every block qualifies, the x
-// windows and index records (encode_layout in layout.cpp).
+// Uploads the column dictionaries, the block records of fully coded matrices
+// and, when every block qualifies, the x windows (encode_layout, layout.cpp).
 static cfd_status upload_layout(DevMat& m, const HostCsr& h, const std::vector<int>& blk, cudaStream_t s) {
   HostLayout L;
   encode_layout(h, blk, L);
@@ -119,11 +119,15 @@ static cfd_status upload_layout(DevMat& m, const HostCsr& h, const std::vector<i
   CFD_TRY_CUDA(cudaMemcpyAsync(m.dict, L.dict.data(), L.dict.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.dict_desc, L.dict_desc.data(), L.dict_desc.size() * sizeof(int2),
                                cudaMemcpyHostToDevice, s));
+  if (L.all_compressed) {
+    CFD_TRY(dmalloc(&m.rec, (int64_t)L.rec.size()));
+    CFD_TRY(dmalloc(&m.roff, (int64_t)L.roff.size()));
+    CFD_TRY_CUDA(cudaMemcpyAsync(m.rec, L.rec.data(), L.rec.size(), cudaMemcpyHostToDevice, s));
+    CFD_TRY_CUDA(cudaMemcpyAsync(m.roff, L.roff.data(), L.roff.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  }
   if (L.xs) {
-    CFD_TRY(dmalloc(&m.xrec, (int64_t)L.xrec.size()));
     CFD_TRY(dmalloc(&m.xwin, (int64_t)L.xwin.size()));
     CFD_TRY(dmalloc(&m.xdesc, (int64_t)L.xdesc.size()));
-    CFD_TRY_CUDA(cudaMemcpyAsync(m.xrec, L.xrec.data(), L.xrec.size(), cudaMemcpyHostToDevice, s));
     CFD_TRY_CUDA(cudaMemcpyAsync(m.xwin, L.xwin.data(), L.xwin.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
     CFD_TRY_CUDA(cudaMemcpyAsync(m.xdesc, L.xdesc.data(), L.xdesc.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
     m.xs = true;
@@ -195,7 +199,8 @@ void devmat_free(DevMat& m) {
   dfree(m.code);
   dfree(m.dict);
   dfree(m.dict_desc);
-  dfree(m.xrec);
+  dfree(m.rec);
+  dfree(m.roff);
   dfree(m.xwin);
   dfree(m.xdesc);
   m.compressed_nnz = 0;

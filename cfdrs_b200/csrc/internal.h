@@ -43,17 +43,20 @@ constexpr int kNnzCap = 4096;
 // are bulk-copied with the block) instead of gathering it from global memory.
 constexpr int kXsCap = 4096;
 constexpr int kXsMaxWin = 8;
-// Index record of an x-staged block (one bulk copy): row offsets relative to
-// the block's first nonzero (uint16, rows + 1 of them), the one-byte codes and
-// the code -> staged-x displacement table (int32), each part 16-byte aligned.
-struct XsRecord {
-  int rp_bytes, code_bytes, e_bytes;
-  __host__ __device__ static XsRecord of(int rows, int nnz, int nd) {
-    return {(2 * (rows + 1) + 15) & ~15, (nnz + 15) & ~15, (4 * nd + 15) & ~15};
+// Index record of a dictionary-coded block, moved by one bulk copy: row
+// offsets relative to the block's first nonzero (uint16, rows + 1 of them),
+// the one-byte codes, the offset dictionary (int32) and, for x-staged
+// matrices, the code -> staged-x displacement table E (int32); each part is
+// 16-byte aligned.
+struct BlockRecord {
+  int rp_bytes, code_bytes, dict_bytes, e_bytes;
+  __host__ __device__ static BlockRecord of(int rows, int nnz, int nd, bool with_e) {
+    const int d = (4 * nd + 15) & ~15;
+    return {(2 * (rows + 1) + 15) & ~15, (nnz + 15) & ~15, d, with_e ? d : 0};
   }
-  __host__ __device__ int bytes() const { return rp_bytes + code_bytes + e_bytes; }
+  __host__ __device__ int bytes() const { return rp_bytes + code_bytes + dict_bytes + e_bytes; }
 };
-constexpr int kXsRecordCap = ((2 * (kRowsPerBlock + 1) + 15) & ~15) + kNnzCap + 4 * 256;
+constexpr int kRecordCap = ((2 * (kRowsPerBlock + 1) + 15) & ~15) + kNnzCap + 2 * 4 * 256;
 // Grid of the streaming vector kernels: 148 SMs x 8 resident CTAs.
 constexpr int kVecGrid = 148 * 8;
 // Device-side scratch for two-stage reductions (per-CTA partials, up to 4 values).
@@ -91,14 +94,17 @@ struct DevMat {
   // base(row) = (row * base_mult) >> 20 with base_mult = (ncols << 20) / nrows:
   // the reference point of the column offsets (row itself for square matrices).
   uint64_t base_mult = 1u << 20;
+  // Block records (all_compressed matrices): rec + 16 * roff[b] is block b's
+  // BlockRecord, the staging unit of the codes-only and x-staged pipelines.
+  uint8_t* rec = nullptr;
+  int* roff = nullptr;
   // x staging (all blocks dictionary-coded and within kXsCap / kXsMaxWin).
   // Windows are 4-entry aligned column ranges [src, src + len) placed one after
   // another in shared memory; a window that would run past ncols copies up to
   // the last full 4-entry group and its `tail` (< 4) entries are read one by
   // one. The x entry of a nonzero with code q in row r sits at shared entry
-  // base(r) - base(r0) + E[q], E being the block's table in its XsRecord.
-  uint8_t* xrec = nullptr;  // concatenated 16-byte aligned XsRecords
-  int4* xwin = nullptr;     // per block kXsMaxWin slots of {src, len}, two per int4
+  // base(r) - base(r0) + E[q], E being the table in the block's record.
+  int4* xwin = nullptr;  // per block kXsMaxWin slots of {src, len}, two per int4
   // per block {windows | tail << 16, zero-offset code or -1, record offset / 16, entries copied}
   int4* xdesc = nullptr;
   bool xs = false;
@@ -114,8 +120,9 @@ struct HostLayout {
   std::vector<int2> dict_desc;
   int64_t compressed_nnz = 0;
   bool all_compressed = false;
+  std::vector<uint8_t> rec;   // BlockRecords (all_compressed)
+  std::vector<int> roff;      // per block record offset / 16
   std::vector<int> xe;        // code -> staged-x displacement (dictionary layout)
-  std::vector<uint8_t> xrec;  // XsRecords
   std::vector<int4> xwin, xdesc;
   bool xs = false;
 };

@@ -39,6 +39,8 @@ struct MatView {
   const uint8_t* __restrict__ code;    // dictionary codes (nullptr: no compressed block)
   const int* __restrict__ dict;        // concatenated offset dictionaries
   const int2* __restrict__ dict_desc;  // per block {first entry, entries}
+  const uint8_t* __restrict__ rec;     // BlockRecords (fully coded matrices)
+  const int* __restrict__ roff;        // per block record offset / 16
   unsigned long long base_mult;        // base(row) = (row * base_mult) >> 20
   int tpr_log2;  // log2 of the threads cooperating on one row
 };
@@ -53,11 +55,13 @@ template <typename VT>
 inline MatView<VT> mat_view(const DevMat& m);
 template <>
 inline MatView<double> mat_view<double>(const DevMat& m) {
-  return {m.rp, m.col, m.v64, m.blk, m.desc, m.code, m.dict, m.dict_desc, (unsigned long long)m.base_mult, ilog2(m.tpr)};
+  return {m.rp,        m.col,   m.v64,  m.blk, m.desc, m.code, m.dict, m.dict_desc,
+          m.rec,       m.roff,  (unsigned long long)m.base_mult,      ilog2(m.tpr)};
 }
 template <>
 inline MatView<float> mat_view<float>(const DevMat& m) {
-  return {m.rp, m.col, m.v32, m.blk, m.desc, m.code, m.dict, m.dict_desc, (unsigned long long)m.base_mult, ilog2(m.tpr)};
+  return {m.rp,        m.col,   m.v32,  m.blk, m.desc, m.code, m.dict, m.dict_desc,
+          m.rec,       m.roff,  (unsigned long long)m.base_mult,      ilog2(m.tpr)};
 }
 
 // Scratch of one two-stage reduction.
@@ -376,8 +380,20 @@ struct ColDict {
   __device__ __forceinline__ int at(int k, int rowbase) const { return rowbase + sdict[scode[k]]; }
 };
 
-template <typename VT, typename XT, bool OFFDIAG, class Epi, class Col>
-__device__ __forceinline__ void rows_from_stage(const Epi& epi, const int* srp, const Col& sc, const VT* sv, int r0,
+// Row offsets as staged: int32 absolute, or the record's uint16 offsets from
+// the block's first nonzero.
+struct RpAbs {
+  const int* p;
+  __device__ __forceinline__ int operator()(int row) const { return p[row]; }
+};
+struct RpRec {
+  const uint16_t* p;
+  int r0, k0;
+  __device__ __forceinline__ int operator()(int row) const { return (int)p[row - r0] + k0; }
+};
+
+template <typename VT, typename XT, bool OFFDIAG, class Epi, class Col, class Rp>
+__device__ __forceinline__ void rows_from_stage(const Epi& epi, const Rp& srp, const Col& sc, const VT* sv, int r0,
                                                 int r1, int tl, int tid, const XT* __restrict__ x, double* red) {
   const int lane = tid & ((1 << tl) - 1);
   const int step = 1 << tl;
@@ -390,8 +406,8 @@ __device__ __forceinline__ void rows_from_stage(const Epi& epi, const int* srp, 
   for (int q = 0; q < kRowsPerThread; ++q) {
     row[q] = r0 + g + q * ngroups;
     const bool live = row[q] < r1;
-    ra[q] = live ? srp[row[q]] + lane : 0;
-    re[q] = live ? srp[row[q] + 1] : 0;
+    ra[q] = live ? srp(row[q]) + lane : 0;
+    re[q] = live ? srp(row[q] + 1) : 0;
     rb[q] = live ? sc.base(row[q]) : 0;
     pre[q] = typename Epi::Pre{};
     if (live && lane == 0) pre[q] = epi.load(row[q]);
@@ -466,16 +482,34 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                : "memory");
 }
 
-// Stage layout. CODES: every staged block is dictionary-coded, so the column
-// region holds one byte per nonzero instead of four and the ring gets deeper.
+// Per-thread asynchronous copies into shared memory (the load path, not the
+// bulk-copy engine), committed and waited on in groups.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_small(uint32_t dst, const void* src) {
+  static_assert(N == 4 || N == 8, "4 or 8 bytes");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst), "l"(src), "n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Stage layout. CODES: every staged block is dictionary-coded and arrives as
+// values plus its BlockRecord (two bulk copies), so the column region holds
+// the record and the ring gets deeper; otherwise values, columns (int32 or
+// codes), row offsets and dictionary arrive separately.
 template <typename VT, bool CODES>
 struct PipeLayout {
   static constexpr int kStages = (CODES && sizeof(VT) == 4) ? 3 : 2;
   static constexpr int kValSlack = 16 / (int)sizeof(VT);
   static constexpr int kValBytes = ((kNnzCap + 2 * kValSlack) * (int)sizeof(VT) + 127) / 128 * 128;
-  static constexpr int kColBytes = CODES ? ((kNnzCap + 32) + 127) / 128 * 128 : ((kNnzCap + 8) * 4 + 127) / 128 * 128;
-  static constexpr int kRpBytes = ((kRowsPerBlock + 1 + 8) * 4 + 127) / 128 * 128;
-  static constexpr int kDictBytes = ((256 + 8) * 4 + 127) / 128 * 128;
+  static constexpr int kColBytes = CODES ? (kRecordCap + 127) / 128 * 128 : ((kNnzCap + 8) * 4 + 127) / 128 * 128;
+  static constexpr int kRpBytes = CODES ? 0 : ((kRowsPerBlock + 1 + 8) * 4 + 127) / 128 * 128;
+  static constexpr int kDictBytes = CODES ? 0 : ((256 + 8) * 4 + 127) / 128 * 128;
   static constexpr int kStageBytes = kValBytes + kColBytes + kRpBytes + kDictBytes;
   static constexpr int kSmemBytes = kStages * kStageBytes;
 };
@@ -529,6 +563,7 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
       const int bl = base + lane * gridDim.x;
       const int4 dl = bl < nblk ? A.desc[bl] : make_int4(0, 0, 0, 0);
       const int2 ddl = (bl < nblk && A.dict_desc) ? A.dict_desc[bl] : make_int2(0, 0);
+      const int rol = (CODES && bl < nblk) ? A.roff[bl] : 0;
       for (int j = 0; j < 32; ++j, ++it) {
         const int b = base + j * gridDim.x;
         if (b >= nblk) {
@@ -543,6 +578,7 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
         int2 md;
         md.x = __shfl_sync(0xffffffffu, ddl.x, j);
         md.y = __shfl_sync(0xffffffffu, ddl.y, j);
+        const int ro = __shfl_sync(0xffffffffu, rol, j);
         int ok = 1;
         if (lane == 0) {
           const int s = it % kStages;
@@ -557,7 +593,27 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
             dmeta[s] = md;
             const int p0 = m.x & ~3, p1 = (m.y + 1 + 3) & ~3;
             const unsigned brp = (unsigned)(p1 - p0) * 4u;
-            if (m.w - m.z > kNnzCap || m.w == m.z) {
+            if constexpr (CODES) {
+              if (m.w - m.z <= kNnzCap && m.y - m.x <= kRowsPerBlock) {
+                // values and the block record
+                const unsigned br = (unsigned)BlockRecord::of(m.y - m.x, m.w - m.z, md.y, false).bytes();
+                const uint8_t* rec = A.rec + (size_t)ro * 16;
+                if (m.w > m.z) {
+                  const int v0 = m.z & ~(mv - 1), v1 = (m.w + mv - 1) & ~(mv - 1);
+                  const unsigned bv = (unsigned)(v1 - v0) * sizeof(VT);
+                  mbar_expect_tx(&full[s], bv + br);
+                  bulk_g2s(stage_val(s), A.val + v0, bv, &full[s]);
+                } else {
+                  mbar_expect_tx(&full[s], br);
+                }
+                bulk_g2s(stage_col(s), rec, br, &full[s]);
+              } else {
+                // a block outside the codes-only invariant: complete the
+                // phase without data and flag it
+                atomicExch(err, 2);
+                mbar_arrive(&full[s]);
+              }
+            } else if (m.w - m.z > kNnzCap || m.w == m.z) {
               mbar_expect_tx(&full[s], brp);
               bulk_g2s(stage_rp(s), A.rp + p0, brp, &full[s]);
             } else if (md.y > 0) {
@@ -572,7 +628,7 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
               bulk_g2s(stage_col(s), A.code + c0, bc, &full[s]);
               bulk_g2s(stage_rp(s), A.rp + p0, brp, &full[s]);
               bulk_g2s(stage_dict(s), A.dict + d0, bd, &full[s]);
-            } else if (!CODES) {
+            } else {
               const int v0 = m.z & ~(mv - 1), v1 = (m.w + mv - 1) & ~(mv - 1);
               const int c0 = m.z & ~3, c1 = (m.w + 3) & ~3;
               const unsigned bv = (unsigned)(v1 - v0) * sizeof(VT), bc = (unsigned)(c1 - c0) * 4u;
@@ -580,11 +636,6 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
               bulk_g2s(stage_val(s), A.val + v0, bv, &full[s]);
               bulk_g2s(stage_col(s), A.col + c0, bc, &full[s]);
               bulk_g2s(stage_rp(s), A.rp + p0, brp, &full[s]);
-            } else {
-              // An int32 block in the codes-only layout breaks the launch
-              // invariant: complete the phase without data and flag it.
-              atomicExch(err, 2);
-              mbar_arrive(&full[s]);
             }
           }
         }
@@ -619,7 +670,21 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
       mbar_wait_bounded(&full[s], parity);  // completes at once; acquires the stage for this thread
       const int4 m = meta[s];
       const int2 md = dmeta[s];
-      const int* srp = stage_rp(s) - (m.x & ~3);
+      if constexpr (CODES) {
+        if (m.w - m.z <= kNnzCap && m.y - m.x <= kRowsPerBlock) {
+          // row offsets, codes and dictionary from the staged block record
+          const BlockRecord R = BlockRecord::of(m.y - m.x, m.w - m.z, md.y, false);
+          const uint8_t* rec = reinterpret_cast<const uint8_t*>(stage_col(s));
+          const RpRec rp{reinterpret_cast<const uint16_t*>(rec), m.x, m.z};
+          const ColDict cd{rec + R.rp_bytes - m.z, reinterpret_cast<const int*>(rec + R.rp_bytes + R.code_bytes),
+                           A.base_mult};
+          rows_from_stage<VT, XT, OFFDIAG>(epi, rp, cd, stage_val(s) - (m.z & ~(mv - 1)), m.x, m.y, tl, tid, x, red);
+        }
+        __syncwarp();
+        if ((tid & 31) == 0) mbar_arrive(&empty[s]);
+        continue;
+      }
+      const RpAbs srp{stage_rp(s) - (m.x & ~3)};
       if (m.w - m.z <= kNnzCap && (md.y > 0 || m.w == m.z)) {
         // codes index the block's own dictionary, staged from entry md.x & ~3
         // (a block of empty rows reads no entry and still runs its epilogue)
@@ -627,11 +692,6 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
                          A.base_mult};
         rows_from_stage<VT, XT, OFFDIAG>(epi, srp, cd, stage_val(s) - (m.z & ~(mv - 1)), m.x, m.y, tl, tid, x, red);
       } else if (m.w - m.z <= kNnzCap) {
-        if (CODES) {  // no int32 columns were staged (flagged by the producer)
-          __syncwarp();
-          if ((tid & 31) == 0) mbar_arrive(&empty[s]);
-          continue;
-        }
         const ColRaw cr{stage_col(s) - (m.z & ~3)};
         rows_from_stage<VT, XT, OFFDIAG>(epi, srp, cr, stage_val(s) - (m.z & ~(mv - 1)), m.x, m.y, tl, tid, x, red);
       } else {
@@ -664,18 +724,21 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
 }
 
 // ---------------------------------------------------------------------------
-// x-staged pipeline (DevMat::xs): each stage receives the block's values, its
-// index record (row offsets, codes, displacement table) and its x windows by
-// bulk copy, so the consumers read every operand from shared memory and no
+// x-staged pipeline (DevMat::xs): each stage receives the block's values and
+// its record (row offsets, codes, dictionary, displacement table) by two bulk
+// copies, and its x windows by 16-byte cp.async copies that the consumer
+// threads issue a ring-depth ahead (the bulk-copy engine serves a limited
+// number of copies per SM at a time, so the windows go through the load
+// path); the consumers then read every operand from shared memory and no
 // gather leaves the SM. One CTA per SM with 16 consumer warps (one row or row
 // group per thread) on a ring sized to fill the SM's shared memory; the
 // consumers take the stages in order, so a parity wait always names the phase
-// it means. Entry addresses are 32-bit shared-window offsets. Summation order
+// it means. Copies address stages by 32-bit shared-window offsets. Summation order
 // per row equals k_spmv_pipe's, so both paths give bit-identical results.
 struct XsView {
   const int4* __restrict__ xdesc;    // per block {windows | tail << 16, zero code, record offset / 16, entries copied}
   const int4* __restrict__ xwin;     // per block 4 x int4 = 8 windows {src, len, src, len}
-  const uint8_t* __restrict__ xrec;  // XsRecords
+  const uint8_t* __restrict__ rec;   // BlockRecords, with displacement tables
   int ncols;
 };
 
@@ -686,7 +749,7 @@ template <typename VT>
 struct XsLayout {
   static constexpr int kValSlack = 16 / (int)sizeof(VT);
   static constexpr int kValBytes = ((kNnzCap + 2 * kValSlack) * (int)sizeof(VT) + 127) / 128 * 128;
-  static constexpr int kRecBytes = (kXsRecordCap + 127) / 128 * 128;
+  static constexpr int kRecBytes = (kRecordCap + 127) / 128 * 128;
   static constexpr int kXBytes = (kXsCap * (int)sizeof(VT) + 127) / 128 * 128;
   static constexpr int kStageBytes = kValBytes + kRecBytes + kXBytes;
   // 227 KB per CTA less 2 KB for the static barriers and reduction scratch
@@ -695,70 +758,52 @@ struct XsLayout {
   static_assert(kStages >= 2, "x-staged ring needs two stages");
 };
 
-__device__ __forceinline__ unsigned lds_u8(uint32_t a) {
-  unsigned v;
-  asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(a));
-  return v;
-}
-__device__ __forceinline__ int lds_u16(uint32_t a) {
-  unsigned v;
-  asm volatile("ld.shared.u16 %0, [%1];" : "=r"(v) : "r"(a));
-  return (int)v;
-}
-__device__ __forceinline__ int lds_s32(uint32_t a) {
-  int v;
-  asm volatile("ld.shared.s32 %0, [%1];" : "=r"(v) : "r"(a));
-  return v;
-}
-template <typename T>
-__device__ __forceinline__ T lds(uint32_t a);
-template <>
-__device__ __forceinline__ float lds<float>(uint32_t a) {
-  float v;
-  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
-  return v;
-}
-template <>
-__device__ __forceinline__ double lds<double>(uint32_t a) {
-  double v;
-  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
-  return v;
-}
-
 // Rows of one staged block (ctid in [0, kXsConsumers)): row group g of 2^tl
 // threads owns row r0 + g; the strided loop and butterfly per row are those of
-// rows_from_stage, so every row is summed in the same order.
+// rows_from_stage, so every row is summed in the same order. Entries are read
+// eight at a time through plain shared-memory pointers, so the compiler can
+// issue the code and value loads of a batch together before the dependent
+// table and x loads (volatile asm loads would pin them in program order).
 template <typename VT, bool OFFDIAG, class Epi>
-__device__ __forceinline__ void rows_from_stage_xs(const Epi& epi, uint32_t a_rp16, uint32_t a_code, uint32_t a_val,
-                                                   uint32_t a_e, uint32_t a_x, int zq, int r0, int r1,
-                                                   unsigned long long mult, int tl, int ctid, double* red) {
-  constexpr int vs = (int)sizeof(VT);
+__device__ __forceinline__ void rows_from_stage_xs(const Epi& epi, const uint16_t* srp, const uint8_t* scode,
+                                                   const VT* sval, const int* se, const VT* sx, int zq, int r0,
+                                                   int r1, unsigned long long mult, int tl, int ctid, double* red) {
+  constexpr int kBatch = 8;
   const int lane = ctid & ((1 << tl) - 1);
   const int step = 1 << tl;
   const int i = ctid >> tl;
   const int row = r0 + i;
   const bool live = row < r1;
   int ka = 0, ke = 0;
-  uint32_t xr = a_x;
+  const VT* xr = sx;
   typename Epi::Pre pre{};
   if (live) {
-    ka = lds_u16(a_rp16 + 2u * (uint32_t)i) + lane;  // offsets from the block's first nonzero
-    ke = lds_u16(a_rp16 + 2u * (uint32_t)i + 2u);
+    ka = srp[i] + lane;  // offsets from the block's first nonzero
+    ke = srp[i + 1];
     const int b0 = (int)(((unsigned long long)r0 * mult) >> 20);
-    xr += (uint32_t)(((int)(((unsigned long long)row * mult) >> 20) - b0) * vs);
+    xr += (int)(((unsigned long long)row * mult) >> 20) - b0;
     if (lane == 0) pre = epi.load(row);
   }
   VT sum = VT(0), diag = VT(0);
-#pragma unroll 4
-  for (int k = ka; k < ke; k += step) {
-    const unsigned c = lds_u8(a_code + (uint32_t)k);
-    const int e = lds_s32(a_e + 4u * c);
-    const VT xv = lds<VT>(xr + (uint32_t)(e * vs));
-    const VT v = lds<VT>(a_val + (uint32_t)(k * vs));
-    if (OFFDIAG && (int)c == zq)
-      diag = v;
-    else
-      sum += v * xv;
+  for (int kb = ka; kb < ke; kb += kBatch * step) {
+    unsigned c[kBatch];
+    VT v[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int k = kb + u * step;
+      c[u] = k < ke ? scode[k] : 0u;
+      v[u] = k < ke ? sval[k] : VT(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      if (kb + u * step < ke) {
+        const VT xv = xr[se[c[u]]];
+        if (OFFDIAG && (int)c[u] == zq)
+          diag = v[u];
+        else
+          sum += v[u] * xv;
+      }
+    }
   }
   for (int o = step >> 1; o > 0; o >>= 1) {
     sum += __shfl_xor_sync(0xffffffffu, sum, o);
@@ -816,9 +861,6 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
       const int4 m = have ? A.desc[bl] : make_int4(0, 0, 0, 0);
       const int2 md = have ? A.dict_desc[bl] : make_int2(0, 0);
       const int4 xd = have ? X.xdesc[bl] : make_int4(0, -1, 0, 0);
-      int4 w[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) w[i] = have ? X.xwin[(size_t)bl * 4 + i] : make_int4(0, 0, 0, 0);
       const int nj = min(32, (nblk - base + (int)gridDim.x - 1) / (int)gridDim.x);
       for (int j = 0; j < nj; ++j, ++it) {
         int ok = 1;
@@ -832,10 +874,9 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
             ok = 0;
           } else {
             meta[s] = m;
-            const int nwin = xd.x & 0xffff;
-            xmeta[s] = make_int4(md.y, xd.y, xd.x >> 16, xd.w);
-            const XsRecord R = XsRecord::of(m.y - m.x, m.w - m.z, md.y);
-            const uint8_t* rec = X.xrec + (size_t)xd.z * 16;
+            xmeta[s] = make_int4(md.y, xd.y, 0, 0);
+            const BlockRecord R = BlockRecord::of(m.y - m.x, m.w - m.z, md.y, true);
+            const uint8_t* rec = X.rec + (size_t)xd.z * 16;
             if (m.w - m.z > kNnzCap || m.y - m.x > kRowsPerBlock) {
               // outside the x-staged invariant: complete the phase and flag it
               atomicExch(err, 2);
@@ -845,20 +886,10 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
               bulk_g2s(p_of(a_rec(s)), rec, (unsigned)R.bytes(), &full[s]);
             } else {
               const int v0 = m.z & ~(mv - 1), v1 = (m.w + mv - 1) & ~(mv - 1);
-              const unsigned bv = (unsigned)(v1 - v0) * vs, bx = (unsigned)xd.w * vs;
-              mbar_expect_tx(&full[s], bv + (unsigned)R.bytes() + bx);
+              const unsigned bv = (unsigned)(v1 - v0) * vs;
+              mbar_expect_tx(&full[s], bv + (unsigned)R.bytes());
               bulk_g2s(p_of(a_val(s)), A.val + v0, bv, &full[s]);
               bulk_g2s(p_of(a_rec(s)), rec, (unsigned)R.bytes(), &full[s]);
-              uint32_t soff = a_x(s);
-#pragma unroll
-              for (int i = 0; i < 8; ++i) {
-                const int src = (i & 1) ? w[i >> 1].z : w[i >> 1].x;
-                const int len = (i & 1) ? w[i >> 1].w : w[i >> 1].y;
-                if (i < nwin && len > 0) {
-                  bulk_g2s(p_of(soff), x + src, (unsigned)len * vs, &full[s]);
-                  soff += (uint32_t)(len * vs);
-                }
-              }
             }
           }
         }
@@ -875,24 +906,56 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
         mbar_wait_bounded(&full[j % kStages], (unsigned)(j / kStages) & 1u);
     }
   } else {
-    // ---- consumers: every block of this CTA in order
+    // ---- consumers: every block of this CTA in order. The x windows of
+    // iteration j go into stage j % kStages during iteration j - kAhead, after
+    // every consumer has left iteration j - kStages (the stage's previous
+    // block); one cp.async group per iteration, waited kAhead iterations later.
+    constexpr int kAhead = kStages - 1;
     const int tl = A.tpr_log2;
-    const int ncols4 = X.ncols & ~3;
+    const VT* xtail = x + (X.ncols & ~3);
+    int4 nd, nw0, nw1, nw2, nw3;  // descriptors of the next block to prefetch
+    auto load_desc = [&](int j) {
+      const int bj = blockIdx.x + j * (int)gridDim.x;
+      if (bj < nblk) {
+        nd = X.xdesc[bj];
+        nw0 = X.xwin[(size_t)bj * 4 + 0];
+        nw1 = X.xwin[(size_t)bj * 4 + 1];
+        nw2 = X.xwin[(size_t)bj * 4 + 2];
+        nw3 = X.xwin[(size_t)bj * 4 + 3];
+      } else {
+        nd = make_int4(0, -1, 0, 0);
+      }
+    };
+    auto issue_x = [&](int j) {
+      const int s = j % kStages;
+      const int nwin = nd.x & 0xffff, tail = nd.x >> 16;
+      const int4 wq[4] = {nw0, nw1, nw2, nw3};
+      uint32_t dst = a_x(s);
+#pragma unroll
+      for (int i = 0; i < kXsMaxWin; ++i) {
+        if (i < nwin) {
+          const int src = (i & 1) ? wq[i >> 1].z : wq[i >> 1].x;
+          const int len = (i & 1) ? wq[i >> 1].w : wq[i >> 1].y;
+          const int chunks = len * vs / 16;
+          for (int c = tid; c < chunks; c += kXsConsumers) cp_async16(dst + 16u * c, x + src + c * (16 / vs));
+          dst += (uint32_t)(len * vs);
+        }
+      }
+      // the 1-3 entries past the last 16-byte boundary of x
+      if (tid < tail) cp_async_small<vs>(a_x(s) + (uint32_t)((nd.w + tid) * vs), xtail + tid);
+      cp_async_commit();
+    };
+    for (int j = 0; j < kAhead; ++j) {
+      load_desc(j);
+      issue_x(j);
+    }
+    load_desc(kAhead);
     int it = 0;
     for (int b = blockIdx.x; b < nblk; b += (int)gridDim.x, ++it) {
       const int s = it % kStages;
       const unsigned parity = (unsigned)(it / kStages) & 1u;
-      if (tid == 0) {
-        const int ok = (!s_abort && mbar_wait_bounded(&full[s], parity)) ? 1 : 0;
-        s_ok[s] = ok;
-        const int4 xm = xmeta[s];
-        if (ok && xm.z > 0) {
-          // the 1-3 entries past the last 16-byte boundary of x
-          const uint32_t at = a_x(s) + (uint32_t)(xm.w * vs);
-          for (int t = 0; t < xm.z; ++t) *reinterpret_cast<VT*>(p_of(at + (uint32_t)(t * vs))) = x[ncols4 + t];
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        }
-      }
+      if (tid == 0) s_ok[s] = (!s_abort && mbar_wait_bounded(&full[s], parity)) ? 1 : 0;
+      cp_async_wait<kAhead - 1>();  // this thread's windows of block `it` have landed
       asm volatile("bar.sync 1, %0;" ::"n"(kXsConsumers) : "memory");
       if (!s_ok[s]) {
         if (tid == 0) {
@@ -905,15 +968,20 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
       const int4 m = meta[s];
       const int4 xm = xmeta[s];
       if (m.w - m.z <= kNnzCap && m.y - m.x <= kRowsPerBlock) {
-        const XsRecord R = XsRecord::of(m.y - m.x, m.w - m.z, xm.x);
-        rows_from_stage_xs<VT, OFFDIAG>(epi, a_rec(s), a_rec(s) + (uint32_t)R.rp_bytes,
-                                        a_val(s) + (uint32_t)((m.z & (mv - 1)) * vs),
-                                        a_rec(s) + (uint32_t)(R.rp_bytes + R.code_bytes), a_x(s), xm.y, m.x, m.y,
-                                        A.base_mult, tl, tid, red);
+        const BlockRecord R = BlockRecord::of(m.y - m.x, m.w - m.z, xm.x, true);
+        const unsigned char* rec = smem + (a_rec(s) - sbase);
+        rows_from_stage_xs<VT, OFFDIAG>(
+            epi, reinterpret_cast<const uint16_t*>(rec), rec + R.rp_bytes,
+            reinterpret_cast<const VT*>(smem + (a_val(s) - sbase)) + (m.z & (mv - 1)),
+            reinterpret_cast<const int*>(rec + R.rp_bytes + R.code_bytes + R.dict_bytes),
+            reinterpret_cast<const VT*>(smem + (a_x(s) - sbase)), xm.y, m.x, m.y, A.base_mult, tl, tid, red);
       }
+      issue_x(it + kAhead);  // into the stage left by iteration it - 1
+      load_desc(it + kAhead + 1);
       __syncwarp();
       if ((tid & 31) == 0) mbar_arrive(&empty[s]);
     }
+    cp_async_wait<0>();  // no copy may land after the CTA leaves
   }
   __syncthreads();
   if (s_abort) return;

@@ -79,7 +79,6 @@ void drop_xs(HostLayout& L) {
   L.xwin.clear();
   L.xdesc.clear();
   L.xe.clear();
-  L.xrec.clear();
 }
 
 }  // namespace
@@ -133,6 +132,7 @@ void encode_layout(const HostCsr& h, const std::vector<int>& blk, HostLayout& L)
   L.all_compressed = comp > 0 && raw_blocks == 0;
   if (!L.all_compressed) return;
 
+  // x windows: every non-empty block must fit the staging limits
   L.xwin.assign((size_t)nb * (kXsMaxWin / 2), make_int4(0, 0, 0, 0));
   L.xdesc.assign(nb, make_int4(0, -1, 0, 0));
   L.xe.assign(L.dict.size(), 0);
@@ -145,49 +145,57 @@ void encode_layout(const HostCsr& h, const std::vector<int>& blk, HostLayout& L)
                        L.xe.data() + L.dict_desc[b].x))
       ++bad;
   }
-  if (bad > 0) {
-    drop_xs(L);
-    return;
-  }
-  // index records, back to back
-  std::vector<int64_t> roff(nb + 1, 0);
+  bool xs = bad == 0;
+  if (!xs) drop_xs(L);
+  // block records, back to back
+  std::vector<int64_t> off(nb + 1, 0);
   for (int b = 0; b < nb; ++b) {
     const int rows = blk[b + 1] - blk[b];
     const int nnz = (int)(h.rp[blk[b + 1]] - h.rp[blk[b]]);
-    if (rows > kRowsPerBlock) {
+    if (rows > kRowsPerBlock) {  // partitions never make such blocks; stay on the int32 path
       drop_xs(L);
+      L.all_compressed = false;
       return;
     }
-    roff[b + 1] = roff[b] + XsRecord::of(rows, nnz, L.dict_desc[b].y).bytes();
-    L.xdesc[b].z = (int)(roff[b] / 16);
+    off[b + 1] = off[b] + BlockRecord::of(rows, nnz, L.dict_desc[b].y, xs).bytes();
   }
-  if (roff[nb] / 16 >= INT32_MAX) {
+  if (off[nb] / 16 >= INT32_MAX) {
     drop_xs(L);
+    L.all_compressed = false;
     return;
   }
-  L.xrec.assign(roff[nb] + 16, 0);
+  L.roff.resize(nb);
+  for (int b = 0; b < nb; ++b) {
+    L.roff[b] = (int)(off[b] / 16);
+    if (xs) L.xdesc[b].z = L.roff[b];
+  }
+  L.rec.assign(off[nb] + 16, 0);
 #pragma omp parallel for schedule(dynamic, 64)
   for (int b = 0; b < nb; ++b) {
     const int r0 = blk[b], r1 = blk[b + 1];
     const int64_t k0 = h.rp[r0], k1 = h.rp[r1];
     const int2 dd = L.dict_desc[b];
-    const XsRecord R = XsRecord::of(r1 - r0, (int)(k1 - k0), dd.y);
-    uint8_t* rec = L.xrec.data() + roff[b];
+    const BlockRecord R = BlockRecord::of(r1 - r0, (int)(k1 - k0), dd.y, xs);
+    uint8_t* rec = L.rec.data() + off[b];
     uint16_t* rp16 = reinterpret_cast<uint16_t*>(rec);
     for (int r = r0; r <= r1; ++r) rp16[r - r0] = (uint16_t)(h.rp[r] - k0);
     std::copy(L.code.begin() + k0, L.code.begin() + k1, rec + R.rp_bytes);
-    std::copy(L.xe.begin() + dd.x, L.xe.begin() + dd.x + dd.y,
+    std::copy(L.dict.begin() + dd.x, L.dict.begin() + dd.x + dd.y,
               reinterpret_cast<int*>(rec + R.rp_bytes + R.code_bytes));
+    if (xs)
+      std::copy(L.xe.begin() + dd.x, L.xe.begin() + dd.x + dd.y,
+                reinterpret_cast<int*>(rec + R.rp_bytes + R.code_bytes + R.dict_bytes));
   }
-  L.xs = true;
+  L.xs = xs;
 }
 
-// Host walk of one SpMV through the device layout. For x-staged layouts it
+// Host walk of one SpMV through the device layout. Codes-only layouts are read
+// from the block records as k_spmv_pipe reads them. For x-staged layouts it
 // rebuilds each block's shared-memory x image from the windows and the tail
 // exactly as k_spmv_xs does, reads row offsets, codes and the displacement
-// table from the block's index record, checks that every one of them lies
-// inside its region and that the staged entry is x[col], and sums rows in the
-// kernel's order for one thread per row. Returns false with a message on the
+// table from the block's record, checks that every one of them lies inside its
+// region and that the staged entry is x[col], and sums rows in the kernel's
+// order for one thread per row. Returns false with a message on the
 // first violation.
 bool check_layout(const HostCsr& h, const std::vector<int>& blk, const HostLayout& L, const double* x, double* y,
                   std::string* why, int64_t* staged_entries, int* max_windows) {
@@ -212,14 +220,31 @@ bool check_layout(const HostCsr& h, const std::vector<int>& blk, const HostLayou
     if (L.all_compressed && k1 > k0 && !coded)
       return fail("block %d: all_compressed but nonzeros %lld..%lld uncoded", b, k0, k1);
     if (!L.xs) {
+      // codes-only pipeline: row offsets, codes and dictionary from the record
+      const uint16_t* rp16 = nullptr;
+      const uint8_t* rcode = nullptr;
+      const int* rdict = nullptr;
+      if (L.all_compressed) {
+        const BlockRecord R = BlockRecord::of(r1 - r0, (int)(k1 - k0), dd.y, false);
+        if (r1 - r0 > kRowsPerBlock || R.bytes() > kRecordCap)
+          return fail("block %d: %lld rows, record of %lld bytes", b, r1 - r0, R.bytes());
+        const int64_t ro = (int64_t)L.roff[b] * 16;
+        if (ro + R.bytes() > (int64_t)L.rec.size())
+          return fail("block %d: record end %lld > %lld", b, ro + R.bytes(), (int64_t)L.rec.size());
+        rp16 = reinterpret_cast<const uint16_t*>(L.rec.data() + ro);
+        rcode = L.rec.data() + ro + R.rp_bytes;
+        rdict = reinterpret_cast<const int*>(L.rec.data() + ro + R.rp_bytes + R.code_bytes);
+      }
       for (int r = r0; r < r1; ++r) {
+        if (rp16 && (rp16[r - r0] != h.rp[r] - k0 || rp16[r - r0 + 1] != h.rp[r + 1] - k0))
+          return fail("block %d: record row offsets %lld..%lld", b, rp16[r - r0], rp16[r - r0 + 1]);
         double s = 0.0;
         for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k) {
           int64_t c = h.ci[k];
           if (coded) {
-            const int q = L.code[k];
+            const int q = rcode ? rcode[k - k0] : L.code[k];
             if (q >= dd.y) return fail("block %d: code %lld >= %lld entries", b, q, dd.y);
-            c = row_base(r) + L.dict[dd.x + q];
+            c = row_base(r) + (rdict ? rdict[q] : L.dict[dd.x + q]);
             if (c != h.ci[k]) return fail("block %d: decoded column %lld != %lld", b, c, h.ci[k]);
           }
           s += h.v[k] * x[c];
@@ -235,16 +260,17 @@ bool check_layout(const HostCsr& h, const std::vector<int>& blk, const HostLayou
     if (nwin > kXsMaxWin) return fail("block %d: %lld windows > %lld", b, nwin, kXsMaxWin);
     if (tail < 0 || tail > 3 || copied + tail > kXsCap) return fail("block %d: tail %lld copied %lld", b, tail, copied);
     if ((k1 == k0) != (dd.y == 0)) return fail("block %d: dictionary size %lld for %lld nonzeros", b, dd.y, k1 - k0);
-    const XsRecord R = XsRecord::of(r1 - r0, (int)(k1 - k0), dd.y);
-    if (r1 - r0 > kRowsPerBlock || R.bytes() > kXsRecordCap)
+    const BlockRecord R = BlockRecord::of(r1 - r0, (int)(k1 - k0), dd.y, true);
+    if (r1 - r0 > kRowsPerBlock || R.bytes() > kRecordCap)
       return fail("block %d: %lld rows, record of %lld bytes", b, r1 - r0, R.bytes());
-    const int64_t roff = (int64_t)xd.z * 16;
-    if (roff + R.bytes() > (int64_t)L.xrec.size())
-      return fail("block %d: record end %lld > %lld", b, roff + R.bytes(), (int64_t)L.xrec.size());
-    const uint8_t* rec = L.xrec.data() + roff;
+    if (xd.z != L.roff[b]) return fail("block %d: record offset %lld != %lld", b, xd.z, L.roff[b]);
+    const int64_t ro = (int64_t)xd.z * 16;
+    if (ro + R.bytes() > (int64_t)L.rec.size())
+      return fail("block %d: record end %lld > %lld", b, ro + R.bytes(), (int64_t)L.rec.size());
+    const uint8_t* rec = L.rec.data() + ro;
     const uint16_t* rp16 = reinterpret_cast<const uint16_t*>(rec);
     const uint8_t* rcode = rec + R.rp_bytes;
-    const int* rE = reinterpret_cast<const int*>(rec + R.rp_bytes + R.code_bytes);
+    const int* rE = reinterpret_cast<const int*>(rec + R.rp_bytes + R.code_bytes + R.dict_bytes);
     std::fill(src.begin(), src.end(), -1);
     const int* slot = reinterpret_cast<const int*>(&L.xwin[(size_t)b * (kXsMaxWin / 2)]);
     int64_t soff = 0;

@@ -345,7 +345,7 @@ struct Launcher {
       attr[ctx->device] = true;
     }
     const int grid = std::min(m.nblk, ctx->num_sms);
-    const XsView xv{m.xdesc, m.xwin, m.xrec, (int)m.ncols};
+    const XsView xv{m.xdesc, m.xwin, m.rec, (int)m.ncols};
     kern<<<grid, kXsThreads, smem, s>>>(mat_view<VT>(m), xv, m.nblk, x, epi, ctx->err);
     ctx->stats.xs_launches++;
     return CFD_OK;

@@ -18,10 +18,12 @@ def _events(torch):
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def time_spmv(torch, d, n_rows, n_cols, nnz, fp32, reps):
+def time_spmv(torch, d, n_rows, n_cols, nnz, fp32, reps, gather=False):
+    """Mean time of one SpMV. gather=True passes x one element into its buffer
+    (not 16-byte aligned), which keeps an x-staged matrix on the gather pipeline."""
     dt = torch.float32 if fp32 else torch.float64
     vs = 4 if fp32 else 8
-    x = torch.rand(n_cols, device="cuda", dtype=dt)
+    x = torch.rand(n_cols + 1, device="cuda", dtype=dt)[1:] if gather else torch.rand(n_cols, device="cuda", dtype=dt)
     y = torch.empty(n_rows, device="cuda", dtype=dt)
     for _ in range(3):
         d.spmv(x.data_ptr(), y.data_ptr(), fp32=fp32)
@@ -61,9 +63,13 @@ def main(argv=None):
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
     if a.case == "spmv":
         d = DeviceCsr(A, ctx)
+        staged = d.layout()["x_staged"]
         for fp32 in (True, False):
-            ms, nb, x, y = time_spmv(torch, d, A.nrows, A.ncols, A.nnz, fp32, a.reps)
-            print(f"{a.n}^3 {'f32' if fp32 else 'f64'}: {ms * 1e3:.1f} us {nb / ms / 1e6:.0f} GB/s", flush=True)
+            for gather in ((False, True) if staged else (False,)):
+                ms, nb, x, y = time_spmv(torch, d, A.nrows, A.ncols, A.nnz, fp32, a.reps, gather)
+                path = "x-staged" if staged and not gather else "gather"
+                print(f"{a.n}^3 {'f32' if fp32 else 'f64'} {path}: {ms * 1e3:.1f} us {nb / ms / 1e6:.0f} GB/s",
+                      flush=True)
         return 0
     amg = cf.AlgebraicMultigrid(A, cf.AMGConfig.pressure_poisson(), ctx=ctx)
     if a.case == "levels":
@@ -74,10 +80,14 @@ def main(argv=None):
                     continue
                 m = amg.level(l, which)
                 d = DeviceCsr(m, ctx)
+                staged = d.layout()["x_staged"]
                 for fp32 in (True, False):
-                    ms, nb, _, _ = time_spmv(torch, d, m.nrows, m.ncols, m.nnz, fp32, a.reps)
-                    print(f"L{l} {name} {m.nrows}x{m.ncols} nnz={m.nnz} ({m.nnz / max(m.nrows, 1):.1f}/row) "
-                          f"{'f32' if fp32 else 'f64'}: {ms * 1e3:8.1f} us {nb / ms / 1e6:6.0f} GB/s", flush=True)
+                    for gather in ((False, True) if staged else (False,)):
+                        ms, nb, _, _ = time_spmv(torch, d, m.nrows, m.ncols, m.nnz, fp32, a.reps, gather)
+                        path = "x-staged" if staged and not gather else "gather"
+                        print(f"L{l} {name} {m.nrows}x{m.ncols} nnz={m.nnz} ({m.nnz / max(m.nrows, 1):.1f}/row) "
+                              f"{'f32' if fp32 else 'f64'} {path:8s}: {ms * 1e3:8.1f} us {nb / ms / 1e6:6.0f} GB/s",
+                              flush=True)
         return 0
     bd = torch.as_tensor(b, device="cuda")
     x = torch.zeros_like(bd)
