@@ -21,7 +21,7 @@ EXPORTS = [
     "cfd_last_error", "cfd_version",
     "cfd_context_create", "cfd_context_set_stream", "cfd_context_synchronize", "cfd_context_destroy",
     "cfd_csr_create", "cfd_csr_create_i32", "cfd_csr_update_values", "cfd_csr_info", "cfd_csr_destroy",
-    "cfd_csr_layout", "cfd_layout_check",
+    "cfd_csr_layout", "cfd_csr_set_path", "cfd_layout_check",
     "cfd_spmv", "cfd_spmv_f32",
     "cfd_amg_config_default", "cfd_amg_setup", "cfd_amg_recompute", "cfd_amg_apply", "cfd_amg_stats",
     "cfd_amg_level", "cfd_amg_destroy",
@@ -72,7 +72,7 @@ class BatchReportC(C.Structure):
 class LayoutInfoC(C.Structure):
     _fields_ = [("blocks", C.c_int64), ("compressed_nnz", C.c_int64), ("all_compressed", C.c_int32),
                 ("x_staged", C.c_int32), ("threads_per_row", C.c_int32), ("max_windows", C.c_int32),
-                ("staged_x_entries", C.c_int64)]
+                ("staged_x_entries", C.c_int64), ("path_f32", C.c_int32), ("path_f64", C.c_int32)]
 
 
 class KernelStatsC(C.Structure):
@@ -115,6 +115,7 @@ def load():
         "cfd_csr_info": (C.c_int, [P, P, P, P]),
         "cfd_csr_destroy": (C.c_int, [P]),
         "cfd_csr_layout": (C.c_int, [P, P]),
+        "cfd_csr_set_path": (C.c_int, [P, I32, I32]),
         "cfd_layout_check": (C.c_int, [I64, I64, I64, P, P, P, P, P, P]),
         "cfd_spmv": (C.c_int, [P, P, P]),
         "cfd_spmv_f32": (C.c_int, [P, P, P]),

@@ -206,6 +206,7 @@ void devmat_free(DevMat& m) {
   m.compressed_nnz = 0;
   m.all_compressed = false;
   m.xs = false;
+  m.path[0] = m.path[1] = -1;
   m.nblk = 0;
 }
 
@@ -556,6 +557,26 @@ cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out) {
   out->all_compressed = m.all_compressed ? 1 : 0;
   out->x_staged = m.xs ? 1 : 0;
   out->threads_per_row = m.tpr;
+  out->path_f32 = m.path[0];
+  out->path_f64 = m.path[1];
+  return CFD_OK;
+}
+
+cfd_status cfd_csr_set_path(cfd_csr* a, int32_t fp32, int32_t path) {
+  if (!a) {
+    set_error("cfd_csr_set_path: null matrix");
+    return CFD_ERR_STATE;
+  }
+  const DevMat& m = a->dev;
+  const bool ok = path == CFD_PATH_AUTO || path == CFD_PATH_SPLIT ||
+                  (path == CFD_PATH_RECORD && m.all_compressed) || (path == CFD_PATH_X_STAGED && m.xs);
+  if (!ok) {
+    set_error("SpMV pipeline %d not available for this matrix (all blocks coded: %d, x staged: %d)", path,
+              (int)m.all_compressed, (int)m.xs);
+    return CFD_ERR_CONFIG;
+  }
+  std::lock_guard<std::mutex> g(a->ctx->mu);
+  m.path[fp32 ? 0 : 1] = (int8_t)path;
   return CFD_OK;
 }
 

@@ -482,22 +482,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                : "memory");
 }
 
-// Per-thread asynchronous copies into shared memory (the load path, not the
-// bulk-copy engine), committed and waited on in groups.
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_small(uint32_t dst, const void* src) {
-  static_assert(N == 4 || N == 8, "4 or 8 bytes");
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst), "l"(src), "n"(N) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 // Stage layout. CODES: every staged block is dictionary-coded and arrives as
 // values plus its BlockRecord (two bulk copies), so the column region holds
 // the record and the ring gets deeper; otherwise values, columns (int32 or
@@ -724,13 +708,10 @@ __global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, in
 }
 
 // ---------------------------------------------------------------------------
-// x-staged pipeline (DevMat::xs): each stage receives the block's values and
-// its record (row offsets, codes, dictionary, displacement table) by two bulk
-// copies, and its x windows by 16-byte cp.async copies that the consumer
-// threads issue a ring-depth ahead (the bulk-copy engine serves a limited
-// number of copies per SM at a time, so the windows go through the load
-// path); the consumers then read every operand from shared memory and no
-// gather leaves the SM. One CTA per SM with 16 consumer warps (one row or row
+// x-staged pipeline (DevMat::xs): each stage receives the block's values, its
+// record (row offsets, codes, dictionary, displacement table) and its x
+// windows by bulk copy, so the consumers read every operand from shared
+// memory and no gather leaves the SM. One CTA per SM with 16 consumer warps (one row or row
 // group per thread) on a ring sized to fill the SM's shared memory; the
 // consumers take the stages in order, so a parity wait always names the phase
 // it means. Copies address stages by 32-bit shared-window offsets. Summation order
@@ -861,6 +842,9 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
       const int4 m = have ? A.desc[bl] : make_int4(0, 0, 0, 0);
       const int2 md = have ? A.dict_desc[bl] : make_int2(0, 0);
       const int4 xd = have ? X.xdesc[bl] : make_int4(0, -1, 0, 0);
+      int4 w[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) w[i] = have ? X.xwin[(size_t)bl * 4 + i] : make_int4(0, 0, 0, 0);
       const int nj = min(32, (nblk - base + (int)gridDim.x - 1) / (int)gridDim.x);
       for (int j = 0; j < nj; ++j, ++it) {
         int ok = 1;
@@ -874,7 +858,8 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
             ok = 0;
           } else {
             meta[s] = m;
-            xmeta[s] = make_int4(md.y, xd.y, 0, 0);
+            const int nwin = xd.x & 0xffff;
+            xmeta[s] = make_int4(md.y, xd.y, xd.x >> 16, xd.w);
             const BlockRecord R = BlockRecord::of(m.y - m.x, m.w - m.z, md.y, true);
             const uint8_t* rec = X.rec + (size_t)xd.z * 16;
             if (m.w - m.z > kNnzCap || m.y - m.x > kRowsPerBlock) {
@@ -886,10 +871,20 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
               bulk_g2s(p_of(a_rec(s)), rec, (unsigned)R.bytes(), &full[s]);
             } else {
               const int v0 = m.z & ~(mv - 1), v1 = (m.w + mv - 1) & ~(mv - 1);
-              const unsigned bv = (unsigned)(v1 - v0) * vs;
-              mbar_expect_tx(&full[s], bv + (unsigned)R.bytes());
+              const unsigned bv = (unsigned)(v1 - v0) * vs, bx = (unsigned)xd.w * vs;
+              mbar_expect_tx(&full[s], bv + (unsigned)R.bytes() + bx);
               bulk_g2s(p_of(a_val(s)), A.val + v0, bv, &full[s]);
               bulk_g2s(p_of(a_rec(s)), rec, (unsigned)R.bytes(), &full[s]);
+              uint32_t soff = a_x(s);
+#pragma unroll
+              for (int i = 0; i < kXsMaxWin; ++i) {
+                const int src = (i & 1) ? w[i >> 1].z : w[i >> 1].x;
+                const int len = (i & 1) ? w[i >> 1].w : w[i >> 1].y;
+                if (i < nwin && len > 0) {
+                  bulk_g2s(p_of(soff), x + src, (unsigned)len * vs, &full[s]);
+                  soff += (uint32_t)(len * vs);
+                }
+              }
             }
           }
         }
@@ -906,56 +901,24 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
         mbar_wait_bounded(&full[j % kStages], (unsigned)(j / kStages) & 1u);
     }
   } else {
-    // ---- consumers: every block of this CTA in order. The x windows of
-    // iteration j go into stage j % kStages during iteration j - kAhead, after
-    // every consumer has left iteration j - kStages (the stage's previous
-    // block); one cp.async group per iteration, waited kAhead iterations later.
-    constexpr int kAhead = kStages - 1;
+    // ---- consumers: every block of this CTA in order
     const int tl = A.tpr_log2;
-    const VT* xtail = x + (X.ncols & ~3);
-    int4 nd, nw0, nw1, nw2, nw3;  // descriptors of the next block to prefetch
-    auto load_desc = [&](int j) {
-      const int bj = blockIdx.x + j * (int)gridDim.x;
-      if (bj < nblk) {
-        nd = X.xdesc[bj];
-        nw0 = X.xwin[(size_t)bj * 4 + 0];
-        nw1 = X.xwin[(size_t)bj * 4 + 1];
-        nw2 = X.xwin[(size_t)bj * 4 + 2];
-        nw3 = X.xwin[(size_t)bj * 4 + 3];
-      } else {
-        nd = make_int4(0, -1, 0, 0);
-      }
-    };
-    auto issue_x = [&](int j) {
-      const int s = j % kStages;
-      const int nwin = nd.x & 0xffff, tail = nd.x >> 16;
-      const int4 wq[4] = {nw0, nw1, nw2, nw3};
-      uint32_t dst = a_x(s);
-#pragma unroll
-      for (int i = 0; i < kXsMaxWin; ++i) {
-        if (i < nwin) {
-          const int src = (i & 1) ? wq[i >> 1].z : wq[i >> 1].x;
-          const int len = (i & 1) ? wq[i >> 1].w : wq[i >> 1].y;
-          const int chunks = len * vs / 16;
-          for (int c = tid; c < chunks; c += kXsConsumers) cp_async16(dst + 16u * c, x + src + c * (16 / vs));
-          dst += (uint32_t)(len * vs);
-        }
-      }
-      // the 1-3 entries past the last 16-byte boundary of x
-      if (tid < tail) cp_async_small<vs>(a_x(s) + (uint32_t)((nd.w + tid) * vs), xtail + tid);
-      cp_async_commit();
-    };
-    for (int j = 0; j < kAhead; ++j) {
-      load_desc(j);
-      issue_x(j);
-    }
-    load_desc(kAhead);
+    const int ncols4 = X.ncols & ~3;
     int it = 0;
     for (int b = blockIdx.x; b < nblk; b += (int)gridDim.x, ++it) {
       const int s = it % kStages;
       const unsigned parity = (unsigned)(it / kStages) & 1u;
-      if (tid == 0) s_ok[s] = (!s_abort && mbar_wait_bounded(&full[s], parity)) ? 1 : 0;
-      cp_async_wait<kAhead - 1>();  // this thread's windows of block `it` have landed
+      if (tid == 0) {
+        const int ok = (!s_abort && mbar_wait_bounded(&full[s], parity)) ? 1 : 0;
+        s_ok[s] = ok;
+        const int4 xm = xmeta[s];
+        if (ok && xm.z > 0) {
+          // the 1-3 entries past the last 16-byte boundary of x
+          VT* at = reinterpret_cast<VT*>(smem + (a_x(s) - sbase)) + xm.w;
+          for (int t = 0; t < xm.z; ++t) at[t] = x[ncols4 + t];
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        }
+      }
       asm volatile("bar.sync 1, %0;" ::"n"(kXsConsumers) : "memory");
       if (!s_ok[s]) {
         if (tid == 0) {
@@ -976,12 +939,9 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
             reinterpret_cast<const int*>(rec + R.rp_bytes + R.code_bytes + R.dict_bytes),
             reinterpret_cast<const VT*>(smem + (a_x(s) - sbase)), xm.y, m.x, m.y, A.base_mult, tl, tid, red);
       }
-      issue_x(it + kAhead);  // into the stage left by iteration it - 1
-      load_desc(it + kAhead + 1);
       __syncwarp();
       if ((tid & 31) == 0) mbar_arrive(&empty[s]);
     }
-    cp_async_wait<0>();  // no copy may land after the CTA leaves
   }
   __syncthreads();
   if (s_abort) return;

@@ -350,25 +350,93 @@ struct Launcher {
     ctx->stats.xs_launches++;
     return CFD_OK;
   }
-  // Every SpMV runs a persistent bulk-copy pipeline. Matrices whose blocks all
-  // have dictionary codes and compact x windows stage x with the block (when x
-  // is 16-byte aligned); other fully coded matrices use the codes-only ring,
-  // the rest the int32-column ring.
+  // Every SpMV runs a persistent bulk-copy pipeline: the split one (values,
+  // columns or codes, row offsets and dictionary copied separately; any
+  // matrix), the record one (values plus one block record; fully coded
+  // matrices) or the x-staged one (x windows staged with the block). All three
+  // sum each row in the same order, so the choice changes speed only; it is
+  // made per matrix and precision by timing the eligible pipelines once.
+  static constexpr int kPathSplit = 0, kPathRecord = 1, kPathXs = 2;
   template <typename VT, typename XT, bool OFF, class Epi>
   cfd_status spmv(const DevMat& m, const XT* x, Epi epi) {
     if (m.nrows == 0) return CFD_OK;
     epi.red = red();
+    const int p = sizeof(VT) == 4 ? 0 : 1;
+    if (m.path[p] < 0) CFD_TRY(tune<VT>(m));
+    int path = m.path[p];
+    if (path == kPathXs && !(m.xs && ((uintptr_t)x & 15) == 0)) path = kPathRecord;
+    if (path == kPathRecord && !m.all_compressed) path = kPathSplit;
     if constexpr (std::is_same<VT, XT>::value) {
-      if (m.xs && ((uintptr_t)x & 15) == 0) {
+      if (path == kPathXs) {
         CFD_TRY((spmv_xs_launch<VT, OFF, Epi>(m, x, epi)));
         return finish_spmv<VT, XT>(m);
       }
     }
-    if (m.all_compressed)
+    if (path == kPathRecord)
       CFD_TRY((spmv_launch<VT, XT, OFF, Epi, true>(m, x, epi)));
     else
       CFD_TRY((spmv_launch<VT, XT, OFF, Epi, false>(m, x, epi)));
     return finish_spmv<VT, XT>(m);
+  }
+  // Times y = A x on each eligible pipeline (two warm-up and five timed
+  // launches on scratch vectors) and records the fastest in m.path.
+  template <typename VT>
+  cfd_status tune(const DevMat& m) {
+    const int p = sizeof(VT) == 4 ? 0 : 1;
+    if (!m.all_compressed) {
+      m.path[p] = kPathSplit;
+      return CFD_OK;
+    }
+    VT *xs = nullptr, *ys = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const KernelStats keep = ctx->stats;
+    cfd_status st = CFD_OK;
+    float best_ms = 0.0f;
+    int best = kPathSplit;
+    auto fail = [&](cudaError_t e) {
+      set_error("SpMV pipeline timing: %s", cudaGetErrorString(e));
+      st = CFD_ERR_CUDA;
+    };
+    cudaError_t e = cudaMalloc((void**)&xs, (size_t)(m.ncols + 16) * sizeof(VT));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&ys, (size_t)(m.nrows + 16) * sizeof(VT));
+    if (e == cudaSuccess) e = cudaMemsetAsync(xs, 0, (size_t)m.ncols * sizeof(VT), s);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e != cudaSuccess) fail(e);
+    for (int path = kPathSplit; st == CFD_OK && path <= (m.xs ? kPathXs : kPathRecord); ++path) {
+      const EpiStore<VT> epi{ys, nullptr, red()};
+      auto run = [&]() -> cfd_status {
+        if (path == kPathXs) return spmv_xs_launch<VT, false, EpiStore<VT>>(m, xs, epi);
+        if (path == kPathRecord) return spmv_launch<VT, VT, false, EpiStore<VT>, true>(m, xs, epi);
+        return spmv_launch<VT, VT, false, EpiStore<VT>, false>(m, xs, epi);
+      };
+      for (int i = 0; i < 2 && st == CFD_OK; ++i) st = run();
+      if (st == CFD_OK) st = check();
+      if (st != CFD_OK) break;
+      cudaEventRecord(e0, s);
+      for (int i = 0; i < 5 && st == CFD_OK; ++i) st = run();
+      cudaEventRecord(e1, s);
+      if (st == CFD_OK) st = check();
+      e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) {
+        fail(e);
+        break;
+      }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (path == kPathSplit || ms < best_ms) {
+        best_ms = ms;
+        best = path;
+      }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(xs);
+    cudaFree(ys);
+    ctx->stats = keep;
+    if (st != CFD_OK) return st;
+    m.path[p] = (int8_t)best;
+    return check_device_flag(ctx);
   }
   template <typename VT, typename XT>
   cfd_status finish_spmv(const DevMat& m) {

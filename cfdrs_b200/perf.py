@@ -18,12 +18,12 @@ def _events(torch):
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def time_spmv(torch, d, n_rows, n_cols, nnz, fp32, reps, gather=False):
-    """Mean time of one SpMV. gather=True passes x one element into its buffer
-    (not 16-byte aligned), which keeps an x-staged matrix on the gather pipeline."""
+def time_spmv(torch, d, n_rows, n_cols, nnz, fp32, reps, path="auto"):
+    """Mean time of one SpMV on the given pipeline ("auto": the library's choice)."""
     dt = torch.float32 if fp32 else torch.float64
     vs = 4 if fp32 else 8
-    x = torch.rand(n_cols + 1, device="cuda", dtype=dt)[1:] if gather else torch.rand(n_cols, device="cuda", dtype=dt)
+    d.set_path(path, fp32)
+    x = torch.rand(n_cols, device="cuda", dtype=dt)
     y = torch.empty(n_rows, device="cuda", dtype=dt)
     for _ in range(3):
         d.spmv(x.data_ptr(), y.data_ptr(), fp32=fp32)
@@ -38,6 +38,11 @@ def time_spmv(torch, d, n_rows, n_cols, nnz, fp32, reps, gather=False):
     ms = e0.elapsed_time(e1) / reps
     nbytes = nnz * (vs + 4) + 4 * (n_rows + 1) + vs * (n_rows + n_cols)
     return ms, nbytes, x, y
+
+
+def _paths(d):
+    lay = d.layout()
+    return ["split"] + (["record"] if lay["all_compressed"] else []) + (["x_staged"] if lay["x_staged"] else [])
 
 
 def main(argv=None):
@@ -63,11 +68,9 @@ def main(argv=None):
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
     if a.case == "spmv":
         d = DeviceCsr(A, ctx)
-        staged = d.layout()["x_staged"]
         for fp32 in (True, False):
-            for gather in ((False, True) if staged else (False,)):
-                ms, nb, x, y = time_spmv(torch, d, A.nrows, A.ncols, A.nnz, fp32, a.reps, gather)
-                path = "x-staged" if staged and not gather else "gather"
+            for path in _paths(d):
+                ms, nb, x, y = time_spmv(torch, d, A.nrows, A.ncols, A.nnz, fp32, a.reps, path)
                 print(f"{a.n}^3 {'f32' if fp32 else 'f64'} {path}: {ms * 1e3:.1f} us {nb / ms / 1e6:.0f} GB/s",
                       flush=True)
         return 0
@@ -80,11 +83,9 @@ def main(argv=None):
                     continue
                 m = amg.level(l, which)
                 d = DeviceCsr(m, ctx)
-                staged = d.layout()["x_staged"]
                 for fp32 in (True, False):
-                    for gather in ((False, True) if staged else (False,)):
-                        ms, nb, _, _ = time_spmv(torch, d, m.nrows, m.ncols, m.nnz, fp32, a.reps, gather)
-                        path = "x-staged" if staged and not gather else "gather"
+                    for path in _paths(d):
+                        ms, nb, _, _ = time_spmv(torch, d, m.nrows, m.ncols, m.nnz, fp32, a.reps, path)
                         print(f"L{l} {name} {m.nrows}x{m.ncols} nnz={m.nnz} ({m.nnz / max(m.nrows, 1):.1f}/row) "
                               f"{'f32' if fp32 else 'f64'} {path:8s}: {ms * 1e3:8.1f} us {nb / ms / 1e6:6.0f} GB/s",
                               flush=True)

@@ -108,30 +108,43 @@ def test_spmv_vs_oracle(cuda, oracle, shape):
 
 
 @pytest.mark.parametrize("shape", ["stencil", "stencil_tail", "empty_blocks", "narrow", "prolongation",
-                                   "restriction"])
-def test_x_staged_equals_gather_path(cuda, shape):
-    """The x-staged kernel (x 16-byte aligned) and the gather kernel (the same x
-    one element into a buffer, so not 16-byte aligned) sum every row in the same
-    order: FP64 and FP32 results are bit-identical."""
+                                   "restriction", "coarse_operator", "mixed"])
+def test_spmv_pipelines_bit_identical(cuda, shape):
+    """Every SpMV pipeline a matrix is eligible for (split, record, x-staged)
+    sums each row in the same order: FP64 and FP32 results are bit-identical,
+    and an x-staged request with an x that is not 16-byte aligned runs on the
+    record pipeline with the same result."""
     from cfdrs_b200.device import DeviceCsr
     A, staged = spmv_case(shape)
-    assert staged
     d = DeviceCsr(A)
-    assert d.layout()["x_staged"] == 1
+    lay = d.layout()
+    if staged:
+        assert lay["x_staged"] == 1
+    paths = ["split"] + (["record"] if lay["all_compressed"] else []) + (["x_staged"] if lay["x_staged"] else [])
     x = np.random.default_rng(5).uniform(-1, 1, A.ncols)
     for dt in (cuda.float64, cuda.float32):
+        fp32 = dt == cuda.float32
         xa = dev(cuda, x, dt)
         buf = cuda.zeros(A.ncols + 1, device="cuda", dtype=dt)
         buf[1:] = xa
-        ya = cuda.zeros(A.nrows, device="cuda", dtype=dt)
-        yb = cuda.full((A.nrows,), float("nan"), device="cuda", dtype=dt)
-        fp32 = dt == cuda.float32
-        d.spmv(xa.data_ptr(), ya.data_ptr(), fp32=fp32)
-        d.spmv(buf[1:].data_ptr(), yb.data_ptr(), fp32=fp32)
-        cuda.cuda.synchronize()
         assert buf[1:].data_ptr() % 16 != 0
-        assert cuda.equal(ya, yb), f"{shape} {dt}"
-
+        ys = []
+        for path in paths:
+            d.set_path(path, fp32)
+            for xp in ((xa, buf[1:]) if path == "x_staged" else (xa,)):
+                y = cuda.full((A.nrows,), float("nan"), device="cuda", dtype=dt)
+                d.spmv(xp.data_ptr(), y.data_ptr(), fp32=fp32)
+                ys.append((path, y))
+        cuda.cuda.synchronize()
+        for path, y in ys[1:]:
+            assert cuda.equal(ys[0][1], y), f"{shape} {dt} {path}"
+        d.set_path("auto", fp32)
+        y = cuda.zeros(A.nrows, device="cuda", dtype=dt)
+        d.spmv(xa.data_ptr(), y.data_ptr(), fp32=fp32)  # times the pipelines, keeps the fastest
+        cuda.cuda.synchronize()
+        assert cuda.equal(ys[0][1], y)
+        assert d.layout()["path_f32" if fp32 else "path_f64"] in [{"split": 0, "record": 1, "x_staged": 2}[p]
+                                                                   for p in paths]
 
 @pytest.mark.parametrize("interp,order", [(0, 0), (2, 0), (2, 1)])
 def test_amg_hierarchy_matches_oracle(cuda, oracle, interp, order):
