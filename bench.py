@@ -318,6 +318,9 @@ def main():
         bytes_ = nnz * (vs + 4) + 4 * (N + 1) + 2 * N * vs
         spmv[label] = {"ms": t, "bytes": bytes_, "gbs": bytes_ / t / 1e6}
     ctx.set_stream(None)
+    names = {0: "split", 1: "record", 2: "x_staged", -1: "unset"}
+    lay = dA.layout()
+    spmv_path = {"f32": names[lay["path_f32"]], "f64": names[lay["path_f64"]]}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -335,8 +338,10 @@ def main():
             "gpu_launches": int(launches * args.steps),
             "roofline": {"bound": "hbm", "achieved": f32["gbs"], "peak": peak, "unit": "GB/s",
                          "frac": f32["gbs"] / peak, "traffic": traffic,
-                         "kernel": "k_spmv FP32 fine operator (256^3, 117M nnz), timed alone",
+                         "kernel": f"SpMV FP32 fine operator (256^3, 117M nnz, {spmv_path['f32']} pipeline), "
+                                   "timed alone; achieved counts CSR bytes (8-byte value+index per nonzero)",
                          "peak_kind": peak_kind},
+            "spmv_path": spmv_path,
             "spmv_gbs": {"f32": f32["gbs"], "f64": spmv["f64"]["gbs"],
                          "frac_f32": f32["gbs"] / peak, "frac_f64": spmv["f64"]["gbs"] / peak},
             "fp64_pcg_ms": min(fp64_ms), "speedup_vs_fp64_pcg": min(fp64_ms) / ms,
