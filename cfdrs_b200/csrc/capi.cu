@@ -568,7 +568,7 @@ cfd_status cfd_csr_set_path(cfd_csr* a, int32_t fp32, int32_t path) {
     return CFD_ERR_STATE;
   }
   const DevMat& m = a->dev;
-  const bool ok = path == CFD_PATH_AUTO || path == CFD_PATH_SPLIT ||
+  const bool ok = path == CFD_PATH_AUTO || path == CFD_PATH_TIMED || path == CFD_PATH_SPLIT ||
                   (path == CFD_PATH_RECORD && m.all_compressed) || (path == CFD_PATH_X_STAGED && m.xs);
   if (!ok) {
     set_error("SpMV pipeline %d not available for this matrix (all blocks coded: %d, x staged: %d)", path,

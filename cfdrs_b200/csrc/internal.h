@@ -108,8 +108,8 @@ struct DevMat {
   // per block {windows | tail << 16, zero-offset code or -1, record offset / 16, entries copied}
   int4* xdesc = nullptr;
   bool xs = false;
-  // SpMV pipeline per precision ([0] FP32, [1] FP64), chosen by timing the
-  // eligible ones at the first use (-1: not chosen yet); see Launcher::tune.
+  // SpMV pipeline per precision ([0] FP32, [1] FP64): a cfd_spmv_path value;
+  // CFD_PATH_TIMED is replaced by the fastest after timing (Launcher::tune).
   mutable int8_t path[2] = {-1, -1};
   int nblk = 0;
   int tpr = 1;         // threads cooperating on one row (power of two, <= 32)

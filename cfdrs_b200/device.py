@@ -96,10 +96,11 @@ class DeviceCsr:
         _lib.check(_lib.load().cfd_csr_layout(self.h, C.byref(info)))
         return {f: getattr(info, f) for f, _ in info._fields_}
 
-    PATHS = {"auto": -1, "split": 0, "record": 1, "x_staged": 2}
+    PATHS = {"timed": -2, "auto": -1, "split": 0, "record": 1, "x_staged": 2}
 
     def set_path(self, path: str, fp32: bool) -> None:
-        """Pin the SpMV pipeline of one precision ("auto" re-times them)."""
+        """Set the SpMV pipeline of one precision: "auto" (the default rule),
+        "timed" (time the eligible pipelines at the next SpMV), or a pipeline."""
         _lib.check(_lib.load().cfd_csr_set_path(self.h, 1 if fp32 else 0, self.PATHS[path]))
 
     def spmv(self, x_dev_ptr: int, y_dev_ptr: int, fp32: bool = False) -> None:

@@ -103,18 +103,26 @@ typedef struct {
   int32_t threads_per_row;
   int32_t max_windows;       /* cfd_layout_check only */
   int64_t staged_x_entries;  /* cfd_layout_check only: x entries staged over all blocks */
-  int32_t path_f32;          /* SpMV pipeline in use per precision (cfd_spmv_path), -1 = not chosen yet */
+  int32_t path_f32;          /* SpMV pipeline setting per precision (cfd_spmv_path) */
   int32_t path_f64;
 } cfd_layout_info;
 cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out);
 /* SpMV pipelines. All sum every row in the same order, so they give identical
- * results; the library times the eligible ones at a matrix's first SpMV in each
- * precision and keeps the fastest. SPLIT takes any matrix, RECORD needs every
- * block coded, X_STAGED needs x staging and a 16-byte aligned x (otherwise it
- * runs as RECORD). */
-typedef enum { CFD_PATH_AUTO = -1, CFD_PATH_SPLIT = 0, CFD_PATH_RECORD = 1, CFD_PATH_X_STAGED = 2 } cfd_spmv_path;
-/* Pin (or with CFD_PATH_AUTO re-time) the pipeline of one precision (fp32 != 0:
- * FP32 values). CFD_ERR_CONFIG when the matrix is not eligible for it. */
+ * results. SPLIT takes any matrix, RECORD needs every block coded (otherwise it
+ * runs as SPLIT), X_STAGED needs x staging and a 16-byte aligned x (otherwise
+ * it runs as RECORD). AUTO (the default): RECORD for FP32, X_STAGED for FP64
+ * when eligible with one thread per row. TIMED: at the next SpMV in that
+ * precision, time the eligible pipelines (allocates scratch vectors) and keep
+ * the fastest. */
+typedef enum {
+  CFD_PATH_TIMED = -2,
+  CFD_PATH_AUTO = -1,
+  CFD_PATH_SPLIT = 0,
+  CFD_PATH_RECORD = 1,
+  CFD_PATH_X_STAGED = 2
+} cfd_spmv_path;
+/* Set the pipeline of one precision (fp32 != 0: FP32 values). CFD_ERR_CONFIG
+ * when the matrix is not eligible for it. */
 cfd_status cfd_csr_set_path(cfd_csr* a, int32_t fp32, int32_t path);
 /* Host only, no GPU: builds the layout of a CSR matrix and evaluates y = A x by
  * walking the device kernels' index arithmetic (staged x image, index record,

@@ -138,13 +138,17 @@ def test_spmv_pipelines_bit_identical(cuda, shape):
         cuda.cuda.synchronize()
         for path, y in ys[1:]:
             assert cuda.equal(ys[0][1], y), f"{shape} {dt} {path}"
-        d.set_path("auto", fp32)
-        y = cuda.zeros(A.nrows, device="cuda", dtype=dt)
-        d.spmv(xa.data_ptr(), y.data_ptr(), fp32=fp32)  # times the pipelines, keeps the fastest
-        cuda.cuda.synchronize()
-        assert cuda.equal(ys[0][1], y)
-        assert d.layout()["path_f32" if fp32 else "path_f64"] in [{"split": 0, "record": 1, "x_staged": 2}[p]
-                                                                   for p in paths]
+        for mode in ("timed", "auto"):
+            d.set_path(mode, fp32)
+            y = cuda.zeros(A.nrows, device="cuda", dtype=dt)
+            d.spmv(xa.data_ptr(), y.data_ptr(), fp32=fp32)  # "timed" keeps the fastest pipeline
+            cuda.cuda.synchronize()
+            assert cuda.equal(ys[0][1], y), f"{shape} {dt} {mode}"
+            chosen = d.layout()["path_f32" if fp32 else "path_f64"]
+            if mode == "timed":
+                assert chosen in [{"split": 0, "record": 1, "x_staged": 2}[p] for p in paths]
+            else:
+                assert chosen == -1
 
 @pytest.mark.parametrize("interp,order", [(0, 0), (2, 0), (2, 1)])
 def test_amg_hierarchy_matches_oracle(cuda, oracle, interp, order):
