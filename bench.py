@@ -318,7 +318,7 @@ def main():
         bytes_ = nnz * (vs + 4) + 4 * (N + 1) + 2 * N * vs
         spmv[label] = {"ms": t, "bytes": bytes_, "gbs": bytes_ / t / 1e6}
     ctx.set_stream(None)
-    names = {0: "split", 1: "record", 2: "x_staged", -1: "unset"}
+    names = {0: "split", 1: "record", 2: "x_staged", -2: "timed"}
     lay = dA.layout()
     spmv_path = {"f32": names[lay["path_f32"]], "f64": names[lay["path_f64"]]}
 

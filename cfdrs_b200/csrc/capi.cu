@@ -557,8 +557,8 @@ cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out) {
   out->all_compressed = m.all_compressed ? 1 : 0;
   out->x_staged = m.xs ? 1 : 0;
   out->threads_per_row = m.tpr;
-  out->path_f32 = m.path[0];
-  out->path_f64 = m.path[1];
+  out->path_f32 = spmv_path(m, 0);
+  out->path_f64 = spmv_path(m, 1);
   return CFD_OK;
 }
 

@@ -115,6 +115,20 @@ struct DevMat {
   int tpr = 1;         // threads cooperating on one row (power of two, <= 32)
 };
 
+// SpMV pipeline that an SpMV of precision p ([0] FP32, [1] FP64) runs: the
+// setting, with CFD_PATH_AUTO resolved to RECORD for FP32 and X_STAGED for
+// FP64 one-thread rows (SPLIT for other FP64 matrices), as measured fastest on
+// the 256^3 AMG hierarchy, and ineligible pipelines stepped down. CFD_PATH_TIMED
+// is returned as is (the launcher times the pipelines first).
+inline int spmv_path(const DevMat& m, int p) {
+  int path = m.path[p];
+  if (path == CFD_PATH_TIMED) return path;
+  if (path == CFD_PATH_AUTO) path = p == 0 ? CFD_PATH_RECORD : (m.xs && m.tpr == 1 ? CFD_PATH_X_STAGED : CFD_PATH_SPLIT);
+  if (path == CFD_PATH_X_STAGED && !m.xs) path = CFD_PATH_RECORD;
+  if (path == CFD_PATH_RECORD && !m.all_compressed) path = CFD_PATH_SPLIT;
+  return path;
+}
+
 // Host image of DevMat's compression and x-staging arrays (layout.cpp).
 struct HostLayout {
   uint64_t base_mult = 1u << 20;

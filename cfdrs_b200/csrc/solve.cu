@@ -354,21 +354,19 @@ struct Launcher {
   // columns or codes, row offsets and dictionary copied separately; any
   // matrix), the record one (values plus one block record; fully coded
   // matrices) or the x-staged one (x windows staged with the block). All three
-  // sum each row in the same order, so the choice changes speed only. By
-  // default (CFD_PATH_AUTO) FP32 takes the record pipeline, whose x gathers
-  // hit L2, and FP64 the x-staged one for one-thread rows, whose x no longer
-  // fits L2 at large sizes; CFD_PATH_TIMED times the eligible ones once.
-  static constexpr int kPathTimed = -2, kPathAuto = -1, kPathSplit = 0, kPathRecord = 1, kPathXs = 2;
+  // sum each row in the same order, so the choice changes speed only
+  // (spmv_path: by default FP32 takes the record pipeline, whose x gathers hit
+  // L2, and FP64 the x-staged one for one-thread rows, whose x no longer fits
+  // L2 at large sizes; CFD_PATH_TIMED times the eligible ones once).
+  static constexpr int kPathTimed = -2, kPathSplit = 0, kPathRecord = 1, kPathXs = 2;
   template <typename VT, typename XT, bool OFF, class Epi>
   cfd_status spmv(const DevMat& m, const XT* x, Epi epi) {
     if (m.nrows == 0) return CFD_OK;
     epi.red = red();
     const int p = sizeof(VT) == 4 ? 0 : 1;
     if (m.path[p] == kPathTimed) CFD_TRY(tune<VT>(m));
-    int path = m.path[p];
-    if (path == kPathAuto) path = (sizeof(VT) == 8 && m.xs && m.tpr == 1) ? kPathXs : kPathRecord;
-    if (path == kPathXs && !(m.xs && ((uintptr_t)x & 15) == 0)) path = kPathRecord;
-    if (path == kPathRecord && !m.all_compressed) path = kPathSplit;
+    int path = spmv_path(m, p);
+    if (path == kPathXs && ((uintptr_t)x & 15) != 0) path = m.all_compressed ? kPathRecord : kPathSplit;
     if constexpr (std::is_same<VT, XT>::value) {
       if (path == kPathXs) {
         CFD_TRY((spmv_xs_launch<VT, OFF, Epi>(m, x, epi)));

@@ -103,15 +103,15 @@ typedef struct {
   int32_t threads_per_row;
   int32_t max_windows;       /* cfd_layout_check only */
   int64_t staged_x_entries;  /* cfd_layout_check only: x entries staged over all blocks */
-  int32_t path_f32;          /* SpMV pipeline setting per precision (cfd_spmv_path) */
+  int32_t path_f32;          /* SpMV pipeline an SpMV runs per precision (cfd_spmv_path; TIMED until timed) */
   int32_t path_f64;
 } cfd_layout_info;
 cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out);
 /* SpMV pipelines. All sum every row in the same order, so they give identical
  * results. SPLIT takes any matrix, RECORD needs every block coded (otherwise it
  * runs as SPLIT), X_STAGED needs x staging and a 16-byte aligned x (otherwise
- * it runs as RECORD). AUTO (the default): RECORD for FP32, X_STAGED for FP64
- * when eligible with one thread per row. TIMED: at the next SpMV in that
+ * it runs as RECORD). AUTO (the default): RECORD for FP32; X_STAGED for FP64
+ * when eligible with one thread per row, SPLIT otherwise. TIMED: at the next SpMV in that
  * precision, time the eligible pipelines (allocates scratch vectors) and keep
  * the fastest. */
 typedef enum {

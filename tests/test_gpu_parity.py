@@ -145,10 +145,9 @@ def test_spmv_pipelines_bit_identical(cuda, shape):
             cuda.cuda.synchronize()
             assert cuda.equal(ys[0][1], y), f"{shape} {dt} {mode}"
             chosen = d.layout()["path_f32" if fp32 else "path_f64"]
-            if mode == "timed":
-                assert chosen in [{"split": 0, "record": 1, "x_staged": 2}[p] for p in paths]
-            else:
-                assert chosen == -1
+            assert chosen in [{"split": 0, "record": 1, "x_staged": 2}[p] for p in paths]
+            if mode == "auto" and fp32:
+                assert chosen == (1 if lay["all_compressed"] else 0)
 
 @pytest.mark.parametrize("interp,order", [(0, 0), (2, 0), (2, 1)])
 def test_amg_hierarchy_matches_oracle(cuda, oracle, interp, order):
