@@ -715,6 +715,25 @@ cfd_status cfd_amg_apply(cfd_amg* amg, const double* r, double* z) {
   return check_device_flag(amg->ctx);
 }
 
+cfd_status cfd_amg_set_path(cfd_amg* amg, int32_t fp32, int32_t path) {
+  if (!amg) {
+    set_error("cfd_amg_set_path: null handle");
+    return CFD_ERR_STATE;
+  }
+  if (path < CFD_PATH_TIMED || path > CFD_PATH_X_STAGED) {
+    set_error("cfd_amg_set_path: unknown pipeline %d", path);
+    return CFD_ERR_CONFIG;
+  }
+  std::lock_guard<std::mutex> g(amg->ctx->mu);
+  for (DevLevel& L : amg->dev)
+    for (DevMat* m : {&L.A, &L.P, &L.R}) {
+      int q = path;  // an ineligible request keeps the default rule for that operator
+      if ((q == CFD_PATH_RECORD && !m->all_compressed) || (q == CFD_PATH_X_STAGED && !m->xs)) q = CFD_PATH_AUTO;
+      m->path[fp32 ? 0 : 1] = (int8_t)q;
+    }
+  return CFD_OK;
+}
+
 cfd_status cfd_amg_stats(const cfd_amg* amg, cfd_amg_stats_t* out) {
   if (!amg || !out) return CFD_ERR_STATE;
   std::memset(out, 0, sizeof(*out));

@@ -129,6 +129,12 @@ class AlgebraicMultigrid:
             return z
         return res
 
+    def set_path(self, path: str, fp32: bool) -> None:
+        """SpMV pipeline of every level operator in one precision ("auto",
+        "timed", "split", "record", "x_staged"); see DeviceCsr.set_path."""
+        from .device import DeviceCsr
+        _lib.check(_lib.load().cfd_amg_set_path(self.h, 1 if fp32 else 0, DeviceCsr.PATHS[path]))
+
     def statistics(self) -> AMGStatistics:
         s = _lib.AmgStatsC()
         _lib.check(_lib.load().cfd_amg_stats(self.h, C.byref(s)))

@@ -190,6 +190,10 @@ cfd_status cfd_amg_recompute(cfd_amg* amg, cfd_csr* a);
 /* z = M^-1 r (one V-cycle from z = 0), device pointers, FP64. */
 cfd_status cfd_amg_apply(cfd_amg* amg, const double* r_dev, double* z_dev);
 cfd_status cfd_amg_stats(const cfd_amg* amg, cfd_amg_stats_t* out);
+/* SpMV pipeline of every level operator (A, P, R) in one precision, as
+ * cfd_csr_set_path; an operator not eligible for the pipeline keeps AUTO.
+ * No reference counterpart (CFDrs has one CSR SpMV). */
+cfd_status cfd_amg_set_path(cfd_amg* amg, int32_t fp32, int32_t path);
 /* Copy level `level`'s operator (which: 0 = A_l, 1 = P_l, 2 = R_l) to host
  * arrays; pass NULL arrays to query sizes only. */
 cfd_status cfd_amg_level(const cfd_amg* amg, int level, int which, int64_t* nrows, int64_t* ncols,

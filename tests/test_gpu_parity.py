@@ -372,3 +372,35 @@ def test_recompute_matches_fresh_setup(cuda):
     np.testing.assert_array_equal(amg.level(0, 1).val, fresh_P.level(0, 1).val)
     np.testing.assert_allclose(amg.level(0, 0).val, A2.val)
     assert np.all(np.isfinite(z))
+
+
+def test_solve_identical_on_every_pipeline(cuda):
+    """The AMG-PCG solve (FP64 and FP32 + refinement) gives bit-identical
+    iterates whichever SpMV pipeline the operators run."""
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.device import device_matrix
+    A, b, _ = P.poisson_3d_variable(24, 8.0, 1.0, seed=1)
+    cfg = cf.AMGConfig.pressure_poisson()
+    cfg.min_coarse_size = 200
+    amg = cf.AlgebraicMultigrid(A, cfg)
+    dA = device_matrix(A)
+    bd = dev(cuda, b)
+    conf = cf.IterativeSolverConfig(0.0, 1e-10, 500)
+    for prec in (cf.Precision.FP64, cf.Precision.FP32_REFINE):
+        fp32 = prec == cf.Precision.FP32_REFINE
+        xs = []
+        for path in ("auto", "split", "record", "x_staged", "timed"):
+            amg.set_path(path, fp32)
+            try:
+                dA.set_path(path, fp32)
+            except Exception:
+                dA.set_path("auto", fp32)
+            x = cuda.zeros_like(bd)
+            rep = cf.cg_preconditioned(A, bd, amg, x, conf, precision=prec)
+            assert rep.termination == cf.Termination.CONVERGED
+            xs.append(x)
+        amg.set_path("auto", fp32)
+        dA.set_path("auto", fp32)
+        for x in xs[1:]:
+            assert cuda.equal(xs[0], x), prec
