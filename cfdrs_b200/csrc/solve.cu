@@ -354,7 +354,9 @@ struct Launcher {
   // columns or codes, row offsets and dictionary copied separately; any
   // matrix), the record one (values plus one block record; fully coded
   // matrices) or the x-staged one (x windows staged with the block). All three
-  // sum each row in the same order, so the choice changes speed only
+  // sum each row in the same order (fused dot products add per-CTA partials
+  // over each pipeline's own grid), so the choice changes speed, not the row
+  // results
   // (spmv_path: by default FP32 takes the record pipeline, whose x gathers hit
   // L2, and FP64 the x-staged one for one-thread rows, whose x no longer fits
   // L2 at large sizes; CFD_PATH_TIMED times the eligible ones once).

@@ -107,8 +107,10 @@ typedef struct {
   int32_t path_f64;
 } cfd_layout_info;
 cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out);
-/* SpMV pipelines. All sum every row in the same order, so they give identical
- * results. SPLIT takes any matrix, RECORD needs every block coded (otherwise it
+/* SpMV pipelines. All sum every row in the same order, so y = A x is identical
+ * on each; dot products fused into solver SpMVs add per-CTA partials over each
+ * pipeline's own grid (deterministic for a pipeline, equal to rounding across
+ * pipelines). SPLIT takes any matrix, RECORD needs every block coded (otherwise it
  * runs as SPLIT), X_STAGED needs x staging and a 16-byte aligned x (otherwise
  * it runs as RECORD). AUTO (the default): RECORD for FP32; X_STAGED for FP64
  * when eligible with one thread per row, SPLIT otherwise. TIMED: at the next SpMV in that

@@ -374,9 +374,11 @@ def test_recompute_matches_fresh_setup(cuda):
     assert np.all(np.isfinite(z))
 
 
-def test_solve_identical_on_every_pipeline(cuda):
-    """The AMG-PCG solve (FP64 and FP32 + refinement) gives bit-identical
-    iterates whichever SpMV pipeline the operators run."""
+def test_solve_on_every_pipeline(cuda):
+    """The AMG-PCG solve (FP64 and FP32 + refinement) converges to the same
+    solution whichever SpMV pipeline the operators run. Row products are
+    identical; the fused dot products sum their per-CTA partials over each
+    pipeline's own grid, so iterates agree to rounding, not bit for bit."""
     import cfdrs_b200 as cf
     from cfdrs_b200 import problems as P
     from cfdrs_b200.device import device_matrix
@@ -399,8 +401,10 @@ def test_solve_identical_on_every_pipeline(cuda):
             x = cuda.zeros_like(bd)
             rep = cf.cg_preconditioned(A, bd, amg, x, conf, precision=prec)
             assert rep.termination == cf.Termination.CONVERGED
-            xs.append(x)
+            xs.append((x.cpu().numpy(), rep.iterations))
         amg.set_path("auto", fp32)
         dA.set_path("auto", fp32)
-        for x in xs[1:]:
-            assert cuda.equal(xs[0], x), prec
+        x0, it0 = xs[0]
+        for x, it in xs[1:]:
+            assert abs(it - it0) <= 1, prec
+            assert rel(x, x0) < 1e-8, prec
