@@ -484,11 +484,15 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 
 // Stage layout. CODES: every staged block is dictionary-coded and arrives as
 // values plus its BlockRecord (two bulk copies), so the column region holds
-// the record and the ring gets deeper; otherwise values, columns (int32 or
-// codes), row offsets and dictionary arrive separately.
+// the record; otherwise values, columns (int32 or codes), row offsets and
+// dictionary arrive separately.
 template <typename VT, bool CODES>
 struct PipeLayout {
-  static constexpr int kStages = (CODES && sizeof(VT) == 4) ? 3 : 2;
+  // FP32 record stages are small enough for four CTAs per SM with two stages
+  // each: 36 warps per SM hide the x-gather latency better than a deeper ring
+  // (256^3 fine operator: 178 us at 2 stages x 4 CTAs, 215 us at 3 x 3).
+  static constexpr int kStages = 2;
+  static constexpr int kMinBlocks = (CODES && sizeof(VT) == 4) ? 4 : 2;
   static constexpr int kValSlack = 16 / (int)sizeof(VT);
   static constexpr int kValBytes = ((kNnzCap + 2 * kValSlack) * (int)sizeof(VT) + 127) / 128 * 128;
   static constexpr int kColBytes = CODES ? (kRecordCap + 127) / 128 * 128 : ((kNnzCap + 8) * 4 + 127) / 128 * 128;
@@ -499,7 +503,7 @@ struct PipeLayout {
 };
 
 template <typename VT, typename XT, bool OFFDIAG, class Epi, bool CODES>
-__global__ void __launch_bounds__(kPipeThreads, 2) k_spmv_pipe(MatView<VT> A, int nblk, const XT* __restrict__ x,
+__global__ void __launch_bounds__(kPipeThreads, PipeLayout<VT, CODES>::kMinBlocks) k_spmv_pipe(MatView<VT> A, int nblk, const XT* __restrict__ x,
                                                                 Epi epi, int* err) {
   if (epi.skip()) return;
   using L = PipeLayout<VT, CODES>;
