@@ -1008,6 +1008,138 @@ int or_pcg_equilibrated(const or_csr* a, const double* b, double* x, const or_so
 }
 
 // Right-preconditioned BiCGSTAB (Saad 2003, Alg. 7.7 with M^-1 applied to p and s).
+// GMRES restart ladder, RestartWidth::covering (krylov.rs:96-120): the
+// smallest of 8, 16, 32, 64, 128, 256 at least as large as the request,
+// saturating at 256.
+int or_gmres_width(int64_t requested) {
+  int w = 8;
+  while (w < 256 && w < requested) w *= 2;
+  return w;
+}
+
+// Restarted GMRES(m) with right preconditioning, the solver behind
+// krylov::gmres_preconditioned (krylov.rs:150-221; the recurrence lives in
+// athena-core, not vendored, so it is restated from Saad 2003, Alg. 9.5):
+//   cycle: beta = ||r||, v0 = r / beta; for j < m: w = A M^-1 v_j, classical
+//   Gram-Schmidt against v_0..v_j applied twice (CGS2), h_{j+1,j} = ||w||,
+//   Givens rotations on the Hessenberg column, implicit residual |g_{j+1}|;
+//   the cycle ends at the threshold, at the budget or when h_{j+1,j} = 0;
+//   then x += M^-1 (V y) with H y = g, and the true residual b - A x decides:
+//   converged, budget spent, or restart.
+// iterations counts Arnoldi steps over all cycles; history[k] is the implicit
+// residual after step k (history[0] = ||r0||).
+int or_gmres(const or_csr* a, int precond, const or_amg* amg, int64_t restart, const double* b, double* x,
+             const or_solver_config* cfg, or_report* rep, double* history) {
+  const int64_t n = a->nrows;
+  if (a->ncols != n) return -1;
+  Precond M{precond, amg, {}};
+  if (precond == OR_PRE_JACOBI && jacobi_inverse(*a, M.inv) != 0) return -2;
+  const int m = or_gmres_width(restart);
+  std::vector<double> V((size_t)(m + 1) * n), w(n), z(n), r(n), t(n);
+  std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), y(m), h1(m + 1), h2(m + 1);
+  auto vec = [&](int k) { return V.data() + (size_t)k * n; };
+  auto residual = [&]() {
+    spmv_raw(*a, x, t.data());
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) r[i] = b[i] - t[i];
+    return std::sqrt(dot(n, r.data(), r.data()));
+  };
+  // h = V[0..k)^T w (one dot per basis vector)
+  auto project = [&](int k, std::vector<double>& h) {
+    for (int q = 0; q < k; ++q) h[q] = dot(n, vec(q), w.data());
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (int q = 0; q < k; ++q) s += h[q] * vec(q)[i];
+      w[i] -= s;
+    }
+  };
+  double rn = residual();
+  rep->initial_residual = rn;
+  rep->threshold = std::max(cfg->tolerance, cfg->relative_tolerance * rn);
+  rep->final_residual = rn;
+  rep->iterations = 0;
+  if (history) history[0] = rn;
+  if (rn <= rep->threshold) {
+    rep->termination = OR_TERM_INITIAL_RESIDUAL;
+    return 0;
+  }
+  int64_t it = 0;
+  for (;;) {
+    const double beta = rn;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) vec(0)[i] = r[i] / beta;
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int cols = 0;
+    for (int j = 0; j < m; ++j) {
+      M.apply(vec(j), z.data(), n);
+      spmv_raw(*a, z.data(), w.data());
+      project(j + 1, h1);
+      project(j + 1, h2);
+      double* h = H.data() + (size_t)j * (m + 1);
+      for (int q = 0; q <= j; ++q) h[q] = h1[q] + h2[q];
+      const double hn = std::sqrt(dot(n, w.data(), w.data()));
+      h[j + 1] = hn;
+      if (hn > 0.0) {
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < n; ++i) vec(j + 1)[i] = w[i] / hn;
+      }
+      for (int q = 0; q < j; ++q) {
+        const double tq = cs[q] * h[q] + sn[q] * h[q + 1];
+        h[q + 1] = -sn[q] * h[q] + cs[q] * h[q + 1];
+        h[q] = tq;
+      }
+      const double d = std::hypot(h[j], h[j + 1]);
+      cs[j] = d > 0.0 ? h[j] / d : 1.0;
+      sn[j] = d > 0.0 ? h[j + 1] / d : 0.0;
+      h[j] = d;
+      h[j + 1] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      ++it;
+      cols = j + 1;
+      const double res = std::fabs(g[j + 1]);
+      rep->iterations = it;
+      if (history) history[it] = res;
+      if (!std::isfinite(res)) {
+        rep->termination = OR_TERM_BREAKDOWN;
+        return 0;
+      }
+      if (res <= rep->threshold || it >= cfg->max_iterations || hn == 0.0) break;
+    }
+    // y = H^-1 g (upper triangular), x += M^-1 (V y)
+    for (int q = cols - 1; q >= 0; --q) {
+      double s = g[q];
+      for (int l = q + 1; l < cols; ++l) s -= H[(size_t)l * (m + 1) + q] * y[l];
+      y[q] = H[(size_t)q * (m + 1) + q] != 0.0 ? s / H[(size_t)q * (m + 1) + q] : 0.0;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (int q = 0; q < cols; ++q) s += y[q] * vec(q)[i];
+      w[i] = s;
+    }
+    M.apply(w.data(), z.data(), n);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) x[i] += z[i];
+    rn = residual();
+    rep->final_residual = rn;
+    if (!std::isfinite(rn)) {
+      rep->termination = OR_TERM_BREAKDOWN;
+      return 0;
+    }
+    if (rn <= rep->threshold) {
+      rep->termination = OR_TERM_CONVERGED;
+      return 0;
+    }
+    if (it >= cfg->max_iterations) {
+      rep->termination = OR_TERM_MAX_ITERATIONS;
+      return 0;
+    }
+  }
+}
+
 int or_bicgstab(const or_csr* a, int precond, const or_amg* amg, const double* b, double* x,
                 const or_solver_config* cfg, or_report* rep, double* history) {
   const int64_t n = a->nrows;

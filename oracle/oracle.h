@@ -125,6 +125,11 @@ int or_pcg_equilibrated(const or_csr* a, const double* b, double* x, const or_so
                         or_report* rep);
 int or_bicgstab(const or_csr* a, int precond, const or_amg* amg, const double* b, double* x,
                 const or_solver_config* cfg, or_report* rep, double* history);
+/* Restart width actually used for a requested restart (the ladder of krylov.rs:96-120). */
+int or_gmres_width(int64_t requested);
+/* Restarted right-preconditioned GMRES(m); history[k] = implicit residual after k steps. */
+int or_gmres(const or_csr* a, int precond, const or_amg* amg, int64_t restart, const double* b, double* x,
+             const or_solver_config* cfg, or_report* rep, double* history);
 
 #ifdef __cplusplus
 }

@@ -98,6 +98,10 @@ def lib():
         for fn in (L.or_pcg, L.or_bicgstab):
             fn.restype = C.c_int
             fn.argtypes = [P, C.c_int, P, P, P, P, P, P]
+        L.or_gmres.restype = C.c_int
+        L.or_gmres.argtypes = [P, C.c_int, P, C.c_int64, P, P, P, P, P]
+        L.or_gmres_width.restype = C.c_int
+        L.or_gmres_width.argtypes = [C.c_int64]
         _lib = L
     return _lib
 
@@ -302,6 +306,19 @@ def pcg(a, b, **kw):
 
 def bicgstab(a, b, **kw):
     return _krylov(lib().or_bicgstab, a, b, **kw)
+
+
+def gmres(a: Csr, b, restart=30, **kw):
+    """Restarted right-preconditioned GMRES(m), m from the restart ladder."""
+    fn = lib().or_gmres
+
+    def call(h, pre, amg, bp, xp, cfg, rep, hist):
+        return fn(h, pre, amg, restart, bp, xp, cfg, rep, hist)
+    return _krylov(call, a, b, **kw)
+
+
+def gmres_width(requested: int) -> int:
+    return lib().or_gmres_width(requested)
 
 
 def pcg_equilibrated(a: Csr, b, x0=None, tol=0.0, rtol=1e-10, max_it=20000):

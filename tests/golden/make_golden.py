@@ -80,6 +80,70 @@ GOLDEN = {
         "contraction_steps": 5,
         "contraction_bound": 1.0,
     },
+    "gmres_restart_ladder": {
+        "source": "crates/cfd-math/src/linear_solver/krylov.rs:440-463 (RestartWidth::covering, :96-120)",
+        "requested_width": [[1, 8], [8, 8], [9, 16], [30, 32], [100, 128], [200, 256], [10000, 256]],
+    },
+    "gmres_diagonal_2": {
+        "source": "crates/cfd-math/src/linear_solver/krylov.rs:466-492 (workspace reused for two solves)",
+        "row_ptr": [0, 1, 2],
+        "col": [0, 1],
+        "val": [2.0, 3.0],
+        "b": [2.0, 6.0],
+        "x": [1.0, 2.0],
+        "restart": 30,
+        "tolerance": 1e-12,
+        "max_iterations": 20,
+        "tol": 1e-10,
+    },
+    "gmres_basic_5": {
+        "source": "crates/cfd-math/tests/simple_gmres_tests.rs:61-93",
+        "entries": [[0, 0, 2.0], [0, 1, -1.0], [1, 0, -1.0], [1, 1, 2.0], [1, 2, -1.0], [2, 1, -1.0],
+                    [2, 2, 3.0], [2, 3, -1.0], [3, 2, -1.0], [3, 3, 2.0], [3, 4, -1.0], [4, 3, -1.0],
+                    [4, 4, 2.0]],
+        "n": 5,
+        "b": [1.0, 2.0, 3.0, 2.0, 1.0],
+        "restart": 4,
+        "tolerance": 1e-8,
+        "max_iterations": 100,
+        "residual_below": 1.5,
+    },
+    "gmres_restart_8": {
+        "source": "crates/cfd-math/tests/simple_gmres_tests.rs:96-121",
+        "matrix": "tridiagonal n = 8: 2 on the diagonal, -1 off it; b = 1",
+        "n": 8,
+        "restart": 3,
+        "tolerance": 1e-8,
+        "max_iterations": 200,
+        "residual_below": 1e-6,
+    },
+    "gmres_diag_precond_6": {
+        "source": "crates/cfd-math/tests/simple_gmres_tests.rs:124-145",
+        "matrix": "diagonal 1 + 0.1 i, i < 6; b = 1; identity preconditioner",
+        "n": 6,
+        "restart": 6,
+        "tolerance": 1e-10,
+        "max_iterations": 50,
+        "residual_below": 1e-8,
+    },
+    "gmres_core_tridiag_6": {
+        "source": "crates/cfd-math/tests/core_solver_tests.rs:125-150",
+        "matrix": "tridiagonal n = 6: 3 on the diagonal, -1 off it; b = 1",
+        "n": 6,
+        "restart": 4,
+        "tolerance": 1e-8,
+        "max_iterations": 50,
+        "residual_below": 0.3,
+    },
+    "amg_gmres_2d_16": {
+        "source": "crates/cfd-math/tests/amg_integration_test.rs:125-142",
+        "matrix": "poisson_2d(16), manufactured x*, AMGConfig::default",
+        "n": 16,
+        "restart": 30,
+        "tolerance": 1e-10,
+        "max_iterations": 200,
+        "max_abs_error": 1e-6,
+    },
     "kirchhoff_abc": {
         "source": "crates/cfd-1d/src/solver/core/matrix_assembly.rs:270-410",
         "edges": [[0, 1, 1.0], [1, 2, 2.0]],

@@ -203,3 +203,79 @@ def test_cpu_adjoint_against_fd_and_assembly():
     fd = AC.central_fd(theta, col, cells)
     ga = np.array([g[j, i] for j, i in cells])
     assert np.abs(ga - fd).max() <= 1e-6 * np.abs(g).max()
+
+
+def _entries_csr(n, entries):
+    import scipy.sparse as sp
+    from cfdrs_b200.sparse import CsrMatrix
+    e = np.array(entries, dtype=float)
+    return CsrMatrix.from_scipy(sp.csr_matrix((e[:, 2], (e[:, 0].astype(int), e[:, 1].astype(int))), shape=(n, n)))
+
+
+def gmres_golden_cases(golden):
+    """(name, matrix, b, restart, tolerance, max_iterations, residual bound) of
+    the reference's GMRES tests (simple_gmres_tests.rs, core_solver_tests.rs)."""
+    cases = []
+    g = golden["gmres_basic_5"]
+    cases.append(("basic_5", _entries_csr(g["n"], g["entries"]), np.array(g["b"]), g))
+    g = golden["gmres_restart_8"]
+    cases.append(("restart_8", tridiag(g["n"]), np.ones(g["n"]), g))
+    g = golden["gmres_diag_precond_6"]
+    cases.append(("diag_6", _entries_csr(g["n"], [[i, i, 1.0 + 0.1 * i] for i in range(g["n"])]), np.ones(g["n"]), g))
+    g = golden["gmres_core_tridiag_6"]
+    cases.append(("core_6", tridiag(g["n"], lo=-1.0, d=3.0, hi=-1.0), np.ones(g["n"]), g))
+    return cases
+
+
+def test_gmres_restart_ladder(oracle, golden):
+    for requested, width in golden["gmres_restart_ladder"]["requested_width"]:
+        assert oracle.gmres_width(requested) == width, requested
+
+
+def test_gmres_golden(oracle, golden):
+    g = golden["gmres_diagonal_2"]
+    A = oracle.Csr.from_matrix(csr_from_lists(g["row_ptr"], g["col"], g["val"]))
+    for _ in range(2):
+        x, rep = oracle.gmres(A, np.array(g["b"]), restart=g["restart"], tol=g["tolerance"], rtol=0.0,
+                              max_it=g["max_iterations"])
+        assert rep.final_residual <= rep.threshold
+        np.testing.assert_allclose(x, g["x"], atol=g["tol"])
+    for name, M, b, g in gmres_golden_cases(golden):
+        x, rep = oracle.gmres(oracle.Csr.from_matrix(M), b, restart=g["restart"], tol=g["tolerance"], rtol=0.0,
+                              max_it=g["max_iterations"])
+        assert rep.termination == "Converged", name
+        assert np.linalg.norm(M.to_scipy() @ x - b) < g["residual_below"], name
+
+
+def test_amg_gmres_golden(oracle, golden):
+    """amg_integration_test.rs:125-142: AMG(default)-preconditioned GMRES(30)."""
+    g = golden["amg_gmres_2d_16"]
+    n = g["n"]
+    A = grid_laplacian(n)
+    xs = manufactured(n * n)
+    Ao = oracle.Csr.from_matrix(A)
+    x, rep = oracle.gmres(Ao, A.matvec(xs), restart=g["restart"], precond=oracle.PRE_AMG,
+                          amg=oracle.Amg(Ao, oracle.AmgConfig()), tol=g["tolerance"], rtol=0.0,
+                          max_it=g["max_iterations"])
+    assert rep.termination == "Converged"
+    assert np.max(np.abs(x - xs)) < g["max_abs_error"]
+
+
+def test_gmres_against_scipy_and_history(oracle):
+    """Nonsymmetric convection-diffusion-like tridiagonal system, Jacobi-right-
+    preconditioned GMRES(8) with restarts: solution vs sparse direct, the
+    implicit residual history is non-increasing within each run, and the
+    budget ends in MaxIterations."""
+    n = 300
+    A = tridiag(n, lo=-1.3, d=3.0, hi=-0.7)
+    b = np.random.default_rng(1).uniform(-1, 1, n)
+    Ao = oracle.Csr.from_matrix(A)
+    x, rep = oracle.gmres(Ao, b, restart=8, precond=oracle.PRE_JACOBI, rtol=1e-12, max_it=1000)
+    assert rep.termination == "Converged" and rep.iterations > 8
+    np.testing.assert_allclose(x, spla.spsolve(A.to_scipy().tocsc(), b), rtol=1e-9, atol=1e-10)
+    h = rep.history
+    assert np.all(np.diff(h) <= 1e-10 * h[0])  # GMRES never increases the residual
+    _, rep = oracle.gmres(Ao, b, restart=8, precond=oracle.PRE_JACOBI, rtol=1e-14, max_it=5)
+    assert rep.termination == "MaxIterations" and rep.iterations == 5
+    _, rep = oracle.gmres(Ao, np.zeros(n), restart=8, rtol=1e-8)
+    assert rep.termination == "InitialResidual" and rep.iterations == 0
