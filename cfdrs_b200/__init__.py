@@ -1,7 +1,7 @@
 """B200-native (sm_100a) sparse linear-solve path of CFDrs.
 
 Drop-in for cfd-math's preconditioned Krylov surface: ``krylov`` (CG /
-BiCGSTAB entry points, reports and outcome mapping), ``multigrid`` (AMG
+BiCGSTAB / GMRES entry points, reports and outcome mapping), ``multigrid`` (AMG
 configuration and the device V-cycle), ``sparse`` (host CSR), ``problems``
 (seeded assembly of the pressure / Kirchhoff systems). The compute runs in
 ``libcfdgpu.so`` through the C ABI of ``include/cfdgpu.h``.
@@ -9,7 +9,8 @@ configuration and the device V-cycle), ``sparse`` (host CSR), ``problems``
 from .sparse import CsrMatrix, SparseMatrixBuilder, SparseError  # noqa: F401
 from .krylov import (  # noqa: F401
     IterativeSolverConfig, Precision, SolveError, SolveOutcome, SolveReport, SolverKind, Termination,
-    bicgstab, bicgstab_preconditioned, cg, cg_preconditioned, converged_or_none, interpret,
+    bicgstab, bicgstab_preconditioned, cg, cg_preconditioned, converged_or_none, gmres, gmres_preconditioned,
+    gmres_width, interpret,
 )
 from .multigrid import (  # noqa: F401
     AMGConfig, AMGStatistics, AlgebraicMultigrid, CoarseOrder, CoarseSolve, CoarseningStrategy, IdentityPreconditioner,

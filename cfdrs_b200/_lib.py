@@ -54,7 +54,7 @@ class SolverConfigC(C.Structure):
 class SolveOptionsC(C.Structure):
     _fields_ = [("solver", C.c_int32), ("precond", C.c_int32), ("precision", C.c_int32),
                 ("memory", C.c_int32), ("inner_tolerance", C.c_double), ("max_outer", C.c_int32),
-                ("check_every", C.c_int32)]
+                ("check_every", C.c_int32), ("restart", C.c_int32)]
 
 
 class SolveReportC(C.Structure):

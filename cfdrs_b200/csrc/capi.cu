@@ -786,6 +786,7 @@ void cfd_solve_options_default(cfd_solve_options* o) {
   o->inner_tolerance = 1e-4;
   o->max_outer = 20;
   o->check_every = 0;
+  o->restart = 30;
 }
 
 cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, const double* b, double* x,
@@ -802,8 +803,8 @@ cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, con
               cfg->tolerance, cfg->relative_tolerance, (long long)cfg->max_iterations);
     return CFD_ERR_CONFIG;
   }
-  if (opt->solver < 0 || opt->solver > 1 || opt->precond < 0 || opt->precond > 2 || opt->precision < 0 ||
-      opt->precision > 1 || opt->memory < 0 || opt->memory > 1) {
+  if (opt->solver < 0 || opt->solver > 2 || opt->precond < 0 || opt->precond > 2 || opt->precision < 0 ||
+      opt->precision > 1 || opt->memory < 0 || opt->memory > 1 || (opt->solver == CFD_SOLVER_GMRES && opt->restart < 1)) {
     set_error("invalid solve options");
     return CFD_ERR_CONFIG;
   }

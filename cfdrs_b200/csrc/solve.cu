@@ -259,6 +259,183 @@ __global__ void __launch_bounds__(kThreads) k_axpy_state(int64_t n, XT* __restri
   GRID_STRIDE(i, n) x[i] = x[i] + a * y[i];
 }
 
+// ---- GMRES(m): restarted, right preconditioned (krylov.rs:150-221) -----------
+// Arnoldi with classical Gram-Schmidt applied twice (CGS2): the j + 1
+// projections of a step are dot products over the whole basis at once
+// (k_mdot per-CTA partials, k_mdot_finish in fixed order), the subtraction one
+// pass (k_gemv_sub); the Hessenberg column, the Givens rotations and the
+// implicit residual live on the device (k_gmres_rot, one thread).
+constexpr int kGmresGrid = 148 * 2;
+constexpr int kDotTile = 8;
+
+struct GmresDev {
+  int m;            // restart width
+  int* flags;       // [0] columns of the cycle, [1] cycle ended
+  double* H;        // (m + 1) x m Hessenberg, column j at H + j (m + 1)
+  double* cs;       // Givens cosines
+  double* sn;       // Givens sines
+  double* g;        // rotated right-hand side, m + 1
+  double* y;        // least-squares solution, m
+  double* h;        // second-pass projection coefficients, m + 1
+  double* partials; // kGmresGrid x (m + 1)
+};
+
+// partials[cta (m+1) + k] = this CTA's share of V_k . w, k < nv.
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_mdot(int64_t n, const XT* __restrict__ V, int64_t ldv, int nv,
+                                                   const XT* __restrict__ w, int stride, double* partials,
+                                                   const int* skip) {
+  if (flag_set(skip)) return;
+  for (int t0 = 0; t0 < nv; t0 += kDotTile) {
+    double acc[kDotTile];
+#pragma unroll
+    for (int u = 0; u < kDotTile; ++u) acc[u] = 0.0;
+    GRID_STRIDE(i, n) {
+      const double wi = (double)w[i];
+#pragma unroll
+      for (int u = 0; u < kDotTile; ++u)
+        if (t0 + u < nv) acc[u] += (double)V[(int64_t)(t0 + u) * ldv + i] * wi;
+    }
+#pragma unroll
+    for (int u = 0; u < kDotTile; ++u) {
+      const double b = block_sum(acc[u]);
+      if (threadIdx.x == 0 && t0 + u < nv) partials[(size_t)blockIdx.x * stride + t0 + u] = b;
+    }
+  }
+}
+
+// out[k] = sum over CTAs of partials (one CTA per k, fixed order); mode 1: sqrt.
+__global__ void __launch_bounds__(kThreads) k_mdot_finish(int grid, const double* __restrict__ partials, int stride,
+                                                          double* out, int mode, const int* skip) {
+  if (flag_set(skip)) return;
+  const int k = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < grid; b += blockDim.x) s += partials[(size_t)b * stride + k];
+  s = block_sum(s);
+  if (threadIdx.x == 0) out[k] = mode == 1 ? sqrt(s) : s;
+}
+
+// w -= sum_k h_k V_k (k < nv), summed in k order in FP64.
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_gemv_sub(int64_t n, const XT* __restrict__ V, int64_t ldv, int nv,
+                                                       const double* __restrict__ h, XT* __restrict__ w,
+                                                       const int* skip) {
+  if (flag_set(skip)) return;
+  GRID_STRIDE(i, n) {
+    double s = 0.0;
+    for (int k = 0; k < nv; ++k) s += h[k] * (double)V[(int64_t)k * ldv + i];
+    w[i] = (XT)((double)w[i] - s);
+  }
+}
+
+// u = sum_k y_k V_k over the cycle's columns.
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_gemv_cols(int64_t n, const XT* __restrict__ V, int64_t ldv,
+                                                        const int* __restrict__ cols, const double* __restrict__ y,
+                                                        XT* __restrict__ u, const int* skip) {
+  if (flag_set(skip)) return;
+  const int nc = *cols;
+  GRID_STRIDE(i, n) {
+    double s = 0.0;
+    for (int k = 0; k < nc; ++k) s += y[k] * (double)V[(int64_t)k * ldv + i];
+    u[i] = (XT)s;
+  }
+}
+
+// dst = src / *div (nothing when *div is 0: the Krylov space is exhausted).
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_scale_div(int64_t n, const XT* src, XT* dst,
+                                                        const double* __restrict__ div, const int* skip) {
+  if (flag_set(skip)) return;
+  const double d = *div;
+  if (d == 0.0) return;
+  GRID_STRIDE(i, n) dst[i] = (XT)((double)src[i] / d);
+}
+
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_jacobi_apply(int64_t n, const XT* __restrict__ r,
+                                                           const XT* __restrict__ jinv, XT* __restrict__ z,
+                                                           const int* skip) {
+  if (flag_set(skip)) return;
+  GRID_STRIDE(i, n) z[i] = r[i] * jinv[i];
+}
+
+template <typename XT>
+__global__ void __launch_bounds__(kThreads) k_add(int64_t n, XT* __restrict__ x, const XT* __restrict__ z,
+                                                  const int* skip) {
+  if (flag_set(skip)) return;
+  GRID_STRIDE(i, n) x[i] = x[i] + z[i];
+}
+
+// Cycle start: no columns yet, the cycle open unless the solve is done;
+// g = (beta, 0, ..., 0) once beta lands in g[0].
+__global__ void k_gmres_begin(GmresDev G, const DevState* st) {
+  G.flags[0] = 0;
+  G.flags[1] = st->done ? 1 : 0;
+  for (int k = 1; k <= G.m; ++k) G.g[k] = 0.0;
+}
+
+// Step j: second projection pass added to the column, earlier rotations
+// applied, the new rotation formed, the implicit residual |g_{j+1}| tested.
+__global__ void k_gmres_rot(GmresDev G, int j, DevState* st) {
+  if (G.flags[1]) return;
+  const int m = G.m;
+  double* h = G.H + (size_t)j * (m + 1);
+  for (int q = 0; q <= j; ++q) h[q] += G.h[q];
+  const double hn = h[j + 1];
+  for (int q = 0; q < j; ++q) {
+    const double t = G.cs[q] * h[q] + G.sn[q] * h[q + 1];
+    h[q + 1] = -G.sn[q] * h[q] + G.cs[q] * h[q + 1];
+    h[q] = t;
+  }
+  const double d = hypot(h[j], h[j + 1]);
+  G.cs[j] = d > 0.0 ? h[j] / d : 1.0;
+  G.sn[j] = d > 0.0 ? h[j + 1] / d : 0.0;
+  h[j] = d;
+  h[j + 1] = 0.0;
+  G.g[j + 1] = -G.sn[j] * G.g[j];
+  G.g[j] = G.cs[j] * G.g[j];
+  st->iter += 1;
+  const double res = fabs(G.g[j + 1]);
+  st->rnorm = res;
+  G.flags[0] = j + 1;
+  if (!isfinite(res)) {
+    G.flags[1] = 1;
+    st->term = CFD_TERM_BREAKDOWN;
+    st->done = 1;
+  } else if (res <= st->threshold || st->iter >= st->max_iter || hn == 0.0 || j + 1 == m) {
+    G.flags[1] = 1;
+  }
+}
+
+// y = R^-1 g on the cycle's columns (back substitution).
+__global__ void k_gmres_lsq(GmresDev G, const int* skip) {
+  if (flag_set(skip)) return;
+  const int m = G.m, cols = G.flags[0];
+  for (int q = cols - 1; q >= 0; --q) {
+    double s = G.g[q];
+    for (int l = q + 1; l < cols; ++l) s -= G.H[(size_t)l * (m + 1) + q] * G.y[l];
+    const double dqq = G.H[(size_t)q * (m + 1) + q];
+    G.y[q] = dqq != 0.0 ? s / dqq : 0.0;
+  }
+}
+
+// After x += M^-1 V y and r = b - A x (rnorm = ||r||): the true residual decides.
+__global__ void k_gmres_check(DevState* st) {
+  if (st->done) return;
+  const double rn = st->rnorm;
+  if (!isfinite(rn)) {
+    st->term = CFD_TERM_BREAKDOWN;
+    st->done = 1;
+  } else if (rn <= st->threshold) {
+    st->term = CFD_TERM_CONVERGED;
+    st->done = 1;
+  } else if (st->iter >= st->max_iter) {
+    st->term = CFD_TERM_MAX_ITERATIONS;
+    st->done = 1;
+  }
+}
+
 // ---- refinement ----------------------------------------------------------------
 // Inner right-hand side r32 = r64 / ||r64||, inner iterate zeroed; sets up the
 // inner state (threshold = inner_tol * ||r32||).
@@ -578,6 +755,22 @@ static cfd_status vcycle(Launcher& lc, cfd_amg* amg, size_t l, const XT* b, XT* 
 // only polls the state to stop launching, choosing how many iterations to
 // enqueue from the observed convergence rate.
 
+// Stream-ordered workspace (the default memory pool keeps freed blocks for reuse).
+template <typename XT>
+struct Alloc {
+  cudaStream_t s;
+  std::vector<void*> ptrs;
+  XT* get(int64_t n) {
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, (size_t)std::max<int64_t>(n, 1) * sizeof(XT), s) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return (XT*)p;
+  }
+  ~Alloc() {
+    for (void* p : ptrs) cudaFreeAsync(p, s);
+  }
+};
+
 struct Poller {
   cfd_context* ctx;
   DevState* dev;
@@ -697,9 +890,103 @@ static cfd_status bicgstab_loop(Launcher& lc, cfd_csr* a, cfd_amg* amg, KrylovBu
   return CFD_OK;
 }
 
+// Restart width for a requested restart: RestartWidth::covering (krylov.rs:96-120).
+int gmres_width(int64_t requested) {
+  int w = 8;
+  while (w < 256 && w < requested) w *= 2;
+  return w;
+}
+
+// Restarted GMRES(m) with right preconditioning. Expects the state's start
+// (rnorm0, threshold, done, iter) set, r = b - A x and b the right-hand side.
+// One host poll per restart cycle; the steps of a cycle after it ended are
+// launched but return at once.
+template <typename XT, int PRE>
+static cfd_status gmres_loop(Launcher& lc, cfd_csr* a, cfd_amg* amg, KrylovBufs<XT>& B, DevState* st, Poller& pl,
+                             int64_t restart) {
+  const int64_t n = a->dev.nrows;
+  const int m = gmres_width(restart);
+  const XT* jinv = jinv_of<XT>(a);
+  Alloc<XT> ax{lc.s, {}};
+  Alloc<double> ad{lc.s, {}};
+  Alloc<int> ai{lc.s, {}};
+  XT* V = ax.get((int64_t)(m + 1) * n);
+  GmresDev G{m, ai.get(4), ad.get((int64_t)(m + 1) * m), ad.get(m), ad.get(m), ad.get(m + 1), ad.get(m),
+             ad.get(m + 1), ad.get((int64_t)kGmresGrid * (m + 1))};
+  if (!V || !G.flags || !G.H || !G.cs || !G.sn || !G.g || !G.y || !G.h || !G.partials) {
+    set_error("GMRES workspace allocation failed (%lld unknowns, restart %d)", (long long)n, m);
+    return CFD_ERR_ALLOC;
+  }
+  CFD_TRY_CUDA(cudaMemsetAsync(G.H, 0, sizeof(double) * (m + 1) * m, lc.s));
+  const int stride = m + 1;
+  const int* done = &st->done;
+  const int* ended = G.flags + 1;
+  auto dots = [&](const XT* Vb, int nv, const XT* w, double* out, int mode, const int* skip) -> cfd_status {
+    k_mdot<XT><<<kGmresGrid, kThreads, 0, lc.s>>>(n, Vb, n, nv, w, stride, G.partials, skip);
+    k_mdot_finish<<<nv, kThreads, 0, lc.s>>>(kGmresGrid, G.partials, stride, out, mode, skip);
+    lc.ctx->stats.launches += 2;
+    return lc.check();
+  };
+  auto precond = [&](const XT* v, XT* z, const int* skip) -> const XT* {
+    if (PRE == kPreAmg) {
+      if (vcycle<XT>(lc, amg, 0, v, z, 0, st, skip) != CFD_OK) return nullptr;
+      return z;
+    }
+    if (PRE == kPreJacobi) {
+      if (lc.vec(n, k_jacobi_apply<XT>, v, jinv, z, skip) != CFD_OK) return nullptr;
+      return z;
+    }
+    return v;
+  };
+  int64_t cycles = 0;
+  for (;;) {
+    // cycle start: beta = ||r||, v_0 = r / beta
+    k_gmres_begin<<<1, 1, 0, lc.s>>>(G, st);
+    CFD_TRY(dots(B.r, 1, B.r, G.g, 1, done));
+    CFD_TRY(lc.vec(n, k_scale_div<XT>, (const XT*)B.r, V, (const double*)G.g, done));
+    for (int j = 0; j < m; ++j) {
+      XT* vj = V + (int64_t)j * n;
+      XT* w = V + (int64_t)(j + 1) * n;
+      double* hc = G.H + (size_t)j * (m + 1);
+      const XT* z = precond(vj, B.z, ended);
+      if (!z) return CFD_ERR_CUDA;
+      CFD_TRY(lc.spmv<XT, XT, false>(a->dev, z, EpiStore<XT>{w, ended, {}}));
+      CFD_TRY(dots(V, j + 1, w, hc, 0, ended));
+      CFD_TRY(lc.vec(n, k_gemv_sub<XT>, (const XT*)V, n, j + 1, (const double*)hc, w, ended));
+      CFD_TRY(dots(V, j + 1, w, G.h, 0, ended));
+      CFD_TRY(lc.vec(n, k_gemv_sub<XT>, (const XT*)V, n, j + 1, (const double*)G.h, w, ended));
+      CFD_TRY(dots(w, 1, w, hc + j + 1, 1, ended));
+      CFD_TRY(lc.vec(n, k_scale_div<XT>, (const XT*)w, w, (const double*)(hc + j + 1), ended));
+      k_gmres_rot<<<1, 1, 0, lc.s>>>(G, j, st);
+      CFD_TRY(lc.check());
+    }
+    // x += M^-1 (V y); r = b - A x; the true residual decides
+    k_gmres_lsq<<<1, 1, 0, lc.s>>>(G, done);
+    CFD_TRY(lc.vec(n, k_gemv_cols<XT>, (const XT*)V, n, (const int*)G.flags, (const double*)G.y, B.q, done));
+    const XT* zc = precond(B.q, B.z, done);
+    if (!zc) return CFD_ERR_CUDA;
+    CFD_TRY(lc.vec(n, k_add<XT>, B.x, zc, done));
+    CFD_TRY(lc.spmv<XT, XT, false>(a->dev, B.x, EpiResidual<XT, 2>{B.r, B.b, st, done, {}}));
+    k_gmres_check<<<1, 1, 0, lc.s>>>(st);
+    CFD_TRY(lc.check());
+    CFD_TRY(pl.poll());
+    if (pl.host->done) break;
+    if (++cycles > pl.host->max_iter + 2) {
+      set_error("GMRES did not terminate within its iteration budget");
+      return CFD_ERR_TIMEOUT;
+    }
+  }
+  return CFD_OK;
+}
+
 template <typename XT>
 static cfd_status krylov_loop(Launcher& lc, int solver, int pre, cfd_csr* a, cfd_amg* amg, KrylovBufs<XT>& B,
-                              DevState* st, Poller& pl) {
+                              DevState* st, Poller& pl, int64_t restart) {
+  if (solver == CFD_SOLVER_GMRES) {
+    if (pre == kPreJacobi) return gmres_loop<XT, kPreJacobi>(lc, a, amg, B, st, pl, restart);
+    if (pre == kPreAmg) return gmres_loop<XT, kPreAmg>(lc, a, amg, B, st, pl, restart);
+    return gmres_loop<XT, kPreNone>(lc, a, amg, B, st, pl, restart);
+  }
   if (solver == CFD_SOLVER_BICGSTAB) {
     if (pre == kPreJacobi) return bicgstab_loop<XT, kPreJacobi>(lc, a, amg, B, st, pl);
     if (pre == kPreAmg) return bicgstab_loop<XT, kPreAmg>(lc, a, amg, B, st, pl);
@@ -709,22 +996,6 @@ static cfd_status krylov_loop(Launcher& lc, int solver, int pre, cfd_csr* a, cfd
   if (pre == kPreAmg) return pcg_loop<XT, kPreAmg>(lc, a, amg, B, st, pl);
   return pcg_loop<XT, kPreNone>(lc, a, amg, B, st, pl);
 }
-
-// Stream-ordered workspace (the default memory pool keeps freed blocks for reuse).
-template <typename XT>
-struct Alloc {
-  cudaStream_t s;
-  std::vector<void*> ptrs;
-  XT* get(int64_t n) {
-    void* p = nullptr;
-    if (cudaMallocAsync(&p, (size_t)std::max<int64_t>(n, 1) * sizeof(XT), s) != cudaSuccess) return nullptr;
-    ptrs.push_back(p);
-    return (XT*)p;
-  }
-  ~Alloc() {
-    for (void* p : ptrs) cudaFreeAsync(p, s);
-  }
-};
 
 static void init_state(DevState& h, const cfd_solver_config& cfg) {
   std::memset(&h, 0, sizeof(h));
@@ -799,7 +1070,7 @@ cfd_status solve_fp64(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg, co
   CFD_TRY(lc.spmv<double, double, false>(a->dev, B.x, EpiResidual<double, 1>{B.r, B.b, st, nullptr, {}}));
   Poller pl{ctx, st, hs};
   pl.fixed = opt.check_every;
-  CFD_TRY(krylov_loop<double>(lc, opt.solver, opt.precond, a, amg, B, st, pl));
+  CFD_TRY(krylov_loop<double>(lc, opt.solver, opt.precond, a, amg, B, st, pl, opt.restart));
   if (host_mem) CFD_TRY_CUDA(cudaMemcpyAsync(x, B.x, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CFD_TRY_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
   CFD_TRY(pl.poll());
@@ -833,6 +1104,7 @@ cfd_status solve_refine(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg, 
   double* r64 = ad.get(n);
   KrylovBufs<float> B{};
   B.x = af.get(n);
+  if (opt.solver == CFD_SOLVER_GMRES) B.b = af.get(n);  // inner right-hand side for restarts
   B.r = af.get(n);
   B.p = af.get(n);
   B.q = af.get(n);
@@ -845,7 +1117,7 @@ cfd_status solve_refine(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg, 
     B.t = af.get(n);
   }
   if (!x64 || !b64 || !r64 || !B.x || !B.r || !B.p || !B.q || !B.z ||
-      (opt.solver == CFD_SOLVER_BICGSTAB && !B.t)) {
+      (opt.solver == CFD_SOLVER_BICGSTAB && !B.t) || (opt.solver == CFD_SOLVER_GMRES && !B.b)) {
     set_error("device workspace allocation failed (%lld unknowns)", (long long)n);
     return CFD_ERR_ALLOC;
   }
@@ -885,7 +1157,8 @@ cfd_status solve_refine(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg, 
     Poller pl{ctx, inner, hs + 1};
     pl.fixed = opt.check_every;
     pl.poll();
-    CFD_TRY(krylov_loop<float>(lc, opt.solver, opt.precond, a, amg, B, inner, pl));
+    if (opt.solver == CFD_SOLVER_GMRES) CFD_TRY(lc.vec(n, k_copy<float>, (const float*)B.r, B.b, (const int*)nullptr));
+    CFD_TRY(krylov_loop<float>(lc, opt.solver, opt.precond, a, amg, B, inner, pl, opt.restart));
     inner_iters += hs[1].iter;
     ++outer_steps;
     const int iterm = hs[1].term;

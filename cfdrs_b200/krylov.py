@@ -114,13 +114,13 @@ def converged_or_none(context: str, report: SolveReport) -> SolveReport | None:
     return report if out.converged() else None
 
 
-_SOLVER_CG, _SOLVER_BICGSTAB = 0, 1
+_SOLVER_CG, _SOLVER_BICGSTAB, _SOLVER_GMRES = 0, 1, 2
 _PRE_NONE, _PRE_JACOBI, _PRE_AMG = 0, 1, 2
 
 
 def _solve(solver: int, matrix, rhs, preconditioner, solution, config: IterativeSolverConfig,
            precision: Precision = Precision.FP64, inner_tolerance: float = 1e-4, check_every: int = 0,
-           max_outer: int = 20) -> SolveReport:
+           max_outer: int = 20, restart: int = 30) -> SolveReport:
     import torch
     L = _lib.load()
     amg_h = None
@@ -135,7 +135,9 @@ def _solve(solver: int, matrix, rhs, preconditioner, solution, config: Iterative
         raise SolveError(f"unsupported preconditioner {type(preconditioner).__name__}")
     dm = device_matrix(matrix, preconditioner.ctx if pre == _PRE_AMG else None)
     n = dm.shape[0]
-    opt = _lib.SolveOptionsC(solver, pre, int(precision), 0, inner_tolerance, max_outer, check_every)
+    if restart < 1:
+        raise SolveError(f"GMRES restart must be positive, got {restart}")
+    opt = _lib.SolveOptionsC(solver, pre, int(precision), 0, inner_tolerance, max_outer, check_every, restart)
     rep = _lib.SolveReportC()
     cfg = config.to_c()
     if isinstance(solution, torch.Tensor):
@@ -188,18 +190,64 @@ def bicgstab(matrix, rhs, solution, config, **kw) -> SolveReport:
     return _solve(_SOLVER_BICGSTAB, matrix, rhs, None, solution, config, **kw)
 
 
-class SolverKind(enum.Enum):
-    """``SolverKind`` (``krylov.rs:533-612``); GMRES is not part of this path."""
-    CONJUGATE_GRADIENT = "ConjugateGradient"
-    BICGSTAB = "BiCGSTAB"
+def gmres_preconditioned(matrix, rhs, preconditioner, solution, config, restart: int = 30, **kw) -> SolveReport:
+    """``krylov::gmres_preconditioned`` (``krylov.rs:150-170``): restarted GMRES,
+    right preconditioned, the restart rounded up the ladder 8, 16, ..., 256."""
+    return _solve(_SOLVER_GMRES, matrix, rhs, preconditioner, solution, config, restart=restart, **kw)
+
+
+def gmres(matrix, rhs, solution, config, restart: int = 30, **kw) -> SolveReport:
+    """``krylov::gmres`` (``krylov.rs:228-246``)."""
+    return _solve(_SOLVER_GMRES, matrix, rhs, None, solution, config, restart=restart, **kw)
+
+
+def gmres_width(requested: int) -> int:
+    """``RestartWidth::covering`` (``krylov.rs:96-120``): the smallest of 8, 16,
+    32, 64, 128, 256 covering the request, saturating at 256."""
+    w = 8
+    while w < 256 and w < requested:
+        w *= 2
+    return w
+
+
+class SolverKind:
+    """``SolverKind`` (``krylov.rs:533-612``): ConjugateGradient, BiCgStab or
+    Gmres { restart } (``SolverKind.gmres(restart)``)."""
+    CONJUGATE_GRADIENT: "SolverKind"
+    BICGSTAB: "SolverKind"
+
+    def __init__(self, kind: str, restart: int | None = None):
+        self.kind = kind
+        self.restart = restart
+
+    @classmethod
+    def gmres(cls, restart: int) -> "SolverKind":
+        return cls("GMRES", restart)
 
     def name_(self) -> str:
-        return self.value
+        return self.kind
+
+    def __eq__(self, other) -> bool:
+        return isinstance(other, SolverKind) and (self.kind, self.restart) == (other.kind, other.restart)
+
+    def __hash__(self) -> int:
+        return hash((self.kind, self.restart))
+
+    def __repr__(self) -> str:
+        return f"SolverKind.{self.kind}" + (f"{{restart: {self.restart}}}" if self.kind == "GMRES" else "")
 
     def solve(self, matrix, rhs, solution, config, **kw) -> SolveReport:
-        f = cg if self is SolverKind.CONJUGATE_GRADIENT else bicgstab
+        if self.kind == "GMRES":
+            return gmres(matrix, rhs, solution, config, self.restart, **kw)
+        f = cg if self.kind == "ConjugateGradient" else bicgstab
         return f(matrix, rhs, solution, config, **kw)
 
     def solve_preconditioned(self, matrix, rhs, preconditioner, solution, config, **kw) -> SolveReport:
-        f = cg_preconditioned if self is SolverKind.CONJUGATE_GRADIENT else bicgstab_preconditioned
+        if self.kind == "GMRES":
+            return gmres_preconditioned(matrix, rhs, preconditioner, solution, config, self.restart, **kw)
+        f = cg_preconditioned if self.kind == "ConjugateGradient" else bicgstab_preconditioned
         return f(matrix, rhs, preconditioner, solution, config, **kw)
+
+
+SolverKind.CONJUGATE_GRADIENT = SolverKind("ConjugateGradient")
+SolverKind.BICGSTAB = SolverKind("BiCGSTAB")

@@ -11,6 +11,7 @@
  * Reference interfaces replaced (paths relative to the CFDrs repository):
  *   cfd_solve                krylov::cg_preconditioned       crates/cfd-math/src/linear_solver/krylov.rs:318-343
  *                            krylov::bicgstab_preconditioned  krylov.rs:253-278
+ *                            krylov::gmres_preconditioned     krylov.rs:150-221 (gmres :228-246)
  *                            krylov::cg / krylov::bicgstab    krylov.rs:350-360 / :285-308
  *                            SolverKind::solve[_preconditioned] krylov.rs:562-612
  *   cfd_solver_config        IterativeSolverConfig -> convergence_policy, krylov.rs:123-139
@@ -203,7 +204,10 @@ cfd_status cfd_amg_level(const cfd_amg* amg, int level, int which, int64_t* nrow
 cfd_status cfd_amg_destroy(cfd_amg* amg);
 
 /* ---- Krylov solve ------------------------------------------------------ */
-typedef enum { CFD_SOLVER_CG = 0, CFD_SOLVER_BICGSTAB = 1 } cfd_solver_kind;
+/* GMRES: restarted GMRES(m), right preconditioned, krylov::gmres_preconditioned
+ * (krylov.rs:150-221); m = the requested restart rounded up the ladder 8, 16, 32,
+ * 64, 128, 256 (RestartWidth::covering, krylov.rs:96-120), saturating at 256. */
+typedef enum { CFD_SOLVER_CG = 0, CFD_SOLVER_BICGSTAB = 1, CFD_SOLVER_GMRES = 2 } cfd_solver_kind;
 typedef enum { CFD_PRECOND_NONE = 0, CFD_PRECOND_JACOBI = 1, CFD_PRECOND_AMG = 2 } cfd_precond_kind;
 typedef enum { CFD_PRECISION_FP64 = 0, CFD_PRECISION_FP32_REFINE = 1 } cfd_precision;
 typedef enum { CFD_MEMORY_HOST = 0, CFD_MEMORY_DEVICE = 1 } cfd_memory;
@@ -222,6 +226,7 @@ typedef struct {
   double inner_tolerance;   /* FP32 inner relative tolerance (refinement), e.g. 1e-4 */
   int32_t max_outer;        /* refinement steps cap */
   int32_t check_every;      /* device iterations between host convergence polls (0 = auto) */
+  int32_t restart;          /* GMRES restart request (default 30, the pressure solver's GMRES(30)) */
 } cfd_solve_options;
 
 void cfd_solve_options_default(cfd_solve_options* opt);
