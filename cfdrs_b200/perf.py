@@ -5,6 +5,7 @@
     python -m cfdrs_b200.perf levels --n 256              # SpMV bandwidth of every hierarchy operator
     python -m cfdrs_b200.perf batch --systems 4096        # batched network solve, FP64 and FP32+refinement
     python -m cfdrs_b200.perf adjoint --n 512             # dL/dtheta of the 2-D Darcy column loss
+    python -m cfdrs_b200.perf gmres --n 128               # AMG-GMRES(30), FP64 and FP32+refinement
 
 All cases use the seeded 3-D variable-coefficient Poisson system of bench.py.
 """
@@ -47,7 +48,7 @@ def _paths(d):
 
 def main(argv=None):
     p = argparse.ArgumentParser()
-    p.add_argument("case", choices=["spmv", "solve", "levels", "batch", "adjoint"])
+    p.add_argument("case", choices=["spmv", "solve", "levels", "batch", "adjoint", "gmres"])
     p.add_argument("--fd-cells", type=int, default=64)
     p.add_argument("--systems", type=int, default=4096)
     p.add_argument("--n", type=int, default=128)
@@ -93,6 +94,15 @@ def main(argv=None):
     bd = torch.as_tensor(b, device="cuda")
     x = torch.zeros_like(bd)
     cfg = cf.IterativeSolverConfig(0.0, 1e-8, 1000)
+    if a.case == "gmres":
+        for prec in (cf.Precision.FP64, cf.Precision.FP32_REFINE):
+            for rep_i in range(3):
+                x.zero_()
+                torch.cuda.synchronize()
+                r = cf.gmres_preconditioned(A, bd, amg, x, cfg, restart=30, precision=prec)
+            print(f"GMRES(30) {prec.name}: {r.device_ms:.1f} ms device, {r.iterations} iterations, "
+                  f"{r.outer_iterations} refinements, final {r.final_residual:.3e} <= {r.threshold:.3e}", flush=True)
+        return 0
     r1 = cf.cg_preconditioned(A, bd, amg, x, cfg, precision=cf.Precision.FP32_REFINE)
     x.zero_()
     r2 = cf.cg_preconditioned(A, bd, amg, x, cfg)
