@@ -101,7 +101,7 @@ def main(argv=None):
                 torch.cuda.synchronize()
                 r = cf.gmres_preconditioned(A, bd, amg, x, cfg, restart=30, precision=prec)
             print(f"GMRES(30) {prec.name}: {r.device_ms:.1f} ms device, {r.iterations} iterations, "
-                  f"{r.outer_iterations} refinements, final {r.final_residual:.3e} <= {r.threshold:.3e}", flush=True)
+                  f"{r.outer_iterations} refinements, final {r.final_residual_norm:.3e} <= {r.threshold:.3e}", flush=True)
         return 0
     r1 = cf.cg_preconditioned(A, bd, amg, x, cfg, precision=cf.Precision.FP32_REFINE)
     x.zero_()
