@@ -579,11 +579,4 @@ std::vector<HostLevel> build_hierarchy(const HostCsr& a, const cfd_amg_config& c
   return levels;
 }
 
-// AlgebraicMultigrid::recompute, amg.rs:179-214.
-void recompute_hierarchy(std::vector<HostLevel>& levels, const HostCsr& a) {
-  levels[0].A.v = a.v;
-  for (size_t l = 0; l + 1 < levels.size(); ++l)
-    levels[l + 1].A = spgemm(spgemm(levels[l].R, levels[l].A), levels[l].P);
-}
-
 }  // namespace cfd

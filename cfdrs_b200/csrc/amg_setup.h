@@ -39,7 +39,5 @@ struct HostLevel {
 
 // AlgebraicMultigrid::setup / build_next_level.
 std::vector<HostLevel> build_hierarchy(const HostCsr& a, const cfd_amg_config& cfg);
-// AlgebraicMultigrid::recompute: new fine values, cached P/R.
-void recompute_hierarchy(std::vector<HostLevel>& levels, const HostCsr& a);
 
 }  // namespace cfd

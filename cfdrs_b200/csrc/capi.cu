@@ -293,6 +293,7 @@ void amg_free_device(cfd_amg* amg) {
     dfree(L.d32);
     free_level_vecs(L.v64);
     free_level_vecs(L.v32);
+    free_ra(L.ra);
   }
   amg->dev.clear();
   dfree(amg->coarse_inv);
@@ -700,11 +701,13 @@ cfd_status cfd_amg_recompute(cfd_amg* amg, cfd_csr* a) {
     set_error("recompute needs the hierarchy's sparsity pattern");
     return CFD_ERR_DIM;
   }
+  if (a->ctx != amg->ctx) {
+    set_error("recompute: the matrix and the hierarchy belong to different contexts");
+    return CFD_ERR_STATE;
+  }
   std::lock_guard<std::mutex> g(a->ctx->mu);
   CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
-  const bool want32 = amg->have32;
-  recompute_hierarchy(amg->host, a->host);
-  return amg_upload(amg, want32);
+  return amg_recompute_device(amg, a);
 }
 
 cfd_status cfd_amg_apply(cfd_amg* amg, const double* r, double* z) {
@@ -756,6 +759,12 @@ cfd_status cfd_amg_stats(const cfd_amg* amg, cfd_amg_stats_t* out) {
 cfd_status cfd_amg_level(const cfd_amg* amg, int level, int which, int64_t* nrows, int64_t* ncols, int64_t* nnz,
                          int64_t* row_ptr, int64_t* col, double* val) {
   if (!amg || level < 0 || level >= (int)amg->host.size() || which < 0 || which > 2) return CFD_ERR_DIM;
+  if (which == 0 && val && amg->host_values_stale) {
+    cfd_amg* mut = const_cast<cfd_amg*>(amg);  // the host mirror is a cache of the device values
+    std::lock_guard<std::mutex> g(mut->ctx->mu);
+    CFD_TRY_CUDA(cudaSetDevice(mut->ctx->device));
+    CFD_TRY(amg_sync_host_values(mut));
+  }
   const HostLevel& L = amg->host[level];
   if (which > 0 && level + 1 == (int)amg->host.size()) return CFD_ERR_DIM;
   const HostCsr& m = which == 0 ? L.A : (which == 1 ? L.P : L.R);
