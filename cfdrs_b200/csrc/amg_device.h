@@ -60,4 +60,8 @@ cfd_status amg_recompute_device(cfd_amg* amg, const cfd_csr* a);
 // Brings the host copies of the level A values up to date after a device recompute.
 cfd_status amg_sync_host_values(cfd_amg* amg);
 void free_ra(DevRA& ra);
+// Gauss-Jordan inverse (partial pivoting, the host dense_inverse's operations
+// in its order) of an n x n device CSR operator into inv (n x n, row-major).
+cfd_status dense_inverse_device(cfd_context* ctx, int64_t n, const int* rp, const int* ci, const double* v,
+                                double* inv);
 }  // namespace cfd

@@ -91,20 +91,6 @@ __device__ __forceinline__ T block_sum(T v) {
   return t;
 }
 
-// Sum over the kThreads consumer threads only (named barrier 1); valid in thread 0.
-template <typename T>
-__device__ __forceinline__ T consumer_sum(T v) {
-  __shared__ T sm[kThreads / 32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  v = warp_sum(v);
-  asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory");
-  if (lane == 0) sm[w] = v;
-  asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory");
-  T t = threadIdx.x < kThreads / 32 ? sm[threadIdx.x] : T(0);
-  if (w == 0) t = warp_sum(t);
-  return t;
-}
-
 // Two-stage grid reduction of NV doubles. Every thread of every CTA must call
 // it. Returns true in the last CTA, whose thread 0 then holds the totals.
 template <int NV>
@@ -513,7 +499,8 @@ __global__ void __launch_bounds__(kPipeThreads, PipeLayout<VT, CODES>::kMinBlock
   __shared__ __align__(8) uint64_t empty[kStages];
   __shared__ int4 meta[kStages];  // r0, r1, k0, k1 of the staged block
   __shared__ int2 dmeta[kStages];  // dictionary {first entry, entries} of the staged block
-  __shared__ int s_ok[kStages];
+  __shared__ VT s_psum[kStages][kThreads / 32], s_pdiag[kStages][kThreads / 32];  // long-row partials
+  __shared__ int s_pcnt[kStages];
   __shared__ volatile int s_abort;
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
@@ -531,6 +518,7 @@ __global__ void __launch_bounds__(kPipeThreads, PipeLayout<VT, CODES>::kMinBlock
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], kThreads / 32);
+      s_pcnt[s] = 0;
     }
     s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -641,21 +629,28 @@ __global__ void __launch_bounds__(kPipeThreads, PipeLayout<VT, CODES>::kMinBlock
     }
   } else {
     // ---- consumers ----
+    // Each warp takes the stages in order on its own (no CTA-wide barrier per
+    // stage). A stage is refilled only after all consumer warps released it,
+    // so a warp runs at most kStages blocks ahead of the slowest one and the
+    // full-barrier phase it waits for is always the pending one.
     const int tl = A.tpr_log2;
+    const int lane = tid & 31;
+    const int G = (int)gridDim.x;
     int it = 0;
-    for (int b = blockIdx.x; b < nblk; b += gridDim.x, ++it) {
+    for (int b = blockIdx.x; b < nblk; b += G, ++it) {
       const int s = it % kStages;
       const unsigned parity = (unsigned)(it / kStages) & 1u;
-      if (tid == 0) s_ok[s] = (!s_abort && mbar_wait_bounded(&full[s], parity)) ? 1 : 0;
-      asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory");
-      if (!s_ok[s]) {
-        if (tid == 0) {
+      int ok = 1;
+      if (lane == 0) ok = (!s_abort && mbar_wait_bounded(&full[s], parity)) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        if (lane == 0) {
           s_abort = 1;
           atomicExch(err, 1);
         }
         break;
       }
-      mbar_wait_bounded(&full[s], parity);  // completes at once; acquires the stage for this thread
+      mbar_wait_bounded(&full[s], parity);  // completes at once; acquires the stage for this lane
       const int4 m = meta[s];
       const int2 md = dmeta[s];
       if constexpr (CODES) {
@@ -683,6 +678,10 @@ __global__ void __launch_bounds__(kPipeThreads, PipeLayout<VT, CODES>::kMinBlock
         const ColRaw cr{stage_col(s) - (m.z & ~3)};
         rows_from_stage<VT, XT, OFFDIAG>(epi, srp, cr, stage_val(s) - (m.z & ~(mv - 1)), m.x, m.y, tl, tid, x, red);
       } else {
+        // One row longer than kNnzCap, shared by all consumer warps: each warp
+        // leaves its partial sums in shared memory and warp 0 adds them in a
+        // fixed order after a bounded wait. No named barrier: a warp that
+        // leaves the loop early cannot hold the others.
         const int row = m.x;
         typename Epi::Pre pre{};
         if (tid == 0) pre = epi.load(row);
@@ -695,12 +694,42 @@ __global__ void __launch_bounds__(kPipeThreads, PipeLayout<VT, CODES>::kMinBlock
           else
             sum += v * (VT)__ldg(x + c);
         }
-        sum = consumer_sum(sum);
-        diag = consumer_sum(diag);
-        if (tid == 0) epi.row(row, sum, diag, pre, red);
+        sum = warp_sum(sum);
+        diag = warp_sum(diag);
+        if (lane == 0) {
+          s_psum[s][warp] = sum;
+          s_pdiag[s][warp] = diag;
+          __threadfence_block();
+          atomicAdd(&s_pcnt[s], 1);
+        }
+        if (warp == 0) {
+          int all = 1;
+          if (lane == 0) {
+            unsigned i = 0;
+            while (*reinterpret_cast<volatile int*>(&s_pcnt[s]) < kThreads / 32 && ++i < kWaitLimit) {
+            }
+            all = i < kWaitLimit;
+            __threadfence_block();
+          }
+          all = __shfl_sync(0xffffffffu, all, 0);
+          __threadfence_block();
+          if (all) {
+            VT ts = lane < kThreads / 32 ? s_psum[s][lane] : VT(0);
+            VT td = lane < kThreads / 32 ? s_pdiag[s][lane] : VT(0);
+            ts = warp_sum(ts);
+            td = warp_sum(td);
+            if (lane == 0) {
+              s_pcnt[s] = 0;  // the stage is refilled only after this warp releases it
+              epi.row(row, ts, td, pre, red);
+            }
+          } else if (lane == 0) {
+            s_abort = 1;
+            atomicExch(err, 1);
+          }
+        }
       }
       __syncwarp();
-      if ((tid & 31) == 0) mbar_arrive(&empty[s]);
+      if (lane == 0) mbar_arrive(&empty[s]);
     }
   }
   __syncthreads();
@@ -810,7 +839,6 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
   __shared__ __align__(8) uint64_t empty[kStages];
   __shared__ int4 meta[kStages];   // r0, r1, k0, k1
   __shared__ int4 xmeta[kStages];  // dictionary entries, zero code, tail entries, entries copied
-  __shared__ int s_ok[kStages];
   __shared__ volatile int s_abort;
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
@@ -866,6 +894,15 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
             xmeta[s] = make_int4(md.y, xd.y, xd.x >> 16, xd.w);
             const BlockRecord R = BlockRecord::of(m.y - m.x, m.w - m.z, md.y, true);
             const uint8_t* rec = X.rec + (size_t)xd.z * 16;
+            const int tail = xd.x >> 16;
+            if (tail > 0 && m.w - m.z <= kNnzCap && m.y - m.x <= kRowsPerBlock) {
+              // the 1-3 entries of x past its last 16-byte boundary, stored
+              // after the copied windows; the arrive below publishes them
+              asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+              VT* at = reinterpret_cast<VT*>(p_of(a_x(s))) + xd.w;
+              for (int t = 0; t < tail; ++t) at[t] = x[(X.ncols & ~3) + t];
+              asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            }
             if (m.w - m.z > kNnzCap || m.y - m.x > kRowsPerBlock) {
               // outside the x-staged invariant: complete the phase and flag it
               atomicExch(err, 2);
@@ -905,33 +942,26 @@ __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView
         mbar_wait_bounded(&full[j % kStages], (unsigned)(j / kStages) & 1u);
     }
   } else {
-    // ---- consumers: every block of this CTA in order
+    // ---- consumers: every block of this CTA in order. Each warp waits for
+    // the stages itself; a stage is refilled only after all consumer warps
+    // released it, so the phase a warp waits for is always the pending one.
     const int tl = A.tpr_log2;
-    const int ncols4 = X.ncols & ~3;
+    const int lane = tid & 31;
     int it = 0;
     for (int b = blockIdx.x; b < nblk; b += (int)gridDim.x, ++it) {
       const int s = it % kStages;
       const unsigned parity = (unsigned)(it / kStages) & 1u;
-      if (tid == 0) {
-        const int ok = (!s_abort && mbar_wait_bounded(&full[s], parity)) ? 1 : 0;
-        s_ok[s] = ok;
-        const int4 xm = xmeta[s];
-        if (ok && xm.z > 0) {
-          // the 1-3 entries past the last 16-byte boundary of x
-          VT* at = reinterpret_cast<VT*>(smem + (a_x(s) - sbase)) + xm.w;
-          for (int t = 0; t < xm.z; ++t) at[t] = x[ncols4 + t];
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        }
-      }
-      asm volatile("bar.sync 1, %0;" ::"n"(kXsConsumers) : "memory");
-      if (!s_ok[s]) {
-        if (tid == 0) {
+      int ok = 1;
+      if (lane == 0) ok = (!s_abort && mbar_wait_bounded(&full[s], parity)) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        if (lane == 0) {
           s_abort = 1;
           atomicExch(err, 1);
         }
         break;
       }
-      mbar_wait_bounded(&full[s], parity);  // completes at once; acquires the stage for this thread
+      mbar_wait_bounded(&full[s], parity);  // completes at once; acquires the stage for this lane
       const int4 m = meta[s];
       const int4 xm = xmeta[s];
       if (m.w - m.z <= kNnzCap && m.y - m.x <= kRowsPerBlock) {
