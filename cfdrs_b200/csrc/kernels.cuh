@@ -411,10 +411,17 @@ __device__ __forceinline__ void rows_from_stage(const Epi& epi, const Rp& srp, c
       if (k < re[q]) {
         const int c = sc.at(k, rb[q]);
         const VT v = sv[k];
-        if (OFFDIAG && c == row[q])
-          diag[q] = v;
-        else
-          sum[q] += v * (VT)__ldg(x + c);
+        // The gather is issued for the diagonal entry too (a valid, cached
+        // address) and the diagonal test selects instead of branching; the
+        // row sum sees the same terms in the same order.
+        const VT xv = (VT)__ldg(x + c);
+        if constexpr (OFFDIAG) {
+          const bool isd = (c == row[q]);
+          diag[q] = isd ? v : diag[q];
+          sum[q] = isd ? sum[q] : sum[q] + v * xv;
+        } else {
+          sum[q] += v * xv;
+        }
       }
     }
   }
@@ -812,10 +819,13 @@ __device__ __forceinline__ void rows_from_stage_xs(const Epi& epi, const uint16_
     for (int u = 0; u < kBatch; ++u) {
       if (kb + u * step < ke) {
         const VT xv = xr[se[c[u]]];
-        if (OFFDIAG && (int)c[u] == zq)
-          diag = v[u];
-        else
+        if constexpr (OFFDIAG) {
+          const bool isd = ((int)c[u] == zq);
+          diag = isd ? v[u] : diag;
+          sum = isd ? sum : sum + v[u] * xv;
+        } else {
           sum += v[u] * xv;
+        }
       }
     }
   }
