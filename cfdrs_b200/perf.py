@@ -48,7 +48,7 @@ def _paths(d):
 
 def main(argv=None):
     p = argparse.ArgumentParser()
-    p.add_argument("case", choices=["spmv", "solve", "levels", "batch", "adjoint", "gmres"])
+    p.add_argument("case", choices=["spmv", "solve", "levels", "batch", "adjoint", "gmres", "timeline"])
     p.add_argument("--fd-cells", type=int, default=64)
     p.add_argument("--systems", type=int, default=4096)
     p.add_argument("--n", type=int, default=128)
@@ -103,6 +103,8 @@ def main(argv=None):
             print(f"GMRES(30) {prec.name}: {r.device_ms:.1f} ms device, {r.iterations} iterations, "
                   f"{r.outer_iterations} refinements, final {r.final_residual_norm:.3e} <= {r.threshold:.3e}", flush=True)
         return 0
+    if a.case == "timeline":
+        return timeline_case(torch, cf, A, bd, amg, x, cfg)
     r1 = cf.cg_preconditioned(A, bd, amg, x, cfg, precision=cf.Precision.FP32_REFINE)
     x.zero_()
     r2 = cf.cg_preconditioned(A, bd, amg, x, cfg)
@@ -110,6 +112,80 @@ def main(argv=None):
     print(r1)
     print(r2)
     print(amg.statistics())
+    return 0
+
+
+def _short_kernel_name(name):
+    """k_spmv_pipe<f,f,true,Jacobi0,true> style names from demangled signatures."""
+    import re
+    name = re.sub(r"cfd::", "", name)
+    m = re.match(r"(?:void )?(?:\(anonymous namespace\)::)?(\w+)<(.*)>\(", name)
+    if not m:
+        m2 = re.match(r"(?:void )?(?:\(anonymous namespace\)::)?(\w+)", name)
+        return m2.group(1) if m2 else name[:40]
+    k, t = m.group(1), m.group(2)
+    t = re.sub(r"Epi(\w+)<(float|double)(, (\d))?>", lambda mm: mm.group(1) + (mm.group(4) or ""), t)
+    return f"{k}<{t.replace('float', 'f').replace('double', 'd').replace(' ', '')}>"
+
+
+def timeline_case(torch, cf, A, bd, amg, x, cfg):
+    """Kernel timeline (CUPTI activity records through torch.profiler) of one
+    FP32 + refinement and one FP64 AMG-PCG solve after warm-up: span, busy and
+    idle device time, the kernel families by total time, and the kernels of one
+    mid-solve PCG iteration in launch order. Durations are those of the plain
+    run (no replay, no serialisation)."""
+    import collections
+    import json
+    import os
+    import tempfile
+
+    from torch.profiler import ProfilerActivity, profile
+
+    def solve(prec):
+        x.zero_()
+        return cf.cg_preconditioned(A, bd, amg, x, cfg, precision=prec)
+
+    precs = (("FP32+refinement", cf.Precision.FP32_REFINE), ("FP64", cf.Precision.FP64))
+    for _ in range(3):
+        for _, p in precs:
+            solve(p)
+    torch.cuda.synchronize()
+    spans = []
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for _, p in precs:
+            torch.cuda.synchronize()
+            spans.append(solve(p))
+            torch.cuda.synchronize()
+    fd, path = tempfile.mkstemp(suffix=".json")
+    os.close(fd)
+    try:
+        prof.export_chrome_trace(path)
+        with open(path) as f:
+            events = [e for e in json.load(f)["traceEvents"] if e.get("cat") == "kernel"]
+    finally:
+        os.unlink(path)
+    events.sort(key=lambda e: e["ts"])
+    starts = [i for i, e in enumerate(events) if "at::native" in e["name"]]  # x.zero_() opens each solve
+    parts = [events[starts[0] + 1:starts[1]], events[starts[1] + 1:]]
+    for (name, _), rep, ev in zip(precs, spans, parts):
+        t0, t1 = ev[0]["ts"], ev[-1]["ts"] + ev[-1]["dur"]
+        busy = sum(e["dur"] for e in ev)
+        print(f"== {name}: {rep.iterations} iterations, {rep.outer_iterations} refinements; {len(ev)} kernels, "
+              f"span {(t1 - t0) / 1e3:.2f} ms, busy {busy / 1e3:.2f} ms, idle {(t1 - t0 - busy) / 1e3:.2f} ms")
+        grp = collections.defaultdict(lambda: [0, 0.0])
+        for e in ev:
+            g = grp[_short_kernel_name(e["name"])]
+            g[0] += 1
+            g[1] += e["dur"]
+        for k, (c, t) in sorted(grp.items(), key=lambda kv: -kv[1][1])[:16]:
+            print(f"   {k:48s} {c:5d} launches {t / 1e3:8.3f} ms  avg {t / c:7.1f} us")
+        upd = [i for i, e in enumerate(ev) if "k_p_update" in e["name"]]
+        if len(upd) >= 2:
+            lo, hi = upd[len(upd) // 2 - 1], upd[len(upd) // 2]
+            print(f"   one PCG iteration ({hi - lo} kernels, {(ev[hi]['ts'] - ev[lo]['ts']) / 1e3:.3f} ms):")
+            for e in ev[lo:hi]:
+                grid = e.get("args", {}).get("grid", ["?"])[0]
+                print(f"     {_short_kernel_name(e['name']):48s} {e['dur']:8.1f} us  grid {grid}")
     return 0
 
 
