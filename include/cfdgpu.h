@@ -189,6 +189,12 @@ typedef struct {
 
 typedef struct cfd_amg cfd_amg;
 cfd_status cfd_amg_setup(cfd_csr* a, const cfd_amg_config* cfg, cfd_amg** out);
+/* New fine values of the setup's pattern (a on the hierarchy's context): the
+ * Galerkin operators (R_l A_l) P_l, level diagonals, FP32 copies and the dense
+ * coarsest inverse are re-formed on the device with P and R kept
+ * (amg.rs:179-214), in the host product's summation order. CFD_ERR_DIM for
+ * another pattern size, CFD_ERR_CONFIG for a singular coarsest operator
+ * (CFD_COARSE_DENSE). */
 cfd_status cfd_amg_recompute(cfd_amg* amg, cfd_csr* a);
 /* z = M^-1 r (one V-cycle from z = 0), device pointers, FP64. */
 cfd_status cfd_amg_apply(cfd_amg* amg, const double* r_dev, double* z_dev);
@@ -198,7 +204,8 @@ cfd_status cfd_amg_stats(const cfd_amg* amg, cfd_amg_stats_t* out);
  * No reference counterpart (CFDrs has one CSR SpMV). */
 cfd_status cfd_amg_set_path(cfd_amg* amg, int32_t fp32, int32_t path);
 /* Copy level `level`'s operator (which: 0 = A_l, 1 = P_l, 2 = R_l) to host
- * arrays; pass NULL arrays to query sizes only. */
+ * arrays; pass NULL arrays to query sizes only. After cfd_amg_recompute the
+ * values of A_l are read back from the device on the first such call. */
 cfd_status cfd_amg_level(const cfd_amg* amg, int level, int which, int64_t* nrows, int64_t* ncols,
                          int64_t* nnz, int64_t* row_ptr, int64_t* col, double* val);
 cfd_status cfd_amg_destroy(cfd_amg* amg);
@@ -256,7 +263,7 @@ cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, con
 cfd_status cfd_pattern_outer(cfd_csr* a, const double* lambda_dev, const double* x_dev, double scale,
                              double* g_dev);
 /* Replace A's values from device memory (same pattern); the host copy used by
- * AMG setup/recompute is refreshed too. */
+ * AMG setup is refreshed too (cfd_amg_recompute reads the device values). */
 cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev);
 
 /* ---- batched small systems --------------------------------------------
