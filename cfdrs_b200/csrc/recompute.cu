@@ -34,7 +34,10 @@ cfd_status dalloc(T** p, int64_t n) {
   return CFD_OK;
 }
 
-int grid_for(int64_t n, int per) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + per - 1) / per, 148 * 16)); }
+// Blocks for n items at `per` items per block, capped at 16 blocks per SM.
+int grid_for(const cfd_context* ctx, int64_t n, int per) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + per - 1) / per, (int64_t)ctx->num_sms * 16));
+}
 
 constexpr int kGjMaxRows = 8192;  // W, the pivot rows and the row tables stay within one SM's shared memory
 
@@ -376,7 +379,7 @@ cfd_status dense_inverse_device(cfd_context* ctx, int64_t n64, const int* rp, co
     if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(bar, 0, sizeof(unsigned), s);
     if (e == cudaSuccess) {
-      k_gj_fill<<<grid_for(n, 256), 256, 0, s>>>(n, ldw, rp, ci, v, W);
+      k_gj_fill<<<grid_for(ctx, n, 256), 256, 0, s>>>(n, ldw, rp, ci, v, W);
       e = cudaGetLastError();
     }
     g.W = W;
@@ -449,21 +452,27 @@ cfd_status amg_recompute_device(cfd_amg* amg, const cfd_csr* a) {
   cudaStream_t s = amg->ctx->stream;
   const size_t L = amg->dev.size();
   CFD_TRY(ensure_ra(amg, s));
+  const int64_t nc = amg->dev[L - 1].A.nrows;
+  if (amg->cfg.coarse_solve == CFD_COARSE_DENSE && nc > kGjMaxRows) {
+    set_error("dense coarsest inverse: %lld rows exceed %d", (long long)nc, kGjMaxRows);
+    return CFD_ERR_CONFIG;
+  }
   DevMat& A0 = amg->dev[0].A;
+  amg->host_values_stale = true;  // from here on the device holds the newer values
   CFD_TRY_CUDA(cudaMemcpyAsync(A0.v64, a->dev.v64, A0.nnz * sizeof(double), cudaMemcpyDeviceToDevice, s));
   for (size_t l = 0; l + 1 < L; ++l) {
     DevLevel& D = amg->dev[l];
     DevMat& Ac = amg->dev[l + 1].A;
-    k_spgemm_fixed<<<grid_for(D.ra.nrows, 8), 256, 0, s>>>(D.ra.nrows, D.ra.rp, D.ra.ci, D.R.rp, D.R.col, D.R.v64,
-                                                           D.A.rp, D.A.col, D.A.v64, D.ra.v);
-    k_spgemm_fixed<<<grid_for(Ac.nrows, 8), 256, 0, s>>>(Ac.nrows, Ac.rp, Ac.col, D.ra.rp, D.ra.ci, D.ra.v, D.P.rp,
-                                                         D.P.col, D.P.v64, Ac.v64);
+    k_spgemm_fixed<<<grid_for(amg->ctx, D.ra.nrows, 8), 256, 0, s>>>(
+        D.ra.nrows, D.ra.rp, D.ra.ci, D.R.rp, D.R.col, D.R.v64, D.A.rp, D.A.col, D.A.v64, D.ra.v);
+    k_spgemm_fixed<<<grid_for(amg->ctx, Ac.nrows, 8), 256, 0, s>>>(
+        Ac.nrows, Ac.rp, Ac.col, D.ra.rp, D.ra.ci, D.ra.v, D.P.rp, D.P.col, D.P.v64, Ac.v64);
     CFD_TRY_CUDA(cudaGetLastError());
   }
   for (size_t l = 0; l < L; ++l) {
     DevLevel& D = amg->dev[l];
-    if (D.A.v32) k_cast32<<<grid_for(D.A.nnz, 256), 256, 0, s>>>(D.A.nnz, D.A.v64, D.A.v32);
-    k_diag<<<grid_for(D.A.nrows, 256), 256, 0, s>>>(D.A.nrows, D.A.rp, D.A.col, D.A.v64, D.d64, D.d32);
+    if (D.A.v32) k_cast32<<<grid_for(amg->ctx, D.A.nnz, 256), 256, 0, s>>>(D.A.nnz, D.A.v64, D.A.v32);
+    k_diag<<<grid_for(amg->ctx, D.A.nrows, 256), 256, 0, s>>>(D.A.nrows, D.A.rp, D.A.col, D.A.v64, D.d64, D.d32);
     CFD_TRY_CUDA(cudaGetLastError());
   }
   if (amg->cfg.coarse_solve == CFD_COARSE_DENSE) {
@@ -480,7 +489,6 @@ cfd_status amg_recompute_device(cfd_amg* amg, const cfd_csr* a) {
     amg->coarse_n = Ac.nrows;
   }
   CFD_TRY_CUDA(cudaStreamSynchronize(s));
-  amg->host_values_stale = true;
   return CFD_OK;
 }
 

@@ -194,7 +194,9 @@ cfd_status cfd_amg_setup(cfd_csr* a, const cfd_amg_config* cfg, cfd_amg** out);
  * coarsest inverse are re-formed on the device with P and R kept
  * (amg.rs:179-214), in the host product's summation order. CFD_ERR_DIM for
  * another pattern size, CFD_ERR_CONFIG for a singular coarsest operator
- * (CFD_COARSE_DENSE). */
+ * (CFD_COARSE_DENSE); the level operators then hold the new values while the
+ * coarsest inverse is still the previous one, so recompute with nonsingular
+ * values before the next apply or solve. */
 cfd_status cfd_amg_recompute(cfd_amg* amg, cfd_csr* a);
 /* z = M^-1 r (one V-cycle from z = 0), device pointers, FP64. */
 cfd_status cfd_amg_apply(cfd_amg* amg, const double* r_dev, double* z_dev);
