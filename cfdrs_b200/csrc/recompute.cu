@@ -8,9 +8,8 @@
 //    the terms per column) does, so device and host recomputes agree bit for
 //    bit.
 //  * The dense coarsest inverse is Gauss-Jordan with partial pivoting, the
-//    host's dense_inverse step for step: per pivot one CTA finds the pivot
-//    (first maximum), swaps, scales and saves the pivot column, then one grid
-//    eliminates every other row.
+//    host's dense_inverse operation for operation, in one cooperative launch
+//    with one grid barrier per pivot (k_gj_coop, below).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,7 +38,7 @@ int grid_for(const cfd_context* ctx, int64_t n, int per) {
   return (int)std::max<int64_t>(1, std::min<int64_t>((n + per - 1) / per, (int64_t)ctx->num_sms * 16));
 }
 
-constexpr int kGjMaxRows = 8192;  // W, the pivot rows and the row tables stay within one SM's shared memory
+constexpr int kGjMaxRows = 8192;  // the staged pivot rows and the row tables fit one CTA's shared memory
 
 // C = A B on C's pattern.
 __global__ void __launch_bounds__(256) k_spgemm_fixed(int64_t nrows, const int* __restrict__ c_rp,
