@@ -13,8 +13,8 @@ from .krylov import (  # noqa: F401
     gmres_width, interpret,
 )
 from .multigrid import (  # noqa: F401
-    AMGConfig, AMGStatistics, AlgebraicMultigrid, CoarseOrder, CoarseSolve, CoarseningStrategy, IdentityPreconditioner,
-    InterpolationStrategy, JacobiPreconditioner, SmootherType,
+    AMGConfig, AMGStatistics, AlgebraicMultigrid, CoarseOrder, CoarseSolve, CoarseningStrategy, HostHierarchy,
+    IdentityPreconditioner, InterpolationStrategy, JacobiPreconditioner, SmootherType,
 )
 
 __version__ = "0.1.0"

@@ -662,9 +662,7 @@ void cfd_amg_config_default(cfd_amg_config* c) {
   c->reserved = 0;
 }
 
-cfd_status cfd_amg_setup(cfd_csr* a, const cfd_amg_config* cfg, cfd_amg** out) {
-  if (!a || !cfg || !out) return CFD_ERR_STATE;
-  *out = nullptr;
+static cfd_status check_amg_config(const cfd_amg_config* cfg) {
   if (cfg->max_levels < 1 || cfg->max_levels > 16 || cfg->smoother != CFD_SMOOTH_JACOBI ||
       cfg->pre_smooth < 0 || cfg->post_smooth < 0 || !(cfg->strength_threshold >= 0.0) ||
       !std::isfinite(cfg->relaxation) || cfg->coarsening < 0 || cfg->coarsening > 2 || cfg->interpolation < 0 ||
@@ -672,6 +670,22 @@ cfd_status cfd_amg_setup(cfd_csr* a, const cfd_amg_config* cfg, cfd_amg** out) {
     set_error("invalid AMG configuration");
     return CFD_ERR_CONFIG;
   }
+  return CFD_OK;
+}
+
+// A hierarchy handle built by cfd_amg_setup_host has no context and no device data.
+static cfd_status need_device_hierarchy(const cfd_amg* amg, const char* what) {
+  if (!amg->ctx) {
+    set_error("%s: the hierarchy was built on the host only (cfd_amg_setup_host)", what);
+    return CFD_ERR_STATE;
+  }
+  return CFD_OK;
+}
+
+cfd_status cfd_amg_setup(cfd_csr* a, const cfd_amg_config* cfg, cfd_amg** out) {
+  if (!a || !cfg || !out) return CFD_ERR_STATE;
+  *out = nullptr;
+  CFD_TRY(check_amg_config(cfg));
   if (a->host.nrows != a->host.ncols) {
     set_error("AMG needs a square matrix");
     return CFD_ERR_DIM;
@@ -694,9 +708,34 @@ cfd_status cfd_amg_setup(cfd_csr* a, const cfd_amg_config* cfg, cfd_amg** out) {
   return CFD_OK;
 }
 
+cfd_status cfd_amg_setup_host(int64_t n, const int64_t* row_ptr, const int64_t* col, const double* val,
+                              const cfd_amg_config* cfg, cfd_amg** out) {
+  if (!cfg || !out) return CFD_ERR_STATE;
+  *out = nullptr;
+  CFD_TRY(check_amg_config(cfg));
+  if (n < 0 || !row_ptr) {
+    set_error("invalid CSR arguments");
+    return CFD_ERR_DIM;
+  }
+  const int64_t nnz = row_ptr[n];
+  CFD_TRY(validate_csr(n, n, nnz, row_ptr, nullptr, col));
+  if (nnz > 0 && !val) {
+    set_error("null value array");
+    return CFD_ERR_DIM;
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  cfd_amg* amg = new cfd_amg;
+  amg->cfg = *cfg;
+  amg->host = build_hierarchy(host_from(n, n, nnz, row_ptr, nullptr, col, val), *cfg);
+  amg->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  *out = amg;
+  return CFD_OK;
+}
+
 cfd_status cfd_amg_recompute(cfd_amg* amg, cfd_csr* a) {
   if (!amg || !a) return CFD_ERR_STATE;
   if (amg->host.empty()) return CFD_ERR_STATE;
+  CFD_TRY(need_device_hierarchy(amg, "cfd_amg_recompute"));
   if (a->host.nrows != amg->host[0].A.nrows || a->host.nnz() != amg->host[0].A.nnz()) {
     set_error("recompute needs the hierarchy's sparsity pattern");
     return CFD_ERR_DIM;
@@ -712,6 +751,7 @@ cfd_status cfd_amg_recompute(cfd_amg* amg, cfd_csr* a) {
 
 cfd_status cfd_amg_apply(cfd_amg* amg, const double* r, double* z) {
   if (!amg || !r || !z) return CFD_ERR_STATE;
+  CFD_TRY(need_device_hierarchy(amg, "cfd_amg_apply"));
   std::lock_guard<std::mutex> g(amg->ctx->mu);
   CFD_TRY_CUDA(cudaSetDevice(amg->ctx->device));
   CFD_TRY(amg_apply_fp64(amg, r, z));
@@ -727,6 +767,7 @@ cfd_status cfd_amg_set_path(cfd_amg* amg, int32_t fp32, int32_t path) {
     set_error("cfd_amg_set_path: unknown pipeline %d", path);
     return CFD_ERR_CONFIG;
   }
+  CFD_TRY(need_device_hierarchy(amg, "cfd_amg_set_path"));
   std::lock_guard<std::mutex> g(amg->ctx->mu);
   for (DevLevel& L : amg->dev)
     for (DevMat* m : {&L.A, &L.P, &L.R}) {
@@ -780,9 +821,11 @@ cfd_status cfd_amg_level(const cfd_amg* amg, int level, int which, int64_t* nrow
 
 cfd_status cfd_amg_destroy(cfd_amg* amg) {
   if (!amg) return CFD_OK;
-  cudaSetDevice(amg->ctx->device);
-  cudaStreamSynchronize(amg->ctx->stream);
-  amg_free_device(amg);
+  if (amg->ctx) {
+    cudaSetDevice(amg->ctx->device);
+    cudaStreamSynchronize(amg->ctx->stream);
+    amg_free_device(amg);
+  }
   delete amg;
   return CFD_OK;
 }

@@ -1012,6 +1012,10 @@ cfd_status check_precond(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg)
       set_error("AMG preconditioner requested without an AMG handle");
       return CFD_ERR_CONFIG;
     }
+    if (!amg->ctx) {
+      set_error("AMG preconditioner: the hierarchy was built on the host only (cfd_amg_setup_host)");
+      return CFD_ERR_STATE;
+    }
     if (amg->dev.empty() || amg->dev[0].A.nrows != a->dev.nrows) {
       set_error("AMG hierarchy does not match the matrix (%lld rows)", (long long)a->dev.nrows);
       return CFD_ERR_DIM;

@@ -136,28 +136,77 @@ class AlgebraicMultigrid:
         _lib.check(_lib.load().cfd_amg_set_path(self.h, 1 if fp32 else 0, DeviceCsr.PATHS[path]))
 
     def statistics(self) -> AMGStatistics:
-        s = _lib.AmgStatsC()
-        _lib.check(_lib.load().cfd_amg_stats(self.h, C.byref(s)))
-        n = s.num_levels
-        return AMGStatistics(n, list(s.level_rows[:min(n, 16)]), list(s.level_nnz[:min(n, 16)]),
-                             s.operator_complexity, s.grid_complexity, s.setup_seconds)
+        return _statistics(self.h)
 
     def level(self, level: int, which: int = 0) -> CsrMatrix:
         """Host copy of level ``level``'s A (0), P (1) or R (2)."""
-        L = _lib.load()
-        nr, nc, nnz = C.c_int64(), C.c_int64(), C.c_int64()
-        _lib.check(L.cfd_amg_level(self.h, level, which, C.byref(nr), C.byref(nc), C.byref(nnz),
-                                   None, None, None))
-        rp = np.empty(nr.value + 1, np.int64)
-        col = np.empty(nnz.value, np.int64)
-        val = np.empty(nnz.value, np.float64)
-        _lib.check(L.cfd_amg_level(self.h, level, which, None, None, None, rp.ctypes.data_as(C.c_void_p),
-                                   col.ctypes.data_as(C.c_void_p), val.ctypes.data_as(C.c_void_p)))
-        return CsrMatrix(rp, col, val, (nr.value, nc.value))
+        return _level(self.h, level, which)
 
     @property
     def num_levels(self) -> int:
         return self.statistics().num_levels
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            try:
+                _lib.load().cfd_amg_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+
+def _statistics(h) -> AMGStatistics:
+    s = _lib.AmgStatsC()
+    _lib.check(_lib.load().cfd_amg_stats(h, C.byref(s)))
+    n = s.num_levels
+    return AMGStatistics(n, list(s.level_rows[:min(n, 16)]), list(s.level_nnz[:min(n, 16)]),
+                         s.operator_complexity, s.grid_complexity, s.setup_seconds)
+
+
+def _level(h, level: int, which: int) -> CsrMatrix:
+    L = _lib.load()
+    nr, nc, nnz = C.c_int64(), C.c_int64(), C.c_int64()
+    _lib.check(L.cfd_amg_level(h, level, which, C.byref(nr), C.byref(nc), C.byref(nnz), None, None, None))
+    rp = np.empty(nr.value + 1, np.int64)
+    col = np.empty(nnz.value, np.int64)
+    val = np.empty(nnz.value, np.float64)
+    _lib.check(L.cfd_amg_level(h, level, which, None, None, None, rp.ctypes.data_as(C.c_void_p),
+                               col.ctypes.data_as(C.c_void_p), val.ctypes.data_as(C.c_void_p)))
+    return CsrMatrix(rp, col, val, (nr.value, nc.value))
+
+
+class HostHierarchy:
+    """The AMG hierarchy of ``AlgebraicMultigrid::new`` built on the host only
+    (``cfd_amg_setup_host``): the same levels as :class:`AlgebraicMultigrid`
+    without a device, for inspecting or serialising a hierarchy and for checking
+    the setup where no GPU is present. It cannot precondition a solve."""
+
+    def __init__(self, matrix, config: AMGConfig | None = None):
+        m = matrix if isinstance(matrix, CsrMatrix) else CsrMatrix.from_scipy(matrix)
+        if m.nrows != m.ncols:
+            raise _lib.CfdError(1, "AMG needs a square matrix")
+        self.config = config or AMGConfig()
+        rp = np.ascontiguousarray(m.row_ptr, dtype=np.int64)
+        col = np.ascontiguousarray(m.col, dtype=np.int64)
+        val = np.ascontiguousarray(m.val, dtype=np.float64)
+        h = C.c_void_p()
+        cfg = self.config.to_c()
+        _lib.check(_lib.load().cfd_amg_setup_host(m.nrows, rp.ctypes.data_as(C.c_void_p),
+                                                  col.ctypes.data_as(C.c_void_p), val.ctypes.data_as(C.c_void_p),
+                                                  C.byref(cfg), C.byref(h)))
+        self.h = h
+
+    def statistics(self) -> AMGStatistics:
+        return _statistics(self.h)
+
+    @property
+    def num_levels(self) -> int:
+        return self.statistics().num_levels
+
+    def level(self, level: int, which: int = 0) -> CsrMatrix:
+        """Level ``level``'s A (0), P (1) or R (2)."""
+        return _level(self.h, level, which)
 
     def __del__(self):
         h = getattr(self, "h", None)

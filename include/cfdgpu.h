@@ -201,6 +201,14 @@ cfd_status cfd_amg_recompute(cfd_amg* amg, cfd_csr* a);
 /* z = M^-1 r (one V-cycle from z = 0), device pointers, FP64. */
 cfd_status cfd_amg_apply(cfd_amg* amg, const double* r_dev, double* z_dev);
 cfd_status cfd_amg_stats(const cfd_amg* amg, cfd_amg_stats_t* out);
+/* The same hierarchy (AlgebraicMultigrid::setup, amg.rs:217-288, the host
+ * part of cfd_amg_setup) built on the host only, from an n x n CSR with
+ * int64 indices: no context, no device memory, no CUDA call. The handle
+ * answers cfd_amg_stats, cfd_amg_level and cfd_amg_destroy; calls that need
+ * the device return CFD_ERR_STATE. For callers that inspect or serialise the
+ * hierarchy, and for checking the setup without a GPU. */
+cfd_status cfd_amg_setup_host(int64_t n, const int64_t* row_ptr, const int64_t* col, const double* val,
+                              const cfd_amg_config* cfg, cfd_amg** out);
 /* SpMV pipeline of every level operator (A, P, R) in one precision, as
  * cfd_csr_set_path; an operator not eligible for the pipeline keeps AUTO.
  * No reference counterpart (CFDrs has one CSR SpMV). */
