@@ -571,10 +571,11 @@ std::vector<HostLevel> build_hierarchy(const HostCsr& a, const cfd_amg_config& c
     HostCsr ac = spgemm(spgemm(r, cur), p);
     levels.back().P = std::move(p);
     levels.back().R = std::move(r);
+    const int64_t n_cur = cur.nrows;  // `cur` refers into `levels`, which the push_back may move
     HostLevel next;
     next.A = std::move(ac);
     levels.push_back(std::move(next));
-    if (nc == 0 || nc >= cur.nrows) break;
+    if (nc == 0 || nc >= n_cur) break;
   }
   return levels;
 }

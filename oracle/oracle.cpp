@@ -792,10 +792,11 @@ or_amg* or_amg_setup(const or_csr* a, const or_amg_config* cfg) {
     or_csr r = transpose(p);
     or_csr ra = spgemm(r, cur);
     or_csr ac = spgemm(ra, p);
+    const int64_t n_cur = cur.nrows;  // `cur` refers into h->A, which the push_back may move
     h->P.push_back(std::move(p));
     h->R.push_back(std::move(r));
     h->A.push_back(std::move(ac));
-    if (nc == 0 || nc >= cur.nrows) break;  // no progress: stop coarsening
+    if (nc == 0 || nc >= n_cur) break;  // no progress: stop coarsening
   }
   if (cfg->coarse_solve == OR_COARSE_DENSE) lu_factor(h->A.back(), h->lu, h->piv);
   size_t L = h->A.size();
