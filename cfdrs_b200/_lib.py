@@ -10,7 +10,8 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libcfdgpu.so")
+# CFDGPU_LIB selects another build of the same library (e.g. the sanitizer build).
+LIB_PATH = os.environ.get("CFDGPU_LIB") or os.path.join(_HERE, "libcfdgpu.so")
 
 CFD_OK = 0
 STATUS_NAMES = {0: "CFD_OK", 1: "CFD_ERR_DIM", 2: "CFD_ERR_CONFIG", 3: "CFD_ERR_CUDA",

@@ -14,7 +14,8 @@ from dataclasses import dataclass
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+# CFD_ORACLE_LIB selects another build of the oracle (e.g. the sanitizer build).
+_LIB_PATH = os.environ.get("CFD_ORACLE_LIB") or os.path.join(_HERE, "liboracle.so")
 
 RUGE_STUEBEN, AGGREGATION, PMIS = 0, 1, 2
 SMOOTH_JACOBI, SMOOTH_GS, SMOOTH_SGS = 0, 1, 2
@@ -24,8 +25,10 @@ TERMINATIONS = ["Converged", "InitialResidual", "MaxIterations", "Breakdown", "N
 
 
 def build() -> str:
-    """Compile liboracle.so with the committed Makefile (no-op when up to date)."""
-    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    """Compile liboracle.so with the committed Makefile (no-op when up to date,
+    and when CFD_ORACLE_LIB names a build made elsewhere)."""
+    if not os.environ.get("CFD_ORACLE_LIB"):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
 
 
