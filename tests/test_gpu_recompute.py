@@ -160,3 +160,19 @@ def test_recompute_then_fp32_refinement(cuda):
     r32 = cf.cg_preconditioned(A2, b2, amg, x32, conf, precision=cf.Precision.FP32_REFINE)
     assert r64.termination == cf.Termination.CONVERGED and r32.termination == cf.Termination.CONVERGED
     assert np.linalg.norm(x32 - x64) <= 1e-8 * np.linalg.norm(x64)
+
+
+def test_recompute_large_coarsest_inverse(cuda):
+    """A 3843-row coarsest operator: more rows than the cooperative inverse
+    has warps (148 SMs x 16), so warps take several rows per pivot step. A
+    recompute with the setup's values reproduces the host inverse: the V-cycle
+    output is unchanged bit for bit."""
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    A = P.poisson_3d_variable(36, 4.0, 1.0, seed=2)[0]
+    amg = cf.AlgebraicMultigrid(A, pressure_cfg(4096))
+    assert amg.statistics().level_sizes[-1] > 148 * 16
+    r = np.random.default_rng(3).uniform(-1, 1, A.nrows)
+    z0 = amg.apply_to(r)
+    amg.recompute(A)
+    np.testing.assert_array_equal(amg.apply_to(r), z0)
