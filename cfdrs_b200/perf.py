@@ -238,7 +238,7 @@ def adjoint_case(a):
     from cfdrs_b200.adjoint import (SparseSolver, column_loss, darcy_2d_pattern, darcy_2d_torch,
                                     loss_column_index, sparse_solve)
     sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
-    import adjoint_cpu as AC  # the checker
+    import adjoint_cpu as AC  # the oracle's adjoint
 
     n = a.n
     theta = P.gaussian_random_field((n, n), 16.0, 0.5, seed=0)

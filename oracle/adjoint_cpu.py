@@ -1,6 +1,6 @@
 """FP64 CPU adjoint of the 2-D Darcy column loss (TEST INFRASTRUCTURE ONLY).
 
-The checker for cfdrs_b200.adjoint: forward and adjoint by sparse direct
+The oracle for cfdrs_b200.adjoint: forward and adjoint by sparse direct
 solves (scipy SuperLU), and dL/dtheta from the face-by-face adjoint formula
 derived by hand -- an independent route from the device path, which
 differentiates its torch assembly automatically.

@@ -1,7 +1,7 @@
 /*
  * CPU oracle for the CFDrs preconditioned sparse linear-solve path.
  *
- * TEST INFRASTRUCTURE ONLY. This library is the checker used by tests/,
+ * TEST INFRASTRUCTURE ONLY. This library is the oracle used by tests/,
  * __graft_entry__.smoke() and the CPU-baseline leg of bench.py. The product
  * library (cfdrs_b200/libcfdgpu.so) never links, loads or calls it.
  *

@@ -1,7 +1,7 @@
 """ctypes front end of the CPU oracle (oracle/liboracle.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
-CPU-baseline leg of bench.py as the checker; the product package never
+CPU-baseline leg of bench.py as the oracle; the product package never
 imports it. The algorithms and their reference citations are in oracle.h.
 """
 from __future__ import annotations

@@ -183,7 +183,7 @@ def test_equilibrated_pcg_networks(oracle):
 
 
 def test_cpu_adjoint_against_fd_and_assembly():
-    """The CPU adjoint checker: its assembly equals problems.darcy_2d and the
+    """The CPU adjoint oracle: its assembly equals problems.darcy_2d and the
     torch assembly, and its hand-derived gradient matches central differences."""
     import adjoint_cpu as AC
     import torch
