@@ -48,7 +48,7 @@ def _paths(d):
 
 def main(argv=None):
     p = argparse.ArgumentParser()
-    p.add_argument("case", choices=["spmv", "solve", "levels", "batch", "adjoint", "gmres", "timeline"])
+    p.add_argument("case", choices=["spmv", "solve", "levels", "batch", "adjoint", "gmres", "timeline", "configs"])
     p.add_argument("--systems", type=int, default=4096)
     p.add_argument("--n", type=int, default=128)
     p.add_argument("--reps", type=int, default=20)
@@ -63,6 +63,8 @@ def main(argv=None):
         return batch_case(a)
     if a.case == "adjoint":
         return adjoint_case(a)
+    if a.case == "configs":
+        return configs_case(a)
     A, b, _ = P.poisson_3d_variable(a.n, 8.0, 1.0, seed=0)
     ctx = context(0)
     ctx.set_stream(torch.cuda.current_stream().cuda_stream)
@@ -185,6 +187,79 @@ def timeline_case(torch, cf, A, bd, amg, x, cfg):
             for e in ev[lo:hi]:
                 grid = e.get("args", {}).get("grid", ["?"])[0]
                 print(f"     {_short_kernel_name(e['name']):48s} {e['dur']:8.1f} us  grid {grid}")
+    return 0
+
+
+def configs_case(a):
+    """The two plain-FP64 configurations beside the mixed-precision workload.
+    C1: 2-D pressure Poisson on 128^2 cells (homogeneous Dirichlet walls,
+    b ~ U[-1, 1]), Jacobi-PCG from zero to relative residual 1e-8. C2: 3-D
+    constant-coefficient Poisson on n^3 cells (Dirichlet x = 0, 1, Neumann
+    elsewhere), AMG-PCG V(1,1), damped Jacobi w = 2/3, coarsest <= 4096, FP64 to
+    1e-8, with the FP32 + FP64 refinement solve beside it. Device time per
+    solve (best of 5, events on the solve stream), iterations, the true
+    relative residual, and the AMG setup time."""
+    import time
+
+    import numpy as np
+    import torch
+
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.device import context
+
+    ctx = context(0)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+
+    def best_of(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = _events(torch)
+        best, rep = None, None
+        for _ in range(reps):
+            e0.record(stream)
+            rep = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1)
+            best = t if best is None else min(best, t)
+        return best, rep
+
+    A, b = P.poisson_2d_dirichlet(128, seed=0)
+    bd = torch.as_tensor(b, device="cuda")
+    x = torch.zeros_like(bd)
+    jac = cf.JacobiPreconditioner(A)
+    cfg = cf.IterativeSolverConfig(0.0, 1e-8, 20000)
+
+    def c1():
+        x.zero_()
+        return cf.cg_preconditioned(A, bd, jac, x, cfg)
+
+    ms, rep = best_of(c1)
+    rel = np.linalg.norm(b - A.matvec(x.cpu().numpy())) / np.linalg.norm(b)
+    print(f"C1 2-D Poisson 128^2 ({A.nrows} unknowns, {A.nnz} nnz), Jacobi-PCG FP64 to 1e-8: {ms:.3f} ms, "
+          f"{rep.iterations} iterations, true relative residual {rel:.2e}", flush=True)
+
+    A, b = P.poisson_3d_fv(a.n, None, seed=0)
+    t0 = time.perf_counter()
+    amg = cf.AlgebraicMultigrid(A, cf.AMGConfig.pressure_poisson(), ctx=ctx)
+    setup_s = time.perf_counter() - t0
+    st = amg.statistics()
+    bd = torch.as_tensor(b, device="cuda")
+    x = torch.zeros_like(bd)
+    for name, prec in (("FP64", cf.Precision.FP64), ("FP32+refinement", cf.Precision.FP32_REFINE)):
+        def c2():
+            x.zero_()
+            return cf.cg_preconditioned(A, bd, amg, x, cfg, precision=prec)
+
+        ms, rep = best_of(c2)
+        rel = np.linalg.norm(b - A.matvec(x.double().cpu().numpy())) / np.linalg.norm(b)
+        print(f"C2 3-D Poisson k = 1, {a.n}^3 ({A.nrows} unknowns, {A.nnz} nnz), AMG-PCG {name} to 1e-8: "
+              f"{ms:.2f} ms, {rep.iterations} iterations, {rep.outer_iterations} refinements, "
+              f"true relative residual {rel:.2e}", flush=True)
+    print(f"   AMG setup {setup_s:.1f} s, {st.num_levels} levels {st.level_sizes}, "
+          f"operator complexity {st.operator_complexity:.3f}", flush=True)
     return 0
 
 
