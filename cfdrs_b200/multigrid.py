@@ -107,10 +107,13 @@ class AlgebraicMultigrid:
     new = classmethod(lambda cls, matrix, config=None: cls(matrix, config))
 
     def recompute(self, matrix) -> None:
-        """Re-form the Galerkin operators for new fine-level values (same pattern)."""
-        if isinstance(matrix, CsrMatrix):
-            self.matrix.update_values(matrix.val)
-        _lib.check(_lib.load().cfd_amg_recompute(self.h, self.matrix.h))
+        """``AlgebraicMultigrid::recompute`` (amg.rs:179-214): re-form the
+        Galerkin operators for the values of ``matrix`` (the setup's sparsity
+        pattern), P and R kept. ``matrix`` is a host matrix (its device copy is
+        made once, as for a solve) or a DeviceCsr on this hierarchy's context;
+        the values of no other matrix change."""
+        dm = device_matrix(matrix, self.ctx)
+        _lib.check(_lib.load().cfd_amg_recompute(self.h, dm.h))
 
     def apply_to(self, r, z=None):
         """z = M^-1 r (one V-cycle from zero). Host numpy in/out, or CUDA torch tensors."""

@@ -176,3 +176,20 @@ def test_recompute_large_coarsest_inverse(cuda):
     z0 = amg.apply_to(r)
     amg.recompute(A)
     np.testing.assert_array_equal(amg.apply_to(r), z0)
+
+
+def test_recompute_leaves_other_matrices_alone(cuda):
+    """A recompute reads the given matrix's values and changes no other
+    matrix: after recomputing for A2, a solve with A1 still solves A1 (here
+    with the hierarchy of A2 as its preconditioner)."""
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    A1, b1, _ = P.poisson_3d_variable(16, 4.0, 1.0, seed=1)
+    A2 = P.poisson_3d_variable(16, 3.0, 1.5, seed=7)[0]
+    amg = cf.AlgebraicMultigrid(A1, pressure_cfg(100))
+    amg.recompute(A2)
+    np.testing.assert_array_equal(amg.level(0, 0).val, A2.val)
+    x = np.zeros(A1.nrows)
+    rep = cf.cg_preconditioned(A1, b1, amg, x, cf.IterativeSolverConfig(0.0, 1e-10, 1000))
+    assert rep.termination == cf.Termination.CONVERGED
+    assert np.linalg.norm(A1.to_scipy() @ x - b1) <= 1e-9 * np.linalg.norm(b1)
