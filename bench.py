@@ -40,12 +40,13 @@ SAMPLE_ITERATIONS = 2  # PCG iterations per CPU-reference step (scaled to the fu
 
 
 def parse():
-    p = argparse.ArgumentParser()
+    p = argparse.ArgumentParser(allow_abbrev=False)
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--n", type=int, default=256, help="grid edge (cells per side)")
+    # (named --grid, not --n: torch.distributed.run would take --n as an abbreviation of its own options)
+    p.add_argument("--grid", dest="n", type=int, default=256, help="grid edge (cells per side)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
 
