@@ -149,6 +149,11 @@ def dist_setup(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
+        # torch.distributed.run sets OMP_NUM_THREADS=1 per process; the host AMG
+        # setup (OpenMP) of each replica gets its share of the host cores
+        # instead. Set before any OpenMP runtime is loaded into the process.
+        per_node = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
+        os.environ["OMP_NUM_THREADS"] = str(max(1, (os.cpu_count() or 1) // max(per_node, 1)))
         import datetime
 
         import torch.distributed as dist
