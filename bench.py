@@ -153,7 +153,8 @@ def dist_setup(args):
         # setup (OpenMP) of each replica gets its share of the host cores
         # instead. Set before any OpenMP runtime is loaded into the process.
         per_node = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
-        os.environ["OMP_NUM_THREADS"] = str(max(1, (os.cpu_count() or 1) // max(per_node, 1)))
+        cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+        os.environ["OMP_NUM_THREADS"] = str(max(1, cores // max(per_node, 1)))
         import datetime
 
         import torch.distributed as dist
