@@ -61,7 +61,10 @@ cfd_status amg_recompute_device(cfd_amg* amg, const cfd_csr* a);
 cfd_status amg_sync_host_values(cfd_amg* amg);
 void free_ra(DevRA& ra);
 // Gauss-Jordan inverse (partial pivoting, the host dense_inverse's operations
-// in its order) of an n x n device CSR operator into inv (n x n, row-major).
+// in its order) of an n x n device CSR operator into inv (n x n, row-major),
+// for n <= kDenseInverseDeviceMaxRows (the staged pivot rows and row tables fit
+// one CTA's shared memory).
+constexpr int64_t kDenseInverseDeviceMaxRows = 8192;
 cfd_status dense_inverse_device(cfd_context* ctx, int64_t n, const int* rp, const int* ci, const double* v,
                                 double* inv);
 }  // namespace cfd

@@ -328,15 +328,23 @@ cfd_status amg_upload(cfd_amg* amg, bool want32) {
   }
   CFD_TRY(ensure_partials(amg->ctx, maxblk));
   if (amg->cfg.coarse_solve == CFD_COARSE_DENSE) {
-    const HostCsr& Ac = amg->host.back().A;
-    std::vector<double> inv;
-    if (!dense_inverse(Ac, inv)) {
-      set_error("AMG coarsest operator (%lld rows) is singular", (long long)Ac.nrows);
-      return CFD_ERR_CONFIG;
+    // The device Gauss-Jordan performs the host dense_inverse's operations in
+    // its order (same inverse); the host one serves operators beyond its size.
+    const DevMat& Ad = amg->dev.back().A;
+    amg->coarse_n = Ad.nrows;
+    CFD_TRY(dmalloc(&amg->coarse_inv, std::max<int64_t>(Ad.nrows * Ad.nrows, 1)));
+    if (Ad.nrows <= kDenseInverseDeviceMaxRows) {
+      CFD_TRY(dense_inverse_device(amg->ctx, Ad.nrows, Ad.rp, Ad.col, Ad.v64, amg->coarse_inv));
+    } else {
+      const HostCsr& Ac = amg->host.back().A;
+      std::vector<double> inv;
+      if (!dense_inverse(Ac, inv)) {
+        set_error("AMG coarsest operator (%lld rows) is singular", (long long)Ac.nrows);
+        return CFD_ERR_CONFIG;
+      }
+      CFD_TRY_CUDA(
+          cudaMemcpyAsync(amg->coarse_inv, inv.data(), inv.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     }
-    amg->coarse_n = Ac.nrows;
-    CFD_TRY(dmalloc(&amg->coarse_inv, (int64_t)inv.size()));
-    CFD_TRY_CUDA(cudaMemcpyAsync(amg->coarse_inv, inv.data(), inv.size() * sizeof(double), cudaMemcpyHostToDevice, s));
   }
   CFD_TRY_CUDA(cudaStreamSynchronize(s));
   if (want32) CFD_TRY(amg_ensure32(amg));

@@ -38,7 +38,7 @@ int grid_for(const cfd_context* ctx, int64_t n, int per) {
   return (int)std::max<int64_t>(1, std::min<int64_t>((n + per - 1) / per, (int64_t)ctx->num_sms * 16));
 }
 
-constexpr int kGjMaxRows = 8192;  // the staged pivot rows and the row tables fit one CTA's shared memory
+constexpr int kGjMaxRows = (int)kDenseInverseDeviceMaxRows;
 
 // C = A B on C's pattern.
 __global__ void __launch_bounds__(256) k_spgemm_fixed(int64_t nrows, const int* __restrict__ c_rp,

@@ -1,6 +1,7 @@
 """Device Galerkin recompute (AlgebraicMultigrid::recompute, amg.rs:179-214):
 with the transfer operators fixed, new fine values re-form every coarse
-operator as (R_l A_l) P_l and the dense coarsest inverse, all on the device.
+operator as (R_l A_l) P_l and the dense coarsest inverse, all on the device
+(setup forms the coarsest inverse with the same device Gauss-Jordan).
 
 The products are summed in the order of the reference-side Gustavson product
 (terms of one output entry in the order of the left operand's row), the
@@ -91,10 +92,10 @@ def test_recompute_matches_oracle_galerkin_chain(cuda, oracle):
 
 
 def test_recompute_dense_inverse_bitwise(cuda):
-    """One-level hierarchy (the V-cycle is the dense coarse solve): the device
-    Gauss-Jordan inverse of the new values equals the host inverse of a fresh
-    setup bit for bit. Random nonsymmetric values force row exchanges at most
-    pivots."""
+    """One-level hierarchy (the V-cycle is the dense coarse solve): the inverse
+    a recompute forms for the new values equals the one a fresh setup forms,
+    bit for bit, and solves the new operator. Random nonsymmetric values force
+    row exchanges at most pivots."""
     import cfdrs_b200 as cf
     n = 300
     rng = np.random.default_rng(11)
@@ -165,8 +166,8 @@ def test_recompute_then_fp32_refinement(cuda):
 def test_recompute_large_coarsest_inverse(cuda):
     """A 3843-row coarsest operator: more rows than the cooperative inverse
     has warps (148 SMs x 16), so warps take several rows per pivot step. A
-    recompute with the setup's values reproduces the host inverse: the V-cycle
-    output is unchanged bit for bit."""
+    recompute with the setup's values reproduces the setup's inverse: the
+    V-cycle output is unchanged bit for bit."""
     import cfdrs_b200 as cf
     from cfdrs_b200 import problems as P
     A = P.poisson_3d_variable(36, 4.0, 1.0, seed=2)[0]
