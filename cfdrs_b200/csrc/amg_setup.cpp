@@ -87,36 +87,33 @@ HostCsr transpose(const HostCsr& a) {
   return t;
 }
 
-// Row-wise product C = A B. Each output row gathers (column, product) terms in
-// the order A's row and then B's rows present them, stable-sorts by column and
-// sums duplicates in that order (first term, then +=), so every entry is the
-// same left-to-right sum a dense-accumulator Gustavson product forms.
+// Row-wise product C = A B (Gustavson). Each output row accumulates its terms
+// in a dense per-thread accumulator in the order A's row and then B's rows
+// present them (first term assigned, the rest added), so every entry is the
+// same left-to-right sum over A's row; the row's distinct columns are then
+// sorted. The accumulator is stamped with the row index, so it is never reset.
 HostCsr spgemm(const HostCsr& a, const HostCsr& b) {
   HostCsr c;
   c.nrows = a.nrows;
   c.ncols = b.ncols;
   c.rp.assign(a.nrows + 1, 0);
-  const int nt = omp_get_max_threads();
-  // Pass 1: row lengths. Pass 2: fill. Row terms are rebuilt in pass 2 to keep
-  // memory proportional to the output.
-  std::vector<std::vector<std::pair<int32_t, double>>> scratch(nt);
+  // Pass 1: row lengths. Pass 2: values (the row is formed again).
 #pragma omp parallel
   {
-    auto& terms = scratch[omp_get_thread_num()];
+    std::vector<int32_t> stamp(b.ncols, -1);
 #pragma omp for schedule(dynamic, 2048)
     for (int64_t i = 0; i < a.nrows; ++i) {
-      terms.clear();
+      int64_t u = 0;
       for (int64_t ka = a.rp[i]; ka < a.rp[i + 1]; ++ka) {
         const int64_t k = a.ci[ka];
-        for (int64_t kb = b.rp[k]; kb < b.rp[k + 1]; ++kb) terms.emplace_back(b.ci[kb], 0.0);
+        for (int64_t kb = b.rp[k]; kb < b.rp[k + 1]; ++kb) {
+          const int32_t j = b.ci[kb];
+          if (stamp[j] != (int32_t)i) {
+            stamp[j] = (int32_t)i;
+            ++u;
+          }
+        }
       }
-      std::sort(terms.begin(), terms.end(),
-                [](const std::pair<int32_t, double>& x, const std::pair<int32_t, double>& y) {
-                  return x.first < y.first;
-                });
-      int64_t u = 0;
-      for (size_t q = 0; q < terms.size(); ++q)
-        if (q == 0 || terms[q].first != terms[q - 1].first) ++u;
       c.rp[i + 1] = u;
     }
   }
@@ -125,28 +122,33 @@ HostCsr spgemm(const HostCsr& a, const HostCsr& b) {
   c.v.resize(c.rp[a.nrows]);
 #pragma omp parallel
   {
-    auto& terms = scratch[omp_get_thread_num()];
+    std::vector<int32_t> stamp(b.ncols, -1);
+    std::vector<double> acc(b.ncols);
+    std::vector<int32_t> cols;
 #pragma omp for schedule(dynamic, 2048)
     for (int64_t i = 0; i < a.nrows; ++i) {
-      terms.clear();
+      cols.clear();
       for (int64_t ka = a.rp[i]; ka < a.rp[i + 1]; ++ka) {
         const int64_t k = a.ci[ka];
         const double av = a.v[ka];
-        for (int64_t kb = b.rp[k]; kb < b.rp[k + 1]; ++kb) terms.emplace_back(b.ci[kb], av * b.v[kb]);
-      }
-      std::stable_sort(terms.begin(), terms.end(),
-                       [](const std::pair<int32_t, double>& x, const std::pair<int32_t, double>& y) {
-                         return x.first < y.first;
-                       });
-      int64_t o = c.rp[i] - 1;
-      for (size_t q = 0; q < terms.size(); ++q) {
-        if (q == 0 || terms[q].first != terms[q - 1].first) {
-          ++o;
-          c.ci[o] = terms[q].first;
-          c.v[o] = terms[q].second;
-        } else {
-          c.v[o] += terms[q].second;
+        for (int64_t kb = b.rp[k]; kb < b.rp[k + 1]; ++kb) {
+          const int32_t j = b.ci[kb];
+          const double t = av * b.v[kb];
+          if (stamp[j] != (int32_t)i) {
+            stamp[j] = (int32_t)i;
+            acc[j] = t;
+            cols.push_back(j);
+          } else {
+            acc[j] += t;
+          }
         }
+      }
+      std::sort(cols.begin(), cols.end());
+      int64_t o = c.rp[i];
+      for (const int32_t j : cols) {
+        c.ci[o] = j;
+        c.v[o] = acc[j];
+        ++o;
       }
     }
   }
@@ -172,6 +174,9 @@ class MaxTree {
     key_[i] = k;
     for (int64_t p = (i + size_) >> 1; p >= 1; p >>= 1) {
       const int32_t nb = pick(best_[2 * p], best_[2 * p + 1]);
+      // Same winner here, and not the point whose key changed: every ancestor
+      // compares the same keys as before, so the tree above is already right.
+      if (nb == best_[p] && nb != (int32_t)i) break;
       best_[p] = nb;
     }
   }
