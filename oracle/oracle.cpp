@@ -189,7 +189,11 @@ struct MaxTree {
   int64_t pick(int64_t l, int64_t r) const { return key[r] > key[l] ? r : l; }
   void set(int64_t i, int64_t k) {
     key[i] = k;
-    for (int64_t p = (i + size) >> 1; p >= 1; p >>= 1) best[p] = pick(best[2 * p], best[2 * p + 1]);
+    for (int64_t p = (i + size) >> 1; p >= 1; p >>= 1) {
+      const int64_t nb = pick(best[2 * p], best[2 * p + 1]);
+      if (nb == best[p] && nb != i) break;  // same winner, unchanged key: ancestors stand
+      best[p] = nb;
+    }
   }
   int64_t top() const { return best[1]; }
 };
