@@ -25,7 +25,7 @@ EXPORTS = [
     "cfd_csr_layout", "cfd_csr_set_path", "cfd_layout_check",
     "cfd_spmv", "cfd_spmv_f32",
     "cfd_amg_config_default", "cfd_amg_setup", "cfd_amg_recompute", "cfd_amg_apply", "cfd_amg_stats",
-    "cfd_amg_level", "cfd_amg_set_path", "cfd_amg_destroy", "cfd_amg_setup_host",
+    "cfd_amg_level", "cfd_amg_set_path", "cfd_amg_destroy", "cfd_amg_setup_host", "cfd_selftest_wait_timeout",
     "cfd_solve_options_default", "cfd_solve", "cfd_last_kernel_stats",
     "cfd_pattern_outer", "cfd_csr_set_values_device",
     "cfd_batch_create", "cfd_batch_update_values", "cfd_batch_solve", "cfd_batch_autotune", "cfd_batch_config",
@@ -127,6 +127,7 @@ def load():
         "cfd_amg_stats": (C.c_int, [P, P]),
         "cfd_amg_level": (C.c_int, [P, C.c_int, C.c_int, P, P, P, P, P, P]),
         "cfd_amg_setup_host": (C.c_int, [C.c_int64, P, P, P, P, PP]),
+        "cfd_selftest_wait_timeout": (C.c_int, [P, C.c_int32]),
         "cfd_amg_set_path": (C.c_int, [P, I32, I32]),
         "cfd_amg_destroy": (C.c_int, [P]),
         "cfd_solve_options_default": (None, [P]),

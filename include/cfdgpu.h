@@ -317,6 +317,15 @@ cfd_status cfd_batch_config(const cfd_batch* batch, int32_t precision, int32_t* 
                             int32_t* threads, int32_t* systems);
 cfd_status cfd_batch_destroy(cfd_batch* batch);
 
+/* ---- diagnostics --------------------------------------------------------
+ * The failure path of the bounded device waits (no reference counterpart):
+ * every wait of the bulk-copy SpMV pipelines gives up after a bounded number
+ * of tries, flags the context and lets the call return CFD_ERR_TIMEOUT. This
+ * runs that wait (the same primitive) on a barrier nothing completes, bounded
+ * by `tries`, so the path can be exercised without a fault or a hang. Returns
+ * CFD_ERR_TIMEOUT with the wait's message; the context stays usable. */
+cfd_status cfd_selftest_wait_timeout(cfd_context* ctx, int32_t tries);
+
 /* ---- residual without device allocation ---------------------------------
  * No counterpart in the reference: an addition for callers that cannot
  * allocate device memory -- a solver embedded in a host application whose
