@@ -48,6 +48,10 @@ def parse():
     # (named --grid, not --n: torch.distributed.run would take --n as an abbreviation of its own options)
     p.add_argument("--grid", dest="n", type=int, default=256, help="grid edge (cells per side)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    # c3 (default) is the mixed-precision workload above; c1 and c2 are the plain
+    # FP64 configurations beside it (c1: 2-D Poisson 128^2, Jacobi-PCG; c2: 3-D
+    # Poisson k = 1 on --grid^3, AMG-PCG), measured the same way.
+    p.add_argument("--workload", default="c3", choices=["c1", "c2", "c3"])
     return p.parse_args()
 
 
@@ -173,6 +177,72 @@ def max_over_ranks(v, world):
     return float(t.item())
 
 
+PLAIN_METRIC = {
+    "c1": "ms to 1e-8 rel-residual (FP64 Jacobi-PCG), 128^2 2-D pressure Poisson",
+    "c2": "ms to 1e-8 rel-residual (FP64 AMG-PCG), {n}^3 constant-coefficient Poisson",
+}
+
+
+def plain_problem(args, P):
+    """(A, b, config) of the c1 / c2 workloads."""
+    if args.workload == "c1":
+        A, b = P.poisson_2d_dirichlet(128, seed=0)
+        cfg = {"workload": "2-D pressure Poisson 128^2 cells, 5-point, homogeneous Dirichlet walls, "
+                           "b ~ U[-1,1]; Jacobi-PCG FP64 from x = 0 to rel-res 1e-8",
+               "unknowns": A.nrows, "nnz": A.nnz, "l2": "L2-resident (1.3 MB CSR): latency-bound", "seed": 0}
+    else:
+        A, b = P.poisson_3d_fv(args.n, None, seed=0)
+        cfg = {"workload": f"3-D constant-coefficient Poisson {args.n}^3, 7-point FV, Dirichlet x=0,1, Neumann "
+                           "elsewhere, b ~ U[-1,1]; AMG-PCG V(1,1) damped Jacobi w=2/3, Ruge-Stueben + modified "
+                           "classical interpolation, dense FP64 coarsest <= 4096; FP64 to rel-res 1e-8",
+               "unknowns": A.nrows, "nnz": A.nnz, "l2": "inputs larger than L2" if args.n >= 128 else "small",
+               "seed": 0}
+    return A, b, cfg
+
+
+def run_reference_plain(args, O, P, cores):
+    """The oracle on the c1 / c2 workload: c1 times full Jacobi-PCG solves (a
+    few ms each); c2 builds the oracle's hierarchy and samples like c3."""
+    A, b, cfg = plain_problem(args, P)
+    Ao = O.Csr.from_matrix(A)
+    extra = {}
+    if args.workload == "c1":
+        _, full = O.pcg(Ao, b, precond=O.PRE_JACOBI, rtol=RTOL, max_it=20000)
+        times = []
+        for s in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            O.pcg(Ao, b, precond=O.PRE_JACOBI, rtol=RTOL, max_it=20000)
+            if s >= args.warmup:
+                times.append((time.perf_counter() - t0) * 1e3)
+        sample = "full FP64 Jacobi-PCG solves to 1e-8 (each step one solve)"
+    else:
+        t0 = time.perf_counter()
+        amg = O.Amg(Ao, O.AmgConfig(max_levels=16, min_coarse_size=4096, smoother=O.SMOOTH_JACOBI, pre_smooth=1,
+                                    post_smooth=1, relaxation=2 / 3, coarse_solve=O.COARSE_DENSE, interpolation=2,
+                                    coarse_order=1))
+        extra["setup_s"] = time.perf_counter() - t0
+        _, full = O.pcg(Ao, b, precond=O.PRE_AMG, amg=amg, rtol=RTOL, max_it=1000)
+        k = min(SAMPLE_ITERATIONS, max(full.iterations, 1))
+        times = []
+        for s in range(args.warmup + args.steps):
+            dt = oracle_solve_estimate(O, Ao, b, amg, full.iterations, k)
+            if s >= args.warmup:
+                times.append(dt)
+        sample = (f"per step the start-up, {k} FP64 AMG-PCG iterations and one V-cycle: start-up + "
+                  f"{full.iterations} x per-iteration time - one V-cycle (oracle hierarchy, setup excluded)")
+    ms = sum(times) / len(times)
+    line = {
+        "impl": "reference", "metric": PLAIN_METRIC[args.workload].format(n=args.n), "value": ms, "unit": "ms",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": cfg, "iterations": full.iterations, "termination": full.termination,
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank):
     """CPU restatement of the reference algorithm (oracle/), all host threads.
 
@@ -189,6 +259,8 @@ def run_reference(args, world, rank):
     from cfdrs_b200 import problems as P
     O.build()
     cores = O.get_threads()
+    if args.workload != "c3":
+        return run_reference_plain(args, O, P, cores)
     A, b, _ = P.poisson_3d_variable(args.n, 8.0, 1.0, seed=0)
     Ao = O.Csr.from_matrix(A)
     t0 = time.perf_counter()
@@ -223,9 +295,151 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_plain(args, world, rank, local):
+    """GPU arm of the c1 / c2 workloads: the FP64 solve from x = 0 to 1e-8 per
+    step, timed like c3 (warm-up, barrier and synchronize around the timed
+    region, device events on the solve's stream, max over ranks, clocks sampled
+    during it); e2e through the C ABI with pinned host buffers; the fine
+    operator's FP64 SpMV against the copy peak; the oracle beside it on rank 0."""
+    import torch
+    torch.cuda.set_device(local)
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.device import context, device_matrix
+
+    A, b, config = plain_problem(args, P)
+    N = A.nrows
+    ctx = context(local)
+    dA = device_matrix(A, ctx)
+    setup_s, stats = None, None
+    if args.workload == "c1":
+        pre = cf.JacobiPreconditioner(A)
+    else:
+        t0 = time.perf_counter()
+        pre = cf.AlgebraicMultigrid(A, cf.AMGConfig.pressure_poisson(), ctx=ctx)
+        setup_s = time.perf_counter() - t0
+        stats = pre.statistics()
+        config.update(amg_levels=int(stats.num_levels), operator_complexity=round(stats.operator_complexity, 3))
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    bd = torch.as_tensor(b, device="cuda")
+    cfg = cf.IterativeSolverConfig(0.0, RTOL, 20000)
+    x = torch.zeros_like(bd)
+
+    def solve(precision=cf.Precision.FP64):
+        x.zero_()
+        return cf.cg_preconditioned(A, bd, pre, x, cfg, precision=precision)
+
+    for _ in range(args.warmup):
+        solve()
+    launches = ctx.kernel_stats()["launches"]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            rep = solve()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
+    true_rel = float(np.linalg.norm(b - A.matvec(x.cpu().numpy())) / np.linalg.norm(b))
+    extra = {}
+    if args.workload == "c2":
+        solve(cf.Precision.FP32_REFINE)
+        t32 = []
+        for _ in range(3):
+            ev0.record(stream)
+            r32 = solve(cf.Precision.FP32_REFINE)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            t32.append(ev0.elapsed_time(ev1))
+        extra = {"fp32_refine_ms": min(t32), "fp32_refine_iterations": {"inner": r32.iterations,
+                                                                          "outer": r32.outer_iterations},
+                 "amg_setup_s": setup_s}
+
+    # end to end through the C ABI with pinned host buffers
+    ctx.set_stream(None)
+    b_pin = torch.from_numpy(b).pin_memory()
+    x_pin = torch.zeros(N, dtype=torch.float64).pin_memory()
+    bh, xh = b_pin.numpy(), x_pin.numpy()
+    e2e = []
+    for s in range(args.warmup + args.steps):
+        xh[:] = 0.0
+        t0 = time.perf_counter()
+        cf.cg_preconditioned(A, bh, pre, xh, cfg)
+        if s >= args.warmup:
+            e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = max_over_ranks(sum(e2e) / len(e2e), world)
+
+    # FP64 SpMV of the operator against the copy peak
+    ctx.set_stream(stream.cuda_stream)
+    peak, peak_kind = measured_peak()
+    xv = torch.rand(N, device="cuda", dtype=torch.float64)
+    yv = torch.empty_like(xv)
+    for _ in range(3):
+        dA.spmv(xv.data_ptr(), yv.data_ptr(), fp32=False)
+    reps = 50
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(reps):
+        dA.spmv(xv.data_ptr(), yv.data_ptr(), fp32=False)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_spmv = ev0.elapsed_time(ev1) / reps
+    spmv_bytes = A.nnz * 12 + 4 * (N + 1) + 16 * N
+    gbs = spmv_bytes / t_spmv / 1e6
+    ctx.set_stream(None)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        if args.workload == "c1":
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+            O.build()
+            Ao = O.Csr.from_matrix(A)
+            O.pcg(Ao, b, precond=O.PRE_JACOBI, rtol=RTOL, max_it=20000)
+            t0 = time.perf_counter()
+            for _ in range(5):
+                O.pcg(Ao, b, precond=O.PRE_JACOBI, rtol=RTOL, max_it=20000)
+            cpu = {"value": (time.perf_counter() - t0) * 1e3 / 5, "unit": "ms", "cores": O.get_threads(),
+                   "kind": "port", "sample": "5 full FP64 Jacobi-PCG solves to 1e-8 on the oracle"}
+        else:
+            cpu = cpu_baseline_from_hierarchy(pre, A, b, rep.iterations)
+
+    if rank == 0:
+        line = {
+            "metric": PLAIN_METRIC[args.workload].format(n=args.n), "value": ms, "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (U[-1,1] RHS)",
+            "config": config,
+            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": N * 8},
+            "gpu_launches": int(launches * args.steps),
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                         "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "SpMV FP64 of the operator, timed alone; achieved counts CSR bytes"
+                                   + (" (L2-resident: the HBM fraction does not bound it)"
+                                      if args.workload == "c1" else "")},
+            "iterations": rep.iterations, "true_rel_residual": true_rel, "clocks": clk.summary(),
+        }
+        line.update(extra)
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.impl != "reference" and args.workload != "c3":
+        return run_plain(args, world, rank, local)
     if args.impl == "reference":
         run_reference(args, world, rank)
         if world > 1:

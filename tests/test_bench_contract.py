@@ -44,6 +44,19 @@ def test_reference_arm_line():
     check_reference_line(lines[0], 1, 2, 1)
 
 
+def test_reference_arm_plain_workload():
+    """--workload c1: the oracle's Jacobi-PCG on the 2-D 128^2 system."""
+    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--workload", "c1", "--steps", "2",
+                          "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = json_lines(out.stdout)
+    assert len(lines) == 1
+    d = lines[0]
+    check_reference_line(d, 1, 2, 1)
+    assert "Jacobi-PCG" in d["metric"] and d["config"]["unknowns"] == 128 * 128
+    assert d["iterations"] == 383  # the device solve's count as well (perf configs)
+
+
 def test_reference_arm_two_ranks():
     """As the driver launches N > 1: one rank per process over gloo; rank 0
     alone measures and prints, the other rank exits 0 without work."""
