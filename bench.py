@@ -50,8 +50,9 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     # c3 (default) is the mixed-precision workload above; c1 and c2 are the plain
     # FP64 configurations beside it (c1: 2-D Poisson 128^2, Jacobi-PCG; c2: 3-D
-    # Poisson k = 1 on --grid^3, AMG-PCG), measured the same way.
-    p.add_argument("--workload", default="c3", choices=["c1", "c2", "c3"])
+    # Poisson k = 1 on --grid^3, AMG-PCG), c4 the 4096 batched networks
+    # (Jacobi-PCG per network, equilibrated residual), measured the same way.
+    p.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4"])
     return p.parse_args()
 
 
@@ -177,7 +178,12 @@ def max_over_ranks(v, world):
     return float(t.item())
 
 
+BATCH_SYSTEMS = 4096
+BATCH_CPU_STRIDE = 16  # the CPU arms solve every 16th network per step, scaled by 16
+BATCH_RTOL = 1e-10
+
 PLAIN_METRIC = {
+    "c4": "ms to 1e-10 equilibrated residual, 4096 batched Kirchhoff networks (FP64 Jacobi-PCG)",
     "c1": "ms to 1e-8 rel-residual (FP64 Jacobi-PCG), 128^2 2-D pressure Poisson",
     "c2": "ms to 1e-8 rel-residual (FP64 AMG-PCG), {n}^3 constant-coefficient Poisson",
 }
@@ -198,6 +204,56 @@ def plain_problem(args, P):
                "unknowns": A.nrows, "nnz": A.nnz, "l2": "inputs larger than L2" if args.n >= 128 else "small",
                "seed": 0}
     return A, b, cfg
+
+
+def oracle_batch_sample(O, systems, cores, stride):
+    """ms of the oracle solving all networks, one serial Jacobi-PCG per network
+    on a pool of `cores` worker threads (each with a one-thread OpenMP pool),
+    estimated from every `stride`-th network and scaled by `stride`; and the
+    reports of the networks solved."""
+    from concurrent.futures import ThreadPoolExecutor
+    picked = [(O.Csr.from_matrix(A), b) for A, b in systems[::stride]]
+
+    def one(item):
+        return O.pcg_equilibrated(item[0], item[1], rtol=BATCH_RTOL, max_it=20000)[1]
+
+    with ThreadPoolExecutor(max_workers=cores, initializer=O.set_threads, initargs=(1,)) as ex:
+        t0 = time.perf_counter()
+        reps = list(ex.map(one, picked))
+        ms = (time.perf_counter() - t0) * 1e3 * stride
+    return ms, reps
+
+
+def run_reference_batch(args, O, P, cores):
+    systems = P.network_batch(BATCH_SYSTEMS, seed=0)
+    times, reps = [], []
+    for s in range(args.warmup + args.steps):
+        ms, reps = oracle_batch_sample(O, systems, cores, BATCH_CPU_STRIDE)
+        if s >= args.warmup:
+            times.append(ms)
+    ms = sum(times) / len(times)
+    sample = (f"per step every {BATCH_CPU_STRIDE}th of the {BATCH_SYSTEMS} networks "
+              f"({len(reps)} networks), one serial FP64 Jacobi-PCG each (equilibrated residual to "
+              f"{BATCH_RTOL:g}) on {cores} worker threads, scaled by {BATCH_CPU_STRIDE}")
+    line = {
+        "impl": "reference", "metric": PLAIN_METRIC["c4"], "value": ms, "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": batch_config(systems),
+        "converged_systems_in_sample": sum(r.termination == "Converged" for r in reps),
+        "iterations_in_sample": int(sum(r.iterations for r in reps)),
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def batch_config(systems):
+    return {"workload": f"{len(systems)} seeded Kirchhoff networks, n ~ U[20, 2000], spanning tree + 10 % loop "
+                        "edges, Hagen-Poiseuille conductances, inlet 1000 Pa / outlet 0 Pa; Jacobi-PCG per "
+                        f"network to {BATCH_RTOL:g} on the row-equilibrated residual",
+            "systems": len(systems), "rows": int(sum(A.nrows for A, _ in systems)),
+            "nnz": int(sum(A.nnz for A, _ in systems)), "seed": 0}
 
 
 def run_reference_plain(args, O, P, cores):
@@ -259,6 +315,8 @@ def run_reference(args, world, rank):
     from cfdrs_b200 import problems as P
     O.build()
     cores = O.get_threads()
+    if args.workload == "c4":
+        return run_reference_batch(args, O, P, cores)
     if args.workload != "c3":
         return run_reference_plain(args, O, P, cores)
     A, b, _ = P.poisson_3d_variable(args.n, 8.0, 1.0, seed=0)
@@ -435,9 +493,83 @@ def run_plain(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def run_batch(args, world, rank, local):
+    """GPU arm of c4: all networks in one batched solve per step (persistent
+    CTA-per-system kernels replayed from a CUDA graph, autotuned widths), FP64;
+    value = the solve's device time (events around copies in, graph, copies
+    out), e2e = host wall clock around the call; FP32 + refinement beside it;
+    the oracle beside it on rank 0 (every BATCH_CPU_STRIDE-th network)."""
+    import torch
+    torch.cuda.set_device(local)
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.batch import NetworkBatch
+    from cfdrs_b200.device import context
+
+    systems = P.network_batch(BATCH_SYSTEMS, seed=0)
+    b = np.concatenate([bb for _, bb in systems])
+    nb = NetworkBatch([A for A, _ in systems], ctx=context(local))
+    cfg = cf.IterativeSolverConfig(0.0, BATCH_RTOL, 40000)
+    tuned = {p.name: nb.autotune(p, sample_iterations=64) for p in (cf.Precision.FP64, cf.Precision.FP32_REFINE)}
+    for _ in range(args.warmup):
+        nb.solve(b, config=cfg)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    dev, wall = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            x, rep = nb.solve(b, config=cfg)
+            wall.append((time.perf_counter() - t0) * 1e3)
+            dev.append(rep.device_ms)
+    ms = max_over_ranks(sum(dev) / len(dev), world)
+    e2e_ms = max_over_ranks(sum(wall) / len(wall), world)
+    nb.solve(b, config=cfg, precision=cf.Precision.FP32_REFINE)
+    _, rep32 = nb.solve(b, config=cfg, precision=cf.Precision.FP32_REFINE)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        O.build()
+        cores = O.get_threads()
+        cpu_ms, reps = oracle_batch_sample(O, systems, cores, BATCH_CPU_STRIDE)
+        cpu = {"value": cpu_ms, "unit": "ms", "cores": cores, "kind": "port",
+               "sample": f"every {BATCH_CPU_STRIDE}th network ({len(reps)}), one serial FP64 Jacobi-PCG each on "
+                         f"{cores} worker threads, scaled by {BATCH_CPU_STRIDE}"}
+    if rank == 0:
+        rows, nnz = nb.rows, int(nb.val.size)
+        moved = nnz * (8 + 2) + rows * 8 * 6  # one pass over values, 16-bit columns and six vectors
+        line = {
+            "metric": PLAIN_METRIC["c4"], "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded networks)",
+            "config": batch_config(systems),
+            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * rows * 8, "d2h_bytes_per_step": rows * 8},
+            "gpu_launches": args.steps * sum(1 for c in tuned["FP64"]["systems"] if c > 0),  # one per bucket
+            "roofline": {"bound": "hbm", "achieved": moved / ms / 1e6, "peak": measured_peak()[0], "unit": "GB/s",
+                         "frac": moved / ms / 1e6 / measured_peak()[0], "traffic": None,
+                         "kernel": "batched Jacobi-PCG: each system lives in shared memory for its whole solve, so "
+                                   "an iteration is bound by barrier latency, not HBM; achieved = one pass over the "
+                                   "systems' bytes per solve"},
+            "converged_systems": rep.converged_systems, "total_iterations": rep.total_iterations,
+            "max_rel_residual": rep.max_rel_residual,
+            "fp32_refine_ms": rep32.device_ms, "fp32_refine_total_inner_iterations": rep32.total_iterations,
+            "autotuned": tuned, "clocks": clk.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.impl != "reference" and args.workload == "c4":
+        return run_batch(args, world, rank, local)
     if args.impl != "reference" and args.workload != "c3":
         return run_plain(args, world, rank, local)
     if args.impl == "reference":

@@ -57,6 +57,20 @@ def test_reference_arm_plain_workload():
     assert d["iterations"] == 383  # the device solve's count as well (perf configs)
 
 
+def test_reference_arm_batched_networks():
+    """--workload c4: the oracle on every 16th of the 4096 networks, one serial
+    Jacobi-PCG per network on worker threads, scaled to the whole batch."""
+    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--workload", "c4", "--steps", "1",
+                          "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = json_lines(out.stdout)
+    assert len(lines) == 1
+    d = lines[0]
+    assert d["impl"] == "reference" and d["value"] > 0 and d["config"]["systems"] == 4096
+    assert d["converged_systems_in_sample"] == 256
+    assert d["cpu_baseline"]["value"] == d["value"] and "every 16th" in d["cpu_baseline"]["sample"]
+
+
 def test_reference_arm_two_ranks():
     """As the driver launches N > 1: one rank per process over gloo; rank 0
     alone measures and prints, the other rank exits 0 without work."""
