@@ -51,8 +51,9 @@ def parse():
     # c3 (default) is the mixed-precision workload above; c1 and c2 are the plain
     # FP64 configurations beside it (c1: 2-D Poisson 128^2, Jacobi-PCG; c2: 3-D
     # Poisson k = 1 on --grid^3, AMG-PCG), c4 the 4096 batched networks
-    # (Jacobi-PCG per network, equilibrated residual), measured the same way.
-    p.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4"])
+    # (Jacobi-PCG per network, equilibrated residual), c5 the 512^2 Darcy
+    # adjoint gradient, measured the same way.
+    p.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"])
     return p.parse_args()
 
 
@@ -182,7 +183,10 @@ BATCH_SYSTEMS = 4096
 BATCH_CPU_STRIDE = 16  # the CPU arms solve every 16th network per step, scaled by 16
 BATCH_RTOL = 1e-10
 
+ADJOINT_N = 512
+
 PLAIN_METRIC = {
+    "c5": "ms per theta update (dL/dtheta by the adjoint, forward and adjoint to 1e-10), 512^2 Darcy",
     "c4": "ms to 1e-10 equilibrated residual, 4096 batched Kirchhoff networks (FP64 Jacobi-PCG)",
     "c1": "ms to 1e-8 rel-residual (FP64 Jacobi-PCG), 128^2 2-D pressure Poisson",
     "c2": "ms to 1e-8 rel-residual (FP64 AMG-PCG), {n}^3 constant-coefficient Poisson",
@@ -246,6 +250,121 @@ def run_reference_batch(args, O, P, cores):
         "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def adjoint_config():
+    return {"workload": f"2-D Darcy {ADJOINT_N}^2 cells, k = exp(theta), theta GRF l=16 sigma=0.5, p=1 left / 0 right, "
+                        "no-flux top and bottom; L = sum p^2 over the column at x = 0.75; dL/dtheta by the adjoint "
+                        "(transposed solve, same preconditioner, pattern outer product), forward and adjoint "
+                        "FP32 AMG-PCG inside FP64 refinement to 1e-10, Galerkin recompute per update",
+            "unknowns": ADJOINT_N * ADJOINT_N, "seed": 0}
+
+
+def run_reference_adjoint(args):
+    """The oracle's FP64 adjoint (sparse direct forward and transposed solves,
+    hand-derived face formula), one full gradient per step."""
+    import adjoint_cpu as AC
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.adjoint import loss_column_index
+    theta = P.gaussian_random_field((ADJOINT_N, ADJOINT_N), 16.0, 0.5, seed=0)
+    col = loss_column_index(ADJOINT_N)
+    times = []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        L, _, _ = AC.loss_and_grad(theta, col)
+        if s >= args.warmup:
+            times.append((time.perf_counter() - t0) * 1e3)
+    ms = sum(times) / len(times)
+    line = {
+        "impl": "reference", "metric": PLAIN_METRIC["c5"], "value": ms, "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": adjoint_config(),
+        "loss": L,
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "port",
+                         "sample": "one full FP64 gradient per step (scipy SuperLU forward and transposed solves)"},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args, world, rank, local):
+    """GPU arm of c5: one theta update per step (torch assembly of the Darcy
+    system from theta, forward solve, loss, adjoint solve through the
+    hand-written backward, chain rule to dL/dtheta) with the Galerkin operators
+    recomputed for the new values; value with theta resident on the device,
+    e2e with theta copied in from pinned host memory and dL/dtheta copied out."""
+    import torch
+    torch.cuda.set_device(local)
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.adjoint import (SparseSolver, column_loss, darcy_2d_pattern, darcy_2d_torch,
+                                    loss_column_index, sparse_solve)
+    n = ADJOINT_N
+    theta = P.gaussian_random_field((n, n), 16.0, 0.5, seed=0)
+    col = loss_column_index(n)
+    pattern, mask = darcy_2d_pattern(n)
+    maskd = torch.as_tensor(mask, device="cuda")
+    solver = SparseSolver(pattern, precision=cf.Precision.FP32_REFINE,
+                          config=cf.IterativeSolverConfig(0.0, 1e-10, 500))
+    th = torch.as_tensor(theta, device="cuda")
+    th_pin = torch.from_numpy(theta).pin_memory()
+
+    def update(src, first=False):
+        t = src.to("cuda", non_blocking=True).clone().requires_grad_(True)
+        vals, b = darcy_2d_torch(t, maskd)
+        L = column_loss(sparse_solve(vals, b, solver, first), n, col)
+        L.backward()
+        return t.grad, L
+
+    update(th, True)  # AMG setup
+    for _ in range(args.warmup):
+        update(th)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            g, L = update(th)
+            torch.cuda.synchronize()
+            times.append((time.perf_counter() - t0) * 1e3)
+    ms = max_over_ranks(sum(times) / len(times), world)
+    e2e = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        g, L = update(th_pin)
+        g_host = g.cpu()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = max_over_ranks(sum(e2e) / len(e2e), world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import adjoint_cpu as AC
+        t0 = time.perf_counter()
+        L_cpu, g_cpu, _ = AC.loss_and_grad(theta, col)
+        cpu = {"value": (time.perf_counter() - t0) * 1e3, "unit": "ms", "cores": 1, "kind": "port",
+               "sample": "one full FP64 gradient (scipy SuperLU forward and transposed solves)",
+               "gradient_rel_diff": float(np.linalg.norm(g_host.numpy() - g_cpu) / np.linalg.norm(g_cpu))}
+    if rank == 0:
+        line = {
+            "metric": PLAIN_METRIC["c5"], "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded GRF theta)",
+            "config": adjoint_config(),
+            "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8},
+            "gpu_launches": None,
+            "roofline": None,
+            "adjoint_solve_device_ms": solver.last_report.device_ms, "loss": float(L.item()),
+            "clocks": clk.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 def batch_config(systems):
@@ -317,6 +436,8 @@ def run_reference(args, world, rank):
     cores = O.get_threads()
     if args.workload == "c4":
         return run_reference_batch(args, O, P, cores)
+    if args.workload == "c5":
+        return run_reference_adjoint(args)
     if args.workload != "c3":
         return run_reference_plain(args, O, P, cores)
     A, b, _ = P.poisson_3d_variable(args.n, 8.0, 1.0, seed=0)
@@ -570,6 +691,8 @@ def main():
     world, rank, local = dist_setup(args)
     if args.impl != "reference" and args.workload == "c4":
         return run_batch(args, world, rank, local)
+    if args.impl != "reference" and args.workload == "c5":
+        return run_adjoint(args, world, rank, local)
     if args.impl != "reference" and args.workload != "c3":
         return run_plain(args, world, rank, local)
     if args.impl == "reference":

@@ -71,6 +71,18 @@ def test_reference_arm_batched_networks():
     assert d["cpu_baseline"]["value"] == d["value"] and "every 16th" in d["cpu_baseline"]["sample"]
 
 
+def test_reference_arm_adjoint():
+    """--workload c5: the oracle's FP64 adjoint gradient of the 512^2 Darcy loss."""
+    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--workload", "c5", "--steps", "1",
+                          "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = json_lines(out.stdout)
+    assert len(lines) == 1
+    d = lines[0]
+    assert d["impl"] == "reference" and d["value"] > 0 and d["loss"] > 0
+    assert d["config"]["unknowns"] == 512 * 512 and d["cpu_baseline"]["value"] == d["value"]
+
+
 def test_reference_arm_two_ranks():
     """As the driver launches N > 1: one rank per process over gloo; rank 0
     alone measures and prints, the other rank exits 0 without work."""
