@@ -461,39 +461,71 @@ cfd_status set_params(cfd_batch* bt, const cfd_solver_config& cfg, const cfd_sol
 
 extern "C" {
 
-cfd_status cfd_batch_create(cfd_context* ctx, int32_t num_systems, const int64_t* sys_row_offsets,
-                            const int64_t* row_ptr, const int32_t* col, const double* val, cfd_batch** out) {
-  if (!ctx || !out || num_systems < 0 || (num_systems > 0 && (!sys_row_offsets || !row_ptr))) {
+// The caller's layout, checked in an order that never indexes past what the
+// earlier checks have bounded: the offsets (num_systems + 1 of them, from 0,
+// non-decreasing, ending at the total row count), then per system its rows
+// (row_ptr non-decreasing and within [0, nnz]) before its local columns.
+// Touches no device state.
+static cfd_status validate_batch(int32_t num_systems, const int64_t* sys_row_offsets, const int64_t* row_ptr,
+                                 const int32_t* col, const double* val) {
+  if (num_systems < 0 || !sys_row_offsets || !row_ptr) {
     set_error("cfd_batch_create: invalid arguments");
     return CFD_ERR_STATE;
   }
-  *out = nullptr;
   const int64_t rows = sys_row_offsets[num_systems];
+  if (sys_row_offsets[0] != 0 || rows < 0 || rows >= INT32_MAX) {
+    set_error("cfd_batch_create: system offsets must start at 0 and end at a row count that fits int32");
+    return CFD_ERR_DIM;
+  }
   const int64_t nnz = row_ptr[rows];
-  if (sys_row_offsets[0] != 0 || row_ptr[0] != 0 || rows >= INT32_MAX || nnz >= INT32_MAX) {
-    set_error("cfd_batch_create: offsets must start at 0 and fit int32");
+  if (row_ptr[0] != 0 || nnz < 0 || nnz >= INT32_MAX) {
+    set_error("cfd_batch_create: row_ptr must start at 0 and end at a nonzero count that fits int32");
+    return CFD_ERR_DIM;
+  }
+  if (nnz > 0 && (!col || !val)) {
+    set_error("cfd_batch_create: null column or value array");
     return CFD_ERR_DIM;
   }
   for (int s = 0; s < num_systems; ++s) {
     const int64_t r0 = sys_row_offsets[s], r1 = sys_row_offsets[s + 1];
-    if (r1 < r0 || r1 - r0 > kBatchMaxRows || row_ptr[r1] - row_ptr[r0] > kBatchMaxNnz) {
+    if (r1 < r0 || r1 > rows) {
+      set_error("cfd_batch_create: system offsets decrease or pass the row count at system %d", s);
+      return CFD_ERR_DIM;
+    }
+    for (int64_t i = r0; i < r1; ++i)
+      if (row_ptr[i + 1] < row_ptr[i] || row_ptr[i + 1] > nnz) {
+        set_error("cfd_batch_create: row_ptr decreases or passes nnz at row %lld", (long long)i);
+        return CFD_ERR_DIM;
+      }
+    if (r1 - r0 > kBatchMaxRows || row_ptr[r1] - row_ptr[r0] > kBatchMaxNnz) {
       set_error("cfd_batch_create: system %d has %lld rows / %lld nonzeros; the batched solver holds at most "
                 "%d rows and %d nonzeros per system (use cfd_solve for larger systems)",
                 s, (long long)(r1 - r0), (long long)(row_ptr[r1] - row_ptr[r0]), kBatchMaxRows, kBatchMaxNnz);
       return CFD_ERR_DIM;
     }
-    for (int64_t i = r0; i < r1; ++i) {
-      if (row_ptr[i + 1] < row_ptr[i]) {
-        set_error("cfd_batch_create: row_ptr decreases at row %lld", (long long)i);
+    for (int64_t e = row_ptr[r0]; e < row_ptr[r1]; ++e)
+      if (col[e] < 0 || col[e] >= r1 - r0) {
+        set_error("cfd_batch_create: local column %d out of range in system %d", col[e], s);
         return CFD_ERR_DIM;
       }
-      for (int64_t e = row_ptr[i]; e < row_ptr[i + 1]; ++e)
-        if (col[e] < 0 || col[e] >= r1 - r0) {
-          set_error("cfd_batch_create: local column %d out of range in system %d", col[e], s);
-          return CFD_ERR_DIM;
-        }
-    }
   }
+  return CFD_OK;
+}
+
+cfd_status cfd_batch_create(cfd_context* ctx, int32_t num_systems, const int64_t* sys_row_offsets,
+                            const int64_t* row_ptr, const int32_t* col, const double* val, cfd_batch** out) {
+  if (!out) {
+    set_error("cfd_batch_create: null output handle");
+    return CFD_ERR_STATE;
+  }
+  *out = nullptr;
+  CFD_TRY(validate_batch(num_systems, sys_row_offsets, row_ptr, col, val));
+  if (!ctx) {
+    set_error("cfd_batch_create: null context");
+    return CFD_ERR_STATE;
+  }
+  const int64_t rows = sys_row_offsets[num_systems];
+  const int64_t nnz = row_ptr[rows];
   std::lock_guard<std::mutex> g(ctx->mu);
   CFD_TRY_CUDA(cudaSetDevice(ctx->device));
   cfd_batch* bt = new cfd_batch;

@@ -398,8 +398,10 @@ static cfd_status validate_csr(int64_t nrows, int64_t ncols, int64_t nnz, const 
     return CFD_ERR_DIM;
   }
   for (int64_t i = 0; i < nrows; ++i) {
-    if (rp[i + 1] < rp[i]) {
-      set_error("row_ptr decreases at row %lld", (long long)i);
+    // rp[i + 1] <= nnz as well: the column scan below reads up to it before
+    // the end of row_ptr has been compared with nnz.
+    if (rp[i + 1] < rp[i] || rp[i + 1] > nnz) {
+      set_error("row_ptr decreases or passes nnz at row %lld", (long long)i);
       return CFD_ERR_DIM;
     }
     for (int64_t k = rp[i]; k < rp[i + 1]; ++k) {

@@ -54,3 +54,84 @@ def test_no_device_fails_loudly():
     assert st != _lib.CFD_OK and L.cfd_last_error()
     with pytest.raises(_lib.CfdError):
         _lib.check(st)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _i64(*v):
+    import numpy as np
+    return np.array(v, dtype=np.int64)
+
+
+def test_csr_row_ptr_past_nnz_is_refused_before_the_column_scan():
+    """row_ptr = [0, 100, 5] with 5 nonzeros: row 0's end passes nnz. The
+    check must fire at row 0, before the column scan reads col[5..99]
+    (without it the call still fails, but on a column it read past the end)."""
+    import numpy as np
+    from cfdrs_b200 import _lib
+    L = _lib.load()
+    rp, col, val = _i64(0, 100, 5), np.arange(5, dtype=np.int32), np.ones(5)
+    x, y = np.ones(8), np.zeros(2)
+    info = (C.c_int64 * 64)()
+    st = L.cfd_layout_check(2, 8, 5, _ptr(rp), _ptr(col), _ptr(val), _ptr(x), _ptr(y), C.byref(info))
+    assert st == 1 and b"passes nnz at row 0" in L.cfd_last_error()
+    cfg = _lib.AmgConfigC()
+    L.cfd_amg_config_default(C.byref(cfg))
+    out = C.c_void_p()
+    col64 = np.arange(5, dtype=np.int64)
+    assert L.cfd_amg_setup_host(2, _ptr(rp), _ptr(col64), _ptr(val), C.byref(cfg), C.byref(out)) == 1
+    assert b"passes nnz at row 0" in L.cfd_last_error() and not out.value
+
+
+BATCH_LAYOUTS = {
+    # name: (num_systems, offsets, row_ptr, col, with_values, status, message)
+    "null_offsets": (0, None, _i64(0), None, False, 7, b"invalid arguments"),
+    "negative_count": (-1, _i64(0), _i64(0), None, False, 7, b"invalid arguments"),
+    "negative_rows": (1, _i64(0, -5), _i64(0), None, False, 1, b"system offsets must start at 0"),
+    "offsets_not_from_zero": (1, _i64(1, 2), _i64(0, 1, 2), None, False, 1, b"system offsets must start at 0"),
+    # system 0 claims 100 rows of a 50-row batch: row_ptr[100] must not be read
+    "offsets_decrease": (2, _i64(0, 100, 50), _i64(*range(51)), "diag", True, 1, b"decrease or pass the row count"),
+    "row_ptr_past_nnz": (1, _i64(0, 2), _i64(0, 100, 2), "diag", True, 1, b"passes nnz at row 0"),
+    "null_columns": (1, _i64(0, 2), _i64(0, 1, 2), None, True, 1, b"null column or value array"),
+    "null_values": (1, _i64(0, 2), _i64(0, 1, 2), "diag", False, 1, b"null column or value array"),
+    "local_column_out_of_range": (2, _i64(0, 2, 4), _i64(0, 1, 2, 3, 4), "global", True, 1, b"local column 2"),
+    "system_too_large": (1, _i64(0, 2049), _i64(*range(2050)), "diag", True, 1, b"at most 2048 rows"),
+}
+
+
+@pytest.mark.parametrize("case", sorted(BATCH_LAYOUTS))
+def test_batch_layout_is_checked_before_the_context(case):
+    """cfd_batch_create checks the caller's layout before it touches the
+    context, in an order that reads no array past a bound an earlier check
+    established; a null context is reported only for a valid layout."""
+    import numpy as np
+    from cfdrs_b200 import _lib
+    L = _lib.load()
+    nsys, offs, rp, col, with_values, status, msg = BATCH_LAYOUTS[case]
+    nnz = int(rp[-1]) if rp is not None and rp[-1] >= 0 else 0
+    cols = None
+    if col == "diag":          # local column = the row's index inside its system
+        cols = np.array([i - offs[np.searchsorted(offs, i, side="right") - 1] for i in range(nnz)], dtype=np.int32)
+    elif col == "global":      # global row numbers: system 1's columns leave its 2 rows
+        cols = np.arange(nnz, dtype=np.int32)
+    vals = np.ones(nnz) if with_values else None
+    out = C.c_void_p(1)
+    st = L.cfd_batch_create(None, nsys, _ptr(offs), _ptr(rp), _ptr(cols), _ptr(vals), C.byref(out))
+    assert st == status, L.cfd_last_error()
+    assert msg in L.cfd_last_error() and not out.value
+
+
+def test_batch_valid_layout_reaches_the_context_check():
+    import numpy as np
+    from cfdrs_b200 import _lib
+    L = _lib.load()
+    out = C.c_void_p()
+    offs, rp = _i64(0, 2, 2, 5), _i64(0, 1, 2, 3, 4, 5)   # system 1 is empty
+    cols, vals = np.array([0, 1, 0, 1, 2], dtype=np.int32), np.ones(5)
+    assert L.cfd_batch_create(None, 3, _ptr(offs), _ptr(rp), _ptr(cols), _ptr(vals), C.byref(out)) == 7
+    assert b"null context" in L.cfd_last_error()
+    z = _i64(0)
+    assert L.cfd_batch_create(None, 0, _ptr(z), _ptr(z), None, None, C.byref(out)) == 7
+    assert b"null context" in L.cfd_last_error()
