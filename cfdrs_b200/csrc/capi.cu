@@ -443,20 +443,29 @@ cfd_status cfd_context_create(int device, cfd_context** out) {
   CFD_TRY_CUDA(cudaSetDevice(device));
   cfd_context* c = new cfd_context;
   c->device = device;
-  CFD_TRY_CUDA(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
-  c->stream = c->own;
-  CFD_TRY(dmalloc(&c->counter, 1));
-  CFD_TRY_CUDA(cudaMemset(c->counter, 0, sizeof(unsigned)));
-  CFD_TRY(dmalloc(&c->state, 2));
-  CFD_TRY_CUDA(cudaMallocHost((void**)&c->h_state, 2 * sizeof(DevState)));
-  CFD_TRY_CUDA(cudaEventCreate(&c->ev0));
-  CFD_TRY_CUDA(cudaEventCreate(&c->ev1));
-  CFD_TRY(ensure_partials(c, kVecGrid));
-  CFD_TRY(dmalloc(&c->err, 1));
-  CFD_TRY_CUDA(cudaMemset(c->err, 0, sizeof(int)));
-  CFD_TRY_CUDA(cudaMallocHost((void**)&c->h_err, sizeof(int)));
-  *c->h_err = 0;
-  CFD_TRY_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+  // Any failure below releases what was made so far (destroy skips nulls).
+  const cfd_status st = [&]() -> cfd_status {
+    CFD_TRY_CUDA(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+    c->stream = c->own;
+    CFD_TRY(dmalloc(&c->counter, 1));
+    CFD_TRY_CUDA(cudaMemset(c->counter, 0, sizeof(unsigned)));
+    CFD_TRY(dmalloc(&c->state, 2));
+    CFD_TRY_CUDA(cudaMallocHost((void**)&c->h_state, 2 * sizeof(DevState)));
+    CFD_TRY_CUDA(cudaEventCreate(&c->ev0));
+    CFD_TRY_CUDA(cudaEventCreate(&c->ev1));
+    CFD_TRY_CUDA(cudaEventCreateWithFlags(&c->ev_switch, cudaEventDisableTiming));
+    CFD_TRY(ensure_partials(c, kVecGrid));
+    CFD_TRY(dmalloc(&c->err, 1));
+    CFD_TRY_CUDA(cudaMemset(c->err, 0, sizeof(int)));
+    CFD_TRY_CUDA(cudaMallocHost((void**)&c->h_err, sizeof(int)));
+    *c->h_err = 0;
+    CFD_TRY_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+    return CFD_OK;
+  }();
+  if (st != CFD_OK) {
+    cfd_context_destroy(c);
+    return st;
+  }
   // Keep freed stream-ordered workspace in the pool for the next solve.
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -469,12 +478,23 @@ cfd_status cfd_context_create(int device, cfd_context** out) {
 
 cfd_status cfd_context_set_stream(cfd_context* ctx, void* stream) {
   if (!ctx) return CFD_ERR_STATE;
-  ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  const cudaStream_t next = stream ? (cudaStream_t)stream : ctx->own;
+  if (next == ctx->stream) return CFD_OK;
+  CFD_TRY_CUDA(cudaSetDevice(ctx->device));
+  // What is queued on the old stream (an asynchronous SpMV, say) runs before
+  // anything queued on the new one: an ordering on the device, the host does
+  // not wait.
+  CFD_TRY_CUDA(cudaEventRecord(ctx->ev_switch, ctx->stream));
+  CFD_TRY_CUDA(cudaStreamWaitEvent(next, ctx->ev_switch, 0));
+  ctx->stream = next;
   return CFD_OK;
 }
 
 cfd_status cfd_context_synchronize(cfd_context* ctx) {
   if (!ctx) return CFD_ERR_STATE;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  CFD_TRY_CUDA(cudaSetDevice(ctx->device));
   CFD_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
   return CFD_OK;
 }
@@ -491,6 +511,7 @@ cfd_status cfd_context_destroy(cfd_context* ctx) {
   if (ctx->h_err) cudaFreeHost(ctx->h_err);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->ev_switch) cudaEventDestroy(ctx->ev_switch);
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
   return CFD_OK;
@@ -538,8 +559,11 @@ cfd_status cfd_csr_create_i32(cfd_context* ctx, int64_t nrows, int64_t ncols, in
 cfd_status cfd_csr_update_values(cfd_csr* a, const double* val) {
   if (!a || !val) return CFD_ERR_STATE;
   std::lock_guard<std::mutex> g(a->ctx->mu);
-  std::copy(val, val + a->host.nnz(), a->host.v.begin());
+  CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+  // Device first: the host mirror (read by AMG setup) takes the new values
+  // only once the device copy and the FP32 cast have succeeded.
   CFD_TRY(devmat_update_values(a->dev, val, a->host.nnz(), false, a->ctx->stream));
+  std::copy(val, val + a->host.nnz(), a->host.v.begin());
   dfree(a->diag64);
   dfree(a->diag32);
   dfree(a->jinv64);

@@ -184,6 +184,7 @@ struct cfd_context {
   cfd::DevState* state = nullptr;  // two states: [0] outer/FP64, [1] inner
   cfd::DevState* h_state = nullptr;  // pinned mirror
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_switch = nullptr;  // orders the old stream before the new one on a stream switch
   int* err = nullptr;    // set by a kernel whose bounded wait ran out
   int* h_err = nullptr;  // pinned mirror
   int num_sms = 148;
