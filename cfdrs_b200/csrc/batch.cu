@@ -514,208 +514,217 @@ static cfd_status validate_batch(int32_t num_systems, const int64_t* sys_row_off
 
 cfd_status cfd_batch_create(cfd_context* ctx, int32_t num_systems, const int64_t* sys_row_offsets,
                             const int64_t* row_ptr, const int32_t* col, const double* val, cfd_batch** out) {
-  if (!out) {
-    set_error("cfd_batch_create: null output handle");
-    return CFD_ERR_STATE;
-  }
-  *out = nullptr;
-  CFD_TRY(validate_batch(num_systems, sys_row_offsets, row_ptr, col, val));
-  if (!ctx) {
-    set_error("cfd_batch_create: null context");
-    return CFD_ERR_STATE;
-  }
-  const int64_t rows = sys_row_offsets[num_systems];
-  const int64_t nnz = row_ptr[rows];
-  std::lock_guard<std::mutex> g(ctx->mu);
-  CFD_TRY_CUDA(cudaSetDevice(ctx->device));
-  cfd_batch* bt = new cfd_batch;
-  bt->ctx = ctx;
-  bt->nsys = num_systems;
-  bt->rows = rows;
-  bt->nnz = nnz;
-  bt->h_sys_row.resize(num_systems + 1);
-  for (int s = 0; s <= num_systems; ++s) bt->h_sys_row[s] = (int)sys_row_offsets[s];
-  std::vector<int> rp32(rows + 1);
-  for (int64_t i = 0; i <= rows; ++i) rp32[i] = (int)row_ptr[i];
-  // Buckets by row count (bucket 0 also takes empty systems), largest system
-  // first inside each bucket.
-  std::vector<int> ord(num_systems);
-  std::iota(ord.begin(), ord.end(), 0);
-  auto nrows = [&](int s) { return bt->h_sys_row[s + 1] - bt->h_sys_row[s]; };
-  auto bucket_of = [&](int s) {
-    int k = 0;
-    while (k + 1 < kBuckets && nrows(s) > kBucketRows[k]) ++k;
-    return k;
-  };
-  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
-    const int ka = bucket_of(a), kb = bucket_of(b);
-    return ka != kb ? ka < kb : nrows(a) > nrows(b);
-  });
-  std::vector<int> sorted = ord;
-  for (int k = 0; k <= kBuckets; ++k) bt->bucket_begin[k] = num_systems;
-  for (int q = num_systems - 1; q >= 0; --q) bt->bucket_begin[bucket_of(sorted[q])] = q;
-  for (int k = kBuckets - 1; k >= 0; --k)
-    if (bt->bucket_begin[k] > bt->bucket_begin[k + 1]) bt->bucket_begin[k] = bt->bucket_begin[k + 1];
-  for (int k = 0; k < kBuckets; ++k) {
-    int nmax = 1, zmax = 1;
-    for (int q = bt->bucket_begin[k]; q < bt->bucket_begin[k + 1]; ++q) {
-      const int sy = sorted[q];
-      nmax = std::max(nmax, nrows(sy));
-      zmax = std::max(zmax, (int)(row_ptr[bt->h_sys_row[sy + 1]] - row_ptr[bt->h_sys_row[sy]]));
+  return guarded("cfd_batch_create", [&]() -> cfd_status {
+    if (!out) {
+      set_error("cfd_batch_create: null output handle");
+      return CFD_ERR_STATE;
     }
-    bt->bucket_nmax[k] = nmax;
-    bt->bucket_zmax[k] = zmax;
-  }
-  cudaStream_t s = ctx->stream;
-  cfd_status st = CFD_OK;
-  auto fail = [&](cfd_status e) {
-    cfd_batch_destroy(bt);
-    return e;
-  };
-  if ((st = dalloc(&bt->sys_row, num_systems + 1)) != CFD_OK) return fail(st);
-  if ((st = dalloc(&bt->rp, rows + 1)) != CFD_OK) return fail(st);
-  if ((st = dalloc(&bt->col, nnz)) != CFD_OK) return fail(st);
-  if ((st = dalloc(&bt->v64, nnz)) != CFD_OK) return fail(st);
-  if ((st = dalloc(&bt->v32, nnz)) != CFD_OK) return fail(st);
-  if ((st = dalloc(&bt->x, rows)) != CFD_OK) return fail(st);
-  if ((st = dalloc(&bt->b, rows)) != CFD_OK) return fail(st);
-  if ((st = dalloc(&bt->term, num_systems)) != CFD_OK) return fail(st);
-  if ((st = dalloc(&bt->iters, num_systems)) != CFD_OK) return fail(st);
-  if ((st = dalloc(&bt->resid, num_systems)) != CFD_OK) return fail(st);
-  if ((st = dalloc(&bt->order, num_systems)) != CFD_OK) return fail(st);
-  if ((st = dalloc(&bt->queues, kBuckets)) != CFD_OK) return fail(st);
-  if ((st = dalloc(&bt->params, 1)) != CFD_OK) return fail(st);
-  if (cudaMallocHost((void**)&bt->h_params, sizeof(BatchParams)) != cudaSuccess) return fail(CFD_ERR_ALLOC);
-  std::vector<float> v32(val, val + nnz);
-  if (cudaMemcpyAsync(bt->sys_row, bt->h_sys_row.data(), (num_systems + 1) * sizeof(int), cudaMemcpyHostToDevice,
-                      s) != cudaSuccess ||
-      cudaMemcpyAsync(bt->rp, rp32.data(), (rows + 1) * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(bt->col, col, nnz * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(bt->v64, val, nnz * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      cudaMemcpyAsync(bt->v32, v32.data(), nnz * sizeof(float), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-      (num_systems > 0 &&
-       cudaMemcpyAsync(bt->order, sorted.data(), num_systems * sizeof(int), cudaMemcpyHostToDevice, s) !=
-           cudaSuccess) ||
-      cudaStreamSynchronize(s) != cudaSuccess) {
-    set_error("cfd_batch_create: upload failed");
-    return fail(CFD_ERR_CUDA);
-  }
-  *out = bt;
-  return CFD_OK;
+    *out = nullptr;
+    CFD_TRY(validate_batch(num_systems, sys_row_offsets, row_ptr, col, val));
+    if (!ctx) {
+      set_error("cfd_batch_create: null context");
+      return CFD_ERR_STATE;
+    }
+    const int64_t rows = sys_row_offsets[num_systems];
+    const int64_t nnz = row_ptr[rows];
+    std::lock_guard<std::mutex> g(ctx->mu);
+    CFD_TRY_CUDA(cudaSetDevice(ctx->device));
+    cfd_batch* bt = new cfd_batch;
+    OnUnwind release([&] { cfd_batch_destroy(bt); });
+    bt->ctx = ctx;
+    bt->nsys = num_systems;
+    bt->rows = rows;
+    bt->nnz = nnz;
+    bt->h_sys_row.resize(num_systems + 1);
+    for (int s = 0; s <= num_systems; ++s) bt->h_sys_row[s] = (int)sys_row_offsets[s];
+    std::vector<int> rp32(rows + 1);
+    for (int64_t i = 0; i <= rows; ++i) rp32[i] = (int)row_ptr[i];
+    // Buckets by row count (bucket 0 also takes empty systems), largest system
+    // first inside each bucket.
+    std::vector<int> ord(num_systems);
+    std::iota(ord.begin(), ord.end(), 0);
+    auto nrows = [&](int s) { return bt->h_sys_row[s + 1] - bt->h_sys_row[s]; };
+    auto bucket_of = [&](int s) {
+      int k = 0;
+      while (k + 1 < kBuckets && nrows(s) > kBucketRows[k]) ++k;
+      return k;
+    };
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+      const int ka = bucket_of(a), kb = bucket_of(b);
+      return ka != kb ? ka < kb : nrows(a) > nrows(b);
+    });
+    std::vector<int> sorted = ord;
+    for (int k = 0; k <= kBuckets; ++k) bt->bucket_begin[k] = num_systems;
+    for (int q = num_systems - 1; q >= 0; --q) bt->bucket_begin[bucket_of(sorted[q])] = q;
+    for (int k = kBuckets - 1; k >= 0; --k)
+      if (bt->bucket_begin[k] > bt->bucket_begin[k + 1]) bt->bucket_begin[k] = bt->bucket_begin[k + 1];
+    for (int k = 0; k < kBuckets; ++k) {
+      int nmax = 1, zmax = 1;
+      for (int q = bt->bucket_begin[k]; q < bt->bucket_begin[k + 1]; ++q) {
+        const int sy = sorted[q];
+        nmax = std::max(nmax, nrows(sy));
+        zmax = std::max(zmax, (int)(row_ptr[bt->h_sys_row[sy + 1]] - row_ptr[bt->h_sys_row[sy]]));
+      }
+      bt->bucket_nmax[k] = nmax;
+      bt->bucket_zmax[k] = zmax;
+    }
+    cudaStream_t s = ctx->stream;
+    cfd_status st = CFD_OK;
+    auto fail = [&](cfd_status e) {
+      cfd_batch_destroy(bt);
+      return e;
+    };
+    if ((st = dalloc(&bt->sys_row, num_systems + 1)) != CFD_OK) return fail(st);
+    if ((st = dalloc(&bt->rp, rows + 1)) != CFD_OK) return fail(st);
+    if ((st = dalloc(&bt->col, nnz)) != CFD_OK) return fail(st);
+    if ((st = dalloc(&bt->v64, nnz)) != CFD_OK) return fail(st);
+    if ((st = dalloc(&bt->v32, nnz)) != CFD_OK) return fail(st);
+    if ((st = dalloc(&bt->x, rows)) != CFD_OK) return fail(st);
+    if ((st = dalloc(&bt->b, rows)) != CFD_OK) return fail(st);
+    if ((st = dalloc(&bt->term, num_systems)) != CFD_OK) return fail(st);
+    if ((st = dalloc(&bt->iters, num_systems)) != CFD_OK) return fail(st);
+    if ((st = dalloc(&bt->resid, num_systems)) != CFD_OK) return fail(st);
+    if ((st = dalloc(&bt->order, num_systems)) != CFD_OK) return fail(st);
+    if ((st = dalloc(&bt->queues, kBuckets)) != CFD_OK) return fail(st);
+    if ((st = dalloc(&bt->params, 1)) != CFD_OK) return fail(st);
+    if (cudaMallocHost((void**)&bt->h_params, sizeof(BatchParams)) != cudaSuccess) return fail(CFD_ERR_ALLOC);
+    std::vector<float> v32(val, val + nnz);
+    if (cudaMemcpyAsync(bt->sys_row, bt->h_sys_row.data(), (num_systems + 1) * sizeof(int), cudaMemcpyHostToDevice,
+                        s) != cudaSuccess ||
+        cudaMemcpyAsync(bt->rp, rp32.data(), (rows + 1) * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(bt->col, col, nnz * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(bt->v64, val, nnz * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(bt->v32, v32.data(), nnz * sizeof(float), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        (num_systems > 0 &&
+         cudaMemcpyAsync(bt->order, sorted.data(), num_systems * sizeof(int), cudaMemcpyHostToDevice, s) !=
+             cudaSuccess) ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      set_error("cfd_batch_create: upload failed");
+      return fail(CFD_ERR_CUDA);
+    }
+    *out = bt;
+    return CFD_OK;
+  });
 }
 
 cfd_status cfd_batch_update_values(cfd_batch* bt, const double* val) {
-  if (!bt || !val) return CFD_ERR_STATE;
-  std::lock_guard<std::mutex> g(bt->ctx->mu);
-  CFD_TRY_CUDA(cudaSetDevice(bt->ctx->device));
-  std::vector<float> v32(val, val + bt->nnz);
-  CFD_TRY_CUDA(cudaMemcpyAsync(bt->v64, val, bt->nnz * sizeof(double), cudaMemcpyHostToDevice, bt->ctx->stream));
-  CFD_TRY_CUDA(
-      cudaMemcpyAsync(bt->v32, v32.data(), bt->nnz * sizeof(float), cudaMemcpyHostToDevice, bt->ctx->stream));
-  CFD_TRY_CUDA(cudaStreamSynchronize(bt->ctx->stream));
-  return CFD_OK;
+  return guarded("cfd_batch_update_values", [&]() -> cfd_status {
+    if (!bt || !val) return CFD_ERR_STATE;
+    std::lock_guard<std::mutex> g(bt->ctx->mu);
+    CFD_TRY_CUDA(cudaSetDevice(bt->ctx->device));
+    std::vector<float> v32(val, val + bt->nnz);
+    CFD_TRY_CUDA(cudaMemcpyAsync(bt->v64, val, bt->nnz * sizeof(double), cudaMemcpyHostToDevice, bt->ctx->stream));
+    CFD_TRY_CUDA(
+        cudaMemcpyAsync(bt->v32, v32.data(), bt->nnz * sizeof(float), cudaMemcpyHostToDevice, bt->ctx->stream));
+    CFD_TRY_CUDA(cudaStreamSynchronize(bt->ctx->stream));
+    return CFD_OK;
+  });
 }
 
 cfd_status cfd_batch_solve(cfd_batch* bt, const cfd_solve_options* opt, const double* b, double* x,
                            const cfd_solver_config* cfg, int32_t* term_out, int32_t* iters_out,
                            double* resid_out, cfd_batch_report* rep) {
-  if (!bt || !opt || !b || !x || !cfg || !rep) {
-    set_error("null argument to cfd_batch_solve");
-    return CFD_ERR_STATE;
-  }
-  if (!(cfg->tolerance >= 0.0) || !(cfg->relative_tolerance >= 0.0) || cfg->max_iterations <= 0 ||
-      opt->solver != CFD_SOLVER_CG || opt->precond != CFD_PRECOND_JACOBI || opt->precision < 0 ||
-      opt->precision > 1) {
-    set_error("cfd_batch_solve: needs CG with Jacobi, valid tolerances and a positive iteration budget");
-    return CFD_ERR_CONFIG;
-  }
-  std::lock_guard<std::mutex> g(bt->ctx->mu);
-  cfd_context* ctx = bt->ctx;
-  CFD_TRY_CUDA(cudaSetDevice(ctx->device));
-  cudaStream_t s = ctx->stream;
-  const int prec = opt->precision;
-  std::memset(rep, 0, sizeof(*rep));
-  rep->num_systems = bt->nsys;
-  if (bt->nsys == 0) return CFD_OK;
-  const cudaMemcpyKind in = opt->memory == CFD_MEMORY_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-  const cudaMemcpyKind outk = opt->memory == CFD_MEMORY_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-  CFD_TRY(capture_graph(bt, prec));
-  CFD_TRY_CUDA(cudaEventRecord(ctx->ev0, s));
-  CFD_TRY(set_params(bt, *cfg, *opt));
-  CFD_TRY_CUDA(cudaMemcpyAsync(bt->b, b, bt->rows * sizeof(double), in, s));
-  CFD_TRY_CUDA(cudaMemcpyAsync(bt->x, x, bt->rows * sizeof(double), in, s));
-  CFD_TRY_CUDA(cudaGraphLaunch(bt->graph[prec], s));
-  CFD_TRY_CUDA(cudaMemcpyAsync(x, bt->x, bt->rows * sizeof(double), outk, s));
-  CFD_TRY_CUDA(cudaEventRecord(ctx->ev1, s));
-  std::vector<int> term(bt->nsys), iters(bt->nsys);
-  std::vector<double> resid(bt->nsys);
-  CFD_TRY_CUDA(cudaMemcpyAsync(term.data(), bt->term, bt->nsys * sizeof(int), cudaMemcpyDeviceToHost, s));
-  CFD_TRY_CUDA(cudaMemcpyAsync(iters.data(), bt->iters, bt->nsys * sizeof(int), cudaMemcpyDeviceToHost, s));
-  CFD_TRY_CUDA(cudaMemcpyAsync(resid.data(), bt->resid, bt->nsys * sizeof(double), cudaMemcpyDeviceToHost, s));
-  CFD_TRY_CUDA(cudaStreamSynchronize(s));
-  float ms = 0.f;
-  CFD_TRY_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-  for (int k = 0; k < bt->nsys; ++k) {
-    if (term[k] == CFD_TERM_CONVERGED || term[k] == CFD_TERM_INITIAL_RESIDUAL) rep->converged_systems++;
-    rep->total_iterations += iters[k];
-    rep->max_iterations = std::max(rep->max_iterations, iters[k]);
-    rep->max_rel_residual = std::max(rep->max_rel_residual, resid[k]);
-  }
-  rep->device_ms = ms;
-  if (term_out) std::copy(term.begin(), term.end(), term_out);
-  if (iters_out) std::copy(iters.begin(), iters.end(), iters_out);
-  if (resid_out) std::copy(resid.begin(), resid.end(), resid_out);
-  return CFD_OK;
+  return guarded("cfd_batch_solve", [&]() -> cfd_status {
+    if (!bt || !opt || !b || !x || !cfg || !rep) {
+      set_error("null argument to cfd_batch_solve");
+      return CFD_ERR_STATE;
+    }
+    if (!(cfg->tolerance >= 0.0) || !(cfg->relative_tolerance >= 0.0) || cfg->max_iterations <= 0 ||
+        opt->solver != CFD_SOLVER_CG || opt->precond != CFD_PRECOND_JACOBI || opt->precision < 0 ||
+        opt->precision > 1) {
+      set_error("cfd_batch_solve: needs CG with Jacobi, valid tolerances and a positive iteration budget");
+      return CFD_ERR_CONFIG;
+    }
+    std::lock_guard<std::mutex> g(bt->ctx->mu);
+    cfd_context* ctx = bt->ctx;
+    CFD_TRY_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const int prec = opt->precision;
+    std::memset(rep, 0, sizeof(*rep));
+    rep->num_systems = bt->nsys;
+    if (bt->nsys == 0) return CFD_OK;
+    const cudaMemcpyKind in = opt->memory == CFD_MEMORY_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    const cudaMemcpyKind outk = opt->memory == CFD_MEMORY_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    CFD_TRY(capture_graph(bt, prec));
+    CFD_TRY_CUDA(cudaEventRecord(ctx->ev0, s));
+    CFD_TRY(set_params(bt, *cfg, *opt));
+    CFD_TRY_CUDA(cudaMemcpyAsync(bt->b, b, bt->rows * sizeof(double), in, s));
+    CFD_TRY_CUDA(cudaMemcpyAsync(bt->x, x, bt->rows * sizeof(double), in, s));
+    CFD_TRY_CUDA(cudaGraphLaunch(bt->graph[prec], s));
+    CFD_TRY_CUDA(cudaMemcpyAsync(x, bt->x, bt->rows * sizeof(double), outk, s));
+    CFD_TRY_CUDA(cudaEventRecord(ctx->ev1, s));
+    std::vector<int> term(bt->nsys), iters(bt->nsys);
+    std::vector<double> resid(bt->nsys);
+    CFD_TRY_CUDA(cudaMemcpyAsync(term.data(), bt->term, bt->nsys * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CFD_TRY_CUDA(cudaMemcpyAsync(iters.data(), bt->iters, bt->nsys * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CFD_TRY_CUDA(cudaMemcpyAsync(resid.data(), bt->resid, bt->nsys * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CFD_TRY_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    CFD_TRY_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    for (int k = 0; k < bt->nsys; ++k) {
+      if (term[k] == CFD_TERM_CONVERGED || term[k] == CFD_TERM_INITIAL_RESIDUAL) rep->converged_systems++;
+      rep->total_iterations += iters[k];
+      rep->max_iterations = std::max(rep->max_iterations, iters[k]);
+      rep->max_rel_residual = std::max(rep->max_rel_residual, resid[k]);
+    }
+    rep->device_ms = ms;
+    if (term_out) std::copy(term.begin(), term.end(), term_out);
+    if (iters_out) std::copy(iters.begin(), iters.end(), iters_out);
+    if (resid_out) std::copy(resid.begin(), resid.end(), resid_out);
+    return CFD_OK;
+  });
 }
 
 cfd_status cfd_batch_autotune(cfd_batch* bt, int32_t precision, int32_t sample_iterations) {
-  if (!bt || precision < 0 || precision > 1 || sample_iterations <= 0) return CFD_ERR_CONFIG;
-  std::lock_guard<std::mutex> g(bt->ctx->mu);
-  cfd_context* ctx = bt->ctx;
-  CFD_TRY_CUDA(cudaSetDevice(ctx->device));
-  cudaStream_t s = ctx->stream;
-  // Representative inputs: x = 0, b = 1; a fixed iteration budget and a zero
-  // tolerance make every candidate do the same work.
-  std::vector<double> ones(bt->rows, 1.0);
-  CFD_TRY_CUDA(cudaMemcpyAsync(bt->b, ones.data(), bt->rows * sizeof(double), cudaMemcpyHostToDevice, s));
-  cfd_solver_config cfg{0.0, 0.0, sample_iterations};
-  cfd_solve_options opt;
-  cfd_solve_options_default(&opt);
-  opt.max_outer = 1;
-  opt.inner_tolerance = 0.0;
-  CFD_TRY(set_params(bt, cfg, opt));
-  bt->h_params->inner_tol = 0.0;
-  CFD_TRY_CUDA(cudaMemcpyAsync(bt->params, bt->h_params, sizeof(BatchParams), cudaMemcpyHostToDevice, s));
-  for (int k = 0; k < kBuckets; ++k) {
-    if (bt->bucket_begin[k + 1] == bt->bucket_begin[k]) continue;
-    float best = 1e30f;
-    int best_t = bt->threads[precision][k];
-    for (int t : kCandidates) {
-      if (t > 2 * std::max(32, bt->bucket_nmax[k])) continue;
-      float ms_min = 1e30f;
-      for (int rep = 0; rep < 2; ++rep) {
-        CFD_TRY_CUDA(cudaMemsetAsync(bt->x, 0, bt->rows * sizeof(double), s));
-        CFD_TRY_CUDA(cudaMemsetAsync(bt->queues + k, 0, sizeof(unsigned), s));
-        CFD_TRY_CUDA(cudaEventRecord(ctx->ev0, s));
-        cfd_status st = precision ? run_bucket<true>(bt, k, t, s) : run_bucket<false>(bt, k, t, s);
-        if (st == CFD_ERR_CONFIG) break;  // does not fit at this width
-        CFD_TRY(st);
-        CFD_TRY_CUDA(cudaEventRecord(ctx->ev1, s));
-        CFD_TRY_CUDA(cudaStreamSynchronize(s));
-        float ms = 0.f;
-        CFD_TRY_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-        ms_min = std::min(ms_min, ms);
+  return guarded("cfd_batch_autotune", [&]() -> cfd_status {
+    if (!bt || precision < 0 || precision > 1 || sample_iterations <= 0) return CFD_ERR_CONFIG;
+    std::lock_guard<std::mutex> g(bt->ctx->mu);
+    cfd_context* ctx = bt->ctx;
+    CFD_TRY_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    // Representative inputs: x = 0, b = 1; a fixed iteration budget and a zero
+    // tolerance make every candidate do the same work.
+    std::vector<double> ones(bt->rows, 1.0);
+    CFD_TRY_CUDA(cudaMemcpyAsync(bt->b, ones.data(), bt->rows * sizeof(double), cudaMemcpyHostToDevice, s));
+    cfd_solver_config cfg{0.0, 0.0, sample_iterations};
+    cfd_solve_options opt;
+    cfd_solve_options_default(&opt);
+    opt.max_outer = 1;
+    opt.inner_tolerance = 0.0;
+    CFD_TRY(set_params(bt, cfg, opt));
+    bt->h_params->inner_tol = 0.0;
+    CFD_TRY_CUDA(cudaMemcpyAsync(bt->params, bt->h_params, sizeof(BatchParams), cudaMemcpyHostToDevice, s));
+    for (int k = 0; k < kBuckets; ++k) {
+      if (bt->bucket_begin[k + 1] == bt->bucket_begin[k]) continue;
+      float best = 1e30f;
+      int best_t = bt->threads[precision][k];
+      for (int t : kCandidates) {
+        if (t > 2 * std::max(32, bt->bucket_nmax[k])) continue;
+        float ms_min = 1e30f;
+        for (int rep = 0; rep < 2; ++rep) {
+          CFD_TRY_CUDA(cudaMemsetAsync(bt->x, 0, bt->rows * sizeof(double), s));
+          CFD_TRY_CUDA(cudaMemsetAsync(bt->queues + k, 0, sizeof(unsigned), s));
+          CFD_TRY_CUDA(cudaEventRecord(ctx->ev0, s));
+          cfd_status st = precision ? run_bucket<true>(bt, k, t, s) : run_bucket<false>(bt, k, t, s);
+          if (st == CFD_ERR_CONFIG) break;  // does not fit at this width
+          CFD_TRY(st);
+          CFD_TRY_CUDA(cudaEventRecord(ctx->ev1, s));
+          CFD_TRY_CUDA(cudaStreamSynchronize(s));
+          float ms = 0.f;
+          CFD_TRY_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+          ms_min = std::min(ms_min, ms);
+        }
+        if (ms_min < best) {
+          best = ms_min;
+          best_t = t;
+        }
       }
-      if (ms_min < best) {
-        best = ms_min;
-        best_t = t;
-      }
+      bt->threads[precision][k] = best_t;
     }
-    bt->threads[precision][k] = best_t;
-  }
-  bt->tuned[precision] = true;
-  drop_graphs(bt);
-  return CFD_OK;
+    bt->tuned[precision] = true;
+    drop_graphs(bt);
+    return CFD_OK;
+  });
 }
 
 cfd_status cfd_batch_config(const cfd_batch* bt, int32_t precision, int32_t* bucket_rows, int32_t* threads,

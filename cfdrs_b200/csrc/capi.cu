@@ -432,48 +432,50 @@ const char* cfd_last_error(void) { return g_err; }
 const char* cfd_version(void) { return "cfdgpu 0.1.0 (sm_100a)"; }
 
 cfd_status cfd_context_create(int device, cfd_context** out) {
-  if (!out) return CFD_ERR_CONFIG;
-  *out = nullptr;
-  int count = 0;
-  CFD_TRY_CUDA(cudaGetDeviceCount(&count));
-  if (device < 0 || device >= count) {
-    set_error("device %d not present (%d devices)", device, count);
-    return CFD_ERR_CONFIG;
-  }
-  CFD_TRY_CUDA(cudaSetDevice(device));
-  cfd_context* c = new cfd_context;
-  c->device = device;
-  // Any failure below releases what was made so far (destroy skips nulls).
-  const cfd_status st = [&]() -> cfd_status {
-    CFD_TRY_CUDA(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
-    c->stream = c->own;
-    CFD_TRY(dmalloc(&c->counter, 1));
-    CFD_TRY_CUDA(cudaMemset(c->counter, 0, sizeof(unsigned)));
-    CFD_TRY(dmalloc(&c->state, 2));
-    CFD_TRY_CUDA(cudaMallocHost((void**)&c->h_state, 2 * sizeof(DevState)));
-    CFD_TRY_CUDA(cudaEventCreate(&c->ev0));
-    CFD_TRY_CUDA(cudaEventCreate(&c->ev1));
-    CFD_TRY_CUDA(cudaEventCreateWithFlags(&c->ev_switch, cudaEventDisableTiming));
-    CFD_TRY(ensure_partials(c, kVecGrid));
-    CFD_TRY(dmalloc(&c->err, 1));
-    CFD_TRY_CUDA(cudaMemset(c->err, 0, sizeof(int)));
-    CFD_TRY_CUDA(cudaMallocHost((void**)&c->h_err, sizeof(int)));
-    *c->h_err = 0;
-    CFD_TRY_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+  return guarded("cfd_context_create", [&]() -> cfd_status {
+    if (!out) return CFD_ERR_CONFIG;
+    *out = nullptr;
+    int count = 0;
+    CFD_TRY_CUDA(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) {
+      set_error("device %d not present (%d devices)", device, count);
+      return CFD_ERR_CONFIG;
+    }
+    CFD_TRY_CUDA(cudaSetDevice(device));
+    cfd_context* c = new cfd_context;
+    c->device = device;
+    // Any failure below releases what was made so far (destroy skips nulls).
+    const cfd_status st = [&]() -> cfd_status {
+      CFD_TRY_CUDA(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+      c->stream = c->own;
+      CFD_TRY(dmalloc(&c->counter, 1));
+      CFD_TRY_CUDA(cudaMemset(c->counter, 0, sizeof(unsigned)));
+      CFD_TRY(dmalloc(&c->state, 2));
+      CFD_TRY_CUDA(cudaMallocHost((void**)&c->h_state, 2 * sizeof(DevState)));
+      CFD_TRY_CUDA(cudaEventCreate(&c->ev0));
+      CFD_TRY_CUDA(cudaEventCreate(&c->ev1));
+      CFD_TRY_CUDA(cudaEventCreateWithFlags(&c->ev_switch, cudaEventDisableTiming));
+      CFD_TRY(ensure_partials(c, kVecGrid));
+      CFD_TRY(dmalloc(&c->err, 1));
+      CFD_TRY_CUDA(cudaMemset(c->err, 0, sizeof(int)));
+      CFD_TRY_CUDA(cudaMallocHost((void**)&c->h_err, sizeof(int)));
+      *c->h_err = 0;
+      CFD_TRY_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+      return CFD_OK;
+    }();
+    if (st != CFD_OK) {
+      cfd_context_destroy(c);
+      return st;
+    }
+    // Keep freed stream-ordered workspace in the pool for the next solve.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    *out = c;
     return CFD_OK;
-  }();
-  if (st != CFD_OK) {
-    cfd_context_destroy(c);
-    return st;
-  }
-  // Keep freed stream-ordered workspace in the pool for the next solve.
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-    uint64_t thr = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-  }
-  *out = c;
-  return CFD_OK;
+  });
 }
 
 cfd_status cfd_context_set_stream(cfd_context* ctx, void* stream) {
@@ -520,30 +522,36 @@ cfd_status cfd_context_destroy(cfd_context* ctx) {
 static cfd_status csr_create_common(cfd_context* ctx, int64_t nrows, int64_t ncols, int64_t nnz,
                                     const int64_t* rp, const int32_t* c32, const int64_t* c64, const double* val,
                                     cfd_csr** out) {
-  if (!ctx || !out) {
-    set_error("null context or output handle");
-    return CFD_ERR_STATE;
-  }
-  *out = nullptr;
-  CFD_TRY(validate_csr(nrows, ncols, nnz, rp, c32, c64));
-  if (nnz > 0 && !val) {
-    set_error("null value array");
-    return CFD_ERR_DIM;
-  }
-  CFD_TRY_CUDA(cudaSetDevice(ctx->device));
-  std::lock_guard<std::mutex> g(ctx->mu);
-  cfd_csr* a = new cfd_csr;
-  a->ctx = ctx;
-  a->host = host_from(nrows, ncols, nnz, rp, c32, c64, val);
-  cfd_status s = devmat_upload(a->dev, a->host, false, ctx->stream);
-  if (s == CFD_OK) s = ensure_partials(ctx, a->dev.nblk);
-  if (s != CFD_OK) {
-    devmat_free(a->dev);
-    delete a;
-    return s;
-  }
-  *out = a;
-  return CFD_OK;
+  return guarded("cfd_csr_create", [&]() -> cfd_status {
+    if (!ctx || !out) {
+      set_error("null context or output handle");
+      return CFD_ERR_STATE;
+    }
+    *out = nullptr;
+    CFD_TRY(validate_csr(nrows, ncols, nnz, rp, c32, c64));
+    if (nnz > 0 && !val) {
+      set_error("null value array");
+      return CFD_ERR_DIM;
+    }
+    CFD_TRY_CUDA(cudaSetDevice(ctx->device));
+    std::lock_guard<std::mutex> g(ctx->mu);
+    cfd_csr* a = new cfd_csr;
+    OnUnwind release([&] {
+      devmat_free(a->dev);
+      delete a;
+    });
+    a->ctx = ctx;
+    a->host = host_from(nrows, ncols, nnz, rp, c32, c64, val);
+    cfd_status s = devmat_upload(a->dev, a->host, false, ctx->stream);
+    if (s == CFD_OK) s = ensure_partials(ctx, a->dev.nblk);
+    if (s != CFD_OK) {
+      devmat_free(a->dev);
+      delete a;
+      return s;
+    }
+    *out = a;
+    return CFD_OK;
+  });
 }
 
 cfd_status cfd_csr_create(cfd_context* ctx, int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* row_ptr,
@@ -557,19 +565,21 @@ cfd_status cfd_csr_create_i32(cfd_context* ctx, int64_t nrows, int64_t ncols, in
 }
 
 cfd_status cfd_csr_update_values(cfd_csr* a, const double* val) {
-  if (!a || !val) return CFD_ERR_STATE;
-  std::lock_guard<std::mutex> g(a->ctx->mu);
-  CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
-  // Device first: the host mirror (read by AMG setup) takes the new values
-  // only once the device copy and the FP32 cast have succeeded.
-  CFD_TRY(devmat_update_values(a->dev, val, a->host.nnz(), false, a->ctx->stream));
-  std::copy(val, val + a->host.nnz(), a->host.v.begin());
-  dfree(a->diag64);
-  dfree(a->diag32);
-  dfree(a->jinv64);
-  dfree(a->jinv32);
-  a->jacobi_status = -1;
-  return CFD_OK;
+  return guarded("cfd_csr_update_values", [&]() -> cfd_status {
+    if (!a || !val) return CFD_ERR_STATE;
+    std::lock_guard<std::mutex> g(a->ctx->mu);
+    CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+    // Device first: the host mirror (read by AMG setup) takes the new values
+    // only once the device copy and the FP32 cast have succeeded.
+    CFD_TRY(devmat_update_values(a->dev, val, a->host.nnz(), false, a->ctx->stream));
+    std::copy(val, val + a->host.nnz(), a->host.v.begin());
+    dfree(a->diag64);
+    dfree(a->diag32);
+    dfree(a->jinv64);
+    dfree(a->jinv32);
+    a->jacobi_status = -1;
+    return CFD_OK;
+  });
 }
 
 cfd_status cfd_csr_info(const cfd_csr* a, int64_t* nrows, int64_t* ncols, int64_t* nnz) {
@@ -617,34 +627,36 @@ cfd_status cfd_csr_set_path(cfd_csr* a, int32_t fp32, int32_t path) {
 
 cfd_status cfd_layout_check(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* row_ptr, const int32_t* col,
                             const double* val, const double* x, double* y, cfd_layout_info* out) {
-  CFD_TRY(validate_csr(nrows, ncols, nnz, row_ptr, col, nullptr));
-  if ((nnz > 0 && !val) || (ncols > 0 && !x) || (nrows > 0 && !y)) {
-    set_error("cfd_layout_check: null array");
-    return CFD_ERR_DIM;
-  }
-  const HostCsr h = host_from(nrows, ncols, nnz, row_ptr, col, nullptr, val);
-  const int tpr = threads_per_row(h.nnz(), h.nrows);
-  const std::vector<int> blk = row_partition(h.rp.data(), h.nrows, tpr);
-  HostLayout L;
-  encode_layout(h, blk, L);
-  std::string why;
-  int64_t staged = 0;
-  int maxw = 0;
-  if (!check_layout(h, blk, L, x, y, &why, &staged, &maxw)) {
-    set_error("layout check: %s", why.c_str());
-    return CFD_ERR_STATE;
-  }
-  if (out) {
-    *out = cfd_layout_info{};
-    out->blocks = (int64_t)blk.size() - 1;
-    out->compressed_nnz = L.compressed_nnz;
-    out->all_compressed = L.all_compressed ? 1 : 0;
-    out->x_staged = L.xs ? 1 : 0;
-    out->threads_per_row = tpr;
-    out->max_windows = maxw;
-    out->staged_x_entries = staged;
-  }
-  return CFD_OK;
+  return guarded("cfd_layout_check", [&]() -> cfd_status {
+    CFD_TRY(validate_csr(nrows, ncols, nnz, row_ptr, col, nullptr));
+    if ((nnz > 0 && !val) || (ncols > 0 && !x) || (nrows > 0 && !y)) {
+      set_error("cfd_layout_check: null array");
+      return CFD_ERR_DIM;
+    }
+    const HostCsr h = host_from(nrows, ncols, nnz, row_ptr, col, nullptr, val);
+    const int tpr = threads_per_row(h.nnz(), h.nrows);
+    const std::vector<int> blk = row_partition(h.rp.data(), h.nrows, tpr);
+    HostLayout L;
+    encode_layout(h, blk, L);
+    std::string why;
+    int64_t staged = 0;
+    int maxw = 0;
+    if (!check_layout(h, blk, L, x, y, &why, &staged, &maxw)) {
+      set_error("layout check: %s", why.c_str());
+      return CFD_ERR_STATE;
+    }
+    if (out) {
+      *out = cfd_layout_info{};
+      out->blocks = (int64_t)blk.size() - 1;
+      out->compressed_nnz = L.compressed_nnz;
+      out->all_compressed = L.all_compressed ? 1 : 0;
+      out->x_staged = L.xs ? 1 : 0;
+      out->threads_per_row = tpr;
+      out->max_windows = maxw;
+      out->staged_x_entries = staged;
+    }
+    return CFD_OK;
+  });
 }
 
 cfd_status cfd_csr_destroy(cfd_csr* a) {
@@ -661,19 +673,23 @@ cfd_status cfd_csr_destroy(cfd_csr* a) {
 }
 
 cfd_status cfd_spmv(cfd_csr* a, const double* x, double* y) {
-  if (!a || !x || !y) return CFD_ERR_STATE;
-  std::lock_guard<std::mutex> g(a->ctx->mu);
-  CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
-  CFD_TRY(spmv_fp64(a, x, y));
-  return check_device_flag(a->ctx);
+  return guarded("cfd_spmv", [&]() -> cfd_status {
+    if (!a || !x || !y) return CFD_ERR_STATE;
+    std::lock_guard<std::mutex> g(a->ctx->mu);
+    CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+    CFD_TRY(spmv_fp64(a, x, y));
+    return check_device_flag(a->ctx);
+  });
 }
 
 cfd_status cfd_spmv_f32(cfd_csr* a, const float* x, float* y) {
-  if (!a || !x || !y) return CFD_ERR_STATE;
-  std::lock_guard<std::mutex> g(a->ctx->mu);
-  CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
-  CFD_TRY(spmv_fp32(a, x, y));
-  return check_device_flag(a->ctx);
+  return guarded("cfd_spmv_f32", [&]() -> cfd_status {
+    if (!a || !x || !y) return CFD_ERR_STATE;
+    std::lock_guard<std::mutex> g(a->ctx->mu);
+    CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+    CFD_TRY(spmv_fp32(a, x, y));
+    return check_device_flag(a->ctx);
+  });
 }
 
 void cfd_amg_config_default(cfd_amg_config* c) {
@@ -717,79 +733,92 @@ static cfd_status need_device_hierarchy(const cfd_amg* amg, const char* what) {
 }
 
 cfd_status cfd_amg_setup(cfd_csr* a, const cfd_amg_config* cfg, cfd_amg** out) {
-  if (!a || !cfg || !out) return CFD_ERR_STATE;
-  *out = nullptr;
-  CFD_TRY(check_amg_config(cfg));
-  if (a->host.nrows != a->host.ncols) {
-    set_error("AMG needs a square matrix");
-    return CFD_ERR_DIM;
-  }
-  std::lock_guard<std::mutex> g(a->ctx->mu);
-  CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
-  auto t0 = std::chrono::steady_clock::now();
-  cfd_amg* amg = new cfd_amg;
-  amg->ctx = a->ctx;
-  amg->cfg = *cfg;
-  amg->host = build_hierarchy(a->host, *cfg);
-  cfd_status s = amg_upload(amg, false);
-  if (s != CFD_OK) {
-    amg_free_device(amg);
-    delete amg;
-    return s;
-  }
-  amg->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  *out = amg;
-  return CFD_OK;
+  return guarded("cfd_amg_setup", [&]() -> cfd_status {
+    if (!a || !cfg || !out) return CFD_ERR_STATE;
+    *out = nullptr;
+    CFD_TRY(check_amg_config(cfg));
+    if (a->host.nrows != a->host.ncols) {
+      set_error("AMG needs a square matrix");
+      return CFD_ERR_DIM;
+    }
+    std::lock_guard<std::mutex> g(a->ctx->mu);
+    CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+    auto t0 = std::chrono::steady_clock::now();
+    cfd_amg* amg = new cfd_amg;
+    OnUnwind release([&] {
+      amg_free_device(amg);
+      delete amg;
+    });
+    amg->ctx = a->ctx;
+    amg->cfg = *cfg;
+    amg->host = build_hierarchy(a->host, *cfg);
+    cfd_status s = amg_upload(amg, false);
+    if (s != CFD_OK) {
+      amg_free_device(amg);
+      delete amg;
+      return s;
+    }
+    amg->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = amg;
+    return CFD_OK;
+  });
 }
 
 cfd_status cfd_amg_setup_host(int64_t n, const int64_t* row_ptr, const int64_t* col, const double* val,
                               const cfd_amg_config* cfg, cfd_amg** out) {
-  if (!cfg || !out) return CFD_ERR_STATE;
-  *out = nullptr;
-  CFD_TRY(check_amg_config(cfg));
-  if (n < 0 || !row_ptr) {
-    set_error("invalid CSR arguments");
-    return CFD_ERR_DIM;
-  }
-  const int64_t nnz = row_ptr[n];
-  CFD_TRY(validate_csr(n, n, nnz, row_ptr, nullptr, col));
-  if (nnz > 0 && !val) {
-    set_error("null value array");
-    return CFD_ERR_DIM;
-  }
-  auto t0 = std::chrono::steady_clock::now();
-  cfd_amg* amg = new cfd_amg;
-  amg->cfg = *cfg;
-  amg->host = build_hierarchy(host_from(n, n, nnz, row_ptr, nullptr, col, val), *cfg);
-  amg->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  *out = amg;
-  return CFD_OK;
+  return guarded("cfd_amg_setup_host", [&]() -> cfd_status {
+    if (!cfg || !out) return CFD_ERR_STATE;
+    *out = nullptr;
+    CFD_TRY(check_amg_config(cfg));
+    if (n < 0 || !row_ptr) {
+      set_error("invalid CSR arguments");
+      return CFD_ERR_DIM;
+    }
+    const int64_t nnz = row_ptr[n];
+    CFD_TRY(validate_csr(n, n, nnz, row_ptr, nullptr, col));
+    if (nnz > 0 && !val) {
+      set_error("null value array");
+      return CFD_ERR_DIM;
+    }
+    auto t0 = std::chrono::steady_clock::now();
+    cfd_amg* amg = new cfd_amg;
+    OnUnwind release([&] { delete amg; });
+    amg->cfg = *cfg;
+    amg->host = build_hierarchy(host_from(n, n, nnz, row_ptr, nullptr, col, val), *cfg);
+    amg->setup_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    *out = amg;
+    return CFD_OK;
+  });
 }
 
 cfd_status cfd_amg_recompute(cfd_amg* amg, cfd_csr* a) {
-  if (!amg || !a) return CFD_ERR_STATE;
-  if (amg->host.empty()) return CFD_ERR_STATE;
-  CFD_TRY(need_device_hierarchy(amg, "cfd_amg_recompute"));
-  if (a->host.nrows != amg->host[0].A.nrows || a->host.nnz() != amg->host[0].A.nnz()) {
-    set_error("recompute needs the hierarchy's sparsity pattern");
-    return CFD_ERR_DIM;
-  }
-  if (a->ctx != amg->ctx) {
-    set_error("recompute: the matrix and the hierarchy belong to different contexts");
-    return CFD_ERR_STATE;
-  }
-  std::lock_guard<std::mutex> g(a->ctx->mu);
-  CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
-  return amg_recompute_device(amg, a);
+  return guarded("cfd_amg_recompute", [&]() -> cfd_status {
+    if (!amg || !a) return CFD_ERR_STATE;
+    if (amg->host.empty()) return CFD_ERR_STATE;
+    CFD_TRY(need_device_hierarchy(amg, "cfd_amg_recompute"));
+    if (a->host.nrows != amg->host[0].A.nrows || a->host.nnz() != amg->host[0].A.nnz()) {
+      set_error("recompute needs the hierarchy's sparsity pattern");
+      return CFD_ERR_DIM;
+    }
+    if (a->ctx != amg->ctx) {
+      set_error("recompute: the matrix and the hierarchy belong to different contexts");
+      return CFD_ERR_STATE;
+    }
+    std::lock_guard<std::mutex> g(a->ctx->mu);
+    CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+    return amg_recompute_device(amg, a);
+  });
 }
 
 cfd_status cfd_amg_apply(cfd_amg* amg, const double* r, double* z) {
-  if (!amg || !r || !z) return CFD_ERR_STATE;
-  CFD_TRY(need_device_hierarchy(amg, "cfd_amg_apply"));
-  std::lock_guard<std::mutex> g(amg->ctx->mu);
-  CFD_TRY_CUDA(cudaSetDevice(amg->ctx->device));
-  CFD_TRY(amg_apply_fp64(amg, r, z));
-  return check_device_flag(amg->ctx);
+  return guarded("cfd_amg_apply", [&]() -> cfd_status {
+    if (!amg || !r || !z) return CFD_ERR_STATE;
+    CFD_TRY(need_device_hierarchy(amg, "cfd_amg_apply"));
+    std::lock_guard<std::mutex> g(amg->ctx->mu);
+    CFD_TRY_CUDA(cudaSetDevice(amg->ctx->device));
+    CFD_TRY(amg_apply_fp64(amg, r, z));
+    return check_device_flag(amg->ctx);
+  });
 }
 
 cfd_status cfd_amg_set_path(cfd_amg* amg, int32_t fp32, int32_t path) {
@@ -833,24 +862,26 @@ cfd_status cfd_amg_stats(const cfd_amg* amg, cfd_amg_stats_t* out) {
 
 cfd_status cfd_amg_level(const cfd_amg* amg, int level, int which, int64_t* nrows, int64_t* ncols, int64_t* nnz,
                          int64_t* row_ptr, int64_t* col, double* val) {
-  if (!amg || level < 0 || level >= (int)amg->host.size() || which < 0 || which > 2) return CFD_ERR_DIM;
-  if (which == 0 && val && amg->host_values_stale) {
-    cfd_amg* mut = const_cast<cfd_amg*>(amg);  // the host mirror is a cache of the device values
-    std::lock_guard<std::mutex> g(mut->ctx->mu);
-    CFD_TRY_CUDA(cudaSetDevice(mut->ctx->device));
-    CFD_TRY(amg_sync_host_values(mut));
-  }
-  const HostLevel& L = amg->host[level];
-  if (which > 0 && level + 1 == (int)amg->host.size()) return CFD_ERR_DIM;
-  const HostCsr& m = which == 0 ? L.A : (which == 1 ? L.P : L.R);
-  if (nrows) *nrows = m.nrows;
-  if (ncols) *ncols = m.ncols;
-  if (nnz) *nnz = m.nnz();
-  if (row_ptr) std::copy(m.rp.begin(), m.rp.end(), row_ptr);
-  if (col)
-    for (int64_t k = 0; k < m.nnz(); ++k) col[k] = m.ci[k];
-  if (val) std::copy(m.v.begin(), m.v.end(), val);
-  return CFD_OK;
+  return guarded("cfd_amg_level", [&]() -> cfd_status {
+    if (!amg || level < 0 || level >= (int)amg->host.size() || which < 0 || which > 2) return CFD_ERR_DIM;
+    if (which == 0 && val && amg->host_values_stale) {
+      cfd_amg* mut = const_cast<cfd_amg*>(amg);  // the host mirror is a cache of the device values
+      std::lock_guard<std::mutex> g(mut->ctx->mu);
+      CFD_TRY_CUDA(cudaSetDevice(mut->ctx->device));
+      CFD_TRY(amg_sync_host_values(mut));
+    }
+    const HostLevel& L = amg->host[level];
+    if (which > 0 && level + 1 == (int)amg->host.size()) return CFD_ERR_DIM;
+    const HostCsr& m = which == 0 ? L.A : (which == 1 ? L.P : L.R);
+    if (nrows) *nrows = m.nrows;
+    if (ncols) *ncols = m.ncols;
+    if (nnz) *nnz = m.nnz();
+    if (row_ptr) std::copy(m.rp.begin(), m.rp.end(), row_ptr);
+    if (col)
+      for (int64_t k = 0; k < m.nnz(); ++k) col[k] = m.ci[k];
+    if (val) std::copy(m.v.begin(), m.v.end(), val);
+    return CFD_OK;
+  });
 }
 
 cfd_status cfd_amg_destroy(cfd_amg* amg) {
@@ -877,42 +908,44 @@ void cfd_solve_options_default(cfd_solve_options* o) {
 
 cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, const double* b, double* x,
                      const cfd_solver_config* cfg, cfd_solve_report* rep) {
-  if (!a || !opt || !b || !x || !cfg || !rep) {
-    set_error("null argument to cfd_solve");
-    return CFD_ERR_STATE;
-  }
-  // convergence_policy (krylov.rs:123-139) rejects non-finite or negative
-  // tolerances and a zero iteration budget at construction.
-  if (!(cfg->tolerance >= 0.0) || !(cfg->relative_tolerance >= 0.0) || !std::isfinite(cfg->tolerance) ||
-      !std::isfinite(cfg->relative_tolerance) || cfg->max_iterations <= 0) {
-    set_error("invalid iterative solver configuration: tolerance %g, relative %g, max_iterations %lld",
-              cfg->tolerance, cfg->relative_tolerance, (long long)cfg->max_iterations);
-    return CFD_ERR_CONFIG;
-  }
-  if (opt->solver < 0 || opt->solver > 2 || opt->precond < 0 || opt->precond > 2 || opt->precision < 0 ||
-      opt->precision > 1 || opt->memory < 0 || opt->memory > 1 || (opt->solver == CFD_SOLVER_GMRES && opt->restart < 1)) {
-    set_error("invalid solve options");
-    return CFD_ERR_CONFIG;
-  }
-  if (a->host.nrows != a->host.ncols) {
-    set_error("Krylov solve needs a square matrix (%lld x %lld)", (long long)a->host.nrows,
-              (long long)a->host.ncols);
-    return CFD_ERR_DIM;
-  }
-  std::lock_guard<std::mutex> g(a->ctx->mu);
-  CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
-  CFD_TRY(check_precond(a, *opt, amg));
-  a->ctx->stats.reset();
-  std::memset(rep, 0, sizeof(*rep));
-  if (a->host.nrows == 0) {
-    rep->termination = CFD_TERM_INITIAL_RESIDUAL;
-    return CFD_OK;
-  }
-  if (opt->precision == CFD_PRECISION_FP32_REFINE)
-    CFD_TRY(solve_refine(a, *opt, amg, b, x, *cfg, *rep));
-  else
-    CFD_TRY(solve_fp64(a, *opt, amg, b, x, *cfg, *rep));
-  return check_device_flag(a->ctx);
+  return guarded("cfd_solve", [&]() -> cfd_status {
+    if (!a || !opt || !b || !x || !cfg || !rep) {
+      set_error("null argument to cfd_solve");
+      return CFD_ERR_STATE;
+    }
+    // convergence_policy (krylov.rs:123-139) rejects non-finite or negative
+    // tolerances and a zero iteration budget at construction.
+    if (!(cfg->tolerance >= 0.0) || !(cfg->relative_tolerance >= 0.0) || !std::isfinite(cfg->tolerance) ||
+        !std::isfinite(cfg->relative_tolerance) || cfg->max_iterations <= 0) {
+      set_error("invalid iterative solver configuration: tolerance %g, relative %g, max_iterations %lld",
+                cfg->tolerance, cfg->relative_tolerance, (long long)cfg->max_iterations);
+      return CFD_ERR_CONFIG;
+    }
+    if (opt->solver < 0 || opt->solver > 2 || opt->precond < 0 || opt->precond > 2 || opt->precision < 0 ||
+        opt->precision > 1 || opt->memory < 0 || opt->memory > 1 || (opt->solver == CFD_SOLVER_GMRES && opt->restart < 1)) {
+      set_error("invalid solve options");
+      return CFD_ERR_CONFIG;
+    }
+    if (a->host.nrows != a->host.ncols) {
+      set_error("Krylov solve needs a square matrix (%lld x %lld)", (long long)a->host.nrows,
+                (long long)a->host.ncols);
+      return CFD_ERR_DIM;
+    }
+    std::lock_guard<std::mutex> g(a->ctx->mu);
+    CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+    CFD_TRY(check_precond(a, *opt, amg));
+    a->ctx->stats.reset();
+    std::memset(rep, 0, sizeof(*rep));
+    if (a->host.nrows == 0) {
+      rep->termination = CFD_TERM_INITIAL_RESIDUAL;
+      return CFD_OK;
+    }
+    if (opt->precision == CFD_PRECISION_FP32_REFINE)
+      CFD_TRY(solve_refine(a, *opt, amg, b, x, *cfg, *rep));
+    else
+      CFD_TRY(solve_fp64(a, *opt, amg, b, x, *cfg, *rep));
+    return check_device_flag(a->ctx);
+  });
 }
 
 cfd_status cfd_last_kernel_stats(cfd_context* ctx, cfd_kernel_stats* out) {

@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <exception>
 #include <mutex>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -14,6 +16,43 @@ namespace cfd {
 
 // Error message of the last failure on this thread (cfd_last_error()).
 void set_error(const char* fmt, ...);
+
+// Runs an entry point's body with C++ exceptions turned into status codes: a
+// host allocation that fails (std::bad_alloc from a std::vector) must not
+// unwind into a C, Rust or ctypes caller.
+template <typename F>
+cfd_status guarded(const char* what, F&& body) noexcept {
+  try {
+    return body();
+  } catch (const std::bad_alloc&) {
+    set_error("%s: host memory allocation failed", what);
+    return CFD_ERR_ALLOC;
+  } catch (const std::exception& e) {
+    set_error("%s: %s", what, e.what());
+    return CFD_ERR_STATE;
+  } catch (...) {
+    set_error("%s: unexpected exception", what);
+    return CFD_ERR_STATE;
+  }
+}
+
+// Runs `undo` when the scope is left by an exception, so that a half-built
+// handle is released before guarded() turns the exception into a status.
+// Returns by status code do not trigger it (those paths release for themselves).
+template <typename F>
+class OnUnwind {
+ public:
+  explicit OnUnwind(F f) : f_(f), depth_(std::uncaught_exceptions()) {}
+  ~OnUnwind() {
+    if (std::uncaught_exceptions() > depth_) f_();
+  }
+  OnUnwind(const OnUnwind&) = delete;
+  OnUnwind& operator=(const OnUnwind&) = delete;
+
+ private:
+  F f_;
+  int depth_;
+};
 
 #define CFD_TRY_CUDA(...)                                                                           \
   do {                                                                                              \

@@ -1016,6 +1016,12 @@ cfd_status check_precond(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg)
       set_error("AMG preconditioner: the hierarchy was built on the host only (cfd_amg_setup_host)");
       return CFD_ERR_STATE;
     }
+    // The V-cycle runs on the matrix's context (its stream, its device, its
+    // lock held): level buffers of another context may sit on another device.
+    if (amg->ctx != a->ctx) {
+      set_error("AMG preconditioner: the matrix and the hierarchy belong to different contexts");
+      return CFD_ERR_STATE;
+    }
     if (amg->dev.empty() || amg->dev[0].A.nrows != a->dev.nrows) {
       set_error("AMG hierarchy does not match the matrix (%lld rows)", (long long)a->dev.nrows);
       return CFD_ERR_DIM;

@@ -135,3 +135,43 @@ def test_batch_valid_layout_reaches_the_context_check():
     z = _i64(0)
     assert L.cfd_batch_create(None, 0, _ptr(z), _ptr(z), None, None, C.byref(out)) == 7
     assert b"null context" in L.cfd_last_error()
+
+
+HOST_OOM_SCRIPT = r"""
+import ctypes as C, resource, sys
+import numpy as np
+from cfdrs_b200 import _lib
+from cfdrs_b200 import problems as P
+L = _lib.load()
+A = P.poisson_3d_variable(40, 4.0, 1.0, seed=1)[0]
+rp, col = np.ascontiguousarray(A.row_ptr, np.int64), np.ascontiguousarray(A.col, np.int64)
+val = np.ascontiguousarray(A.val)
+cfg = _lib.AmgConfigC()
+L.cfd_amg_config_default(C.byref(cfg))
+vm = int([l for l in open("/proc/self/status") if l.startswith("VmSize")][0].split()[1]) * 1024
+resource.setrlimit(resource.RLIMIT_AS, (vm + (8 << 20), resource.RLIM_INFINITY))
+out = C.c_void_p()
+st = L.cfd_amg_setup_host(A.nrows, rp.ctypes.data_as(C.c_void_p), col.ctypes.data_as(C.c_void_p),
+                          val.ctypes.data_as(C.c_void_p), C.byref(cfg), C.byref(out))
+resource.setrlimit(resource.RLIMIT_AS, (resource.RLIM_INFINITY, resource.RLIM_INFINITY))
+print(st, L.cfd_last_error().decode(), out.value is None)
+"""
+
+
+@pytest.mark.skipif(not os.path.exists("/proc/self/status"), reason="needs /proc for the address-space size")
+@pytest.mark.skipif("libasan" in os.environ.get("LD_PRELOAD", ""),
+                    reason="the sanitizer's allocator aborts on exhaustion instead of throwing std::bad_alloc")
+def test_host_allocation_failure_is_a_status():
+    """A host allocation that fails inside an entry point comes back as
+    CFD_ERR_ALLOC with no handle, and the caller's process carries on (an
+    exception unwinding out of the C ABI would end it with std::terminate).
+    The child caps its address space at 8 MiB above its size before the host
+    AMG setup of a 40^3 operator; one OpenMP thread, so that no thread is
+    created under the cap."""
+    import sys
+    env = dict(os.environ, OMP_NUM_THREADS="1", PYTHONPATH=ROOT)
+    out = subprocess.run([sys.executable, "-c", HOST_OOM_SCRIPT], cwd=ROOT, env=env, capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    st, rest = out.stdout.strip().split(" ", 1)
+    assert int(st) == 6 and "host memory allocation failed" in rest and rest.endswith("True")
