@@ -25,6 +25,8 @@ Reference semantics restated here:
 """
 from __future__ import annotations
 
+from typing import NamedTuple
+
 import numpy as np
 
 from .sparse import CsrMatrix
@@ -241,12 +243,37 @@ def hagen_poiseuille_conductance(d, length, mu=1.0e-3):
     return np.pi * np.asarray(d) ** 4 / (128.0 * mu * np.asarray(length))
 
 
+class Network(NamedTuple):
+    """A pipe network as edges: node pair, conductance, and the Dirichlet
+    nodes as a 0/1 mask with their pressures (one entry per node)."""
+    n_nodes: int
+    edges_i: np.ndarray
+    edges_j: np.ndarray
+    conductance: np.ndarray
+    fixed: np.ndarray
+    fixed_value: np.ndarray
+
+    def dirichlet(self) -> dict:
+        return {int(k): float(self.fixed_value[k]) for k in np.flatnonzero(self.fixed)}
+
+    def assemble(self, neumann: dict | None = None):
+        return kirchhoff_assemble(self.n_nodes, self.edges_i, self.edges_j, self.conductance, self.dirichlet(),
+                                  neumann)
+
+
 def random_network(n_nodes: int, rng: np.random.Generator, loop_fraction: float = 0.1,
                    p_in: float = 1000.0, p_out: float = 0.0):
+    """Seeded pipe network (:func:`random_network_edges`) assembled by
+    :func:`kirchhoff_assemble`. Returns ``(A, b)``."""
+    return random_network_edges(n_nodes, rng, loop_fraction, p_in, p_out).assemble()
+
+
+def random_network_edges(n_nodes: int, rng: np.random.Generator, loop_fraction: float = 0.1,
+                         p_in: float = 1000.0, p_out: float = 0.0) -> Network:
     """Seeded pipe network: a random spanning tree (node i attaches to a uniform
     j < i) plus ``floor(loop_fraction * n)`` extra distinct edges; diameters
     U[50, 500] um, lengths U[1, 20] mm, mu = 1e-3 Pa s; node 0 fixed at ``p_in``,
-    node n-1 at ``p_out``. Returns ``(A, b)`` from :func:`kirchhoff_assemble`."""
+    node n-1 at ``p_out``."""
     n = int(n_nodes)
     child = np.arange(1, n, dtype=np.int64)
     parent = np.minimum((rng.random(n - 1) * child).astype(np.int64), child - 1)
@@ -269,12 +296,22 @@ def random_network(n_nodes: int, rng: np.random.Generator, loop_fraction: float 
     d = rng.uniform(50e-6, 500e-6, size=m)
     length = rng.uniform(1e-3, 20e-3, size=m)
     g = hagen_poiseuille_conductance(d, length)
-    return kirchhoff_assemble(n, ei, ej, g, {0: p_in, n - 1: p_out})
+    fixed = np.zeros(n, dtype=np.int8)
+    fixed_value = np.zeros(n)
+    fixed[[0, n - 1]] = 1
+    fixed_value[0], fixed_value[n - 1] = p_in, p_out
+    return Network(n, np.asarray(ei, dtype=np.int32), np.asarray(ej, dtype=np.int32), g, fixed, fixed_value)
 
 
 def network_batch(num: int, seed: int = 0, n_min: int = 20, n_max: int = 2000, loop_fraction: float = 0.1):
     """``num`` seeded networks with node counts uniform in [n_min, n_max]
     (:func:`random_network` each). Returns a list of ``(A, b)``."""
+    return [net.assemble() for net in network_batch_edges(num, seed, n_min, n_max, loop_fraction)]
+
+
+def network_batch_edges(num: int, seed: int = 0, n_min: int = 20, n_max: int = 2000,
+                        loop_fraction: float = 0.1) -> list[Network]:
+    """The networks of :func:`network_batch` (same seed, same networks) as edges."""
     rng = np.random.default_rng(seed)
     sizes = rng.integers(n_min, n_max + 1, size=num)
-    return [random_network(int(n), rng, loop_fraction) for n in sizes]
+    return [random_network_edges(int(n), rng, loop_fraction) for n in sizes]

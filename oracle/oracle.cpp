@@ -1234,4 +1234,68 @@ int or_bicgstab(const or_csr* a, int precond, const or_amg* amg, const double* b
   return 0;
 }
 
+// MatrixAssembler::assemble_into (crates/cfd-1d/src/solver/core/matrix_assembly.rs:163-250):
+// per edge in order, the self-loop and conductance checks (:184-203), then the
+// COO pushes and RHS eliminations of the four cases (:208-231); Neumann
+// sources added (:234-238); identity rows and RHS = p for fixed nodes
+// (:240-246). The COO becomes CSR by a stable sort on (row, column) with
+// duplicates summed in push order.
+int or_network_assemble(int64_t n, int64_t m, const int64_t* ei, const int64_t* ej, const double* g,
+                        const int8_t* fixed, const double* fixed_value, const double* neumann, or_csr** out,
+                        double* rhs, int64_t* bad_edge) {
+  struct Entry {
+    int64_t r, c;
+    double v;
+  };
+  *out = nullptr;
+  *bad_edge = -1;
+  std::vector<Entry> coo;
+  std::fill(rhs, rhs + n, 0.0);
+  for (int64_t e = 0; e < m; ++e) {
+    const int64_t i = ei[e], j = ej[e];
+    const double c = g[e];
+    if (i == j || !std::isfinite(c) || c <= 0.0) {
+      *bad_edge = e;
+      return i == j ? 1 : (!std::isfinite(c) ? 2 : 3);
+    }
+    const bool fi = fixed[i] != 0, fj = fixed[j] != 0;
+    if (!fi && !fj) {
+      coo.push_back({i, i, c});
+      coo.push_back({j, j, c});
+      coo.push_back({i, j, -c});
+      coo.push_back({j, i, -c});
+    } else if (fi && !fj) {
+      coo.push_back({j, j, c});
+      rhs[j] += c * fixed_value[i];
+    } else if (!fi && fj) {
+      coo.push_back({i, i, c});
+      rhs[i] += c * fixed_value[j];
+    }
+  }
+  if (neumann)
+    for (int64_t k = 0; k < n; ++k) rhs[k] += neumann[k];
+  for (int64_t k = 0; k < n; ++k)
+    if (fixed[k]) {
+      coo.push_back({k, k, 1.0});
+      rhs[k] = fixed_value[k];
+    }
+  std::stable_sort(coo.begin(), coo.end(),
+                   [](const Entry& a, const Entry& b) { return a.r != b.r ? a.r < b.r : a.c < b.c; });
+  or_csr* a = new or_csr;
+  a->nrows = a->ncols = n;
+  a->rp.assign(n + 1, 0);
+  for (size_t q = 0; q < coo.size();) {
+    size_t t = q + 1;
+    double v = coo[q].v;
+    while (t < coo.size() && coo[t].r == coo[q].r && coo[t].c == coo[q].c) v += coo[t++].v;
+    a->ci.push_back(coo[q].c);
+    a->v.push_back(v);
+    a->rp[coo[q].r + 1]++;
+    q = t;
+  }
+  for (int64_t r = 0; r < n; ++r) a->rp[r + 1] += a->rp[r];
+  *out = a;
+  return 0;
+}
+
 }  // extern "C"

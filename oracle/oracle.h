@@ -131,6 +131,16 @@ int or_gmres_width(int64_t requested);
 int or_gmres(const or_csr* a, int precond, const or_amg* amg, int64_t restart, const double* b, double* x,
              const or_solver_config* cfg, or_report* rep, double* history);
 
+/* MatrixAssembler::assemble_into for one network (crates/cfd-1d/src/solver/core/
+ * matrix_assembly.rs:163-250). Nodes 0..n-1, edges (ei[e], ej[e]) with
+ * conductance g[e]; fixed[k] != 0 marks a Dirichlet node of pressure
+ * fixed_value[k]; neumann may be NULL. Returns 0 and a new CSR in *out with the
+ * right-hand side in rhs[n]; 1 self-loop, 2 non-finite conductance, 3
+ * non-positive conductance, with the edge in *bad_edge. */
+int or_network_assemble(int64_t n, int64_t m, const int64_t* ei, const int64_t* ej, const double* g,
+                        const int8_t* fixed, const double* fixed_value, const double* neumann, or_csr** out,
+                        double* rhs, int64_t* bad_edge);
+
 #ifdef __cplusplus
 }
 #endif

@@ -105,6 +105,8 @@ def lib():
         L.or_gmres.argtypes = [P, C.c_int, P, C.c_int64, P, P, P, P, P]
         L.or_gmres_width.restype = C.c_int
         L.or_gmres_width.argtypes = [C.c_int64]
+        L.or_network_assemble.restype = C.c_int
+        L.or_network_assemble.argtypes = [I64, I64, P, P, P, P, P, P, P, P, P]
         _lib = L
     return _lib
 
@@ -343,3 +345,28 @@ def set_threads(n: int):
 
 def get_threads() -> int:
     return lib().or_get_threads()
+
+
+NETWORK_ERRORS = {1: "self-loop edge", 2: "non-finite conductance", 3: "non-positive conductance"}
+
+
+def network_assemble(n_nodes, edges_i, edges_j, conductance, fixed, fixed_value, neumann=None):
+    """The grounded conductance Laplacian and right-hand side of one network
+    (``or_network_assemble``). ``fixed`` is a per-node 0/1 mask of Dirichlet
+    nodes and ``fixed_value`` their pressures. Returns ``(Csr, rhs)``; raises
+    ``ValueError`` naming the first offending edge as the reference does."""
+    n = int(n_nodes)
+    ei = np.ascontiguousarray(edges_i, dtype=np.int64)
+    ej = np.ascontiguousarray(edges_j, dtype=np.int64)
+    g = np.ascontiguousarray(conductance, dtype=np.float64)
+    fx = np.ascontiguousarray(fixed, dtype=np.int8)
+    fv = np.ascontiguousarray(fixed_value, dtype=np.float64)
+    q = None if neumann is None else np.ascontiguousarray(neumann, dtype=np.float64)
+    rhs = np.zeros(n)
+    out = C.c_void_p()
+    bad = C.c_int64()
+    rc = lib().or_network_assemble(n, ei.shape[0], _ptr(ei), _ptr(ej), _ptr(g), _ptr(fx), _ptr(fv),
+                                   None if q is None else _ptr(q), C.byref(out), _ptr(rhs), C.byref(bad))
+    if rc != 0:
+        raise ValueError(f"{NETWORK_ERRORS[rc]} at edge {bad.value}")
+    return Csr(out.value), rhs

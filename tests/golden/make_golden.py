@@ -153,6 +153,17 @@ GOLDEN = {
         "rhs_b_with_neumann_5": 105.0,
         "tol": 1e-12,
     },
+    # The reference test checks only that the free block is symmetric; the
+    # entries below follow from assemble_into's rules (:208-246) by hand:
+    # B = 1 (AB, A fixed) + 3 (BC); C = 2 (AC, A fixed) + 3 (BC) + 4 (CD, D fixed);
+    # B-C = -3; RHS_B = 1 * 100, RHS_C = 2 * 100 + 4 * 0.
+    "kirchhoff_active_block": {
+        "source": "crates/cfd-1d/src/solver/core/matrix_assembly.rs:404-450 (entries derived from :208-246)",
+        "edges": [[0, 1, 1.0], [0, 2, 2.0], [1, 2, 3.0], [2, 3, 4.0]],
+        "dirichlet": {"0": 100.0, "3": 0.0},
+        "dense": [[1.0, 0.0, 0.0, 0.0], [0.0, 4.0, -3.0, 0.0], [0.0, -3.0, 9.0, 0.0], [0.0, 0.0, 0.0, 1.0]],
+        "rhs": [100.0, 100.0, 200.0, 0.0],
+    },
 }
 
 

@@ -171,6 +171,76 @@ def test_kirchhoff_abc_golden(golden):
     assert abs(b5[1] - g["rhs_b_with_neumann_5"]) < g["tol"]
 
 
+def _oracle_network(oracle, edges, dirichlet, n, neumann=None):
+    e = np.array(edges)
+    fixed, value = np.zeros(n, np.int8), np.zeros(n)
+    for k, v in dirichlet.items():
+        fixed[int(k)], value[int(k)] = 1, v
+    q = None
+    if neumann:
+        q = np.zeros(n)
+        for k, v in neumann.items():
+            q[k] = v
+    A, b = oracle.network_assemble(n, e[:, 0], e[:, 1], e[:, 2], fixed, value, q)
+    return A.to_scipy().toarray(), b
+
+
+def test_oracle_network_assembly_golden(oracle, golden):
+    """or_network_assemble on the reference's assembly tests
+    (matrix_assembly.rs:270-450): identity rows for fixed nodes, Dirichlet
+    columns eliminated into the RHS, the Neumann source, the free block."""
+    g = golden["kirchhoff_abc"]
+    D, b = _oracle_network(oracle, g["edges"], g["dirichlet"], 3)
+    assert D[1, 1] == g["diag_b"] and b[1] == g["rhs_b"]
+    assert D[0, 0] == 1.0 and D[2, 2] == 1.0 and b[0] == 100.0 and b[2] == 0.0
+    assert D[1, 0] == 0.0 and D[1, 2] == 0.0 and D[0, 1] == 0.0 and D[2, 1] == 0.0
+    _, b5 = _oracle_network(oracle, g["edges"], g["dirichlet"], 3, {1: 5.0})
+    assert b5[1] == g["rhs_b_with_neumann_5"] and b5[0] == 100.0  # the fixed row keeps p
+    g = golden["kirchhoff_active_block"]
+    D, b = _oracle_network(oracle, g["edges"], g["dirichlet"], 4)
+    assert np.array_equal(D, np.array(g["dense"])) and np.array_equal(b, np.array(g["rhs"]))
+
+
+@pytest.mark.parametrize("bad,kind", [((1, 1, 1.0), "self-loop"), ((0, 2, np.nan), "non-finite"),
+                                      ((0, 2, np.inf), "non-finite"), ((0, 2, 0.0), "non-positive"),
+                                      ((0, 2, -1.0), "non-positive")])
+def test_oracle_network_assembly_rejects(oracle, bad, kind):
+    """matrix_assembly.rs:184-203: the first offending edge is reported."""
+    with pytest.raises(ValueError, match=f"{kind}.*at edge 1"):
+        _oracle_network(oracle, [(0, 1, 1.0), bad, (1, 2, 2.0)], {0: 1.0}, 3)
+
+
+def test_oracle_network_assembly_parallel_edges_and_sources(oracle):
+    """Parallel edges merge into one entry per (row, column), summed in edge
+    order; a free node with several fixed neighbours sums g p in edge order;
+    an edge between two fixed nodes contributes nothing; every node may carry
+    a Neumann source, fixed rows ignore theirs."""
+    edges = [(0, 1, 0.1), (1, 2, 0.2), (2, 1, 0.3), (1, 3, 0.7), (3, 4, 1.1), (4, 0, 1.3), (2, 4, 1.7),
+             (1, 2, 0.9)]
+    D, b = _oracle_network(oracle, edges, {0: 3.0, 4: -2.0}, 5, {1: 0.5, 2: -0.25, 4: 9.0})
+    assert D[1, 2] == (-0.2 + -0.3) + -0.9 and D[2, 1] == D[1, 2]
+    assert D[1, 1] == (((0.1 + 0.2) + 0.3) + 0.7) + 0.9
+    assert D[2, 2] == ((0.2 + 0.3) + 1.7) + 0.9
+    assert D[3, 3] == 0.7 + 1.1 and D[3, 4] == 0.0 and D[0, 0] == 1.0 and D[4, 4] == 1.0
+    assert b[1] == 0.1 * 3.0 + 0.5 and b[2] == 1.7 * -2.0 + -0.25 and b[3] == 1.1 * -2.0
+    assert b[0] == 3.0 and b[4] == -2.0
+
+
+def test_oracle_network_assembly_matches_problem_assembly(oracle):
+    """The oracle and problems.kirchhoff_assemble (scipy's COO merge) give the
+    same pattern and, up to the order of the diagonal sums, the same values on
+    the seeded C4-style networks."""
+    from cfdrs_b200 import problems as P
+    for net in P.network_batch_edges(12, seed=5, n_min=20, n_max=800):
+        A, b = net.assemble()
+        O, ob = oracle.network_assemble(net.n_nodes, net.edges_i, net.edges_j, net.conductance, net.fixed,
+                                        net.fixed_value)
+        rp, ci, v, _ = O.arrays()
+        assert np.array_equal(rp, A.row_ptr) and np.array_equal(ci, A.col)
+        np.testing.assert_allclose(v, A.val, rtol=4e-16 * 16, atol=0)
+        assert np.array_equal(ob, b)
+
+
 def test_equilibrated_pcg_networks(oracle):
     """Jacobi-PCG with the 1-D solver's equilibrated residual test reaches the
     direct solution on seeded networks (linear_system.rs:157-204)."""
