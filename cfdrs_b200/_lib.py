@@ -29,6 +29,7 @@ EXPORTS = [
     "cfd_solve_options_default", "cfd_solve", "cfd_last_kernel_stats",
     "cfd_pattern_outer", "cfd_csr_set_values_device",
     "cfd_batch_create", "cfd_batch_update_values", "cfd_batch_solve", "cfd_batch_autotune", "cfd_batch_config",
+    "cfd_batch_create_networks", "cfd_batch_assemble", "cfd_batch_values", "cfd_network_assemble_host",
     "cfd_batch_destroy",
     "cfd_residual_norm_noalloc",
 ]
@@ -136,6 +137,10 @@ def load():
         "cfd_pattern_outer": (C.c_int, [P, P, P, D, P]),
         "cfd_csr_set_values_device": (C.c_int, [P, P]),
         "cfd_batch_create": (C.c_int, [P, I32, P, P, P, P, PP]),
+        "cfd_batch_create_networks": (C.c_int, [P, I32, P, P, P, P, P, P, PP]),
+        "cfd_batch_assemble": (C.c_int, [P, P, P, I32]),
+        "cfd_batch_values": (C.c_int, [P, P, P]),
+        "cfd_network_assemble_host": (C.c_int, [I32, P, P, P, P, P, P, P, P, P, P, P, P, P]),
         "cfd_batch_update_values": (C.c_int, [P, P]),
         "cfd_batch_solve": (C.c_int, [P, P, P, P, P, P, P, P, P]),
         "cfd_batch_autotune": (C.c_int, [P, I32, I32]),

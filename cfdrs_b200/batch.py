@@ -34,7 +34,75 @@ class BatchReport:
 
 
 def _p(a):
-    return a.ctypes.data_as(C.c_void_p)
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass
+class PackedNetworks:
+    """Networks concatenated as cfd_batch_create_networks takes them: node and
+    edge offsets per network, edge endpoints local to their network, and the
+    Dirichlet mask and pressures per global node."""
+    node_off: np.ndarray
+    edge_off: np.ndarray
+    edge_i: np.ndarray
+    edge_j: np.ndarray
+    fixed: np.ndarray
+    fixed_value: np.ndarray
+    conductance: np.ndarray
+
+    @property
+    def num_systems(self) -> int:
+        return self.node_off.shape[0] - 1
+
+    @property
+    def rows(self) -> int:
+        return int(self.node_off[-1])
+
+    @property
+    def edges(self) -> int:
+        return int(self.edge_off[-1])
+
+
+def pack_networks(networks) -> PackedNetworks:
+    """From objects with ``n_nodes, edges_i, edges_j, conductance, fixed,
+    fixed_value`` (``problems.Network``)."""
+    nodes = np.array([int(n.n_nodes) for n in networks], dtype=np.int64)
+    edges = np.array([len(n.edges_i) for n in networks], dtype=np.int64)
+    node_off = np.concatenate([[0], np.cumsum(nodes)]).astype(np.int64)
+    edge_off = np.concatenate([[0], np.cumsum(edges)]).astype(np.int64)
+
+    def cat(name, dtype):
+        parts = [np.asarray(getattr(n, name), dtype=dtype) for n in networks]
+        return np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros(0, dtype))
+    return PackedNetworks(node_off, edge_off, cat("edges_i", np.int32), cat("edges_j", np.int32),
+                          cat("fixed", np.int8), cat("fixed_value", np.float64), cat("conductance", np.float64))
+
+
+def network_assemble_host(packed: PackedNetworks, conductance=None, neumann=None):
+    """The device assembly's pattern and values computed on the host by the
+    same code (``cfd_network_assemble_host``). Returns ``(row_ptr, col, val,
+    rhs)``; ``val`` and ``rhs`` are None without conductances."""
+    L = _lib.load()
+    nnz = C.c_int64()
+    args = (packed.num_systems, _p(packed.node_off), _p(packed.edge_off), _p(packed.edge_i), _p(packed.edge_j),
+            _p(packed.fixed), _p(packed.fixed_value))
+    _lib.check(L.cfd_network_assemble_host(*args, None, None, C.byref(nnz), None, None, None, None))
+    rp = np.zeros(packed.rows + 1, np.int64)
+    col = np.zeros(nnz.value, np.int32)
+    g = None if conductance is None else np.ascontiguousarray(conductance, dtype=np.float64)
+    q = None if neumann is None else np.ascontiguousarray(neumann, dtype=np.float64)
+    val = None if g is None else np.zeros(nnz.value)
+    rhs = None if g is None else np.zeros(packed.rows)
+    _lib.check(L.cfd_network_assemble_host(*args, _p(g), _p(q), C.byref(nnz), _p(rp), _p(col), _p(val), _p(rhs)))
+    return rp, col, val, rhs
+
+
+def _torch_cuda(a) -> bool:
+    try:
+        import torch
+    except ImportError:
+        return False
+    return isinstance(a, torch.Tensor) and a.is_cuda
 
 
 class NetworkBatch:
@@ -63,6 +131,63 @@ class NetworkBatch:
                                                 _p(self.col), _p(self.val), C.byref(h)))
         self.h = h
 
+    @classmethod
+    def from_networks(cls, networks, ctx: Context | None = None) -> "NetworkBatch":
+        """A batch of pipe networks given as edges (``problems.Network``); the
+        matrices are assembled on the device by :meth:`assemble`
+        (``cfd_batch_create_networks``). The networks' own conductances are
+        kept in ``packed.conductance`` but not assembled."""
+        self = cls.__new__(cls)
+        self.ctx = ctx or context()
+        self.packed = pk = pack_networks(networks)
+        h = C.c_void_p()
+        _lib.check(_lib.load().cfd_batch_create_networks(self.ctx.h, pk.num_systems, _p(pk.node_off),
+                                                         _p(pk.edge_off), _p(pk.edge_i), _p(pk.edge_j),
+                                                         _p(pk.fixed), _p(pk.fixed_value), C.byref(h)))
+        self.h = h
+        self.sys_row = pk.node_off
+        self.row_ptr, self.col, _, _ = network_assemble_host(pk)
+        self.val = np.zeros(self.col.shape[0])
+        self.num_systems = pk.num_systems
+        self.rows = pk.rows
+        return self
+
+    def assemble(self, conductance, neumann=None) -> None:
+        """Values and right-hand sides from per-edge conductances (and
+        optional per-node Neumann sources), both numpy arrays (host) or both
+        float64 CUDA tensors (device, read on torch's current stream)."""
+        pk = getattr(self, "packed", None)
+        if pk is None:
+            raise SolveError("assemble needs a batch made by NetworkBatch.from_networks")
+        L = _lib.load()
+        if _torch_cuda(conductance):
+            import torch
+            if conductance.dtype != torch.float64 or conductance.numel() != pk.edges or not conductance.is_contiguous():
+                raise SolveError("conductance must be a contiguous float64 tensor with one entry per edge")
+            if neumann is not None and (not _torch_cuda(neumann) or neumann.dtype != torch.float64
+                                        or neumann.numel() != pk.rows or not neumann.is_contiguous()):
+                raise SolveError("neumann must be a contiguous float64 CUDA tensor with one entry per node")
+            self.ctx.set_stream(torch.cuda.current_stream(conductance.device).cuda_stream)
+            try:
+                st = L.cfd_batch_assemble(self.h, C.c_void_p(conductance.data_ptr()),
+                                          None if neumann is None else C.c_void_p(neumann.data_ptr()), 1)
+            finally:
+                self.ctx.set_stream(None)
+        else:
+            g = np.ascontiguousarray(conductance, dtype=np.float64)
+            q = None if neumann is None else np.ascontiguousarray(neumann, dtype=np.float64)
+            if g.shape[0] != pk.edges or (q is not None and q.shape[0] != pk.rows):
+                raise SolveError(f"need {pk.edges} conductances and {pk.rows} Neumann sources")
+            st = L.cfd_batch_assemble(self.h, _p(g), _p(q), 0)
+        _lib.check(st)
+
+    def values(self) -> tuple[np.ndarray, np.ndarray]:
+        """The batch's current values and right-hand sides (host copies)."""
+        val = np.zeros(self.col.shape[0])
+        rhs = np.zeros(self.rows)
+        _lib.check(_lib.load().cfd_batch_values(self.h, _p(val), _p(rhs)))
+        return val, rhs
+
     def split(self, v: np.ndarray) -> list[np.ndarray]:
         return [v[self.sys_row[s]:self.sys_row[s + 1]] for s in range(self.num_systems)]
 
@@ -73,22 +198,43 @@ class NetworkBatch:
         _lib.check(_lib.load().cfd_batch_update_values(self.h, _p(v)))
         self.val = v
 
-    def solve(self, b, x=None, config: IterativeSolverConfig | None = None,
+    def solve(self, b=None, x=None, config: IterativeSolverConfig | None = None,
               precision: Precision = Precision.FP64, inner_tolerance: float = 1e-4,
               max_outer: int = 20) -> tuple[np.ndarray, BatchReport]:
-        """Solve every system; b and x are concatenated over the systems (host)."""
+        """Solve every system; b and x are concatenated over the systems.
+        Host arrays, or float64 CUDA tensors (x then holds the initial guess
+        and is overwritten with the solution, on torch's current stream).
+        b = None solves with the right-hand sides of the last
+        :meth:`assemble`."""
         cfg = (config or IterativeSolverConfig(0.0, 1e-10, 20000)).to_c()
-        bb = np.ascontiguousarray(b, dtype=np.float64)
-        if bb.shape[0] != self.rows:
-            raise SolveError(f"rhs has {bb.shape[0]} entries, the batch {self.rows} rows")
-        xx = np.zeros(self.rows) if x is None else np.array(x, dtype=np.float64, copy=True)
-        opt = _lib.SolveOptionsC(0, 1, int(precision), 0, inner_tolerance, max_outer, 0)
+        device = _torch_cuda(x)
+        if device:
+            import torch
+            if x.dtype != torch.float64 or x.numel() != self.rows or not x.is_contiguous():
+                raise SolveError("x must be a contiguous float64 CUDA tensor with one entry per row")
+            if b is not None and (not _torch_cuda(b) or b.dtype != torch.float64 or b.numel() != self.rows
+                                  or not b.is_contiguous()):
+                raise SolveError("with a CUDA x, b must be None or a matching contiguous float64 CUDA tensor")
+            xx, bp, xp = x, (None if b is None else C.c_void_p(b.data_ptr())), C.c_void_p(x.data_ptr())
+        else:
+            bb = None if b is None else np.ascontiguousarray(b, dtype=np.float64)
+            if bb is not None and bb.shape[0] != self.rows:
+                raise SolveError(f"rhs has {bb.shape[0]} entries, the batch {self.rows} rows")
+            xx = np.zeros(self.rows) if x is None else np.array(x, dtype=np.float64, copy=True)
+            bp, xp = _p(bb), _p(xx)
+        opt = _lib.SolveOptionsC(0, 1, int(precision), 1 if device else 0, inner_tolerance, max_outer, 0)
         term = np.zeros(self.num_systems, np.int32)
         its = np.zeros(self.num_systems, np.int32)
         res = np.zeros(self.num_systems, np.float64)
         rep = _lib.BatchReportC()
-        st = _lib.load().cfd_batch_solve(self.h, C.byref(opt), _p(bb), _p(xx), C.byref(cfg), _p(term), _p(its),
-                                         _p(res), C.byref(rep))
+        if device:
+            self.ctx.set_stream(torch.cuda.current_stream(x.device).cuda_stream)
+        try:
+            st = _lib.load().cfd_batch_solve(self.h, C.byref(opt), bp, xp, C.byref(cfg), _p(term), _p(its),
+                                             _p(res), C.byref(rep))
+        finally:
+            if device:
+                self.ctx.set_stream(None)
         if st != _lib.CFD_OK:
             raise SolveError(f"batched solve failed: {_lib.STATUS_NAMES.get(st, st)}: "
                              f"{_lib.load().cfd_last_error().decode()}")
@@ -116,4 +262,4 @@ class NetworkBatch:
             self.h = None
 
 
-__all__ = ["NetworkBatch", "BatchReport", "Termination"]
+__all__ = ["NetworkBatch", "BatchReport", "Termination", "PackedNetworks", "pack_networks", "network_assemble_host"]

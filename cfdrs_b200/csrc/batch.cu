@@ -26,22 +26,14 @@
 #include <type_traits>
 #include <vector>
 
+#include "batch_internal.h"
 #include "internal.h"
 #include "kernels.cuh"
 
 namespace cfd {
 namespace {
 
-constexpr int kBatchMaxRows = 2048;   // rows per system held in shared memory
-constexpr int kBatchMaxNnz = 8192;    // nonzeros per system held in shared memory
-constexpr int kBuckets = 4;
-constexpr int kBucketRows[kBuckets] = {64, 256, 1024, kBatchMaxRows};
 constexpr int kCandidates[] = {32, 64, 128, 256, 512};
-
-struct BatchParams {
-  double tol_abs, tol_rel, inner_tol;
-  int32_t max_iter, max_outer;
-};
 
 struct BatchSys {
   const int* __restrict__ sys_row;   // first global row of each system (nsys + 1)
@@ -307,32 +299,6 @@ __global__ void k_batch_pcg(BatchSys S, BatchOut O, const int* __restrict__ orde
 
 using namespace cfd;
 
-struct cfd_batch {
-  cfd_context* ctx = nullptr;
-  int nsys = 0;
-  int64_t rows = 0, nnz = 0;
-  std::vector<int> h_sys_row;
-  int* sys_row = nullptr;
-  int* rp = nullptr;
-  int* col = nullptr;
-  double* v64 = nullptr;
-  float* v32 = nullptr;
-  double* x = nullptr;
-  double* b = nullptr;
-  int* term = nullptr;
-  int* iters = nullptr;
-  double* resid = nullptr;
-  int* order = nullptr;  // systems of each bucket, largest first, bucket after bucket
-  int bucket_begin[kBuckets + 1] = {};
-  int bucket_nmax[kBuckets] = {}, bucket_zmax[kBuckets] = {};
-  int threads[2][kBuckets] = {{32, 64, 128, 256}, {32, 64, 128, 256}};  // [precision][bucket]
-  bool tuned[2] = {false, false};
-  unsigned* queues = nullptr;  // one ticket per bucket
-  BatchParams* params = nullptr;
-  BatchParams* h_params = nullptr;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-};
-
 namespace {
 
 template <typename T>
@@ -459,15 +425,15 @@ cfd_status set_params(cfd_batch* bt, const cfd_solver_config& cfg, const cfd_sol
 
 }  // namespace
 
-extern "C" {
+namespace cfd {
 
 // The caller's layout, checked in an order that never indexes past what the
 // earlier checks have bounded: the offsets (num_systems + 1 of them, from 0,
 // non-decreasing, ending at the total row count), then per system its rows
 // (row_ptr non-decreasing and within [0, nnz]) before its local columns.
 // Touches no device state.
-static cfd_status validate_batch(int32_t num_systems, const int64_t* sys_row_offsets, const int64_t* row_ptr,
-                                 const int32_t* col, const double* val) {
+cfd_status batch_validate(int32_t num_systems, const int64_t* sys_row_offsets, const int64_t* row_ptr,
+                          const int32_t* col, const double* val) {
   if (num_systems < 0 || !sys_row_offsets || !row_ptr) {
     set_error("cfd_batch_create: invalid arguments");
     return CFD_ERR_STATE;
@@ -512,6 +478,93 @@ static cfd_status validate_batch(int32_t num_systems, const int64_t* sys_row_off
   return CFD_OK;
 }
 
+cfd_status batch_build(cfd_context* ctx, int32_t num_systems, const int64_t* sys_row_offsets,
+                       const int64_t* row_ptr, const int32_t* col, const double* val, cfd_batch** out) {
+  const int64_t rows = sys_row_offsets[num_systems];
+  const int64_t nnz = row_ptr[rows];
+  std::lock_guard<std::mutex> g(ctx->mu);
+  CFD_TRY_CUDA(cudaSetDevice(ctx->device));
+  cfd_batch* bt = new cfd_batch;
+  OnUnwind release([&] { cfd_batch_destroy(bt); });
+  bt->ctx = ctx;
+  bt->nsys = num_systems;
+  bt->rows = rows;
+  bt->nnz = nnz;
+  bt->h_sys_row.resize(num_systems + 1);
+  for (int s = 0; s <= num_systems; ++s) bt->h_sys_row[s] = (int)sys_row_offsets[s];
+  std::vector<int> rp32(rows + 1);
+  for (int64_t i = 0; i <= rows; ++i) rp32[i] = (int)row_ptr[i];
+  // Buckets by row count (bucket 0 also takes empty systems), largest system
+  // first inside each bucket.
+  std::vector<int> ord(num_systems);
+  std::iota(ord.begin(), ord.end(), 0);
+  auto nrows = [&](int s) { return bt->h_sys_row[s + 1] - bt->h_sys_row[s]; };
+  auto bucket_of = [&](int s) {
+    int k = 0;
+    while (k + 1 < kBuckets && nrows(s) > kBucketRows[k]) ++k;
+    return k;
+  };
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+    const int ka = bucket_of(a), kb = bucket_of(b);
+    return ka != kb ? ka < kb : nrows(a) > nrows(b);
+  });
+  std::vector<int> sorted = ord;
+  for (int k = 0; k <= kBuckets; ++k) bt->bucket_begin[k] = num_systems;
+  for (int q = num_systems - 1; q >= 0; --q) bt->bucket_begin[bucket_of(sorted[q])] = q;
+  for (int k = kBuckets - 1; k >= 0; --k)
+    if (bt->bucket_begin[k] > bt->bucket_begin[k + 1]) bt->bucket_begin[k] = bt->bucket_begin[k + 1];
+  for (int k = 0; k < kBuckets; ++k) {
+    int nmax = 1, zmax = 1;
+    for (int q = bt->bucket_begin[k]; q < bt->bucket_begin[k + 1]; ++q) {
+      const int sy = sorted[q];
+      nmax = std::max(nmax, nrows(sy));
+      zmax = std::max(zmax, (int)(row_ptr[bt->h_sys_row[sy + 1]] - row_ptr[bt->h_sys_row[sy]]));
+    }
+    bt->bucket_nmax[k] = nmax;
+    bt->bucket_zmax[k] = zmax;
+  }
+  cudaStream_t s = ctx->stream;
+  cfd_status st = CFD_OK;
+  auto fail = [&](cfd_status e) {
+    cfd_batch_destroy(bt);
+    return e;
+  };
+  if ((st = dalloc(&bt->sys_row, num_systems + 1)) != CFD_OK) return fail(st);
+  if ((st = dalloc(&bt->rp, rows + 1)) != CFD_OK) return fail(st);
+  if ((st = dalloc(&bt->col, nnz)) != CFD_OK) return fail(st);
+  if ((st = dalloc(&bt->v64, nnz)) != CFD_OK) return fail(st);
+  if ((st = dalloc(&bt->v32, nnz)) != CFD_OK) return fail(st);
+  if ((st = dalloc(&bt->x, rows)) != CFD_OK) return fail(st);
+  if ((st = dalloc(&bt->b, rows)) != CFD_OK) return fail(st);
+  if ((st = dalloc(&bt->term, num_systems)) != CFD_OK) return fail(st);
+  if ((st = dalloc(&bt->iters, num_systems)) != CFD_OK) return fail(st);
+  if ((st = dalloc(&bt->resid, num_systems)) != CFD_OK) return fail(st);
+  if ((st = dalloc(&bt->order, num_systems)) != CFD_OK) return fail(st);
+  if ((st = dalloc(&bt->queues, kBuckets)) != CFD_OK) return fail(st);
+  if ((st = dalloc(&bt->params, 1)) != CFD_OK) return fail(st);
+  if (cudaMallocHost((void**)&bt->h_params, sizeof(BatchParams)) != cudaSuccess) return fail(CFD_ERR_ALLOC);
+  std::vector<float> v32(val, val + nnz);
+  if (cudaMemcpyAsync(bt->sys_row, bt->h_sys_row.data(), (num_systems + 1) * sizeof(int), cudaMemcpyHostToDevice,
+                      s) != cudaSuccess ||
+      cudaMemcpyAsync(bt->rp, rp32.data(), (rows + 1) * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(bt->col, col, nnz * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(bt->v64, val, nnz * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(bt->v32, v32.data(), nnz * sizeof(float), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      (num_systems > 0 &&
+       cudaMemcpyAsync(bt->order, sorted.data(), num_systems * sizeof(int), cudaMemcpyHostToDevice, s) !=
+           cudaSuccess) ||
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    set_error("cfd_batch_create: upload failed");
+    return fail(CFD_ERR_CUDA);
+  }
+  *out = bt;
+  return CFD_OK;
+}
+
+}  // namespace cfd
+
+extern "C" {
+
 cfd_status cfd_batch_create(cfd_context* ctx, int32_t num_systems, const int64_t* sys_row_offsets,
                             const int64_t* row_ptr, const int32_t* col, const double* val, cfd_batch** out) {
   return guarded("cfd_batch_create", [&]() -> cfd_status {
@@ -520,90 +573,12 @@ cfd_status cfd_batch_create(cfd_context* ctx, int32_t num_systems, const int64_t
       return CFD_ERR_STATE;
     }
     *out = nullptr;
-    CFD_TRY(validate_batch(num_systems, sys_row_offsets, row_ptr, col, val));
+    CFD_TRY(batch_validate(num_systems, sys_row_offsets, row_ptr, col, val));
     if (!ctx) {
       set_error("cfd_batch_create: null context");
       return CFD_ERR_STATE;
     }
-    const int64_t rows = sys_row_offsets[num_systems];
-    const int64_t nnz = row_ptr[rows];
-    std::lock_guard<std::mutex> g(ctx->mu);
-    CFD_TRY_CUDA(cudaSetDevice(ctx->device));
-    cfd_batch* bt = new cfd_batch;
-    OnUnwind release([&] { cfd_batch_destroy(bt); });
-    bt->ctx = ctx;
-    bt->nsys = num_systems;
-    bt->rows = rows;
-    bt->nnz = nnz;
-    bt->h_sys_row.resize(num_systems + 1);
-    for (int s = 0; s <= num_systems; ++s) bt->h_sys_row[s] = (int)sys_row_offsets[s];
-    std::vector<int> rp32(rows + 1);
-    for (int64_t i = 0; i <= rows; ++i) rp32[i] = (int)row_ptr[i];
-    // Buckets by row count (bucket 0 also takes empty systems), largest system
-    // first inside each bucket.
-    std::vector<int> ord(num_systems);
-    std::iota(ord.begin(), ord.end(), 0);
-    auto nrows = [&](int s) { return bt->h_sys_row[s + 1] - bt->h_sys_row[s]; };
-    auto bucket_of = [&](int s) {
-      int k = 0;
-      while (k + 1 < kBuckets && nrows(s) > kBucketRows[k]) ++k;
-      return k;
-    };
-    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
-      const int ka = bucket_of(a), kb = bucket_of(b);
-      return ka != kb ? ka < kb : nrows(a) > nrows(b);
-    });
-    std::vector<int> sorted = ord;
-    for (int k = 0; k <= kBuckets; ++k) bt->bucket_begin[k] = num_systems;
-    for (int q = num_systems - 1; q >= 0; --q) bt->bucket_begin[bucket_of(sorted[q])] = q;
-    for (int k = kBuckets - 1; k >= 0; --k)
-      if (bt->bucket_begin[k] > bt->bucket_begin[k + 1]) bt->bucket_begin[k] = bt->bucket_begin[k + 1];
-    for (int k = 0; k < kBuckets; ++k) {
-      int nmax = 1, zmax = 1;
-      for (int q = bt->bucket_begin[k]; q < bt->bucket_begin[k + 1]; ++q) {
-        const int sy = sorted[q];
-        nmax = std::max(nmax, nrows(sy));
-        zmax = std::max(zmax, (int)(row_ptr[bt->h_sys_row[sy + 1]] - row_ptr[bt->h_sys_row[sy]]));
-      }
-      bt->bucket_nmax[k] = nmax;
-      bt->bucket_zmax[k] = zmax;
-    }
-    cudaStream_t s = ctx->stream;
-    cfd_status st = CFD_OK;
-    auto fail = [&](cfd_status e) {
-      cfd_batch_destroy(bt);
-      return e;
-    };
-    if ((st = dalloc(&bt->sys_row, num_systems + 1)) != CFD_OK) return fail(st);
-    if ((st = dalloc(&bt->rp, rows + 1)) != CFD_OK) return fail(st);
-    if ((st = dalloc(&bt->col, nnz)) != CFD_OK) return fail(st);
-    if ((st = dalloc(&bt->v64, nnz)) != CFD_OK) return fail(st);
-    if ((st = dalloc(&bt->v32, nnz)) != CFD_OK) return fail(st);
-    if ((st = dalloc(&bt->x, rows)) != CFD_OK) return fail(st);
-    if ((st = dalloc(&bt->b, rows)) != CFD_OK) return fail(st);
-    if ((st = dalloc(&bt->term, num_systems)) != CFD_OK) return fail(st);
-    if ((st = dalloc(&bt->iters, num_systems)) != CFD_OK) return fail(st);
-    if ((st = dalloc(&bt->resid, num_systems)) != CFD_OK) return fail(st);
-    if ((st = dalloc(&bt->order, num_systems)) != CFD_OK) return fail(st);
-    if ((st = dalloc(&bt->queues, kBuckets)) != CFD_OK) return fail(st);
-    if ((st = dalloc(&bt->params, 1)) != CFD_OK) return fail(st);
-    if (cudaMallocHost((void**)&bt->h_params, sizeof(BatchParams)) != cudaSuccess) return fail(CFD_ERR_ALLOC);
-    std::vector<float> v32(val, val + nnz);
-    if (cudaMemcpyAsync(bt->sys_row, bt->h_sys_row.data(), (num_systems + 1) * sizeof(int), cudaMemcpyHostToDevice,
-                        s) != cudaSuccess ||
-        cudaMemcpyAsync(bt->rp, rp32.data(), (rows + 1) * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(bt->col, col, nnz * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(bt->v64, val, nnz * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(bt->v32, v32.data(), nnz * sizeof(float), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        (num_systems > 0 &&
-         cudaMemcpyAsync(bt->order, sorted.data(), num_systems * sizeof(int), cudaMemcpyHostToDevice, s) !=
-             cudaSuccess) ||
-        cudaStreamSynchronize(s) != cudaSuccess) {
-      set_error("cfd_batch_create: upload failed");
-      return fail(CFD_ERR_CUDA);
-    }
-    *out = bt;
-    return CFD_OK;
+    return batch_build(ctx, num_systems, sys_row_offsets, row_ptr, col, val, out);
   });
 }
 
@@ -617,6 +592,7 @@ cfd_status cfd_batch_update_values(cfd_batch* bt, const double* val) {
     CFD_TRY_CUDA(
         cudaMemcpyAsync(bt->v32, v32.data(), bt->nnz * sizeof(float), cudaMemcpyHostToDevice, bt->ctx->stream));
     CFD_TRY_CUDA(cudaStreamSynchronize(bt->ctx->stream));
+    bt->values_valid = true;
     return CFD_OK;
   });
 }
@@ -625,8 +601,16 @@ cfd_status cfd_batch_solve(cfd_batch* bt, const cfd_solve_options* opt, const do
                            const cfd_solver_config* cfg, int32_t* term_out, int32_t* iters_out,
                            double* resid_out, cfd_batch_report* rep) {
   return guarded("cfd_batch_solve", [&]() -> cfd_status {
-    if (!bt || !opt || !b || !x || !cfg || !rep) {
+    if (!bt || !opt || !x || !cfg || !rep) {
       set_error("null argument to cfd_batch_solve");
+      return CFD_ERR_STATE;
+    }
+    if (!b && !bt->rhs_resident) {
+      set_error("cfd_batch_solve: b is NULL but no assembled right-hand side is resident (cfd_batch_assemble)");
+      return CFD_ERR_STATE;
+    }
+    if (!bt->values_valid) {
+      set_error("cfd_batch_solve: the batch holds no valid matrix (assemble it, or update its values, first)");
       return CFD_ERR_STATE;
     }
     if (!(cfg->tolerance >= 0.0) || !(cfg->relative_tolerance >= 0.0) || cfg->max_iterations <= 0 ||
@@ -648,7 +632,10 @@ cfd_status cfd_batch_solve(cfd_batch* bt, const cfd_solve_options* opt, const do
     CFD_TRY(capture_graph(bt, prec));
     CFD_TRY_CUDA(cudaEventRecord(ctx->ev0, s));
     CFD_TRY(set_params(bt, *cfg, *opt));
-    CFD_TRY_CUDA(cudaMemcpyAsync(bt->b, b, bt->rows * sizeof(double), in, s));
+    if (b) {
+      bt->rhs_resident = false;  // the caller's b replaces an assembled one
+      CFD_TRY_CUDA(cudaMemcpyAsync(bt->b, b, bt->rows * sizeof(double), in, s));
+    }
     CFD_TRY_CUDA(cudaMemcpyAsync(bt->x, x, bt->rows * sizeof(double), in, s));
     CFD_TRY_CUDA(cudaGraphLaunch(bt->graph[prec], s));
     CFD_TRY_CUDA(cudaMemcpyAsync(x, bt->x, bt->rows * sizeof(double), outk, s));
@@ -678,12 +665,18 @@ cfd_status cfd_batch_solve(cfd_batch* bt, const cfd_solve_options* opt, const do
 cfd_status cfd_batch_autotune(cfd_batch* bt, int32_t precision, int32_t sample_iterations) {
   return guarded("cfd_batch_autotune", [&]() -> cfd_status {
     if (!bt || precision < 0 || precision > 1 || sample_iterations <= 0) return CFD_ERR_CONFIG;
+    if (!bt->values_valid) {
+      set_error("cfd_batch_autotune: the batch holds no valid matrix (assemble it, or update its values, first)");
+      return CFD_ERR_STATE;
+    }
     std::lock_guard<std::mutex> g(bt->ctx->mu);
     cfd_context* ctx = bt->ctx;
     CFD_TRY_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
     // Representative inputs: x = 0, b = 1; a fixed iteration budget and a zero
-    // tolerance make every candidate do the same work.
+    // tolerance make every candidate do the same work. b = 1 replaces an
+    // assembled right-hand side.
+    bt->rhs_resident = false;
     std::vector<double> ones(bt->rows, 1.0);
     CFD_TRY_CUDA(cudaMemcpyAsync(bt->b, ones.data(), bt->rows * sizeof(double), cudaMemcpyHostToDevice, s));
     cfd_solver_config cfg{0.0, 0.0, sample_iterations};
@@ -748,6 +741,7 @@ cfd_status cfd_batch_destroy(cfd_batch* bt) {
                   (void*)bt->queues, (void*)bt->params})
     if (p) cudaFree(p);
   if (bt->h_params) cudaFreeHost(bt->h_params);
+  network_plan_free(bt->net);
   delete bt;
   return CFD_OK;
 }

@@ -305,7 +305,9 @@ cfd_status cfd_batch_create(cfd_context* ctx, int32_t num_systems, const int64_t
 cfd_status cfd_batch_update_values(cfd_batch* batch, const double* val_host);
 /* opt: solver CG, precond JACOBI, precision FP64 or FP32_REFINE, memory of b/x.
  * x carries the initial guesses in and the solutions out. Per-system outputs
- * (host arrays of num_systems entries) may be NULL. */
+ * (host arrays of num_systems entries) may be NULL. b may be NULL after
+ * cfd_batch_assemble: the assembled right-hand sides, resident on the device,
+ * are used (a solve with a b of its own replaces them). */
 cfd_status cfd_batch_solve(cfd_batch* batch, const cfd_solve_options* opt, const double* b, double* x,
                            const cfd_solver_config* cfg, int32_t* termination, int32_t* iterations,
                            double* rel_residual, cfd_batch_report* rep);
@@ -316,6 +318,45 @@ cfd_status cfd_batch_autotune(cfd_batch* batch, int32_t precision, int32_t sampl
 cfd_status cfd_batch_config(const cfd_batch* batch, int32_t precision, int32_t* bucket_rows,
                             int32_t* threads, int32_t* systems);
 cfd_status cfd_batch_destroy(cfd_batch* batch);
+
+/* ---- network assembly on the device --------------------------------------
+ * MatrixAssembler::assemble_into (crates/cfd-1d/src/solver/core/
+ * matrix_assembly.rs:163-250) for every network of a batch in one launch, so
+ * that the Picard loop of NetworkSolver (network_solver.rs:289-340: assemble,
+ * then solve from the last iterate) runs without the matrix crossing PCIe.
+ * Network s owns global nodes [node_offsets[s], node_offsets[s+1]) and edges
+ * [edge_offsets[s], edge_offsets[s+1]); edge_i / edge_j hold node indices
+ * LOCAL to the edge's network. fixed[k] != 0 makes global node k a Dirichlet
+ * node of pressure fixed_value[k]. The pattern (free-free edges: the 2x2
+ * Laplacian block; edges to fixed nodes: the free node's diagonal, eliminated
+ * into its right-hand side; fixed nodes: identity rows) is built once here,
+ * with duplicate entries of parallel edges summed in edge order. A self-loop
+ * is CFD_ERR_CONFIG (:184-189), nodes out of range CFD_ERR_DIM; the per-network
+ * limits of cfd_batch_create apply. The batch has no valid matrix until the
+ * first cfd_batch_assemble. */
+cfd_status cfd_batch_create_networks(cfd_context* ctx, int32_t num_systems, const int64_t* node_offsets,
+                                     const int64_t* edge_offsets, const int32_t* edge_i, const int32_t* edge_j,
+                                     const int8_t* fixed, const double* fixed_value, cfd_batch** out);
+/* Values (FP64 and the FP32 copy) and right-hand sides from per-edge
+ * conductances (total-edges entries) and optional Neumann sources (one per
+ * node, NULL for none; a fixed node's is ignored), both in `memory`
+ * (CFD_MEMORY_HOST or CFD_MEMORY_DEVICE). A non-finite or non-positive
+ * conductance is CFD_ERR_CONFIG naming the first such edge (:191-203); the
+ * batch then holds no valid matrix until a successful assembly. */
+cfd_status cfd_batch_assemble(cfd_batch* batch, const double* conductance, const double* neumann,
+                              int32_t memory);
+/* Copies the batch's current values (nnz) and right-hand sides (total rows)
+ * to host arrays; either may be NULL. */
+cfd_status cfd_batch_values(cfd_batch* batch, double* val_host, double* rhs_host);
+/* The same assembly on the host, through the same pattern and value code, for
+ * checks without a device: *nnz_out receives the entry count, and each
+ * non-NULL output (row_ptr: total nodes + 1, col: nnz, val: nnz, rhs: total
+ * nodes) is filled; conductance is read only when val or rhs is asked for. */
+cfd_status cfd_network_assemble_host(int32_t num_systems, const int64_t* node_offsets,
+                                     const int64_t* edge_offsets, const int32_t* edge_i,
+                                     const int32_t* edge_j, const int8_t* fixed, const double* fixed_value,
+                                     const double* conductance, const double* neumann, int64_t* nnz_out,
+                                     int64_t* row_ptr, int32_t* col, double* val, double* rhs);
 
 /* ---- diagnostics --------------------------------------------------------
  * The failure path of the bounded device waits (no reference counterpart):
