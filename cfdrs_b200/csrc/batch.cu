@@ -373,7 +373,10 @@ cfd_status enqueue_solve(cfd_batch* bt, int prec, const int* grid, const size_t*
 
 cfd_status capture_graph(cfd_batch* bt, int prec) {
   if (bt->graph[prec]) return CFD_OK;
-  cudaStream_t s = bt->ctx->stream;
+  // Captured on the context's own stream, whatever stream the solve runs on:
+  // CUDA does not capture the legacy default stream (torch's default stream
+  // arrives as cudaStreamLegacy), and the graph launches into any stream.
+  cudaStream_t s = bt->ctx->own;
   int grid[kBuckets];
   size_t smem[kBuckets] = {};
   for (int k = 0; k < kBuckets; ++k) {
