@@ -48,7 +48,8 @@ def _paths(d):
 
 def main(argv=None):
     p = argparse.ArgumentParser()
-    p.add_argument("case", choices=["spmv", "solve", "levels", "batch", "adjoint", "gmres", "timeline", "configs"])
+    p.add_argument("case", choices=["spmv", "solve", "levels", "batch", "assembly", "adjoint", "gmres", "timeline",
+                                    "configs"])
     p.add_argument("--systems", type=int, default=4096)
     p.add_argument("--n", type=int, default=128)
     p.add_argument("--reps", type=int, default=20)
@@ -61,6 +62,8 @@ def main(argv=None):
 
     if a.case == "batch":
         return batch_case(a)
+    if a.case == "assembly":
+        return assembly_case(a)
     if a.case == "adjoint":
         return adjoint_case(a)
     if a.case == "configs":
@@ -292,6 +295,93 @@ def batch_case(a):
         print(f"{prec.name}: device {rep.device_ms:.2f} ms, wall {min(times):.2f} ms, converged "
               f"{rep.converged_systems}/{rep.num_systems}, iterations total {rep.total_iterations} max "
               f"{rep.max_iterations}, max rel residual {rep.max_rel_residual:.2e}, widths {tc}", flush=True)
+    return 0
+
+
+def network_counts(nets) -> dict:
+    """Edges (free-free, free-fixed), fixed nodes and rows of a set of
+    networks: the sizes the device assembly's compulsory bytes follow from."""
+    import numpy as np
+    c = dict(edges=0, ff=0, fd=0, fixed=0, rows=0)
+    for n in nets:
+        fi, fj = n.fixed[n.edges_i] != 0, n.fixed[n.edges_j] != 0
+        c["edges"] += len(n.edges_i)
+        c["ff"] += int(np.sum(~fi & ~fj))
+        c["fd"] += int(np.sum(fi ^ fj))
+        c["fixed"] += int(np.sum(n.fixed != 0))
+        c["rows"] += n.n_nodes
+    return c
+
+
+def assembly_case(a):
+    """Device assembly of the C4 networks (cfd_batch_assemble) from host and
+    from device conductances, its bandwidth on the compulsory bytes, the host
+    path of the same code for comparison, and one Picard pass (assemble from
+    new device conductances, solve from the last iterate with b resident)."""
+    import time
+
+    import numpy as np
+    import torch
+
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.batch import NetworkBatch, network_assemble_host
+    t0 = time.perf_counter()
+    nets = P.network_batch_edges(a.systems, seed=0)
+    nb = NetworkBatch.from_networks(nets)
+    pk = nb.packed
+    nnz = nb.col.shape[0]
+    c = network_counts(nets)
+    edges, fd, rows = c["edges"], c["fd"], c["rows"]
+    contributions = 4 * c["ff"] + fd + c["fixed"]
+    # compulsory bytes: conductances read once; per slot its pointer, its
+    # contribution codes and the FP64 + FP32 values written; per row its
+    # pointer, fixed flag and pressure, its (edge, node) pairs and b written
+    algo = (8 * edges + 4 * (nnz + 1) + 4 * contributions + 12 * nnz + 4 * (rows + 1) + 8 * fd
+            + (1 + 8 + 8) * rows)
+    print(f"{a.systems} networks: {rows} nodes, {edges} edges, {nnz} entries, {contributions} contributions; "
+          f"plan built in {time.perf_counter() - t0:.1f} s; compulsory bytes per assembly {algo / 1e6:.1f} MB",
+          flush=True)
+    stream = torch.cuda.current_stream()
+    gd = torch.tensor(pk.conductance, device="cuda")
+
+    def timed(fn, reps=10):
+        fn()
+        torch.cuda.synchronize()
+        best = None
+        for _ in range(reps):
+            e0, e1 = _events(torch)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1)
+            best = t if best is None else min(best, t)
+        return best
+
+    ms_dev = timed(lambda: nb.assemble(gd))
+    ms_host_in = timed(lambda: nb.assemble(pk.conductance))
+    t0 = time.perf_counter()
+    network_assemble_host(pk, pk.conductance)
+    ms_cpu = (time.perf_counter() - t0) * 1e3
+    print(f"assemble, device conductances: {ms_dev * 1e3:.1f} us ({algo / ms_dev / 1e6:.0f} GB/s on compulsory "
+          f"bytes, includes the 4-byte status read back); host conductances (+ H2D): {ms_host_in * 1e3:.1f} us; "
+          f"the same code on one host core: {ms_cpu:.1f} ms", flush=True)
+    cfg = cf.IterativeSolverConfig(0.0, 1e-10, 40000)
+    x = torch.zeros(pk.rows, dtype=torch.float64, device="cuda")
+    nb.assemble(gd)
+    nb.solve(None, x, config=cfg)
+    g1 = gd * 1.01
+    x_warm = x.clone()
+
+    def picard():
+        nb.assemble(g1)
+        x.copy_(x_warm)
+        return nb.solve(None, x, config=cfg)
+    ms_pass = timed(picard, reps=3)
+    _, rep = picard()
+    print(f"Picard pass (assemble + warm solve, FP64): {ms_pass:.2f} ms, converged {rep.converged_systems}/"
+          f"{rep.num_systems}, iterations total {rep.total_iterations}", flush=True)
     return 0
 
 
