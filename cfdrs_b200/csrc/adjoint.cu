@@ -74,6 +74,7 @@ cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev) {
   // The host copy feeds AMG setup (the Galerkin recompute reads the device values).
   CFD_TRY_CUDA(cudaMemcpyAsync(a->host.v.data(), val_dev, nnz * sizeof(double), cudaMemcpyDeviceToHost, s));
   CFD_TRY_CUDA(cudaStreamSynchronize(s));
+  a->simple_stale = a->simple_nv >= 0;
   if (a->diag64) {
     cudaFree(a->diag64);
     cudaFree(a->diag32);

@@ -12,6 +12,7 @@
 #include "amg_device.h"
 #include "amg_setup.h"
 #include "internal.h"
+#include "simple.h"
 
 namespace cfd {
 
@@ -368,7 +369,7 @@ cfd_status amg_ensure32(cfd_amg* amg) {
   return CFD_OK;
 }
 
-static HostCsr host_from(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* rp, const int32_t* c32,
+HostCsr host_from(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* rp, const int32_t* c32,
                          const int64_t* c64, const double* v) {
   HostCsr h;
   h.nrows = nrows;
@@ -383,7 +384,7 @@ static HostCsr host_from(int64_t nrows, int64_t ncols, int64_t nnz, const int64_
   return h;
 }
 
-static cfd_status validate_csr(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* rp, const int32_t* c32,
+cfd_status validate_csr(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* rp, const int32_t* c32,
                                const int64_t* c64) {
   if (nrows < 0 || ncols < 0 || nnz < 0 || !rp || (nnz > 0 && !c32 && !c64)) {
     set_error("invalid CSR arguments");
@@ -573,6 +574,7 @@ cfd_status cfd_csr_update_values(cfd_csr* a, const double* val) {
     // only once the device copy and the FP32 cast have succeeded.
     CFD_TRY(devmat_update_values(a->dev, val, a->host.nnz(), false, a->ctx->stream));
     std::copy(val, val + a->host.nnz(), a->host.v.begin());
+    a->simple_stale = a->simple_nv >= 0;
     dfree(a->diag64);
     dfree(a->diag32);
     dfree(a->jinv64);
@@ -668,6 +670,7 @@ cfd_status cfd_csr_destroy(cfd_csr* a) {
   dfree(a->diag32);
   dfree(a->jinv64);
   dfree(a->jinv32);
+  simple_free(a->simple);
   delete a;
   return CFD_OK;
 }
@@ -921,7 +924,7 @@ cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, con
                 cfg->tolerance, cfg->relative_tolerance, (long long)cfg->max_iterations);
       return CFD_ERR_CONFIG;
     }
-    if (opt->solver < 0 || opt->solver > 2 || opt->precond < 0 || opt->precond > 2 || opt->precision < 0 ||
+    if (opt->solver < 0 || opt->solver > 2 || opt->precond < 0 || opt->precond > 3 || opt->precision < 0 ||
         opt->precision > 1 || opt->memory < 0 || opt->memory > 1 || (opt->solver == CFD_SOLVER_GMRES && opt->restart < 1)) {
       set_error("invalid solve options");
       return CFD_ERR_CONFIG;

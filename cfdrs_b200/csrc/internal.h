@@ -14,6 +14,8 @@
 
 namespace cfd {
 
+struct SimpleDev;  // simple.h
+
 // Error message of the last failure on this thread (cfd_last_error()).
 void set_error(const char* fmt, ...);
 
@@ -111,6 +113,16 @@ struct HostCsr {
   std::vector<double> v;
   int64_t nnz() const { return (int64_t)ci.size(); }
 };
+
+// A caller's CSR (int64 row offsets; int32 or int64 columns, one of c32/c64),
+// checked without reading past a bound an earlier check established: sizes,
+// row_ptr from 0 to nnz and non-decreasing, columns in range and strictly
+// increasing within a row.
+cfd_status validate_csr(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* rp, const int32_t* c32,
+                        const int64_t* c64);
+// Host copy of a CSR validate_csr accepted.
+HostCsr host_from(int64_t nrows, int64_t ncols, int64_t nnz, const int64_t* rp, const int32_t* c32,
+                  const int64_t* c64, const double* v);
 
 // Device CSR. Indices are int32 (nnz < 2^31); values are kept in FP64 and,
 // once asked for, an FP32 copy sharing the same index arrays.
@@ -240,6 +252,12 @@ struct cfd_csr {
   double* jinv64 = nullptr;  // DiagJacobi inverse diagonal (identity for |d| <= eps)
   float* jinv32 = nullptr;
   int jacobi_status = -1;    // -1 unknown, 0 ok, 1 non-finite diagonal
+  // SIMPLE saddle-point preconditioner (cfd_simple_setup): velocity count,
+  // or -1 when not set up; its device arrays are rebuilt from the host values
+  // after a value update.
+  int64_t simple_nv = -1;
+  cfd::SimpleDev* simple = nullptr;
+  bool simple_stale = false;
 };
 
 namespace cfd {

@@ -10,13 +10,14 @@
 
 #include "amg_device.h"
 #include "internal.h"
+#include "simple.h"
 #include "kernels.cuh"
 
 namespace cfd {
 
 namespace {
 
-constexpr int kPreNone = 0, kPreJacobi = 1, kPreAmg = 2;
+constexpr int kPreNone = 0, kPreJacobi = 1, kPreAmg = 2, kPreSimple = 3;
 
 inline int vec_grid(int64_t n) {
   int64_t g = (n + kThreads - 1) / kThreads;
@@ -936,6 +937,10 @@ static cfd_status gmres_loop(Launcher& lc, cfd_csr* a, cfd_amg* amg, KrylovBufs<
       if (lc.vec(n, k_jacobi_apply<XT>, v, jinv, z, skip) != CFD_OK) return nullptr;
       return z;
     }
+    if (PRE == kPreSimple) {
+      if (simple_apply_device<XT>(a, v, z, skip, lc.s) != CFD_OK) return nullptr;
+      return z;
+    }
     return v;
   };
   int64_t cycles = 0;
@@ -985,7 +990,12 @@ static cfd_status krylov_loop(Launcher& lc, int solver, int pre, cfd_csr* a, cfd
   if (solver == CFD_SOLVER_GMRES) {
     if (pre == kPreJacobi) return gmres_loop<XT, kPreJacobi>(lc, a, amg, B, st, pl, restart);
     if (pre == kPreAmg) return gmres_loop<XT, kPreAmg>(lc, a, amg, B, st, pl, restart);
+    if (pre == kPreSimple) return gmres_loop<XT, kPreSimple>(lc, a, amg, B, st, pl, restart);
     return gmres_loop<XT, kPreNone>(lc, a, amg, B, st, pl, restart);
+  }
+  if (pre == kPreSimple) {
+    set_error("the SIMPLE preconditioner is applied with GMRES only");
+    return CFD_ERR_CONFIG;
   }
   if (solver == CFD_SOLVER_BICGSTAB) {
     if (pre == kPreJacobi) return bicgstab_loop<XT, kPreJacobi>(lc, a, amg, B, st, pl);
@@ -1026,6 +1036,14 @@ cfd_status check_precond(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg)
       set_error("AMG hierarchy does not match the matrix (%lld rows)", (long long)a->dev.nrows);
       return CFD_ERR_DIM;
     }
+  }
+  if (opt.precond == CFD_PRECOND_SIMPLE) {
+    // LinearSolverChain pairs SIMPLE with GMRES (chain.rs:216-238).
+    if (opt.solver != CFD_SOLVER_GMRES) {
+      set_error("the SIMPLE preconditioner is applied with GMRES only (chain.rs:216-238)");
+      return CFD_ERR_CONFIG;
+    }
+    CFD_TRY(simple_ensure(a));
   }
   if (opt.precond == CFD_PRECOND_JACOBI) {
     CFD_TRY(ensure_diagonals(a));

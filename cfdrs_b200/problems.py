@@ -315,3 +315,78 @@ def network_batch_edges(num: int, seed: int = 0, n_min: int = 20, n_max: int = 2
     rng = np.random.default_rng(seed)
     sizes = rng.integers(n_min, n_max + 1, size=num)
     return [random_network_edges(int(n), rng, loop_fraction) for n in sizes]
+
+
+def stokes_2d_mac(n: int, nu: float = 1.0, eps: float = 0.1, seed: int = 0):
+    """2-D Stokes on an ``n x n`` cell MAC (staggered) grid of the unit square,
+    a saddle-point system for the SIMPLE-preconditioned GMRES tier
+    (``crates/cfd-math/src/linear_solver/chain.rs:216-238``).
+
+    Unknowns: u on the interior vertical faces ((n-1) n), v on the interior
+    horizontal faces (n (n-1)), then p per cell (n^2). Momentum rows: the
+    viscous 5-point Laplacian (no-slip walls: normal faces are zero, a
+    tangential wall adds nu/h^2 through the mirrored ghost) and the pressure
+    gradient (p_right - p_left)/h; continuity rows D = G^T; pressure block
+    -eps I (stabilisation, which removes the constant-pressure null space).
+    The matrix is scaled by h^2. Returns ``(A, b, n_velocity)``, b a seeded
+    body force in U[-1, 1] with zero continuity right-hand side."""
+    import scipy.sparse as sp
+    h = 1.0 / n
+    nu_n = (n - 1) * n
+    nv = 2 * nu_n
+    rows, cols, vals = [], [], []
+
+    def add(r, c, v):
+        rows.append(r)
+        cols.append(c)
+        vals.append(v)
+
+    def uid(i, j):  # face x = i h, 1 <= i <= n-1; cell row j
+        return (i - 1) * n + j
+
+    def vid(i, j):  # face y = j h, 1 <= j <= n-1; cell column i
+        return nu_n + i * (n - 1) + (j - 1)
+
+    def pid(i, j):
+        return nv + i * n + j
+    c = nu / (h * h)
+    for i in range(1, n):
+        for j in range(n):
+            r = uid(i, j)
+            d = 4.0 * c
+            for ii in (i - 1, i + 1):
+                if 1 <= ii <= n - 1:
+                    add(r, uid(ii, j), -c)
+            for jj in (j - 1, j + 1):
+                if 0 <= jj <= n - 1:
+                    add(r, uid(i, jj), -c)
+                else:
+                    d += c
+            add(r, r, d)
+            add(r, pid(i, j), 1.0 / h)
+            add(r, pid(i - 1, j), -1.0 / h)
+    for i in range(n):
+        for j in range(1, n):
+            r = vid(i, j)
+            d = 4.0 * c
+            for jj in (j - 1, j + 1):
+                if 1 <= jj <= n - 1:
+                    add(r, vid(i, jj), -c)
+            for ii in (i - 1, i + 1):
+                if 0 <= ii <= n - 1:
+                    add(r, vid(ii, j), -c)
+                else:
+                    d += c
+            add(r, r, d)
+            add(r, pid(i, j), 1.0 / h)
+            add(r, pid(i, j - 1), -1.0 / h)
+    top = sp.coo_matrix((vals, (rows, cols)), shape=(nv, nv + n * n)).tocsr()
+    G = top[:, nv:]
+    D = G.T.tocsr()
+    C = -eps * sp.identity(n * n, format="csr")
+    M = sp.bmat([[top[:, :nv], G], [D, C]], format="csr") * (h * h)
+    M.sum_duplicates()
+    M.sort_indices()
+    rng = np.random.default_rng(seed)
+    b = np.concatenate([rng.uniform(-1.0, 1.0, nv), np.zeros(n * n)])
+    return CsrMatrix(M.indptr, M.indices, M.data, M.shape), b, nv

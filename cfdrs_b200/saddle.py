@@ -1,0 +1,68 @@
+"""SIMPLE saddle-point preconditioner (``cfd_simple_*``).
+
+``SimplePreconditioner`` of ``crates/cfd-math/src/linear_solver/
+block_preconditioner.rs:400-568``, which ``LinearSolverChain`` pairs with
+GMRES for saddle-point systems (``chain.rs:216-238``). The first
+``n_velocity`` unknowns are velocities, the rest pressures; setup extracts
+diag(A)^-1, the divergence rows D, the gradient block G and the diagonal Schur
+approximation diag(C - D diag(A)^-1 G) from the matrix's current values, and
+the apply is u* = diag(A)^-1 f, p = S^-1 (g - D u*), u = u* - diag(A)^-1 G p.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .device import Context, device_matrix
+from .krylov import SolveError
+
+
+class SimplePreconditioner:
+    """``SimplePreconditioner::new(matrix, n_velocity, n_pressure)``. Use it
+    with :func:`cfdrs_b200.gmres_preconditioned` on the same matrix object."""
+
+    def __init__(self, matrix, n_velocity: int, n_pressure: int | None = None, ctx: Context | None = None):
+        n = matrix.shape[0]
+        if n_pressure is None:
+            n_pressure = n - n_velocity
+        if n_velocity < 0 or n_pressure < 0 or n_velocity + n_pressure != n or matrix.shape[1] != n:
+            raise SolveError(f"SIMPLE needs a square matrix of n_velocity + n_pressure rows "
+                             f"({n_velocity} + {n_pressure} != {matrix.shape})")
+        self.matrix = matrix
+        self.n_velocity = int(n_velocity)
+        self.n_pressure = int(n_pressure)
+        self.dm = device_matrix(matrix, ctx)
+        self.ctx = self.dm.ctx
+        _lib.check(_lib.load().cfd_simple_setup(self.dm.h, self.n_velocity))
+
+    def apply(self, r):
+        """z = M^-1 r for a float64 CUDA tensor (``cfd_simple_apply``)."""
+        import torch
+        if not (isinstance(r, torch.Tensor) and r.is_cuda and r.dtype == torch.float64):
+            raise SolveError("apply takes a float64 CUDA tensor")
+        r = r.contiguous()
+        z = torch.empty_like(r)
+        self.ctx.set_stream(torch.cuda.current_stream(r.device).cuda_stream)
+        try:
+            _lib.check(_lib.load().cfd_simple_apply(self.dm.h, C.c_void_p(r.data_ptr()), C.c_void_p(z.data_ptr())))
+        finally:
+            self.ctx.set_stream(None)
+        return z
+
+
+def simple_apply_host(matrix, n_velocity: int, b) -> np.ndarray:
+    """The same setup and apply on the host (``cfd_simple_apply_host``)."""
+    rp = np.ascontiguousarray(matrix.row_ptr, dtype=np.int64)
+    col = np.ascontiguousarray(matrix.col, dtype=np.int32)
+    val = np.ascontiguousarray(matrix.val, dtype=np.float64)
+    bb = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros(matrix.shape[0])
+    p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    _lib.check(_lib.load().cfd_simple_apply_host(matrix.shape[0], p(rp), p(col), p(val), int(n_velocity), p(bb),
+                                                 p(x)))
+    return x
+
+
+__all__ = ["SimplePreconditioner", "simple_apply_host"]

@@ -225,7 +225,12 @@ cfd_status cfd_amg_destroy(cfd_amg* amg);
  * (krylov.rs:150-221); m = the requested restart rounded up the ladder 8, 16, 32,
  * 64, 128, 256 (RestartWidth::covering, krylov.rs:96-120), saturating at 256. */
 typedef enum { CFD_SOLVER_CG = 0, CFD_SOLVER_BICGSTAB = 1, CFD_SOLVER_GMRES = 2 } cfd_solver_kind;
-typedef enum { CFD_PRECOND_NONE = 0, CFD_PRECOND_JACOBI = 1, CFD_PRECOND_AMG = 2 } cfd_precond_kind;
+typedef enum {
+  CFD_PRECOND_NONE = 0,
+  CFD_PRECOND_JACOBI = 1,
+  CFD_PRECOND_AMG = 2,
+  CFD_PRECOND_SIMPLE = 3 /* GMRES only; cfd_simple_setup on the matrix first */
+} cfd_precond_kind;
 typedef enum { CFD_PRECISION_FP64 = 0, CFD_PRECISION_FP32_REFINE = 1 } cfd_precision;
 typedef enum { CFD_MEMORY_HOST = 0, CFD_MEMORY_DEVICE = 1 } cfd_memory;
 
@@ -275,6 +280,24 @@ cfd_status cfd_pattern_outer(cfd_csr* a, const double* lambda_dev, const double*
 /* Replace A's values from device memory (same pattern); the host copy used by
  * AMG setup is refreshed too (cfd_amg_recompute reads the device values). */
 cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev);
+
+/* ---- SIMPLE saddle-point preconditioner -----------------------------------
+ * SimplePreconditioner (crates/cfd-math/src/linear_solver/
+ * block_preconditioner.rs:400-568), the preconditioner of LinearSolverChain's
+ * GMRES + SIMPLE tier (chain.rs:216-238). The first n_velocity unknowns are
+ * velocities, the rest pressures. Setup builds, from the matrix's current
+ * values, diag(A)^-1 (1 where |a_ii| <= 1e-14), the divergence rows D, the
+ * gradient block G and diag(C - D diag(A)^-1 G)^-1; a later value update
+ * (cfd_csr_update_values, cfd_csr_set_values_device) rebuilds them before the
+ * next use. Solve with opt->solver = CFD_SOLVER_GMRES and opt->precond =
+ * CFD_PRECOND_SIMPLE. Apply: u* = diag(A)^-1 f, p = S^-1 (g - D u*),
+ * u = u* - diag(A)^-1 G p. */
+cfd_status cfd_simple_setup(cfd_csr* a, int64_t n_velocity);
+/* z = M^-1 r on the device (FP64; r and z distinct device arrays of n). */
+cfd_status cfd_simple_apply(cfd_csr* a, const double* r_dev, double* z_dev);
+/* The same setup and apply on the host, for checks without a device. */
+cfd_status cfd_simple_apply_host(int64_t n, const int64_t* row_ptr, const int32_t* col, const double* val,
+                                 int64_t n_velocity, const double* b, double* x);
 
 /* ---- batched small systems --------------------------------------------
  * Many independent systems (e.g. the Kirchhoff networks of many design

@@ -19,6 +19,14 @@ struct or_csr {
   int64_t nnz() const { return (int64_t)ci.size(); }
 };
 
+// SimplePreconditioner (crates/cfd-math/src/linear_solver/block_preconditioner.rs:411-424).
+struct or_simple {
+  int64_t nv = 0, np = 0;
+  std::vector<double> dinv, sinv;                                 // diag(A)^-1, diag(S)^-1
+  std::vector<std::vector<std::pair<int64_t, double>>> div_rows;  // D, per pressure row
+  std::vector<std::vector<std::pair<int64_t, double>>> grad_cols; // G, per pressure column
+};
+
 namespace {
 
 // diagonal_epsilon() in multigrid/amg.rs:58-61 and smoothers.rs (|diag| > 1e-15).
@@ -681,12 +689,15 @@ struct Precond {
   int kind;
   const or_amg* amg;
   std::vector<double> inv;
+  const or_simple* simple = nullptr;
   void apply(const double* r, double* z, int64_t n) const {
     if (kind == OR_PRE_JACOBI) {
 #pragma omp parallel for schedule(static)
       for (int64_t i = 0; i < n; ++i) z[i] = r[i] * inv[i];
     } else if (kind == OR_PRE_AMG) {
       or_amg_apply(amg, r, z);
+    } else if (kind == OR_PRE_SIMPLE) {
+      or_simple_apply(simple, r, z);
     } else {
       std::copy(r, r + n, z);
     }
@@ -1033,12 +1044,9 @@ int or_gmres_width(int64_t requested) {
 //   converged, budget spent, or restart.
 // iterations counts Arnoldi steps over all cycles; history[k] is the implicit
 // residual after step k (history[0] = ||r0||).
-int or_gmres(const or_csr* a, int precond, const or_amg* amg, int64_t restart, const double* b, double* x,
-             const or_solver_config* cfg, or_report* rep, double* history) {
+static int gmres_impl(const or_csr* a, const Precond& M, int64_t restart, const double* b, double* x,
+                      const or_solver_config* cfg, or_report* rep, double* history) {
   const int64_t n = a->nrows;
-  if (a->ncols != n) return -1;
-  Precond M{precond, amg, {}};
-  if (precond == OR_PRE_JACOBI && jacobi_inverse(*a, M.inv) != 0) return -2;
   const int m = or_gmres_width(restart);
   std::vector<double> V((size_t)(m + 1) * n), w(n), z(n), r(n), t(n);
   std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), y(m), h1(m + 1), h2(m + 1);
@@ -1144,6 +1152,85 @@ int or_gmres(const or_csr* a, int precond, const or_amg* amg, int64_t restart, c
     }
   }
 }
+
+int or_gmres(const or_csr* a, int precond, const or_amg* amg, int64_t restart, const double* b, double* x,
+             const or_solver_config* cfg, or_report* rep, double* history) {
+  if (a->ncols != a->nrows) return -1;
+  Precond M{precond, amg, {}};
+  if (precond == OR_PRE_JACOBI && jacobi_inverse(*a, M.inv) != 0) return -2;
+  return gmres_impl(a, M, restart, b, x, cfg, rep, history);
+}
+
+int or_gmres_simple(const or_csr* a, const or_simple* simple, int64_t restart, const double* b, double* x,
+                    const or_solver_config* cfg, or_report* rep, double* history) {
+  if (a->ncols != a->nrows || !simple || simple->nv + simple->np != a->nrows) return -1;
+  Precond M{OR_PRE_SIMPLE, nullptr, {}, simple};
+  return gmres_impl(a, M, restart, b, x, cfg, rep, history);
+}
+
+// SimplePreconditioner::new (block_preconditioner.rs:432-508): the momentum
+// diagonal inverse (1 where |a_ii| <= 1e-14, diagonal_epsilon :40-42), the
+// divergence rows D (pressure rows, velocity columns) and gradient columns G
+// (velocity rows' pressure columns, gathered per pressure column in velocity
+// order), and the inverse of diag(C - D diag(A)^-1 G) over the entries of D
+// whose transposed position holds a G entry.
+or_simple* or_simple_new(const or_csr* a, int64_t n_velocity) {
+  const int64_t n = a->nrows;
+  if (a->ncols != n || n_velocity < 0 || n_velocity > n) return nullptr;
+  constexpr double eps = 1e-14;
+  or_simple* S = new or_simple;
+  S->nv = n_velocity;
+  S->np = n - n_velocity;
+  auto diag = [&](int64_t r) {
+    for (int64_t k = a->rp[r]; k < a->rp[r + 1]; ++k)
+      if (a->ci[k] == r) return a->v[k];
+    return 0.0;
+  };
+  S->dinv.resize(S->nv);
+  for (int64_t i = 0; i < S->nv; ++i) {
+    const double d = diag(i);
+    S->dinv[i] = std::fabs(d) > eps ? 1.0 / d : 1.0;
+  }
+  S->div_rows.resize(S->np);
+  for (int64_t i = 0; i < S->np; ++i)
+    for (int64_t k = a->rp[S->nv + i]; k < a->rp[S->nv + i + 1]; ++k)
+      if (a->ci[k] < S->nv) S->div_rows[i].push_back({a->ci[k], a->v[k]});
+  S->grad_cols.resize(S->np);
+  for (int64_t v = 0; v < S->nv; ++v)
+    for (int64_t k = a->rp[v]; k < a->rp[v + 1]; ++k)
+      if (a->ci[k] >= S->nv && a->ci[k] < n) S->grad_cols[a->ci[k] - S->nv].push_back({v, a->v[k]});
+  S->sinv.resize(S->np);
+  for (int64_t i = 0; i < S->np; ++i) {
+    double s = diag(S->nv + i);
+    for (const auto& dv : S->div_rows[i])
+      for (const auto& gv : S->grad_cols[i])
+        if (gv.first == dv.first) {
+          s -= dv.second * S->dinv[dv.first] * gv.second;
+          break;
+        }
+    S->sinv[i] = std::fabs(s) > eps ? 1.0 / s : 1.0;
+  }
+  return S;
+}
+
+// SimplePreconditioner::apply (block_preconditioner.rs:521-568):
+// u* = diag(A)^-1 f; p = S^-1 (g - D u*); u = u* - diag(A)^-1 G p, the last
+// step pressure column by pressure column.
+void or_simple_apply(const or_simple* S, const double* b, double* x) {
+  std::vector<double> us(S->nv), p(S->np);
+  for (int64_t v = 0; v < S->nv; ++v) us[v] = b[v] * S->dinv[v];
+  for (int64_t i = 0; i < S->np; ++i) {
+    double bu = 0.0;
+    for (const auto& dv : S->div_rows[i]) bu += dv.second * us[dv.first];
+    p[i] = (b[S->nv + i] - bu) * S->sinv[i];
+  }
+  for (int64_t v = 0; v < S->nv; ++v) x[v] = us[v];
+  for (int64_t i = 0; i < S->np; ++i)
+    for (const auto& gv : S->grad_cols[i]) x[gv.first] -= S->dinv[gv.first] * gv.second * p[i];
+  for (int64_t i = 0; i < S->np; ++i) x[S->nv + i] = p[i];
+}
+
+void or_simple_free(or_simple* S) { delete S; }
 
 int or_bicgstab(const or_csr* a, int precond, const or_amg* amg, const double* b, double* x,
                 const or_solver_config* cfg, or_report* rep, double* history) {

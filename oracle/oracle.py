@@ -105,6 +105,12 @@ def lib():
         L.or_gmres.argtypes = [P, C.c_int, P, C.c_int64, P, P, P, P, P]
         L.or_gmres_width.restype = C.c_int
         L.or_gmres_width.argtypes = [C.c_int64]
+        L.or_simple_new.restype = P
+        L.or_simple_new.argtypes = [P, I64]
+        L.or_simple_apply.argtypes = [P, P, P]
+        L.or_simple_free.argtypes = [P]
+        L.or_gmres_simple.restype = C.c_int
+        L.or_gmres_simple.argtypes = [P, P, C.c_int64, P, P, P, P, P]
         L.or_network_assemble.restype = C.c_int
         L.or_network_assemble.argtypes = [I64, I64, P, P, P, P, P, P, P, P, P]
         _lib = L
@@ -370,3 +376,34 @@ def network_assemble(n_nodes, edges_i, edges_j, conductance, fixed, fixed_value,
     if rc != 0:
         raise ValueError(f"{NETWORK_ERRORS[rc]} at edge {bad.value}")
     return Csr(out.value), rhs
+
+
+class Simple:
+    """SimplePreconditioner of a saddle-point matrix whose first ``n_velocity``
+    unknowns are velocities (``or_simple_new``)."""
+
+    def __init__(self, a: Csr, n_velocity: int):
+        self.h = lib().or_simple_new(a.h, int(n_velocity))
+        if not self.h:
+            raise ValueError("SIMPLE needs a square matrix and 0 <= n_velocity <= n")
+        self.n = a.info()[0]
+
+    def apply(self, b):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n)
+        lib().or_simple_apply(self.h, _ptr(b), _ptr(x))
+        return x
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_simple_free(self.h)
+            self.h = None
+
+
+def gmres_simple(a: Csr, simple: Simple, b, restart=30, **kw):
+    """GMRES(m) right-preconditioned by SIMPLE (``or_gmres_simple``)."""
+    fn = lib().or_gmres_simple
+
+    def call(h, pre, amg, bp, xp, cfg, rep, hist):
+        return fn(h, simple.h, restart, bp, xp, cfg, rep, hist)
+    return _krylov(call, a, b, **kw)

@@ -153,6 +153,19 @@ GOLDEN = {
         "rhs_b_with_neumann_5": 105.0,
         "tol": 1e-12,
     },
+    "simple_apply": {
+        "source": "crates/cfd-math/src/linear_solver/block_preconditioner.rs:987-1016, 1059-1085",
+        "n_velocity": 2,
+        "b": [4.0, 4.0, 2.0, 2.0],
+        # entries (row, col, value) as the tests' SparseMatrixBuilder adds them
+        "stabilized": {"entries": [[0, 0, 4.0], [1, 1, 4.0], [0, 2, 1.0], [1, 3, 1.0], [2, 0, 1.0], [3, 1, 1.0],
+                                   [2, 2, 1.0], [3, 3, 1.0]],
+                       "x": [0.6666666666666666, 0.6666666666666666, 1.3333333333333333, 1.3333333333333333]},
+        "normalized": {"entries": [[0, 0, 4.0], [1, 1, 4.0], [0, 2, -1.0], [1, 3, -1.0], [2, 0, -1.0],
+                                   [3, 1, -1.0]],
+                       "x": [-2.0, -2.0, -12.0, -12.0]},
+        "tol": 1e-10,
+    },
     # The reference test checks only that the free block is symmetric; the
     # entries below follow from assemble_into's rules (:208-246) by hand:
     # B = 1 (AB, A fixed) + 3 (BC); C = 2 (AC, A fixed) + 3 (BC) + 4 (CD, D fixed);
