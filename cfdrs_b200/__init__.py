@@ -2,8 +2,8 @@
 
 Drop-in for cfd-math's preconditioned Krylov surface: ``krylov`` (CG /
 BiCGSTAB / GMRES entry points, reports and outcome mapping), ``multigrid`` (AMG
-configuration and the device V-cycle), ``saddle`` (the SIMPLE saddle-point
-preconditioner), ``sparse`` (host CSR), ``problems``
+configuration and the device V-cycle), ``saddle`` (the SIMPLE and block-diagonal
+saddle-point preconditioners), ``sparse`` (host CSR), ``problems``
 (seeded assembly of the pressure / Kirchhoff systems). The compute runs in
 ``libcfdgpu.so`` through the C ABI of ``include/cfdgpu.h``.
 """
@@ -17,6 +17,6 @@ from .multigrid import (  # noqa: F401
     AMGConfig, AMGStatistics, AlgebraicMultigrid, CoarseOrder, CoarseSolve, CoarseningStrategy, HostHierarchy,
     IdentityPreconditioner, InterpolationStrategy, JacobiPreconditioner, SmootherType,
 )
-from .saddle import SimplePreconditioner  # noqa: F401
+from .saddle import BlockDiagonalPreconditioner, SimplePreconditioner  # noqa: F401
 
 __version__ = "0.1.0"

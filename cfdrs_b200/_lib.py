@@ -26,7 +26,8 @@ EXPORTS = [
     "cfd_spmv", "cfd_spmv_f32",
     "cfd_amg_config_default", "cfd_amg_setup", "cfd_amg_recompute", "cfd_amg_apply", "cfd_amg_stats",
     "cfd_amg_level", "cfd_amg_set_path", "cfd_amg_destroy", "cfd_amg_setup_host", "cfd_selftest_wait_timeout",
-    "cfd_simple_setup", "cfd_simple_apply", "cfd_simple_apply_host",
+    "cfd_saddle_setup", "cfd_simple_apply", "cfd_block_diagonal_apply", "cfd_simple_apply_host",
+    "cfd_block_diagonal_host",
     "cfd_solve_options_default", "cfd_solve", "cfd_last_kernel_stats",
     "cfd_pattern_outer", "cfd_csr_set_values_device",
     "cfd_batch_create", "cfd_batch_update_values", "cfd_batch_solve", "cfd_batch_autotune", "cfd_batch_config",
@@ -138,8 +139,10 @@ def load():
         "cfd_pattern_outer": (C.c_int, [P, P, P, D, P]),
         "cfd_csr_set_values_device": (C.c_int, [P, P]),
         "cfd_batch_create": (C.c_int, [P, I32, P, P, P, P, PP]),
-        "cfd_simple_setup": (C.c_int, [P, C.c_int64]),
+        "cfd_saddle_setup": (C.c_int, [P, C.c_int64]),
         "cfd_simple_apply": (C.c_int, [P, P, P]),
+        "cfd_block_diagonal_apply": (C.c_int, [P, P, P]),
+        "cfd_block_diagonal_host": (C.c_int, [C.c_int64, P, P, P, C.c_int64, P]),
         "cfd_simple_apply_host": (C.c_int, [C.c_int64, P, P, P, C.c_int64, P, P]),
         "cfd_batch_create_networks": (C.c_int, [P, I32, P, P, P, P, P, P, PP]),
         "cfd_batch_assemble": (C.c_int, [P, P, P, I32]),

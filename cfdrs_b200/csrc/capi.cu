@@ -924,7 +924,7 @@ cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, con
                 cfg->tolerance, cfg->relative_tolerance, (long long)cfg->max_iterations);
       return CFD_ERR_CONFIG;
     }
-    if (opt->solver < 0 || opt->solver > 2 || opt->precond < 0 || opt->precond > 3 || opt->precision < 0 ||
+    if (opt->solver < 0 || opt->solver > 2 || opt->precond < 0 || opt->precond > 4 || opt->precision < 0 ||
         opt->precision > 1 || opt->memory < 0 || opt->memory > 1 || (opt->solver == CFD_SOLVER_GMRES && opt->restart < 1)) {
       set_error("invalid solve options");
       return CFD_ERR_CONFIG;

@@ -252,9 +252,9 @@ struct cfd_csr {
   double* jinv64 = nullptr;  // DiagJacobi inverse diagonal (identity for |d| <= eps)
   float* jinv32 = nullptr;
   int jacobi_status = -1;    // -1 unknown, 0 ok, 1 non-finite diagonal
-  // SIMPLE saddle-point preconditioner (cfd_simple_setup): velocity count,
-  // or -1 when not set up; its device arrays are rebuilt from the host values
-  // after a value update.
+  // Saddle-point split (cfd_saddle_setup): velocity count, or -1 when not
+  // set up; the SIMPLE and block-diagonal arrays are rebuilt from the host
+  // values after a value update.
   int64_t simple_nv = -1;
   cfd::SimpleDev* simple = nullptr;
   bool simple_stale = false;

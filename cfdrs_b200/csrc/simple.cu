@@ -79,6 +79,37 @@ cfd_status simple_build(const HostCsr& a, int64_t n_velocity, SimpleHost& S) {
     }
     S.sinv[i] = std::fabs(s) > eps ? 1.0 / s : 1.0;
   }
+  // BlockDiagonalPreconditioner::new (:258-366)
+  S.bdinv.assign(n, 1.0);
+  std::vector<double> md(S.nv);
+  for (int64_t i = 0; i < S.nv; ++i) {
+    const double d = diag(i);
+    md[i] = std::fabs(d) > eps ? d : 1.0;
+    S.bdinv[i] = std::fabs(md[i]) > eps ? 1.0 / md[i] : 1.0;
+  }
+  bool have_mean = false;
+  double mean = 1.0;  // mean |momentum diagonal| over entries above eps; 1 without velocities
+  for (int64_t i = 0; i < S.np; ++i) {
+    double row_sum = 0.0;
+    for (int64_t k = a.rp[S.nv + i]; k < a.rp[S.nv + i + 1]; ++k)
+      if (a.ci[k] >= S.nv) row_sum += std::fabs(a.v[k]);
+    double pd = row_sum;
+    if (!(row_sum > eps)) {
+      if (!have_mean) {
+        double sum = 0.0;
+        int64_t count = 0;
+        for (int64_t v = 0; v < S.nv; ++v)
+          if (std::fabs(md[v]) > eps) {
+            sum += std::fabs(md[v]);
+            ++count;
+          }
+        mean = count == 0 ? 1.0 : sum / (double)count;
+        have_mean = true;
+      }
+      pd = mean;
+    }
+    S.bdinv[S.nv + i] = std::fabs(pd) > eps ? 1.0 / pd : 1.0;
+  }
   return CFD_OK;
 }
 
@@ -134,6 +165,8 @@ cfd_status simple_upload(const SimpleHost& S, SimpleDev& D, cudaStream_t s) {
   CFD_TRY(put(&D.g_val32, narrow(S.g_val), s));
   CFD_TRY(put(&D.dinv32, narrow(S.dinv), s));
   CFD_TRY(put(&D.sinv32, narrow(S.sinv), s));
+  CFD_TRY(put(&D.bdinv64, S.bdinv, s));
+  CFD_TRY(put(&D.bdinv32, narrow(S.bdinv), s));
   CFD_TRY_CUDA(cudaStreamSynchronize(s));  // the host vectors may go
   return CFD_OK;
 }
@@ -142,7 +175,7 @@ void simple_free(SimpleDev* D) {
   if (!D) return;
   for (void* p : {(void*)D->d_rp, (void*)D->d_col, (void*)D->g_rp, (void*)D->g_col, (void*)D->d_val64,
                   (void*)D->g_val64, (void*)D->dinv64, (void*)D->sinv64, (void*)D->d_val32, (void*)D->g_val32,
-                  (void*)D->dinv32, (void*)D->sinv32})
+                  (void*)D->dinv32, (void*)D->sinv32, (void*)D->bdinv64, (void*)D->bdinv32})
     if (p) cudaFree(p);
   delete D;
 }
@@ -151,7 +184,8 @@ void simple_free(SimpleDev* D) {
 // the context lock with the device selected.
 cfd_status simple_ensure(cfd_csr* a) {
   if (a->simple_nv < 0) {
-    set_error("SIMPLE preconditioner requested but not set up on this matrix (cfd_simple_setup)");
+    set_error("saddle-point preconditioner requested but no velocity/pressure split set on this matrix "
+              "(cfd_saddle_setup)");
     return CFD_ERR_STATE;
   }
   if (a->simple && !a->simple_stale) return CFD_OK;
@@ -183,14 +217,42 @@ cfd_status simple_apply_device(cfd_csr* a, const T* r, T* z, const int* skip, cu
 template cfd_status simple_apply_device<double>(cfd_csr*, const double*, double*, const int*, cudaStream_t);
 template cfd_status simple_apply_device<float>(cfd_csr*, const float*, float*, const int*, cudaStream_t);
 
+namespace {
+template <typename T>
+__global__ void k_scale_by(int64_t n, const T* __restrict__ r, const T* __restrict__ inv, T* __restrict__ z,
+                           const int* skip) {
+  if (skip && *skip) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    z[i] = r[i] * inv[i];
+}
+}  // namespace
+
+template <typename T>
+cfd_status block_diagonal_apply_device(cfd_csr* a, const T* r, T* z, const int* skip, cudaStream_t s) {
+  const int64_t n = a->simple->nv + a->simple->np;
+  const T* inv;
+  if constexpr (sizeof(T) == 8)
+    inv = a->simple->bdinv64;
+  else
+    inv = a->simple->bdinv32;
+  if (n > 0) {
+    k_scale_by<T><<<grid_of(a->ctx, n), 256, 0, s>>>(n, r, inv, z, skip);
+    a->ctx->stats.launches++;
+  }
+  CFD_TRY_CUDA(cudaGetLastError());
+  return CFD_OK;
+}
+template cfd_status block_diagonal_apply_device<double>(cfd_csr*, const double*, double*, const int*, cudaStream_t);
+template cfd_status block_diagonal_apply_device<float>(cfd_csr*, const float*, float*, const int*, cudaStream_t);
+
 }  // namespace cfd
 
 using namespace cfd;
 
 extern "C" {
 
-cfd_status cfd_simple_setup(cfd_csr* a, int64_t n_velocity) {
-  return guarded("cfd_simple_setup", [&]() -> cfd_status {
+cfd_status cfd_saddle_setup(cfd_csr* a, int64_t n_velocity) {
+  return guarded("cfd_saddle_setup", [&]() -> cfd_status {
     if (!a) return CFD_ERR_STATE;
     std::lock_guard<std::mutex> g(a->ctx->mu);
     CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
@@ -214,6 +276,38 @@ cfd_status cfd_simple_apply(cfd_csr* a, const double* r, double* z) {
     CFD_TRY(simple_ensure(a));
     CFD_TRY(simple_apply_device<double>(a, r, z, nullptr, a->ctx->stream));
     CFD_TRY_CUDA(cudaStreamSynchronize(a->ctx->stream));
+    return CFD_OK;
+  });
+}
+
+cfd_status cfd_block_diagonal_apply(cfd_csr* a, const double* r, double* z) {
+  return guarded("cfd_block_diagonal_apply", [&]() -> cfd_status {
+    if (!a || !r || !z) return CFD_ERR_STATE;
+    std::lock_guard<std::mutex> g(a->ctx->mu);
+    CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+    CFD_TRY(simple_ensure(a));
+    CFD_TRY(block_diagonal_apply_device<double>(a, r, z, nullptr, a->ctx->stream));
+    CFD_TRY_CUDA(cudaStreamSynchronize(a->ctx->stream));
+    return CFD_OK;
+  });
+}
+
+cfd_status cfd_block_diagonal_host(int64_t n, const int64_t* row_ptr, const int32_t* col, const double* val,
+                                   int64_t n_velocity, double* inv_diag) {
+  return guarded("cfd_block_diagonal_host", [&]() -> cfd_status {
+    if (n < 0 || !row_ptr) {
+      set_error("cfd_block_diagonal_host: invalid CSR arguments");
+      return CFD_ERR_DIM;
+    }
+    const int64_t nnz = row_ptr[n];
+    CFD_TRY(validate_csr(n, n, nnz, row_ptr, col, nullptr));
+    if ((nnz > 0 && !val) || (n > 0 && !inv_diag)) {
+      set_error("cfd_block_diagonal_host: null array");
+      return CFD_ERR_DIM;
+    }
+    SimpleHost S;
+    CFD_TRY(simple_build(host_from(n, n, nnz, row_ptr, col, nullptr, val), n_velocity, S));
+    std::copy(S.bdinv.begin(), S.bdinv.end(), inv_diag);
     return CFD_OK;
   });
 }

@@ -1,7 +1,13 @@
-// SIMPLE saddle-point preconditioner, SimplePreconditioner of
-// crates/cfd-math/src/linear_solver/block_preconditioner.rs:400-568, as used by
-// the GMRES + SIMPLE tier of LinearSolverChain (chain.rs:216-238).
+// The saddle-point preconditioners of LinearSolverChain over one
+// velocity/pressure split: SimplePreconditioner
+// (crates/cfd-math/src/linear_solver/block_preconditioner.rs:400-568, the
+// GMRES + SIMPLE tier, chain.rs:216-238) and BlockDiagonalPreconditioner
+// (:189-398, the GMRES + block-diagonal tier, chain.rs:265-285). The block
+// diagonal is an inverse diagonal applied like Jacobi: the momentum diagonal
+// (1 where |a_ii| <= 1e-14), and per pressure row the absolute row sum over
+// the pressure block, or the mean |momentum diagonal| where that sum is <= 1e-14.
 //
+// SIMPLE:
 // The first nv unknowns are velocities, the other np pressures. Setup (host,
 // from the matrix's values): the momentum diagonal inverse dinv (1 where
 // |a_ii| <= 1e-14, diagonal_epsilon :40-42), the divergence block D (pressure
@@ -33,6 +39,7 @@ struct SimpleHost {
   std::vector<int32_t> g_rp, g_col;  // G: nv rows, pressure columns counted from 0
   std::vector<double> g_val;
   std::vector<double> dinv, sinv;
+  std::vector<double> bdinv;  // BlockDiagonalPreconditioner's inverse diagonal, all n unknowns
 };
 
 // Arrays in one precision, the view both the host check and the kernels read.
@@ -54,6 +61,8 @@ struct SimpleDev {
   int32_t *d_rp = nullptr, *d_col = nullptr, *g_rp = nullptr, *g_col = nullptr;
   double *d_val64 = nullptr, *g_val64 = nullptr, *dinv64 = nullptr, *sinv64 = nullptr;
   float *d_val32 = nullptr, *g_val32 = nullptr, *dinv32 = nullptr, *sinv32 = nullptr;
+  double* bdinv64 = nullptr;  // block-diagonal inverse, n entries
+  float* bdinv32 = nullptr;
   template <typename T>
   SimpleView<T> view() const;
 };
@@ -70,6 +79,9 @@ cfd_status simple_ensure(cfd_csr* a);
 // skip is non-null and *skip is set.
 template <typename T>
 cfd_status simple_apply_device(cfd_csr* a, const T* r, T* z, const int* skip, cudaStream_t s);
+// z = r * the block-diagonal inverse, same conventions.
+template <typename T>
+cfd_status block_diagonal_apply_device(cfd_csr* a, const T* r, T* z, const int* skip, cudaStream_t s);
 
 template <typename T>
 __host__ __device__ inline T sp_mul(T a, T b) {

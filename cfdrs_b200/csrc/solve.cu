@@ -17,7 +17,7 @@ namespace cfd {
 
 namespace {
 
-constexpr int kPreNone = 0, kPreJacobi = 1, kPreAmg = 2, kPreSimple = 3;
+constexpr int kPreNone = 0, kPreJacobi = 1, kPreAmg = 2, kPreSimple = 3, kPreBlockDiag = 4;
 
 inline int vec_grid(int64_t n) {
   int64_t g = (n + kThreads - 1) / kThreads;
@@ -941,6 +941,10 @@ static cfd_status gmres_loop(Launcher& lc, cfd_csr* a, cfd_amg* amg, KrylovBufs<
       if (simple_apply_device<XT>(a, v, z, skip, lc.s) != CFD_OK) return nullptr;
       return z;
     }
+    if (PRE == kPreBlockDiag) {
+      if (block_diagonal_apply_device<XT>(a, v, z, skip, lc.s) != CFD_OK) return nullptr;
+      return z;
+    }
     return v;
   };
   int64_t cycles = 0;
@@ -991,10 +995,11 @@ static cfd_status krylov_loop(Launcher& lc, int solver, int pre, cfd_csr* a, cfd
     if (pre == kPreJacobi) return gmres_loop<XT, kPreJacobi>(lc, a, amg, B, st, pl, restart);
     if (pre == kPreAmg) return gmres_loop<XT, kPreAmg>(lc, a, amg, B, st, pl, restart);
     if (pre == kPreSimple) return gmres_loop<XT, kPreSimple>(lc, a, amg, B, st, pl, restart);
+    if (pre == kPreBlockDiag) return gmres_loop<XT, kPreBlockDiag>(lc, a, amg, B, st, pl, restart);
     return gmres_loop<XT, kPreNone>(lc, a, amg, B, st, pl, restart);
   }
-  if (pre == kPreSimple) {
-    set_error("the SIMPLE preconditioner is applied with GMRES only");
+  if (pre == kPreSimple || pre == kPreBlockDiag) {
+    set_error("the saddle-point preconditioners are applied with GMRES only");
     return CFD_ERR_CONFIG;
   }
   if (solver == CFD_SOLVER_BICGSTAB) {
@@ -1037,10 +1042,10 @@ cfd_status check_precond(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg)
       return CFD_ERR_DIM;
     }
   }
-  if (opt.precond == CFD_PRECOND_SIMPLE) {
-    // LinearSolverChain pairs SIMPLE with GMRES (chain.rs:216-238).
+  if (opt.precond == CFD_PRECOND_SIMPLE || opt.precond == CFD_PRECOND_BLOCK_DIAGONAL) {
+    // LinearSolverChain pairs both with GMRES (chain.rs:216-238, 265-285).
     if (opt.solver != CFD_SOLVER_GMRES) {
-      set_error("the SIMPLE preconditioner is applied with GMRES only (chain.rs:216-238)");
+      set_error("the saddle-point preconditioners are applied with GMRES only (chain.rs:216-285)");
       return CFD_ERR_CONFIG;
     }
     CFD_TRY(simple_ensure(a));

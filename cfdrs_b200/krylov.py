@@ -115,7 +115,7 @@ def converged_or_none(context: str, report: SolveReport) -> SolveReport | None:
 
 
 _SOLVER_CG, _SOLVER_BICGSTAB, _SOLVER_GMRES = 0, 1, 2
-_PRE_NONE, _PRE_JACOBI, _PRE_AMG, _PRE_SIMPLE = 0, 1, 2, 3
+_PRE_NONE, _PRE_JACOBI, _PRE_AMG, _PRE_SIMPLE, _PRE_BLOCK_DIAGONAL = 0, 1, 2, 3, 4
 
 
 def _solve(solver: int, matrix, rhs, preconditioner, solution, config: IterativeSolverConfig,
@@ -131,13 +131,13 @@ def _solve(solver: int, matrix, rhs, preconditioner, solution, config: Iterative
     elif isinstance(preconditioner, AlgebraicMultigrid):
         pre = _PRE_AMG
         amg_h = preconditioner.h
-    elif type(preconditioner).__name__ == "SimplePreconditioner":
-        pre = _PRE_SIMPLE
+    elif type(preconditioner).__name__ in ("SimplePreconditioner", "BlockDiagonalPreconditioner"):
+        pre = _PRE_SIMPLE if type(preconditioner).__name__ == "SimplePreconditioner" else _PRE_BLOCK_DIAGONAL
         if preconditioner.matrix is not matrix:
-            raise SolveError("the SIMPLE preconditioner was set up on another matrix object")
+            raise SolveError("the saddle-point preconditioner was set up on another matrix object")
     else:
         raise SolveError(f"unsupported preconditioner {type(preconditioner).__name__}")
-    dm = device_matrix(matrix, preconditioner.ctx if pre in (_PRE_AMG, _PRE_SIMPLE) else None)
+    dm = device_matrix(matrix, preconditioner.ctx if pre in (_PRE_AMG, _PRE_SIMPLE, _PRE_BLOCK_DIAGONAL) else None)
     n = dm.shape[0]
     if restart < 1:
         raise SolveError(f"GMRES restart must be positive, got {restart}")

@@ -229,7 +229,8 @@ typedef enum {
   CFD_PRECOND_NONE = 0,
   CFD_PRECOND_JACOBI = 1,
   CFD_PRECOND_AMG = 2,
-  CFD_PRECOND_SIMPLE = 3 /* GMRES only; cfd_simple_setup on the matrix first */
+  CFD_PRECOND_SIMPLE = 3,        /* GMRES only; cfd_saddle_setup on the matrix first */
+  CFD_PRECOND_BLOCK_DIAGONAL = 4 /* GMRES only; cfd_saddle_setup on the matrix first */
 } cfd_precond_kind;
 typedef enum { CFD_PRECISION_FP64 = 0, CFD_PRECISION_FP32_REFINE = 1 } cfd_precision;
 typedef enum { CFD_MEMORY_HOST = 0, CFD_MEMORY_DEVICE = 1 } cfd_memory;
@@ -281,23 +282,33 @@ cfd_status cfd_pattern_outer(cfd_csr* a, const double* lambda_dev, const double*
  * AMG setup is refreshed too (cfd_amg_recompute reads the device values). */
 cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev);
 
-/* ---- SIMPLE saddle-point preconditioner -----------------------------------
- * SimplePreconditioner (crates/cfd-math/src/linear_solver/
- * block_preconditioner.rs:400-568), the preconditioner of LinearSolverChain's
- * GMRES + SIMPLE tier (chain.rs:216-238). The first n_velocity unknowns are
- * velocities, the rest pressures. Setup builds, from the matrix's current
- * values, diag(A)^-1 (1 where |a_ii| <= 1e-14), the divergence rows D, the
- * gradient block G and diag(C - D diag(A)^-1 G)^-1; a later value update
- * (cfd_csr_update_values, cfd_csr_set_values_device) rebuilds them before the
- * next use. Solve with opt->solver = CFD_SOLVER_GMRES and opt->precond =
- * CFD_PRECOND_SIMPLE. Apply: u* = diag(A)^-1 f, p = S^-1 (g - D u*),
- * u = u* - diag(A)^-1 G p. */
-cfd_status cfd_simple_setup(cfd_csr* a, int64_t n_velocity);
+/* ---- saddle-point preconditioners -----------------------------------------
+ * The two of LinearSolverChain's GMRES tiers for saddle-point systems
+ * (crates/cfd-math/src/linear_solver/chain.rs:216-238, 265-285), over one
+ * velocity/pressure split: the first n_velocity unknowns are velocities, the
+ * rest pressures. cfd_saddle_setup builds both from the matrix's current
+ * values; a later value update (cfd_csr_update_values,
+ * cfd_csr_set_values_device) rebuilds them before the next use. Solve with
+ * opt->solver = CFD_SOLVER_GMRES and opt->precond = CFD_PRECOND_SIMPLE or
+ * CFD_PRECOND_BLOCK_DIAGONAL.
+ * SIMPLE (SimplePreconditioner, block_preconditioner.rs:400-568): diag(A)^-1
+ * (1 where |a_ii| <= 1e-14), the divergence rows D, the gradient block G and
+ * diag(C - D diag(A)^-1 G)^-1; apply u* = diag(A)^-1 f, p = S^-1 (g - D u*),
+ * u = u* - diag(A)^-1 G p.
+ * Block diagonal (BlockDiagonalPreconditioner, :189-398): z = r / d with d the
+ * momentum diagonal (1 where |a_ii| <= 1e-14) and, per pressure row, the
+ * absolute row sum over the pressure block, or the mean |momentum diagonal|
+ * where that sum is <= 1e-14. */
+cfd_status cfd_saddle_setup(cfd_csr* a, int64_t n_velocity);
 /* z = M^-1 r on the device (FP64; r and z distinct device arrays of n). */
 cfd_status cfd_simple_apply(cfd_csr* a, const double* r_dev, double* z_dev);
+cfd_status cfd_block_diagonal_apply(cfd_csr* a, const double* r_dev, double* z_dev);
 /* The same setup and apply on the host, for checks without a device. */
 cfd_status cfd_simple_apply_host(int64_t n, const int64_t* row_ptr, const int32_t* col, const double* val,
                                  int64_t n_velocity, const double* b, double* x);
+/* The block-diagonal inverse (n entries) on the host. */
+cfd_status cfd_block_diagonal_host(int64_t n, const int64_t* row_ptr, const int32_t* col, const double* val,
+                                   int64_t n_velocity, double* inv_diag);
 
 /* ---- batched small systems --------------------------------------------
  * Many independent systems (e.g. the Kirchhoff networks of many design

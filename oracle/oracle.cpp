@@ -25,6 +25,7 @@ struct or_simple {
   std::vector<double> dinv, sinv;                                 // diag(A)^-1, diag(S)^-1
   std::vector<std::vector<std::pair<int64_t, double>>> div_rows;  // D, per pressure row
   std::vector<std::vector<std::pair<int64_t, double>>> grad_cols; // G, per pressure column
+  std::vector<double> bdinv;  // BlockDiagonalPreconditioner's inverse diagonal (all n unknowns)
 };
 
 namespace {
@@ -698,6 +699,8 @@ struct Precond {
       or_amg_apply(amg, r, z);
     } else if (kind == OR_PRE_SIMPLE) {
       or_simple_apply(simple, r, z);
+    } else if (kind == OR_PRE_BLOCK_DIAGONAL) {
+      for (int64_t i = 0; i < n; ++i) z[i] = r[i] * simple->bdinv[i];
     } else {
       std::copy(r, r + n, z);
     }
@@ -1161,10 +1164,11 @@ int or_gmres(const or_csr* a, int precond, const or_amg* amg, int64_t restart, c
   return gmres_impl(a, M, restart, b, x, cfg, rep, history);
 }
 
-int or_gmres_simple(const or_csr* a, const or_simple* simple, int64_t restart, const double* b, double* x,
-                    const or_solver_config* cfg, or_report* rep, double* history) {
+int or_gmres_saddle(const or_csr* a, const or_simple* simple, int precond, int64_t restart, const double* b,
+                    double* x, const or_solver_config* cfg, or_report* rep, double* history) {
   if (a->ncols != a->nrows || !simple || simple->nv + simple->np != a->nrows) return -1;
-  Precond M{OR_PRE_SIMPLE, nullptr, {}, simple};
+  if (precond != OR_PRE_SIMPLE && precond != OR_PRE_BLOCK_DIAGONAL) return -1;
+  Precond M{precond, nullptr, {}, simple};
   return gmres_impl(a, M, restart, b, x, cfg, rep, history);
 }
 
@@ -1210,7 +1214,39 @@ or_simple* or_simple_new(const or_csr* a, int64_t n_velocity) {
         }
     S->sinv[i] = std::fabs(s) > eps ? 1.0 / s : 1.0;
   }
+  // BlockDiagonalPreconditioner::new (:258-366): the momentum diagonal (1 where
+  // |a_ii| <= eps) inverted; per pressure row the absolute row sum over the
+  // pressure block, or, where that is <= eps, the mean |momentum diagonal|
+  // over the entries above eps (1 without velocities), inverted.
+  S->bdinv.assign(n, 1.0);
+  std::vector<double> md(S->nv);
+  for (int64_t i = 0; i < S->nv; ++i) {
+    const double d = diag(i);
+    md[i] = std::fabs(d) > eps ? d : 1.0;
+    S->bdinv[i] = std::fabs(md[i]) > eps ? 1.0 / md[i] : 1.0;
+  }
+  for (int64_t i = 0; i < S->np; ++i) {
+    double row_sum = 0.0;
+    for (int64_t k = a->rp[S->nv + i]; k < a->rp[S->nv + i + 1]; ++k)
+      if (a->ci[k] >= S->nv) row_sum += std::fabs(a->v[k]);
+    double pd = row_sum;
+    if (!(row_sum > eps)) {
+      double sum = 0.0;
+      int64_t count = 0;
+      for (int64_t v = 0; v < S->nv; ++v)
+        if (std::fabs(md[v]) > eps) {
+          sum += std::fabs(md[v]);
+          ++count;
+        }
+      pd = count == 0 ? 1.0 : sum / (double)count;
+    }
+    S->bdinv[S->nv + i] = std::fabs(pd) > eps ? 1.0 / pd : 1.0;
+  }
   return S;
+}
+
+void or_block_diagonal_apply(const or_simple* S, const double* b, double* x) {
+  for (int64_t i = 0; i < S->nv + S->np; ++i) x[i] = b[i] * S->bdinv[i];
 }
 
 // SimplePreconditioner::apply (block_preconditioner.rs:521-568):

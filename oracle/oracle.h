@@ -96,7 +96,7 @@ void or_amg_apply(const or_amg* h, const double* r, double* z);
 void or_amg_free(or_amg* h);
 
 /* Krylov. */
-enum { OR_PRE_NONE = 0, OR_PRE_JACOBI = 1, OR_PRE_AMG = 2, OR_PRE_SIMPLE = 3 };
+enum { OR_PRE_NONE = 0, OR_PRE_JACOBI = 1, OR_PRE_AMG = 2, OR_PRE_SIMPLE = 3, OR_PRE_BLOCK_DIAGONAL = 4 };
 enum {
   OR_TERM_CONVERGED = 0,
   OR_TERM_INITIAL_RESIDUAL = 1,
@@ -139,9 +139,14 @@ typedef struct or_simple or_simple;
 or_simple* or_simple_new(const or_csr* a, int64_t n_velocity);
 void or_simple_apply(const or_simple* s, const double* b, double* x);
 void or_simple_free(or_simple* s);
-/* GMRES(m) right-preconditioned by SIMPLE (chain.rs:216-238). */
-int or_gmres_simple(const or_csr* a, const or_simple* simple, int64_t restart, const double* b, double* x,
-                    const or_solver_config* cfg, or_report* rep, double* history);
+/* BlockDiagonalPreconditioner (block_preconditioner.rs:189-398) of the same
+ * split: x = b * its inverse diagonal. */
+void or_block_diagonal_apply(const or_simple* s, const double* b, double* x);
+/* GMRES(m) right-preconditioned by SIMPLE (precond OR_PRE_SIMPLE,
+ * chain.rs:216-238) or by the block diagonal (OR_PRE_BLOCK_DIAGONAL,
+ * chain.rs:265-285) of the split. */
+int or_gmres_saddle(const or_csr* a, const or_simple* simple, int precond, int64_t restart, const double* b,
+                    double* x, const or_solver_config* cfg, or_report* rep, double* history);
 
 /* MatrixAssembler::assemble_into for one network (crates/cfd-1d/src/solver/core/
  * matrix_assembly.rs:163-250). Nodes 0..n-1, edges (ei[e], ej[e]) with

@@ -109,8 +109,9 @@ def lib():
         L.or_simple_new.argtypes = [P, I64]
         L.or_simple_apply.argtypes = [P, P, P]
         L.or_simple_free.argtypes = [P]
-        L.or_gmres_simple.restype = C.c_int
-        L.or_gmres_simple.argtypes = [P, P, C.c_int64, P, P, P, P, P]
+        L.or_block_diagonal_apply.argtypes = [P, P, P]
+        L.or_gmres_saddle.restype = C.c_int
+        L.or_gmres_saddle.argtypes = [P, P, C.c_int, C.c_int64, P, P, P, P, P]
         L.or_network_assemble.restype = C.c_int
         L.or_network_assemble.argtypes = [I64, I64, P, P, P, P, P, P, P, P, P]
         _lib = L
@@ -394,16 +395,28 @@ class Simple:
         lib().or_simple_apply(self.h, _ptr(b), _ptr(x))
         return x
 
+    def apply_block_diagonal(self, b):
+        """BlockDiagonalPreconditioner of the same split."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n)
+        lib().or_block_diagonal_apply(self.h, _ptr(b), _ptr(x))
+        return x
+
     def __del__(self):
         if getattr(self, "h", None):
             lib().or_simple_free(self.h)
             self.h = None
 
 
-def gmres_simple(a: Csr, simple: Simple, b, restart=30, **kw):
-    """GMRES(m) right-preconditioned by SIMPLE (``or_gmres_simple``)."""
-    fn = lib().or_gmres_simple
+PRE_SIMPLE, PRE_BLOCK_DIAGONAL = 3, 4
+
+
+def gmres_simple(a: Csr, simple: Simple, b, restart=30, precond=PRE_SIMPLE, **kw):
+    """GMRES(m) right-preconditioned by SIMPLE, or with ``precond =
+    PRE_BLOCK_DIAGONAL`` by the block diagonal of the same split
+    (``or_gmres_saddle``)."""
+    fn = lib().or_gmres_saddle
 
     def call(h, pre, amg, bp, xp, cfg, rep, hist):
-        return fn(h, simple.h, restart, bp, xp, cfg, rep, hist)
+        return fn(h, simple.h, precond, restart, bp, xp, cfg, rep, hist)
     return _krylov(call, a, b, **kw)

@@ -164,6 +164,8 @@ GOLDEN = {
         "normalized": {"entries": [[0, 0, 4.0], [1, 1, 4.0], [0, 2, -1.0], [1, 3, -1.0], [2, 0, -1.0],
                                    [3, 1, -1.0]],
                        "x": [-2.0, -2.0, -12.0, -12.0]},
+        # BlockDiagonalPreconditioner on the stabilized matrix (:1044-1058)
+        "block_diagonal": {"b": [4.0, 4.0, 1.0, 1.0], "x": [1.0, 1.0, 1.0, 1.0]},
         "tol": 1e-10,
     },
     # The reference test checks only that the free block is symmetric; the

@@ -1,6 +1,7 @@
-"""GMRES + SIMPLE on the device (the saddle-point tier of LinearSolverChain,
-chain.rs:216-238), against the host path of the same preconditioner code
-(bit for bit) and the oracle's GMRES + SIMPLE (iterations within 10 % + 5,
+"""GMRES + SIMPLE and GMRES + block diagonal on the device (the saddle-point
+tiers of LinearSolverChain, chain.rs:216-238, 265-285), against the host path
+of the same preconditioner code (bit for bit) and the oracle's GMRES with the
+same preconditioner (iterations within 10 % + 5,
 error against the direct solution within 10x the oracle's own, or 1e-9
 relative; FP32 inside FP64 refinement: error <= 1e-8 relative)."""
 import numpy as np
@@ -72,3 +73,25 @@ def test_simple_rules_and_value_updates(cuda):
     rep = cf.gmres_preconditioned(A, b, M, x2, cfg, restart=30)
     assert rep.termination == cf.Termination.CONVERGED
     assert np.linalg.norm(2.0 * x2 - x1) <= 1e-8 * np.linalg.norm(x1)
+
+
+def test_block_diagonal_device(cuda, oracle):
+    import torch
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.saddle import block_diagonal_host
+    A, b, nv = P.stokes_2d_mac(16)
+    M = cf.BlockDiagonalPreconditioner(A, nv)
+    r = np.random.default_rng(3).standard_normal(A.shape[0])
+    z = M.apply(torch.tensor(r, device="cuda")).cpu().numpy()
+    assert same_bits(z, r * block_diagonal_host(A, nv))
+    x_ref = spla.spsolve(A.to_scipy().tocsc(), b)
+    Ao = oracle.Csr.from_matrix(A)
+    xo, ro = oracle.gmres_simple(Ao, oracle.Simple(Ao, nv), b, restart=30, precond=oracle.PRE_BLOCK_DIAGONAL,
+                                 rtol=1e-10, max_it=20000)
+    x = np.zeros(A.shape[0])
+    rep = cf.gmres_preconditioned(A, b, M, x, cf.IterativeSolverConfig(0.0, 1e-10, 20000), restart=30)
+    assert rep.termination == cf.Termination.CONVERGED
+    assert abs(rep.iterations - ro.iterations) <= 0.10 * ro.iterations + 5, (rep.iterations, ro.iterations)
+    err, err_o = np.linalg.norm(x - x_ref), np.linalg.norm(xo - x_ref)
+    assert err <= max(10 * err_o, 1e-9 * np.linalg.norm(x_ref)), (err, err_o)

@@ -1,8 +1,9 @@
-"""SIMPLE saddle-point preconditioner on the CPU: the oracle's restatement
-(or_simple_*) on the reference's own tests, the product's host path
-(cfd_simple_apply_host: the setup and the row code the device kernels run)
+"""Saddle-point preconditioners on the CPU (SIMPLE and block diagonal): the
+oracle's restatement (or_simple_*, or_block_diagonal_apply) on the
+reference's own tests, the product's host path (cfd_simple_apply_host,
+cfd_block_diagonal_host: the setup and the row code the device kernels run)
 against the oracle bit for bit, edge cases of the velocity/pressure split,
-and the oracle's GMRES + SIMPLE on a MAC-grid Stokes system."""
+and the oracle's GMRES with each on a MAC-grid Stokes system."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -109,3 +110,43 @@ def test_oracle_gmres_simple_on_stokes(oracle):
     assert np.linalg.norm(x - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
     _, rep_none = oracle.gmres(Ao, b, restart=30, rtol=1e-10, max_it=5000)
     assert rep.iterations < rep_none.iterations
+
+
+def test_block_diagonal_golden(golden, oracle):
+    """block_preconditioner.rs:1044-1058: u = 4/4, p = 1/1."""
+    from cfdrs_b200.saddle import block_diagonal_host
+    g = golden["simple_apply"]
+    A = from_entries(g["stabilized"]["entries"], 4)
+    bd = g["block_diagonal"]
+    xo = oracle.Simple(oracle.Csr.from_matrix(A), g["n_velocity"]).apply_block_diagonal(bd["b"])
+    xp = np.array(bd["b"]) * block_diagonal_host(A, g["n_velocity"])
+    assert np.max(np.abs(xo - np.array(bd["x"]))) < g["tol"] and same_bits(xo, xp)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_block_diagonal_host_equals_oracle(oracle, seed):
+    """Including systems without a pressure block (every pressure row falls
+    back to the mean |momentum diagonal|) and the all-velocity and
+    all-pressure splits."""
+    from cfdrs_b200.saddle import block_diagonal_host
+    rng = np.random.default_rng(50 + seed)
+    nv, np_ = int(rng.integers(5, 90)), int(rng.integers(1, 40))
+    A = random_saddle(rng, nv, np_, stab=seed % 2 == 0)
+    b = rng.standard_normal(nv + np_)
+    for split in (nv, 0, nv + np_):
+        xo = oracle.Simple(oracle.Csr.from_matrix(A), split).apply_block_diagonal(b)
+        assert same_bits(xo, b * block_diagonal_host(A, split))
+
+
+def test_oracle_gmres_block_diagonal_on_stokes(oracle):
+    """GMRES(30) + block diagonal (chain.rs:265-285) converges on the 16 x 16
+    Stokes system, between SIMPLE and no preconditioner in iterations."""
+    A, b, nv = P.stokes_2d_mac(16)
+    x_ref = spla.spsolve(A.to_scipy().tocsc(), b)
+    Ao = oracle.Csr.from_matrix(A)
+    S = oracle.Simple(Ao, nv)
+    x, rep = oracle.gmres_simple(Ao, S, b, restart=30, precond=oracle.PRE_BLOCK_DIAGONAL, rtol=1e-10, max_it=5000)
+    assert rep.termination == "Converged" and np.linalg.norm(x - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
+    _, rs = oracle.gmres_simple(Ao, S, b, restart=30, rtol=1e-10, max_it=5000)
+    _, rn = oracle.gmres(Ao, b, restart=30, rtol=1e-10, max_it=5000)
+    assert rs.iterations < rep.iterations < rn.iterations
