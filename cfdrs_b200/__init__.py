@@ -3,7 +3,7 @@
 Drop-in for cfd-math's preconditioned Krylov surface: ``krylov`` (CG /
 BiCGSTAB / GMRES entry points, reports and outcome mapping), ``multigrid`` (AMG
 configuration and the device V-cycle), ``saddle`` (the SIMPLE and block-diagonal
-saddle-point preconditioners), ``sparse`` (host CSR), ``problems``
+saddle-point preconditioners), ``chain`` (``LinearSolverChain`` over them), ``sparse`` (host CSR), ``problems``
 (seeded assembly of the pressure / Kirchhoff systems). The compute runs in
 ``libcfdgpu.so`` through the C ABI of ``include/cfdgpu.h``.
 """
@@ -18,5 +18,6 @@ from .multigrid import (  # noqa: F401
     IdentityPreconditioner, InterpolationStrategy, JacobiPreconditioner, SmootherType,
 )
 from .saddle import BlockDiagonalPreconditioner, SimplePreconditioner  # noqa: F401
+from .chain import LinearSolverChain, LinearSolverState  # noqa: F401
 
 __version__ = "0.1.0"

@@ -95,3 +95,29 @@ def test_block_diagonal_device(cuda, oracle):
     assert abs(rep.iterations - ro.iterations) <= 0.10 * ro.iterations + 5, (rep.iterations, ro.iterations)
     err, err_o = np.linalg.norm(x - x_ref), np.linalg.norm(xo - x_ref)
     assert err <= max(10 * err_o, 1e-9 * np.linalg.norm(x_ref)), (err, err_o)
+
+
+def test_chain_on_stokes(cuda):
+    """LinearSolverChain on the 16 x 16 Stokes system: GMRES + SIMPLE is the
+    first tier that exists here and converges; with a budget of 20 iterations
+    every tier fails and the chain reports it."""
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.chain import LinearSolverChain
+    A, b, nv = P.stokes_2d_mac(16)
+    x_ref = spla.spsolve(A.to_scipy().tocsc(), b)
+    chain = LinearSolverChain(cf.IterativeSolverConfig(0.0, 1e-10, 20000)).with_krylov_restart(30)
+    x = chain.solve(A, b, nv)
+    assert chain.trace[-1][0] == "GMRES+SIMPLE" and chain.trace[-1][1].startswith("converged")
+    assert np.linalg.norm(x - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
+    # warm: from a perturbed solution, to an absolute residual (a relative one
+    # would be relative to the guess's already small residual)
+    nb = np.linalg.norm(b)
+    warm = LinearSolverChain(cf.IterativeSolverConfig(1e-9 * nb, 0.0, 20000)).with_krylov_restart(30)
+    guess = x_ref * (1.0 + 1e-3 * np.random.default_rng(0).standard_normal(x_ref.shape[0]))
+    x = warm.solve_with_guess(A, b, nv, guess)
+    assert np.linalg.norm(b - A.to_scipy() @ x) <= 1.5e-9 * nb
+    tight = LinearSolverChain(cf.IterativeSolverConfig(0.0, 1e-10, 20)).with_krylov_restart(30)
+    with pytest.raises(cf.SolveError, match="all solver tiers failed"):
+        tight.solve(A, b, nv)
+    assert [t for t, _ in tight.trace if not _.startswith("skipped")][-1] == "BiCGSTAB"
