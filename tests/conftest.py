@@ -34,3 +34,19 @@ def cuda():
     import cfdrs_b200._lib as L
     L.load()
     return torch
+
+
+# Under `pytest -x` the first failure ends the run, so the suites of the solve
+# path itself (parity, GMRES, batch, adjoint, recompute) run before the
+# components added on top of them (device network assembly, the saddle-point
+# tiers), and the suites that must come last (the no-alloc and wait-timeout
+# checks) keep their place at the end.
+_FILE_ORDER = ["test_gpu_parity", "test_gpu_gmres", "test_gpu_batch", "test_gpu_adjoint", "test_gpu_recompute",
+               "test_gpu_network_assembly", "test_gpu_simple", "test_zz_no_alloc", "test_zz_wait_timeout"]
+
+
+def pytest_collection_modifyitems(session, config, items):
+    def rank(item):
+        stem = os.path.splitext(os.path.basename(str(item.fspath)))[0]
+        return _FILE_ORDER.index(stem) if stem in _FILE_ORDER else -1
+    items.sort(key=rank)  # stable: CPU suites (rank -1) first, in their collected order
