@@ -190,3 +190,37 @@ def test_create_networks_checks_before_the_context():
                                      C.byref(out))
     assert st == 1 and b"at most 2048" in L.cfd_last_error()
     assert L.cfd_batch_assemble(None, None, None, 0) == 7
+
+
+def test_degenerate_networks_bit_for_bit(oracle):
+    """A single fixed node; a single free node without edges (an empty row);
+    an edgeless network; every node fixed with edges only between fixed
+    nodes (identity rows, nothing else); a free node isolated inside a
+    network; parallel edges only."""
+    N = P.Network
+    i32 = lambda *v: np.array(v, np.int32)  # noqa: E731
+    nets = [
+        N(1, i32(), i32(), np.zeros(0), np.array([1], np.int8), np.array([7.5])),
+        N(1, i32(), i32(), np.zeros(0), np.array([0], np.int8), np.zeros(1)),
+        N(4, i32(), i32(), np.zeros(0), np.array([1, 0, 0, 1], np.int8), np.array([1.0, 0, 0, 2.0])),
+        N(3, i32(0, 1, 0), i32(1, 2, 2), np.array([0.5, 0.25, 4.0]), np.ones(3, np.int8), np.array([1.0, 2.0, 3.0])),
+        N(5, i32(0, 1, 3), i32(1, 3, 4), np.array([1.0, 2.0, 3.0]), np.array([1, 0, 0, 0, 1], np.int8),
+          np.array([10.0, 0, 0, 0, -10.0])),
+        N(2, i32(0, 1, 0, 1), i32(1, 0, 1, 0), np.array([1.0, 2.0, 3.0, 4.0]), np.array([0, 1], np.int8),
+          np.array([0.0, 5.0])),
+    ]
+    rp, col, val, rhs = check_against_oracle(oracle, nets, np.linspace(-1, 1, sum(n.n_nodes for n in nets)))
+    assert rp[2] - rp[1] == 0  # the lone free node: an empty row
+    # network 4's node 2 (global 1 + 1 + 4 + 3 + 2 = 11) has no edge: empty row, RHS = its source
+    assert rp[12] - rp[11] == 0
+    # the all-fixed network: identity rows only
+    k0, k1 = rp[6], rp[9]
+    assert np.array_equal(val[k0:k1], np.ones(3)) and np.array_equal(col[k0:k1], [0, 1, 2])
+
+
+def test_empty_batch():
+    from cfdrs_b200.batch import PackedNetworks
+    pk = PackedNetworks(np.zeros(1, np.int64), np.zeros(1, np.int64), np.zeros(0, np.int32), np.zeros(0, np.int32),
+                        np.zeros(0, np.int8), np.zeros(0), np.zeros(0))
+    rp, col, val, rhs = network_assemble_host(pk, pk.conductance)
+    assert rp.tolist() == [0] and col.size == 0 and val.size == 0 and rhs.size == 0
