@@ -217,6 +217,8 @@ class NetworkBatch:
                 raise SolveError("with a CUDA x, b must be None or a matching contiguous float64 CUDA tensor")
             xx, bp, xp = x, (None if b is None else C.c_void_p(b.data_ptr())), C.c_void_p(x.data_ptr())
         else:
+            if _torch_cuda(b):
+                raise SolveError("b is a CUDA tensor: pass x as a float64 CUDA tensor as well (device solve)")
             bb = None if b is None else np.ascontiguousarray(b, dtype=np.float64)
             if bb is not None and bb.shape[0] != self.rows:
                 raise SolveError(f"rhs has {bb.shape[0]} entries, the batch {self.rows} rows")
