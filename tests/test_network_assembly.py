@@ -224,3 +224,11 @@ def test_empty_batch():
                         np.zeros(0, np.int8), np.zeros(0), np.zeros(0))
     rp, col, val, rhs = network_assemble_host(pk, pk.conductance)
     assert rp.tolist() == [0] and col.size == 0 and val.size == 0 and rhs.size == 0
+
+
+def test_full_c4_workload_bit_for_bit(oracle):
+    """All 4096 networks of the C4 workload (about 4.2 M nodes and 13 M
+    entries), the full size the device assembly runs at."""
+    nets = P.network_batch_edges(4096, seed=0)
+    rp, col, val, rhs = check_against_oracle(oracle, nets)
+    assert rp.shape[0] == sum(n.n_nodes for n in nets) + 1 and col.size > 13_000_000
