@@ -72,11 +72,13 @@ def test_host_path_equals_oracle_bit_for_bit(oracle, seed):
     assert same_bits(xo, xp)
 
 
-@pytest.mark.parametrize("n", [4, 9, 16])
+@pytest.mark.parametrize("n", [4, 9, 16, 64])
 def test_stokes_host_path_equals_oracle(oracle, n):
+    from cfdrs_b200.saddle import block_diagonal_host
     A, b, nv = P.stokes_2d_mac(n)
-    xo = oracle.Simple(oracle.Csr.from_matrix(A), nv).apply(b)
-    assert same_bits(xo, simple_apply_host(A, nv, b))
+    S = oracle.Simple(oracle.Csr.from_matrix(A), nv)
+    assert same_bits(S.apply(b), simple_apply_host(A, nv, b))
+    assert same_bits(S.apply_block_diagonal(b), b * block_diagonal_host(A, nv))
 
 
 def test_split_edge_cases(oracle):
