@@ -33,8 +33,8 @@ struct NetworkPlanDev {
   double* fixed_value = nullptr;
   double* g = nullptr;  // staging for conductances given in host memory
   double* q = nullptr;  // staging for Neumann sources given in host memory
-  int* bad = nullptr;   // smallest rejected edge; >= edges when none
-  int* h_bad = nullptr;  // pinned mirror
+  int* bad = nullptr;    // [0] smallest rejected edge (>= edges when none); [1] non-finite flags
+  int* h_bad = nullptr;  // pinned mirror of both
 
   NetworkView view() const { return {slot_ptr, slot_src, rhs_ptr, rhs_edge, rhs_node, fixed, fixed_value}; }
 };
@@ -53,6 +53,8 @@ namespace {
 
 constexpr int kAsmThreads = 256;
 
+// bad[0]: smallest edge with a rejected conductance; bad[1]: bit 0 a
+// non-finite matrix entry, bit 1 a non-finite right-hand side.
 __global__ void k_network_assemble(NetworkView V, int64_t edges, int64_t nnz, int64_t rows,
                                    const double* __restrict__ g, const double* __restrict__ q, double* v64,
                                    float* v32, double* b, int* bad) {
@@ -64,8 +66,13 @@ __global__ void k_network_assemble(NetworkView V, int64_t edges, int64_t nnz, in
     const double v = net_slot_value(V, k, g);
     v64[k] = v;
     v32[k] = (float)v;
+    if (!isfinite(v)) atomicOr(bad + 1, 1);
   }
-  for (int64_t r = t0; r < rows; r += stride) b[r] = net_rhs_value(V, r, g, q);
+  for (int64_t r = t0; r < rows; r += stride) {
+    const double br = net_rhs_value(V, r, g, q);
+    b[r] = br;
+    if (!isfinite(br)) atomicOr(bad + 1, 2);
+  }
 }
 
 template <typename T>
@@ -83,6 +90,15 @@ cfd_status bad_conductance(const char* what, int64_t e, double g) {
   set_error("%s: %s conductance %g at edge %lld (matrix_assembly.rs:191-203)", what,
             std::isfinite(g) ? "non-positive" : "non-finite", g, (long long)e);
   return CFD_ERR_CONFIG;
+}
+
+// validate_linear_system (solver_detection.rs:66-93): the assembled matrix and
+// right-hand side must be finite (a Neumann source or fixed pressure that is
+// not, or a conductance sum that overflows).
+cfd_status nonfinite_system(const char* what, int flags) {
+  set_error("%s: %s", what, (flags & 1) ? "assembled matrix has a non-finite entry (solver_detection.rs:66-93)"
+                                        : "RHS contains non-finite entries (solver_detection.rs:84-93)");
+  return CFD_ERR_NONFINITE;
 }
 
 }  // namespace
@@ -237,11 +253,11 @@ cfd_status cfd_batch_create_networks(cfd_context* ctx, int32_t num_systems, cons
         (st = upload(&d->fixed_value, P.fixed_value, s)) != CFD_OK ||
         (st = upload(&d->g, std::vector<double>(P.edges), s)) != CFD_OK ||
         (st = upload(&d->q, std::vector<double>(P.rows), s)) != CFD_OK ||
-        (st = upload(&d->bad, std::vector<int>(1), s)) != CFD_OK) {
+        (st = upload(&d->bad, std::vector<int>(2), s)) != CFD_OK) {
       cfd_batch_destroy(bt);
       return st;
     }
-    if (cudaMallocHost((void**)&d->h_bad, sizeof(int)) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+    if (cudaMallocHost((void**)&d->h_bad, 2 * sizeof(int)) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
       cfd_batch_destroy(bt);
       set_error("cfd_batch_create_networks: plan upload failed");
       return CFD_ERR_CUDA;
@@ -284,6 +300,7 @@ cfd_status cfd_batch_assemble(cfd_batch* bt, const double* conductance, const do
     }
     // Every byte 0x7f: an int above any edge index (edges <= kMaxNetworkEdges).
     CFD_TRY_CUDA(cudaMemsetAsync(d->bad, 0x7f, sizeof(int), s));
+    CFD_TRY_CUDA(cudaMemsetAsync(d->bad + 1, 0, sizeof(int), s));
     // From here until a successful end the batch holds no usable system.
     bt->values_valid = false;
     bt->rhs_resident = false;
@@ -296,7 +313,7 @@ cfd_status cfd_batch_assemble(cfd_batch* bt, const double* conductance, const do
       CFD_TRY_CUDA(cudaGetLastError());
       ctx->stats.launches++;
     }
-    CFD_TRY_CUDA(cudaMemcpyAsync(d->h_bad, d->bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CFD_TRY_CUDA(cudaMemcpyAsync(d->h_bad, d->bad, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
     CFD_TRY_CUDA(cudaStreamSynchronize(s));
     const int64_t e = *d->h_bad;
     if (e < d->edges) {
@@ -307,6 +324,7 @@ cfd_status cfd_batch_assemble(cfd_batch* bt, const double* conductance, const do
         CFD_TRY_CUDA(cudaMemcpy(&ge, conductance + e, sizeof(double), cudaMemcpyDeviceToHost));
       return bad_conductance("cfd_batch_assemble", e, ge);
     }
+    if (d->h_bad[1]) return nonfinite_system("cfd_batch_assemble", d->h_bad[1]);
     bt->values_valid = true;
     bt->rhs_resident = true;
     return CFD_OK;
@@ -352,11 +370,18 @@ cfd_status cfd_network_assemble_host(int32_t num_systems, const int64_t* node_of
       if (!net_conductance_ok(conductance[e])) return bad_conductance("cfd_network_assemble_host", e, conductance[e]);
     const NetworkView V{P.slot_ptr.data(), P.slot_src.data(), P.rhs_ptr.data(), P.rhs_edge.data(),
                         P.rhs_node.data(), P.fixed.data(), P.fixed_value.data()};
+    int flags = 0;
     if (val)
-      for (int64_t k = 0; k < nnz; ++k) val[k] = net_slot_value(V, k, conductance);
+      for (int64_t k = 0; k < nnz; ++k) {
+        val[k] = net_slot_value(V, k, conductance);
+        if (!std::isfinite(val[k])) flags |= 1;
+      }
     if (rhs)
-      for (int64_t r = 0; r < P.rows; ++r) rhs[r] = net_rhs_value(V, r, conductance, neumann);
-    return CFD_OK;
+      for (int64_t r = 0; r < P.rows; ++r) {
+        rhs[r] = net_rhs_value(V, r, conductance, neumann);
+        if (!std::isfinite(rhs[r])) flags |= 2;
+      }
+    return flags ? nonfinite_system("cfd_network_assemble_host", flags) : CFD_OK;
   });
 }
 

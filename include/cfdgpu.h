@@ -375,8 +375,11 @@ cfd_status cfd_batch_create_networks(cfd_context* ctx, int32_t num_systems, cons
  * conductances (total-edges entries) and optional Neumann sources (one per
  * node, NULL for none; a fixed node's is ignored), both in `memory`
  * (CFD_MEMORY_HOST or CFD_MEMORY_DEVICE). A non-finite or non-positive
- * conductance is CFD_ERR_CONFIG naming the first such edge (:191-203); the
- * batch then holds no valid matrix until a successful assembly. */
+ * conductance is CFD_ERR_CONFIG naming the first such edge (:191-203); a
+ * non-finite assembled entry or right-hand side (a source or fixed pressure
+ * that is not finite, an overflowing sum) is CFD_ERR_NONFINITE, as
+ * validate_linear_system rejects it (solver_detection.rs:66-93). After either
+ * the batch holds no valid matrix until a successful assembly. */
 cfd_status cfd_batch_assemble(cfd_batch* batch, const double* conductance, const double* neumann,
                               int32_t memory);
 /* Copies the batch's current values (nnz) and right-hand sides (total rows)

@@ -161,3 +161,25 @@ def test_state_rules(cuda, nets):
     # other CTA widths after the autotune: other reduction orders, so equal to
     # the solve tolerance, not bit for bit
     assert np.linalg.norm(x3 - x) <= 1e-8 * np.linalg.norm(x)
+
+
+def test_nonfinite_system_rejected_on_device(cuda, nets):
+    """A non-finite Neumann source makes a non-finite right-hand side, which
+    the assembly rejects (validate_linear_system, solver_detection.rs:66-93);
+    the batch then holds no matrix until a good assembly."""
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import _lib
+    from cfdrs_b200.batch import NetworkBatch
+    from cfdrs_b200.krylov import SolveError
+    nb = NetworkBatch.from_networks(nets[:3])
+    pk = nb.packed
+    q = np.zeros(pk.rows)
+    q[5] = np.inf
+    with pytest.raises(_lib.CfdError, match="RHS contains non-finite") as e:
+        nb.assemble(pk.conductance, q)
+    assert e.value.status == 5
+    with pytest.raises(SolveError, match="no valid matrix"):
+        nb.solve(np.ones(pk.rows), config=cf.IterativeSolverConfig(0.0, 1e-10, 20000))
+    nb.assemble(pk.conductance)
+    _, rep = nb.solve(None, config=cf.IterativeSolverConfig(0.0, 1e-10, 20000))
+    assert rep.converged_systems == rep.num_systems

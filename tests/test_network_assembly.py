@@ -232,3 +232,21 @@ def test_full_c4_workload_bit_for_bit(oracle):
     nets = P.network_batch_edges(4096, seed=0)
     rp, col, val, rhs = check_against_oracle(oracle, nets)
     assert rp.shape[0] == sum(n.n_nodes for n in nets) + 1 and col.size > 13_000_000
+
+
+def test_nonfinite_system_is_rejected():
+    """validate_linear_system (solver_detection.rs:66-93): a fixed pressure or
+    Neumann source that is not finite, or conductances whose sum overflows."""
+    L = _lib.load()
+    net = _line(4)
+    pk = pack_networks([net])
+    for kw, msg in ((dict(fixed_value=np.array([np.inf, 0, 0, 0])), b"RHS contains non-finite"),
+                    (dict(conductance=np.array([1.7e308, 1.7e308, 1.0])), b"non-finite entry")):
+        d = dict(pk.__dict__)
+        d.update(kw)
+        bad = type(pk)(**d)
+        with pytest.raises(_lib.CfdError, match="non-finite") as e:
+            network_assemble_host(bad, bad.conductance)
+        assert e.value.status == 5 and msg in L.cfd_last_error()  # CFD_ERR_NONFINITE
+    with pytest.raises(_lib.CfdError, match="RHS contains non-finite"):
+        network_assemble_host(pk, pk.conductance, np.array([0.0, np.nan, 0.0, 0.0]))
