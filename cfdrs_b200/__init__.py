@@ -3,7 +3,8 @@
 Drop-in for cfd-math's preconditioned Krylov surface: ``krylov`` (CG /
 BiCGSTAB / GMRES entry points, reports and outcome mapping), ``multigrid`` (AMG
 configuration and the device V-cycle), ``saddle`` (the SIMPLE and block-diagonal
-saddle-point preconditioners), ``chain`` (``LinearSolverChain`` over them), ``sparse`` (host CSR), ``problems``
+saddle-point preconditioners), ``chain`` (``LinearSolverChain`` over them), ``pressure`` (the 2-D
+pressure-correction dispatch), ``sparse`` (host CSR), ``problems``
 (seeded assembly of the pressure / Kirchhoff systems). The compute runs in
 ``libcfdgpu.so`` through the C ABI of ``include/cfdgpu.h``.
 """
@@ -19,5 +20,6 @@ from .multigrid import (  # noqa: F401
 )
 from .saddle import BlockDiagonalPreconditioner, SimplePreconditioner  # noqa: F401
 from .chain import LinearSolverChain, LinearSolverState  # noqa: F401
+from .pressure import PressureCorrectionDispatch, PressureLinearSolver  # noqa: F401
 
 __version__ = "0.1.0"
