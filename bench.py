@@ -36,7 +36,6 @@ sys.path.insert(0, ROOT)
 
 METRIC = "ms to 1e-8 rel-residual (FP32 AMG-PCG + FP64 refinement), 256^3 variable-k Poisson"
 RTOL = 1e-8
-SAMPLE_ITERATIONS = 2  # PCG iterations per CPU-reference step (scaled to the full solve)
 
 
 def parse():
@@ -376,8 +375,8 @@ def batch_config(systems):
 
 
 def run_reference_plain(args, O, P, cores):
-    """The oracle on the c1 / c2 workload: c1 times full Jacobi-PCG solves (a
-    few ms each); c2 builds the oracle's hierarchy and samples like c3."""
+    """The oracle on the c1 / c2 workload: each step one full solve (c1
+    Jacobi-PCG; c2 AMG-PCG on the oracle's own hierarchy, built once)."""
     A, b, cfg = plain_problem(args, P)
     Ao = O.Csr.from_matrix(A)
     extra = {}
@@ -392,19 +391,17 @@ def run_reference_plain(args, O, P, cores):
         sample = "full FP64 Jacobi-PCG solves to 1e-8 (each step one solve)"
     else:
         t0 = time.perf_counter()
-        amg = O.Amg(Ao, O.AmgConfig(max_levels=16, min_coarse_size=4096, smoother=O.SMOOTH_JACOBI, pre_smooth=1,
-                                    post_smooth=1, relaxation=2 / 3, coarse_solve=O.COARSE_DENSE, interpolation=2,
-                                    coarse_order=1))
+        amg = oracle_amg(O, Ao)
         extra["setup_s"] = time.perf_counter() - t0
-        _, full = O.pcg(Ao, b, precond=O.PRE_AMG, amg=amg, rtol=RTOL, max_it=1000)
-        k = min(SAMPLE_ITERATIONS, max(full.iterations, 1))
+        rows, nnz, opc = oracle_hierarchy_stats(amg)
+        cfg.update(hierarchy_config(nnz[0], len(rows), opc))
         times = []
         for s in range(args.warmup + args.steps):
-            dt = oracle_solve_estimate(O, Ao, b, amg, full.iterations, k)
+            dt, _, full = oracle_full_solve(O, Ao, b, amg)
             if s >= args.warmup:
                 times.append(dt)
-        sample = (f"per step the start-up, {k} FP64 AMG-PCG iterations and one V-cycle: start-up + "
-                  f"{full.iterations} x per-iteration time - one V-cycle (oracle hierarchy, setup excluded)")
+        sample = (f"each step one full FP64 AMG-PCG solve from x = 0 to 1e-8 ({full.iterations} iterations; "
+                  "oracle hierarchy built once, setup excluded)")
     ms = sum(times) / len(times)
     line = {
         "impl": "reference", "metric": PLAIN_METRIC[args.workload].format(n=args.n), "value": ms, "unit": "ms",
@@ -422,11 +419,10 @@ def run_reference(args, world, rank):
     """CPU restatement of the reference algorithm (oracle/), all host threads.
 
     The oracle builds its own hierarchy (the same definition as the device
-    one) and runs one untimed full FP64 AMG-PCG solve to 1e-8 for the
-    iteration count. Each step is then a bounded sample (oracle_solve_estimate):
-    the start-up alone and SAMPLE_ITERATIONS iterations, both from x = 0,
-    give start-up + iterations x per-iteration time (less the V-cycle a
-    converged solve skips). The line's value is the mean estimate per solve."""
+    one) once; each step (warm-up and timed) is one full FP64 AMG-PCG solve
+    from x = 0 to 1e-8, timed on the host clock. The line's value is the mean
+    over the timed steps; its config carries the oracle hierarchy's nnz, level
+    count and operator complexity, the same keys as the GPU arm's."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -443,32 +439,26 @@ def run_reference(args, world, rank):
     A, b, _ = P.poisson_3d_variable(args.n, 8.0, 1.0, seed=0)
     Ao = O.Csr.from_matrix(A)
     t0 = time.perf_counter()
-    amg = O.Amg(Ao, O.AmgConfig(max_levels=16, min_coarse_size=4096, smoother=O.SMOOTH_JACOBI, pre_smooth=1,
-                                post_smooth=1, relaxation=2 / 3, coarse_solve=O.COARSE_DENSE, interpolation=2, coarse_order=1))
+    amg = oracle_amg(O, Ao)
     setup_s = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    _, full = O.pcg(Ao, b, precond=O.PRE_AMG, amg=amg, rtol=RTOL, max_it=1000)
-    full_ms = (time.perf_counter() - t0) * 1e3
-    iters = full.iterations
-    sample = min(SAMPLE_ITERATIONS, max(iters, 1))
+    rows, nnz, opc = oracle_hierarchy_stats(amg)
     times = []
     for s in range(args.warmup + args.steps):
-        dt = oracle_solve_estimate(O, Ao, b, amg, iters, sample)
+        dt, _, full = oracle_full_solve(O, Ao, b, amg)
         if s >= args.warmup:
             times.append(dt)
     ms = sum(times) / len(times)
+    cfg = workload_config(args.n)
+    cfg.update(hierarchy_config(nnz[0], len(rows), opc))
     line = {
         "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args.n),
-        "iterations": iters, "termination": full.termination, "setup_s": setup_s, "full_solve_ms": full_ms,
+        "config": cfg, "iterations": full.iterations, "termination": full.termination, "setup_s": setup_s,
         "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "port",
-                         "sample": f"per step the start-up, {sample} FP64 AMG-PCG iterations from x = 0 and one "
-                                   f"V-cycle on the full {args.n}^3 system: start-up + {iters} x per-iteration "
-                                   f"time - one V-cycle, {iters} "
-                                   f"from an untimed full solve ({full_ms:.0f} ms); hierarchy built once by the "
-                                   "oracle, setup excluded"},
+                         "sample": f"each step one full FP64 AMG-PCG solve of the {args.n}^3 system from x = 0 "
+                                   f"to 1e-8 ({full.iterations} iterations; the CPU path has no FP32 inner "
+                                   "solve); hierarchy built once by the oracle, setup excluded"},
         "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -498,7 +488,7 @@ def run_plain(args, world, rank, local):
         pre = cf.AlgebraicMultigrid(A, cf.AMGConfig.pressure_poisson(), ctx=ctx)
         setup_s = time.perf_counter() - t0
         stats = pre.statistics()
-        config.update(amg_levels=int(stats.num_levels), operator_complexity=round(stats.operator_complexity, 3))
+        config.update(hierarchy_config(stats.level_nnz[0], stats.num_levels, stats.operator_complexity))
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     bd = torch.as_tensor(b, device="cuda")
@@ -588,7 +578,11 @@ def run_plain(args, world, rank, local):
             cpu = {"value": (time.perf_counter() - t0) * 1e3 / 5, "unit": "ms", "cores": O.get_threads(),
                    "kind": "port", "sample": "5 full FP64 Jacobi-PCG solves to 1e-8 on the oracle"}
         else:
-            cpu = cpu_baseline_from_hierarchy(pre, A, b, rep.iterations)
+            ctx.set_stream(stream.cuda_stream)
+            rep = solve()  # the FP64 solution (x last held the FP32 solve's)
+            ctx.set_stream(None)
+            parity, cpu = oracle_parity(A, b, pre, x.cpu().numpy(), rep.iterations)
+            extra["oracle_parity"] = parity
 
     if rank == 0:
         line = {
@@ -840,9 +834,11 @@ def main():
     lay = dA.layout()
     spmv_path = {"f32": names[lay["path_f32"]], "f64": names[lay["path_f64"]]}
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_from_hierarchy(amg, A, b, rep64.iterations)
+        x64.zero_()
+        rep64 = solve(x64, cf.Precision.FP64)
+        parity, cpu = oracle_parity(A, b, amg, x64.cpu().numpy(), rep64.iterations)
 
     if rank == 0:
         f32 = spmv["f32"]
@@ -874,54 +870,73 @@ def main():
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+            line["oracle_parity"] = parity
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
 
 
-def cpu_baseline_from_hierarchy(amg, A, b, iterations):
-    """FP64 AMG-PCG of the CPU oracle on the same hierarchy (exported from the
-    device handle): a bounded sample of 2 iterations, extrapolated to the
-    iteration count of the FP64 solve."""
+def oracle_amg(O, Ao):
+    """The oracle's own AMG hierarchy of the 3-D workloads (the device setup's
+    definition: Ruge-Stueben, modified classical interpolation, ascending
+    coarse numbering, V(1,1) damped Jacobi w = 2/3, dense coarsest <= 4096)."""
+    return O.Amg(Ao, O.AmgConfig(max_levels=16, min_coarse_size=4096, smoother=O.SMOOTH_JACOBI, pre_smooth=1,
+                                 post_smooth=1, relaxation=2 / 3, coarse_solve=O.COARSE_DENSE, interpolation=2,
+                                 coarse_order=1))
+
+
+def oracle_hierarchy_stats(amg):
+    """(level rows, level nnz, operator complexity) of an oracle hierarchy."""
+    rows, nnz = [], []
+    for l in range(amg.num_levels):
+        r, _, z = amg.level(l).info()
+        rows.append(int(r))
+        nnz.append(int(z))
+    return rows, nnz, sum(nnz) / nnz[0]
+
+
+def hierarchy_config(nnz, levels, opc):
+    return {"nnz": int(nnz), "amg_levels": int(levels), "operator_complexity": round(float(opc), 3)}
+
+
+def oracle_full_solve(O, Ao, b, amg, rtol=RTOL):
+    """One full FP64 AMG-PCG solve of the oracle from x = 0 to rtol, timed:
+    (ms, solution, report)."""
+    t0 = time.perf_counter()
+    x, rep = O.pcg(Ao, b, precond=O.PRE_AMG, amg=amg, rtol=rtol, max_it=1000)
+    return (time.perf_counter() - t0) * 1e3, x, rep
+
+
+def oracle_parity(A, b, gpu_amg, x_gpu, gpu_iterations, solves=2):
+    """The drop-in check of the plain FP64 path on the full system: the oracle
+    builds its own hierarchy from the same matrix, solves from x = 0 to the same
+    1e-8 relative residual, and the GPU FP64 solution is compared with it.
+    Returns (parity dict, cpu_baseline dict): the CPU figure is the mean of
+    `solves` measured full oracle solves (setup excluded) on all host threads."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     O.build()
-    levels = []
-    for l in range(amg.num_levels):
-        mats = [amg.level(l, 0)]
-        if l + 1 < amg.num_levels:
-            mats += [amg.level(l, 1), amg.level(l, 2)]
-        levels.append([O.Csr.from_matrix(m) for m in mats])
-    oamg = O.Amg.from_levels(levels, O.AmgConfig(max_levels=16, min_coarse_size=4096, smoother=O.SMOOTH_JACOBI,
-                                                 pre_smooth=1, post_smooth=1, relaxation=2 / 3,
-                                                 coarse_solve=O.COARSE_DENSE, interpolation=2, coarse_order=1))
-    Ao = levels[0][0]
-    sample = SAMPLE_ITERATIONS
-    O.pcg(Ao, b, precond=O.PRE_AMG, amg=oamg, rtol=0.0, tol=0.0, max_it=1)  # warm caches
-    ms = oracle_solve_estimate(O, Ao, b, oamg, iterations, sample)
-    return {"value": ms, "unit": "ms", "cores": O.get_threads(), "kind": "port",
-            "sample": f"the start-up, {sample} FP64 AMG-PCG iterations and one V-cycle of the full system on "
-                      f"the oracle, same hierarchy: start-up + {iterations} x per-iteration time - one V-cycle, "
-                      f"{iterations} being the FP64 solve's iteration count (setup excluded)"}
-
-
-def oracle_solve_estimate(O, Ao, b, amg, iterations, sample):
-    """ms of a full oracle AMG-PCG solve from a bounded sample: the start-up
-    alone (initial residual and preconditioner, max_it = 0), `sample`
-    iterations, both from x = 0, and one V-cycle; start-up + iterations x
-    per-iteration time - one V-cycle (a converged solve's last iteration
-    stops before its preconditioner application)."""
+    Ao = O.Csr.from_matrix(A)
     t0 = time.perf_counter()
-    O.pcg(Ao, b, precond=O.PRE_AMG, amg=amg, rtol=0.0, tol=0.0, max_it=0)
-    start = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    O.pcg(Ao, b, precond=O.PRE_AMG, amg=amg, rtol=0.0, tol=0.0, max_it=sample)
-    per_it = max(time.perf_counter() - t0 - start, 0.0) / sample
-    t0 = time.perf_counter()
-    amg.apply(b)
-    vcycle = time.perf_counter() - t0
-    return max(start + iterations * per_it - vcycle, start) * 1e3
+    amg = oracle_amg(O, Ao)
+    setup_s = time.perf_counter() - t0
+    rows, nnz, opc = oracle_hierarchy_stats(amg)
+    st = gpu_amg.statistics()
+    same = rows == [int(v) for v in st.level_sizes] and nnz == [int(v) for v in st.level_nnz]
+    times, xo, rep = [], None, None
+    for _ in range(solves):
+        ms, xo, rep = oracle_full_solve(O, Ao, b, amg)
+        times.append(ms)
+    diff = float(np.linalg.norm(x_gpu - xo) / np.linalg.norm(xo))
+    parity = {"rel_solution_diff_fp64_gpu_vs_oracle": diff, "iterations_gpu": int(gpu_iterations),
+              "iterations_oracle": int(rep.iterations), "oracle_termination": rep.termination,
+              "hierarchy_levels_and_nnz_equal": bool(same), "oracle_setup_s": setup_s,
+              "note": "both FP64 AMG-PCG from x = 0 to rel-res 1e-8; oracle hierarchy built by the oracle"}
+    cpu = {"value": sum(times) / len(times), "unit": "ms", "cores": O.get_threads(), "kind": "port",
+           "sample": f"{solves} full FP64 AMG-PCG solves from x = 0 to 1e-8 on the oracle ({rep.iterations} "
+                     "iterations each; oracle hierarchy built once, setup excluded), all host threads"}
+    return parity, cpu
 
 
 if __name__ == "__main__":

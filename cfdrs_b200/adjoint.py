@@ -20,7 +20,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .device import device_matrix
+from .device import device_matrix, mark_synced
 from .krylov import IterativeSolverConfig, Precision, SolveError, Termination, cg_preconditioned
 from .multigrid import AlgebraicMultigrid, AMGConfig, JacobiPreconditioner
 from .sparse import CsrMatrix
@@ -68,7 +68,8 @@ class SparseSolver:
             raise SolveError("values must be a CUDA float64 tensor with one entry per stored nonzero")
         _lib.check(_lib.load().cfd_csr_set_values_device(self.dm.h, C.c_void_p(v.data_ptr())))
         host = v.cpu().numpy()
-        self.pattern.val[:] = host
+        self.pattern.set_values(host)
+        mark_synced(self.pattern, self.dm)
         self.symmetric = self.pattern_symmetric and bool(
             np.allclose(host, host[self._transpose_pos], rtol=1e-13, atol=0.0))
         if self.kind == "amg":

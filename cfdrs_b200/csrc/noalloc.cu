@@ -33,7 +33,10 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
-unsigned char* g_scratch_addr[kMaxDevices] = {};  // device address of g_noalloc_scratch, per device
+// Device address of g_noalloc_scratch, per device, looked up once and kept for
+// the life of the process: stale after a cudaDeviceReset of that device, after
+// which the entry point must not be used there (documented in cfdgpu.h).
+unsigned char* g_scratch_addr[kMaxDevices] = {};
 
 __global__ void __launch_bounds__(kThreads) k_residual_norm_noalloc(int nrows, const int* __restrict__ rp,
                                                                     const int* __restrict__ col,

@@ -83,6 +83,7 @@ class DeviceCsr:
         _lib.check(_lib.load().cfd_csr_create_i32(self.ctx.h, m.nrows, m.ncols, m.nnz, _ptr(rp), _ptr(col),
                                                   _ptr(val), C.byref(h)))
         self.h = h
+        self.version = getattr(m, "version", 0)  # host value version this copy holds
 
     def update_values(self, values) -> None:
         v = np.ascontiguousarray(values, dtype=np.float64)
@@ -139,11 +140,30 @@ _uploads: "weakref.WeakKeyDictionary[CsrMatrix, DeviceCsr]" = weakref.WeakKeyDic
 
 
 def device_matrix(m, ctx: Context | None = None) -> DeviceCsr:
-    """Upload ``m`` once and reuse the device copy while ``m`` is alive."""
+    """Upload ``m`` once and reuse the device copy while ``m`` is alive; values
+    changed since the upload (``CsrMatrix.set_values``) are copied to the
+    device first, with the pattern's layout kept."""
     if isinstance(m, DeviceCsr):
         return m
     d = _uploads.get(m)
     if d is None or (ctx is not None and d.ctx is not ctx):
         d = DeviceCsr(m, ctx)
         _uploads[m] = d
+    elif d.version != getattr(m, "version", 0):
+        d.update_values(m.val)
+        d.version = m.version
     return d
+
+
+def mark_synced(m, d: DeviceCsr) -> None:
+    """Record that ``d`` already holds ``m``'s current values (written on the
+    device by the caller), so no upload follows."""
+    d.version = m.version
+
+
+def refresh_device_values(m) -> None:
+    """Copy ``m``'s current values to its device copy, if it has one."""
+    d = _uploads.get(m) if isinstance(m, CsrMatrix) else None
+    if d is not None:
+        d.update_values(m.val)
+        d.version = m.version

@@ -20,6 +20,7 @@ import numpy as np
 
 from . import _lib
 from . import krylov as K
+from .device import refresh_device_values
 
 AMG_SETUP_MATRIX_SIZE_LIMIT = 10_000
 
@@ -57,6 +58,7 @@ class PressureCorrectionDispatch:
         self.linear_solver_config = config or K.IterativeSolverConfig(1e-10, 0.0, 1000)
         self.amg = None
         self.amg_values = None
+        self.solved_values = None
         self.recomputes = 0
         self.last_outcome: K.SolveOutcome | None = None
 
@@ -80,6 +82,12 @@ class PressureCorrectionDispatch:
         """Solves into ``solution`` (a host array or CUDA tensor) and returns
         the final outcome."""
         values = np.asarray(matrix.val)
+        if self.solved_values is not None and not np.array_equal(self.solved_values, values):
+            # values written into the matrix's array since the last call (also
+            # directly, bypassing CsrMatrix.set_values): push them to the
+            # device copy that the recompute and the solve read
+            refresh_device_values(matrix)
+        self.solved_values = values.copy()
         unchanged = (self.amg is not None and self.amg_values is not None
                      and np.array_equal(self.amg_values, values))
         allowed = matrix.shape[0] < AMG_SETUP_MATRIX_SIZE_LIMIT
@@ -87,7 +95,9 @@ class PressureCorrectionDispatch:
             if self.amg is None:
                 try:
                     self.amg = self._new_amg(matrix)
-                except (K.SolveError, _lib.CfdError):
+                except (K.SolveError, _lib.CfdError, ValueError):
+                    # the reference keeps going without AMG on any Err of
+                    # AlgebraicMultigrid::new (`if let Ok(amg)`, correction.rs:63-80)
                     self.amg = None
             else:
                 self.amg.recompute(matrix)  # an error here propagates, as the reference's `?` does

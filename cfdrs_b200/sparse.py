@@ -17,17 +17,44 @@ class SparseError(ValueError):
 
 
 class CsrMatrix:
-    __slots__ = ("row_ptr", "col", "val", "shape", "__weakref__")
+    """CSR matrix. ``val`` is a read-only view: values change through
+    :meth:`set_values`, which bumps :attr:`version` so that a device copy made
+    earlier (``device.device_matrix``) is refreshed before its next use. The
+    reference reads ``matrix.values()`` on every call, so a solve after a value
+    change always sees the new values; a stale device copy would not."""
+
+    __slots__ = ("row_ptr", "col", "_val", "shape", "version", "__weakref__")
 
     def __init__(self, row_ptr, col, val, shape):
         self.row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
         self.col = np.ascontiguousarray(col, dtype=np.int32)
-        self.val = np.ascontiguousarray(val, dtype=np.float64)
+        v = np.ascontiguousarray(val, dtype=np.float64).view()
+        v.flags.writeable = False
+        self._val = v
+        self.version = 0
         self.shape = (int(shape[0]), int(shape[1]))
         if self.row_ptr.shape[0] != self.shape[0] + 1:
             raise SparseError("row_ptr length must be nrows + 1")
-        if self.col.shape[0] != self.val.shape[0] or self.row_ptr[-1] != self.col.shape[0]:
+        if self.col.shape[0] != self._val.shape[0] or self.row_ptr[-1] != self.col.shape[0]:
             raise SparseError("col/val length must equal row_ptr[-1]")
+
+    @property
+    def val(self) -> np.ndarray:
+        """The stored values (read-only view; see :meth:`set_values`)."""
+        return self._val
+
+    def set_values(self, values) -> None:
+        """Replace the values (same pattern; the matrix keeps its own copy) and
+        bump ``version`` (``values_mut()`` of the reference's CsrMatrix). The
+        constructor keeps the caller's value array by reference, so values
+        written into that array directly are not seen as a change."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        if v.shape != self._val.shape:
+            raise SparseError("value array must match the pattern's nnz")
+        w = v.copy()
+        w.flags.writeable = False
+        self._val = w
+        self.version += 1
 
     @classmethod
     def from_parts(cls, values, col_indices, row_ptr, nrows, ncols):

@@ -421,7 +421,10 @@ cfd_status cfd_selftest_wait_timeout(cfd_context* ctx, int32_t tries);
  * larger inputs return CFD_ERR_DIM. The first call on a device looks up the
  * array's device address (set-up) and should come before any stream capture.
  * All calls share the array, so calls that overlap on the GPU (other streams,
- * other threads) race; serialize them. */
+ * other threads) race; serialize them. The looked-up address is kept for the
+ * life of the process: do not use this entry point on a device after
+ * cudaDeviceReset (the library's module, and with it the array, may then sit
+ * at another address). */
 cfd_status cfd_residual_norm_noalloc(int64_t nrows, int64_t ncols, const int32_t* row_ptr,
                                      const int32_t* col, const double* val, const double* x,
                                      const double* b, double* r, double* norm2, void* cuda_stream);

@@ -98,3 +98,40 @@ def central_fd(theta: np.ndarray, column: int, cells, h: float = 1e-6):
         tm[j, i] -= h
         out.append((loss(tp, column) - loss(tm, column)) / (2.0 * h))
     return np.array(out)
+
+
+def central_fd_lowrank(theta: np.ndarray, column: int, cells, h: float = 1e-6):
+    """The same central differences as central_fd, with every perturbed system
+    solved from ONE sparse LU of the unperturbed A: perturbing theta at one
+    cell changes A only on the rows and columns S of that cell and its (at
+    most 4) neighbours, A' = A + E_S M E_S^T with M = (A' - A)[S, S], so by the
+    Woodbury identity
+        A'^-1 b' = y - Z M (I + Z_S M)^-1 y_S,  y = A^-1 b',  Z = A^-1 E_S,
+    (Z_S, y_S: the rows S of Z and y). Exact algebra, |S| + 2 triangular solve
+    pairs per cell instead of two factorizations."""
+    n = theta.shape[0]
+    A, b = assemble(theta)
+    lu = spla.splu(A.tocsc())
+    out = []
+    for (j, i) in cells:
+        S = [j * n + i]
+        for dj, di in ((-1, 0), (1, 0), (0, -1), (0, 1)):
+            jj, ii = j + dj, i + di
+            if 0 <= jj < n and 0 <= ii < n:
+                S.append(jj * n + ii)
+        S = np.array(S)
+        E = np.zeros((n * n, S.size))
+        E[S, np.arange(S.size)] = 1.0
+        Z = lu.solve(E)
+        vals = []
+        for sgn in (1.0, -1.0):
+            t = theta.copy()
+            t[j, i] += sgn * h
+            A2, b2 = assemble(t)
+            M = (A2 - A)[S][:, S].toarray()
+            y = lu.solve(b2)
+            K = np.eye(S.size) + Z[S, :] @ M
+            p = y - Z @ (M @ np.linalg.solve(K, y[S]))
+            vals.append(float((p.reshape(n, n)[:, column] ** 2).sum()))
+        out.append((vals[0] - vals[1]) / (2.0 * h))
+    return np.array(out)

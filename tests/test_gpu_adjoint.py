@@ -86,10 +86,12 @@ def test_darcy_512_gradient_vs_cpu_adjoint_and_fd(cuda):
     """The adjoint workload at full size (512^2 cells, theta GRF l = 16,
     sigma = 0.5, forward and adjoint FP32 + FP64 refinement to 1e-10): the
     device gradient against the FP64 CPU adjoint, and both against central
-    differences (h = 1e-6, FP64 sparse direct solves) on the first 8 of the 64
-    seeded cells (two direct solves of 262 144 unknowns per cell). At
-    kappa ~ 1e6 the differences carry noise near 3e-4 max|g| for either
-    gradient, which bounds the FD check."""
+    differences (h = 1e-6, FP64) on the 64 seeded cells of the configuration.
+    Every perturbed system is solved from one sparse LU of the unperturbed
+    matrix by the Woodbury identity (adjoint_cpu.central_fd_lowrank): exact
+    algebra, and the rounding of a single factorization cancels in the
+    difference, so the FD noise is about 1.5e-5 max|g| at kappa ~ 1e6 instead
+    of the 3e-4 of two independent factorizations per cell."""
     torch = cuda
     import adjoint_cpu as AC
     import cfdrs_b200 as cf
@@ -110,10 +112,10 @@ def test_darcy_512_gradient_vs_cpu_adjoint_and_fd(cuda):
     assert abs(L.item() - L_cpu) <= 1e-9 * abs(L_cpu)
     assert np.linalg.norm(g - g_cpu) <= 1e-8 * np.linalg.norm(g_cpu)
     rng = np.random.default_rng(64)
-    cells = [(int(j), int(i)) for j, i in rng.integers(0, n, size=(64, 2))][:8]
-    fd = AC.central_fd(theta, col, cells, h=1e-6)
+    cells = [(int(j), int(i)) for j, i in rng.integers(0, n, size=(64, 2))]
+    fd = AC.central_fd_lowrank(theta, col, cells, h=1e-6)
     ga = np.array([g[j, i] for j, i in cells])
     gc = np.array([g_cpu[j, i] for j, i in cells])
     scale = np.abs(g_cpu).max()
-    assert np.abs(ga - fd).max() <= 1e-3 * scale
-    assert np.abs(ga - fd).max() <= 2.0 * np.abs(gc - fd).max() + 1e-12 * scale  # no worse than the CPU adjoint
+    assert np.abs(ga - fd).max() <= 1e-4 * scale
+    assert np.abs(ga - fd).max() <= 2.0 * np.abs(gc - fd).max() + 1e-9 * scale  # no worse than the CPU adjoint

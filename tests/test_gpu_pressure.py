@@ -43,3 +43,50 @@ def test_dispatch_above_the_limit_runs_without_amg(cuda):
     out = d.dispatch_solve(A, b, x)
     assert d.amg is None and out.kind in (SolveOutcome.CONVERGED, SolveOutcome.STALLED)
     assert np.linalg.norm(x) > 0  # a stalled solve keeps its last iterate
+
+
+def test_dispatch_sees_values_changed_in_place(cuda):
+    """A SIMPLE loop reuses one matrix and changes its values between calls:
+    the recompute and the solve must read the new values, whether they came in
+    through CsrMatrix.set_values or were written into the caller's own array."""
+    import scipy.sparse.linalg as spla
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.pressure import PressureCorrectionDispatch
+    from cfdrs_b200.sparse import CsrMatrix
+    A0, b = P.poisson_2d_dirichlet(48)
+    own = np.array(A0.val)  # the caller's value array, held by reference
+    A = CsrMatrix(A0.row_ptr, A0.col, own, A0.shape)
+    d = PressureCorrectionDispatch(config=cf.IterativeSolverConfig(0.0, 1e-10, 2000))
+    x = np.zeros(A.shape[0])
+    assert d.dispatch_solve(A, b, x).converged()
+    rng = np.random.default_rng(3)
+    for scale_rows, direct in ((rng.uniform(0.5, 2.0, A.shape[0]), False), (rng.uniform(0.5, 2.0, A.shape[0]), True)):
+        S = A0.to_scipy()
+        Dh = np.sqrt(scale_rows)
+        new = (S.multiply(Dh[:, None]).multiply(Dh[None, :])).tocsr()  # stays SPD, same pattern
+        new.sort_indices()
+        if direct:
+            own[:] = new.data
+        else:
+            A.set_values(new.data)
+        x = np.zeros(A.shape[0])
+        assert d.dispatch_solve(A, b, x).converged()
+        x_ref = spla.spsolve(new.tocsc(), b)
+        assert np.linalg.norm(x - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
+    assert d.recomputes == 2
+
+
+def test_solve_after_set_values_uses_the_new_values(cuda):
+    import scipy.sparse.linalg as spla
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    A, b = P.poisson_2d_dirichlet(40)
+    x = np.zeros(A.shape[0])
+    cfg = cf.IterativeSolverConfig(0.0, 1e-12, 4000)
+    assert cf.cg_preconditioned(A, b, cf.JacobiPreconditioner(A), x, cfg).termination == cf.Termination.CONVERGED
+    A.set_values(3.0 * np.asarray(A.val))
+    x = np.zeros(A.shape[0])
+    assert cf.cg_preconditioned(A, b, cf.JacobiPreconditioner(A), x, cfg).termination == cf.Termination.CONVERGED
+    x_ref = spla.spsolve(A.to_scipy().tocsc(), b)
+    assert np.linalg.norm(x - x_ref) <= 1e-9 * np.linalg.norm(x_ref)

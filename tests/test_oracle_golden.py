@@ -273,6 +273,10 @@ def test_cpu_adjoint_against_fd_and_assembly():
     fd = AC.central_fd(theta, col, cells)
     ga = np.array([g[j, i] for j, i in cells])
     assert np.abs(ga - fd).max() <= 1e-6 * np.abs(g).max()
+    # the Woodbury route to the same differences (corner, wall and interior cells)
+    fd_lr = AC.central_fd_lowrank(theta, col, cells)
+    assert np.abs(fd_lr - fd).max() <= 1e-6 * np.abs(g).max()
+    assert np.abs(ga - fd_lr).max() <= 1e-7 * np.abs(g).max()
 
 
 def _entries_csr(n, entries):

@@ -99,3 +99,15 @@ def test_breakdown_without_amg_is_not_retried():
     d = Stub([T.BREAKDOWN], amg_fails=True)
     out = d.dispatch_solve(matrix(8), np.ones(8), np.zeros(8))
     assert len(d.calls) == 1 and out.kind == K.SolveOutcome.BROKEN_DOWN
+
+
+def test_csr_values_are_read_only_and_set_values_bumps_the_version():
+    from helpers import tridiag
+    A = tridiag(5)
+    with pytest.raises(ValueError):
+        A.val[0] = 7.0
+    v0 = A.version
+    A.set_values(2.0 * np.asarray(A.val))
+    assert A.version == v0 + 1 and np.array_equal(A.val, 2.0 * tridiag(5).val)
+    with pytest.raises(ValueError):
+        A.set_values(np.ones(3))
