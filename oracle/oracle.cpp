@@ -1421,4 +1421,277 @@ int or_network_assemble(int64_t n, int64_t m, const int64_t* ei, const int64_t* 
   return 0;
 }
 
+// ---- the 1-D network solve (LinearSystemSolver, crates/cfd-1d/src/solver/core/linear_system.rs) ----
+
+// NetworkSolver::detect_solver_method (solver_detection.rs:36-64): CG when
+// every off-diagonal is <= 0 and every row has diag >= sum |off| and diag > 0
+// (identity Dirichlet rows exempt), the sum taken in column order; else
+// BiCGSTAB.
+int or_detect_solver_method(const or_csr* a) {
+  for (int64_t i = 0; i < a->nrows; ++i) {
+    double diag = 0.0, sum_off = 0.0;
+    for (int64_t k = a->rp[i]; k < a->rp[i + 1]; ++k) {
+      const double v = a->v[k];
+      if (a->ci[k] == i) {
+        diag = v;
+      } else if (v > 0.0) {
+        return OR_LS_BICGSTAB;
+      } else {
+        sum_off += std::fabs(v);
+      }
+    }
+    const bool identity_dirichlet = diag == 1.0 && sum_off == 0.0;
+    if ((diag < sum_off || diag <= 0.0) && !identity_dirichlet) return OR_LS_BICGSTAB;
+  }
+  return OR_LS_CG;
+}
+
+// Dense LU with partial pivoting (right-looking Doolittle; the pivot is the
+// first row of largest |a_ik| at or below the diagonal), forward elimination
+// carried on b, then back substitution; the restated lu_decompose + solve of
+// linear_system.rs:248-256 (leto_ops, not vendored).
+int or_dense_lu_solve(int64_t n, double* m, double* b) {
+  for (int64_t k = 0; k < n; ++k) {
+    int64_t p = k;
+    double best = std::fabs(m[k * n + k]);
+    for (int64_t i = k + 1; i < n; ++i) {
+      const double v = std::fabs(m[i * n + k]);
+      if (v > best) {
+        best = v;
+        p = i;
+      }
+    }
+    if (!(best > 0.0) || !std::isfinite(best)) return -1;
+    if (p != k) {
+      for (int64_t j = 0; j < n; ++j) std::swap(m[k * n + j], m[p * n + j]);
+      std::swap(b[k], b[p]);
+    }
+    const double piv = m[k * n + k];
+    for (int64_t i = k + 1; i < n; ++i) {
+      const double l = m[i * n + k] / piv;
+      m[i * n + k] = l;
+      if (l == 0.0) continue;
+      for (int64_t j = k + 1; j < n; ++j) m[i * n + j] -= l * m[k * n + j];
+      b[i] -= l * b[k];
+    }
+  }
+  for (int64_t i = n - 1; i >= 0; --i) {
+    double t = b[i];
+    for (int64_t j = i + 1; j < n; ++j) t -= m[i * n + j] * b[j];
+    b[i] = t / m[i * n + i];
+  }
+  return 0;
+}
+
+namespace {
+
+// 1 / max_j |a_ij| of row i, 1 where the maximum is not above f64::EPSILON or
+// not finite (row_equilibrated_system, linear_system.rs:157-186).
+double ls_row_scale(const or_csr& a, int64_t i) {
+  double mx = 0.0;
+  for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k) mx = std::max(mx, std::fabs(a.v[k]));
+  return (mx > DBL_EPSILON && std::isfinite(mx)) ? 1.0 / mx : 1.0;
+}
+
+// ||D (A x - b)|| / ||D b|| (or ||D (A x - b)|| when ||D b|| <= f64::EPSILON):
+// compute_equilibrated_residual_norm / _rhs_norm (linear_system.rs:206-246).
+double ls_target_ratio(const or_csr& a, const double* x, const double* b, bool* meets, double tol) {
+  double r2 = 0.0, b2 = 0.0;
+  for (int64_t i = 0; i < a.nrows; ++i) {
+    double ax = 0.0;
+    for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k) ax += a.v[k] * x[a.ci[k]];
+    const double s = ls_row_scale(a, i);
+    const double r = (ax - b[i]) * s;
+    r2 += r * r;
+    const double bb = b[i] * s;
+    b2 += bb * bb;
+  }
+  const double rn = std::sqrt(r2), bn = std::sqrt(b2);
+  if (!std::isfinite(rn)) {
+    *meets = false;
+    return rn;
+  }
+  const double ratio = bn > DBL_EPSILON ? rn / bn : rn;
+  *meets = ratio <= tol;
+  return ratio;
+}
+
+int ls_dense(const or_csr& a, const double* b, double* x) {
+  const int64_t n = a.nrows;
+  std::vector<double> m((size_t)(n * n), 0.0), rhs(b, b + n);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k) m[i * n + a.ci[k]] += a.v[k];
+  if (or_dense_lu_solve(n, m.data(), rhs.data()) != 0) return -1;
+  std::copy(rhs.begin(), rhs.end(), x);
+  return 0;
+}
+
+double ls_dot(int64_t n, const double* u, const double* v) {
+  double t = 0.0;
+  for (int64_t i = 0; i < n; ++i) t += u[i] * v[i];
+  return t;
+}
+
+void ls_spmv(const or_csr& a, const double* x, double* y) {
+  for (int64_t i = 0; i < a.nrows; ++i) {
+    double t = 0.0;
+    for (int64_t k = a.rp[i]; k < a.rp[i + 1]; ++k) t += a.v[k] * x[a.ci[k]];
+    y[i] = t;
+  }
+}
+
+// Jacobi-PCG, the recurrence of or_pcg (serial: one network per thread, as
+// the caller's parallel candidate loop runs them).
+int ls_pcg(const or_csr& a, const std::vector<double>& inv, const double* b, double* x, double tol, int64_t max_it,
+           int64_t* iters) {
+  const int64_t n = a.nrows;
+  std::vector<double> r(n), z(n), p(n), q(n);
+  ls_spmv(a, x, q.data());
+  for (int64_t i = 0; i < n; ++i) r[i] = b[i] - q[i];
+  double rn = std::sqrt(ls_dot(n, r.data(), r.data()));
+  *iters = 0;
+  if (rn <= tol) return OR_TERM_INITIAL_RESIDUAL;
+  for (int64_t i = 0; i < n; ++i) z[i] = r[i] * inv[i];
+  double rho = ls_dot(n, r.data(), z.data());
+  p = z;
+  for (int64_t it = 1; it <= max_it; ++it) {
+    ls_spmv(a, p.data(), q.data());
+    const double pq = ls_dot(n, p.data(), q.data());
+    if (!(pq > 0.0)) return OR_TERM_NON_POSITIVE_CURVATURE;
+    const double alpha = rho / pq;
+    for (int64_t i = 0; i < n; ++i) {
+      x[i] += alpha * p[i];
+      r[i] -= alpha * q[i];
+    }
+    *iters = it;
+    rn = std::sqrt(ls_dot(n, r.data(), r.data()));
+    if (!std::isfinite(rn)) return OR_TERM_BREAKDOWN;
+    if (rn <= tol) return OR_TERM_CONVERGED;
+    for (int64_t i = 0; i < n; ++i) z[i] = r[i] * inv[i];
+    const double rz = ls_dot(n, r.data(), z.data());
+    if (rz == 0.0 || !std::isfinite(rz)) return OR_TERM_BREAKDOWN;
+    const double beta = rz / rho;
+    for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+    rho = rz;
+  }
+  return OR_TERM_MAX_ITERATIONS;
+}
+
+// Jacobi-preconditioned BiCGSTAB, the recurrence of or_bicgstab (serial).
+int ls_bicgstab(const or_csr& a, const std::vector<double>& inv, const double* b, double* x, double tol,
+                int64_t max_it, int64_t* iters) {
+  const int64_t n = a.nrows;
+  std::vector<double> r(n), rh(n), p(n, 0.0), v(n, 0.0), ph(n), s(n), sh(n), t(n);
+  ls_spmv(a, x, t.data());
+  for (int64_t i = 0; i < n; ++i) r[i] = b[i] - t[i];
+  rh = r;
+  double rn = std::sqrt(ls_dot(n, r.data(), r.data()));
+  *iters = 0;
+  if (rn <= tol) return OR_TERM_INITIAL_RESIDUAL;
+  double rho = 1.0, alpha = 1.0, omega = 1.0;
+  for (int64_t it = 1; it <= max_it; ++it) {
+    const double rho_new = ls_dot(n, rh.data(), r.data());
+    if (rho_new == 0.0 || !std::isfinite(rho_new)) return OR_TERM_BREAKDOWN;
+    if (it == 1) {
+      p = r;
+    } else {
+      const double beta = (rho_new / rho) * (alpha / omega);
+      for (int64_t i = 0; i < n; ++i) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+    }
+    for (int64_t i = 0; i < n; ++i) ph[i] = p[i] * inv[i];
+    ls_spmv(a, ph.data(), v.data());
+    const double rv = ls_dot(n, rh.data(), v.data());
+    if (rv == 0.0 || !std::isfinite(rv)) return OR_TERM_BREAKDOWN;
+    alpha = rho_new / rv;
+    // x takes alpha * p^ at once (the half step), then omega * s^ below: the
+    // two updates of Saad's x += alpha p^ + omega s^ applied one after the
+    // other, so that p^ and s^ can share storage on the device.
+    for (int64_t i = 0; i < n; ++i) {
+      s[i] = r[i] - alpha * v[i];
+      x[i] += alpha * ph[i];
+    }
+    const double sn = std::sqrt(ls_dot(n, s.data(), s.data()));
+    *iters = it;
+    if (sn <= tol) return OR_TERM_CONVERGED;
+    for (int64_t i = 0; i < n; ++i) sh[i] = s[i] * inv[i];
+    ls_spmv(a, sh.data(), t.data());
+    const double tt = ls_dot(n, t.data(), t.data());
+    if (tt == 0.0 || !std::isfinite(tt)) return OR_TERM_BREAKDOWN;
+    omega = ls_dot(n, t.data(), s.data()) / tt;
+    for (int64_t i = 0; i < n; ++i) {
+      x[i] += omega * sh[i];
+      r[i] = s[i] - omega * t[i];
+    }
+    rn = std::sqrt(ls_dot(n, r.data(), r.data()));
+    if (!std::isfinite(rn)) return OR_TERM_BREAKDOWN;
+    if (rn <= tol) return OR_TERM_CONVERGED;
+    if (omega == 0.0) return OR_TERM_BREAKDOWN;
+    rho = rho_new;
+  }
+  return OR_TERM_MAX_ITERATIONS;
+}
+
+}  // namespace
+
+int or_linear_system_solve(const or_csr* a, const double* b, double* x, int method, double tolerance,
+                           int64_t max_iterations, or_ls_report* rep) {
+  const int64_t n = a->nrows;
+  if (a->ncols != n) return -1;
+  *rep = or_ls_report{};
+  rep->method = method == OR_LS_DETECT ? or_detect_solver_method(a) : method;
+  rep->termination = -1;
+  // Row-equilibrated copy (D A, D b).
+  or_csr sa = *a;
+  std::vector<double> sb(n);
+  for (int64_t i = 0; i < n; ++i) {
+    const double s = ls_row_scale(*a, i);
+    for (int64_t k = sa.rp[i]; k < sa.rp[i + 1]; ++k) sa.v[k] *= s;
+    sb[i] = b[i] * s;
+  }
+  bool meets = false;
+  if (n <= 256) {
+    std::vector<double> xd(n);
+    if (ls_dense(sa, sb.data(), xd.data()) == 0) {
+      rep->residual = ls_target_ratio(*a, xd.data(), b, &meets, tolerance);
+      if (meets) {
+        std::copy(xd.begin(), xd.end(), x);
+        rep->path = OR_LS_PATH_DIRECT;
+        return 0;
+      }
+    }
+    rep->path = OR_LS_PATH_DIRECT_UNSCALED;
+  } else {
+    std::vector<double> inv(n, 1.0);
+    for (int64_t i = 0; i < n; ++i) {
+      const double d = csr_value(sa, i, i);
+      if (!std::isfinite(d)) {
+        rep->path = OR_LS_PATH_ERROR;
+        return 0;
+      }
+      inv[i] = std::fabs(d) <= DBL_EPSILON ? 1.0 : 1.0 / d;
+    }
+    int64_t it = 0;
+    rep->termination = rep->method == OR_LS_CG ? ls_pcg(sa, inv, sb.data(), x, tolerance, max_iterations, &it)
+                                               : ls_bicgstab(sa, inv, sb.data(), x, tolerance, max_iterations, &it);
+    rep->iterations = it;
+    const bool converged = rep->termination == OR_TERM_CONVERGED || rep->termination == OR_TERM_INITIAL_RESIDUAL;
+    if (converged) {
+      rep->residual = ls_target_ratio(*a, x, b, &meets, tolerance);
+      if (meets) {
+        rep->path = OR_LS_PATH_KRYLOV;
+        return 0;
+      }
+    }
+    rep->path = OR_LS_PATH_KRYLOV_FALLBACK;
+  }
+  std::vector<double> xd(n);
+  if (ls_dense(*a, b, xd.data()) != 0) {
+    rep->path = OR_LS_PATH_FAILED;
+    return 0;
+  }
+  std::copy(xd.begin(), xd.end(), x);
+  rep->residual = ls_target_ratio(*a, x, b, &meets, tolerance);
+  return 0;
+}
+
 }  // extern "C"

@@ -148,6 +148,49 @@ void or_block_diagonal_apply(const or_simple* s, const double* b, double* x);
 int or_gmres_saddle(const or_csr* a, const or_simple* simple, int precond, int64_t restart, const double* b,
                     double* x, const or_solver_config* cfg, or_report* rep, double* history);
 
+/* The 1-D network solve, LinearSystemSolver::solve_with_initial_guess
+ * (crates/cfd-1d/src/solver/core/linear_system.rs:114-155) with the method of
+ * NetworkSolver::detect_solver_method (solver_detection.rs:36-64):
+ *   - rows equilibrated by 1 / max_j |a_ij| (identity where that maximum is not
+ *     above f64::EPSILON or not finite, :157-186);
+ *   - n <= 256: dense LU of the equilibrated system, kept if it meets the
+ *     residual target on the original system (:188-204), else dense LU of
+ *     the original system (:124-130);
+ *   - n > 256: CG or BiCGSTAB on the equilibrated system with DiagJacobi of
+ *     it, IterativeSolverConfig::new(tol) (absolute tolerance tol on the
+ *     2-norm of its residual, max_iterations), x in as the initial guess; kept
+ *     if converged and the residual target holds, else dense LU of the
+ *     original system (:131-155).
+ * Dense LU: partial pivoting (first largest |a_ik| in row order), fails on a
+ * zero or non-finite pivot; the reference then tries a QR least-squares solve
+ * (:248-267), which is not restated: the system is reported failed. */
+enum { OR_LS_CG = 0, OR_LS_BICGSTAB = 1, OR_LS_DETECT = 2 };
+enum {
+  OR_LS_PATH_KRYLOV = 0,          /* the Krylov solution was kept */
+  OR_LS_PATH_DIRECT = 1,          /* dense LU of the equilibrated system */
+  OR_LS_PATH_DIRECT_UNSCALED = 2, /* dense LU of the original system after the first missed the target */
+  OR_LS_PATH_KRYLOV_FALLBACK = 3, /* dense LU of the original system after the Krylov solve */
+  OR_LS_PATH_FAILED = 4,          /* the last dense LU met a zero pivot */
+  OR_LS_PATH_ERROR = 5            /* DiagJacobi::new refused a non-finite diagonal (an Err) */
+};
+typedef struct {
+  int32_t method;       /* OR_LS_CG or OR_LS_BICGSTAB (the detected one under OR_LS_DETECT) */
+  int32_t path;         /* OR_LS_PATH_* */
+  int32_t termination;  /* of the Krylov solve (OR_TERM_*), -1 when none ran */
+  int32_t pad;
+  int64_t iterations;   /* Krylov iterations */
+  double residual;      /* ||D (A x - b)|| / ||D b|| of the returned x (the target test's ratio) */
+} or_ls_report;
+/* NetworkSolver::detect_solver_method: OR_LS_CG or OR_LS_BICGSTAB. */
+int or_detect_solver_method(const or_csr* a);
+/* Dense LU with partial pivoting of the row-major n x n matrix m (overwritten),
+ * solving m x = b in place of b. 0, or -1 on a zero or non-finite pivot. */
+int or_dense_lu_solve(int64_t n, double* m, double* b);
+/* x holds the initial guess in and the solution out. Returns 0, or -1 for a
+ * non-square matrix. */
+int or_linear_system_solve(const or_csr* a, const double* b, double* x, int method, double tolerance,
+                           int64_t max_iterations, or_ls_report* rep);
+
 /* MatrixAssembler::assemble_into for one network (crates/cfd-1d/src/solver/core/
  * matrix_assembly.rs:163-250). Nodes 0..n-1, edges (ei[e], ej[e]) with
  * conductance g[e]; fixed[k] != 0 marks a Dirichlet node of pressure

@@ -112,6 +112,12 @@ def lib():
         L.or_block_diagonal_apply.argtypes = [P, P, P]
         L.or_gmres_saddle.restype = C.c_int
         L.or_gmres_saddle.argtypes = [P, P, C.c_int, C.c_int64, P, P, P, P, P]
+        L.or_detect_solver_method.restype = C.c_int
+        L.or_detect_solver_method.argtypes = [P]
+        L.or_dense_lu_solve.restype = C.c_int
+        L.or_dense_lu_solve.argtypes = [I64, P, P]
+        L.or_linear_system_solve.restype = C.c_int
+        L.or_linear_system_solve.argtypes = [P, P, P, C.c_int, D, I64, P]
         L.or_network_assemble.restype = C.c_int
         L.or_network_assemble.argtypes = [I64, I64, P, P, P, P, P, P, P, P, P]
         _lib = L
@@ -344,6 +350,48 @@ def pcg_equilibrated(a: Csr, b, x0=None, tol=0.0, rtol=1e-10, max_it=20000):
         raise ValueError(f"oracle solve setup failed ({rc})")
     return x, Report(TERMINATIONS[rep.termination], rep.iterations, rep.initial_residual, rep.final_residual,
                      rep.threshold, np.zeros(0))
+
+
+LS_CG, LS_BICGSTAB, LS_DETECT = 0, 1, 2
+LS_PATHS = ["krylov", "direct", "direct_unscaled", "krylov_fallback", "failed", "error"]
+
+
+class _LsReport(C.Structure):
+    _fields_ = [("method", C.c_int32), ("path", C.c_int32), ("termination", C.c_int32), ("pad", C.c_int32),
+                ("iterations", C.c_int64), ("residual", C.c_double)]
+
+
+@dataclass
+class LsReport:
+    method: int       # LS_CG or LS_BICGSTAB
+    path: str         # one of LS_PATHS
+    termination: str  # of the Krylov solve, "" when none ran
+    iterations: int
+    residual: float   # ||D (A x - b)|| / ||D b||
+
+
+def detect_solver_method(a: Csr) -> int:
+    """NetworkSolver::detect_solver_method: LS_CG or LS_BICGSTAB."""
+    return lib().or_detect_solver_method(a.h)
+
+
+def dense_lu_solve(m: np.ndarray, b):
+    """Dense LU with partial pivoting; None on a zero pivot."""
+    mm = np.array(m, dtype=np.float64, order="C")
+    bb = np.array(b, dtype=np.float64)
+    return bb if lib().or_dense_lu_solve(mm.shape[0], _ptr(mm), _ptr(bb)) == 0 else None
+
+
+def linear_system_solve(a: Csr, b, x0=None, method=LS_DETECT, tolerance=1e-10, max_iterations=20000):
+    """LinearSystemSolver::solve_with_initial_guess of the 1-D network solver."""
+    n = a.info()[0]
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    rep = _LsReport()
+    if lib().or_linear_system_solve(a.h, _ptr(b), _ptr(x), method, tolerance, max_iterations, C.byref(rep)) != 0:
+        raise ValueError("linear_system_solve: matrix is not square")
+    term = TERMINATIONS[rep.termination] if rep.termination >= 0 else ""
+    return x, LsReport(rep.method, LS_PATHS[rep.path], term, rep.iterations, rep.residual)
 
 
 def set_threads(n: int):

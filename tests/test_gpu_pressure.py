@@ -61,12 +61,15 @@ def test_dispatch_sees_values_changed_in_place(cuda):
     x = np.zeros(A.shape[0])
     assert d.dispatch_solve(A, b, x).converged()
     rng = np.random.default_rng(3)
-    for scale_rows, direct in ((rng.uniform(0.5, 2.0, A.shape[0]), False), (rng.uniform(0.5, 2.0, A.shape[0]), True)):
+    # the direct write first: set_values gives the matrix its own copy, after
+    # which the caller's array is no longer the matrix's
+    for scale_rows, direct in ((rng.uniform(0.5, 2.0, A.shape[0]), True), (rng.uniform(0.5, 2.0, A.shape[0]), False)):
         S = A0.to_scipy()
         Dh = np.sqrt(scale_rows)
         new = (S.multiply(Dh[:, None]).multiply(Dh[None, :])).tocsr()  # stays SPD, same pattern
         new.sort_indices()
         if direct:
+            assert np.shares_memory(A.val, own)
             own[:] = new.data
         else:
             A.set_values(new.data)
