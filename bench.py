@@ -20,6 +20,7 @@ independent replicas and reports the slowest.
 from __future__ import annotations
 
 import argparse
+import collections
 import ctypes as C
 import json
 import os
@@ -181,12 +182,13 @@ def max_over_ranks(v, world):
 BATCH_SYSTEMS = 4096
 BATCH_CPU_STRIDE = 16  # the CPU arms solve every 16th network per step, scaled by 16
 BATCH_RTOL = 1e-10
+BATCH_MAX_IT = 1000  # iteration budget of each network's Krylov solve (NetworkSolver::new)
 
 ADJOINT_N = 512
 
 PLAIN_METRIC = {
     "c5": "ms per theta update (dL/dtheta by the adjoint, forward and adjoint to 1e-10), 512^2 Darcy",
-    "c4": "ms to 1e-10 equilibrated residual, 4096 batched Kirchhoff networks (FP64 Jacobi-PCG)",
+    "c4": "ms per batched 1-D network solve (LinearSystemSolver, detected method, tol 1e-10), 4096 Kirchhoff networks",
     "c1": "ms to 1e-8 rel-residual (FP64 Jacobi-PCG), 128^2 2-D pressure Poisson",
     "c2": "ms to 1e-8 rel-residual (FP64 AMG-PCG), {n}^3 constant-coefficient Poisson",
 }
@@ -209,16 +211,22 @@ def plain_problem(args, P):
     return A, b, cfg
 
 
-def oracle_batch_sample(O, systems, cores, stride):
-    """ms of the oracle solving all networks, one serial Jacobi-PCG per network
-    on a pool of `cores` worker threads (each with a one-thread OpenMP pool),
-    estimated from every `stride`-th network and scaled by `stride`; and the
-    reports of the networks solved."""
+def oracle_batch_sample(O, systems, cores, stride, cascade=True):
+    """ms of the oracle solving all networks on a pool of `cores` worker
+    threads (each with a one-thread OpenMP pool), estimated from every
+    `stride`-th network and scaled by `stride`; and the reports of the networks
+    solved. cascade: LinearSystemSolver::solve_with_initial_guess with
+    detect_solver_method (equilibration, dense LU for n <= 256, Krylov with
+    the residual recheck and the dense fallback); else one Jacobi-PCG per
+    network with the equilibrated residual test."""
     from concurrent.futures import ThreadPoolExecutor
     picked = [(O.Csr.from_matrix(A), b) for A, b in systems[::stride]]
 
     def one(item):
-        return O.pcg_equilibrated(item[0], item[1], rtol=BATCH_RTOL, max_it=20000)[1]
+        if cascade:
+            return O.linear_system_solve(item[0], item[1], method=O.LS_DETECT, tolerance=BATCH_RTOL,
+                                         max_iterations=BATCH_MAX_IT)[1]
+        return O.pcg_equilibrated(item[0], item[1], rtol=BATCH_RTOL, max_it=BATCH_MAX_IT)[1]
 
     with ThreadPoolExecutor(max_workers=cores, initializer=O.set_threads, initargs=(1,)) as ex:
         t0 = time.perf_counter()
@@ -229,22 +237,27 @@ def oracle_batch_sample(O, systems, cores, stride):
 
 def run_reference_batch(args, O, P, cores):
     systems = P.network_batch(BATCH_SYSTEMS, seed=0)
-    times, reps = [], []
+    times, reps, pcg_times = [], [], []
     for s in range(args.warmup + args.steps):
         ms, reps = oracle_batch_sample(O, systems, cores, BATCH_CPU_STRIDE)
         if s >= args.warmup:
             times.append(ms)
+    for _ in range(2):
+        pcg_ms, _ = oracle_batch_sample(O, systems, cores, BATCH_CPU_STRIDE, cascade=False)
+        pcg_times.append(pcg_ms)
     ms = sum(times) / len(times)
-    sample = (f"per step every {BATCH_CPU_STRIDE}th of the {BATCH_SYSTEMS} networks "
-              f"({len(reps)} networks), one serial FP64 Jacobi-PCG each (equilibrated residual to "
-              f"{BATCH_RTOL:g}) on {cores} worker threads, scaled by {BATCH_CPU_STRIDE}")
+    sample = (f"per step every {BATCH_CPU_STRIDE}th of the {BATCH_SYSTEMS} networks ({len(reps)} networks), "
+              f"the 1-D solve of each (detected method, equilibration, dense LU for n <= 256, Krylov to "
+              f"{BATCH_RTOL:g} with recheck and dense fallback) on {cores} worker threads, scaled by "
+              f"{BATCH_CPU_STRIDE}")
     line = {
         "impl": "reference", "metric": PLAIN_METRIC["c4"], "value": ms, "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": batch_config(systems),
-        "converged_systems_in_sample": sum(r.termination == "Converged" for r in reps),
+        "paths_in_sample": dict(collections.Counter(r.path for r in reps)),
         "iterations_in_sample": int(sum(r.iterations for r in reps)),
+        "jacobi_pcg_ms": min(pcg_times),
         "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -368,8 +381,10 @@ def run_adjoint(args, world, rank, local):
 
 def batch_config(systems):
     return {"workload": f"{len(systems)} seeded Kirchhoff networks, n ~ U[20, 2000], spanning tree + 10 % loop "
-                        "edges, Hagen-Poiseuille conductances, inlet 1000 Pa / outlet 0 Pa; Jacobi-PCG per "
-                        f"network to {BATCH_RTOL:g} on the row-equilibrated residual",
+                        "edges, Hagen-Poiseuille conductances, inlet 1000 Pa / outlet 0 Pa; per network "
+                        "LinearSystemSolver::solve_with_initial_guess with detect_solver_method: rows equilibrated, "
+                        f"dense LU for n <= 256, Jacobi-preconditioned CG or BiCGSTAB to {BATCH_RTOL:g} (absolute, "
+                        f"equilibrated system, {BATCH_MAX_IT} iterations), residual recheck, dense LU fallback",
             "systems": len(systems), "rows": int(sum(A.nrows for A, _ in systems)),
             "nnz": int(sum(A.nnz for A, _ in systems)), "seed": 0}
 
@@ -609,16 +624,18 @@ def run_plain(args, world, rank, local):
 
 
 def run_batch(args, world, rank, local):
-    """GPU arm of c4: all networks in one batched solve per step (persistent
-    CTA-per-system kernels replayed from a CUDA graph, autotuned widths), FP64;
-    value = the solve's device time (events around copies in, graph, copies
-    out), e2e = host wall clock around the call; FP32 + refinement beside it;
-    the oracle beside it on rank 0 (every BATCH_CPU_STRIDE-th network)."""
+    """GPU arm of c4: the 1-D solve of all networks in one batched call per
+    step (cfd_batch_linear_system_solve: detection, equilibration, dense LU
+    for n <= 256, persistent CTA-per-system CG / BiCGSTAB, recheck, dense LU
+    fallback), FP64; value = the call's device time (events around copies in,
+    kernels, copies out), e2e = host wall clock around the call; Jacobi-PCG per
+    network (cfd_batch_solve, CUDA graph) and FP32 + refinement beside it; the
+    oracle beside it on rank 0 (every BATCH_CPU_STRIDE-th network)."""
     import torch
     torch.cuda.set_device(local)
     import cfdrs_b200 as cf
     from cfdrs_b200 import problems as P
-    from cfdrs_b200.batch import NetworkBatch
+    from cfdrs_b200.batch import LS_DETECT, LS_PATHS, NetworkBatch
     from cfdrs_b200.device import context
 
     systems = P.network_batch(BATCH_SYSTEMS, seed=0)
@@ -626,8 +643,12 @@ def run_batch(args, world, rank, local):
     nb = NetworkBatch([A for A, _ in systems], ctx=context(local))
     cfg = cf.IterativeSolverConfig(0.0, BATCH_RTOL, 40000)
     tuned = {p.name: nb.autotune(p, sample_iterations=64) for p in (cf.Precision.FP64, cf.Precision.FP32_REFINE)}
+
+    def cascade(precision=cf.Precision.FP64):
+        return nb.solve_linear_systems(b, tolerance=BATCH_RTOL, max_iterations=BATCH_MAX_IT, method=LS_DETECT,
+                                       precision=precision)
     for _ in range(args.warmup):
-        nb.solve(b, config=cfg)
+        cascade()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -635,13 +656,18 @@ def run_batch(args, world, rank, local):
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            x, rep = nb.solve(b, config=cfg)
+            x, rep = cascade()
             wall.append((time.perf_counter() - t0) * 1e3)
             dev.append(rep.device_ms)
     ms = max_over_ranks(sum(dev) / len(dev), world)
     e2e_ms = max_over_ranks(sum(wall) / len(wall), world)
+    _, rep32 = cascade(cf.Precision.FP32_REFINE)
+    pcg = []
+    for _ in range(3):
+        _, prep = nb.solve(b, config=cfg)
+        pcg.append(prep.device_ms)
     nb.solve(b, config=cfg, precision=cf.Precision.FP32_REFINE)
-    _, rep32 = nb.solve(b, config=cfg, precision=cf.Precision.FP32_REFINE)
+    _, prep32 = nb.solve(b, config=cfg, precision=cf.Precision.FP32_REFINE)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -650,26 +676,29 @@ def run_batch(args, world, rank, local):
         cores = O.get_threads()
         cpu_ms, reps = oracle_batch_sample(O, systems, cores, BATCH_CPU_STRIDE)
         cpu = {"value": cpu_ms, "unit": "ms", "cores": cores, "kind": "port",
-               "sample": f"every {BATCH_CPU_STRIDE}th network ({len(reps)}), one serial FP64 Jacobi-PCG each on "
-                         f"{cores} worker threads, scaled by {BATCH_CPU_STRIDE}"}
+               "sample": f"every {BATCH_CPU_STRIDE}th network ({len(reps)}), the 1-D solve of each on {cores} "
+                         f"worker threads, scaled by {BATCH_CPU_STRIDE}"}
     if rank == 0:
         rows, nnz = nb.rows, int(nb.val.size)
-        moved = nnz * (8 + 2) + rows * 8 * 6  # one pass over values, 16-bit columns and six vectors
+        paths = dict(collections.Counter(LS_PATHS[p] for p in rep.path))
         line = {
             "metric": PLAIN_METRIC["c4"], "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded networks)",
             "config": batch_config(systems),
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * rows * 8, "d2h_bytes_per_step": rows * 8},
-            "gpu_launches": args.steps * sum(1 for c in tuned["FP64"]["systems"] if c > 0),  # one per bucket
-            "roofline": {"bound": "hbm", "achieved": moved / ms / 1e6, "peak": measured_peak()[0], "unit": "GB/s",
-                         "frac": moved / ms / 1e6 / measured_peak()[0], "traffic": None,
-                         "kernel": "batched Jacobi-PCG: each system lives in shared memory for its whole solve, so "
-                                   "an iteration is bound by barrier latency, not HBM; achieved = one pass over the "
-                                   "systems' bytes per solve"},
-            "converged_systems": rep.converged_systems, "total_iterations": rep.total_iterations,
-            "max_rel_residual": rep.max_rel_residual,
-            "fp32_refine_ms": rep32.device_ms, "fp32_refine_total_inner_iterations": rep32.total_iterations,
+            "gpu_launches": args.steps * (2 + sum(1 for c in tuned["FP64"]["systems"][2:] if c > 0)
+                                          + (1 if paths.get("krylov_fallback", 0) else 0)),
+            "roofline": {"bound": "latency", "achieved": None, "peak": measured_peak()[0], "unit": "GB/s",
+                         "frac": None, "traffic": None,
+                         "kernel": "batched 1-D solve: each Krylov system lives in shared memory for its whole "
+                                   "solve (an iteration is bound by CTA barrier latency, not HBM); the dense LU "
+                                   "fallback is FP64-FMA bound"},
+            "paths": paths, "total_iterations": rep.total_iterations, "max_iterations": rep.max_iterations,
+            "max_residual": rep.max_residual,
+            "fp32_refine_ms": rep32.device_ms,
+            "jacobi_pcg_ms": min(pcg), "jacobi_pcg_total_iterations": prep.total_iterations,
+            "jacobi_pcg_fp32_refine_ms": prep32.device_ms,
             "autotuned": tuned, "clocks": clk.summary(),
         }
         if cpu is not None:

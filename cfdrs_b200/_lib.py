@@ -32,7 +32,7 @@ EXPORTS = [
     "cfd_pattern_outer", "cfd_csr_set_values_device",
     "cfd_batch_create", "cfd_batch_update_values", "cfd_batch_solve", "cfd_batch_autotune", "cfd_batch_config",
     "cfd_batch_create_networks", "cfd_batch_assemble", "cfd_batch_values", "cfd_network_assemble_host",
-    "cfd_batch_destroy",
+    "cfd_batch_destroy", "cfd_ls_options_default", "cfd_batch_linear_system_solve",
     "cfd_residual_norm_noalloc",
 ]
 
@@ -70,13 +70,26 @@ class SolveReportC(C.Structure):
 class BatchReportC(C.Structure):
     _fields_ = [("num_systems", C.c_int32), ("converged_systems", C.c_int32), ("total_iterations", C.c_int64),
                 ("max_iterations", C.c_int32), ("pad", C.c_int32), ("max_rel_residual", C.c_double),
-                ("device_ms", C.c_double)]
+                ("device_ms", C.c_double), ("direct_ms", C.c_double), ("krylov_ms", C.c_double),
+                ("fallback_ms", C.c_double)]
+
+
+class LsOptionsC(C.Structure):
+    _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_int64), ("method", C.c_int32),
+                ("precision", C.c_int32), ("memory", C.c_int32), ("max_outer", C.c_int32),
+                ("inner_tolerance", C.c_double)]
+
+
+class LsResultC(C.Structure):
+    _fields_ = [("method", C.c_int32), ("path", C.c_int32), ("termination", C.c_int32),
+                ("iterations", C.c_int32), ("residual", C.c_double)]
 
 
 class LayoutInfoC(C.Structure):
     _fields_ = [("blocks", C.c_int64), ("compressed_nnz", C.c_int64), ("all_compressed", C.c_int32),
                 ("x_staged", C.c_int32), ("threads_per_row", C.c_int32), ("max_windows", C.c_int32),
-                ("staged_x_entries", C.c_int64), ("path_f32", C.c_int32), ("path_f64", C.c_int32)]
+                ("staged_x_entries", C.c_int64), ("path_f32", C.c_int32), ("path_f64", C.c_int32),
+                ("sliced", C.c_int32), ("pad", C.c_int32), ("sliced_slots", C.c_int64)]
 
 
 class KernelStatsC(C.Structure):
@@ -153,6 +166,8 @@ def load():
         "cfd_batch_autotune": (C.c_int, [P, I32, I32]),
         "cfd_batch_config": (C.c_int, [P, I32, P, P, P]),
         "cfd_batch_destroy": (C.c_int, [P]),
+        "cfd_ls_options_default": (None, [P]),
+        "cfd_batch_linear_system_solve": (C.c_int, [P, P, P, P, P, P]),
         "cfd_residual_norm_noalloc": (C.c_int, [I64, I64, P, P, P, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():

@@ -4,8 +4,10 @@ The 1-D network solver of CFDrs solves one Kirchhoff system per design
 candidate (``LinearSystemSolver::solve_with_initial_guess``,
 ``crates/cfd-1d/src/solver/core/linear_system.rs:114-155``, called per
 candidate from ``crates/cfd-optim/src/metrics/blueprint_graph.rs:48-135``).
-:class:`NetworkBatch` solves all of them in one device call: Jacobi-PCG per
-system with the reference's row-equilibrated residual test.
+:class:`NetworkBatch` solves all of them in one device call: the solver's
+full cascade (:meth:`NetworkBatch.solve_linear_systems`), or Jacobi-PCG per
+system with the reference's row-equilibrated residual test
+(:meth:`NetworkBatch.solve`).
 """
 from __future__ import annotations
 
@@ -31,6 +33,30 @@ class BatchReport:
     termination: np.ndarray
     iterations: np.ndarray
     rel_residual: np.ndarray
+
+
+LS_CG, LS_BICGSTAB, LS_DETECT = 0, 1, 2
+LS_PATHS = ["krylov", "direct", "direct_unscaled", "krylov_fallback", "failed", "error"]
+
+
+@dataclass
+class LinearSystemReport:
+    """Per batch and per system outcome of :meth:`NetworkBatch.solve_linear_systems`:
+    ``method`` (LS_CG / LS_BICGSTAB), ``path`` (an index into LS_PATHS),
+    ``termination`` of the Krylov solve (-1 when none ran), its ``iterations``
+    and ``residual`` = ||D (A x - b)|| / ||D b|| of the returned solution."""
+    num_systems: int
+    solved_systems: int
+    total_iterations: int
+    max_iterations: int
+    max_residual: float
+    device_ms: float
+    method: np.ndarray
+    path: np.ndarray
+    termination: np.ndarray
+    iterations: np.ndarray
+    residual: np.ndarray
+    phase_ms: dict = None  # device time of the direct, Krylov and fallback phases
 
 
 def _p(a):
@@ -243,6 +269,56 @@ class NetworkBatch:
         return xx, BatchReport(rep.num_systems, rep.converged_systems, rep.total_iterations, rep.max_iterations,
                                rep.max_rel_residual, rep.device_ms, term, its, res)
 
+    def solve_linear_systems(self, b=None, x=None, tolerance: float = 1e-6, max_iterations: int = 1000,
+                             method: int = LS_DETECT, precision: Precision = Precision.FP64,
+                             inner_tolerance: float = 1e-4, max_outer: int = 40):
+        """``LinearSystemSolver::new().with_method(..).with_tolerance(..)
+        .with_max_iterations(..).solve_with_initial_guess`` for every system
+        (``cfd_batch_linear_system_solve``): equilibration, dense LU for n <=
+        256, CG or BiCGSTAB (``method``: LS_CG, LS_BICGSTAB, or LS_DETECT for
+        ``NetworkSolver::detect_solver_method``) with the residual recheck and
+        the dense fallback for larger systems. b and x as for :meth:`solve`.
+        Returns ``(x, LinearSystemReport)``."""
+        device = _torch_cuda(x)
+        if device:
+            import torch
+            if x.dtype != torch.float64 or x.numel() != self.rows or not x.is_contiguous():
+                raise SolveError("x must be a contiguous float64 CUDA tensor with one entry per row")
+            if b is not None and (not _torch_cuda(b) or b.dtype != torch.float64 or b.numel() != self.rows
+                                  or not b.is_contiguous()):
+                raise SolveError("with a CUDA x, b must be None or a matching contiguous float64 CUDA tensor")
+            xx, bp, xp = x, (None if b is None else C.c_void_p(b.data_ptr())), C.c_void_p(x.data_ptr())
+        else:
+            if _torch_cuda(b):
+                raise SolveError("b is a CUDA tensor: pass x as a float64 CUDA tensor as well (device solve)")
+            bb = None if b is None else np.ascontiguousarray(b, dtype=np.float64)
+            if bb is not None and bb.shape[0] != self.rows:
+                raise SolveError(f"rhs has {bb.shape[0]} entries, the batch {self.rows} rows")
+            xx = np.zeros(self.rows) if x is None else np.array(x, dtype=np.float64, copy=True)
+            bp, xp = _p(bb), _p(xx)
+        opt = _lib.LsOptionsC(tolerance, max_iterations, method, int(precision), 1 if device else 0, max_outer,
+                              inner_tolerance)
+        res = (_lib.LsResultC * max(self.num_systems, 1))()
+        rep = _lib.BatchReportC()
+        if device:
+            self.ctx.set_stream(torch.cuda.current_stream(x.device).cuda_stream)
+        try:
+            st = _lib.load().cfd_batch_linear_system_solve(self.h, C.byref(opt), bp, xp, res, C.byref(rep))
+        finally:
+            if device:
+                self.ctx.set_stream(None)
+        if st != _lib.CFD_OK:
+            raise SolveError(f"batched linear-system solve failed: {_lib.STATUS_NAMES.get(st, st)}: "
+                             f"{_lib.load().cfd_last_error().decode()}")
+        arr = np.ctypeslib.as_array(res)[:self.num_systems]
+        return xx, LinearSystemReport(rep.num_systems, rep.converged_systems, rep.total_iterations,
+                                      rep.max_iterations, rep.max_rel_residual, rep.device_ms,
+                                      arr["method"].astype(np.int32), arr["path"].astype(np.int32),
+                                      arr["termination"].astype(np.int32), arr["iterations"].astype(np.int32),
+                                      arr["residual"].astype(np.float64),
+                                      {"direct": rep.direct_ms, "krylov": rep.krylov_ms,
+                                       "fallback": rep.fallback_ms})
+
     def autotune(self, precision: Precision = Precision.FP64, sample_iterations: int = 64) -> dict:
         _lib.check(_lib.load().cfd_batch_autotune(self.h, int(precision), sample_iterations))
         return self.config(precision)
@@ -264,4 +340,5 @@ class NetworkBatch:
             self.h = None
 
 
-__all__ = ["NetworkBatch", "BatchReport", "Termination", "PackedNetworks", "pack_networks", "network_assemble_host"]
+__all__ = ["NetworkBatch", "BatchReport", "LinearSystemReport", "LS_CG", "LS_BICGSTAB", "LS_DETECT", "LS_PATHS",
+           "Termination", "PackedNetworks", "pack_networks", "network_assemble_host"]

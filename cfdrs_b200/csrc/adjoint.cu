@@ -71,6 +71,7 @@ cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev) {
     k_cast64to32<<<grid, 256, 0, s>>>(nnz, a->dev.v64, a->dev.v32);
     CFD_TRY_CUDA(cudaGetLastError());
   }
+  a->dev.sl_stale = true;
   // The host copy feeds AMG setup (the Galerkin recompute reads the device values).
   CFD_TRY_CUDA(cudaMemcpyAsync(a->host.v.data(), val_dev, nnz * sizeof(double), cudaMemcpyDeviceToHost, s));
   CFD_TRY_CUDA(cudaStreamSynchronize(s));

@@ -512,6 +512,7 @@ cfd_status batch_build(cfd_context* ctx, int32_t num_systems, const int64_t* sys
     return ka != kb ? ka < kb : nrows(a) > nrows(b);
   });
   std::vector<int> sorted = ord;
+  bt->h_order = sorted;
   for (int k = 0; k <= kBuckets; ++k) bt->bucket_begin[k] = num_systems;
   for (int q = num_systems - 1; q >= 0; --q) bt->bucket_begin[bucket_of(sorted[q])] = q;
   for (int k = kBuckets - 1; k >= 0; --k)
@@ -547,6 +548,8 @@ cfd_status batch_build(cfd_context* ctx, int32_t num_systems, const int64_t* sys
   if ((st = dalloc(&bt->params, 1)) != CFD_OK) return fail(st);
   if (cudaMallocHost((void**)&bt->h_params, sizeof(BatchParams)) != cudaSuccess) return fail(CFD_ERR_ALLOC);
   std::vector<float> v32(val, val + nnz);
+  for (int64_t k = 0; k < nnz; ++k)
+    if (std::isfinite(val[k]) && !std::isfinite(v32[k])) bt->f32_out_of_range = true;
   if (cudaMemcpyAsync(bt->sys_row, bt->h_sys_row.data(), (num_systems + 1) * sizeof(int), cudaMemcpyHostToDevice,
                       s) != cudaSuccess ||
       cudaMemcpyAsync(bt->rp, rp32.data(), (rows + 1) * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
@@ -591,11 +594,15 @@ cfd_status cfd_batch_update_values(cfd_batch* bt, const double* val) {
     std::lock_guard<std::mutex> g(bt->ctx->mu);
     CFD_TRY_CUDA(cudaSetDevice(bt->ctx->device));
     std::vector<float> v32(val, val + bt->nnz);
+    bool out_of_range = false;
+    for (int64_t k = 0; k < bt->nnz; ++k)
+      if (std::isfinite(val[k]) && !std::isfinite(v32[k])) out_of_range = true;
     CFD_TRY_CUDA(cudaMemcpyAsync(bt->v64, val, bt->nnz * sizeof(double), cudaMemcpyHostToDevice, bt->ctx->stream));
     CFD_TRY_CUDA(
         cudaMemcpyAsync(bt->v32, v32.data(), bt->nnz * sizeof(float), cudaMemcpyHostToDevice, bt->ctx->stream));
     CFD_TRY_CUDA(cudaStreamSynchronize(bt->ctx->stream));
     bt->values_valid = true;
+    bt->f32_out_of_range = out_of_range;
     return CFD_OK;
   });
 }
@@ -621,6 +628,10 @@ cfd_status cfd_batch_solve(cfd_batch* bt, const cfd_solve_options* opt, const do
         opt->precision > 1) {
       set_error("cfd_batch_solve: needs CG with Jacobi, valid tolerances and a positive iteration budget");
       return CFD_ERR_CONFIG;
+    }
+    if (bt->f32_out_of_range && opt->precision == CFD_PRECISION_FP32_REFINE) {
+      set_error("cfd_batch_solve: an entry of the batch exceeds the FP32 range; solve in FP64");
+      return CFD_ERR_NONFINITE;
     }
     std::lock_guard<std::mutex> g(bt->ctx->mu);
     cfd_context* ctx = bt->ctx;
@@ -741,7 +752,8 @@ cfd_status cfd_batch_destroy(cfd_batch* bt) {
   drop_graphs(bt);
   for (void* p : {(void*)bt->sys_row, (void*)bt->rp, (void*)bt->col, (void*)bt->v64, (void*)bt->v32, (void*)bt->x,
                   (void*)bt->b, (void*)bt->term, (void*)bt->iters, (void*)bt->resid, (void*)bt->order,
-                  (void*)bt->queues, (void*)bt->params})
+                  (void*)bt->queues, (void*)bt->params, (void*)bt->ls_method, (void*)bt->ls_path,
+                  (void*)bt->ls_list, (void*)bt->ls_params, (void*)bt->ls_queue, (void*)bt->ls_scratch})
     if (p) cudaFree(p);
   if (bt->h_params) cudaFreeHost(bt->h_params);
   network_plan_free(bt->net);

@@ -66,4 +66,17 @@ struct cfd_batch {
   // failed: its values are not a matrix then.
   bool values_valid = true;
   cfd::NetworkPlanDev* net = nullptr;  // network batches only
+  std::vector<int> h_order;            // `order` on the host
+  // An entry that is finite in FP64 but not in FP32: FP32_REFINE solves refuse the batch.
+  bool f32_out_of_range = false;
+  // cfd_batch_linear_system_solve (batch_ls.cu): per-system method and path,
+  // a device list of systems, its parameter block and queues, and the dense
+  // LU scratch (one n x n slot per CTA, grown on demand).
+  int* ls_method = nullptr;
+  int* ls_path = nullptr;
+  int* ls_list = nullptr;
+  double* ls_params = nullptr;
+  unsigned* ls_queue = nullptr;
+  double* ls_scratch = nullptr;
+  size_t ls_scratch_elems = 0;
 };

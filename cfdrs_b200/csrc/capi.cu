@@ -161,6 +161,28 @@ cfd_status devmat_upload(DevMat& m, const HostCsr& h, bool want32, cudaStream_t 
   CFD_TRY(dmalloc(&m.desc, (int64_t)m.nblk));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.desc, desc.data(), desc.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
   CFD_TRY(upload_layout(m, h, blk, s));
+  {
+    HostSliced S;
+    if (encode_sliced(h, m.tpr, m.base_mult, S)) {
+      CFD_TRY(dmalloc(&m.sl_off, (int64_t)S.off.size()));
+      CFD_TRY(dmalloc(&m.sl_code, (int64_t)S.code.size()));
+      CFD_TRY(dmalloc(&m.sl_dict, (int64_t)S.dict.size()));
+      CFD_TRY(dmalloc(&m.sl_doff, (int64_t)S.doff.size()));
+      CFD_TRY(dmalloc(&m.sl_src, S.slots));
+      CFD_TRY(dmalloc(&m.sl_v32, S.slots));
+      CFD_TRY_CUDA(cudaMemcpyAsync(m.sl_off, S.off.data(), S.off.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+      CFD_TRY_CUDA(cudaMemcpyAsync(m.sl_code, S.code.data(), S.code.size(), cudaMemcpyHostToDevice, s));
+      CFD_TRY_CUDA(cudaMemcpyAsync(m.sl_dict, S.dict.data(), S.dict.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+      CFD_TRY_CUDA(cudaMemcpyAsync(m.sl_doff, S.doff.data(), S.doff.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+      CFD_TRY_CUDA(cudaMemcpyAsync(m.sl_src, S.src.data(), S.src.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+      // the host vectors above are released when this block ends
+      CFD_TRY_CUDA(cudaStreamSynchronize(s));
+      m.sl = true;
+      m.sl_slices = S.nslices;
+      m.sl_slots = S.slots;
+      m.sl_stale = true;
+    }
+  }
   CFD_TRY_CUDA(cudaMemcpyAsync(m.rp, rp32.data(), rp32.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.col, h.ci.data(), m.nnz * sizeof(int), cudaMemcpyHostToDevice, s));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.v64, h.v.data(), m.nnz * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -173,6 +195,7 @@ cfd_status devmat_upload(DevMat& m, const HostCsr& h, bool want32, cudaStream_t 
 cfd_status devmat_ensure32(DevMat& m, cudaStream_t s) {
   if (m.v32 || m.nnz == 0) return CFD_OK;
   CFD_TRY(dmalloc(&m.v32, m.nnz));
+  m.sl_stale = true;
   return cast_to_f32(m.v64, m.v32, m.nnz, s);
 }
 
@@ -186,6 +209,7 @@ cfd_status devmat_update_values(DevMat& m, const double* v, int64_t nnz, bool wa
     if (!m.v32) CFD_TRY(dmalloc(&m.v32, m.nnz));
     CFD_TRY(cast_to_f32(m.v64, m.v32, m.nnz, s));
   }
+  m.sl_stale = true;
   CFD_TRY_CUDA(cudaStreamSynchronize(s));
   return CFD_OK;
 }
@@ -204,6 +228,15 @@ void devmat_free(DevMat& m) {
   dfree(m.roff);
   dfree(m.xwin);
   dfree(m.xdesc);
+  dfree(m.sl_off);
+  dfree(m.sl_code);
+  dfree(m.sl_dict);
+  dfree(m.sl_doff);
+  dfree(m.sl_src);
+  dfree(m.sl_v32);
+  m.sl = false;
+  m.sl_slices = m.sl_slots = 0;
+  m.sl_stale = true;
   m.compressed_nnz = 0;
   m.all_compressed = false;
   m.xs = false;
@@ -606,6 +639,8 @@ cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out) {
   out->threads_per_row = m.tpr;
   out->path_f32 = spmv_path(m, 0);
   out->path_f64 = spmv_path(m, 1);
+  out->sliced = m.sl ? 1 : 0;
+  out->sliced_slots = m.sl_slots;
   return CFD_OK;
 }
 
@@ -616,10 +651,11 @@ cfd_status cfd_csr_set_path(cfd_csr* a, int32_t fp32, int32_t path) {
   }
   const DevMat& m = a->dev;
   const bool ok = path == CFD_PATH_AUTO || path == CFD_PATH_TIMED || path == CFD_PATH_SPLIT ||
-                  (path == CFD_PATH_RECORD && m.all_compressed) || (path == CFD_PATH_X_STAGED && m.xs);
+                  (path == CFD_PATH_RECORD && m.all_compressed) || (path == CFD_PATH_X_STAGED && m.xs) ||
+                  (path == CFD_PATH_SLICED && m.sl && fp32);
   if (!ok) {
-    set_error("SpMV pipeline %d not available for this matrix (all blocks coded: %d, x staged: %d)", path,
-              (int)m.all_compressed, (int)m.xs);
+    set_error("SpMV pipeline %d not available for this matrix and precision (all blocks coded: %d, x staged: %d, "
+              "sliced: %d, FP32 only)", path, (int)m.all_compressed, (int)m.xs, (int)m.sl);
     return CFD_ERR_CONFIG;
   }
   std::lock_guard<std::mutex> g(a->ctx->mu);
@@ -647,6 +683,12 @@ cfd_status cfd_layout_check(int64_t nrows, int64_t ncols, int64_t nnz, const int
       set_error("layout check: %s", why.c_str());
       return CFD_ERR_STATE;
     }
+    HostSliced S;
+    const bool sliced = encode_sliced(h, tpr, L.base_mult, S);
+    if (sliced && !check_sliced(h, L.base_mult, S, &why)) {
+      set_error("sliced layout check: %s", why.c_str());
+      return CFD_ERR_STATE;
+    }
     if (out) {
       *out = cfd_layout_info{};
       out->blocks = (int64_t)blk.size() - 1;
@@ -656,6 +698,8 @@ cfd_status cfd_layout_check(int64_t nrows, int64_t ncols, int64_t nnz, const int
       out->threads_per_row = tpr;
       out->max_windows = maxw;
       out->staged_x_entries = staged;
+      out->sliced = sliced ? 1 : 0;
+      out->sliced_slots = sliced ? S.slots : 0;
     }
     return CFD_OK;
   });

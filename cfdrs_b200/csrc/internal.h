@@ -164,7 +164,37 @@ struct DevMat {
   mutable int8_t path[2] = {-1, -1};
   int nblk = 0;
   int tpr = 1;         // threads cooperating on one row (power of two, <= 32)
+  // Sliced layout (FP32 SpMV only; HostSliced): slice offsets, codes,
+  // dictionaries, the CSR entry of every slot and the slot-major FP32 values,
+  // gathered from v32 before the first sliced SpMV after v32 changed.
+  bool sl = false;
+  int64_t sl_slices = 0, sl_slots = 0;
+  int* sl_off = nullptr;
+  uint8_t* sl_code = nullptr;
+  int* sl_dict = nullptr;
+  int* sl_doff = nullptr;
+  int* sl_src = nullptr;
+  float* sl_v32 = nullptr;
+  mutable bool sl_stale = true;
 };
+
+// Sliced layout (sliced.cpp, k_spmv_sl): rows in slices of kSlRows stored
+// slot-major, one dictionary of column offsets per kSlChunkSlices slices.
+constexpr int kSlRows = 32;
+constexpr int kSlChunkSlices = 16;
+constexpr int kSlMaxWidth = 32;
+constexpr int kSlPadCode = 255;
+constexpr double kSlMaxPadding = 1.15;
+struct HostSliced {
+  int64_t nslices = 0, slots = 0;
+  std::vector<int> off;       // nslices + 1 slot offsets (multiples of kSlRows)
+  std::vector<uint8_t> code;  // per slot, kSlPadCode for padding (slots + 16)
+  std::vector<int> dict;      // concatenated chunk dictionaries
+  std::vector<int> doff;      // chunk dictionary offsets
+  std::vector<int> src;       // per slot: CSR entry, -1 for padding
+};
+bool encode_sliced(const HostCsr& h, int tpr, uint64_t base_mult, HostSliced& S);
+bool check_sliced(const HostCsr& h, uint64_t base_mult, const HostSliced& S, std::string* why);
 
 // SpMV pipeline that an SpMV of precision p ([0] FP32, [1] FP64) runs: the
 // setting, with CFD_PATH_AUTO resolved to RECORD for FP32 and X_STAGED for
@@ -174,6 +204,8 @@ struct DevMat {
 inline int spmv_path(const DevMat& m, int p) {
   int path = m.path[p];
   if (path == CFD_PATH_TIMED) return path;
+  if (path == CFD_PATH_AUTO) path = p == 0 ? (m.sl ? CFD_PATH_SLICED : CFD_PATH_RECORD) : path;
+  if (path == CFD_PATH_SLICED && (p != 0 || !m.sl)) path = p == 0 ? CFD_PATH_RECORD : CFD_PATH_AUTO;
   if (path == CFD_PATH_AUTO) path = p == 0 ? CFD_PATH_RECORD : (m.xs && m.tpr == 1 ? CFD_PATH_X_STAGED : CFD_PATH_SPLIT);
   if (path == CFD_PATH_X_STAGED && !m.xs) path = CFD_PATH_RECORD;
   if (path == CFD_PATH_RECORD && !m.all_compressed) path = CFD_PATH_SPLIT;

@@ -748,6 +748,75 @@ __global__ void __launch_bounds__(kPipeThreads, PipeLayout<VT, CODES>::kMinBlock
 }
 
 // ---------------------------------------------------------------------------
+// Sliced pipeline (DevMat::sl, FP32 values): one warp per slice of 32 rows,
+// one row per lane. Slot k of the slice holds the k-th entry of each of its
+// 32 rows, so a warp's value load covers 128 contiguous bytes and its code
+// load 32; the x gathers of neighbouring rows fall on neighbouring entries.
+// No shared-memory staging and no producer: every warp keeps its own loads in
+// flight, so occupancy, not copy issue, hides the latency. Padding slots
+// (code kSlPadCode) are skipped; the row sum adds the entries in CSR order, as
+// the other pipelines do, so y = A x is bit-identical to theirs.
+struct SlView {
+  const int* __restrict__ off;       // slice slot offsets
+  const uint8_t* __restrict__ code;  // per slot dictionary code
+  const int* __restrict__ dict;      // chunk dictionaries
+  const int* __restrict__ doff;      // chunk dictionary offsets
+  const float* __restrict__ val;     // slot-major FP32 values
+  unsigned long long base_mult;
+  int nslices, nrows;
+};
+
+template <typename XT, bool OFFDIAG, class Epi>
+__global__ void __launch_bounds__(kThreads) k_spmv_sl(SlView S, const XT* __restrict__ x, Epi epi) {
+  if (epi.skip()) return;
+  double red[Epi::NRED > 0 ? Epi::NRED : 1];
+#pragma unroll
+  for (int q = 0; q < (Epi::NRED > 0 ? Epi::NRED : 1); ++q) red[q] = 0.0;
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (kThreads / 32);
+  for (int sl = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); sl < S.nslices; sl += nw) {
+    const int row = sl * kSlRows + lane;
+    const bool live = row < S.nrows;
+    typename Epi::Pre pre{};
+    if (live) pre = epi.load(row);
+    const int e0 = S.off[sl], e1 = S.off[sl + 1];
+    const int* __restrict__ dict = S.dict + S.doff[sl / kSlChunkSlices];
+    const int base = (int)(((unsigned long long)row * S.base_mult) >> 20);
+    float sum = 0.0f, diag = 0.0f;
+#pragma unroll 8
+    for (int q = e0 + lane; q < e1; q += kSlRows) {
+      const unsigned c = S.code[q];
+      const float v = S.val[q];
+      if (c != (unsigned)kSlPadCode) {
+        const int col = base + __ldg(dict + c);
+        const float xv = (float)__ldg(x + col);
+        if constexpr (OFFDIAG) {
+          const bool isd = (col == row);
+          diag = isd ? v : diag;
+          sum = isd ? sum : sum + v * xv;
+        } else {
+          sum += v * xv;
+        }
+      }
+    }
+    if (live) epi.row(row, sum, diag, pre, red);
+  }
+  if constexpr (Epi::NRED > 0) {
+    double tot[Epi::NRED];
+    if (grid_reduce<Epi::NRED>(red, epi.red, tot) && threadIdx.x == 0) epi.finish(tot);
+  }
+}
+
+// Slot-major FP32 values of the sliced layout from the CSR-order ones.
+static __global__ void __launch_bounds__(kThreads) k_sl_gather(int64_t slots, const int* __restrict__ src,
+                                                        const float* __restrict__ v32, float* __restrict__ out) {
+  for (int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x; q < slots; q += (int64_t)gridDim.x * kThreads) {
+    const int k = src[q];
+    out[q] = k >= 0 ? v32[k] : 0.0f;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // x-staged pipeline (DevMat::xs): each stage receives the block's values, its
 // record (row offsets, codes, dictionary, displacement table) and its x
 // windows by bulk copy, so the consumers read every operand from shared

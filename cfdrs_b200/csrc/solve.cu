@@ -25,6 +25,25 @@ inline int vec_grid(int64_t n) {
 }
 
 #define GRID_STRIDE(i, n) for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < (n); i += (int64_t)gridDim.x * kThreads)
+// The same loop with four strided elements per pass: the elements are visited
+// in the same order (so per-thread sums are unchanged), but the loads of four
+// iterations are in flight together. One 4- or 8-byte element per thread at a
+// time leaves too few bytes in flight per SM to reach the HBM bandwidth.
+#define GRID_STRIDE_U4(i, n, ...)                                                       \
+  {                                                                                    \
+    const int64_t gs_t_ = (int64_t)gridDim.x * kThreads;                               \
+    int64_t gs_i_ = (int64_t)blockIdx.x * kThreads + threadIdx.x;                      \
+    for (; gs_i_ + 3 * gs_t_ < (n); gs_i_ += 4 * gs_t_) {                              \
+      _Pragma("unroll") for (int gs_u_ = 0; gs_u_ < 4; ++gs_u_) {                      \
+        const int64_t i = gs_i_ + gs_u_ * gs_t_;                                       \
+        __VA_ARGS__                                                                    \
+      }                                                                                \
+    }                                                                                  \
+    for (; gs_i_ < (n); gs_i_ += gs_t_) {                                              \
+      const int64_t i = gs_i_;                                                         \
+      __VA_ARGS__                                                                      \
+    }                                                                                  \
+  }
 
 // ---------------------------------------------------------------------------
 // Vector kernels.
@@ -34,22 +53,22 @@ template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_smooth0(int64_t n, const XT* __restrict__ b, const XT* __restrict__ d,
                                                       XT omega, XT* __restrict__ x, const int* done) {
   if (flag_set(done)) return;
-  GRID_STRIDE(i, n) {
+  GRID_STRIDE_U4(i, n, {
     const XT di = d[i];
     x[i] = diag_ok<XT>(di) ? omega * (b[i] / di) : XT(0);
-  }
+  })
 }
 
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_fill(int64_t n, XT* __restrict__ x, XT v, const int* done) {
   if (flag_set(done)) return;
-  GRID_STRIDE(i, n) x[i] = v;
+  GRID_STRIDE_U4(i, n, x[i] = v;)
 }
 
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_copy(int64_t n, const XT* __restrict__ s, XT* __restrict__ d, const int* done) {
   if (flag_set(done)) return;
-  GRID_STRIDE(i, n) d[i] = s[i];
+  GRID_STRIDE_U4(i, n, d[i] = s[i];)
 }
 
 // Dense coarsest-level solve x = A_c^{-1} b with the FP64 inverse; one warp per row.
@@ -77,13 +96,13 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(int64_t n, XT* __restric
   if (st->done) return;
   const XT a = (XT)st->alpha;
   double acc[2] = {0.0, 0.0};
-  GRID_STRIDE(i, n) {
+  GRID_STRIDE_U4(i, n, {
     x[i] = x[i] + a * p[i];
     const XT ri = r[i] - a * q[i];
     r[i] = ri;
     acc[0] += (double)ri * (double)ri;
     if (PRE == kPreJacobi) acc[1] += (double)ri * (double)(ri * jinv[i]);
-  }
+  })
   double tot[2];
   if (grid_reduce<2>(acc, red, tot) && threadIdx.x == 0) {
     const double rn = sqrt(tot[0]);
@@ -114,12 +133,12 @@ __global__ void __launch_bounds__(kThreads) k_pcg_init(int64_t n, XT* __restrict
                                                        DevState* st, Red red) {
   if (st->done) return;
   double acc[1] = {0.0};
-  GRID_STRIDE(i, n) {
+  GRID_STRIDE_U4(i, n, {
     const XT ri = r[i];
     const XT zi = PRE == kPreAmg ? z[i] : (PRE == kPreJacobi ? ri * jinv[i] : ri);
     p[i] = zi;
     acc[0] += (double)ri * (double)zi;
-  }
+  })
   double tot[1];
   if (grid_reduce<1>(acc, red, tot) && threadIdx.x == 0) st->rho = tot[0];
 }
@@ -131,10 +150,10 @@ __global__ void __launch_bounds__(kThreads) k_p_update(int64_t n, XT* __restrict
                                                        const DevState* st) {
   if (st->done) return;
   const XT beta = (XT)st->beta;
-  GRID_STRIDE(i, n) {
+  GRID_STRIDE_U4(i, n, {
     const XT zi = PRE == kPreAmg ? z[i] : (PRE == kPreJacobi ? r[i] * jinv[i] : r[i]);
     p[i] = zi + beta * p[i];
-  }
+  })
 }
 
 // rho_new = r.z after a preconditioner whose last kernel could not fuse it.
@@ -143,7 +162,7 @@ __global__ void __launch_bounds__(kThreads) k_rz(int64_t n, const XT* __restrict
                                                  DevState* st, int mode, Red red) {
   if (st->done) return;
   double acc[1] = {0.0};
-  GRID_STRIDE(i, n) acc[0] += (double)r[i] * (double)z[i];
+  GRID_STRIDE_U4(i, n, acc[0] += (double)r[i] * (double)z[i];)
   double tot[1];
   if (grid_reduce<1>(acc, red, tot) && threadIdx.x == 0) {
     if (mode == 1)
@@ -160,7 +179,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_rho(int64_t n, const XT* __re
                                                        DevState* st, Red red) {
   if (st->done) return;
   double acc[1] = {0.0};
-  GRID_STRIDE(i, n) acc[0] += (double)rhat[i] * (double)r[i];
+  GRID_STRIDE_U4(i, n, acc[0] += (double)rhat[i] * (double)r[i];)
   double tot[1];
   if (grid_reduce<1>(acc, red, tot) && threadIdx.x == 0) {
     const double rho_new = tot[0];
@@ -181,12 +200,12 @@ __global__ void __launch_bounds__(kThreads) k_bicg_p(int64_t n, XT* __restrict__
                                                      const XT* __restrict__ jinv, const DevState* st, int first) {
   if (st->done) return;
   const XT beta = (XT)st->beta, om = (XT)st->omega;
-  GRID_STRIDE(i, n) {
+  GRID_STRIDE_U4(i, n, {
     const XT pi = first ? r[i] : r[i] + beta * (p[i] - om * v[i]);
     p[i] = pi;
     if (PRE == kPreJacobi) ph[i] = pi * jinv[i];
     if (PRE == kPreNone) ph[i] = pi;
-  }
+  })
 }
 
 // s = r - alpha v; ||s|| (early exit: the host then adds alpha p_hat to x);
@@ -198,13 +217,13 @@ __global__ void __launch_bounds__(kThreads) k_bicg_s(int64_t n, XT* __restrict__
   if (st->done) return;
   const XT a = (XT)st->alpha;
   double acc[1] = {0.0};
-  GRID_STRIDE(i, n) {
+  GRID_STRIDE_U4(i, n, {
     const XT si = r[i] - a * v[i];
     s[i] = si;
     if (PRE == kPreJacobi) sh[i] = si * jinv[i];
     if (PRE == kPreNone) sh[i] = si;
     acc[0] += (double)si * (double)si;
-  }
+  })
   double tot[1];
   if (grid_reduce<1>(acc, red, tot) && threadIdx.x == 0) {
     const double sn = sqrt(tot[0]);
@@ -227,12 +246,12 @@ __global__ void __launch_bounds__(kThreads) k_bicg_x(int64_t n, XT* __restrict__
   if (st->done) return;
   const XT a = (XT)st->alpha, om = (XT)st->omega;
   double acc[1] = {0.0};
-  GRID_STRIDE(i, n) {
+  GRID_STRIDE_U4(i, n, {
     x[i] = x[i] + (a * ph[i] + om * sh[i]);
     const XT ri = s[i] - om * t[i];
     r[i] = ri;
     acc[0] += (double)ri * (double)ri;
-  }
+  })
   double tot[1];
   if (grid_reduce<1>(acc, red, tot) && threadIdx.x == 0) {
     const double rn = sqrt(tot[0]);
@@ -257,7 +276,7 @@ template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_axpy_state(int64_t n, XT* __restrict__ x, const XT* __restrict__ y,
                                                          const DevState* st) {
   const XT a = (XT)st->alpha;
-  GRID_STRIDE(i, n) x[i] = x[i] + a * y[i];
+  GRID_STRIDE_U4(i, n, x[i] = x[i] + a * y[i];)
 }
 
 // ---- GMRES(m): restarted, right preconditioned (krylov.rs:150-221) -----------
@@ -358,14 +377,14 @@ __global__ void __launch_bounds__(kThreads) k_jacobi_apply(int64_t n, const XT* 
                                                            const XT* __restrict__ jinv, XT* __restrict__ z,
                                                            const int* skip) {
   if (flag_set(skip)) return;
-  GRID_STRIDE(i, n) z[i] = r[i] * jinv[i];
+  GRID_STRIDE_U4(i, n, z[i] = r[i] * jinv[i];)
 }
 
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_add(int64_t n, XT* __restrict__ x, const XT* __restrict__ z,
                                                   const int* skip) {
   if (flag_set(skip)) return;
-  GRID_STRIDE(i, n) x[i] = x[i] + z[i];
+  GRID_STRIDE_U4(i, n, x[i] = x[i] + z[i];)
 }
 
 // Cycle start: no columns yet, the cycle open unless the solve is done;
@@ -445,12 +464,12 @@ __global__ void __launch_bounds__(kThreads) k_refine_start(int64_t n, const doub
                                                            const DevState* outer, DevState* inner, Red red) {
   const double sc = 1.0 / outer->rnorm;
   double acc[1] = {0.0};
-  GRID_STRIDE(i, n) {
+  GRID_STRIDE_U4(i, n, {
     const float ri = (float)(r64[i] * sc);
     r32[i] = ri;
     x32[i] = 0.0f;
     acc[0] += (double)ri * (double)ri;
-  }
+  })
   double tot[1];
   if (grid_reduce<1>(acc, red, tot) && threadIdx.x == 0) {
     const double rn = sqrt(tot[0]);
@@ -475,7 +494,7 @@ __global__ void __launch_bounds__(kThreads) k_refine_start(int64_t n, const doub
 __global__ void __launch_bounds__(kThreads) k_refine_accumulate(int64_t n, double* __restrict__ x64,
                                                                 const float* __restrict__ d32, const DevState* outer) {
   const double sc = outer->rnorm;
-  GRID_STRIDE(i, n) x64[i] += sc * (double)d32[i];
+  GRID_STRIDE_U4(i, n, x64[i] += sc * (double)d32[i];)
 }
 
 }  // namespace
@@ -538,7 +557,39 @@ struct Launcher {
   // (spmv_path: by default FP32 takes the record pipeline, whose x gathers hit
   // L2, and FP64 the x-staged one for one-thread rows, whose x no longer fits
   // L2 at large sizes; CFD_PATH_TIMED times the eligible ones once).
-  static constexpr int kPathTimed = -2, kPathSplit = 0, kPathRecord = 1, kPathXs = 2;
+  // Sliced pipeline (FP32 values only): one warp per 32-row slice. The
+  // slot-major values are gathered from v32 first when v32 changed since.
+  template <typename XT, bool OFF, class Epi>
+  cfd_status sl_launch(const DevMat& m, const XT* x, Epi epi) {
+    if (m.sl_stale) {
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>((m.sl_slots + kThreads - 1) / kThreads,
+                                                                (int64_t)ctx->num_sms * 8));
+      k_sl_gather<<<g, kThreads, 0, s>>>(m.sl_slots, m.sl_src, m.v32, m.sl_v32);
+      CFD_TRY(check());
+      ctx->stats.launches++;
+      m.sl_stale = false;
+    }
+    auto kern = k_spmv_sl<XT, OFF, Epi>;
+    static int occ[kLaunchCacheDevices] = {};
+    if (ctx->device >= kLaunchCacheDevices) {
+      set_error("device ordinal %d beyond %d", ctx->device, kLaunchCacheDevices);
+      return CFD_ERR_CUDA;
+    }
+    if (occ[ctx->device] <= 0) {
+      int o = 0;
+      CFD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kThreads, 0));
+      occ[ctx->device] = std::max(1, o);
+    }
+    const int64_t warps_needed = m.sl_slices;
+    const int grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>((warps_needed + kThreads / 32 - 1) / (kThreads / 32),
+                             (int64_t)ctx->num_sms * occ[ctx->device]));
+    const SlView sv{m.sl_off, m.sl_code, m.sl_dict, m.sl_doff, m.sl_v32, (unsigned long long)m.base_mult,
+                    (int)m.sl_slices, (int)m.nrows};
+    kern<<<grid, kThreads, 0, s>>>(sv, x, epi);
+    return CFD_OK;
+  }
+  static constexpr int kPathTimed = -2, kPathSplit = 0, kPathRecord = 1, kPathXs = 2, kPathSliced = 3;
   template <typename VT, typename XT, bool OFF, class Epi>
   cfd_status spmv(const DevMat& m, const XT* x, Epi epi) {
     if (m.nrows == 0) return CFD_OK;
@@ -547,6 +598,13 @@ struct Launcher {
     if (m.path[p] == kPathTimed) CFD_TRY(tune<VT>(m));
     int path = spmv_path(m, p);
     if (path == kPathXs && ((uintptr_t)x & 15) != 0) path = m.all_compressed ? kPathRecord : kPathSplit;
+    if constexpr (std::is_same<VT, float>::value) {
+      if (path == kPathSliced && m.v32) {
+        CFD_TRY((sl_launch<XT, OFF, Epi>(m, x, epi)));
+        return finish_spmv<VT, XT>(m);
+      }
+      if (path == kPathSliced) path = m.all_compressed ? kPathRecord : kPathSplit;
+    }
     if constexpr (std::is_same<VT, XT>::value) {
       if (path == kPathXs) {
         CFD_TRY((spmv_xs_launch<VT, OFF, Epi>(m, x, epi)));
@@ -584,9 +642,14 @@ struct Launcher {
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
     if (e != cudaSuccess) fail(e);
-    for (int path = kPathSplit; st == CFD_OK && path <= (m.xs ? kPathXs : kPathRecord); ++path) {
+    const bool sl_ok = std::is_same<VT, float>::value && m.sl && m.v32;
+    for (int path = kPathSplit; st == CFD_OK && path <= kPathSliced; ++path) {
+      if ((path == kPathXs && !m.xs) || (path == kPathSliced && !sl_ok)) continue;
       const EpiStore<VT> epi{ys, nullptr, red()};
       auto run = [&]() -> cfd_status {
+        if constexpr (std::is_same<VT, float>::value) {
+          if (path == kPathSliced) return sl_launch<VT, false, EpiStore<VT>>(m, xs, epi);
+        }
         if (path == kPathXs) return spmv_xs_launch<VT, false, EpiStore<VT>>(m, xs, epi);
         if (path == kPathRecord) return spmv_launch<VT, VT, false, EpiStore<VT>, true>(m, xs, epi);
         return spmv_launch<VT, VT, false, EpiStore<VT>, false>(m, xs, epi);

@@ -28,9 +28,12 @@
  *   cfd_amg_apply            Preconditioner::apply_to (z = 0, one V-cycle), amg.rs:507-557
  *   cfd_amg_stats            AMGStatistics, multigrid/mod.rs:366-395
  *   cfd_jacobi_*             DiagJacobi, crates/cfd-1d/src/solver/core/linear_system.rs:270-332
- *   cfd_batch_solve          LinearSystemSolver::solve_with_initial_guess called once per network
+ *   cfd_batch_linear_system_solve
+ *                            LinearSystemSolver::solve_with_initial_guess called once per network
  *                            (crates/cfd-1d/src/solver/core/linear_system.rs:114-155) by the
  *                            cfd-optim candidate fold (crates/cfd-optim/src/metrics/blueprint_graph.rs:48-135)
+ *   cfd_batch_solve          krylov::cg_preconditioned with DiagJacobi per system (krylov.rs:318-343,
+ *                            linear_system.rs:270-332), stopping on the 1-D solver's equilibrated residual
  *   cfd_adjoint_*            no reference counterpart (new differentiable-solve layer; see each entry)
  */
 #ifndef CFDGPU_H
@@ -106,6 +109,9 @@ typedef struct {
   int64_t staged_x_entries;  /* cfd_layout_check only: x entries staged over all blocks */
   int32_t path_f32;          /* SpMV pipeline an SpMV runs per precision (cfd_spmv_path; TIMED until timed) */
   int32_t path_f64;
+  int32_t sliced;            /* the sliced layout (CFD_PATH_SLICED) is built */
+  int32_t pad;
+  int64_t sliced_slots;      /* its slots (stored nonzeros plus padding) */
 } cfd_layout_info;
 cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out);
 /* SpMV pipelines. All sum every row in the same order, so y = A x is identical
@@ -113,16 +119,20 @@ cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out);
  * pipeline's own grid (deterministic for a pipeline, equal to rounding across
  * pipelines). SPLIT takes any matrix, RECORD needs every block coded (otherwise it
  * runs as SPLIT), X_STAGED needs x staging and a 16-byte aligned x (otherwise
- * it runs as RECORD). AUTO (the default): RECORD for FP32; X_STAGED for FP64
- * when eligible with one thread per row, SPLIT otherwise. TIMED: at the next SpMV in that
- * precision, time the eligible pipelines (allocates scratch vectors) and keep
- * the fastest. */
+ * it runs as RECORD). SLICED (FP32 only) needs the sliced layout: one thread
+ * per row, rows of at most 32 entries in slices of 32 rows padded by at most
+ * 15 %, at most 255 column offsets per 512 rows (otherwise it runs as RECORD).
+ * AUTO (the default): SLICED for FP32 when eligible, else RECORD; X_STAGED for
+ * FP64 when eligible with one thread per row, SPLIT otherwise. TIMED: at the
+ * next SpMV in that precision, time the eligible pipelines (allocates scratch
+ * vectors) and keep the fastest. */
 typedef enum {
   CFD_PATH_TIMED = -2,
   CFD_PATH_AUTO = -1,
   CFD_PATH_SPLIT = 0,
   CFD_PATH_RECORD = 1,
-  CFD_PATH_X_STAGED = 2
+  CFD_PATH_X_STAGED = 2,
+  CFD_PATH_SLICED = 3
 } cfd_spmv_path;
 /* Set the pipeline of one precision (fp32 != 0: FP32 values). CFD_ERR_CONFIG
  * when the matrix is not eligible for it. */
@@ -312,11 +322,13 @@ cfd_status cfd_block_diagonal_host(int64_t n, const int64_t* row_ptr, const int3
 
 /* ---- batched small systems --------------------------------------------
  * Many independent systems (e.g. the Kirchhoff networks of many design
- * candidates) solved by Jacobi-PCG in one persistent launch per size bucket,
- * replayed from a captured CUDA graph. Replaces calling
- * LinearSystemSolver::solve_with_initial_guess once per network
- * (crates/cfd-1d/src/solver/core/linear_system.rs:114-155) from the cfd-optim
- * candidate fold (crates/cfd-optim/src/metrics/blueprint_graph.rs:48-135).
+ * candidates, solved one per call by the cfd-optim candidate fold,
+ * crates/cfd-optim/src/metrics/blueprint_graph.rs:48-135). cfd_batch_solve:
+ * Jacobi-PCG (krylov::cg_preconditioned with DiagJacobi) on each system as
+ * given, in one persistent launch per size bucket replayed from a captured
+ * CUDA graph. cfd_batch_linear_system_solve (below): the 1-D solver's full
+ * cascade, LinearSystemSolver::solve_with_initial_guess
+ * (crates/cfd-1d/src/solver/core/linear_system.rs:114-155).
  * Layout: system s owns global rows [sys_row_offsets[s], sys_row_offsets[s+1]);
  * row_ptr holds global nonzero offsets (total_rows + 1 entries); col holds the
  * column index LOCAL to the row's system. At most 2048 rows and 8192 nonzeros
@@ -332,6 +344,10 @@ typedef struct {
   int32_t pad;
   double max_rel_residual;    /* largest final equilibrated relative residual */
   double device_ms;           /* copies in, graph, copies out (CUDA events) */
+  /* cfd_batch_linear_system_solve only (0 otherwise), device time of its
+   * phases: the dense solves of the systems of at most 256 rows, the Krylov
+   * launches, and the dense fallback of the Krylov solves not kept. */
+  double direct_ms, krylov_ms, fallback_ms;
 } cfd_batch_report;
 cfd_status cfd_batch_create(cfd_context* ctx, int32_t num_systems, const int64_t* sys_row_offsets,
                             const int64_t* row_ptr, const int32_t* col, const double* val,
@@ -345,6 +361,56 @@ cfd_status cfd_batch_update_values(cfd_batch* batch, const double* val_host);
 cfd_status cfd_batch_solve(cfd_batch* batch, const cfd_solve_options* opt, const double* b, double* x,
                            const cfd_solver_config* cfg, int32_t* termination, int32_t* iterations,
                            double* rel_residual, cfd_batch_report* rep);
+/* The 1-D network solve, LinearSystemSolver::solve_with_initial_guess
+ * (crates/cfd-1d/src/solver/core/linear_system.rs:114-155), for every system
+ * of the batch, with the method of NetworkSolver::detect_solver_method
+ * (crates/cfd-1d/src/solver/core/solver_detection.rs:36-64) or a fixed one
+ * (LinearSystemSolver::with_method). Per system:
+ *   rows equilibrated by D = 1 / max_j |a_ij| (identity where that maximum is
+ *   not above f64::EPSILON or not finite, linear_system.rs:157-186);
+ *   n <= 256: dense LU (partial pivoting) of D A x = D b, kept when
+ *   ||D (A x - b)|| <= tolerance * ||D b|| (:188-204), else dense LU of A x = b;
+ *   n > 256: CG or BiCGSTAB on D A x = D b with DiagJacobi(D A) (identity where
+ *   |d_ii| <= f64::EPSILON), IterativeSolverConfig::new(tolerance): stop at
+ *   ||D b - D A x||_2 <= tolerance or after max_iterations; kept when it
+ *   converged and the target above holds, else dense LU of A x = b.
+ * Not restated: the QR least-squares solve the reference tries when a dense LU
+ * meets a zero pivot; such a system is reported CFD_LS_PATH_FAILED. A
+ * non-finite diagonal of D A (DiagJacobi::new's Err) is CFD_LS_PATH_ERROR.
+ * FP32_REFINE runs the Krylov iterations in FP32 inside FP64 refinement of
+ * the equilibrated system (the dense solves stay FP64). x carries the initial
+ * guesses in and the solutions out; b may be NULL after cfd_batch_assemble.
+ * results (num_systems entries, host) may be NULL. The dense solves use a
+ * device scratch of one n x n FP64 matrix per CTA, allocated on first need
+ * and kept by the batch. */
+typedef enum { CFD_LS_CG = 0, CFD_LS_BICGSTAB = 1, CFD_LS_DETECT = 2 } cfd_ls_method;
+typedef enum {
+  CFD_LS_PATH_KRYLOV = 0,          /* the Krylov solution was kept */
+  CFD_LS_PATH_DIRECT = 1,          /* dense LU of the equilibrated system (n <= 256) */
+  CFD_LS_PATH_DIRECT_UNSCALED = 2, /* dense LU of A x = b after the first missed the target (n <= 256) */
+  CFD_LS_PATH_KRYLOV_FALLBACK = 3, /* dense LU of A x = b after a Krylov solve that was not kept */
+  CFD_LS_PATH_FAILED = 4,          /* the last dense LU met a zero pivot */
+  CFD_LS_PATH_ERROR = 5            /* non-finite diagonal of D A */
+} cfd_ls_path;
+typedef struct {
+  double tolerance;        /* LinearSystemSolver::with_tolerance (default 1e-6) */
+  int64_t max_iterations;  /* LinearSystemSolver::with_max_iterations (default 1000) */
+  int32_t method;          /* cfd_ls_method (default CFD_LS_DETECT) */
+  int32_t precision;       /* cfd_precision */
+  int32_t memory;          /* cfd_memory of b and x */
+  int32_t max_outer;       /* FP32_REFINE: refinement steps cap */
+  double inner_tolerance;  /* FP32_REFINE: inner relative tolerance */
+} cfd_ls_options;
+typedef struct {
+  int32_t method;       /* cfd_ls_method used (CG or BiCGSTAB) */
+  int32_t path;         /* cfd_ls_path */
+  int32_t termination;  /* of the Krylov solve (cfd_termination), -1 when none ran */
+  int32_t iterations;   /* Krylov iterations */
+  double residual;      /* ||D (A x - b)|| / ||D b|| of the returned x */
+} cfd_ls_result;
+void cfd_ls_options_default(cfd_ls_options* opt);
+cfd_status cfd_batch_linear_system_solve(cfd_batch* batch, const cfd_ls_options* opt, const double* b, double* x,
+                                         cfd_ls_result* results, cfd_batch_report* rep);
 /* Time each CTA width (32..512 threads) per size bucket on this batch with a
  * fixed iteration budget and keep the fastest (per precision). */
 cfd_status cfd_batch_autotune(cfd_batch* batch, int32_t precision, int32_t sample_iterations);

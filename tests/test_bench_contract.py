@@ -58,8 +58,9 @@ def test_reference_arm_plain_workload():
 
 
 def test_reference_arm_batched_networks():
-    """--workload c4: the oracle on every 16th of the 4096 networks, one serial
-    Jacobi-PCG per network on worker threads, scaled to the whole batch."""
+    """--workload c4: the oracle on every 16th of the 4096 networks, the 1-D
+    solve of each (LinearSystemSolver cascade) on worker threads, scaled to the
+    whole batch; Jacobi-PCG per network beside it."""
     out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--workload", "c4", "--steps", "1",
                           "--warmup", "1"], cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
@@ -67,7 +68,9 @@ def test_reference_arm_batched_networks():
     assert len(lines) == 1
     d = lines[0]
     assert d["impl"] == "reference" and d["value"] > 0 and d["config"]["systems"] == 4096
-    assert d["converged_systems_in_sample"] == 256
+    paths = d["paths_in_sample"]
+    assert sum(paths.values()) == 256 and "failed" not in paths and "error" not in paths
+    assert d["jacobi_pcg_ms"] > 0
     assert d["cpu_baseline"]["value"] == d["value"] and "every 16th" in d["cpu_baseline"]["sample"]
 
 

@@ -110,10 +110,10 @@ def test_spmv_vs_oracle(cuda, oracle, shape):
 @pytest.mark.parametrize("shape", ["stencil", "stencil_tail", "empty_blocks", "narrow", "prolongation",
                                    "restriction", "coarse_operator", "mixed"])
 def test_spmv_pipelines_bit_identical(cuda, shape):
-    """Every SpMV pipeline a matrix is eligible for (split, record, x-staged)
-    sums each row in the same order: FP64 and FP32 results are bit-identical,
-    and an x-staged request with an x that is not 16-byte aligned runs on the
-    record pipeline with the same result."""
+    """Every SpMV pipeline a matrix is eligible for (split, record, x-staged,
+    and for FP32 the sliced one) sums each row in the same order: FP64 and FP32
+    results are bit-identical, and an x-staged request with an x that is not
+    16-byte aligned runs on the record pipeline with the same result."""
     from cfdrs_b200.device import DeviceCsr
     A, staged = spmv_case(shape)
     d = DeviceCsr(A)
@@ -129,7 +129,7 @@ def test_spmv_pipelines_bit_identical(cuda, shape):
         buf[1:] = xa
         assert buf[1:].data_ptr() % 16 != 0
         ys = []
-        for path in paths:
+        for path in paths + (["sliced"] if fp32 and lay["sliced"] else []):
             d.set_path(path, fp32)
             for xp in ((xa, buf[1:]) if path == "x_staged" else (xa,)):
                 y = cuda.full((A.nrows,), float("nan"), device="cuda", dtype=dt)
@@ -145,9 +145,10 @@ def test_spmv_pipelines_bit_identical(cuda, shape):
             cuda.cuda.synchronize()
             assert cuda.equal(ys[0][1], y), f"{shape} {dt} {mode}"
             chosen = d.layout()["path_f32" if fp32 else "path_f64"]
-            assert chosen in [{"split": 0, "record": 1, "x_staged": 2}[p] for p in paths]
+            eligible = paths + (["sliced"] if fp32 and lay["sliced"] else [])
+            assert chosen in [{"split": 0, "record": 1, "x_staged": 2, "sliced": 3}[p] for p in eligible]
             if mode == "auto" and fp32:
-                assert chosen == (1 if lay["all_compressed"] else 0)
+                assert chosen == (3 if lay["sliced"] else 1 if lay["all_compressed"] else 0)
 
 @pytest.mark.parametrize("interp,order", [(0, 0), (2, 0), (2, 1)])
 def test_amg_hierarchy_matches_oracle(cuda, oracle, interp, order):

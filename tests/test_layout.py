@@ -106,3 +106,45 @@ def test_degenerate_shapes():
 def test_networks():
     for A, _ in P.network_batch(4, seed=5, n_min=200, n_max=900):
         check(A)
+
+
+def test_sliced_layout_on_stencils_and_levels(oracle):
+    """The sliced layout (one warp per 32-row slice, slot-major values and
+    codes) is built for one-thread rows with little padding and checked slot by
+    slot against the CSR columns (cfd_layout_check runs check_sliced): the
+    7-point and 5-point operators get it with under 1 % padding; every operator
+    of a hierarchy is checked when it qualifies."""
+    for A in (P.poisson_3d_variable(33, 4.0, 1.0, seed=2)[0], P.poisson_2d_dirichlet(70, seed=0)[0],
+              grid_laplacian(41)):
+        info = check(A)
+        assert info["sliced"] == 1
+        assert A.nnz <= info["sliced_slots"] <= 1.01 * A.nnz + 32 * 32
+    A = P.poisson_3d_variable(24, 8.0, 1.0, seed=0)[0]
+    amg = oracle.Amg(oracle.Csr.from_matrix(A), oracle.AmgConfig(
+        smoother=oracle.SMOOTH_JACOBI, relaxation=2 / 3, pre_smooth=1, post_smooth=1, interpolation=2,
+        coarse_order=1, min_coarse_size=50, coarse_solve=oracle.COARSE_DENSE))
+    sliced = 0
+    for l in range(amg.num_levels):
+        for which in ((0, 1, 2) if l < amg.num_levels - 1 else (0,)):
+            rp, ci, v, shape = amg.level(l, which).arrays()
+            info = check(CsrMatrix(rp, ci, v, shape), seed=l)
+            if info["sliced"]:
+                sliced += 1
+                assert info["sliced_slots"] <= 1.15 * len(ci) + 1
+    assert sliced >= 1
+
+
+def test_sliced_layout_refused_where_it_does_not_pay():
+    rng = np.random.default_rng(9)
+    # rows of 1 to 30 entries: padding far above 15 %
+    assert check(random_csr(rng, 2000, 2000, rng.integers(1, 31, 2000)))["sliced"] == 0
+    # a row longer than 32 entries
+    lens = np.full(500, 5)
+    lens[77] = 40
+    assert check(random_csr(rng, 500, 500, lens))["sliced"] == 0
+    # an empty matrix, and a single entry (one slice of 32 slots for one nonzero)
+    assert check(csr_from_lists([0, 0, 0], [], [], 4))["sliced"] == 0
+    assert check(csr_from_lists([0, 1], [0], [2.0], 1))["sliced"] == 0
+    # a diagonal of 250 rows: the last slice is partial (rows past the end are padding)
+    n = 250
+    assert check(csr_from_lists(list(range(n + 1)), list(range(n)), [2.0] * n, n))["sliced"] == 1
