@@ -42,7 +42,7 @@ class AmgConfigC(C.Structure):
                 ("interpolation", C.c_int32), ("smoother", C.c_int32), ("pre_smooth", C.c_int32),
                 ("post_smooth", C.c_int32), ("relaxation", C.c_double), ("strength_threshold", C.c_double),
                 ("coarse_solve", C.c_int32), ("coarse_sweeps", C.c_int32), ("aggregate_size", C.c_int64),
-                ("seed", C.c_uint64), ("coarse_order", C.c_int32), ("reserved", C.c_int32)]
+                ("seed", C.c_uint64), ("coarse_order", C.c_int32), ("max_interp_points", C.c_int32)]
 
 
 class AmgStatsC(C.Structure):

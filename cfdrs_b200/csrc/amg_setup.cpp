@@ -541,6 +541,50 @@ bool dense_inverse(const HostCsr& a, std::vector<double>& inv) {
   return true;
 }
 
+// Interpolation truncation (cfd_amg_config::max_interp_points): in every row
+// of P with more than k weights keep the k of largest magnitude (ties: the
+// smaller column) and scale them by (sum of all weights) / (sum of the kept
+// ones), both sums taken in ascending column order, so the row sum is kept.
+HostCsr truncate_interpolation(const HostCsr& p, int k) {
+  if (k <= 0) return p;
+  HostCsr t;
+  t.nrows = p.nrows;
+  t.ncols = p.ncols;
+  t.rp.assign(p.nrows + 1, 0);
+  std::vector<std::vector<std::pair<int32_t, double>>> rows(p.nrows);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t i = 0; i < p.nrows; ++i) {
+    const int64_t a = p.rp[i], b = p.rp[i + 1];
+    auto& out = rows[i];
+    if (b - a <= k) {
+      for (int64_t e = a; e < b; ++e) out.emplace_back(p.ci[e], p.v[e]);
+      continue;
+    }
+    std::vector<int64_t> order;
+    for (int64_t e = a; e < b; ++e) order.push_back(e);
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
+      const double ax = std::fabs(p.v[x]), ay = std::fabs(p.v[y]);
+      return ax != ay ? ax > ay : p.ci[x] < p.ci[y];
+    });
+    order.resize(k);
+    std::sort(order.begin(), order.end());
+    double all = 0.0, kept = 0.0;
+    for (int64_t e = a; e < b; ++e) all += p.v[e];
+    for (int64_t e : order) kept += p.v[e];
+    const double scale = kept != 0.0 ? all / kept : 1.0;
+    for (int64_t e : order) out.emplace_back(p.ci[e], p.v[e] * scale);
+  }
+  for (int64_t i = 0; i < p.nrows; ++i) t.rp[i + 1] = t.rp[i] + (int64_t)rows[i].size();
+  t.ci.resize(t.rp[p.nrows]);
+  t.v.resize(t.rp[p.nrows]);
+  for (int64_t i = 0; i < p.nrows; ++i)
+    for (size_t q = 0; q < rows[i].size(); ++q) {
+      t.ci[t.rp[i] + q] = rows[i][q].first;
+      t.v[t.rp[i] + q] = rows[i][q].second;
+    }
+  return t;
+}
+
 // Renumber the coarse points by ascending fine index (f2c follows).
 void renumber_ascending(Coarsening& c) {
   std::vector<int32_t> sorted(c.coarse_points);
@@ -572,6 +616,7 @@ std::vector<HostLevel> build_hierarchy(const HostCsr& a, const cfd_amg_config& c
     HostCsr p = cfg.interpolation == CFD_INTERP_DIRECT               ? direct_interpolation(c, cur.nrows)
                 : cfg.interpolation == CFD_INTERP_MODIFIED_CLASSICAL ? modified_classical_interpolation(cur, c)
                                                                      : classical_interpolation(cur, c);
+    if (cfg.max_interp_points > 0) p = truncate_interpolation(p, cfg.max_interp_points);
     HostCsr r = transpose(p);
     HostCsr ac = spgemm(spgemm(r, cur), p);
     levels.back().P = std::move(p);

@@ -753,7 +753,8 @@ cfd_status cfd_batch_destroy(cfd_batch* bt) {
   for (void* p : {(void*)bt->sys_row, (void*)bt->rp, (void*)bt->col, (void*)bt->v64, (void*)bt->v32, (void*)bt->x,
                   (void*)bt->b, (void*)bt->term, (void*)bt->iters, (void*)bt->resid, (void*)bt->order,
                   (void*)bt->queues, (void*)bt->params, (void*)bt->ls_method, (void*)bt->ls_path,
-                  (void*)bt->ls_list, (void*)bt->ls_params, (void*)bt->ls_queue, (void*)bt->ls_scratch})
+                  (void*)bt->ls_list, (void*)bt->ls_params, (void*)bt->ls_queue, (void*)bt->ls_scratch,
+                  (void*)bt->ls_pivot})
     if (p) cudaFree(p);
   if (bt->h_params) cudaFreeHost(bt->h_params);
   network_plan_free(bt->net);

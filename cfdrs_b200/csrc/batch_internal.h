@@ -79,4 +79,6 @@ struct cfd_batch {
   unsigned* ls_queue = nullptr;
   double* ls_scratch = nullptr;
   size_t ls_scratch_elems = 0;
+  int* ls_pivot = nullptr;   // per system: the dense fast path's pivot guard fired
+  int64_t ls_pivoted = 0;    // systems handed to the pivoting dense solve, all calls
 };

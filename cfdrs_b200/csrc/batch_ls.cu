@@ -653,6 +653,279 @@ __global__ void __launch_bounds__(kLsThreads) k_ls_dense(LsArgs A, const int* __
   }
 }
 
+// ---- dense LU, blocked, without row exchanges (the common case) --------------
+// The same factorization as lu_solve for the systems on which partial
+// pivoting keeps every diagonal pivot: by panels of kFb columns, the
+// diagonal block is factored in shared memory, its triangular factors are
+// inverted there, and L21 = A21 U11^-1, U12 = L11^-1 A12 and A22 -= L21 U12
+// run as 64 x 64 shared-memory tile products (the right-hand side rides as
+// column n, so forward elimination is part of the factorization). Back
+// substitution runs panel by panel with the stored U11^-1. Partial pivoting
+// would exchange rows only where some |l_ik| > 1; a multiplier above 1 by more
+// than rounding (1e-8), or a zero or non-finite pivot, stops the fast path and
+// marks the system for lu_solve (pivot[sys] = 1), which starts it over.
+constexpr int kFb = 64;
+constexpr int kFld = kFb + 1;
+constexpr double kPivotSlack = 1e-8;
+constexpr size_t kFastSmem = 5 * (size_t)kFb * kFld * sizeof(double);
+
+__host__ __device__ constexpr size_t fast_slot_elems(int n) {
+  return (size_t)n * (n + 1) + (size_t)((n + kFb - 1) / kFb) * kFb * kFb + 64;
+}
+
+// dst[r][c] = M[(r0 + r) ld + c0 + c] for r < rows, c < cols, else 0. The
+// kernel runs kLsThreads threads (one CTA per SM): each issues all of its
+// kFb^2 / kLsThreads loads before the stores, so they are in flight together.
+constexpr int kFastPer = kFb * kFb / kLsThreads;
+__device__ __forceinline__ void fast_load(double (*dst)[kFld], const double* __restrict__ M, size_t ld, int r0,
+                                          int c0, int rows, int cols) {
+  double v[kFastPer];
+#pragma unroll
+  for (int t = 0; t < kFastPer; ++t) {
+    const int q = threadIdx.x + t * kLsThreads, r = q / kFb, c = q % kFb;
+    v[t] = (r < rows && c < cols) ? M[(size_t)(r0 + r) * ld + c0 + c] : 0.0;
+  }
+#pragma unroll
+  for (int t = 0; t < kFastPer; ++t) {
+    const int q = threadIdx.x + t * kLsThreads;
+    dst[q / kFb][q % kFb] = v[t];
+  }
+}
+
+// acc[a][q] = sum_c A[ty + 16 a][c] B[c][tx + 16 q], c < kb.
+__device__ __forceinline__ void fast_mm(const double (*A)[kFld], const double (*B)[kFld], int kb,
+                                        double (&acc)[4][4]) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
+  for (int c = 0; c < kb; ++c) {
+    double lv[4], uv[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) lv[a] = A[ty + 16 * a][c];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) uv[q] = B[c][tx + 16 * q];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[a][q] += lv[a] * uv[q];
+  }
+}
+
+// Factor and solve the n x n system in M (row stride n + 1, right-hand side in
+// column n); on success column n holds x. Returns false (uniformly) when the
+// pivot guard stops the fast path.
+__device__ bool lu_solve_fast(double* __restrict__ M, double* __restrict__ Uinv_store, int n, unsigned char* smem,
+                              int* s_bad, double* s_tmp) {
+  double(*Da)[kFld] = reinterpret_cast<double(*)[kFld]>(smem);
+  double(*Li)[kFld] = Da + kFb;
+  double(*Ui)[kFld] = Li + kFb;
+  double(*At)[kFld] = Ui + kFb;
+  double(*Bt)[kFld] = At + kFb;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int tx = tid & 15, ty = tid >> 4;
+  const size_t ld = (size_t)n + 1;
+  if (tid == 0) *s_bad = 0;
+  __syncthreads();
+  for (int k0 = 0, p = 0; k0 < n; k0 += kFb, ++p) {
+    const int kb = min(kFb, n - k0), m0 = k0 + kb;
+    fast_load(Da, M, ld, k0, k0, kb, kb);
+    __syncthreads();
+    for (int k = 0; k < kb; ++k) {
+      const double piv = Da[k][k];
+      if (tid == 0 && (!(fabs(piv) > 0.0) || !isfinite(piv))) *s_bad = 1;
+      for (int i = k + 1 + tid; i < kb; i += nt) {
+        const double v = Da[i][k];
+        if (fabs(v) > fabs(piv) * (1.0 + kPivotSlack)) *s_bad = 1;
+        Da[i][k] = v / piv;
+      }
+      __syncthreads();
+      const int w = kb - k - 1;
+      for (int q = tid; q < w * w; q += nt) {
+        const int i = k + 1 + q / w, j = k + 1 + q % w;
+        Da[i][j] -= Da[i][k] * Da[k][j];
+      }
+      __syncthreads();
+    }
+    if (*s_bad) return false;
+    // U11^-1 (upper) and L11^-1 (unit lower), one column per thread; zero elsewhere
+    for (int q = tid; q < kFb * kFb; q += nt) {
+      Ui[q / kFb][q % kFb] = 0.0;
+      Li[q / kFb][q % kFb] = 0.0;
+    }
+    __syncthreads();
+    if (tid < kb) {
+      const int j = tid;
+      Ui[j][j] = 1.0 / Da[j][j];
+      for (int i = j - 1; i >= 0; --i) {
+        double t = 0.0;
+        for (int k = i + 1; k <= j; ++k) t += Da[i][k] * Ui[k][j];
+        Ui[i][j] = -t / Da[i][i];
+      }
+      Li[j][j] = 1.0;
+      for (int i = j + 1; i < kb; ++i) {
+        double t = 0.0;
+        for (int k = j; k < i; ++k) t += Da[i][k] * Li[k][j];
+        Li[i][j] = -t;
+      }
+    }
+    __syncthreads();
+    for (int q = tid; q < kFb * kFb; q += nt) Uinv_store[(size_t)p * kFb * kFb + q] = Ui[q / kFb][q % kFb];
+    // L21 = A21 U11^-1
+    for (int rt = m0; rt < n; rt += kFb) {
+      const int rows = min(kFb, n - rt);
+      fast_load(At, M, ld, rt, k0, rows, kb);
+      __syncthreads();
+      double acc[4][4];
+      fast_mm(At, Ui, kb, acc);
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int r = ty + 16 * a, c = tx + 16 * q;
+          if (r < rows && c < kb) {
+            if (fabs(acc[a][q]) > 1.0 + kPivotSlack || !isfinite(acc[a][q])) *s_bad = 1;
+            M[(size_t)(rt + r) * ld + k0 + c] = acc[a][q];
+          }
+        }
+      __syncthreads();
+    }
+    if (*s_bad) return false;
+    // U12 = L11^-1 A12, the right-hand side column included
+    for (int ct = m0; ct <= n; ct += kFb) {
+      const int cols = min(kFb, n + 1 - ct);
+      fast_load(Bt, M, ld, k0, ct, kb, cols);
+      __syncthreads();
+      double acc[4][4];
+      fast_mm(Li, Bt, kb, acc);
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int r = ty + 16 * a, c = tx + 16 * q;
+          if (r < kb && c < cols) M[(size_t)(k0 + r) * ld + ct + c] = acc[a][q];
+        }
+      __syncthreads();
+    }
+    // A22 -= L21 U12 (columns through the right-hand side)
+    for (int rt = m0; rt < n; rt += kFb) {
+      const int rows = min(kFb, n - rt);
+      fast_load(At, M, ld, rt, k0, rows, kb);
+      for (int ct = m0; ct <= n; ct += kFb) {
+        const int cols = min(kFb, n + 1 - ct);
+        fast_load(Bt, M, ld, k0, ct, kb, cols);
+        __syncthreads();
+        // this thread's C entries are loaded before the product, so their
+        // latency overlaps it
+        double cv[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int r = ty + 16 * a, c = tx + 16 * q;
+            cv[a][q] = (r < rows && c < cols) ? M[(size_t)(rt + r) * ld + ct + c] : 0.0;
+          }
+        double acc[4][4];
+        fast_mm(At, Bt, kb, acc);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int r = ty + 16 * a, c = tx + 16 * q;
+            if (r < rows && c < cols) M[(size_t)(rt + r) * ld + ct + c] = cv[a][q] - acc[a][q];
+          }
+        __syncthreads();
+      }
+    }
+  }
+  // back substitution by panels, from the last: x_p = U11^-1 (y_p - U12 x_rest)
+  const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  const int np = (n + kFb - 1) / kFb;
+  for (int p = np - 1; p >= 0; --p) {
+    const int k0 = p * kFb, kb = min(kFb, n - k0), m0 = k0 + kb;
+    for (int i = warp; i < kb; i += nw) {
+      double t = 0.0;
+      for (int j = m0 + lane; j < n; j += 32) t += M[(size_t)(k0 + i) * ld + j] * M[(size_t)j * ld + n];
+      t = warp_sum(t);
+      if (lane == 0) s_tmp[i] = M[(size_t)(k0 + i) * ld + n] - t;
+    }
+    __syncthreads();
+    for (int i = tid; i < kb; i += nt) {
+      double t = 0.0;
+      for (int k = 0; k < kb; ++k) t += Uinv_store[(size_t)p * kFb * kFb + i * kFb + k] * s_tmp[k];
+      M[(size_t)(k0 + i) * ld + n] = t;
+    }
+    __syncthreads();
+  }
+  return true;
+}
+
+// Dense solves of the listed systems on the fast path (modes as k_ls_dense);
+// a system whose pivot guard fires gets pivot[sys] = 1 and is left to k_ls_dense.
+__global__ void __launch_bounds__(kLsThreads) k_ls_dense_fast(LsArgs A, const int* __restrict__ list, int count,
+                                                             int direct, unsigned* queue, double* scratch,
+                                                             size_t slot_elems, const LsParams* __restrict__ prm,
+                                                             int* pivot) {
+  extern __shared__ __align__(16) unsigned char fsm[];
+  __shared__ double red[2][2][32];
+  __shared__ double s_tmp[kFb];
+  __shared__ int s_k, s_bad;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double* slot = scratch + (size_t)blockIdx.x * slot_elems;
+  int rslot = 0;
+  const double tol = prm->tol;
+  for (;;) {
+    if (tid == 0) s_k = (int)atomicAdd(queue, 1u);
+    __syncthreads();
+    const int q = s_k;
+    __syncthreads();
+    if (q >= count) break;
+    const int sys = list[q];
+    const int r0 = A.sys_row[sys], n = A.sys_row[sys + 1] - r0;
+    const size_t ld = (size_t)n + 1;
+    double* M = slot;
+    double* Uinv = slot + (size_t)n * ld;
+    int path = direct ? CFD_LS_PATH_DIRECT : A.path[sys];
+    double ratio = NAN;
+    bool need_pivot = false;
+    for (int attempt = direct ? 0 : 1; attempt < 2; ++attempt) {
+      const bool scaled = attempt == 0;
+      for (size_t e = tid; e < (size_t)n * ld; e += nt) M[e] = 0.0;
+      __syncthreads();
+      for (int i = tid; i < n; i += nt) {
+        const int g = r0 + i, e0 = A.rp[g], e1 = A.rp[g + 1];
+        const double s = scaled ? ls_scale(A.v64, e0, e1) : 1.0;
+        for (int e = e0; e < e1; ++e) M[(size_t)i * ld + A.col[e]] += A.v64[e] * s;
+        M[(size_t)i * ld + n] = A.b[g] * s;
+      }
+      __syncthreads();
+      if (!lu_solve_fast(M, Uinv, n, fsm, &s_bad, s_tmp)) {
+        need_pivot = true;
+        break;
+      }
+      for (int i = tid; i < n; i += nt) A.x[r0 + i] = M[(size_t)i * ld + n];
+      __syncthreads();
+      ratio = ls_target_ratio(A, r0, n, red, rslot);
+      if (!scaled || ratio <= tol) break;
+      path = CFD_LS_PATH_DIRECT_UNSCALED;
+      __syncthreads();
+    }
+    if (tid == 0) {
+      pivot[sys] = need_pivot ? 1 : 0;
+      if (!need_pivot) {
+        A.path[sys] = path;
+        A.resid[sys] = ratio;
+        if (direct) {
+          A.term[sys] = -1;
+          A.iters[sys] = 0;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Detection alone for the direct systems (the method is reported for every system).
 __global__ void k_ls_detect(LsArgs A, const int* __restrict__ list, int count, int fixed) {
   const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
@@ -699,6 +972,7 @@ cfd_status ls_prepare(cfd_batch* bt) {
   CFD_TRY(ls_alloc(&bt->ls_list, bt->nsys));
   CFD_TRY(ls_alloc(&bt->ls_params, (int64_t)((sizeof(LsParams) + 7) / 8)));
   CFD_TRY(ls_alloc(&bt->ls_queue, 2));
+  CFD_TRY(ls_alloc(&bt->ls_pivot, bt->nsys));
   return CFD_OK;
 }
 
@@ -718,22 +992,51 @@ cfd_status ls_ensure_scratch(cfd_batch* bt, size_t slot_elems, int slots) {
   return CFD_OK;
 }
 
-// One dense launch over `list` (host, count entries, all of at most nmax rows).
+// Dense solves of `list` (host, systems of at most nmax rows): the blocked
+// fast path for all, then lu_solve for the systems whose pivot guard fired.
 cfd_status ls_dense_launch(cfd_batch* bt, const LsArgs& A, const std::vector<int>& list, int nmax, bool direct,
                            cudaStream_t s) {
   if (list.empty()) return CFD_OK;
+  const LsParams* prm = reinterpret_cast<const LsParams*>(bt->ls_params);
+  if (cudaFuncSetAttribute(k_ls_dense_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFastSmem) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    set_error("cfd_batch_linear_system_solve: %zu bytes of shared memory for the dense solve are not available",
+              kFastSmem);
+    return CFD_ERR_CONFIG;
+  }
   int occ = 0;
-  CFD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ls_dense, kLsThreads, 0));
-  const size_t slot = (size_t)nmax * nmax + (size_t)nmax + 16;
-  // Enough CTAs to fill the GPU, no more slots than systems; large slots are
-  // capped at one CTA per SM.
+  CFD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ls_dense_fast, kLsThreads, kFastSmem));
   int grid = std::min<int>((int)list.size(), bt->ctx->num_sms * std::max(1, occ));
-  if (nmax > 512) grid = std::min(grid, bt->ctx->num_sms);
+  const size_t slot = fast_slot_elems(nmax);
   CFD_TRY(ls_ensure_scratch(bt, slot, grid));
   CFD_TRY_CUDA(cudaMemcpyAsync(bt->ls_list, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   CFD_TRY_CUDA(cudaMemsetAsync(bt->ls_queue, 0, sizeof(unsigned), s));
-  k_ls_dense<<<grid, kLsThreads, 0, s>>>(A, bt->ls_list, (int)list.size(), direct ? 1 : 0, bt->ls_queue,
-                                         bt->ls_scratch, slot, reinterpret_cast<const LsParams*>(bt->ls_params));
+  k_ls_dense_fast<<<grid, kLsThreads, kFastSmem, s>>>(A, bt->ls_list, (int)list.size(), direct ? 1 : 0,
+                                                      bt->ls_queue, bt->ls_scratch, slot, prm, bt->ls_pivot);
+  CFD_TRY_CUDA(cudaGetLastError());
+  bt->ctx->stats.launches++;
+  std::vector<int> piv(bt->nsys);
+  CFD_TRY_CUDA(cudaMemcpyAsync(piv.data(), bt->ls_pivot, bt->nsys * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CFD_TRY_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> slow;
+  int smax = 1;
+  for (int sy : list)
+    if (piv[sy]) {
+      slow.push_back(sy);
+      smax = std::max(smax, bt->h_sys_row[sy + 1] - bt->h_sys_row[sy]);
+    }
+  bt->ls_pivoted += (int64_t)slow.size();
+  if (slow.empty()) return CFD_OK;
+  CFD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ls_dense, kLsThreads, 0));
+  grid = std::min<int>((int)slow.size(), bt->ctx->num_sms * std::max(1, occ));
+  if (smax > 512) grid = std::min(grid, bt->ctx->num_sms);
+  const size_t slot2 = (size_t)smax * smax + (size_t)smax + 16;
+  CFD_TRY(ls_ensure_scratch(bt, slot2, grid));
+  CFD_TRY_CUDA(cudaMemcpyAsync(bt->ls_list, slow.data(), slow.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  CFD_TRY_CUDA(cudaMemsetAsync(bt->ls_queue, 0, sizeof(unsigned), s));
+  k_ls_dense<<<grid, kLsThreads, 0, s>>>(A, bt->ls_list, (int)slow.size(), direct ? 1 : 0, bt->ls_queue,
+                                         bt->ls_scratch, slot2, prm);
   CFD_TRY_CUDA(cudaGetLastError());
   bt->ctx->stats.launches++;
   return CFD_OK;

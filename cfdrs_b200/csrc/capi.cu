@@ -756,7 +756,7 @@ void cfd_amg_config_default(cfd_amg_config* c) {
   c->aggregate_size = 8;
   c->seed = 0;
   c->coarse_order = CFD_COARSE_ORDER_SELECTION;
-  c->reserved = 0;
+  c->max_interp_points = 0;
 }
 
 static cfd_status check_amg_config(const cfd_amg_config* cfg) {

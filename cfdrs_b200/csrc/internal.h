@@ -204,7 +204,6 @@ bool check_sliced(const HostCsr& h, uint64_t base_mult, const HostSliced& S, std
 inline int spmv_path(const DevMat& m, int p) {
   int path = m.path[p];
   if (path == CFD_PATH_TIMED) return path;
-  if (path == CFD_PATH_AUTO) path = p == 0 ? (m.sl ? CFD_PATH_SLICED : CFD_PATH_RECORD) : path;
   if (path == CFD_PATH_SLICED && (p != 0 || !m.sl)) path = p == 0 ? CFD_PATH_RECORD : CFD_PATH_AUTO;
   if (path == CFD_PATH_AUTO) path = p == 0 ? CFD_PATH_RECORD : (m.xs && m.tpr == 1 ? CFD_PATH_X_STAGED : CFD_PATH_SPLIT);
   if (path == CFD_PATH_X_STAGED && !m.xs) path = CFD_PATH_RECORD;

@@ -24,6 +24,7 @@
 
 #include <cfloat>
 #include <cmath>
+#include <type_traits>
 
 #include "internal.h"
 
@@ -246,7 +247,9 @@ struct EpiJacobi {
   __device__ void row(int i, S s, S d, const Pre& p, double* acc) const {
     XT out = p.xo;
     if (diag_ok<XT>((XT)d)) {
-      const XT nv = (p.b - (XT)s) / (XT)d;
+      // FP32 (inner) sweeps: the fast single-precision division (within 2 ulp)
+      const XT nv = std::is_same<XT, float>::value ? (XT)__fdividef((float)(p.b - (XT)s), (float)d)
+                                                   : (p.b - (XT)s) / (XT)d;
       out = p.xo + omega * (nv - p.xo);
     }
     xn[i] = out;
@@ -766,40 +769,66 @@ struct SlView {
   int nslices, nrows;
 };
 
+// One CTA per chunk of kSlChunkSlices slices (grid-stride over chunks): the
+// chunk's dictionary is staged in shared memory, each warp takes two slices,
+// and a slice is read in batches of kSlBatch slots whose code and value loads
+// are all issued before the x gathers they feed, which are again issued
+// together, so a warp has 2 x kSlBatch loads in flight instead of a chain.
+constexpr int kSlBatch = 8;
+
 template <typename XT, bool OFFDIAG, class Epi>
 __global__ void __launch_bounds__(kThreads) k_spmv_sl(SlView S, const XT* __restrict__ x, Epi epi) {
   if (epi.skip()) return;
+  __shared__ int sdict[256];
   double red[Epi::NRED > 0 ? Epi::NRED : 1];
 #pragma unroll
   for (int q = 0; q < (Epi::NRED > 0 ? Epi::NRED : 1); ++q) red[q] = 0.0;
-  const int lane = threadIdx.x & 31;
-  const int nw = gridDim.x * (kThreads / 32);
-  for (int sl = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5); sl < S.nslices; sl += nw) {
-    const int row = sl * kSlRows + lane;
-    const bool live = row < S.nrows;
-    typename Epi::Pre pre{};
-    if (live) pre = epi.load(row);
-    const int e0 = S.off[sl], e1 = S.off[sl + 1];
-    const int* __restrict__ dict = S.dict + S.doff[sl / kSlChunkSlices];
-    const int base = (int)(((unsigned long long)row * S.base_mult) >> 20);
-    float sum = 0.0f, diag = 0.0f;
-#pragma unroll 8
-    for (int q = e0 + lane; q < e1; q += kSlRows) {
-      const unsigned c = S.code[q];
-      const float v = S.val[q];
-      if (c != (unsigned)kSlPadCode) {
-        const int col = base + __ldg(dict + c);
-        const float xv = (float)__ldg(x + col);
-        if constexpr (OFFDIAG) {
-          const bool isd = (col == row);
-          diag = isd ? v : diag;
-          sum = isd ? sum : sum + v * xv;
-        } else {
-          sum += v * xv;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nchunks = (S.nslices + kSlChunkSlices - 1) / kSlChunkSlices;
+  for (int ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int d0 = S.doff[ch], nd = S.doff[ch + 1] - d0;
+    for (int q = threadIdx.x; q < 256; q += kThreads) sdict[q] = q < nd ? S.dict[d0 + q] : 0;
+    __syncthreads();
+    for (int sl = ch * kSlChunkSlices + warp; sl < min(S.nslices, (ch + 1) * kSlChunkSlices); sl += kThreads / 32) {
+      const int row = sl * kSlRows + lane;
+      const bool live = row < S.nrows;
+      typename Epi::Pre pre{};
+      if (live) pre = epi.load(row);
+      const int e0 = S.off[sl], w = (S.off[sl + 1] - e0) / kSlRows;
+      const int base = (int)(((unsigned long long)row * S.base_mult) >> 20);
+      float sum = 0.0f, diag = 0.0f;
+      for (int k0 = 0; k0 < w; k0 += kSlBatch) {
+        unsigned c[kSlBatch];
+        float v[kSlBatch], xv[kSlBatch];
+        int col[kSlBatch];
+#pragma unroll
+        for (int j = 0; j < kSlBatch; ++j) {
+          const int q = e0 + (k0 + j) * kSlRows + lane;
+          const bool ok = k0 + j < w;
+          c[j] = ok ? (unsigned)S.code[q] : (unsigned)kSlPadCode;
+          v[j] = ok ? S.val[q] : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < kSlBatch; ++j) {
+          col[j] = base + sdict[c[j]];
+          xv[j] = c[j] != (unsigned)kSlPadCode ? (float)__ldg(x + col[j]) : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < kSlBatch; ++j) {
+          if (c[j] != (unsigned)kSlPadCode) {
+            if constexpr (OFFDIAG) {
+              const bool isd = (col[j] == row);
+              diag = isd ? v[j] : diag;
+              sum = isd ? sum : sum + v[j] * xv[j];
+            } else {
+              sum += v[j] * xv[j];
+            }
+          }
         }
       }
+      if (live) epi.row(row, sum, diag, pre, red);
     }
-    if (live) epi.row(row, sum, diag, pre, red);
+    __syncthreads();
   }
   if constexpr (Epi::NRED > 0) {
     double tot[Epi::NRED];

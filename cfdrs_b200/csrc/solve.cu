@@ -48,14 +48,26 @@ inline int vec_grid(int64_t n) {
 // ---------------------------------------------------------------------------
 // Vector kernels.
 
-// First damped-Jacobi sweep from a zero iterate: x = w (b / a_ii).
+// First damped-Jacobi sweep from a zero iterate: x = w (b / a_ii). The FP32
+// (inner) sweep divides with the fast single-precision division (within 2 ulp;
+// the IEEE division's multi-instruction sequence made this pass compute-bound),
+// the FP64 sweep with the IEEE division.
+template <typename XT>
+__device__ __forceinline__ XT sweep_div(XT a, XT b) {
+  return a / b;
+}
+template <>
+__device__ __forceinline__ float sweep_div<float>(float a, float b) {
+  return __fdividef(a, b);
+}
+
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_smooth0(int64_t n, const XT* __restrict__ b, const XT* __restrict__ d,
                                                       XT omega, XT* __restrict__ x, const int* done) {
   if (flag_set(done)) return;
   GRID_STRIDE_U4(i, n, {
     const XT di = d[i];
-    x[i] = diag_ok<XT>(di) ? omega * (b[i] / di) : XT(0);
+    x[i] = diag_ok<XT>(di) ? omega * sweep_div<XT>(b[i], di) : XT(0);
   })
 }
 
@@ -580,10 +592,8 @@ struct Launcher {
       CFD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kThreads, 0));
       occ[ctx->device] = std::max(1, o);
     }
-    const int64_t warps_needed = m.sl_slices;
-    const int grid = (int)std::max<int64_t>(
-        1, std::min<int64_t>((warps_needed + kThreads / 32 - 1) / (kThreads / 32),
-                             (int64_t)ctx->num_sms * occ[ctx->device]));
+    const int64_t chunks = (m.sl_slices + kSlChunkSlices - 1) / kSlChunkSlices;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, (int64_t)ctx->num_sms * occ[ctx->device]));
     const SlView sv{m.sl_off, m.sl_code, m.sl_dict, m.sl_doff, m.sl_v32, (unsigned long long)m.base_mult,
                     (int)m.sl_slices, (int)m.nrows};
     kern<<<grid, kThreads, 0, s>>>(sv, x, epi);

@@ -62,6 +62,10 @@ class AMGConfig:
     aggregate_size: int = 8
     seed: int = 0
     coarse_order: CoarseOrder = CoarseOrder.SELECTION
+    # create_classical_interpolation's max_interpolation_points (interpolation.rs:42),
+    # ignored by the reference: 0 keeps every weight; k > 0 keeps the k largest per
+    # row of P, rescaled to the row sum.
+    max_interpolation_points: int = 0
 
     @classmethod
     def pressure_poisson(cls) -> "AMGConfig":
@@ -79,7 +83,8 @@ class AMGConfig:
                                int(self.interpolation_strategy), int(self.smoother_type),
                                self.pre_smooth_iterations, self.post_smooth_iterations, self.relaxation_factor,
                                self.strength_threshold, int(self.coarse_solve), self.coarse_sweeps,
-                               self.aggregate_size, self.seed, int(self.coarse_order), 0)
+                               self.aggregate_size, self.seed, int(self.coarse_order),
+                               int(self.max_interpolation_points))
 
 
 @dataclass

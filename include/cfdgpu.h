@@ -122,8 +122,9 @@ cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out);
  * it runs as RECORD). SLICED (FP32 only) needs the sliced layout: one thread
  * per row, rows of at most 32 entries in slices of 32 rows padded by at most
  * 15 %, at most 255 column offsets per 512 rows (otherwise it runs as RECORD).
- * AUTO (the default): SLICED for FP32 when eligible, else RECORD; X_STAGED for
- * FP64 when eligible with one thread per row, SPLIT otherwise. TIMED: at the
+ * AUTO (the default): RECORD for FP32 (on the 256^3 fine operator SLICED runs
+ * the plain SpMV as fast and the fused epilogues slower); X_STAGED for FP64
+ * when eligible with one thread per row, SPLIT otherwise. TIMED: at the
  * next SpMV in that precision, time the eligible pipelines (allocates scratch
  * vectors) and keep the fastest. */
 typedef enum {
@@ -182,7 +183,12 @@ typedef struct {
   int64_t aggregate_size;      /* aggregation coarsening (reference passes 8, amg.rs:304) */
   uint64_t seed;               /* PMIS priorities (the reference draws them unseeded) */
   int32_t coarse_order;        /* cfd_coarse_order: numbering of each level's coarse points */
-  int32_t reserved;
+  /* The max_interpolation_points argument of create_classical_interpolation
+   * (interpolation.rs:42), which the reference accepts and ignores: 0 keeps
+   * every weight (the reference); k > 0 keeps the k weights of largest
+   * magnitude in each row of P (ties: the smaller column), scaled so that the
+   * row sum of P is unchanged. */
+  int32_t max_interp_points;
 } cfd_amg_config;
 
 void cfd_amg_config_default(cfd_amg_config* cfg);

@@ -495,6 +495,46 @@ or_csr modified_classical_interp(const or_csr& a, const std::vector<int64_t>& cp
   return p;
 }
 
+// Truncation of the interpolation rows (the max_interpolation_points argument
+// of interpolation.rs:42, unused by the reference): rows with more than k
+// weights keep the k of largest magnitude (ties: the smaller column), scaled by
+// (sum of all) / (sum of kept), both summed in ascending column order.
+or_csr truncate_interp(const or_csr& p, int k) {
+  if (k <= 0) return p;
+  or_csr t;
+  t.nrows = p.nrows;
+  t.ncols = p.ncols;
+  t.rp.assign(p.nrows + 1, 0);
+  for (int64_t i = 0; i < p.nrows; ++i) {
+    const int64_t a = p.rp[i], b = p.rp[i + 1];
+    if (b - a <= k) {
+      for (int64_t e = a; e < b; ++e) {
+        t.ci.push_back(p.ci[e]);
+        t.v.push_back(p.v[e]);
+      }
+    } else {
+      std::vector<int64_t> order;
+      for (int64_t e = a; e < b; ++e) order.push_back(e);
+      std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
+        const double ax = std::fabs(p.v[x]), ay = std::fabs(p.v[y]);
+        return ax != ay ? ax > ay : p.ci[x] < p.ci[y];
+      });
+      order.resize(k);
+      std::sort(order.begin(), order.end());
+      double all = 0.0, kept = 0.0;
+      for (int64_t e = a; e < b; ++e) all += p.v[e];
+      for (int64_t e : order) kept += p.v[e];
+      const double scale = kept != 0.0 ? all / kept : 1.0;
+      for (int64_t e : order) {
+        t.ci.push_back(p.ci[e]);
+        t.v.push_back(p.v[e] * scale);
+      }
+    }
+    t.rp[i + 1] = (int64_t)t.ci.size();
+  }
+  return t;
+}
+
 // create_direct_interpolation, interpolation.rs:191-217.
 or_csr direct_interp(const std::vector<int64_t>& f2c, int64_t n, int64_t nc) {
   or_csr p;
@@ -807,6 +847,7 @@ or_amg* or_amg_setup(const or_csr* a, const or_amg_config* cfg) {
     or_csr p = cfg->interpolation == 0   ? classical_interp(cur, cp, s)
                : cfg->interpolation == 2 ? modified_classical_interp(cur, cp, s)
                                          : direct_interp(map, cur.nrows, nc);
+    if (cfg->max_interp_points > 0) p = truncate_interp(p, cfg->max_interp_points);
     or_csr r = transpose(p);
     or_csr ra = spgemm(r, cur);
     or_csr ac = spgemm(ra, p);

@@ -83,7 +83,8 @@ typedef struct {
   int64_t aggregate_size;  /* reference: 8 */
   uint64_t seed;           /* PMIS priorities */
   int32_t coarse_order;    /* 0 selection order (reference), 1 ascending fine index */
-  int32_t pad;
+  int32_t max_interp_points; /* 0: every weight (the reference ignores the argument, interpolation.rs:42);
+                                k: the k largest-magnitude weights per row, rescaled to the row sum */
 } or_amg_config;
 
 or_amg* or_amg_setup(const or_csr* a, const or_amg_config* cfg);

@@ -39,7 +39,7 @@ class _AmgConfig(C.Structure):
                 ("relaxation", C.c_double), ("strength_threshold", C.c_double),
                 ("coarse_solve", C.c_int32), ("coarse_sweeps", C.c_int32),
                 ("aggregate_size", C.c_int64), ("seed", C.c_uint64), ("coarse_order", C.c_int32),
-                ("pad", C.c_int32)]
+                ("max_interp_points", C.c_int32)]
 
 
 class _SolverConfig(C.Structure):
@@ -239,12 +239,13 @@ class AmgConfig:
     aggregate_size: int = 8
     seed: int = 0
     coarse_order: int = 0  # 0 selection order (reference), 1 ascending fine index
+    max_interp_points: int = 0  # 0: every interpolation weight (the reference)
 
     def _c(self):
         return _AmgConfig(self.max_levels, self.coarsening, self.min_coarse_size, self.interpolation,
                           self.smoother, self.pre_smooth, self.post_smooth, self.relaxation,
                           self.strength_threshold, self.coarse_solve, self.coarse_sweeps,
-                          self.aggregate_size, self.seed, self.coarse_order, 0)
+                          self.aggregate_size, self.seed, self.coarse_order, self.max_interp_points)
 
 
 class Amg:

@@ -101,3 +101,34 @@ def test_host_handle_limits():
     out = C.c_void_p()
     assert L.cfd_amg_setup_host(-1, None, None, None, C.byref(cfg), C.byref(out)) == 1  # CFD_ERR_DIM
     assert not out.value
+
+
+@pytest.mark.parametrize("points", [2, 3, 4])
+@pytest.mark.parametrize("interp", [0, 2])
+def test_truncated_interpolation_matches_oracle(oracle, interp, points):
+    """max_interpolation_points (the argument interpolation.rs:42 accepts and
+    the reference ignores): the product and the oracle truncate P identically,
+    every row keeps at most k weights, and each truncated row keeps its sum."""
+    import cfdrs_b200 as cf
+    A = matrices()["variable_3d_12"]
+    cfg = host_config(0, interp, 1)
+    cfg.max_interpolation_points = points
+    h = cf.HostHierarchy(A, cfg)
+    o = oracle.Amg(oracle.Csr.from_matrix(A), oracle.AmgConfig(
+        max_levels=16, min_coarse_size=60, coarsening=0, interpolation=interp, coarse_order=1,
+        max_interp_points=points))
+    full = cf.HostHierarchy(A, host_config(0, interp, 1))
+    assert h.num_levels == o.num_levels
+    for level in range(h.num_levels):
+        for which in ((0, 1, 2) if level < h.num_levels - 1 else (0,)):
+            mine = h.level(level, which)
+            rp, ci, v, shape = o.level(level, which).arrays()
+            np.testing.assert_array_equal(mine.row_ptr, rp)
+            np.testing.assert_array_equal(mine.col, ci)
+            np.testing.assert_array_equal(mine.val, v)
+    P0, F0 = h.level(0, 1), full.level(0, 1)
+    assert np.diff(P0.row_ptr).max() <= points
+    S0, Sf = P0.to_scipy(), F0.to_scipy()
+    np.testing.assert_allclose(np.asarray(S0.sum(axis=1)).ravel(), np.asarray(Sf.sum(axis=1)).ravel(),
+                               rtol=1e-12, atol=1e-14)
+    assert np.diff(F0.row_ptr).max() > points  # the full P had rows to cut
