@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <numeric>
+#include <map>
 #include <vector>
 
 struct or_csr {
@@ -20,6 +21,15 @@ struct or_csr {
 };
 
 // SimplePreconditioner (crates/cfd-math/src/linear_solver/block_preconditioner.rs:411-424).
+struct or_component_block {
+  int64_t nv = 0, np = 0, cs = 0;
+  std::vector<double> lu[3];      // per component: dense LU with partial pivoting
+  std::vector<int64_t> piv[3];
+  std::vector<double> pinv;       // lumped pressure inverse
+  std::vector<std::vector<std::pair<int64_t, double>>> div_rows;  // D, per pressure row
+  std::vector<std::vector<std::pair<int64_t, double>>> grad_rows; // G, per velocity row (pressure index, value)
+};
+
 struct or_simple {
   int64_t nv = 0, np = 0;
   std::vector<double> dinv, sinv;                                 // diag(A)^-1, diag(S)^-1
@@ -674,13 +684,17 @@ void lu_factor(const or_csr& a, std::vector<double>& m, std::vector<int64_t>& pi
   }
 }
 
+// Solve with the factors of lu_factor: P b first (every exchange, in order),
+// then L y = P b and U x = y. (The stored multipliers of L are those of the
+// rows' final positions, so the exchanges cannot be interleaved with the
+// forward substitution.)
 void lu_solve(const std::vector<double>& m, const std::vector<int64_t>& piv, int64_t n,
               const double* b, double* x) {
   std::vector<double> y(b, b + n);
-  for (int64_t c = 0; c < n; ++c) {
+  for (int64_t c = 0; c < n; ++c)
     if (piv[c] != c) std::swap(y[c], y[piv[c]]);
+  for (int64_t c = 0; c < n; ++c)
     for (int64_t r = c + 1; r < n; ++r) y[r] -= m[(size_t)r * n + c] * y[c];
-  }
   for (int64_t r = n - 1; r >= 0; --r) {
     double s = y[r];
     for (int64_t k = r + 1; k < n; ++k) s -= m[(size_t)r * n + k] * x[k];
@@ -731,6 +745,7 @@ struct Precond {
   const or_amg* amg;
   std::vector<double> inv;
   const or_simple* simple = nullptr;
+  const or_component_block* cblock = nullptr;
   void apply(const double* r, double* z, int64_t n) const {
     if (kind == OR_PRE_JACOBI) {
 #pragma omp parallel for schedule(static)
@@ -741,6 +756,8 @@ struct Precond {
       or_simple_apply(simple, r, z);
     } else if (kind == OR_PRE_BLOCK_DIAGONAL) {
       for (int64_t i = 0; i < n; ++i) z[i] = r[i] * simple->bdinv[i];
+    } else if (kind == OR_PRE_COMPONENT_BLOCK) {
+      or_component_block_apply(cblock, r, z);
     } else {
       std::copy(r, r + n, z);
     }
@@ -1308,6 +1325,138 @@ void or_simple_apply(const or_simple* S, const double* b, double* x) {
 }
 
 void or_simple_free(or_simple* S) { delete S; }
+
+// ComponentBlockPreconditioner::new_with_symbols (block_preconditioner.rs:707-826).
+or_component_block* or_component_block_new(const or_csr* a, int64_t nv, double pivot_tolerance, int* error) {
+  constexpr double eps = 1e-14;  // diagonal_epsilon (:40-42)
+  const int64_t n = a->nrows;
+  *error = 0;
+  if (a->ncols != n || nv <= 0 || nv > n || nv % 3 != 0) {
+    *error = 1;  // size mismatch or velocity count not divisible by 3
+    return nullptr;
+  }
+  // stabilize_preconditioner_diagonal (:71-107) of one block given as rows of
+  // (column, value) in build order, summed per column: a row whose diagonal is
+  // at most eps in magnitude gets max(row_scale * pivot_tolerance, eps) added.
+  auto stabilize = [&](std::vector<std::map<int64_t, double>>& rows) {
+    for (int64_t r = 0; r < (int64_t)rows.size(); ++r) {
+      double diag = 0.0, scale = 0.0;
+      for (const auto& cv : rows[r]) {
+        scale = std::max(scale, std::fabs(cv.second));
+        if (cv.first == r) diag += cv.second;
+      }
+      if (std::fabs(diag) <= eps) rows[r][r] += std::max(scale * pivot_tolerance, eps);
+    }
+  };
+  auto* C = new or_component_block;
+  C->nv = nv;
+  C->np = n - nv;
+  C->cs = nv / 3;
+  const int64_t cs = C->cs;
+  for (int comp = 0; comp < 3; ++comp) {
+    const int64_t off = comp * cs;
+    std::vector<std::map<int64_t, double>> rows(cs);
+    for (int64_t lr = 0; lr < cs; ++lr) {
+      const int64_t g = off + lr;
+      for (int64_t k = a->rp[g]; k < a->rp[g + 1]; ++k) {
+        const int64_t col = a->ci[k];
+        if (col >= nv) continue;
+        if (col / cs != comp) {
+          if (std::fabs(a->v[k]) > eps) {
+            *error = 2;  // velocity component coupling
+            delete C;
+            return nullptr;
+          }
+          continue;
+        }
+        rows[lr][col - off] += a->v[k];
+      }
+    }
+    stabilize(rows);
+    or_csr blk;
+    blk.nrows = blk.ncols = cs;
+    blk.rp.assign(cs + 1, 0);
+    for (int64_t r = 0; r < cs; ++r) {
+      for (const auto& cv : rows[r]) {
+        blk.ci.push_back(cv.first);
+        blk.v.push_back(cv.second);
+      }
+      blk.rp[r + 1] = (int64_t)blk.ci.size();
+    }
+    lu_factor(blk, C->lu[comp], C->piv[comp]);
+    for (int64_t i = 0; i < cs; ++i)
+      if (C->lu[comp][(size_t)i * cs + i] == 0.0) {
+        *error = 3;  // singular component block
+        delete C;
+        return nullptr;
+      }
+  }
+  // SIMPLE's parts (:432-508): diag(A)^-1, D rows, G per pressure column
+  or_simple* S = or_simple_new(a, nv);
+  C->div_rows = S->div_rows;
+  C->grad_rows.assign(nv, {});
+  for (int64_t pc = 0; pc < C->np; ++pc)
+    for (const auto& gv : S->grad_cols[pc]) C->grad_rows[gv.first].push_back({pc, gv.second});
+  for (auto& row : C->grad_rows) std::sort(row.begin(), row.end());
+  // pressure Schur approximation in build order: C entries, then per D entry
+  // (v, d) and pressure column pc in order every G entry (v, pc, g) as -d dinv_v g
+  std::vector<std::map<int64_t, double>> prow(C->np);
+  for (int64_t i = 0; i < C->np; ++i) {
+    auto& row = prow[i];
+    for (int64_t k = a->rp[nv + i]; k < a->rp[nv + i + 1]; ++k)
+      if (a->ci[k] >= nv && a->ci[k] < n) row[a->ci[k] - nv] += a->v[k];
+    for (const auto& dv : S->div_rows[i]) {
+      const double minv = S->dinv[dv.first];
+      for (const auto& gv : C->grad_rows[dv.first]) row[gv.first] += -dv.second * minv * gv.second;
+    }
+  }
+  or_simple_free(S);
+  stabilize(prow);
+  // lumped_pressure_preconditioner (:112-137): signed row sum, else the diagonal
+  C->pinv.assign(C->np, 1.0);
+  for (int64_t i = 0; i < C->np; ++i) {
+    double sum = 0.0, diag = 0.0;
+    for (const auto& cv : prow[i]) {
+      sum += cv.second;
+      if (cv.first == i) diag = cv.second;
+    }
+    const double scale = std::fabs(sum) > eps ? sum : diag;
+    C->pinv[i] = std::fabs(scale) > eps ? 1.0 / scale : 1.0;
+  }
+  return C;
+}
+
+// The athena apply of ComponentBlockPreconditioner (block_preconditioner.rs:920-975).
+void or_component_block_apply(const or_component_block* C, const double* r, double* z) {
+  const int64_t cs = C->cs, nv = C->nv, np = C->np;
+  for (int comp = 0; comp < 3; ++comp) lu_solve(C->lu[comp], C->piv[comp], cs, r + comp * cs, z + comp * cs);
+  for (int64_t i = 0; i < np; ++i) {
+    double t = r[nv + i];
+    for (const auto& dv : C->div_rows[i]) t -= dv.second * z[dv.first];
+    z[nv + i] = t * C->pinv[i];
+  }
+  std::vector<double> rhs(cs), sol(cs);
+  for (int comp = 0; comp < 3; ++comp) {
+    const int64_t off = comp * cs;
+    std::fill(rhs.begin(), rhs.end(), 0.0);
+    // each velocity's gradient entries in ascending pressure column (the
+    // reference loops over pressure columns, then their velocities)
+    for (int64_t v = off; v < off + cs; ++v)
+      for (const auto& gv : C->grad_rows[v]) rhs[v - off] += gv.second * z[nv + gv.first];
+    lu_solve(C->lu[comp], C->piv[comp], cs, rhs.data(), sol.data());
+    for (int64_t k = 0; k < cs; ++k) z[off + k] -= sol[k];
+  }
+}
+
+void or_component_block_free(or_component_block* C) { delete C; }
+
+int or_gmres_component_block(const or_csr* a, const or_component_block* c, int64_t restart, const double* b,
+                             double* x, const or_solver_config* cfg, or_report* rep, double* history) {
+  if (a->ncols != a->nrows || !c || c->nv + c->np != a->nrows) return -1;
+  Precond M{OR_PRE_COMPONENT_BLOCK, nullptr, {}};
+  M.cblock = c;
+  return gmres_impl(a, M, restart, b, x, cfg, rep, history);
+}
 
 int or_bicgstab(const or_csr* a, int precond, const or_amg* amg, const double* b, double* x,
                 const or_solver_config* cfg, or_report* rep, double* history) {

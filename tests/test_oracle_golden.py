@@ -353,3 +353,24 @@ def test_gmres_against_scipy_and_history(oracle):
     assert rep.termination == "MaxIterations" and rep.iterations == 5
     _, rep = oracle.gmres(Ao, np.zeros(n), restart=8, rtol=1e-8)
     assert rep.termination == "InitialResidual" and rep.iterations == 0
+
+
+def test_oracle_dense_coarse_solve_with_row_exchanges(oracle):
+    """The oracle's dense coarsest solve (lu_factor / lu_solve) on matrices
+    whose partial pivoting exchanges rows after the first columns (a Galerkin
+    coarse operator that is not diagonally dominant, such as the 256^3
+    constant-coefficient one, needs this): equal to numpy's solve. The row
+    exchanges must all be applied to b before the forward substitution."""
+    import numpy as np
+    from cfdrs_b200.sparse import CsrMatrix
+    rng = np.random.default_rng(4)
+    for n in (6, 40, 120):
+        M = rng.uniform(-1, 1, (n, n)) + np.diag(rng.uniform(0.05, 0.2, n))  # weak diagonal: many exchanges
+        A = CsrMatrix.from_scipy(__import__("scipy.sparse", fromlist=["csr_matrix"]).csr_matrix(M))
+        amg = oracle.Amg(oracle.Csr.from_matrix(A), oracle.AmgConfig(
+            max_levels=1, min_coarse_size=4096, smoother=oracle.SMOOTH_JACOBI, coarse_solve=oracle.COARSE_DENSE))
+        assert amg.num_levels == 1
+        r = rng.uniform(-1, 1, n)
+        z = amg.apply(r)
+        ref = np.linalg.solve(M, r)
+        assert np.linalg.norm(z - ref) <= 1e-10 * np.linalg.norm(ref), n
