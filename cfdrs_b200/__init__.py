@@ -18,7 +18,7 @@ from .multigrid import (  # noqa: F401
     AMGConfig, AMGStatistics, AlgebraicMultigrid, CoarseOrder, CoarseSolve, CoarseningStrategy, HostHierarchy,
     IdentityPreconditioner, InterpolationStrategy, JacobiPreconditioner, SmootherType,
 )
-from .saddle import BlockDiagonalPreconditioner, SimplePreconditioner  # noqa: F401
+from .saddle import BlockDiagonalPreconditioner, ComponentBlockPreconditioner, SimplePreconditioner  # noqa: F401
 from .chain import LinearSolverChain, LinearSolverState  # noqa: F401
 from .pressure import PressureCorrectionDispatch, PressureLinearSolver  # noqa: F401
 

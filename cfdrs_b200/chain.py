@@ -9,14 +9,14 @@ factorizations outside this package are skipped and recorded as such in
 :attr:`LinearSolverChain.trace`:
 
 * ``solve`` (``chain.rs:160-322``): direct LU [skipped], GMRES + component
-  blocks [skipped], GMRES + SIMPLE (x reset to 0 after it), GMRES + AMG
+  blocks (x reset to 0 after it), GMRES + SIMPLE (x reset to 0 after it), GMRES + AMG
   (``AMGConfig()``; x not reset, as in the reference), GMRES + block diagonal,
   GMRES unpreconditioned (from 0), GMRES + ILU [skipped], BiCGSTAB
   unpreconditioned (from 0; its failure fails the chain).
 * ``solve_with_guess`` (``chain.rs:323-635``): direct LU [skipped], GMRES + SOR
   [skipped], GMRES + AMG (the hierarchy kept in a :class:`LinearSolverState`
   and recomputed for new values while the pattern is unchanged), GMRES +
-  SIMPLE, GMRES + component blocks [skipped], GMRES + block diagonal, GMRES
+  SIMPLE, GMRES + component blocks, GMRES + block diagonal, GMRES
   unpreconditioned only when no block-diagonal preconditioner could be built,
   GMRES + ILU [skipped], BiCGSTAB; every failed tier restarts the next from the
   initial guess.
@@ -67,6 +67,10 @@ class LinearSolverChain:
         from .saddle import SimplePreconditioner
         return SimplePreconditioner(matrix, nv)
 
+    def _component_block(self, matrix, nv):
+        from .saddle import ComponentBlockPreconditioner
+        return ComponentBlockPreconditioner(matrix, nv)
+
     def _block_diagonal(self, matrix, nv):
         from .saddle import BlockDiagonalPreconditioner
         return BlockDiagonalPreconditioner(matrix, nv)
@@ -112,7 +116,11 @@ class LinearSolverChain:
         x = np.zeros(n)
         if n < self.direct_threshold:
             self.trace.append(("direct LU", SKIPPED))
-        self.trace.append(("GMRES+ComponentBlock", SKIPPED))
+        pre = self._setup("GMRES+ComponentBlock", lambda: self._component_block(matrix, n_velocity_dof))
+        if pre is not None:
+            if self._attempt("GMRES+ComponentBlock", lambda: self._gmres(matrix, b, pre, x, restart)):
+                return x
+            x[:] = 0.0
         pre = self._setup("GMRES+SIMPLE", lambda: self._simple(matrix, n_velocity_dof))
         if pre is not None:
             if self._attempt("GMRES+SIMPLE", lambda: self._gmres(matrix, b, pre, x, restart)):
@@ -173,7 +181,11 @@ class LinearSolverChain:
             if self._attempt("GMRES+SIMPLE", lambda: self._gmres(matrix, b, pre, x, restart)):
                 return x
             reset()
-        self.trace.append(("GMRES+ComponentBlock", SKIPPED))
+        pre = self._setup("GMRES+ComponentBlock", lambda: self._component_block(matrix, n_velocity_dof))
+        if pre is not None:
+            if self._attempt("GMRES+ComponentBlock", lambda: self._gmres(matrix, b, pre, x, restart)):
+                return x
+            reset()
         pre = self._setup("GMRES+BlockDiag", lambda: self._block_diagonal(matrix, n_velocity_dof))
         if pre is not None:
             if self._attempt("GMRES+BlockDiag", lambda: self._gmres(matrix, b, pre, x, restart)):

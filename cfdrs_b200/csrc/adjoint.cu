@@ -76,6 +76,7 @@ cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev) {
   CFD_TRY_CUDA(cudaMemcpyAsync(a->host.v.data(), val_dev, nnz * sizeof(double), cudaMemcpyDeviceToHost, s));
   CFD_TRY_CUDA(cudaStreamSynchronize(s));
   a->simple_stale = a->simple_nv >= 0;
+    a->cblock_stale = a->cblock_nv >= 0;
   if (a->diag64) {
     cudaFree(a->diag64);
     cudaFree(a->diag32);

@@ -608,6 +608,7 @@ cfd_status cfd_csr_update_values(cfd_csr* a, const double* val) {
     CFD_TRY(devmat_update_values(a->dev, val, a->host.nnz(), false, a->ctx->stream));
     std::copy(val, val + a->host.nnz(), a->host.v.begin());
     a->simple_stale = a->simple_nv >= 0;
+    a->cblock_stale = a->cblock_nv >= 0;
     dfree(a->diag64);
     dfree(a->diag32);
     dfree(a->jinv64);
@@ -715,6 +716,7 @@ cfd_status cfd_csr_destroy(cfd_csr* a) {
   dfree(a->jinv64);
   dfree(a->jinv32);
   simple_free(a->simple);
+  component_free(a->cblock);
   delete a;
   return CFD_OK;
 }
@@ -968,7 +970,7 @@ cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, con
                 cfg->tolerance, cfg->relative_tolerance, (long long)cfg->max_iterations);
       return CFD_ERR_CONFIG;
     }
-    if (opt->solver < 0 || opt->solver > 2 || opt->precond < 0 || opt->precond > 4 || opt->precision < 0 ||
+    if (opt->solver < 0 || opt->solver > 2 || opt->precond < 0 || opt->precond > 5 || opt->precision < 0 ||
         opt->precision > 1 || opt->memory < 0 || opt->memory > 1 || (opt->solver == CFD_SOLVER_GMRES && opt->restart < 1)) {
       set_error("invalid solve options");
       return CFD_ERR_CONFIG;

@@ -14,7 +14,8 @@
 
 namespace cfd {
 
-struct SimpleDev;  // simple.h
+struct SimpleDev;     // simple.h
+struct ComponentDev;  // simple.h
 
 // Error message of the last failure on this thread (cfd_last_error()).
 void set_error(const char* fmt, ...);
@@ -289,6 +290,12 @@ struct cfd_csr {
   int64_t simple_nv = -1;
   cfd::SimpleDev* simple = nullptr;
   bool simple_stale = false;
+  // Component-block split (cfd_component_block_setup): velocity count or -1,
+  // the stabilization tolerance, and the arrays (rebuilt after a value update).
+  int64_t cblock_nv = -1;
+  double cblock_pivot_tolerance = 1e-12;
+  cfd::ComponentDev* cblock = nullptr;
+  bool cblock_stale = false;
 };
 
 namespace cfd {

@@ -83,6 +83,22 @@ cfd_status simple_apply_device(cfd_csr* a, const T* r, T* z, const int* skip, cu
 template <typename T>
 cfd_status block_diagonal_apply_device(cfd_csr* a, const T* r, T* z, const int* skip, cudaStream_t s);
 
+// ComponentBlockPreconditioner (component.cu): three component-block dense
+// inverses, D and G of the split, the lumped pressure inverse, scratch.
+struct ComponentDev {
+  int64_t nv = 0, np = 0, cs = 0;
+  double* inv[3] = {nullptr, nullptr, nullptr};
+  int32_t *d_rp = nullptr, *d_col = nullptr, *g_rp = nullptr, *g_col = nullptr;
+  double *d_val64 = nullptr, *g_val64 = nullptr, *pinv64 = nullptr, *gp64 = nullptr;
+  float *d_val32 = nullptr, *g_val32 = nullptr, *pinv32 = nullptr, *gp32 = nullptr;
+};
+void component_free(ComponentDev* C);
+// (Re)builds the matrix's component-block arrays when stale; CFD_ERR_STATE
+// when it was never set up. Caller holds the context lock, device selected.
+cfd_status component_ensure(cfd_csr* a);
+template <typename T>
+cfd_status component_apply_device(cfd_csr* a, const T* r, T* z, const int* skip, cudaStream_t s);
+
 template <typename T>
 __host__ __device__ inline T sp_mul(T a, T b) {
 #ifdef __CUDA_ARCH__

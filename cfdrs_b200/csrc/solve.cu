@@ -17,7 +17,7 @@ namespace cfd {
 
 namespace {
 
-constexpr int kPreNone = 0, kPreJacobi = 1, kPreAmg = 2, kPreSimple = 3, kPreBlockDiag = 4;
+constexpr int kPreNone = 0, kPreJacobi = 1, kPreAmg = 2, kPreSimple = 3, kPreBlockDiag = 4, kPreComponent = 5;
 
 inline int vec_grid(int64_t n) {
   int64_t g = (n + kThreads - 1) / kThreads;
@@ -1018,6 +1018,10 @@ static cfd_status gmres_loop(Launcher& lc, cfd_csr* a, cfd_amg* amg, KrylovBufs<
       if (block_diagonal_apply_device<XT>(a, v, z, skip, lc.s) != CFD_OK) return nullptr;
       return z;
     }
+    if (PRE == kPreComponent) {
+      if (component_apply_device<XT>(a, v, z, skip, lc.s) != CFD_OK) return nullptr;
+      return z;
+    }
     return v;
   };
   int64_t cycles = 0;
@@ -1069,9 +1073,10 @@ static cfd_status krylov_loop(Launcher& lc, int solver, int pre, cfd_csr* a, cfd
     if (pre == kPreAmg) return gmres_loop<XT, kPreAmg>(lc, a, amg, B, st, pl, restart);
     if (pre == kPreSimple) return gmres_loop<XT, kPreSimple>(lc, a, amg, B, st, pl, restart);
     if (pre == kPreBlockDiag) return gmres_loop<XT, kPreBlockDiag>(lc, a, amg, B, st, pl, restart);
+    if (pre == kPreComponent) return gmres_loop<XT, kPreComponent>(lc, a, amg, B, st, pl, restart);
     return gmres_loop<XT, kPreNone>(lc, a, amg, B, st, pl, restart);
   }
-  if (pre == kPreSimple || pre == kPreBlockDiag) {
+  if (pre == kPreSimple || pre == kPreBlockDiag || pre == kPreComponent) {
     set_error("the saddle-point preconditioners are applied with GMRES only");
     return CFD_ERR_CONFIG;
   }
@@ -1122,6 +1127,14 @@ cfd_status check_precond(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg)
       return CFD_ERR_CONFIG;
     }
     CFD_TRY(simple_ensure(a));
+  }
+  if (opt.precond == CFD_PRECOND_COMPONENT_BLOCK) {
+    // LinearSolverChain pairs it with GMRES (chain.rs:193-217).
+    if (opt.solver != CFD_SOLVER_GMRES) {
+      set_error("the component-block preconditioner is applied with GMRES only (chain.rs:193-217)");
+      return CFD_ERR_CONFIG;
+    }
+    CFD_TRY(component_ensure(a));
   }
   if (opt.precond == CFD_PRECOND_JACOBI) {
     CFD_TRY(ensure_diagonals(a));

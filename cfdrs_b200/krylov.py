@@ -115,7 +115,9 @@ def converged_or_none(context: str, report: SolveReport) -> SolveReport | None:
 
 
 _SOLVER_CG, _SOLVER_BICGSTAB, _SOLVER_GMRES = 0, 1, 2
-_PRE_NONE, _PRE_JACOBI, _PRE_AMG, _PRE_SIMPLE, _PRE_BLOCK_DIAGONAL = 0, 1, 2, 3, 4
+_PRE_NONE, _PRE_JACOBI, _PRE_AMG, _PRE_SIMPLE, _PRE_BLOCK_DIAGONAL, _PRE_COMPONENT_BLOCK = 0, 1, 2, 3, 4, 5
+_SADDLE_PRE = {"SimplePreconditioner": _PRE_SIMPLE, "BlockDiagonalPreconditioner": _PRE_BLOCK_DIAGONAL,
+               "ComponentBlockPreconditioner": _PRE_COMPONENT_BLOCK}
 
 
 def _solve(solver: int, matrix, rhs, preconditioner, solution, config: IterativeSolverConfig,
@@ -131,13 +133,14 @@ def _solve(solver: int, matrix, rhs, preconditioner, solution, config: Iterative
     elif isinstance(preconditioner, AlgebraicMultigrid):
         pre = _PRE_AMG
         amg_h = preconditioner.h
-    elif type(preconditioner).__name__ in ("SimplePreconditioner", "BlockDiagonalPreconditioner"):
-        pre = _PRE_SIMPLE if type(preconditioner).__name__ == "SimplePreconditioner" else _PRE_BLOCK_DIAGONAL
+    elif type(preconditioner).__name__ in _SADDLE_PRE:
+        pre = _SADDLE_PRE[type(preconditioner).__name__]
         if preconditioner.matrix is not matrix:
             raise SolveError("the saddle-point preconditioner was set up on another matrix object")
     else:
         raise SolveError(f"unsupported preconditioner {type(preconditioner).__name__}")
-    dm = device_matrix(matrix, preconditioner.ctx if pre in (_PRE_AMG, _PRE_SIMPLE, _PRE_BLOCK_DIAGONAL) else None)
+    dm = device_matrix(matrix, preconditioner.ctx if pre in (_PRE_AMG, _PRE_SIMPLE, _PRE_BLOCK_DIAGONAL, _PRE_COMPONENT_BLOCK)
+                       else None)
     n = dm.shape[0]
     if restart < 1:
         raise SolveError(f"GMRES restart must be positive, got {restart}")

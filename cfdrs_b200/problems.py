@@ -390,3 +390,72 @@ def stokes_2d_mac(n: int, nu: float = 1.0, eps: float = 0.1, seed: int = 0):
     rng = np.random.default_rng(seed)
     b = np.concatenate([rng.uniform(-1.0, 1.0, nv), np.zeros(n * n)])
     return CsrMatrix(M.indptr, M.indices, M.data, M.shape), b, nv
+
+
+def stokes_3d_mac(n: int, nu: float = 1.0, eps: float = 0.1, seed: int = 0):
+    """3-D Stokes on an ``n x n x n`` cell MAC grid of the unit cube: the
+    component-major saddle system of the GMRES + ComponentBlock tier
+    (``crates/cfd-math/src/linear_solver/chain.rs:193-217``), whose velocity
+    block has no cross-component entries and three equal components.
+
+    Unknowns: u on the interior x-faces ((n-1) n^2), then v on the interior
+    y-faces and w on the interior z-faces (the same count each), then p per
+    cell (n^3). Momentum rows: the viscous 7-point Laplacian (no-slip walls:
+    normal faces are zero, a tangential wall adds nu/h^2 through the mirrored
+    ghost) and the pressure gradient along the component's axis; continuity
+    rows D = G^T; pressure block -eps I. Scaled by h^2. Returns
+    ``(A, b, n_velocity)``, b a seeded body force in U[-1, 1] with zero
+    continuity right-hand side."""
+    import scipy.sparse as sp
+    h = 1.0 / n
+    ncomp = (n - 1) * n * n
+    nv = 3 * ncomp
+    c = nu / (h * h)
+    cell = lambda i, j, k: i + n * (j + n * k)  # noqa: E731
+    rows, cols, vals = [], [], []
+    for comp in range(3):
+        # face index along `comp` runs 1..n-1; the two other axes 0..n-1
+        ext = [n, n, n]
+        ext[comp] = n - 1
+
+        def fid(f):  # f = (i, j, k) with f[comp] in [1, n-1]
+            g = list(f)
+            g[comp] -= 1
+            return comp * ncomp + g[0] + ext[0] * (g[1] + ext[1] * g[2])
+        for a in range(1, n):
+            for b_ in range(n):
+                for d_ in range(n):
+                    f = [0, 0, 0]
+                    f[comp] = a
+                    others = [ax for ax in range(3) if ax != comp]
+                    f[others[0]] = b_
+                    f[others[1]] = d_
+                    r = fid(f)
+                    diag = 6.0 * c
+                    for ax in range(3):
+                        for s in (-1, 1):
+                            g = list(f)
+                            g[ax] += s
+                            if ax == comp:
+                                if 1 <= g[ax] <= n - 1:
+                                    rows.append(r); cols.append(fid(g)); vals.append(-c)
+                            elif 0 <= g[ax] <= n - 1:
+                                rows.append(r); cols.append(fid(g)); vals.append(-c)
+                            else:
+                                diag += c
+                    rows.append(r); cols.append(r); vals.append(diag)
+                    hi = list(f)
+                    lo = list(f)
+                    lo[comp] -= 1
+                    rows.append(r); cols.append(nv + cell(*hi)); vals.append(1.0 / h)
+                    rows.append(r); cols.append(nv + cell(*lo)); vals.append(-1.0 / h)
+    top = sp.coo_matrix((vals, (rows, cols)), shape=(nv, nv + n ** 3)).tocsr()
+    G = top[:, nv:]
+    D = G.T.tocsr()
+    C = -eps * sp.identity(n ** 3, format="csr")
+    M = sp.bmat([[top[:, :nv], G], [D, C]], format="csr") * (h * h)
+    M.sum_duplicates()
+    M.sort_indices()
+    rng = np.random.default_rng(seed)
+    rhs = np.concatenate([rng.uniform(-1.0, 1.0, nv), np.zeros(n ** 3)])
+    return CsrMatrix(M.indptr, M.indices, M.data, M.shape), rhs, nv

@@ -1,5 +1,5 @@
 """Saddle-point preconditioners (``cfd_saddle_setup``, ``cfd_simple_*``,
-``cfd_block_diagonal_*``).
+``cfd_block_diagonal_*``, ``cfd_component_block_*``).
 
 ``SimplePreconditioner`` and ``BlockDiagonalPreconditioner`` of
 ``crates/cfd-math/src/linear_solver/block_preconditioner.rs``, which
@@ -71,6 +71,35 @@ class BlockDiagonalPreconditioner(_SaddleSplit):
     _apply_fn = "cfd_block_diagonal_apply"
 
 
+class ComponentBlockPreconditioner(_SaddleSplit):
+    """``ComponentBlockPreconditioner::new(matrix, n_velocity, n_pressure)``
+    (``block_preconditioner.rs:609-976``): the velocity block split into three
+    equal, uncoupled components (component-major order), each solved exactly
+    after its zero diagonals are stabilized with ``pivot_tolerance``; the
+    pressure Schur complement lumped by signed row sums. Setup raises
+    :class:`cfdrs_b200.CfdError` where the reference's constructor returns
+    ``Err`` (components that do not split into three equal blocks, entries
+    coupling two components, a singular or oversized block). Use it with
+    :func:`cfdrs_b200.gmres_preconditioned` on the same matrix object."""
+    _apply_fn = "cfd_component_block_apply"
+
+    def __init__(self, matrix, n_velocity: int, n_pressure: int | None = None, ctx: Context | None = None,
+                 pivot_tolerance: float = 1e-12):
+        n = matrix.shape[0]
+        if n_pressure is None:
+            n_pressure = n - n_velocity
+        if n_velocity < 0 or n_pressure < 0 or n_velocity + n_pressure != n or matrix.shape[1] != n:
+            raise SolveError(f"component blocks need a square matrix of n_velocity + n_pressure rows "
+                             f"({n_velocity} + {n_pressure} != {matrix.shape})")
+        self.matrix = matrix
+        self.n_velocity = int(n_velocity)
+        self.n_pressure = int(n_pressure)
+        self.pivot_tolerance = float(pivot_tolerance)
+        self.dm = device_matrix(matrix, ctx)
+        self.ctx = self.dm.ctx
+        _lib.check(_lib.load().cfd_component_block_setup(self.dm.h, self.n_velocity, self.pivot_tolerance))
+
+
 def _csr_args(matrix):
     rp = np.ascontiguousarray(matrix.row_ptr, dtype=np.int64)
     col = np.ascontiguousarray(matrix.col, dtype=np.int32)
@@ -99,4 +128,4 @@ def simple_apply_host(matrix, n_velocity: int, b) -> np.ndarray:
     return x
 
 
-__all__ = ["SimplePreconditioner", "BlockDiagonalPreconditioner", "simple_apply_host", "block_diagonal_host"]
+__all__ = ["SimplePreconditioner", "BlockDiagonalPreconditioner", "ComponentBlockPreconditioner", "simple_apply_host", "block_diagonal_host"]

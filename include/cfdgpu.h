@@ -245,8 +245,9 @@ typedef enum {
   CFD_PRECOND_NONE = 0,
   CFD_PRECOND_JACOBI = 1,
   CFD_PRECOND_AMG = 2,
-  CFD_PRECOND_SIMPLE = 3,        /* GMRES only; cfd_saddle_setup on the matrix first */
-  CFD_PRECOND_BLOCK_DIAGONAL = 4 /* GMRES only; cfd_saddle_setup on the matrix first */
+  CFD_PRECOND_SIMPLE = 3,         /* GMRES only; cfd_saddle_setup on the matrix first */
+  CFD_PRECOND_BLOCK_DIAGONAL = 4, /* GMRES only; cfd_saddle_setup on the matrix first */
+  CFD_PRECOND_COMPONENT_BLOCK = 5 /* GMRES only; cfd_component_block_setup on the matrix first */
 } cfd_precond_kind;
 typedef enum { CFD_PRECISION_FP64 = 0, CFD_PRECISION_FP32_REFINE = 1 } cfd_precision;
 typedef enum { CFD_MEMORY_HOST = 0, CFD_MEMORY_DEVICE = 1 } cfd_memory;
@@ -316,6 +317,24 @@ cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev);
  * absolute row sum over the pressure block, or the mean |momentum diagonal|
  * where that sum is <= 1e-14. */
 cfd_status cfd_saddle_setup(cfd_csr* a, int64_t n_velocity);
+/* ComponentBlockPreconditioner (block_preconditioner.rs:609-976), the
+ * preconditioner of LinearSolverChain's GMRES + ComponentBlock tier
+ * (chain.rs:193-217), for 3-D saddle systems whose velocity block is
+ * component-major: three equal components (n_velocity divisible by 3) with
+ * no entry above 1e-14 coupling two components. Per component the block's
+ * zero diagonals are stabilized (max(row scale * pivot_tolerance, 1e-14)
+ * added, :71-107) and the block is solved exactly: the reference factors it
+ * with its provider's sparse LU, this library forms the dense inverse on the
+ * device (blocks of at most 8192 rows). The pressure Schur approximation
+ * C - D diag(A)^-1 G is lumped by signed row sums (:112-137). Apply:
+ * u* = A_c^-1 r_u, p = (r_p - D u*) / lumped, u = u* - A_c^-1 (G p).
+ * CFD_ERR_DIM for a split that is not three equal components, CFD_ERR_CONFIG
+ * for component coupling, an oversized or singular block (the reference's
+ * constructor Errs there, and the chain skips the tier). A later value update
+ * rebuilds it before the next use. */
+cfd_status cfd_component_block_setup(cfd_csr* a, int64_t n_velocity, double pivot_tolerance);
+/* z = M^-1 r on the device (FP64; r and z distinct device arrays of n). */
+cfd_status cfd_component_block_apply(cfd_csr* a, const double* r_dev, double* z_dev);
 /* z = M^-1 r on the device (FP64; r and z distinct device arrays of n). */
 cfd_status cfd_simple_apply(cfd_csr* a, const double* r_dev, double* z_dev);
 cfd_status cfd_block_diagonal_apply(cfd_csr* a, const double* r_dev, double* z_dev);

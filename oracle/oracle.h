@@ -97,7 +97,8 @@ void or_amg_apply(const or_amg* h, const double* r, double* z);
 void or_amg_free(or_amg* h);
 
 /* Krylov. */
-enum { OR_PRE_NONE = 0, OR_PRE_JACOBI = 1, OR_PRE_AMG = 2, OR_PRE_SIMPLE = 3, OR_PRE_BLOCK_DIAGONAL = 4 };
+enum { OR_PRE_NONE = 0, OR_PRE_JACOBI = 1, OR_PRE_AMG = 2, OR_PRE_SIMPLE = 3, OR_PRE_BLOCK_DIAGONAL = 4,
+       OR_PRE_COMPONENT_BLOCK = 5 };
 enum {
   OR_TERM_CONVERGED = 0,
   OR_TERM_INITIAL_RESIDUAL = 1,
@@ -143,6 +144,27 @@ void or_simple_free(or_simple* s);
 /* BlockDiagonalPreconditioner (block_preconditioner.rs:189-398) of the same
  * split: x = b * its inverse diagonal. */
 void or_block_diagonal_apply(const or_simple* s, const double* b, double* x);
+/* ComponentBlockPreconditioner (block_preconditioner.rs:609-976, the GMRES +
+ * ComponentBlock tier of chain.rs:193-217): the velocity block of a 3-D
+ * saddle system is component-major, three equal components; each component
+ * block (cross-component velocity entries above 1e-14 are refused) gets its
+ * zero diagonals stabilized and an exact factorization (dense LU with partial
+ * pivoting here; the reference's provider sparse LU is not vendored: both are
+ * exact solves), the pressure Schur approximation C - D diag(A)^-1 G is
+ * assembled, stabilized and lumped by signed row sums. Apply (the athena
+ * path, :920-975): u* = A_c^-1 r_u per component, p = lumped^-1 (r_p - D u*),
+ * u = u* - A_c^-1 (G p) per component. NULL (with *error set) when the split
+ * is not 3 equal components, a cross-component entry exceeds 1e-14, or a
+ * block is singular. pivot_tolerance: the stabilization scale of the
+ * provider's sparse LU (not vendored; the tests pass 1e-12). */
+typedef struct or_component_block or_component_block;
+or_component_block* or_component_block_new(const or_csr* a, int64_t n_velocity, double pivot_tolerance,
+                                           int* error);
+void or_component_block_apply(const or_component_block* c, const double* r, double* z);
+void or_component_block_free(or_component_block* c);
+int or_gmres_component_block(const or_csr* a, const or_component_block* c, int64_t restart, const double* b,
+                             double* x, const or_solver_config* cfg, or_report* rep, double* history);
+
 /* GMRES(m) right-preconditioned by SIMPLE (precond OR_PRE_SIMPLE,
  * chain.rs:216-238) or by the block diagonal (OR_PRE_BLOCK_DIAGONAL,
  * chain.rs:265-285) of the split. */

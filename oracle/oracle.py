@@ -118,6 +118,12 @@ def lib():
         L.or_dense_lu_solve.argtypes = [I64, P, P]
         L.or_linear_system_solve.restype = C.c_int
         L.or_linear_system_solve.argtypes = [P, P, P, C.c_int, D, I64, P]
+        L.or_component_block_new.restype = P
+        L.or_component_block_new.argtypes = [P, I64, D, P]
+        L.or_component_block_apply.argtypes = [P, P, P]
+        L.or_component_block_free.argtypes = [P]
+        L.or_gmres_component_block.restype = C.c_int
+        L.or_gmres_component_block.argtypes = [P, P, I64, P, P, P, P, P]
         L.or_network_assemble.restype = C.c_int
         L.or_network_assemble.argtypes = [I64, I64, P, P, P, P, P, P, P, P, P]
         _lib = L
@@ -468,4 +474,34 @@ def gmres_simple(a: Csr, simple: Simple, b, restart=30, precond=PRE_SIMPLE, **kw
 
     def call(h, pre, amg, bp, xp, cfg, rep, hist):
         return fn(h, simple.h, precond, restart, bp, xp, cfg, rep, hist)
+    return _krylov(call, a, b, **kw)
+
+
+class ComponentBlock:
+    """ComponentBlockPreconditioner (block_preconditioner.rs:609-976) on the
+    oracle; ValueError with the reason code when the reference's constructor
+    would return Err (1 split, 2 component coupling, 3 singular block)."""
+
+    def __init__(self, a: Csr, n_velocity: int, pivot_tolerance: float = 1e-12):
+        err = C.c_int(0)
+        self.h = lib().or_component_block_new(a.h, n_velocity, pivot_tolerance, C.byref(err))
+        self.n = a.info()[0]
+        if not self.h:
+            raise ValueError(f"component-block setup refused ({err.value})")
+
+    def apply(self, b):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n)
+        lib().or_component_block_apply(self.h, _ptr(b), _ptr(x))
+        return x
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_component_block_free(self.h)
+            self.h = None
+
+
+def gmres_component_block(a: Csr, cb: ComponentBlock, b, restart=30, **kw):
+    def call(h, pre, amg, bp, xp, cfg, rep, hist):
+        return lib().or_gmres_component_block(h, cb.h, restart, bp, xp, cfg, rep, hist)
     return _krylov(call, a, b, **kw)

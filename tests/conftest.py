@@ -42,7 +42,7 @@ def cuda():
 # tiers, the pressure dispatch), and the suites that must come last (the no-alloc and wait-timeout
 # checks) keep their place at the end.
 _FILE_ORDER = ["test_gpu_parity", "test_gpu_configs", "test_gpu_gmres", "test_gpu_batch", "test_gpu_network_cascade", "test_gpu_adjoint", "test_gpu_recompute",
-               "test_gpu_network_assembly", "test_gpu_simple", "test_gpu_pressure", "test_zz_no_alloc",
+               "test_gpu_network_assembly", "test_gpu_simple", "test_gpu_component", "test_gpu_pressure", "test_zz_no_alloc",
                "test_zz_wait_timeout"]
 
 

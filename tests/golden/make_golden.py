@@ -168,6 +168,17 @@ GOLDEN = {
         "block_diagonal": {"b": [4.0, 4.0, 1.0, 1.0], "x": [1.0, 1.0, 1.0, 1.0]},
         "tol": 1e-10,
     },
+    "component_block": {
+        "source": "crates/cfd-math/src/linear_solver/block_preconditioner.rs:1024-1036, 1100-1116",
+        "n_velocity": 6,
+        # three velocity components of two rows, 4 on the diagonal; gradient and
+        # divergence -1 between u0/p0 and u1/p1; no pressure block
+        "entries": [[0, 0, 4.0], [1, 1, 4.0], [2, 2, 4.0], [3, 3, 4.0], [4, 4, 4.0], [5, 5, 4.0],
+                    [0, 6, -1.0], [1, 7, -1.0], [6, 0, -1.0], [7, 1, -1.0]],
+        "b": [4.0, 4.0, 0.0, 0.0, 0.0, 0.0, 2.0, 2.0],
+        "x": [-2.0, -2.0, 0.0, 0.0, 0.0, 0.0, -12.0, -12.0],
+        "tol": 1e-10,
+    },
     # The reference test checks only that the free block is symmetric; the
     # entries below follow from assemble_into's rules (:208-246) by hand:
     # B = 1 (AB, A fixed) + 3 (BC); C = 2 (AC, A fixed) + 3 (BC) + 4 (CD, D fixed);

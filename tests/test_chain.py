@@ -26,7 +26,7 @@ class Amg:
 class StubChain(LinearSolverChain):
     """Each tier's solve writes a distinct marker into x and records the x it
     started from; outcomes[name] is a termination or an exception."""
-    MARK = {"SIMPLE": 1.0, "AMG": 2.0, "BlockDiag": 3.0, None: 4.0, "BiCGSTAB": 5.0}
+    MARK = {"SIMPLE": 1.0, "AMG": 2.0, "BlockDiag": 3.0, None: 4.0, "BiCGSTAB": 5.0, "ComponentBlock": 6.0}
 
     def __init__(self, outcomes, failing_setups=()):
         super().__init__(K.IterativeSolverConfig(0.0, 1e-8, 100))
@@ -45,6 +45,9 @@ class StubChain(LinearSolverChain):
 
     def _block_diagonal(self, matrix, nv):
         return self._make("BlockDiag", "BlockDiag")
+
+    def _component_block(self, matrix, nv):
+        return self._make("ComponentBlock", "ComponentBlock")
 
     def _amg(self, matrix):
         self.amg_built += 1
@@ -77,18 +80,20 @@ def names(chain):
 def test_cold_order_and_first_success():
     ch = StubChain({"AMG": CONV})
     x = ch.solve(matrix(), np.ones(6), 4)
-    assert names(ch) == ["SIMPLE", "AMG"] and np.all(x == 2.0)
-    assert ch.trace[0] == ("direct LU", SKIPPED) and ch.trace[1] == ("GMRES+ComponentBlock", SKIPPED)
+    assert names(ch) == ["ComponentBlock", "SIMPLE", "AMG"] and np.all(x == 2.0)
+    assert ch.trace[0] == ("direct LU", SKIPPED) and ch.trace[1][0] == "GMRES+ComponentBlock"
     assert ch.trace[-1][0] == "GMRES+AMG" and ch.trace[-1][1].startswith("converged")
 
 
 def test_cold_resets_follow_the_reference():
-    """From 0 after SIMPLE; the block diagonal continues from AMG's iterate;
-    unpreconditioned GMRES and BiCGSTAB start from 0."""
+    """From 0 after the component blocks and SIMPLE; the block diagonal
+    continues from AMG's iterate; unpreconditioned GMRES and BiCGSTAB start
+    from 0."""
     ch = StubChain({"BiCGSTAB": CONV})
     ch.solve(matrix(), np.ones(6), 4)
-    assert names(ch) == ["SIMPLE", "AMG", "BlockDiag", None, "BiCGSTAB"]
+    assert names(ch) == ["ComponentBlock", "SIMPLE", "AMG", "BlockDiag", None, "BiCGSTAB"]
     starts = {n: x for n, x in ch.calls}
+    assert np.all(starts["ComponentBlock"] == 0)
     assert np.all(starts["SIMPLE"] == 0) and np.all(starts["AMG"] == 0)
     assert np.all(starts["BlockDiag"] == 2.0)
     assert np.all(starts[None] == 0) and np.all(starts["BiCGSTAB"] == 0)
@@ -96,10 +101,12 @@ def test_cold_resets_follow_the_reference():
 
 
 def test_cold_setup_failures_and_errors_fall_through():
-    ch = StubChain({"SIMPLE": K.SolveError("boom"), "BlockDiag": BREAK, None: CONV}, failing_setups={"AMG"})
+    ch = StubChain({"SIMPLE": K.SolveError("boom"), "BlockDiag": BREAK, None: CONV},
+                   failing_setups={"AMG", "ComponentBlock"})
     x = ch.solve(matrix(), np.ones(6), 4)
     assert names(ch) == ["SIMPLE", "BlockDiag", None] and np.all(x == 4.0)
     trace = dict(ch.trace)
+    assert trace["GMRES+ComponentBlock"].startswith("setup failed")
     assert trace["GMRES+SIMPLE"].startswith("failed") and trace["GMRES+AMG"].startswith("setup failed")
     assert trace["GMRES+BlockDiag"].startswith("BREAKDOWN")
 
@@ -108,7 +115,7 @@ def test_cold_all_tiers_fail():
     ch = StubChain({})
     with pytest.raises(K.SolveError, match="all solver tiers failed"):
         ch.solve(matrix(), np.ones(6), 4)
-    assert names(ch) == ["SIMPLE", "AMG", "BlockDiag", None, "BiCGSTAB"]
+    assert names(ch) == ["ComponentBlock", "SIMPLE", "AMG", "BlockDiag", None, "BiCGSTAB"]
 
 
 def test_restart_is_capped_by_the_size():
@@ -119,18 +126,18 @@ def test_restart_is_capped_by_the_size():
 
 
 def test_warm_order_resets_to_the_guess_and_skips_gmres():
-    """AMG first, then SIMPLE, then the block diagonal; each restarts from the
-    guess; unpreconditioned GMRES only runs when no block diagonal could be
-    built."""
+    """AMG first, then SIMPLE, the component blocks and the block diagonal;
+    each restarts from the guess; unpreconditioned GMRES only runs when no
+    block diagonal could be built."""
     guess = np.full(6, 9.0)
     ch = StubChain({"BiCGSTAB": CONV})
     ch.solve_with_guess(matrix(), np.ones(6), 4, guess)
-    assert names(ch) == ["AMG", "SIMPLE", "BlockDiag", "BiCGSTAB"]
+    assert names(ch) == ["AMG", "SIMPLE", "ComponentBlock", "BlockDiag", "BiCGSTAB"]
     assert all(np.all(x == 9.0) for _, x in ch.calls)
     assert ch.trace[1] == ("GMRES+SOR", SKIPPED)
     ch = StubChain({None: CONV}, failing_setups={"BlockDiag"})
     x = ch.solve_with_guess(matrix(), np.ones(6), 4, guess)
-    assert names(ch) == ["AMG", "SIMPLE", None] and np.all(x == 4.0)
+    assert names(ch) == ["AMG", "SIMPLE", "ComponentBlock", None] and np.all(x == 4.0)
     assert np.all(dict(ch.calls)[None] == 9.0)
 
 
