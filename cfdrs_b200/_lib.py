@@ -89,7 +89,7 @@ class LayoutInfoC(C.Structure):
     _fields_ = [("blocks", C.c_int64), ("compressed_nnz", C.c_int64), ("all_compressed", C.c_int32),
                 ("x_staged", C.c_int32), ("threads_per_row", C.c_int32), ("max_windows", C.c_int32),
                 ("staged_x_entries", C.c_int64), ("path_f32", C.c_int32), ("path_f64", C.c_int32),
-                ("sliced", C.c_int32), ("pad", C.c_int32), ("sliced_slots", C.c_int64)]
+                ("sliced", C.c_int32), ("diagonals", C.c_int32), ("sliced_slots", C.c_int64)]
 
 
 class KernelStatsC(C.Structure):

@@ -72,6 +72,7 @@ cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev) {
     CFD_TRY_CUDA(cudaGetLastError());
   }
   a->dev.sl_stale = true;
+  a->dev.dia_stale = true;
   // The host copy feeds AMG setup (the Galerkin recompute reads the device values).
   CFD_TRY_CUDA(cudaMemcpyAsync(a->host.v.data(), val_dev, nnz * sizeof(double), cudaMemcpyDeviceToHost, s));
   CFD_TRY_CUDA(cudaStreamSynchronize(s));

@@ -183,6 +183,19 @@ cfd_status devmat_upload(DevMat& m, const HostCsr& h, bool want32, cudaStream_t 
       m.sl_stale = true;
     }
   }
+  {
+    HostDiagonal D;
+    if (encode_diagonal(h, m.tpr, D)) {
+      CFD_TRY(dmalloc(&m.dia64, (int64_t)D.n * D.ld));
+      CFD_TRY_CUDA(cudaMemsetAsync(m.dia64, 0, (size_t)D.n * D.ld * sizeof(double), s));
+      m.dia = true;
+      m.dia_n = D.n;
+      m.dia_main = D.main;
+      for (int d = 0; d < kDiaMax; ++d) m.dia_off[d] = D.off[d];
+      m.dia_ld = D.ld;
+      m.dia_stale = true;
+    }
+  }
   CFD_TRY_CUDA(cudaMemcpyAsync(m.rp, rp32.data(), rp32.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.col, h.ci.data(), m.nnz * sizeof(int), cudaMemcpyHostToDevice, s));
   CFD_TRY_CUDA(cudaMemcpyAsync(m.v64, h.v.data(), m.nnz * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -196,6 +209,11 @@ cfd_status devmat_ensure32(DevMat& m, cudaStream_t s) {
   if (m.v32 || m.nnz == 0) return CFD_OK;
   CFD_TRY(dmalloc(&m.v32, m.nnz));
   m.sl_stale = true;
+  if (m.dia && !m.dia32) {
+    CFD_TRY(dmalloc(&m.dia32, (int64_t)m.dia_n * m.dia_ld));
+    CFD_TRY_CUDA(cudaMemsetAsync(m.dia32, 0, (size_t)m.dia_n * m.dia_ld * sizeof(float), s));
+  }
+  m.dia_stale = true;
   return cast_to_f32(m.v64, m.v32, m.nnz, s);
 }
 
@@ -206,10 +224,11 @@ cfd_status devmat_update_values(DevMat& m, const double* v, int64_t nnz, bool wa
   }
   CFD_TRY_CUDA(cudaMemcpyAsync(m.v64, v, nnz * sizeof(double), cudaMemcpyHostToDevice, s));
   if (m.v32 || want32) {
-    if (!m.v32) CFD_TRY(dmalloc(&m.v32, m.nnz));
+    if (!m.v32) CFD_TRY(devmat_ensure32(m, s));
     CFD_TRY(cast_to_f32(m.v64, m.v32, m.nnz, s));
   }
   m.sl_stale = true;
+  m.dia_stale = true;
   CFD_TRY_CUDA(cudaStreamSynchronize(s));
   return CFD_OK;
 }
@@ -234,6 +253,13 @@ void devmat_free(DevMat& m) {
   dfree(m.sl_doff);
   dfree(m.sl_src);
   dfree(m.sl_v32);
+  dfree(m.dia64);
+  dfree(m.dia32);
+  m.dia = false;
+  m.dia_n = 0;
+  m.dia_main = -1;
+  m.dia_ld = 0;
+  m.dia_stale = true;
   m.sl = false;
   m.sl_slices = m.sl_slots = 0;
   m.sl_stale = true;
@@ -642,6 +668,7 @@ cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out) {
   out->path_f64 = spmv_path(m, 1);
   out->sliced = m.sl ? 1 : 0;
   out->sliced_slots = m.sl_slots;
+  out->diagonals = m.dia ? m.dia_n : 0;
   return CFD_OK;
 }
 
@@ -653,10 +680,11 @@ cfd_status cfd_csr_set_path(cfd_csr* a, int32_t fp32, int32_t path) {
   const DevMat& m = a->dev;
   const bool ok = path == CFD_PATH_AUTO || path == CFD_PATH_TIMED || path == CFD_PATH_SPLIT ||
                   (path == CFD_PATH_RECORD && m.all_compressed) || (path == CFD_PATH_X_STAGED && m.xs) ||
-                  (path == CFD_PATH_SLICED && m.sl && fp32);
+                  (path == CFD_PATH_SLICED && m.sl && fp32) || (path == CFD_PATH_DIAGONAL && m.dia);
   if (!ok) {
     set_error("SpMV pipeline %d not available for this matrix and precision (all blocks coded: %d, x staged: %d, "
-              "sliced: %d, FP32 only)", path, (int)m.all_compressed, (int)m.xs, (int)m.sl);
+              "sliced: %d, FP32 only; diagonals: %d)", path, (int)m.all_compressed, (int)m.xs, (int)m.sl,
+              m.dia ? m.dia_n : 0);
     return CFD_ERR_CONFIG;
   }
   std::lock_guard<std::mutex> g(a->ctx->mu);
@@ -690,6 +718,12 @@ cfd_status cfd_layout_check(int64_t nrows, int64_t ncols, int64_t nnz, const int
       set_error("sliced layout check: %s", why.c_str());
       return CFD_ERR_STATE;
     }
+    HostDiagonal D;
+    const bool diagonal = encode_diagonal(h, tpr, D);
+    if (diagonal && !check_diagonal(h, D, x, &why)) {
+      set_error("diagonal layout check: %s", why.c_str());
+      return CFD_ERR_STATE;
+    }
     if (out) {
       *out = cfd_layout_info{};
       out->blocks = (int64_t)blk.size() - 1;
@@ -701,6 +735,7 @@ cfd_status cfd_layout_check(int64_t nrows, int64_t ncols, int64_t nnz, const int
       out->staged_x_entries = staged;
       out->sliced = sliced ? 1 : 0;
       out->sliced_slots = sliced ? S.slots : 0;
+      out->diagonals = diagonal ? D.n : 0;
     }
     return CFD_OK;
   });
@@ -875,7 +910,7 @@ cfd_status cfd_amg_set_path(cfd_amg* amg, int32_t fp32, int32_t path) {
     set_error("cfd_amg_set_path: null handle");
     return CFD_ERR_STATE;
   }
-  if (path < CFD_PATH_TIMED || path > CFD_PATH_X_STAGED) {
+  if (path < CFD_PATH_TIMED || path > CFD_PATH_DIAGONAL) {
     set_error("cfd_amg_set_path: unknown pipeline %d", path);
     return CFD_ERR_CONFIG;
   }
@@ -884,7 +919,9 @@ cfd_status cfd_amg_set_path(cfd_amg* amg, int32_t fp32, int32_t path) {
   for (DevLevel& L : amg->dev)
     for (DevMat* m : {&L.A, &L.P, &L.R}) {
       int q = path;  // an ineligible request keeps the default rule for that operator
-      if ((q == CFD_PATH_RECORD && !m->all_compressed) || (q == CFD_PATH_X_STAGED && !m->xs)) q = CFD_PATH_AUTO;
+      if ((q == CFD_PATH_RECORD && !m->all_compressed) || (q == CFD_PATH_X_STAGED && !m->xs) ||
+          (q == CFD_PATH_SLICED && !(m->sl && fp32)) || (q == CFD_PATH_DIAGONAL && !m->dia))
+        q = CFD_PATH_AUTO;
       m->path[fp32 ? 0 : 1] = (int8_t)q;
     }
   return CFD_OK;

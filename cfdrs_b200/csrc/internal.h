@@ -103,6 +103,8 @@ constexpr int kRecordCap = ((2 * (kRowsPerBlock + 1) + 15) & ~15) + kNnzCap + 2 
 constexpr int kVecGrid = 148 * 8;
 // Device-side scratch for two-stage reductions (per-CTA partials, up to 4 values).
 constexpr int kMaxRed = 4;
+// Diagonals of the diagonal SpMV layout at most (DevMat::dia).
+constexpr int kDiaMax = 8;
 // Device ordinals covered by the per-device launch-attribute caches.
 constexpr int kLaunchCacheDevices = 64;
 
@@ -177,6 +179,16 @@ struct DevMat {
   int* sl_src = nullptr;
   float* sl_v32 = nullptr;
   mutable bool sl_stale = true;
+  // Diagonal layout (HostDiagonal): values stored diagonal-major, ndia arrays
+  // of dia_ld entries (0 where a row has no entry on that diagonal), refilled
+  // from v64 / v32 before the first diagonal SpMV after the values changed.
+  bool dia = false;
+  int dia_n = 0, dia_main = -1;
+  int dia_off[kDiaMax] = {};
+  int64_t dia_ld = 0;
+  double* dia64 = nullptr;
+  float* dia32 = nullptr;
+  mutable bool dia_stale = true;
 };
 
 // Sliced layout (sliced.cpp, k_spmv_sl): rows in slices of kSlRows stored
@@ -197,6 +209,22 @@ struct HostSliced {
 bool encode_sliced(const HostCsr& h, int tpr, uint64_t base_mult, HostSliced& S);
 bool check_sliced(const HostCsr& h, uint64_t base_mult, const HostSliced& S, std::string* why);
 
+// Diagonal layout (diagonal.cpp, k_spmv_dia): a square matrix with one thread
+// per row whose entries lie on at most kDiaMax diagonals (column - row), stored
+// as kDiaMax or fewer dense diagonals with at most kDiaMaxFill x nnz slots.
+constexpr double kDiaMaxFill = 1.10;
+struct HostDiagonal {
+  int n = 0;          // diagonals, offsets ascending
+  int main = -1;      // index of offset 0, -1 when the main diagonal is empty
+  int off[kDiaMax] = {};
+  int64_t ld = 0;     // entries per stored diagonal (rows rounded up to 32)
+};
+bool encode_diagonal(const HostCsr& h, int tpr, HostDiagonal& D);
+// Evaluates y = A x through the diagonal layout in the device kernel's order
+// and compares it bit for bit with the CSR row sums (sequential, in stored
+// order, each product added by a fused multiply-add).
+bool check_diagonal(const HostCsr& h, const HostDiagonal& D, const double* x, std::string* why);
+
 // SpMV pipeline that an SpMV of precision p ([0] FP32, [1] FP64) runs: the
 // setting, with CFD_PATH_AUTO resolved to RECORD for FP32 and X_STAGED for
 // FP64 one-thread rows (SPLIT for other FP64 matrices), as measured fastest on
@@ -206,6 +234,7 @@ inline int spmv_path(const DevMat& m, int p) {
   int path = m.path[p];
   if (path == CFD_PATH_TIMED) return path;
   if (path == CFD_PATH_SLICED && (p != 0 || !m.sl)) path = p == 0 ? CFD_PATH_RECORD : CFD_PATH_AUTO;
+  if (path == CFD_PATH_DIAGONAL && !m.dia) path = CFD_PATH_AUTO;
   if (path == CFD_PATH_AUTO) path = p == 0 ? CFD_PATH_RECORD : (m.xs && m.tpr == 1 ? CFD_PATH_X_STAGED : CFD_PATH_SPLIT);
   if (path == CFD_PATH_X_STAGED && !m.xs) path = CFD_PATH_RECORD;
   if (path == CFD_PATH_RECORD && !m.all_compressed) path = CFD_PATH_SPLIT;

@@ -846,6 +846,102 @@ static __global__ void __launch_bounds__(kThreads) k_sl_gather(int64_t slots, co
 }
 
 // ---------------------------------------------------------------------------
+// Diagonal pipeline (DevMat::dia): values stored diagonal-major, no indices.
+// Each thread takes kDiaRows rows kThreads apart (grid-stride over spans of
+// kThreads * kDiaRows rows), so every value, x and epilogue access of a warp
+// is to consecutive addresses. All loads of a span are issued before the
+// products: per thread kDiaRows x (values + x) of every stored diagonal. Each
+// row adds its diagonals in ascending offset (= the CSR order) one product at
+// a time with the same expression as rows_from_stage, so y = A x is
+// bit-identical to the other pipelines for finite x (a slot without an entry
+// holds 0 and adds +-0). Values are read with the streaming hint: they are
+// used once, while x is re-read by the rows one plane away.
+template <typename VT>
+struct DiaView {
+  const VT* __restrict__ val;  // n diagonals of ld entries
+  int64_t ld;
+  int nrows, n, main;
+  int off[kDiaMax];
+};
+constexpr int kDiaRows = 2;
+
+template <typename VT, bool OFFDIAG, class Epi>
+__global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, const VT* __restrict__ x, Epi epi) {
+  if (epi.skip()) return;
+  double red[Epi::NRED > 0 ? Epi::NRED : 1];
+#pragma unroll
+  for (int q = 0; q < (Epi::NRED > 0 ? Epi::NRED : 1); ++q) red[q] = 0.0;
+  const int64_t span = (int64_t)kThreads * kDiaRows;
+  for (int64_t s0 = (int64_t)blockIdx.x * span; s0 < D.nrows; s0 += (int64_t)gridDim.x * span) {
+    int row[kDiaRows];
+    bool live[kDiaRows];
+    typename Epi::Pre pre[kDiaRows];
+#pragma unroll
+    for (int q = 0; q < kDiaRows; ++q) {
+      row[q] = (int)(s0 + threadIdx.x + q * kThreads);
+      live[q] = row[q] < D.nrows;
+      pre[q] = typename Epi::Pre{};
+      if (live[q]) pre[q] = epi.load(row[q]);
+    }
+    VT v[kDiaMax][kDiaRows], xv[kDiaMax][kDiaRows];
+#pragma unroll
+    for (int d = 0; d < kDiaMax; ++d) {
+      const bool act = d < D.n;
+      const VT* vd = D.val + (int64_t)d * D.ld;
+      const int o = act ? D.off[d] : 0;
+#pragma unroll
+      for (int q = 0; q < kDiaRows; ++q) {
+        const int j = row[q] + o;
+        const bool in = act && live[q];
+        v[d][q] = in ? __ldcs(vd + row[q]) : VT(0);
+        xv[d][q] = (in && j >= 0 && j < D.nrows) ? __ldg(x + j) : VT(0);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kDiaRows; ++q) {
+      VT sum = VT(0), diag = VT(0);
+#pragma unroll
+      for (int d = 0; d < kDiaMax; ++d) {
+        if (d < D.n) {
+          if (OFFDIAG && d == D.main) {
+            diag = v[d][q];
+          } else {
+            sum += v[d][q] * xv[d][q];
+          }
+        }
+      }
+      if (live[q]) epi.row(row[q], sum, diag, pre[q], red);
+    }
+  }
+  if constexpr (Epi::NRED > 0) {
+    double tot[Epi::NRED];
+    if (grid_reduce<Epi::NRED>(red, epi.red, tot) && threadIdx.x == 0) epi.finish(tot);
+  }
+}
+
+// Diagonal-major values from the CSR ones, one thread per row (every slot of
+// the row written: 0 where the row has no entry on that diagonal).
+template <typename VT>
+__global__ void __launch_bounds__(kThreads) k_dia_fill(DiaView<VT> D, const int* __restrict__ rp,
+                                                       const int* __restrict__ col, const VT* __restrict__ v,
+                                                       VT* __restrict__ out) {
+  for (int r = blockIdx.x * kThreads + threadIdx.x; r < D.nrows; r += gridDim.x * kThreads) {
+    VT slot[kDiaMax];
+#pragma unroll
+    for (int d = 0; d < kDiaMax; ++d) slot[d] = VT(0);
+    for (int k = rp[r]; k < rp[r + 1]; ++k) {
+      const int o = col[k] - r;
+#pragma unroll
+      for (int d = 0; d < kDiaMax; ++d)
+        if (d < D.n && D.off[d] == o) slot[d] = v[k];
+    }
+#pragma unroll
+    for (int d = 0; d < kDiaMax; ++d)
+      if (d < D.n) out[(int64_t)d * D.ld + r] = slot[d];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // x-staged pipeline (DevMat::xs): each stage receives the block's values, its
 // record (row offsets, codes, dictionary, displacement table) and its x
 // windows by bulk copy, so the consumers read every operand from shared

@@ -471,7 +471,8 @@ cfd_status amg_recompute_device(cfd_amg* amg, const cfd_csr* a) {
   for (size_t l = 0; l < L; ++l) {
     DevLevel& D = amg->dev[l];
     if (D.A.v32) k_cast32<<<grid_for(amg->ctx, D.A.nnz, 256), 256, 0, s>>>(D.A.nnz, D.A.v64, D.A.v32);
-    D.A.sl_stale = true;  // the sliced FP32 values are gathered again before their next use
+    D.A.sl_stale = true;   // the sliced FP32 values are gathered again before their next use
+    D.A.dia_stale = true;  // and the diagonal-major ones refilled
     k_diag<<<grid_for(amg->ctx, D.A.nrows, 256), 256, 0, s>>>(D.A.nrows, D.A.rp, D.A.col, D.A.v64, D.d64, D.d32);
     CFD_TRY_CUDA(cudaGetLastError());
   }

@@ -599,7 +599,65 @@ struct Launcher {
     kern<<<grid, kThreads, 0, s>>>(sv, x, epi);
     return CFD_OK;
   }
-  static constexpr int kPathTimed = -2, kPathSplit = 0, kPathRecord = 1, kPathXs = 2, kPathSliced = 3;
+  // Diagonal pipeline: refills the diagonal-major values first when the CSR
+  // values changed since.
+  template <typename VT>
+  DiaView<VT> dia_view(const DevMat& m) const {
+    DiaView<VT> D{};
+    if constexpr (sizeof(VT) == 8)
+      D.val = m.dia64;
+    else
+      D.val = m.dia32;
+    D.ld = m.dia_ld;
+    D.nrows = (int)m.nrows;
+    D.n = m.dia_n;
+    D.main = m.dia_main;
+    for (int d = 0; d < kDiaMax; ++d) D.off[d] = m.dia_off[d];
+    return D;
+  }
+  cfd_status dia_refresh(const DevMat& m) {
+    if (!m.dia_stale) return CFD_OK;
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>((m.nrows + kThreads - 1) / kThreads,
+                                                              (int64_t)ctx->num_sms * 8));
+    if (m.dia64) {
+      k_dia_fill<double><<<g, kThreads, 0, s>>>(dia_view<double>(m), m.rp, m.col, m.v64, m.dia64);
+      ctx->stats.launches++;
+    }
+    if (m.dia32 && m.v32) {
+      k_dia_fill<float><<<g, kThreads, 0, s>>>(dia_view<float>(m), m.rp, m.col, m.v32, m.dia32);
+      ctx->stats.launches++;
+    }
+    CFD_TRY(check());
+    m.dia_stale = false;
+    return CFD_OK;
+  }
+  template <typename VT, bool OFF, class Epi>
+  cfd_status dia_launch(const DevMat& m, const VT* x, Epi epi) {
+    CFD_TRY(dia_refresh(m));
+    auto kern = k_spmv_dia<VT, OFF, Epi>;
+    static int occ[kLaunchCacheDevices] = {};
+    if (ctx->device >= kLaunchCacheDevices) {
+      set_error("device ordinal %d beyond %d", ctx->device, kLaunchCacheDevices);
+      return CFD_ERR_CUDA;
+    }
+    if (occ[ctx->device] <= 0) {
+      int o = 0;
+      CFD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kThreads, 0));
+      occ[ctx->device] = std::max(1, o);
+    }
+    const int64_t spans = (m.nrows + (int64_t)kThreads * kDiaRows - 1) / ((int64_t)kThreads * kDiaRows);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(spans, (int64_t)ctx->num_sms * occ[ctx->device]));
+    kern<<<grid, kThreads, 0, s>>>(dia_view<VT>(m), x, epi);
+    return CFD_OK;
+  }
+  // The diagonal pipeline runs when the values of this precision are there
+  // (the FP32 diagonal copy exists once the FP32 values do).
+  template <typename VT>
+  static bool dia_ready(const DevMat& m) {
+    return m.dia && (sizeof(VT) == 8 ? m.dia64 != nullptr : (m.dia32 != nullptr && m.v32 != nullptr));
+  }
+  static constexpr int kPathTimed = -2, kPathSplit = 0, kPathRecord = 1, kPathXs = 2, kPathSliced = 3,
+                       kPathDiag = 4;
   template <typename VT, typename XT, bool OFF, class Epi>
   cfd_status spmv(const DevMat& m, const XT* x, Epi epi) {
     if (m.nrows == 0) return CFD_OK;
@@ -615,6 +673,13 @@ struct Launcher {
       }
       if (path == kPathSliced) path = m.all_compressed ? kPathRecord : kPathSplit;
     }
+    if constexpr (std::is_same<VT, XT>::value) {
+      if (path == kPathDiag && dia_ready<VT>(m)) {
+        CFD_TRY((dia_launch<VT, OFF, Epi>(m, x, epi)));
+        return finish_spmv<VT, XT>(m);
+      }
+    }
+    if (path == kPathDiag) path = m.all_compressed ? kPathRecord : kPathSplit;
     if constexpr (std::is_same<VT, XT>::value) {
       if (path == kPathXs) {
         CFD_TRY((spmv_xs_launch<VT, OFF, Epi>(m, x, epi)));
@@ -632,7 +697,7 @@ struct Launcher {
   template <typename VT>
   cfd_status tune(const DevMat& m) {
     const int p = sizeof(VT) == 4 ? 0 : 1;
-    if (!m.all_compressed) {
+    if (!m.all_compressed && !dia_ready<VT>(m)) {
       m.path[p] = kPathSplit;
       return CFD_OK;
     }
@@ -653,10 +718,13 @@ struct Launcher {
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
     if (e != cudaSuccess) fail(e);
     const bool sl_ok = std::is_same<VT, float>::value && m.sl && m.v32;
-    for (int path = kPathSplit; st == CFD_OK && path <= kPathSliced; ++path) {
-      if ((path == kPathXs && !m.xs) || (path == kPathSliced && !sl_ok)) continue;
+    for (int path = kPathSplit; st == CFD_OK && path <= kPathDiag; ++path) {
+      if ((path == kPathRecord && !m.all_compressed) || (path == kPathXs && !m.xs) || (path == kPathSliced && !sl_ok) ||
+          (path == kPathDiag && !dia_ready<VT>(m)))
+        continue;
       const EpiStore<VT> epi{ys, nullptr, red()};
       auto run = [&]() -> cfd_status {
+        if (path == kPathDiag) return dia_launch<VT, false, EpiStore<VT>>(m, xs, epi);
         if constexpr (std::is_same<VT, float>::value) {
           if (path == kPathSliced) return sl_launch<VT, false, EpiStore<VT>>(m, xs, epi);
         }

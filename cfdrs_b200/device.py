@@ -97,7 +97,7 @@ class DeviceCsr:
         _lib.check(_lib.load().cfd_csr_layout(self.h, C.byref(info)))
         return {f: getattr(info, f) for f, _ in info._fields_}
 
-    PATHS = {"timed": -2, "auto": -1, "split": 0, "record": 1, "x_staged": 2, "sliced": 3}
+    PATHS = {"timed": -2, "auto": -1, "split": 0, "record": 1, "x_staged": 2, "sliced": 3, "diagonal": 4}
 
     def set_path(self, path: str, fp32: bool) -> None:
         """Set the SpMV pipeline of one precision: "auto" (the default rule),

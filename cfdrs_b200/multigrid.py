@@ -139,7 +139,8 @@ class AlgebraicMultigrid:
 
     def set_path(self, path: str, fp32: bool) -> None:
         """SpMV pipeline of every level operator in one precision ("auto",
-        "timed", "split", "record", "x_staged"); see DeviceCsr.set_path."""
+        "timed", "split", "record", "x_staged", "sliced", "diagonal"); an
+        operator not eligible for the pipeline keeps "auto"; see DeviceCsr.set_path."""
         from .device import DeviceCsr
         _lib.check(_lib.load().cfd_amg_set_path(self.h, 1 if fp32 else 0, DeviceCsr.PATHS[path]))
 

@@ -110,7 +110,7 @@ typedef struct {
   int32_t path_f32;          /* SpMV pipeline an SpMV runs per precision (cfd_spmv_path; TIMED until timed) */
   int32_t path_f64;
   int32_t sliced;            /* the sliced layout (CFD_PATH_SLICED) is built */
-  int32_t pad;
+  int32_t diagonals;         /* stored diagonals of the diagonal layout (CFD_PATH_DIAGONAL), 0 when none */
   int64_t sliced_slots;      /* its slots (stored nonzeros plus padding) */
 } cfd_layout_info;
 cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out);
@@ -122,6 +122,10 @@ cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out);
  * it runs as RECORD). SLICED (FP32 only) needs the sliced layout: one thread
  * per row, rows of at most 32 entries in slices of 32 rows padded by at most
  * 15 %, at most 255 column offsets per 512 rows (otherwise it runs as RECORD).
+ * DIAGONAL needs the diagonal layout: a square matrix, one thread per row,
+ * every entry on one of at most 8 diagonals (column - row) with at most 10 %
+ * empty slots (stencil operators); values stored diagonal-major, no indices.
+ * It adds an empty slot as 0 * x, identical to skipping it for finite x.
  * AUTO (the default): RECORD for FP32 (on the 256^3 fine operator SLICED runs
  * the plain SpMV as fast and the fused epilogues slower); X_STAGED for FP64
  * when eligible with one thread per row, SPLIT otherwise. TIMED: at the
@@ -133,7 +137,8 @@ typedef enum {
   CFD_PATH_SPLIT = 0,
   CFD_PATH_RECORD = 1,
   CFD_PATH_X_STAGED = 2,
-  CFD_PATH_SLICED = 3
+  CFD_PATH_SLICED = 3,
+  CFD_PATH_DIAGONAL = 4
 } cfd_spmv_path;
 /* Set the pipeline of one precision (fp32 != 0: FP32 values). CFD_ERR_CONFIG
  * when the matrix is not eligible for it. */

@@ -59,6 +59,8 @@ def spmv_case(shape):
         from cfdrs_b200.sparse import CsrMatrix
         S = P.poisson_3d_fv(10)[0].to_scipy()
         A, staged = CsrMatrix.from_scipy(sp.block_diag([S, sp.csr_matrix((1300, 1300)), S]).tocsr()), True
+    elif shape == "stencil_2d":  # the 2-D 128^2 operator: five diagonals
+        A = P.poisson_2d_dirichlet(128, seed=0)[0]
     elif shape == "narrow":  # three columns: no bulk-copied window, all tail
         A, staged = random_csr(rng, 2000, 3, rng.integers(0, 4, 2000)), True
     elif shape == "ragged":  # empty rows and short rows of uneven length
@@ -86,8 +88,9 @@ def spmv_case(shape):
     return A, staged
 
 
-@pytest.mark.parametrize("shape", ["stencil", "stencil_tail", "empty_blocks", "narrow", "ragged", "long_rows",
-                                   "rectangular", "mixed", "prolongation", "restriction", "coarse_operator"])
+@pytest.mark.parametrize("shape", ["stencil", "stencil_tail", "stencil_2d", "empty_blocks", "narrow", "ragged",
+                                   "long_rows", "rectangular", "mixed", "prolongation", "restriction",
+                                   "coarse_operator"])
 def test_spmv_vs_oracle(cuda, oracle, shape):
     from cfdrs_b200.device import DeviceCsr
     A, staged = spmv_case(shape)
@@ -107,11 +110,11 @@ def test_spmv_vs_oracle(cuda, oracle, shape):
         assert d.layout()["x_staged"] == 1
 
 
-@pytest.mark.parametrize("shape", ["stencil", "stencil_tail", "empty_blocks", "narrow", "prolongation",
-                                   "restriction", "coarse_operator", "mixed"])
+@pytest.mark.parametrize("shape", ["stencil", "stencil_tail", "stencil_2d", "empty_blocks", "narrow",
+                                   "prolongation", "restriction", "coarse_operator", "mixed"])
 def test_spmv_pipelines_bit_identical(cuda, shape):
     """Every SpMV pipeline a matrix is eligible for (split, record, x-staged,
-    and for FP32 the sliced one) sums each row in the same order: FP64 and FP32
+    diagonal, and for FP32 the sliced one) sums each row in the same order: FP64 and FP32
     results are bit-identical, and an x-staged request with an x that is not
     16-byte aligned runs on the record pipeline with the same result."""
     from cfdrs_b200.device import DeviceCsr
@@ -120,7 +123,10 @@ def test_spmv_pipelines_bit_identical(cuda, shape):
     lay = d.layout()
     if staged:
         assert lay["x_staged"] == 1
-    paths = ["split"] + (["record"] if lay["all_compressed"] else []) + (["x_staged"] if lay["x_staged"] else [])
+    paths = ["split"] + (["record"] if lay["all_compressed"] else []) + (["x_staged"] if lay["x_staged"] else []) + \
+        (["diagonal"] if lay["diagonals"] else [])
+    if shape in ("stencil", "stencil_tail", "stencil_2d"):
+        assert lay["diagonals"] in (5, 7)
     x = np.random.default_rng(5).uniform(-1, 1, A.ncols)
     for dt in (cuda.float64, cuda.float32):
         fp32 = dt == cuda.float32
@@ -146,7 +152,7 @@ def test_spmv_pipelines_bit_identical(cuda, shape):
             assert cuda.equal(ys[0][1], y), f"{shape} {dt} {mode}"
             chosen = d.layout()["path_f32" if fp32 else "path_f64"]
             eligible = paths + (["sliced"] if fp32 and lay["sliced"] else [])
-            assert chosen in [{"split": 0, "record": 1, "x_staged": 2, "sliced": 3}[p] for p in eligible]
+            assert chosen in [{"split": 0, "record": 1, "x_staged": 2, "sliced": 3, "diagonal": 4}[p] for p in eligible]
             if mode == "auto" and fp32:
                 assert chosen == (1 if lay["all_compressed"] else 0)
 
@@ -393,7 +399,8 @@ def test_solve_on_every_pipeline(cuda):
     for prec in (cf.Precision.FP64, cf.Precision.FP32_REFINE):
         fp32 = prec == cf.Precision.FP32_REFINE
         xs = []
-        for path in ("auto", "split", "record", "x_staged", "timed"):
+        assert dA.layout()["diagonals"] == 7
+        for path in ("auto", "split", "record", "x_staged", "diagonal", "timed"):
             amg.set_path(path, fp32)
             try:
                 dA.set_path(path, fp32)

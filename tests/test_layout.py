@@ -148,3 +148,45 @@ def test_sliced_layout_refused_where_it_does_not_pay():
     # a diagonal of 250 rows: the last slice is partial (rows past the end are padding)
     n = 250
     assert check(csr_from_lists(list(range(n + 1)), list(range(n)), [2.0] * n, n))["sliced"] == 1
+
+
+def test_diagonal_layout_on_stencils():
+    """Stencil operators get the diagonal layout (every entry on one of at most
+    8 diagonals, at most 10 % empty slots); cfd_layout_check evaluates y = A x
+    through it in the kernel's order and compares each row bit for bit with
+    the sequential CSR row sum (check_diagonal), boundary rows with missing
+    diagonals included."""
+    # 5^3: 21 % of the slots would be empty (boundary rows), above the 10 % limit
+    cases = [(P.poisson_3d_variable(33, 4.0, 1.0, seed=2)[0], 7), (P.poisson_3d_variable(16, 4.0, 1.0, seed=3)[0], 7),
+             (P.poisson_3d_variable(5, 4.0, 1.0, seed=3)[0], 0),
+             (P.poisson_2d_dirichlet(70, seed=0)[0], 5), (grid_laplacian(41), 5),
+             (csr_from_lists([0, 1], [0], [2.0], 1), 1)]
+    for A, nd in cases:
+        info = check(A)
+        assert info["diagonals"] == nd, (A.shape, info["diagonals"])
+    # a variable-coefficient 2-D Darcy operator
+    A, _ = P.darcy_2d(P.gaussian_random_field((45, 45), 5.0, 0.5, seed=1))
+    assert check(A)["diagonals"] == 5
+
+
+def test_diagonal_layout_refused():
+    rng = np.random.default_rng(4)
+    n = 400
+    # nine distinct diagonals
+    offs = [-40, -20, -3, -1, 0, 1, 3, 20, 40]
+    rows = [[j for j in (i + o for o in offs) if 0 <= j < n] for i in range(n)]
+    rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])])
+    A = csr_from_lists(rp.tolist(), sum(rows, []), rng.uniform(-1, 1, int(rp[-1])).tolist(), n)
+    assert check(A)["diagonals"] == 0
+    # eight diagonals, but far off-diagonal ones mostly outside the matrix: too many empty slots
+    offs = [-300, -200, -1, 0, 1, 200, 300, 350]
+    rows = [[j for j in (i + o for o in offs) if 0 <= j < n] for i in range(n)]
+    rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])])
+    A = csr_from_lists(rp.tolist(), sum(rows, []), rng.uniform(-1, 1, int(rp[-1])).tolist(), n)
+    assert check(A)["diagonals"] == 0
+    # rectangular, empty, and one-thread-per-row violated (rows of 12 and more entries)
+    assert check(random_csr(rng, 300, 200, np.full(300, 3)))["diagonals"] == 0
+    assert check(csr_from_lists([0, 0, 0], [], [], 4))["diagonals"] == 0
+    assert check(random_csr(rng, 300, 300, np.full(300, 30)))["diagonals"] == 0
+    # an AMG Galerkin operator (irregular columns)
+    assert check(P.network_batch(1, seed=5, n_min=200, n_max=300)[0][0])["diagonals"] == 0
