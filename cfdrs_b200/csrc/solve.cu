@@ -593,7 +593,8 @@ struct Launcher {
       occ[ctx->device] = std::max(1, o);
     }
     const int64_t chunks = (m.sl_slices + kSlChunkSlices - 1) / kSlChunkSlices;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, (int64_t)ctx->num_sms * occ[ctx->device]));
+    const int grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>({chunks, (int64_t)ctx->num_sms * occ[ctx->device], (int64_t)ctx->partial_capacity}));
     const SlView sv{m.sl_off, m.sl_code, m.sl_dict, m.sl_doff, m.sl_v32, (unsigned long long)m.base_mult,
                     (int)m.sl_slices, (int)m.nrows};
     kern<<<grid, kThreads, 0, s>>>(sv, x, epi);
@@ -646,7 +647,9 @@ struct Launcher {
       occ[ctx->device] = std::max(1, o);
     }
     const int64_t spans = (m.nrows + (int64_t)kThreads * kDiaRows - 1) / ((int64_t)kThreads * kDiaRows);
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(spans, (int64_t)ctx->num_sms * occ[ctx->device]));
+    // at most one reduction slot per CTA (the context's partials)
+    const int grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>({spans, (int64_t)ctx->num_sms * occ[ctx->device], (int64_t)ctx->partial_capacity}));
     kern<<<grid, kThreads, 0, s>>>(dia_view<VT>(m), x, epi);
     return CFD_OK;
   }

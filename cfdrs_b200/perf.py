@@ -37,13 +37,17 @@ def time_spmv(torch, d, n_rows, n_cols, nnz, fp32, reps, path="auto"):
     e1.record(s)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
-    nbytes = nnz * (vs + 4) + 4 * (n_rows + 1) + vs * (n_rows + n_cols)
+    if path == "diagonal":  # the layout's own bytes: every stored slot, x and y once
+        nbytes = d.layout()["diagonals"] * n_rows * vs + vs * (n_rows + n_cols)
+    else:  # CSR bytes (values, int32 columns and offsets, x and y once)
+        nbytes = nnz * (vs + 4) + 4 * (n_rows + 1) + vs * (n_rows + n_cols)
     return ms, nbytes, x, y
 
 
-def _paths(d):
+def _paths(d, fp32=False):
     lay = d.layout()
-    return ["split"] + (["record"] if lay["all_compressed"] else []) + (["x_staged"] if lay["x_staged"] else [])
+    return ["split"] + (["record"] if lay["all_compressed"] else []) + (["x_staged"] if lay["x_staged"] else []) + \
+        (["sliced"] if fp32 and lay["sliced"] else []) + (["diagonal"] if lay["diagonals"] else [])
 
 
 def main(argv=None):
@@ -53,6 +57,8 @@ def main(argv=None):
     p.add_argument("--systems", type=int, default=4096)
     p.add_argument("--n", type=int, default=128)
     p.add_argument("--reps", type=int, default=20)
+    p.add_argument("--path", default="auto",
+                   help="SpMV pipeline of every operator eligible for it in solve, gmres and timeline")
     a = p.parse_args(argv)
     import torch
 
@@ -76,7 +82,7 @@ def main(argv=None):
     if a.case == "spmv":
         d = DeviceCsr(A, ctx)
         for fp32 in (True, False):
-            for path in _paths(d):
+            for path in _paths(d, fp32):
                 ms, nb, x, y = time_spmv(torch, d, A.nrows, A.ncols, A.nnz, fp32, a.reps, path)
                 print(f"{a.n}^3 {'f32' if fp32 else 'f64'} {path}: {ms * 1e3:.1f} us {nb / ms / 1e6:.0f} GB/s",
                       flush=True)
@@ -91,12 +97,21 @@ def main(argv=None):
                 m = amg.level(l, which)
                 d = DeviceCsr(m, ctx)
                 for fp32 in (True, False):
-                    for path in _paths(d):
+                    for path in _paths(d, fp32):
                         ms, nb, _, _ = time_spmv(torch, d, m.nrows, m.ncols, m.nnz, fp32, a.reps, path)
                         print(f"L{l} {name} {m.nrows}x{m.ncols} nnz={m.nnz} ({m.nnz / max(m.nrows, 1):.1f}/row) "
                               f"{'f32' if fp32 else 'f64'} {path:8s}: {ms * 1e3:8.1f} us {nb / ms / 1e6:6.0f} GB/s",
                               flush=True)
         return 0
+    if a.path != "auto":
+        from cfdrs_b200 import _lib
+        from cfdrs_b200.device import device_matrix
+        for fp32 in (True, False):
+            amg.set_path(a.path, fp32)
+            try:
+                device_matrix(A, ctx).set_path(a.path, fp32)
+            except _lib.CfdError:
+                pass  # the fine operator is not eligible: it keeps the default rule
     bd = torch.as_tensor(b, device="cuda")
     x = torch.zeros_like(bd)
     cfg = cf.IterativeSolverConfig(0.0, 1e-8, 1000)
