@@ -8,7 +8,11 @@ Backward of x = A^{-1} b for an upstream gradient g = dL/dx:
 
 Any differentiable assembly of A's values and b in torch (e.g.
 :func:`darcy_2d_torch`, k = exp(theta) with harmonic-mean faces) then carries
-the chain rule to its parameters. CFDrs has no differentiable solve; its Python
+the chain rule to its parameters. For the 2-D Darcy workload
+:func:`darcy_2d_solve` does the assembly and the face-coefficient chain rule to
+dL/dtheta each in one device kernel (``cfd_darcy2d_assemble``,
+``cfd_darcy2d_theta_grad``), without a dL/dA array or an autograd graph
+through the assembly. CFDrs has no differentiable solve; its Python
 layer (``crates/cfd-python/src/lib.rs:85-158``) exposes physics solvers only, so
 this module is new surface rather than a mirror.
 """
@@ -59,19 +63,29 @@ class SparseSolver:
         ok = (pos < key.size) & (key[order][np.minimum(pos, key.size - 1)] == keyT)
         self.pattern_symmetric = bool(ok.all())
         self._transpose_pos = order[np.minimum(pos, key.size - 1)] if self.pattern_symmetric else None
+        self._transpose_dev = None
         self.symmetric = False
 
     def set_values(self, values: torch.Tensor, rebuild: bool = False) -> None:
-        """New values (device float64, A's CSR order) for the fixed pattern."""
+        """New values (device float64, A's CSR order) for the fixed pattern.
+        The device matrix and the library's host copy (read by AMG setup) take
+        them; ``pattern`` keeps the values it was built with. Symmetry (for the
+        adjoint) is checked on the device."""
         v = values.detach().to(dtype=torch.float64).contiguous()
         if v.numel() != self.pattern.nnz or not v.is_cuda:
             raise SolveError("values must be a CUDA float64 tensor with one entry per stored nonzero")
-        _lib.check(_lib.load().cfd_csr_set_values_device(self.dm.h, C.c_void_p(v.data_ptr())))
-        host = v.cpu().numpy()
-        self.pattern.set_values(host)
+        self.dm.ctx.set_stream(torch.cuda.current_stream(v.device).cuda_stream)
+        try:
+            _lib.check(_lib.load().cfd_csr_set_values_device(self.dm.h, C.c_void_p(v.data_ptr())))
+        finally:
+            self.dm.ctx.set_stream(None)
         mark_synced(self.pattern, self.dm)
-        self.symmetric = self.pattern_symmetric and bool(
-            np.allclose(host, host[self._transpose_pos], rtol=1e-13, atol=0.0))
+        if self.pattern_symmetric:
+            if self._transpose_dev is None or self._transpose_dev.device != v.device:
+                self._transpose_dev = torch.as_tensor(self._transpose_pos, device=v.device)
+            self.symmetric = bool(torch.allclose(v, v[self._transpose_dev], rtol=1e-13, atol=0.0))
+        else:
+            self.symmetric = False
         if self.kind == "amg":
             if self.amg is None or rebuild:
                 self.amg = AlgebraicMultigrid(self.dm, self.amg_config, ctx=self.dm.ctx)
@@ -170,6 +184,65 @@ def darcy_2d_torch(theta: torch.Tensor, mask: torch.Tensor):
     values = vals[mask]
     b = torch.nn.functional.pad(2.0 * k[:, :1], (0, n - 1)).reshape(-1)
     return values, b
+
+
+def darcy_2d_assemble_device(theta: torch.Tensor, solver: SparseSolver):
+    """The values and right-hand side of :func:`darcy_2d_torch` from one
+    kernel (``cfd_darcy2d_assemble``; the same operations, so the same bits),
+    for the pattern of ``solver`` (:func:`darcy_2d_pattern`)."""
+    n = theta.shape[0]
+    th = theta.detach().to(torch.float64).contiguous()
+    if not th.is_cuda or th.shape != (n, n):
+        raise SolveError("theta must be an n x n CUDA tensor")
+    vals = torch.empty(solver.pattern.nnz, dtype=torch.float64, device=th.device)
+    b = torch.empty(n * n, dtype=torch.float64, device=th.device)
+    solver.dm.ctx.set_stream(torch.cuda.current_stream(th.device).cuda_stream)
+    try:
+        _lib.check(_lib.load().cfd_darcy2d_assemble(solver.dm.h, n, C.c_void_p(th.data_ptr()),
+                                                   C.c_void_p(vals.data_ptr()), C.c_void_p(b.data_ptr())))
+    finally:
+        solver.dm.ctx.set_stream(None)
+    return vals, b
+
+
+class DarcySolveFunction(torch.autograd.Function):
+    """p = A(theta)^{-1} b(theta) for the 2-D Darcy system, with the assembly
+    and the chain rule to theta each one kernel: forward assembles on the
+    device and solves; backward solves the adjoint system with the same
+    preconditioner and forms dL/dtheta in ``cfd_darcy2d_theta_grad`` (no dL/dA
+    array, no autograd graph through the assembly)."""
+
+    @staticmethod
+    def forward(ctx, theta, solver: SparseSolver, rebuild: bool = False):
+        vals, b = darcy_2d_assemble_device(theta, solver)
+        solver.set_values(vals, rebuild=rebuild)
+        x = solver.solve(b)
+        ctx.solver = solver
+        ctx.save_for_backward(theta.detach().to(torch.float64).contiguous(), x)
+        return x
+
+    @staticmethod
+    def backward(ctx, gx):
+        solver: SparseSolver = ctx.solver
+        theta, x = ctx.saved_tensors
+        if not solver.symmetric:
+            raise SolveError("the adjoint solve reuses A and its preconditioner, so A must be symmetric")
+        lam = solver.solve(gx.contiguous())
+        n = theta.shape[0]
+        g = torch.empty_like(theta)
+        solver.dm.ctx.set_stream(torch.cuda.current_stream(theta.device).cuda_stream)
+        try:
+            _lib.check(_lib.load().cfd_darcy2d_theta_grad(solver.dm.h, n, C.c_void_p(theta.data_ptr()),
+                                                         C.c_void_p(lam.data_ptr()), C.c_void_p(x.data_ptr()),
+                                                         C.c_void_p(g.data_ptr())))
+        finally:
+            solver.dm.ctx.set_stream(None)
+        return g, None, None
+
+
+def darcy_2d_solve(theta: torch.Tensor, solver: SparseSolver, rebuild: bool = False) -> torch.Tensor:
+    """Differentiable p(theta) of the 2-D Darcy system (:class:`DarcySolveFunction`)."""
+    return DarcySolveFunction.apply(theta, solver, rebuild)
 
 
 def column_loss(p: torch.Tensor, n: int, column: int) -> torch.Tensor:

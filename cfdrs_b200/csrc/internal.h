@@ -325,6 +325,9 @@ struct cfd_csr {
   double cblock_pivot_tolerance = 1e-12;
   cfd::ComponentDev* cblock = nullptr;
   bool cblock_stale = false;
+  // Grid size n of the 2-D Darcy pattern the matrix was checked against
+  // (cfd_darcy2d_*), -1 before the first check.
+  int64_t darcy_n = -1;
 };
 
 namespace cfd {

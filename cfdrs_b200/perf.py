@@ -450,7 +450,7 @@ def adjoint_case(a):
 
     import cfdrs_b200 as cf
     from cfdrs_b200 import problems as P
-    from cfdrs_b200.adjoint import (SparseSolver, column_loss, darcy_2d_pattern, darcy_2d_torch,
+    from cfdrs_b200.adjoint import (SparseSolver, column_loss, darcy_2d_pattern, darcy_2d_solve, darcy_2d_torch,
                                     loss_column_index, sparse_solve)
 
     n = a.n
@@ -458,33 +458,42 @@ def adjoint_case(a):
     col = loss_column_index(n)
     pattern, mask = darcy_2d_pattern(n)
     maskd = torch.as_tensor(mask, device="cuda")
-    s = SparseSolver(pattern, precision=cf.Precision.FP32_REFINE, config=cf.IterativeSolverConfig(0.0, 1e-10, 500))
     th = torch.as_tensor(theta, device="cuda")
 
-    def update(first=False):
-        t = th.clone().requires_grad_(True)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
+    def generic(t, s, first):  # torch assembly, SparseSolveFunction, autograd through the assembly
         vals, b = darcy_2d_torch(t, maskd)
-        p = sparse_solve(vals, b, s, first)
-        fwd = s.last_report
-        L = column_loss(p, n, col)
-        L.backward()
-        torch.cuda.synchronize()
-        return (time.perf_counter() - t0) * 1e3, fwd, s.last_report, L.item()
+        return sparse_solve(vals, b, s, first)
 
-    first_ms = update(True)[0]
-    times = []
-    for _ in range(3):
-        ms, fwd, adj, L = update()
-        times.append(ms)
-    print(f"{n}^2: L = {L:.10e}; forward solve {fwd.device_ms:.1f} ms device ({fwd.iterations} inner its), "
-          f"adjoint solve {adj.device_ms:.1f} ms device", flush=True)
-    s.refresh = "keep"
-    keep = [update()[0] for _ in range(3)]
-    s.refresh = "recompute"
-    print(f"  per theta update end to end: {min(times):.1f} ms with the Galerkin recompute, "
-          f"{min(keep):.1f} ms keeping the hierarchy (first call with AMG setup {first_ms:.1f} ms)", flush=True)
+    def fused(t, s, first):  # DarcySolveFunction: assembly and chain rule each one kernel
+        return darcy_2d_solve(t, s, first)
+
+    for name, fn in (("fused", fused), ("generic", generic)):
+        s = SparseSolver(pattern, precision=cf.Precision.FP32_REFINE,
+                         config=cf.IterativeSolverConfig(0.0, 1e-10, 500))
+
+        def update(first=False):
+            t = th.clone().requires_grad_(True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            p = fn(t, s, first)
+            fwd = s.last_report
+            L = column_loss(p, n, col)
+            L.backward()
+            torch.cuda.synchronize()
+            return (time.perf_counter() - t0) * 1e3, fwd, s.last_report, L.item()
+
+        first_ms = update(True)[0]
+        times = []
+        for _ in range(3):
+            ms, fwd, adj, L = update()
+            times.append(ms)
+        print(f"{n}^2 {name}: L = {L:.10e}; forward solve {fwd.device_ms:.1f} ms device ({fwd.iterations} inner "
+              f"its), adjoint solve {adj.device_ms:.1f} ms device", flush=True)
+        s.refresh = "keep"
+        keep = [update()[0] for _ in range(3)]
+        s.refresh = "recompute"
+        print(f"  per theta update end to end: {min(times):.1f} ms with the Galerkin recompute, "
+              f"{min(keep):.1f} ms keeping the hierarchy (first call with AMG setup {first_ms:.1f} ms)", flush=True)
     return 0
 
 

@@ -303,6 +303,18 @@ cfd_status cfd_pattern_outer(cfd_csr* a, const double* lambda_dev, const double*
 /* Replace A's values from device memory (same pattern); the host copy used by
  * AMG setup is refreshed too (cfd_amg_recompute reads the device values). */
 cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev);
+/* The 2-D Darcy workload's assembly and its chain rule on the device, on the
+ * context's stream. a holds the pattern of an n x n cell grid (row i + n j;
+ * per row south, west, diagonal, east, north as present; checked once):
+ * -div(exp(theta) grad p) = 0, harmonic-mean faces, p = 1 on the left and
+ * p = 0 on the right wall at half a cell, no flux on top and bottom.
+ * assemble: A's values (CSR order) and b from theta (n*n device arrays).
+ * theta_grad: dL/dtheta from x = A^-1 b and lambda = A^-T dL/dx, the
+ * face-coefficient chain rule in one kernel (no dL/dA array). CFD_ERR_DIM
+ * when a is not that pattern. */
+cfd_status cfd_darcy2d_assemble(cfd_csr* a, int64_t n, const double* theta_dev, double* val_dev, double* b_dev);
+cfd_status cfd_darcy2d_theta_grad(cfd_csr* a, int64_t n, const double* theta_dev, const double* lambda_dev,
+                                  const double* x_dev, double* grad_dev);
 
 /* ---- saddle-point preconditioners -----------------------------------------
  * The two of LinearSolverChain's GMRES tiers for saddle-point systems

@@ -119,3 +119,78 @@ def test_darcy_512_gradient_vs_cpu_adjoint_and_fd(cuda):
     scale = np.abs(g_cpu).max()
     assert np.abs(ga - fd).max() <= 1e-4 * scale
     assert np.abs(ga - fd).max() <= 2.0 * np.abs(gc - fd).max() + 1e-9 * scale  # no worse than the CPU adjoint
+
+
+@pytest.mark.parametrize("n", [1, 2, 37, 64])
+def test_darcy_assembly_kernel_equals_torch_assembly(cuda, n):
+    """cfd_darcy2d_assemble performs the torch assembly's operations in its
+    order: values and right-hand side equal bit for bit (1 x 1 and 2 x 2
+    grids included: both walls on one cell)."""
+    torch = cuda
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.adjoint import SparseSolver, darcy_2d_assemble_device, darcy_2d_pattern, darcy_2d_torch
+    theta = P.gaussian_random_field((n, n), 4.0, 0.5, seed=n) if n > 2 else \
+        np.random.default_rng(n).standard_normal((n, n))
+    pattern, mask = darcy_2d_pattern(n)
+    s = SparseSolver(pattern, preconditioner="jacobi", precision=cf.Precision.FP64)
+    th = torch.as_tensor(theta, device="cuda")
+    v_t, b_t = darcy_2d_torch(th, torch.as_tensor(mask, device="cuda"))
+    v_d, b_d = darcy_2d_assemble_device(th, s)
+    assert torch.equal(v_t, v_d) and torch.equal(b_t, b_d)
+    A, b = P.darcy_2d(theta)  # the scipy assembly of the same system
+    np.testing.assert_allclose(v_d.cpu().numpy(), A.val, rtol=1e-14)
+    np.testing.assert_allclose(b_d.cpu().numpy(), b, rtol=1e-14)
+
+
+def test_darcy_kernels_refuse_other_patterns(cuda):
+    torch = cuda
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import _lib
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.adjoint import SparseSolver, darcy_2d_assemble_device
+    A, _ = P.poisson_2d_dirichlet(16)
+    s = SparseSolver(A, preconditioner="jacobi", precision=cf.Precision.FP64)
+    with pytest.raises(_lib.CfdError, match="Darcy pattern") as e:
+        darcy_2d_assemble_device(torch.zeros((16, 16), dtype=torch.float64, device="cuda"), s)
+    assert e.value.status == 1
+
+
+def test_darcy_512_fused_gradient(cuda):
+    """The adjoint workload through DarcySolveFunction (assembly and chain
+    rule each one kernel): loss and dL/dtheta equal the generic path's
+    (torch assembly, SparseSolveFunction, autograd) to 1e-10 and the FP64 CPU
+    adjoint's to 1e-8; on the 64 seeded cells within 1e-4 max|g| of central
+    differences (h = 1e-6, low-rank exact perturbed solves)."""
+    torch = cuda
+    import adjoint_cpu as AC
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.adjoint import (SparseSolver, column_loss, darcy_2d_pattern, darcy_2d_solve, darcy_2d_torch,
+                                    loss_column_index, sparse_solve)
+    n = 512
+    theta = P.gaussian_random_field((n, n), 16.0, 0.5, seed=0)
+    col = loss_column_index(n)
+    pattern, mask = darcy_2d_pattern(n)
+    cfg = cf.IterativeSolverConfig(0.0, 1e-10, 500)
+    s = SparseSolver(pattern, precision=cf.Precision.FP32_REFINE, config=cfg)
+    th = torch.as_tensor(theta, device="cuda").requires_grad_(True)
+    L = column_loss(darcy_2d_solve(th, s, True), n, col)
+    L.backward()
+    g = th.grad.cpu().numpy()
+    s2 = SparseSolver(pattern, precision=cf.Precision.FP32_REFINE, config=cfg)
+    th2 = torch.as_tensor(theta, device="cuda").requires_grad_(True)
+    vals, b = darcy_2d_torch(th2, torch.as_tensor(mask, device="cuda"))
+    L2 = column_loss(sparse_solve(vals, b, s2, True), n, col)
+    L2.backward()
+    g2 = th2.grad.cpu().numpy()
+    assert abs(L.item() - L2.item()) <= 1e-12 * abs(L2.item())
+    assert np.linalg.norm(g - g2) <= 1e-10 * np.linalg.norm(g2)
+    L_cpu, g_cpu, _ = AC.loss_and_grad(theta, col)
+    assert abs(L.item() - L_cpu) <= 1e-9 * abs(L_cpu)
+    assert np.linalg.norm(g - g_cpu) <= 1e-8 * np.linalg.norm(g_cpu)
+    rng = np.random.default_rng(64)
+    cells = [(int(j), int(i)) for j, i in rng.integers(0, n, size=(64, 2))]
+    fd = AC.central_fd_lowrank(theta, col, cells, h=1e-6)
+    ga = np.array([g[j, i] for j, i in cells])
+    assert np.abs(ga - fd).max() <= 1e-4 * np.abs(g_cpu).max()
