@@ -586,7 +586,11 @@ def run_plain(args, world, rank, local):
     ev1.record(stream)
     torch.cuda.synchronize()
     t_spmv = ev0.elapsed_time(ev1) / reps
-    spmv_bytes = A.nnz * 12 + 4 * (N + 1) + 16 * N
+    lay = dA.layout()
+    diagonal = lay["path_f64"] == 4
+    # the pipeline's algorithmic bytes: CSR (value, int32 column, offsets) or,
+    # for the diagonal layout, every stored slot; x and y once
+    spmv_bytes = lay["diagonals"] * N * 8 + 16 * N if diagonal else A.nnz * 12 + 4 * (N + 1) + 16 * N
     gbs = spmv_bytes / t_spmv / 1e6
     ctx.set_stream(None)
 
@@ -620,9 +624,12 @@ def run_plain(args, world, rank, local):
             "gpu_launches": int(launches * args.steps),
             "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
                          "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "SpMV FP64 of the operator, timed alone; achieved counts CSR bytes"
+                         "kernel": "SpMV FP64 of the operator, timed alone ("
+                                   + ("diagonal pipeline; achieved counts the stored diagonals, x and y"
+                                      if diagonal else "achieved counts CSR bytes") + ")"
                                    + (" (L2-resident: the HBM fraction does not bound it)"
-                                      if args.workload == "c1" else "")},
+                                      if args.workload == "c1" else ""),
+                         "bytes_per_launch": spmv_bytes},
             "iterations": rep.iterations, "true_rel_residual": true_rel, "clocks": clk.summary(),
         }
         line.update(extra)
@@ -867,10 +874,16 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
         t = ev0.elapsed_time(ev1) / reps
-        bytes_ = nnz * (vs + 4) + 4 * (N + 1) + 2 * N * vs
-        spmv[label] = {"ms": t, "bytes": bytes_, "gbs": bytes_ / t / 1e6}
+        lay = dA.layout()
+        csr_bytes = nnz * (vs + 4) + 4 * (N + 1) + 2 * N * vs
+        if lay["path_f32" if label == "f32" else "path_f64"] == 4:
+            # diagonal layout: every stored slot once, x and y once (no index bytes)
+            bytes_ = lay["diagonals"] * N * vs + 2 * N * vs
+        else:
+            bytes_ = csr_bytes
+        spmv[label] = {"ms": t, "bytes": bytes_, "gbs": bytes_ / t / 1e6, "csr_equivalent_gbs": csr_bytes / t / 1e6}
     ctx.set_stream(None)
-    names = {0: "split", 1: "record", 2: "x_staged", -2: "timed"}
+    names = {0: "split", 1: "record", 2: "x_staged", 3: "sliced", 4: "diagonal", -2: "timed"}
     lay = dA.layout()
     spmv_path = {"f32": names[lay["path_f32"]], "f64": names[lay["path_f64"]]}
 
@@ -882,7 +895,10 @@ def main():
 
     if rank == 0:
         f32 = spmv["f32"]
-        traffic = profile_traffic("spmv_f32_record_128.md")
+        traffic = profile_traffic("spmv_f32_diagonal_128.md" if spmv_path["f32"] == "diagonal"
+                                  else "spmv_f32_record_128.md")
+        bytes_note = ("algorithmic bytes of the diagonal layout: 7 stored diagonals x 4 B + x and y once"
+                      if spmv_path["f32"] == "diagonal" else "CSR bytes (8-byte value+index per nonzero)")
         line = {
             "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
@@ -893,11 +909,13 @@ def main():
             "roofline": {"bound": "hbm", "achieved": f32["gbs"], "peak": peak, "unit": "GB/s",
                          "frac": f32["gbs"] / peak, "traffic": traffic,
                          "kernel": f"SpMV FP32 fine operator (256^3, 117M nnz, {spmv_path['f32']} pipeline), "
-                                   "timed alone; achieved counts CSR bytes (8-byte value+index per nonzero)",
-                         "peak_kind": peak_kind},
+                                   f"timed alone; achieved counts the {bytes_note}",
+                         "bytes_per_launch": f32["bytes"], "peak_kind": peak_kind},
             "spmv_path": spmv_path,
             "spmv_gbs": {"f32": f32["gbs"], "f64": spmv["f64"]["gbs"],
-                         "frac_f32": f32["gbs"] / peak, "frac_f64": spmv["f64"]["gbs"] / peak},
+                         "frac_f32": f32["gbs"] / peak, "frac_f64": spmv["f64"]["gbs"] / peak,
+                         "csr_equivalent_f32": f32["csr_equivalent_gbs"],
+                         "csr_equivalent_f64": spmv["f64"]["csr_equivalent_gbs"]},
             "fp64_pcg_ms": fp64_best, "speedup_vs_fp64_pcg": fp64_best / ms,
             "fp64_pcg_ms_by_pipeline": {"auto": min(fp64_ms), "timed": min(fp64_timed_ms)},
             "fp32_refine_ms_timed_pipelines": min(fp32_timed_ms),

@@ -235,6 +235,7 @@ inline int spmv_path(const DevMat& m, int p) {
   if (path == CFD_PATH_TIMED) return path;
   if (path == CFD_PATH_SLICED && (p != 0 || !m.sl)) path = p == 0 ? CFD_PATH_RECORD : CFD_PATH_AUTO;
   if (path == CFD_PATH_DIAGONAL && !m.dia) path = CFD_PATH_AUTO;
+  if (path == CFD_PATH_AUTO && m.dia) path = CFD_PATH_DIAGONAL;
   if (path == CFD_PATH_AUTO) path = p == 0 ? CFD_PATH_RECORD : (m.xs && m.tpr == 1 ? CFD_PATH_X_STAGED : CFD_PATH_SPLIT);
   if (path == CFD_PATH_X_STAGED && !m.xs) path = CFD_PATH_RECORD;
   if (path == CFD_PATH_RECORD && !m.all_compressed) path = CFD_PATH_SPLIT;

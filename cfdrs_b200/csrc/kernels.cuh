@@ -849,13 +849,18 @@ static __global__ void __launch_bounds__(kThreads) k_sl_gather(int64_t slots, co
 // Diagonal pipeline (DevMat::dia): values stored diagonal-major, no indices.
 // Each thread takes kDiaRows rows kThreads apart (grid-stride over spans of
 // kThreads * kDiaRows rows), so every value, x and epilogue access of a warp
-// is to consecutive addresses. All loads of a span are issued before the
-// products: per thread kDiaRows x (values + x) of every stored diagonal. Each
-// row adds its diagonals in ascending offset (= the CSR order) one product at
-// a time with the same expression as rows_from_stage, so y = A x is
-// bit-identical to the other pipelines for finite x (a slot without an entry
-// holds 0 and adds +-0). Values are read with the streaming hint: they are
-// used once, while x is re-read by the rows one plane away.
+// is to consecutive addresses. Each row adds its diagonals in ascending offset
+// (= the CSR order) one product at a time with the same expression as
+// rows_from_stage, so y = A x is bit-identical to the other pipelines for
+// finite x (a slot without an entry holds 0 and adds +-0). Values are read with
+// the streaming hint: they are used once, while x is re-read by the rows one
+// plane away.
+// Interior spans (every row live, every x index of every diagonal inside
+// [0, nrows)) take a path without predicates: per diagonal one base pointer
+// for the values and one for x, the kDiaRows loads at immediate offsets, all
+// loads of the span issued before the products. ND > 0 fixes the diagonal
+// count at compile time (the 5- and 7-point stencils); ND = 0 takes any count
+// up to kDiaMax with predicated slots. Boundary spans take the predicated path.
 template <typename VT>
 struct DiaView {
   const VT* __restrict__ val;  // n diagonals of ld entries
@@ -865,52 +870,89 @@ struct DiaView {
 };
 constexpr int kDiaRows = 2;
 
-template <typename VT, bool OFFDIAG, class Epi>
+template <typename VT, bool OFFDIAG, int NS>
+__device__ __forceinline__ void dia_sum(const VT (&v)[NS], const VT (&xv)[NS], int nd, int main, VT& sum,
+                                        VT& diag) {
+#pragma unroll
+  for (int d = 0; d < NS; ++d) {
+    if (d < nd) {
+      if (OFFDIAG && d == main) {
+        diag = v[d];
+      } else {
+        sum += v[d] * xv[d];
+      }
+    }
+  }
+}
+
+template <typename VT, bool OFFDIAG, class Epi, int ND>
 __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, const VT* __restrict__ x, Epi epi) {
   if (epi.skip()) return;
+  constexpr int NS = ND > 0 ? ND : kDiaMax;  // slots per row in registers
   double red[Epi::NRED > 0 ? Epi::NRED : 1];
 #pragma unroll
   for (int q = 0; q < (Epi::NRED > 0 ? Epi::NRED : 1); ++q) red[q] = 0.0;
+  const int nd = ND > 0 ? ND : D.n;
   const int64_t span = (int64_t)kThreads * kDiaRows;
+  const int omin = D.off[0], omax = D.off[nd - 1];
   for (int64_t s0 = (int64_t)blockIdx.x * span; s0 < D.nrows; s0 += (int64_t)gridDim.x * span) {
-    int row[kDiaRows];
-    bool live[kDiaRows];
+    const bool interior = s0 + omin >= 0 && s0 + span + omax <= D.nrows && s0 + span <= D.nrows;
+    const int r0 = (int)s0 + threadIdx.x;
     typename Epi::Pre pre[kDiaRows];
+    VT v[kDiaRows][NS], xv[kDiaRows][NS];
+    if (interior) {
 #pragma unroll
-    for (int q = 0; q < kDiaRows; ++q) {
-      row[q] = (int)(s0 + threadIdx.x + q * kThreads);
-      live[q] = row[q] < D.nrows;
-      pre[q] = typename Epi::Pre{};
-      if (live[q]) pre[q] = epi.load(row[q]);
-    }
-    VT v[kDiaMax][kDiaRows], xv[kDiaMax][kDiaRows];
+      for (int q = 0; q < kDiaRows; ++q) pre[q] = epi.load(r0 + q * kThreads);
 #pragma unroll
-    for (int d = 0; d < kDiaMax; ++d) {
-      const bool act = d < D.n;
-      const VT* vd = D.val + (int64_t)d * D.ld;
-      const int o = act ? D.off[d] : 0;
+      for (int d = 0; d < NS; ++d) {
+        if (ND > 0 || d < nd) {
+          const VT* vp = D.val + (int64_t)d * D.ld + r0;
+          const VT* xp = x + (r0 + D.off[d]);
 #pragma unroll
-      for (int q = 0; q < kDiaRows; ++q) {
-        const int j = row[q] + o;
-        const bool in = act && live[q];
-        v[d][q] = in ? __ldcs(vd + row[q]) : VT(0);
-        xv[d][q] = (in && j >= 0 && j < D.nrows) ? __ldg(x + j) : VT(0);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < kDiaRows; ++q) {
-      VT sum = VT(0), diag = VT(0);
-#pragma unroll
-      for (int d = 0; d < kDiaMax; ++d) {
-        if (d < D.n) {
-          if (OFFDIAG && d == D.main) {
-            diag = v[d][q];
-          } else {
-            sum += v[d][q] * xv[d][q];
+          for (int q = 0; q < kDiaRows; ++q) {
+            v[q][d] = __ldcs(vp + q * kThreads);
+            xv[q][d] = __ldg(xp + q * kThreads);
           }
+        } else {
+#pragma unroll
+          for (int q = 0; q < kDiaRows; ++q) v[q][d] = xv[q][d] = VT(0);
         }
       }
-      if (live[q]) epi.row(row[q], sum, diag, pre[q], red);
+#pragma unroll
+      for (int q = 0; q < kDiaRows; ++q) {
+        VT sum = VT(0), diag = VT(0);
+        dia_sum<VT, OFFDIAG, NS>(v[q], xv[q], nd, D.main, sum, diag);
+        epi.row(r0 + q * kThreads, sum, diag, pre[q], red);
+      }
+    } else {
+      bool live[kDiaRows];
+#pragma unroll
+      for (int q = 0; q < kDiaRows; ++q) {
+        const int row = r0 + q * kThreads;
+        live[q] = row < D.nrows;
+        pre[q] = typename Epi::Pre{};
+        if (live[q]) pre[q] = epi.load(row);
+      }
+#pragma unroll
+      for (int d = 0; d < NS; ++d) {
+        const bool act = d < nd;
+        const VT* vd = D.val + (int64_t)d * D.ld;
+        const int o = act ? D.off[d] : 0;
+#pragma unroll
+        for (int q = 0; q < kDiaRows; ++q) {
+          const int row = r0 + q * kThreads;
+          const int j = row + o;
+          const bool in = act && live[q];
+          v[q][d] = in ? __ldcs(vd + row) : VT(0);
+          xv[q][d] = (in && j >= 0 && j < D.nrows) ? __ldg(x + j) : VT(0);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kDiaRows; ++q) {
+        VT sum = VT(0), diag = VT(0);
+        dia_sum<VT, OFFDIAG, NS>(v[q], xv[q], nd, D.main, sum, diag);
+        if (live[q]) epi.row(r0 + q * kThreads, sum, diag, pre[q], red);
+      }
     }
   }
   if constexpr (Epi::NRED > 0) {

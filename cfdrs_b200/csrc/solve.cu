@@ -634,8 +634,15 @@ struct Launcher {
   }
   template <typename VT, bool OFF, class Epi>
   cfd_status dia_launch(const DevMat& m, const VT* x, Epi epi) {
+    if (m.dia_n == 7) return dia_launch_n<VT, OFF, Epi, 7>(m, x, epi);
+    if (m.dia_n == 5) return dia_launch_n<VT, OFF, Epi, 5>(m, x, epi);
+    return dia_launch_n<VT, OFF, Epi, 0>(m, x, epi);
+  }
+  // ND: the diagonal count fixed at compile time (0: any count up to kDiaMax).
+  template <typename VT, bool OFF, class Epi, int ND>
+  cfd_status dia_launch_n(const DevMat& m, const VT* x, Epi epi) {
     CFD_TRY(dia_refresh(m));
-    auto kern = k_spmv_dia<VT, OFF, Epi>;
+    auto kern = k_spmv_dia<VT, OFF, Epi, ND>;
     static int occ[kLaunchCacheDevices] = {};
     if (ctx->device >= kLaunchCacheDevices) {
       set_error("device ordinal %d beyond %d", ctx->device, kLaunchCacheDevices);

@@ -126,9 +126,11 @@ cfd_status cfd_csr_layout(const cfd_csr* a, cfd_layout_info* out);
  * every entry on one of at most 8 diagonals (column - row) with at most 10 %
  * empty slots (stencil operators); values stored diagonal-major, no indices.
  * It adds an empty slot as 0 * x, identical to skipping it for finite x.
- * AUTO (the default): RECORD for FP32 (on the 256^3 fine operator SLICED runs
- * the plain SpMV as fast and the fused epilogues slower); X_STAGED for FP64
- * when eligible with one thread per row, SPLIT otherwise. TIMED: at the
+ * AUTO (the default): DIAGONAL when eligible (on the 256^3 7-point operator
+ * it beats the record and x-staged pipelines in both precisions); otherwise
+ * RECORD for FP32 (SLICED runs the plain SpMV as fast and the fused epilogues
+ * slower), X_STAGED for FP64 when eligible with one thread per row, SPLIT
+ * otherwise. TIMED: at the
  * next SpMV in that precision, time the eligible pipelines (allocates scratch
  * vectors) and keep the fastest. */
 typedef enum {

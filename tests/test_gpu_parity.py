@@ -153,7 +153,9 @@ def test_spmv_pipelines_bit_identical(cuda, shape):
             chosen = d.layout()["path_f32" if fp32 else "path_f64"]
             eligible = paths + (["sliced"] if fp32 and lay["sliced"] else [])
             assert chosen in [{"split": 0, "record": 1, "x_staged": 2, "sliced": 3, "diagonal": 4}[p] for p in eligible]
-            if mode == "auto" and fp32:
+            if mode == "auto" and lay["diagonals"]:
+                assert chosen == 4
+            elif mode == "auto" and fp32:
                 assert chosen == (1 if lay["all_compressed"] else 0)
 
 @pytest.mark.parametrize("interp,order", [(0, 0), (2, 0), (2, 1)])
