@@ -847,28 +847,55 @@ static __global__ void __launch_bounds__(kThreads) k_sl_gather(int64_t slots, co
 
 // ---------------------------------------------------------------------------
 // Diagonal pipeline (DevMat::dia): values stored diagonal-major, no indices.
-// Each thread takes kDiaRows rows kThreads apart (grid-stride over spans of
-// kThreads * kDiaRows rows), so every value, x and epilogue access of a warp
-// is to consecutive addresses. Each row adds its diagonals in ascending offset
-// (= the CSR order) one product at a time with the same expression as
+// Grid-stride over spans of kThreads * V rows, V = 16 / sizeof(VT) (4 FP32
+// rows, 2 FP64 rows per thread). Each row adds its diagonals in ascending
+// offset (= the CSR order) one product at a time with the same expression as
 // rows_from_stage, so y = A x is bit-identical to the other pipelines for
-// finite x (a slot without an entry holds 0 and adds +-0). Values are read with
-// the streaming hint: they are used once, while x is re-read by the rows one
-// plane away.
-// Interior spans (every row live, every x index of every diagonal inside
-// [0, nrows)) take a path without predicates: per diagonal one base pointer
-// for the values and one for x, the kDiaRows loads at immediate offsets, all
-// loads of the span issued before the products. ND > 0 fixes the diagonal
-// count at compile time (the 5- and 7-point stencils); ND = 0 takes any count
-// up to kDiaMax with predicated slots. Boundary spans take the predicated path.
+// finite x (a slot without an entry holds 0 and adds +-0). Values are read
+// with the streaming hint: they are used once, while x is re-read by the rows
+// one grid line or plane away. Three paths per span:
+//  - interior span (every row live, every x index of every diagonal inside
+//    [0, nrows)) with a 16-byte aligned x: each thread owns V consecutive
+//    rows; per diagonal one 16-byte value load; x for the offset 0 by one
+//    16-byte load, for offsets that are multiples of V by one 16-byte load,
+//    for offsets -1 and +1 from the offset-0 vectors of the neighbouring lanes
+//    by shuffle (the warp's end lanes load their one missing entry), for any
+//    other offset entry by entry. All loads of a span are issued before the
+//    products.
+//  - interior span, x not 16-byte aligned: V rows kThreads apart per thread,
+//    loads at immediate offsets from one base pointer per diagonal.
+//  - boundary span: the same mapping with every load predicated.
+// ND > 0 fixes the diagonal count at compile time (the 5- and 7-point
+// stencils); ND = 0 takes any count up to kDiaMax.
 template <typename VT>
 struct DiaView {
   const VT* __restrict__ val;  // n diagonals of ld entries
   int64_t ld;
-  int nrows, n, main;
+  int nrows, n, main, xvec;  // xvec: x is 16-byte aligned
   int off[kDiaMax];
 };
-constexpr int kDiaRows = 2;
+template <typename VT>
+struct DiaVec;
+template <>
+struct DiaVec<float> {
+  using type = float4;
+  static constexpr int V = 4;
+  __device__ static void unpack(const float4& a, float (&o)[4]) {
+    o[0] = a.x;
+    o[1] = a.y;
+    o[2] = a.z;
+    o[3] = a.w;
+  }
+};
+template <>
+struct DiaVec<double> {
+  using type = double2;
+  static constexpr int V = 2;
+  __device__ static void unpack(const double2& a, double (&o)[2]) {
+    o[0] = a.x;
+    o[1] = a.y;
+  }
+};
 
 template <typename VT, bool OFFDIAG, int NS>
 __device__ __forceinline__ void dia_sum(const VT (&v)[NS], const VT (&xv)[NS], int nd, int main, VT& sum,
@@ -888,46 +915,99 @@ __device__ __forceinline__ void dia_sum(const VT (&v)[NS], const VT (&xv)[NS], i
 template <typename VT, bool OFFDIAG, class Epi, int ND>
 __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, const VT* __restrict__ x, Epi epi) {
   if (epi.skip()) return;
+  using Vec = DiaVec<VT>;
+  constexpr int V = Vec::V;
   constexpr int NS = ND > 0 ? ND : kDiaMax;  // slots per row in registers
   double red[Epi::NRED > 0 ? Epi::NRED : 1];
 #pragma unroll
   for (int q = 0; q < (Epi::NRED > 0 ? Epi::NRED : 1); ++q) red[q] = 0.0;
   const int nd = ND > 0 ? ND : D.n;
-  const int64_t span = (int64_t)kThreads * kDiaRows;
+  const int64_t span = (int64_t)kThreads * V;
   const int omin = D.off[0], omax = D.off[nd - 1];
+  const int lane = threadIdx.x & 31;
   for (int64_t s0 = (int64_t)blockIdx.x * span; s0 < D.nrows; s0 += (int64_t)gridDim.x * span) {
     const bool interior = s0 + omin >= 0 && s0 + span + omax <= D.nrows && s0 + span <= D.nrows;
-    const int r0 = (int)s0 + threadIdx.x;
-    typename Epi::Pre pre[kDiaRows];
-    VT v[kDiaRows][NS], xv[kDiaRows][NS];
-    if (interior) {
+    typename Epi::Pre pre[V];
+    VT v[V][NS], xv[V][NS];
+    if (interior && D.xvec) {
+      const int r0 = (int)s0 + threadIdx.x * V;  // V consecutive rows
 #pragma unroll
-      for (int q = 0; q < kDiaRows; ++q) pre[q] = epi.load(r0 + q * kThreads);
+      for (int q = 0; q < V; ++q) pre[q] = epi.load(r0 + q);
+      VT x0[V];
+      Vec::unpack(__ldg(reinterpret_cast<const typename Vec::type*>(x + r0)), x0);
+#pragma unroll
+      for (int d = 0; d < NS; ++d) {
+        VT vd[V], xd[V];
+        if (ND > 0 || d < nd) {
+          const int o = D.off[d];
+          Vec::unpack(__ldcs(reinterpret_cast<const typename Vec::type*>(D.val + (int64_t)d * D.ld + r0)), vd);
+          if (o == 0) {
+#pragma unroll
+            for (int q = 0; q < V; ++q) xd[q] = x0[q];
+          } else if (o % V == 0) {
+            Vec::unpack(__ldg(reinterpret_cast<const typename Vec::type*>(x + r0 + o)), xd);
+          } else if (o == -1) {
+            VT prev = __shfl_up_sync(0xffffffffu, x0[V - 1], 1);
+            if (lane == 0) prev = __ldg(x + r0 - 1);
+            xd[0] = prev;
+#pragma unroll
+            for (int q = 1; q < V; ++q) xd[q] = x0[q - 1];
+          } else if (o == 1) {
+            VT next = __shfl_down_sync(0xffffffffu, x0[0], 1);
+            if (lane == 31) next = __ldg(x + r0 + V);
+#pragma unroll
+            for (int q = 0; q < V - 1; ++q) xd[q] = x0[q + 1];
+            xd[V - 1] = next;
+          } else {
+#pragma unroll
+            for (int q = 0; q < V; ++q) xd[q] = __ldg(x + r0 + q + o);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < V; ++q) vd[q] = xd[q] = VT(0);
+        }
+#pragma unroll
+        for (int q = 0; q < V; ++q) {
+          v[q][d] = vd[q];
+          xv[q][d] = xd[q];
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < V; ++q) {
+        VT sum = VT(0), diag = VT(0);
+        dia_sum<VT, OFFDIAG, NS>(v[q], xv[q], nd, D.main, sum, diag);
+        epi.row(r0 + q, sum, diag, pre[q], red);
+      }
+    } else if (interior) {
+      const int r0 = (int)s0 + threadIdx.x;  // V rows kThreads apart
+#pragma unroll
+      for (int q = 0; q < V; ++q) pre[q] = epi.load(r0 + q * kThreads);
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
         if (ND > 0 || d < nd) {
           const VT* vp = D.val + (int64_t)d * D.ld + r0;
           const VT* xp = x + (r0 + D.off[d]);
 #pragma unroll
-          for (int q = 0; q < kDiaRows; ++q) {
+          for (int q = 0; q < V; ++q) {
             v[q][d] = __ldcs(vp + q * kThreads);
             xv[q][d] = __ldg(xp + q * kThreads);
           }
         } else {
 #pragma unroll
-          for (int q = 0; q < kDiaRows; ++q) v[q][d] = xv[q][d] = VT(0);
+          for (int q = 0; q < V; ++q) v[q][d] = xv[q][d] = VT(0);
         }
       }
 #pragma unroll
-      for (int q = 0; q < kDiaRows; ++q) {
+      for (int q = 0; q < V; ++q) {
         VT sum = VT(0), diag = VT(0);
         dia_sum<VT, OFFDIAG, NS>(v[q], xv[q], nd, D.main, sum, diag);
         epi.row(r0 + q * kThreads, sum, diag, pre[q], red);
       }
     } else {
-      bool live[kDiaRows];
+      const int r0 = (int)s0 + threadIdx.x;
+      bool live[V];
 #pragma unroll
-      for (int q = 0; q < kDiaRows; ++q) {
+      for (int q = 0; q < V; ++q) {
         const int row = r0 + q * kThreads;
         live[q] = row < D.nrows;
         pre[q] = typename Epi::Pre{};
@@ -939,7 +1019,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, const VT* 
         const VT* vd = D.val + (int64_t)d * D.ld;
         const int o = act ? D.off[d] : 0;
 #pragma unroll
-        for (int q = 0; q < kDiaRows; ++q) {
+        for (int q = 0; q < V; ++q) {
           const int row = r0 + q * kThreads;
           const int j = row + o;
           const bool in = act && live[q];
@@ -948,7 +1028,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, const VT* 
         }
       }
 #pragma unroll
-      for (int q = 0; q < kDiaRows; ++q) {
+      for (int q = 0; q < V; ++q) {
         VT sum = VT(0), diag = VT(0);
         dia_sum<VT, OFFDIAG, NS>(v[q], xv[q], nd, D.main, sum, diag);
         if (live[q]) epi.row(r0 + q * kThreads, sum, diag, pre[q], red);

@@ -653,11 +653,14 @@ struct Launcher {
       CFD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kThreads, 0));
       occ[ctx->device] = std::max(1, o);
     }
-    const int64_t spans = (m.nrows + (int64_t)kThreads * kDiaRows - 1) / ((int64_t)kThreads * kDiaRows);
+    const int64_t span = (int64_t)kThreads * DiaVec<VT>::V;
+    const int64_t spans = (m.nrows + span - 1) / span;
     // at most one reduction slot per CTA (the context's partials)
     const int grid = (int)std::max<int64_t>(
         1, std::min<int64_t>({spans, (int64_t)ctx->num_sms * occ[ctx->device], (int64_t)ctx->partial_capacity}));
-    kern<<<grid, kThreads, 0, s>>>(dia_view<VT>(m), x, epi);
+    DiaView<VT> D = dia_view<VT>(m);
+    D.xvec = ((uintptr_t)x & 15) == 0;
+    kern<<<grid, kThreads, 0, s>>>(D, x, epi);
     return CFD_OK;
   }
   // The diagonal pipeline runs when the values of this precision are there

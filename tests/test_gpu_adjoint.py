@@ -149,11 +149,21 @@ def test_darcy_kernels_refuse_other_patterns(cuda):
     from cfdrs_b200 import _lib
     from cfdrs_b200 import problems as P
     from cfdrs_b200.adjoint import SparseSolver, darcy_2d_assemble_device
-    A, _ = P.poisson_2d_dirichlet(16)
+    import scipy.sparse as sp
+    from cfdrs_b200.sparse import CsrMatrix
+    # 256 rows but a 9-point pattern
+    S = sp.diags([1.0] * 9, [-17, -16, -15, -1, 0, 1, 15, 16, 17], shape=(256, 256)).tocsr()
+    A = CsrMatrix(S.indptr.astype(np.int64), S.indices.astype(np.int64), S.data, S.shape)
     s = SparseSolver(A, preconditioner="jacobi", precision=cf.Precision.FP64)
     with pytest.raises(_lib.CfdError, match="Darcy pattern") as e:
         darcy_2d_assemble_device(torch.zeros((16, 16), dtype=torch.float64, device="cuda"), s)
     assert e.value.status == 1
+    # the 5-point pattern of a 16 x 16 grid is that pattern; a 15 x 15 theta does not fit it
+    A5, _ = P.poisson_2d_dirichlet(16)
+    s5 = SparseSolver(A5, preconditioner="jacobi", precision=cf.Precision.FP64)
+    darcy_2d_assemble_device(torch.zeros((16, 16), dtype=torch.float64, device="cuda"), s5)
+    with pytest.raises(_lib.CfdError, match="Darcy pattern"):
+        darcy_2d_assemble_device(torch.zeros((15, 15), dtype=torch.float64, device="cuda"), s5)
 
 
 def test_darcy_512_fused_gradient(cuda):
