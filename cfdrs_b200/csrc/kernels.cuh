@@ -133,6 +133,25 @@ __device__ __forceinline__ bool diag_ok<float>(float d) {
   return fabsf(d) > 1e-15f;
 }
 
+// Quotient of the damped-Jacobi sweeps: the FP32 (inner) sweeps divide with
+// the fast single-precision division (within 2 ulp; the IEEE division's
+// multi-instruction sequence made the sweep passes compute-bound), the FP64
+// sweeps with the IEEE division.
+template <typename XT>
+__device__ __forceinline__ XT sweep_div(XT a, XT b) {
+  return a / b;
+}
+template <>
+__device__ __forceinline__ float sweep_div<float>(float a, float b) {
+  return __fdividef(a, b);
+}
+// First damped-Jacobi sweep from a zero iterate, one entry: w b / a_ii, or 0
+// where |a_ii| <= 1e-15 (the smoother's skip).
+template <typename XT>
+__device__ __forceinline__ XT smooth0_value(XT b, XT d, XT omega) {
+  return diag_ok<XT>(d) ? omega * sweep_div<XT>(b, d) : XT(0);
+}
+
 // ---------------------------------------------------------------------------
 // Epilogues. load(i) fetches the row's own operands (issued before the x
 // gathers so the latencies overlap); row(i, sum, diag, pre, acc) finishes it.
@@ -248,9 +267,47 @@ struct EpiJacobi {
     XT out = p.xo;
     if (diag_ok<XT>((XT)d)) {
       // FP32 (inner) sweeps: the fast single-precision division (within 2 ulp)
-      const XT nv = std::is_same<XT, float>::value ? (XT)__fdividef((float)(p.b - (XT)s), (float)d)
-                                                   : (p.b - (XT)s) / (XT)d;
+      const XT nv = sweep_div<XT>(p.b - (XT)s, (XT)d);
       out = p.xo + omega * (nv - p.xo);
+    }
+    xn[i] = out;
+    if (DOT) acc[0] += (double)p.b * (double)out;
+  }
+  __device__ void finish(const double* tot) const {
+    if (DOT == 1) st->rho = tot[0];
+    if (DOT == 2) pcg_rho_update(st, tot[0]);
+  }
+};
+
+// The same damped-Jacobi sweep for the FP32 (inner) V-cycle, in residual form
+// over the full row sum s = sum_j a_ij xo_j (no per-entry diagonal test):
+//   xn_i = xo_i + w (b_i - s) / a_ii,  xn_i = xo_i if |a_ii| <= 1e-15,
+// a_ii from the level's diagonal array. Equal to the split form above in exact
+// arithmetic; it rounds differently, and the inner solve only needs a fixed
+// symmetric smoother (the FP64 sweeps keep the split form of
+// smoothers.rs:177-186).
+template <typename XT, int DOT>
+struct EpiJacobiR {
+  static constexpr int NRED = DOT ? 1 : 0;
+  struct Pre {
+    XT xo, b, d;
+  };
+  XT* __restrict__ xn;
+  const XT* __restrict__ xo;
+  const XT* __restrict__ b;
+  const XT* __restrict__ diag;
+  XT omega;
+  DevState* st;
+  const int* done;
+  Red red;
+  __device__ bool skip() const { return flag_set(done); }
+  __device__ Pre load(int i) const { return {xo[i], b[i], diag[i]}; }
+  template <typename S>
+  __device__ void row(int i, S s, S, const Pre& p, double* acc) const {
+    XT out = p.xo;
+    if (diag_ok<XT>(p.d)) {
+      const XT q = sweep_div<XT>(p.b - (XT)s, p.d);
+      out = p.xo + omega * q;
     }
     xn[i] = out;
     if (DOT) acc[0] += (double)p.b * (double)out;
@@ -855,7 +912,7 @@ static __global__ void __launch_bounds__(kThreads) k_sl_gather(int64_t slots, co
 // with the streaming hint: they are used once, while x is re-read by the rows
 // one grid line or plane away. Three paths per span:
 //  - interior span (every row live, every x index of every diagonal inside
-//    [0, nrows)) with a 16-byte aligned x: each thread owns V consecutive
+//    [0, nrows)) with 16-byte aligned x arrays: each thread owns V consecutive
 //    rows; per diagonal one 16-byte value load; x for the offset 0 by one
 //    16-byte load, for offsets that are multiples of V by one 16-byte load,
 //    for offsets -1 and +1 from the offset-0 vectors of the neighbouring lanes
@@ -897,6 +954,46 @@ struct DiaVec<double> {
   }
 };
 
+// x operand of the diagonal pipeline. DiaXPlain reads a stored x.
+// DiaXSmooth0 is the first damped-Jacobi sweep from zero, x_j = w b_j / a_jj,
+// formed where it is read (the V-cycle's pre-smoothing fused into its residual
+// r = b - A x): the same expression as k_smooth0, so the same bits; the
+// kernel also stores x of the span's own rows for the rest of the cycle.
+template <typename VT>
+struct DiaXPlain {
+  using Vec = DiaVec<VT>;
+  static constexpr bool kStore = false;
+  const VT* __restrict__ x;
+  __device__ VT one(int j) const { return __ldg(x + j); }
+  __device__ void vec(int j, VT (&o)[Vec::V]) const {
+    Vec::unpack(__ldg(reinterpret_cast<const typename Vec::type*>(x + j)), o);
+  }
+  __device__ void store(int, const VT (&)[Vec::V]) const {}
+  __device__ void store1(int, VT) const {}
+};
+template <typename VT>
+struct DiaXSmooth0 {
+  using Vec = DiaVec<VT>;
+  static constexpr bool kStore = true;
+  const VT* __restrict__ b;
+  const VT* __restrict__ d;
+  VT omega;
+  VT* __restrict__ xout;
+  __device__ VT one(int j) const { return smooth0_value<VT>(__ldg(b + j), __ldg(d + j), omega); }
+  __device__ void vec(int j, VT (&o)[Vec::V]) const {
+    VT bv[Vec::V], dv[Vec::V];
+    Vec::unpack(__ldg(reinterpret_cast<const typename Vec::type*>(b + j)), bv);
+    Vec::unpack(__ldg(reinterpret_cast<const typename Vec::type*>(d + j)), dv);
+#pragma unroll
+    for (int q = 0; q < Vec::V; ++q) o[q] = smooth0_value<VT>(bv[q], dv[q], omega);
+  }
+  __device__ void store(int r0, const VT (&v)[Vec::V]) const {
+#pragma unroll
+    for (int q = 0; q < Vec::V; ++q) xout[r0 + q] = v[q];
+  }
+  __device__ void store1(int r, VT v) const { xout[r] = v; }
+};
+
 template <typename VT, bool OFFDIAG, int NS>
 __device__ __forceinline__ void dia_sum(const VT (&v)[NS], const VT (&xv)[NS], int nd, int main, VT& sum,
                                         VT& diag) {
@@ -912,8 +1009,8 @@ __device__ __forceinline__ void dia_sum(const VT (&v)[NS], const VT (&xv)[NS], i
   }
 }
 
-template <typename VT, bool OFFDIAG, class Epi, int ND>
-__global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, const VT* __restrict__ x, Epi epi) {
+template <typename VT, bool OFFDIAG, class Epi, int ND, class XS>
+__global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, XS xs, Epi epi) {
   if (epi.skip()) return;
   using Vec = DiaVec<VT>;
   constexpr int V = Vec::V;
@@ -934,7 +1031,8 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, const VT* 
 #pragma unroll
       for (int q = 0; q < V; ++q) pre[q] = epi.load(r0 + q);
       VT x0[V];
-      Vec::unpack(__ldg(reinterpret_cast<const typename Vec::type*>(x + r0)), x0);
+      xs.vec(r0, x0);
+      if constexpr (XS::kStore) xs.store(r0, x0);
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
         VT vd[V], xd[V];
@@ -945,22 +1043,22 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, const VT* 
 #pragma unroll
             for (int q = 0; q < V; ++q) xd[q] = x0[q];
           } else if (o % V == 0) {
-            Vec::unpack(__ldg(reinterpret_cast<const typename Vec::type*>(x + r0 + o)), xd);
+            xs.vec(r0 + o, xd);
           } else if (o == -1) {
             VT prev = __shfl_up_sync(0xffffffffu, x0[V - 1], 1);
-            if (lane == 0) prev = __ldg(x + r0 - 1);
+            if (lane == 0) prev = xs.one(r0 - 1);
             xd[0] = prev;
 #pragma unroll
             for (int q = 1; q < V; ++q) xd[q] = x0[q - 1];
           } else if (o == 1) {
             VT next = __shfl_down_sync(0xffffffffu, x0[0], 1);
-            if (lane == 31) next = __ldg(x + r0 + V);
+            if (lane == 31) next = xs.one(r0 + V);
 #pragma unroll
             for (int q = 0; q < V - 1; ++q) xd[q] = x0[q + 1];
             xd[V - 1] = next;
           } else {
 #pragma unroll
-            for (int q = 0; q < V; ++q) xd[q] = __ldg(x + r0 + q + o);
+            for (int q = 0; q < V; ++q) xd[q] = xs.one(r0 + q + o);
           }
         } else {
 #pragma unroll
@@ -981,16 +1079,19 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, const VT* 
     } else if (interior) {
       const int r0 = (int)s0 + threadIdx.x;  // V rows kThreads apart
 #pragma unroll
-      for (int q = 0; q < V; ++q) pre[q] = epi.load(r0 + q * kThreads);
+      for (int q = 0; q < V; ++q) {
+        pre[q] = epi.load(r0 + q * kThreads);
+        if constexpr (XS::kStore) xs.store1(r0 + q * kThreads, xs.one(r0 + q * kThreads));
+      }
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
         if (ND > 0 || d < nd) {
           const VT* vp = D.val + (int64_t)d * D.ld + r0;
-          const VT* xp = x + (r0 + D.off[d]);
+          const int xo = r0 + D.off[d];
 #pragma unroll
           for (int q = 0; q < V; ++q) {
             v[q][d] = __ldcs(vp + q * kThreads);
-            xv[q][d] = __ldg(xp + q * kThreads);
+            xv[q][d] = xs.one(xo + q * kThreads);
           }
         } else {
 #pragma unroll
@@ -1011,7 +1112,10 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, const VT* 
         const int row = r0 + q * kThreads;
         live[q] = row < D.nrows;
         pre[q] = typename Epi::Pre{};
-        if (live[q]) pre[q] = epi.load(row);
+        if (live[q]) {
+          pre[q] = epi.load(row);
+          if constexpr (XS::kStore) xs.store1(row, xs.one(row));
+        }
       }
 #pragma unroll
       for (int d = 0; d < NS; ++d) {
@@ -1024,7 +1128,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, const VT* 
           const int j = row + o;
           const bool in = act && live[q];
           v[q][d] = in ? __ldcs(vd + row) : VT(0);
-          xv[q][d] = (in && j >= 0 && j < D.nrows) ? __ldg(x + j) : VT(0);
+          xv[q][d] = (in && j >= 0 && j < D.nrows) ? xs.one(j) : VT(0);
         }
       }
 #pragma unroll

@@ -48,26 +48,14 @@ inline int vec_grid(int64_t n) {
 // ---------------------------------------------------------------------------
 // Vector kernels.
 
-// First damped-Jacobi sweep from a zero iterate: x = w (b / a_ii). The FP32
-// (inner) sweep divides with the fast single-precision division (within 2 ulp;
-// the IEEE division's multi-instruction sequence made this pass compute-bound),
-// the FP64 sweep with the IEEE division.
-template <typename XT>
-__device__ __forceinline__ XT sweep_div(XT a, XT b) {
-  return a / b;
-}
-template <>
-__device__ __forceinline__ float sweep_div<float>(float a, float b) {
-  return __fdividef(a, b);
-}
-
+// First damped-Jacobi sweep from a zero iterate: x = w (b / a_ii)
+// (smooth0_value: the FP32 sweep divides with the fast division).
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_smooth0(int64_t n, const XT* __restrict__ b, const XT* __restrict__ d,
                                                       XT omega, XT* __restrict__ x, const int* done) {
   if (flag_set(done)) return;
   GRID_STRIDE_U4(i, n, {
-    const XT di = d[i];
-    x[i] = diag_ok<XT>(di) ? omega * sweep_div<XT>(b[i], di) : XT(0);
+    x[i] = smooth0_value<XT>(b[i], d[i], omega);
   })
 }
 
@@ -634,15 +622,39 @@ struct Launcher {
   }
   template <typename VT, bool OFF, class Epi>
   cfd_status dia_launch(const DevMat& m, const VT* x, Epi epi) {
-    if (m.dia_n == 7) return dia_launch_n<VT, OFF, Epi, 7>(m, x, epi);
-    if (m.dia_n == 5) return dia_launch_n<VT, OFF, Epi, 5>(m, x, epi);
-    return dia_launch_n<VT, OFF, Epi, 0>(m, x, epi);
+    return dia_launch_xs<VT, OFF, Epi>(m, DiaXPlain<VT>{x}, ((uintptr_t)x & 15) == 0, epi);
+  }
+  // xvec: every array the x source reads (and stores) is 16-byte aligned.
+  template <typename VT, bool OFF, class Epi, class XS>
+  cfd_status dia_launch_xs(const DevMat& m, XS xs, bool xvec, Epi epi) {
+    if (m.dia_n == 7) return dia_launch_n<VT, OFF, Epi, 7, XS>(m, xs, xvec, epi);
+    if (m.dia_n == 5) return dia_launch_n<VT, OFF, Epi, 5, XS>(m, xs, xvec, epi);
+    return dia_launch_n<VT, OFF, Epi, 0, XS>(m, xs, xvec, epi);
+  }
+  // The V-cycle's pre-smoothing from zero fused into its residual on the
+  // diagonal pipeline: x = w D^-1 b (stored) and r = b - A x in one pass.
+  // Returns false (nothing launched) when the operator does not run the
+  // diagonal pipeline in this precision.
+  template <typename XT>
+  cfd_status dia_smooth0_residual(const DevMat& m, const XT* b, const XT* d, XT omega, XT* x, XT* r,
+                                  const int* done, bool* ran) {
+    *ran = false;
+    const int p = sizeof(XT) == 4 ? 0 : 1;
+    if (m.nrows == 0 || !dia_ready<XT>(m)) return CFD_OK;
+    if (m.path[p] == kPathTimed) CFD_TRY(tune<XT>(m));
+    if (spmv_path(m, p) != kPathDiag) return CFD_OK;
+    EpiResidual<XT, 0> epi{r, b, nullptr, done, {}};
+    epi.red = red();
+    const bool xvec = (((uintptr_t)b | (uintptr_t)d | (uintptr_t)x) & 15) == 0;
+    CFD_TRY((dia_launch_xs<XT, false, EpiResidual<XT, 0>>(m, DiaXSmooth0<XT>{b, d, omega, x}, xvec, epi)));
+    *ran = true;
+    return finish_spmv<XT, XT>(m);
   }
   // ND: the diagonal count fixed at compile time (0: any count up to kDiaMax).
-  template <typename VT, bool OFF, class Epi, int ND>
-  cfd_status dia_launch_n(const DevMat& m, const VT* x, Epi epi) {
+  template <typename VT, bool OFF, class Epi, int ND, class XS>
+  cfd_status dia_launch_n(const DevMat& m, XS xs, bool xvec, Epi epi) {
     CFD_TRY(dia_refresh(m));
-    auto kern = k_spmv_dia<VT, OFF, Epi, ND>;
+    auto kern = k_spmv_dia<VT, OFF, Epi, ND, XS>;
     static int occ[kLaunchCacheDevices] = {};
     if (ctx->device >= kLaunchCacheDevices) {
       set_error("device ordinal %d beyond %d", ctx->device, kLaunchCacheDevices);
@@ -659,8 +671,8 @@ struct Launcher {
     const int grid = (int)std::max<int64_t>(
         1, std::min<int64_t>({spans, (int64_t)ctx->num_sms * occ[ctx->device], (int64_t)ctx->partial_capacity}));
     DiaView<VT> D = dia_view<VT>(m);
-    D.xvec = ((uintptr_t)x & 15) == 0;
-    kern<<<grid, kThreads, 0, s>>>(D, x, epi);
+    D.xvec = xvec ? 1 : 0;
+    kern<<<grid, kThreads, 0, s>>>(D, xs, epi);
     return CFD_OK;
   }
   // The diagonal pipeline runs when the values of this precision are there
@@ -826,9 +838,17 @@ const float* diag_of<float>(const DevLevel& L) {
 template <typename XT>
 static cfd_status jacobi_sweep(Launcher& lc, const DevLevel& L, const XT* xo, XT* xn, const XT* b, XT omega,
                                int dot, DevState* st, const int* done) {
-  if (dot == 1) return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 1>{xn, xo, b, omega, st, done, {}});
-  if (dot == 2) return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 2>{xn, xo, b, omega, st, done, {}});
-  return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 0>{xn, xo, b, omega, st, done, {}});
+  if constexpr (std::is_same<XT, float>::value) {
+    // FP32 (inner) sweeps: the residual form over the full row (EpiJacobiR)
+    const float* d = diag_of<float>(L);
+    if (dot == 1) return lc.spmv<float, float, false>(L.A, xo, EpiJacobiR<float, 1>{xn, xo, b, d, omega, st, done, {}});
+    if (dot == 2) return lc.spmv<float, float, false>(L.A, xo, EpiJacobiR<float, 2>{xn, xo, b, d, omega, st, done, {}});
+    return lc.spmv<float, float, false>(L.A, xo, EpiJacobiR<float, 0>{xn, xo, b, d, omega, st, done, {}});
+  } else {
+    if (dot == 1) return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 1>{xn, xo, b, omega, st, done, {}});
+    if (dot == 2) return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 2>{xn, xo, b, omega, st, done, {}});
+    return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 0>{xn, xo, b, omega, st, done, {}});
+  }
 }
 
 template <typename XT>
@@ -868,20 +888,25 @@ static cfd_status vcycle(Launcher& lc, cfd_amg* amg, size_t l, const XT* b, XT* 
     }
     return CFD_OK;
   }
-  // 1. pre-smoothing from x = 0
+  // 1. pre-smoothing from x = 0 and 2. the residual r = b - A x; with one
+  // sweep on the diagonal pipeline both in one pass
   XT* x = V.xa;
   XT* y = V.xb;
-  if (c.pre_smooth >= 1) {
-    CFD_TRY(lc.vec(n, k_smooth0<XT>, b, diag_of<XT>(L), omega, x, done));
-    for (int s = 1; s < c.pre_smooth; ++s) {
-      CFD_TRY(jacobi_sweep<XT>(lc, L, x, y, b, omega, 0, st, done));
-      std::swap(x, y);
+  bool fused = false;
+  if (c.pre_smooth == 1)
+    CFD_TRY(lc.dia_smooth0_residual<XT>(L.A, b, diag_of<XT>(L), omega, x, V.r, done, &fused));
+  if (!fused) {
+    if (c.pre_smooth >= 1) {
+      CFD_TRY(lc.vec(n, k_smooth0<XT>, b, diag_of<XT>(L), omega, x, done));
+      for (int s = 1; s < c.pre_smooth; ++s) {
+        CFD_TRY(jacobi_sweep<XT>(lc, L, x, y, b, omega, 0, st, done));
+        std::swap(x, y);
+      }
+    } else {
+      CFD_TRY(lc.vec(n, k_fill<XT>, x, XT(0), done));
     }
-  } else {
-    CFD_TRY(lc.vec(n, k_fill<XT>, x, XT(0), done));
+    CFD_TRY(lc.spmv<XT, XT, false>(L.A, x, EpiResidual<XT, 0>{V.r, b, nullptr, done, {}}));
   }
-  // 2. residual r = b - A x
-  CFD_TRY(lc.spmv<XT, XT, false>(L.A, x, EpiResidual<XT, 0>{V.r, b, nullptr, done, {}}));
   // 3. restriction to the next level's right-hand side
   DevLevel& Lc = amg->dev[l + 1];
   LevelVecs<XT>& Vc = vecs<XT>(Lc);

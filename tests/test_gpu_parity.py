@@ -205,6 +205,27 @@ def test_vcycle_matches_oracle(cuda, oracle, coarse):
     assert rel(z, oamg.apply(r)) < 1e-11
 
 
+def test_vcycle_bits_do_not_depend_on_the_pipeline(cuda):
+    """One V-cycle (FP64, no dot products) gives the same bits whichever
+    pipeline the operators run: on the diagonal pipeline the pre-smoothing
+    sweep is fused into the fine residual (x = w D^-1 b formed where it is
+    read), which must equal the separate sweep and residual of the others."""
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    A = P.poisson_3d_variable(24, 4.0, 1.0, seed=6)[0]
+    cfg = cf.AMGConfig.pressure_poisson()
+    cfg.min_coarse_size = 100
+    amg = cf.AlgebraicMultigrid(A, cfg)
+    r = np.random.default_rng(3).uniform(-1, 1, A.nrows)
+    zs = []
+    for path in ("diagonal", "record", "split", "auto"):
+        amg.set_path(path, False)
+        zs.append(amg.apply_to(r))
+    amg.set_path("auto", False)
+    for z in zs[1:]:
+        assert np.array_equal(z.view(np.int64), zs[0].view(np.int64))
+
+
 def _oracle_solve(oracle, A, b, pre, solver="pcg", amg=None, rtol=1e-8, max_it=5000):
     Ao = oracle.Csr.from_matrix(A)
     return getattr(oracle, solver)(Ao, b, precond=pre, amg=amg, rtol=rtol, max_it=max_it)
