@@ -194,6 +194,12 @@ cfd_status devmat_upload(DevMat& m, const HostCsr& h, bool want32, cudaStream_t 
       for (int d = 0; d < kDiaMax; ++d) m.dia_off[d] = D.off[d];
       m.dia_ld = D.ld;
       m.dia_stale = true;
+      if (!D.mask.empty()) {
+        CFD_TRY(dmalloc(&m.dia_mask, (int64_t)D.mask.size()));
+        CFD_TRY_CUDA(cudaMemcpyAsync(m.dia_mask, D.mask.data(), D.mask.size() * sizeof(uint32_t),
+                                     cudaMemcpyHostToDevice, s));
+        CFD_TRY_CUDA(cudaStreamSynchronize(s));  // D.mask is released when this block ends
+      }
     }
   }
   CFD_TRY_CUDA(cudaMemcpyAsync(m.rp, rp32.data(), rp32.size() * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -255,6 +261,7 @@ void devmat_free(DevMat& m) {
   dfree(m.sl_v32);
   dfree(m.dia64);
   dfree(m.dia32);
+  dfree(m.dia_mask);
   m.dia = false;
   m.dia_n = 0;
   m.dia_main = -1;

@@ -1,19 +1,24 @@
-// Diagonal SpMV layout (DevMat::dia, k_spmv_dia): eligibility and the host
-// evaluation that mirrors the kernel.
+// Diagonal SpMV layout (DevMat::dia, k_spmv_dia, k_spmv_dia_gen): eligibility
+// and the host evaluation that mirrors the kernels.
 //
-// Stencil operators (the 7-point finite-volume operator of a structured grid,
-// the 5-point operator in 2-D) put every entry on a handful of diagonals
-// column - row. Stored diagonal-major, their values stream with coalesced
-// loads and no index array at all: 4 (FP32) or 8 (FP64) bytes per slot instead
-// of value + one-byte code + row record, and the x entries of a warp's rows
-// are consecutive for every diagonal. Slots without an entry hold 0.
+// Stencil operators put every entry on a handful of diagonals column - row:
+// 7 for the 3-D finite-volume operator, 5 in 2-D, and 23 for the Galerkin
+// operator of the first coarse level of a Ruge-Stueben hierarchy on such a grid
+// (its coarse points form a regular sub-lattice in ascending numbering). Stored
+// diagonal-major, their values stream with coalesced loads and no index array:
+// 4 (FP32) or 8 (FP64) bytes per slot instead of value + one-byte code + row
+// record, and the x entries of a warp's rows are consecutive for every
+// diagonal. Slots without an entry hold 0.
 //
-// Summation order: each row adds its diagonals in ascending offset, which is
-// ascending column and so the stored CSR order, one product at a time as the
-// one-thread-per-row CSR pipelines do. A slot without an entry adds 0 * x = +-0,
-// which leaves a finite partial sum unchanged (a sum that starts at +0 never
-// becomes -0 by adding +-0 products), so y = A x is bit-identical to the other
-// pipelines for finite x.
+// Summation order. Every pipeline sums a row in the order of its row group of
+// tpr threads: thread l adds the stored entries at positions l, l + tpr, ...
+// (in column order) one product at a time, then the group combines its partial
+// sums by a butterfly. The diagonal kernels keep tpr partial sums per row and
+// assign each stored entry to the partial its position selects, so their row
+// sums are those of the other pipelines bit for bit. For tpr = 1 an empty slot
+// adds 0 * x = +-0, which leaves a partial sum that starts at +0 unchanged for
+// finite x; for tpr > 1 a per-row presence mask marks the stored entries, so
+// the positions (and the skipped slots) are exact.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -24,24 +29,54 @@
 
 namespace cfd {
 
+namespace {
+
+// Small open-addressing set of diagonal offsets (at most kDiaMax members).
+struct OffsetSet {
+  static constexpr int kSlots = 128;
+  int64_t key[kSlots];
+  bool used[kSlots] = {};
+  int count = 0;
+  // false when a new offset would exceed kDiaMax
+  bool insert(int64_t o) {
+    uint64_t h = (uint64_t)o * 0x9E3779B97F4A7C15ull;
+    int i = (int)(h >> 57);
+    while (used[i]) {
+      if (key[i] == o) return true;
+      i = (i + 1) & (kSlots - 1);
+    }
+    if (count == kDiaMax) return false;
+    used[i] = true;
+    key[i] = o;
+    ++count;
+    return true;
+  }
+};
+
+// The butterfly of a row group: partial l after the steps tpr/2, ..., 1 is
+// s_l + s_{l^o} at each step; lane 0's value is returned.
+double butterfly(std::vector<double> s) {
+  for (int o = (int)s.size() / 2; o > 0; o >>= 1)
+    for (int l = 0; l < o; ++l) s[l] = s[l] + s[l + o];
+  return s[0];
+}
+
+}  // namespace
+
 bool encode_diagonal(const HostCsr& h, int tpr, HostDiagonal& D) {
   D = HostDiagonal{};
   const int64_t n = h.nrows;
-  if (n <= 0 || h.ncols != n || tpr != 1 || n >= INT32_MAX || h.nnz() == 0) return false;
-  int cnt = 0;
-  int64_t off[kDiaMax];
-  for (int64_t r = 0; r < n; ++r) {
-    for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k) {
-      const int64_t o = (int64_t)h.ci[k] - r;
-      int q = 0;
-      while (q < cnt && off[q] != o) ++q;
-      if (q == cnt) {
-        if (cnt == kDiaMax) return false;
-        off[cnt++] = o;
-      }
-    }
-  }
+  if (n <= 0 || h.ncols != n || tpr < 1 || tpr > kDiaMaxTpr || n >= INT32_MAX || h.nnz() == 0) return false;
+  OffsetSet set;
+  for (int64_t r = 0; r < n; ++r)
+    for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k)
+      if (!set.insert((int64_t)h.ci[k] - r)) return false;
+  const int cnt = set.count;
   if ((double)cnt * (double)n > kDiaMaxFill * (double)h.nnz()) return false;
+  int64_t off[kDiaMax];
+  int c = 0;
+  for (int i = 0; i < OffsetSet::kSlots; ++i)
+    if (set.used[i]) off[c++] = set.key[i];
   std::sort(off, off + cnt);
   D.n = cnt;
   for (int q = 0; q < cnt; ++q) {
@@ -49,37 +84,62 @@ bool encode_diagonal(const HostCsr& h, int tpr, HostDiagonal& D) {
     if (off[q] == 0) D.main = q;
   }
   D.ld = (n + 31) / 32 * 32;
+  D.tpr = tpr;
+  if (tpr > 1) {
+    D.mask.assign((size_t)D.ld, 0u);
+    for (int64_t r = 0; r < n; ++r) {
+      int q = 0;
+      for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k) {
+        const int64_t o = (int64_t)h.ci[k] - r;
+        while (D.off[q] != o) ++q;  // columns ascend, so do the offsets
+        D.mask[r] |= 1u << q;
+      }
+    }
+  }
   return true;
 }
 
 bool check_diagonal(const HostCsr& h, const HostDiagonal& D, const double* x, std::string* why) {
   const int64_t n = h.nrows;
+  const int t = D.tpr;
   std::vector<double> val((size_t)D.n * D.ld, 0.0);
-  for (int64_t r = 0; r < n; ++r) {
-    for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k) {
-      const int64_t o = (int64_t)h.ci[k] - r;
-      int q = 0;
-      while (q < D.n && D.off[q] != o) ++q;
-      if (q == D.n) {
-        if (why) *why = "entry (" + std::to_string(r) + ", " + std::to_string(h.ci[k]) + ") on no stored diagonal";
-        return false;
-      }
-      val[(size_t)q * D.ld + r] = h.v[k];
-    }
-  }
   for (int q = 1; q < D.n; ++q)
     if (D.off[q] <= D.off[q - 1]) {
       if (why) *why = "diagonal offsets not ascending";
       return false;
     }
   for (int64_t r = 0; r < n; ++r) {
-    double ycsr = 0.0, ydia = 0.0;
-    for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k) ycsr = std::fma(h.v[k], x[h.ci[k]], ycsr);
+    for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k) {
+      const int64_t o = (int64_t)h.ci[k] - r;
+      int q = 0;
+      while (q < D.n && D.off[q] != o) ++q;
+      if (q == D.n || (t > 1 && !((D.mask[r] >> q) & 1u))) {
+        if (why) *why = "entry (" + std::to_string(r) + ", " + std::to_string(h.ci[k]) + ") on no stored diagonal";
+        return false;
+      }
+      val[(size_t)q * D.ld + r] = h.v[k];
+    }
+  }
+  for (int64_t r = 0; r < n; ++r) {
+    // the CSR pipelines: thread l of the row group adds positions l, l + t, ...
+    std::vector<double> sc(t, 0.0), sd(t, 0.0);
+    for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k) {
+      const int l = (int)((k - h.rp[r]) % t);
+      sc[l] = std::fma(h.v[k], x[h.ci[k]], sc[l]);
+    }
+    // the diagonal kernels: every diagonal in order, stored entries counted
+    int pos = 0;
     for (int q = 0; q < D.n; ++q) {
       const int64_t j = r + D.off[q];
       const double xv = (j >= 0 && j < n) ? x[j] : 0.0;
-      ydia = std::fma(val[(size_t)q * D.ld + r], xv, ydia);
+      if (t == 1) {
+        sd[0] = std::fma(val[(size_t)q * D.ld + r], xv, sd[0]);
+      } else if ((D.mask[r] >> q) & 1u) {
+        sd[pos % t] = std::fma(val[(size_t)q * D.ld + r], xv, sd[pos % t]);
+        ++pos;
+      }
     }
+    const double ycsr = butterfly(sc), ydia = butterfly(sd);
     if (std::memcmp(&ycsr, &ydia, sizeof(double)) != 0) {
       if (why) *why = "row " + std::to_string(r) + " differs from the CSR row sum";
       return false;

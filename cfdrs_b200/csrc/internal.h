@@ -103,8 +103,10 @@ constexpr int kRecordCap = ((2 * (kRowsPerBlock + 1) + 15) & ~15) + kNnzCap + 2 
 constexpr int kVecGrid = 148 * 8;
 // Device-side scratch for two-stage reductions (per-CTA partials, up to 4 values).
 constexpr int kMaxRed = 4;
-// Diagonals of the diagonal SpMV layout at most (DevMat::dia).
-constexpr int kDiaMax = 8;
+// Diagonals of the diagonal SpMV layout at most (DevMat::dia), and the
+// largest threads-per-row whose summation order its kernels reproduce.
+constexpr int kDiaMax = 32;
+constexpr int kDiaMaxTpr = 4;
 // Device ordinals covered by the per-device launch-attribute caches.
 constexpr int kLaunchCacheDevices = 64;
 
@@ -181,13 +183,15 @@ struct DevMat {
   mutable bool sl_stale = true;
   // Diagonal layout (HostDiagonal): values stored diagonal-major, ndia arrays
   // of dia_ld entries (0 where a row has no entry on that diagonal), refilled
-  // from v64 / v32 before the first diagonal SpMV after the values changed.
+  // from v64 / v32 before the first diagonal SpMV after the values changed;
+  // for tpr > 1 the per-row presence bits of the diagonals (dia_mask).
   bool dia = false;
   int dia_n = 0, dia_main = -1;
   int dia_off[kDiaMax] = {};
   int64_t dia_ld = 0;
   double* dia64 = nullptr;
   float* dia32 = nullptr;
+  uint32_t* dia_mask = nullptr;
   mutable bool dia_stale = true;
 };
 
@@ -209,20 +213,24 @@ struct HostSliced {
 bool encode_sliced(const HostCsr& h, int tpr, uint64_t base_mult, HostSliced& S);
 bool check_sliced(const HostCsr& h, uint64_t base_mult, const HostSliced& S, std::string* why);
 
-// Diagonal layout (diagonal.cpp, k_spmv_dia): a square matrix with one thread
-// per row whose entries lie on at most kDiaMax diagonals (column - row), stored
-// as kDiaMax or fewer dense diagonals with at most kDiaMaxFill x nnz slots.
-constexpr double kDiaMaxFill = 1.10;
+// Diagonal layout (diagonal.cpp, k_spmv_dia, k_spmv_dia_gen): a square matrix
+// with at most kDiaMaxTpr threads per row whose entries lie on at most kDiaMax
+// diagonals (column - row), stored as dense diagonals with at most
+// kDiaMaxFill x nnz slots.
+constexpr double kDiaMaxFill = 1.30;
 struct HostDiagonal {
   int n = 0;          // diagonals, offsets ascending
   int main = -1;      // index of offset 0, -1 when the main diagonal is empty
   int off[kDiaMax] = {};
   int64_t ld = 0;     // entries per stored diagonal (rows rounded up to 32)
+  int tpr = 1;
+  std::vector<uint32_t> mask;  // tpr > 1: bit d of row r set when (r, r + off[d]) is stored
 };
 bool encode_diagonal(const HostCsr& h, int tpr, HostDiagonal& D);
 // Evaluates y = A x through the diagonal layout in the device kernel's order
-// and compares it bit for bit with the CSR row sums (sequential, in stored
-// order, each product added by a fused multiply-add).
+// and compares it bit for bit with the CSR row sums in the order of the other
+// pipelines for that threads-per-row (each thread of a row group sums every
+// tpr-th stored entry with fused multiply-adds, then the butterfly).
 bool check_diagonal(const HostCsr& h, const HostDiagonal& D, const double* x, std::string* why);
 
 // SpMV pipeline that an SpMV of precision p ([0] FP32, [1] FP64) runs: the

@@ -922,11 +922,13 @@ static __global__ void __launch_bounds__(kThreads) k_sl_gather(int64_t slots, co
 //  - interior span, x not 16-byte aligned: V rows kThreads apart per thread,
 //    loads at immediate offsets from one base pointer per diagonal.
 //  - boundary span: the same mapping with every load predicated.
-// ND > 0 fixes the diagonal count at compile time (the 5- and 7-point
-// stencils); ND = 0 takes any count up to kDiaMax.
+// k_spmv_dia takes the 5- and 7-point stencils (ND diagonals fixed at compile
+// time, one thread per row in the other pipelines); k_spmv_dia_gen any count
+// up to kDiaMax and row groups of TPR <= kDiaMaxTpr threads.
 template <typename VT>
 struct DiaView {
-  const VT* __restrict__ val;  // n diagonals of ld entries
+  const VT* __restrict__ val;      // n diagonals of ld entries
+  const uint32_t* __restrict__ mask;  // TPR > 1: per-row presence bits of the diagonals
   int64_t ld;
   int nrows, n, main, xvec;  // xvec: x is 16-byte aligned
   int off[kDiaMax];
@@ -954,11 +956,8 @@ struct DiaVec<double> {
   }
 };
 
-// x operand of the diagonal pipeline. DiaXPlain reads a stored x.
-// DiaXSmooth0 is the first damped-Jacobi sweep from zero, x_j = w b_j / a_jj,
-// formed where it is read (the V-cycle's pre-smoothing fused into its residual
-// r = b - A x): the same expression as k_smooth0, so the same bits; the
-// kernel also stores x of the span's own rows for the rest of the cycle.
+// x operand of the diagonal kernels (a stored vector; the kernels take it as
+// a source object so a fused producer of x can take its place).
 template <typename VT>
 struct DiaXPlain {
   using Vec = DiaVec<VT>;
@@ -970,28 +969,6 @@ struct DiaXPlain {
   }
   __device__ void store(int, const VT (&)[Vec::V]) const {}
   __device__ void store1(int, VT) const {}
-};
-template <typename VT>
-struct DiaXSmooth0 {
-  using Vec = DiaVec<VT>;
-  static constexpr bool kStore = true;
-  const VT* __restrict__ b;
-  const VT* __restrict__ d;
-  VT omega;
-  VT* __restrict__ xout;
-  __device__ VT one(int j) const { return smooth0_value<VT>(__ldg(b + j), __ldg(d + j), omega); }
-  __device__ void vec(int j, VT (&o)[Vec::V]) const {
-    VT bv[Vec::V], dv[Vec::V];
-    Vec::unpack(__ldg(reinterpret_cast<const typename Vec::type*>(b + j)), bv);
-    Vec::unpack(__ldg(reinterpret_cast<const typename Vec::type*>(d + j)), dv);
-#pragma unroll
-    for (int q = 0; q < Vec::V; ++q) o[q] = smooth0_value<VT>(bv[q], dv[q], omega);
-  }
-  __device__ void store(int r0, const VT (&v)[Vec::V]) const {
-#pragma unroll
-    for (int q = 0; q < Vec::V; ++q) xout[r0 + q] = v[q];
-  }
-  __device__ void store1(int r, VT v) const { xout[r] = v; }
 };
 
 template <typename VT, bool OFFDIAG, int NS>
@@ -1011,10 +988,11 @@ __device__ __forceinline__ void dia_sum(const VT (&v)[NS], const VT (&xv)[NS], i
 
 template <typename VT, bool OFFDIAG, class Epi, int ND, class XS>
 __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, XS xs, Epi epi) {
+  static_assert(ND > 0 && ND <= 8, "k_spmv_dia holds every diagonal of a row in registers");
   if (epi.skip()) return;
   using Vec = DiaVec<VT>;
   constexpr int V = Vec::V;
-  constexpr int NS = ND > 0 ? ND : kDiaMax;  // slots per row in registers
+  constexpr int NS = ND;  // slots per row in registers
   double red[Epi::NRED > 0 ? Epi::NRED : 1];
 #pragma unroll
   for (int q = 0; q < (Epi::NRED > 0 ? Epi::NRED : 1); ++q) red[q] = 0.0;
@@ -1137,6 +1115,154 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, XS xs, Epi
         dia_sum<VT, OFFDIAG, NS>(v[q], xv[q], nd, D.main, sum, diag);
         if (live[q]) epi.row(r0 + q * kThreads, sum, diag, pre[q], red);
       }
+    }
+  }
+  if constexpr (Epi::NRED > 0) {
+    double tot[Epi::NRED];
+    if (grid_reduce<Epi::NRED>(red, epi.red, tot) && threadIdx.x == 0) epi.finish(tot);
+  }
+}
+
+// Sum of a row group's partial sums in the order of its butterfly
+// (rows_from_stage): steps TPR/2, ..., 1, lane 0 adding its partner's.
+template <typename VT, int TPR>
+__device__ __forceinline__ VT dia_butterfly(VT (&s)[TPR]) {
+#pragma unroll
+  for (int o = TPR / 2; o > 0; o >>= 1) {
+#pragma unroll
+    for (int l = 0; l < o; ++l) s[l] = s[l] + s[l + o];
+  }
+  return s[0];
+}
+
+// Adds one stored slot to the partial sums of its row: with TPR = 1 every
+// slot (an empty one adds +-0), with TPR > 1 only present slots, each to the
+// partial its position among the row's stored entries selects.
+template <typename VT, bool OFFDIAG, int TPR>
+__device__ __forceinline__ void dia_add(VT v, VT xv, int d, int main, uint32_t mk, int& pos, VT (&s)[TPR],
+                                        VT& diag) {
+  if (TPR == 1) {
+    if (OFFDIAG && d == main)
+      diag = v;
+    else
+      s[0] += v * xv;
+  } else if ((mk >> d) & 1u) {
+    const int l = pos & (TPR - 1);
+    ++pos;
+    if (OFFDIAG && d == main) {
+      diag = v;
+    } else {
+#pragma unroll
+      for (int k = 0; k < TPR; ++k)
+        if (k == l) s[k] += v * xv;
+    }
+  }
+}
+
+// Any number of diagonals up to kDiaMax: the diagonals are streamed in order,
+// each adding into the rows' partial sums (loop unrolled by four so the loads
+// of several diagonals are in flight). Interior spans with aligned x: V
+// consecutive rows per thread, one 16-byte value load per diagonal and x from
+// the one or two aligned 16-byte vectors that cover the window
+// [r0 + o, r0 + o + V). Other spans: V rows kThreads apart, predicated loads.
+template <typename VT, bool OFFDIAG, class Epi, int TPR, class XS>
+__global__ void __launch_bounds__(kThreads) k_spmv_dia_gen(DiaView<VT> D, XS xs, Epi epi) {
+  if (epi.skip()) return;
+  using Vec = DiaVec<VT>;
+  constexpr int V = Vec::V;
+  double red[Epi::NRED > 0 ? Epi::NRED : 1];
+#pragma unroll
+  for (int q = 0; q < (Epi::NRED > 0 ? Epi::NRED : 1); ++q) red[q] = 0.0;
+  const int nd = D.n;
+  const int64_t span = (int64_t)kThreads * V;
+  const int omin = D.off[0], omax = D.off[nd - 1];
+  for (int64_t s0 = (int64_t)blockIdx.x * span; s0 < D.nrows; s0 += (int64_t)gridDim.x * span) {
+    // interior: the aligned x vectors of every window (up to V - 1 entries
+    // either side of the rows' own range shifted by the offset) lie inside x
+    const bool interior =
+        s0 + omin - V >= 0 && s0 + span + omax + V <= D.nrows && s0 + span <= D.nrows;
+    typename Epi::Pre pre[V];
+    VT s[V][TPR], diag[V];
+    uint32_t mk[V];
+    int pos[V];
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      diag[q] = VT(0);
+      pos[q] = 0;
+      mk[q] = 0u;
+#pragma unroll
+      for (int k = 0; k < TPR; ++k) s[q][k] = VT(0);
+    }
+    if (interior && D.xvec) {
+      const int r0 = (int)s0 + threadIdx.x * V;  // V consecutive rows
+#pragma unroll
+      for (int q = 0; q < V; ++q) {
+        pre[q] = epi.load(r0 + q);
+        if (TPR > 1) mk[q] = D.mask[r0 + q];
+      }
+      if constexpr (XS::kStore) {
+        VT own[V];
+        xs.vec(r0, own);
+        xs.store(r0, own);
+      }
+#pragma unroll 4
+      for (int d = 0; d < nd; ++d) {
+        const int o = D.off[d];
+        VT vd[V], xa[V], xd[V];
+        Vec::unpack(__ldcs(reinterpret_cast<const typename Vec::type*>(D.val + (int64_t)d * D.ld + r0)), vd);
+        const int k = o & (V - 1);  // x window [r0 + o, r0 + o + V) from the aligned vectors at base, base + V
+        const int base = r0 + o - k;
+        xs.vec(base, xa);
+        if (k == 0) {
+#pragma unroll
+          for (int q = 0; q < V; ++q) xd[q] = xa[q];
+        } else {
+          VT xb[V];
+          xs.vec(base + V, xb);
+#pragma unroll
+          for (int q = 0; q < V; ++q) {
+            VT w = xa[q];
+#pragma unroll
+            for (int c = 1; c < V; ++c)
+              if (k == c) w = q + c < V ? xa[q + c] : xb[q + c - V];
+            xd[q] = w;
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < V; ++q) dia_add<VT, OFFDIAG, TPR>(vd[q], xd[q], d, D.main, mk[q], pos[q], s[q], diag[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < V; ++q) epi.row(r0 + q, dia_butterfly<VT, TPR>(s[q]), diag[q], pre[q], red);
+    } else {
+      const int r0 = (int)s0 + threadIdx.x;  // V rows kThreads apart
+      bool live[V];
+#pragma unroll
+      for (int q = 0; q < V; ++q) {
+        const int row = r0 + q * kThreads;
+        live[q] = row < D.nrows;
+        pre[q] = typename Epi::Pre{};
+        if (live[q]) {
+          pre[q] = epi.load(row);
+          if (TPR > 1) mk[q] = D.mask[row];
+          if constexpr (XS::kStore) xs.store1(row, xs.one(row));
+        }
+      }
+#pragma unroll 4
+      for (int d = 0; d < nd; ++d) {
+        const int o = D.off[d];
+        const VT* vd = D.val + (int64_t)d * D.ld;
+#pragma unroll
+        for (int q = 0; q < V; ++q) {
+          const int row = r0 + q * kThreads;
+          const int j = row + o;
+          const VT v = live[q] ? __ldcs(vd + row) : VT(0);
+          const VT xv = (live[q] && j >= 0 && j < D.nrows) ? xs.one(j) : VT(0);
+          dia_add<VT, OFFDIAG, TPR>(v, xv, d, D.main, mk[q], pos[q], s[q], diag[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < V; ++q)
+        if (live[q]) epi.row(r0 + q * kThreads, dia_butterfly<VT, TPR>(s[q]), diag[q], pre[q], red);
     }
   }
   if constexpr (Epi::NRED > 0) {

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -598,6 +600,7 @@ struct Launcher {
     else
       D.val = m.dia32;
     D.ld = m.dia_ld;
+    D.mask = m.dia_mask;
     D.nrows = (int)m.nrows;
     D.n = m.dia_n;
     D.main = m.dia_main;
@@ -627,49 +630,37 @@ struct Launcher {
   // xvec: every array the x source reads (and stores) is 16-byte aligned.
   template <typename VT, bool OFF, class Epi, class XS>
   cfd_status dia_launch_xs(const DevMat& m, XS xs, bool xvec, Epi epi) {
-    if (m.dia_n == 7) return dia_launch_n<VT, OFF, Epi, 7, XS>(m, xs, xvec, epi);
-    if (m.dia_n == 5) return dia_launch_n<VT, OFF, Epi, 5, XS>(m, xs, xvec, epi);
-    return dia_launch_n<VT, OFF, Epi, 0, XS>(m, xs, xvec, epi);
+    if (m.tpr == 1 && m.dia_n == 7) return dia_launch_k<VT, Epi>(m, k_spmv_dia<VT, OFF, Epi, 7, XS>, xs, xvec, epi);
+    if (m.tpr == 1 && m.dia_n == 5) return dia_launch_k<VT, Epi>(m, k_spmv_dia<VT, OFF, Epi, 5, XS>, xs, xvec, epi);
+    if (m.tpr == 1) return dia_launch_k<VT, Epi>(m, k_spmv_dia_gen<VT, OFF, Epi, 1, XS>, xs, xvec, epi);
+    if (m.tpr == 2) return dia_launch_k<VT, Epi>(m, k_spmv_dia_gen<VT, OFF, Epi, 2, XS>, xs, xvec, epi);
+    return dia_launch_k<VT, Epi>(m, k_spmv_dia_gen<VT, OFF, Epi, 4, XS>, xs, xvec, epi);
   }
-  // The V-cycle's pre-smoothing from zero fused into its residual on the
-  // diagonal pipeline: x = w D^-1 b (stored) and r = b - A x in one pass.
-  // Returns false (nothing launched) when the operator does not run the
-  // diagonal pipeline in this precision.
-  template <typename XT>
-  cfd_status dia_smooth0_residual(const DevMat& m, const XT* b, const XT* d, XT omega, XT* x, XT* r,
-                                  const int* done, bool* ran) {
-    *ran = false;
-    const int p = sizeof(XT) == 4 ? 0 : 1;
-    if (m.nrows == 0 || !dia_ready<XT>(m)) return CFD_OK;
-    if (m.path[p] == kPathTimed) CFD_TRY(tune<XT>(m));
-    if (spmv_path(m, p) != kPathDiag) return CFD_OK;
-    EpiResidual<XT, 0> epi{r, b, nullptr, done, {}};
-    epi.red = red();
-    const bool xvec = (((uintptr_t)b | (uintptr_t)d | (uintptr_t)x) & 15) == 0;
-    CFD_TRY((dia_launch_xs<XT, false, EpiResidual<XT, 0>>(m, DiaXSmooth0<XT>{b, d, omega, x}, xvec, epi)));
-    *ran = true;
-    return finish_spmv<XT, XT>(m);
-  }
-  // ND: the diagonal count fixed at compile time (0: any count up to kDiaMax).
-  template <typename VT, bool OFF, class Epi, int ND, class XS>
-  cfd_status dia_launch_n(const DevMat& m, XS xs, bool xvec, Epi epi) {
+  // One launch of a diagonal kernel (its occupancy looked up once per device).
+  template <typename VT, class Epi, class XS>
+  cfd_status dia_launch_k(const DevMat& m, void (*kern)(DiaView<VT>, XS, Epi), XS xs, bool xvec, Epi epi) {
     CFD_TRY(dia_refresh(m));
-    auto kern = k_spmv_dia<VT, OFF, Epi, ND, XS>;
-    static int occ[kLaunchCacheDevices] = {};
+    static std::mutex occ_mu;
+    static std::map<const void*, int> occ_by_kernel[kLaunchCacheDevices];
     if (ctx->device >= kLaunchCacheDevices) {
       set_error("device ordinal %d beyond %d", ctx->device, kLaunchCacheDevices);
       return CFD_ERR_CUDA;
     }
-    if (occ[ctx->device] <= 0) {
-      int o = 0;
-      CFD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kThreads, 0));
-      occ[ctx->device] = std::max(1, o);
+    int occ = 0;
+    {
+      std::lock_guard<std::mutex> g(occ_mu);
+      int& o = occ_by_kernel[ctx->device][(const void*)kern];
+      if (o <= 0) {
+        CFD_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, kThreads, 0));
+        o = std::max(1, o);
+      }
+      occ = o;
     }
     const int64_t span = (int64_t)kThreads * DiaVec<VT>::V;
     const int64_t spans = (m.nrows + span - 1) / span;
     // at most one reduction slot per CTA (the context's partials)
     const int grid = (int)std::max<int64_t>(
-        1, std::min<int64_t>({spans, (int64_t)ctx->num_sms * occ[ctx->device], (int64_t)ctx->partial_capacity}));
+        1, std::min<int64_t>({spans, (int64_t)ctx->num_sms * occ, (int64_t)ctx->partial_capacity}));
     DiaView<VT> D = dia_view<VT>(m);
     D.xvec = xvec ? 1 : 0;
     kern<<<grid, kThreads, 0, s>>>(D, xs, epi);
@@ -888,25 +879,20 @@ static cfd_status vcycle(Launcher& lc, cfd_amg* amg, size_t l, const XT* b, XT* 
     }
     return CFD_OK;
   }
-  // 1. pre-smoothing from x = 0 and 2. the residual r = b - A x; with one
-  // sweep on the diagonal pipeline both in one pass
+  // 1. pre-smoothing from x = 0
   XT* x = V.xa;
   XT* y = V.xb;
-  bool fused = false;
-  if (c.pre_smooth == 1)
-    CFD_TRY(lc.dia_smooth0_residual<XT>(L.A, b, diag_of<XT>(L), omega, x, V.r, done, &fused));
-  if (!fused) {
-    if (c.pre_smooth >= 1) {
-      CFD_TRY(lc.vec(n, k_smooth0<XT>, b, diag_of<XT>(L), omega, x, done));
-      for (int s = 1; s < c.pre_smooth; ++s) {
-        CFD_TRY(jacobi_sweep<XT>(lc, L, x, y, b, omega, 0, st, done));
-        std::swap(x, y);
-      }
-    } else {
-      CFD_TRY(lc.vec(n, k_fill<XT>, x, XT(0), done));
+  if (c.pre_smooth >= 1) {
+    CFD_TRY(lc.vec(n, k_smooth0<XT>, b, diag_of<XT>(L), omega, x, done));
+    for (int s = 1; s < c.pre_smooth; ++s) {
+      CFD_TRY(jacobi_sweep<XT>(lc, L, x, y, b, omega, 0, st, done));
+      std::swap(x, y);
     }
-    CFD_TRY(lc.spmv<XT, XT, false>(L.A, x, EpiResidual<XT, 0>{V.r, b, nullptr, done, {}}));
+  } else {
+    CFD_TRY(lc.vec(n, k_fill<XT>, x, XT(0), done));
   }
+  // 2. residual r = b - A x
+  CFD_TRY(lc.spmv<XT, XT, false>(L.A, x, EpiResidual<XT, 0>{V.r, b, nullptr, done, {}}));
   // 3. restriction to the next level's right-hand side
   DevLevel& Lc = amg->dev[l + 1];
   LevelVecs<XT>& Vc = vecs<XT>(Lc);

@@ -77,6 +77,11 @@ def spmv_case(shape):
         S2 = random_csr(rng, 1500, S1.shape[1], rng.integers(0, 40, 1500)).to_scipy()
         from cfdrs_b200.sparse import CsrMatrix
         A = CsrMatrix.from_scipy(sp.vstack([S1, S2]).tocsr())
+    elif shape == "coarse_operator_64":  # the 64^3 first coarse level: 23 diagonals, 2 threads per row
+        import cfdrs_b200 as cf
+        from cfdrs_b200.multigrid import HostHierarchy
+        B = P.poisson_3d_variable(64, 8.0, 1.0, seed=0)[0]
+        A, staged = HostHierarchy(B, cf.AMGConfig.pressure_poisson()).level(1, 0), False
     else:  # AMG operators of the 3-D solve: interpolation, restriction, coarse A (2 threads per row)
         import cfdrs_b200 as cf
         B = P.poisson_3d_variable(16, 4.0, 1.0, seed=2)[0]
@@ -90,7 +95,7 @@ def spmv_case(shape):
 
 @pytest.mark.parametrize("shape", ["stencil", "stencil_tail", "stencil_2d", "empty_blocks", "narrow", "ragged",
                                    "long_rows", "rectangular", "mixed", "prolongation", "restriction",
-                                   "coarse_operator"])
+                                   "coarse_operator", "coarse_operator_64"])
 def test_spmv_vs_oracle(cuda, oracle, shape):
     from cfdrs_b200.device import DeviceCsr
     A, staged = spmv_case(shape)
@@ -111,7 +116,7 @@ def test_spmv_vs_oracle(cuda, oracle, shape):
 
 
 @pytest.mark.parametrize("shape", ["stencil", "stencil_tail", "stencil_2d", "empty_blocks", "narrow",
-                                   "prolongation", "restriction", "coarse_operator", "mixed"])
+                                   "prolongation", "restriction", "coarse_operator", "coarse_operator_64", "mixed"])
 def test_spmv_pipelines_bit_identical(cuda, shape):
     """Every SpMV pipeline a matrix is eligible for (split, record, x-staged,
     diagonal, and for FP32 the sliced one) sums each row in the same order: FP64 and FP32
@@ -127,6 +132,8 @@ def test_spmv_pipelines_bit_identical(cuda, shape):
         (["diagonal"] if lay["diagonals"] else [])
     if shape in ("stencil", "stencil_tail", "stencil_2d"):
         assert lay["diagonals"] in (5, 7)
+    if shape == "coarse_operator_64":
+        assert lay["diagonals"] == 23 and lay["threads_per_row"] == 2
     x = np.random.default_rng(5).uniform(-1, 1, A.ncols)
     for dt in (cuda.float64, cuda.float32):
         fp32 = dt == cuda.float32
@@ -207,9 +214,8 @@ def test_vcycle_matches_oracle(cuda, oracle, coarse):
 
 def test_vcycle_bits_do_not_depend_on_the_pipeline(cuda):
     """One V-cycle (FP64, no dot products) gives the same bits whichever
-    pipeline the operators run: on the diagonal pipeline the pre-smoothing
-    sweep is fused into the fine residual (x = w D^-1 b formed where it is
-    read), which must equal the separate sweep and residual of the others."""
+    pipeline the operators run (the fine operator on the diagonal, record and
+    split pipelines; every row sums in the same order on each)."""
     import cfdrs_b200 as cf
     from cfdrs_b200 import problems as P
     A = P.poisson_3d_variable(24, 4.0, 1.0, seed=6)[0]

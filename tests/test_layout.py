@@ -152,13 +152,13 @@ def test_sliced_layout_refused_where_it_does_not_pay():
 
 def test_diagonal_layout_on_stencils():
     """Stencil operators get the diagonal layout (every entry on one of at most
-    8 diagonals, at most 10 % empty slots); cfd_layout_check evaluates y = A x
+    32 diagonals, at most 30 % empty slots); cfd_layout_check evaluates y = A x
     through it in the kernel's order and compares each row bit for bit with
-    the sequential CSR row sum (check_diagonal), boundary rows with missing
-    diagonals included."""
-    # 5^3: 21 % of the slots would be empty (boundary rows), above the 10 % limit
+    the CSR row sum of the other pipelines (check_diagonal), boundary rows with
+    missing diagonals included."""
+    # 5^3: the boundary rows leave 21 % of the slots empty, 3^3: 40 %
     cases = [(P.poisson_3d_variable(33, 4.0, 1.0, seed=2)[0], 7), (P.poisson_3d_variable(16, 4.0, 1.0, seed=3)[0], 7),
-             (P.poisson_3d_variable(5, 4.0, 1.0, seed=3)[0], 0),
+             (P.poisson_3d_variable(5, 4.0, 1.0, seed=3)[0], 7), (P.poisson_3d_variable(3, 4.0, 1.0, seed=3)[0], 0),
              (P.poisson_2d_dirichlet(70, seed=0)[0], 5), (grid_laplacian(41), 5),
              (csr_from_lists([0, 1], [0], [2.0], 1), 1)]
     for A, nd in cases:
@@ -172,8 +172,8 @@ def test_diagonal_layout_on_stencils():
 def test_diagonal_layout_refused():
     rng = np.random.default_rng(4)
     n = 400
-    # nine distinct diagonals
-    offs = [-40, -20, -3, -1, 0, 1, 3, 20, 40]
+    # thirty-three distinct diagonals
+    offs = list(range(-16, 17))
     rows = [[j for j in (i + o for o in offs) if 0 <= j < n] for i in range(n)]
     rp = np.concatenate([[0], np.cumsum([len(r) for r in rows])])
     A = csr_from_lists(rp.tolist(), sum(rows, []), rng.uniform(-1, 1, int(rp[-1])).tolist(), n)
@@ -190,3 +190,19 @@ def test_diagonal_layout_refused():
     assert check(random_csr(rng, 300, 300, np.full(300, 30)))["diagonals"] == 0
     # an AMG Galerkin operator (irregular columns)
     assert check(P.network_batch(1, seed=5, n_min=200, n_max=300)[0][0])["diagonals"] == 0
+
+
+def test_diagonal_layout_on_a_coarse_level():
+    """The first coarse operator of the 64^3 Ruge-Stueben hierarchy (ascending
+    coarse numbering) has 23 diagonals and two threads per row: the layout
+    keeps per-row presence bits so its kernel adds every stored entry to the
+    partial sum of its position, and check_diagonal compares that order with
+    the CSR pipelines' bit for bit."""
+    import cfdrs_b200 as cf
+    from cfdrs_b200.multigrid import HostHierarchy
+    A = P.poisson_3d_variable(64, 8.0, 1.0, seed=0)[0]
+    H = HostHierarchy(A, cf.AMGConfig.pressure_poisson())
+    info = check(H.level(1, 0))
+    assert info["diagonals"] == 23 and info["threads_per_row"] == 2
+    # the level below: hundreds of distinct offsets
+    assert check(H.level(2, 0))["diagonals"] == 0
