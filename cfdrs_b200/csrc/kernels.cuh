@@ -980,7 +980,7 @@ __device__ __forceinline__ void dia_sum(const VT (&v)[NS], const VT (&xv)[NS], i
       if (OFFDIAG && d == main) {
         diag = v[d];
       } else {
-        sum += v[d] * xv[d];
+        sum = fma(v[d], xv[d], sum);
       }
     }
   }
@@ -1141,11 +1141,13 @@ __device__ __forceinline__ VT dia_butterfly(VT (&s)[TPR]) {
 template <typename VT, bool OFFDIAG, int TPR>
 __device__ __forceinline__ void dia_add(VT v, VT xv, int d, int main, uint32_t mk, int& pos, VT (&s)[TPR],
                                         VT& diag) {
+  // explicit fused multiply-adds: the CSR pipelines' sum += v * x contracts to
+  // one, and a product shared by the selected partials must not be split off
   if (TPR == 1) {
     if (OFFDIAG && d == main)
       diag = v;
     else
-      s[0] += v * xv;
+      s[0] = fma(v, xv, s[0]);
   } else if ((mk >> d) & 1u) {
     const int l = pos & (TPR - 1);
     ++pos;
@@ -1154,7 +1156,7 @@ __device__ __forceinline__ void dia_add(VT v, VT xv, int d, int main, uint32_t m
     } else {
 #pragma unroll
       for (int k = 0; k < TPR; ++k)
-        if (k == l) s[k] += v * xv;
+        if (k == l) s[k] = fma(v, xv, s[k]);
     }
   }
 }
