@@ -13,12 +13,11 @@
 // Summation order. Every pipeline sums a row in the order of its row group of
 // tpr threads: thread l adds the stored entries at positions l, l + tpr, ...
 // (in column order) one product at a time, then the group combines its partial
-// sums by a butterfly. The diagonal kernels keep tpr partial sums per row and
-// assign each stored entry to the partial its position selects, so their row
-// sums are those of the other pipelines bit for bit. For tpr = 1 an empty slot
-// adds 0 * x = +-0, which leaves a partial sum that starts at +0 unchanged for
-// finite x; for tpr > 1 a per-row presence mask marks the stored entries, so
-// the positions (and the skipped slots) are exact.
+// sums by a butterfly. The diagonal kernels keep tpr partial sums per row
+// (tpr <= 2) and add each slot to the partial a per-row lane mask names (the
+// parity of the stored entry's position), so their row sums are those of the
+// other pipelines bit for bit: an empty slot holds 0 and adds 0 * x = +-0,
+// which leaves a partial sum that started at +0 unchanged for finite x.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -85,14 +84,14 @@ bool encode_diagonal(const HostCsr& h, int tpr, HostDiagonal& D) {
   }
   D.ld = (n + 31) / 32 * 32;
   D.tpr = tpr;
-  if (tpr > 1) {
+  if (tpr == 2) {
     D.mask.assign((size_t)D.ld, 0u);
     for (int64_t r = 0; r < n; ++r) {
       int q = 0;
       for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k) {
         const int64_t o = (int64_t)h.ci[k] - r;
         while (D.off[q] != o) ++q;  // columns ascend, so do the offsets
-        D.mask[r] |= 1u << q;
+        if ((k - h.rp[r]) & 1) D.mask[r] |= 1u << q;
       }
     }
   }
@@ -113,7 +112,7 @@ bool check_diagonal(const HostCsr& h, const HostDiagonal& D, const double* x, st
       const int64_t o = (int64_t)h.ci[k] - r;
       int q = 0;
       while (q < D.n && D.off[q] != o) ++q;
-      if (q == D.n || (t > 1 && !((D.mask[r] >> q) & 1u))) {
+      if (q == D.n) {
         if (why) *why = "entry (" + std::to_string(r) + ", " + std::to_string(h.ci[k]) + ") on no stored diagonal";
         return false;
       }
@@ -127,17 +126,13 @@ bool check_diagonal(const HostCsr& h, const HostDiagonal& D, const double* x, st
       const int l = (int)((k - h.rp[r]) % t);
       sc[l] = std::fma(h.v[k], x[h.ci[k]], sc[l]);
     }
-    // the diagonal kernels: every diagonal in order, stored entries counted
-    int pos = 0;
+    // the diagonal kernels: every slot in diagonal order, to the partial its
+    // lane bit names (empty slots hold 0 and go to partial 0)
     for (int q = 0; q < D.n; ++q) {
       const int64_t j = r + D.off[q];
       const double xv = (j >= 0 && j < n) ? x[j] : 0.0;
-      if (t == 1) {
-        sd[0] = std::fma(val[(size_t)q * D.ld + r], xv, sd[0]);
-      } else if ((D.mask[r] >> q) & 1u) {
-        sd[pos % t] = std::fma(val[(size_t)q * D.ld + r], xv, sd[pos % t]);
-        ++pos;
-      }
+      const int l = t == 2 ? (int)((D.mask[r] >> q) & 1u) : 0;
+      sd[l] = std::fma(val[(size_t)q * D.ld + r], xv, sd[l]);
     }
     const double ycsr = butterfly(sc), ydia = butterfly(sd);
     if (std::memcmp(&ycsr, &ydia, sizeof(double)) != 0) {

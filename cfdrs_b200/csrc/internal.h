@@ -106,7 +106,7 @@ constexpr int kMaxRed = 4;
 // Diagonals of the diagonal SpMV layout at most (DevMat::dia), and the
 // largest threads-per-row whose summation order its kernels reproduce.
 constexpr int kDiaMax = 32;
-constexpr int kDiaMaxTpr = 4;
+constexpr int kDiaMaxTpr = 2;
 // Device ordinals covered by the per-device launch-attribute caches.
 constexpr int kLaunchCacheDevices = 64;
 
@@ -184,7 +184,7 @@ struct DevMat {
   // Diagonal layout (HostDiagonal): values stored diagonal-major, ndia arrays
   // of dia_ld entries (0 where a row has no entry on that diagonal), refilled
   // from v64 / v32 before the first diagonal SpMV after the values changed;
-  // for tpr > 1 the per-row presence bits of the diagonals (dia_mask).
+  // for tpr = 2 the per-row lane bits of the diagonals (dia_mask).
   bool dia = false;
   int dia_n = 0, dia_main = -1;
   int dia_off[kDiaMax] = {};
@@ -224,7 +224,9 @@ struct HostDiagonal {
   int off[kDiaMax] = {};
   int64_t ld = 0;     // entries per stored diagonal (rows rounded up to 32)
   int tpr = 1;
-  std::vector<uint32_t> mask;  // tpr > 1: bit d of row r set when (r, r + off[d]) is stored
+  // tpr = 2: bit d of row r set when (r, r + off[d]) is stored at an odd
+  // position among the row's stored entries (the row group's second thread adds it)
+  std::vector<uint32_t> mask;
 };
 bool encode_diagonal(const HostCsr& h, int tpr, HostDiagonal& D);
 // Evaluates y = A x through the diagonal layout in the device kernel's order

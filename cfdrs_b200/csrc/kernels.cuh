@@ -924,11 +924,11 @@ static __global__ void __launch_bounds__(kThreads) k_sl_gather(int64_t slots, co
 //  - boundary span: the same mapping with every load predicated.
 // k_spmv_dia takes the 5- and 7-point stencils (ND diagonals fixed at compile
 // time, one thread per row in the other pipelines); k_spmv_dia_gen any count
-// up to kDiaMax and row groups of TPR <= kDiaMaxTpr threads.
+// up to kDiaMax and row groups of TPR <= kDiaMaxTpr = 2 threads.
 template <typename VT>
 struct DiaView {
   const VT* __restrict__ val;      // n diagonals of ld entries
-  const uint32_t* __restrict__ mask;  // TPR > 1: per-row presence bits of the diagonals
+  const uint32_t* __restrict__ mask;  // TPR = 2: per-row lane bits of the diagonals
   int64_t ld;
   int nrows, n, main, xvec;  // xvec: x is 16-byte aligned
   int off[kDiaMax];
@@ -1135,40 +1135,38 @@ __device__ __forceinline__ VT dia_butterfly(VT (&s)[TPR]) {
   return s[0];
 }
 
-// Adds one stored slot to the partial sums of its row: with TPR = 1 every
-// slot (an empty one adds +-0), with TPR > 1 only present slots, each to the
-// partial its position among the row's stored entries selects.
+// Adds one slot to the partial sums of its row. TPR = 1: every slot (an
+// empty one holds 0 and adds +-0, which leaves a partial that started at +0
+// unchanged for finite x). TPR = 2: bit d of the row's lane mask names the
+// partial of the row group's thread that adds this entry in the CSR pipelines
+// (its position among the row's stored entries, mod 2); an empty slot goes to
+// partial 0 and adds +-0. Explicit fused multiply-adds: the CSR pipelines'
+// sum += v * x contracts to one, and a product shared by the two predicated
+// partials must not be split off.
 template <typename VT, bool OFFDIAG, int TPR>
-__device__ __forceinline__ void dia_add(VT v, VT xv, int d, int main, uint32_t mk, int& pos, VT (&s)[TPR],
-                                        VT& diag) {
-  // explicit fused multiply-adds: the CSR pipelines' sum += v * x contracts to
-  // one, and a product shared by the selected partials must not be split off
-  if (TPR == 1) {
-    if (OFFDIAG && d == main)
-      diag = v;
+__device__ __forceinline__ void dia_add(VT v, VT xv, int d, int main, uint32_t lm, VT (&s)[TPR], VT& diag) {
+  if (OFFDIAG && d == main) {
+    diag = v;
+  } else if (TPR == 1) {
+    s[0] = fma(v, xv, s[0]);
+  } else {
+    if ((lm >> d) & 1u)
+      s[TPR - 1] = fma(v, xv, s[TPR - 1]);
     else
       s[0] = fma(v, xv, s[0]);
-  } else if ((mk >> d) & 1u) {
-    const int l = pos & (TPR - 1);
-    ++pos;
-    if (OFFDIAG && d == main) {
-      diag = v;
-    } else {
-#pragma unroll
-      for (int k = 0; k < TPR; ++k)
-        if (k == l) s[k] = fma(v, xv, s[k]);
-    }
   }
 }
 
 // Any number of diagonals up to kDiaMax: the diagonals are streamed in order,
-// each adding into the rows' partial sums (loop unrolled by four so the loads
-// of several diagonals are in flight). Interior spans with aligned x: V
-// consecutive rows per thread, one 16-byte value load per diagonal and x from
-// the one or two aligned 16-byte vectors that cover the window
-// [r0 + o, r0 + o + V). Other spans: V rows kThreads apart, predicated loads.
+// each adding into the rows' partial sums (unrolled by eight so the loads of
+// several diagonals are in flight). Interior spans with aligned x: V
+// consecutive rows per thread, one 16-byte value load per diagonal, x by one
+// 16-byte load where the offset is a multiple of V and entry by entry
+// otherwise (lanes 16 bytes apart: the entries of four loads share their
+// cache lines). Other spans: V rows kThreads apart, predicated loads.
 template <typename VT, bool OFFDIAG, class Epi, int TPR, class XS>
 __global__ void __launch_bounds__(kThreads) k_spmv_dia_gen(DiaView<VT> D, XS xs, Epi epi) {
+  static_assert(TPR == 1 || TPR == 2, "row groups of one or two threads");
   if (epi.skip()) return;
   using Vec = DiaVec<VT>;
   constexpr int V = Vec::V;
@@ -1179,19 +1177,14 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia_gen(DiaView<VT> D, XS xs,
   const int64_t span = (int64_t)kThreads * V;
   const int omin = D.off[0], omax = D.off[nd - 1];
   for (int64_t s0 = (int64_t)blockIdx.x * span; s0 < D.nrows; s0 += (int64_t)gridDim.x * span) {
-    // interior: the aligned x vectors of every window (up to V - 1 entries
-    // either side of the rows' own range shifted by the offset) lie inside x
-    const bool interior =
-        s0 + omin - V >= 0 && s0 + span + omax + V <= D.nrows && s0 + span <= D.nrows;
+    const bool interior = s0 + omin >= 0 && s0 + span + omax <= D.nrows && s0 + span <= D.nrows;
     typename Epi::Pre pre[V];
     VT s[V][TPR], diag[V];
-    uint32_t mk[V];
-    int pos[V];
+    uint32_t lm[V];
 #pragma unroll
     for (int q = 0; q < V; ++q) {
       diag[q] = VT(0);
-      pos[q] = 0;
-      mk[q] = 0u;
+      lm[q] = 0u;
 #pragma unroll
       for (int k = 0; k < TPR; ++k) s[q][k] = VT(0);
     }
@@ -1200,38 +1193,21 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia_gen(DiaView<VT> D, XS xs,
 #pragma unroll
       for (int q = 0; q < V; ++q) {
         pre[q] = epi.load(r0 + q);
-        if (TPR > 1) mk[q] = D.mask[r0 + q];
+        if (TPR > 1) lm[q] = D.mask[r0 + q];
       }
-      if constexpr (XS::kStore) {
-        VT own[V];
-        xs.vec(r0, own);
-        xs.store(r0, own);
-      }
-#pragma unroll 4
+#pragma unroll 8
       for (int d = 0; d < nd; ++d) {
         const int o = D.off[d];
-        VT vd[V], xa[V], xd[V];
+        VT vd[V], xd[V];
         Vec::unpack(__ldcs(reinterpret_cast<const typename Vec::type*>(D.val + (int64_t)d * D.ld + r0)), vd);
-        const int k = o & (V - 1);  // x window [r0 + o, r0 + o + V) from the aligned vectors at base, base + V
-        const int base = r0 + o - k;
-        xs.vec(base, xa);
-        if (k == 0) {
-#pragma unroll
-          for (int q = 0; q < V; ++q) xd[q] = xa[q];
+        if ((o & (V - 1)) == 0) {
+          xs.vec(r0 + o, xd);
         } else {
-          VT xb[V];
-          xs.vec(base + V, xb);
 #pragma unroll
-          for (int q = 0; q < V; ++q) {
-            VT w = xa[q];
-#pragma unroll
-            for (int c = 1; c < V; ++c)
-              if (k == c) w = q + c < V ? xa[q + c] : xb[q + c - V];
-            xd[q] = w;
-          }
+          for (int q = 0; q < V; ++q) xd[q] = xs.one(r0 + o + q);
         }
 #pragma unroll
-        for (int q = 0; q < V; ++q) dia_add<VT, OFFDIAG, TPR>(vd[q], xd[q], d, D.main, mk[q], pos[q], s[q], diag[q]);
+        for (int q = 0; q < V; ++q) dia_add<VT, OFFDIAG, TPR>(vd[q], xd[q], d, D.main, lm[q], s[q], diag[q]);
       }
 #pragma unroll
       for (int q = 0; q < V; ++q) epi.row(r0 + q, dia_butterfly<VT, TPR>(s[q]), diag[q], pre[q], red);
@@ -1245,8 +1221,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia_gen(DiaView<VT> D, XS xs,
         pre[q] = typename Epi::Pre{};
         if (live[q]) {
           pre[q] = epi.load(row);
-          if (TPR > 1) mk[q] = D.mask[row];
-          if constexpr (XS::kStore) xs.store1(row, xs.one(row));
+          if (TPR > 1) lm[q] = D.mask[row];
         }
       }
 #pragma unroll 4
@@ -1259,7 +1234,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia_gen(DiaView<VT> D, XS xs,
           const int j = row + o;
           const VT v = live[q] ? __ldcs(vd + row) : VT(0);
           const VT xv = (live[q] && j >= 0 && j < D.nrows) ? xs.one(j) : VT(0);
-          dia_add<VT, OFFDIAG, TPR>(v, xv, d, D.main, mk[q], pos[q], s[q], diag[q]);
+          dia_add<VT, OFFDIAG, TPR>(v, xv, d, D.main, lm[q], s[q], diag[q]);
         }
       }
 #pragma unroll

@@ -633,8 +633,7 @@ struct Launcher {
     if (m.tpr == 1 && m.dia_n == 7) return dia_launch_k<VT, Epi>(m, k_spmv_dia<VT, OFF, Epi, 7, XS>, xs, xvec, epi);
     if (m.tpr == 1 && m.dia_n == 5) return dia_launch_k<VT, Epi>(m, k_spmv_dia<VT, OFF, Epi, 5, XS>, xs, xvec, epi);
     if (m.tpr == 1) return dia_launch_k<VT, Epi>(m, k_spmv_dia_gen<VT, OFF, Epi, 1, XS>, xs, xvec, epi);
-    if (m.tpr == 2) return dia_launch_k<VT, Epi>(m, k_spmv_dia_gen<VT, OFF, Epi, 2, XS>, xs, xvec, epi);
-    return dia_launch_k<VT, Epi>(m, k_spmv_dia_gen<VT, OFF, Epi, 4, XS>, xs, xvec, epi);
+    return dia_launch_k<VT, Epi>(m, k_spmv_dia_gen<VT, OFF, Epi, 2, XS>, xs, xvec, epi);
   }
   // One launch of a diagonal kernel (its occupancy looked up once per device).
   template <typename VT, class Epi, class XS>
