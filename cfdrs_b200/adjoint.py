@@ -33,7 +33,8 @@ from .sparse import CsrMatrix
 class SparseSolver:
     """Device solver for a fixed sparsity pattern whose values come from torch.
 
-    ``preconditioner``: "amg" (AMG-PCG) or "jacobi". With AMG, :meth:`set_values`
+    ``preconditioner``: "amg" (AMG-PCG; by default the pressure-Poisson
+    configuration coarsened to at most 512 unknowns) or "jacobi". With AMG, :meth:`set_values`
     rebuilds the hierarchy when asked (``rebuild=True``) and otherwise follows
     ``refresh``: "recompute" re-forms the Galerkin operators for the new values
     with the cached transfer operators (``AlgebraicMultigrid::recompute``),
@@ -49,7 +50,13 @@ class SparseSolver:
             raise SolveError("SparseSolver needs a square matrix")
         self.dm = device_matrix(self.pattern)
         self.kind = preconditioner
-        self.amg_config = amg_config or AMGConfig.pressure_poisson()
+        if amg_config is None:
+            # values change at every call, and with them (by the Galerkin
+            # recompute) the coarsest operator's dense inverse, whose cost grows
+            # with its size cubed: coarsen to at most 512 unknowns
+            amg_config = AMGConfig.pressure_poisson()
+            amg_config.min_coarse_size = 512
+        self.amg_config = amg_config
         self.precision = precision
         self.config = config or IterativeSolverConfig(0.0, 1e-10, 2000)
         self.amg = None
