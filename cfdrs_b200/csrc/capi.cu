@@ -560,6 +560,13 @@ cfd_status cfd_context_set_stream(cfd_context* ctx, void* stream) {
   return CFD_OK;
 }
 
+cfd_status cfd_context_set_cluster_solve(cfd_context* ctx, int32_t enable) {
+  if (!ctx) return CFD_ERR_STATE;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  ctx->cluster_solve = enable != 0;
+  return CFD_OK;
+}
+
 cfd_status cfd_context_synchronize(cfd_context* ctx) {
   if (!ctx) return CFD_ERR_STATE;
   std::lock_guard<std::mutex> g(ctx->mu);

@@ -311,6 +311,9 @@ struct cfd_context {
   int* err = nullptr;    // set by a kernel whose bounded wait ran out
   int* h_err = nullptr;  // pinned mirror
   int num_sms = 148;
+  // CG / Jacobi-PCG of small systems as one thread-block-cluster launch
+  // (cluster_pcg.cu) where the system fits; cfd_context_set_cluster_solve
+  bool cluster_solve = true;
   cfd::KernelStats stats;
   std::mutex mu;
 };
@@ -347,4 +350,8 @@ cfd_status ensure_partials(cfd_context* ctx, int blocks);
 // as CFD_ERR_TIMEOUT and the flag and reduction ticket are reset.
 cfd_status check_device_flag(cfd_context* ctx);
 cfd_status ensure_diagonals(cfd_csr* a);
+// Whole CG / Jacobi-PCG solve in one thread-block cluster (cluster_pcg.cu):
+// *ok = false (nothing launched) when the system does not fit.
+cfd_status cluster_pcg_solve(cfd_context* ctx, const DevMat& m, const double* jinv, const double* b, double* x,
+                             DevState* st, bool* ok);
 }  // namespace cfd

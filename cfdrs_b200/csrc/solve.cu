@@ -1276,11 +1276,18 @@ cfd_status solve_fp64(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg, co
     CFD_TRY_CUDA(cudaMemsetAsync(B.v, 0, n * sizeof(double), ctx->stream));
     CFD_TRY_CUDA(cudaMemsetAsync(B.p, 0, n * sizeof(double), ctx->stream));
   }
-  // r0 = b - A x0, ||r0||, threshold, InitialResidual test.
-  CFD_TRY(lc.spmv<double, double, false>(a->dev, B.x, EpiResidual<double, 1>{B.r, B.b, st, nullptr, {}}));
   Poller pl{ctx, st, hs};
   pl.fixed = opt.check_every;
-  CFD_TRY(krylov_loop<double>(lc, opt.solver, opt.precond, a, amg, B, st, pl, opt.restart));
+  bool whole = false;
+  if (ctx->cluster_solve && opt.solver == CFD_SOLVER_CG &&
+      (opt.precond == CFD_PRECOND_NONE || opt.precond == CFD_PRECOND_JACOBI))
+    CFD_TRY(cluster_pcg_solve(ctx, a->dev, opt.precond == CFD_PRECOND_JACOBI ? a->jinv64 : nullptr, B.b, B.x, st,
+                              &whole));
+  if (!whole) {
+    // r0 = b - A x0, ||r0||, threshold, InitialResidual test.
+    CFD_TRY(lc.spmv<double, double, false>(a->dev, B.x, EpiResidual<double, 1>{B.r, B.b, st, nullptr, {}}));
+    CFD_TRY(krylov_loop<double>(lc, opt.solver, opt.precond, a, amg, B, st, pl, opt.restart));
+  }
   if (host_mem) CFD_TRY_CUDA(cudaMemcpyAsync(x, B.x, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CFD_TRY_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
   CFD_TRY(pl.poll());

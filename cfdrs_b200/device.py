@@ -44,6 +44,11 @@ class Context:
     def synchronize(self) -> None:
         _lib.check(_lib.load().cfd_context_synchronize(self.h))
 
+    def set_cluster_solve(self, enable: bool) -> None:
+        """Whole CG / Jacobi-PCG solves of small systems in one thread-block
+        cluster launch (the default) or always the multi-kernel solve."""
+        _lib.check(_lib.load().cfd_context_set_cluster_solve(self.h, 1 if enable else 0))
+
     def kernel_stats(self) -> dict:
         s = _lib.KernelStatsC()
         _lib.check(_lib.load().cfd_last_kernel_stats(self.h, C.byref(s)))

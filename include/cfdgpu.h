@@ -76,6 +76,12 @@ cfd_status cfd_context_create(int device, cfd_context** out);
  * current stream); NULL restores the context's own stream. To run on CUDA's
  * legacy default stream pass cudaStreamLegacy ((void*)0x1). */
 cfd_status cfd_context_set_stream(cfd_context* ctx, void* cuda_stream);
+/* FP64 CG and Jacobi-PCG (cfd_solve) of a system whose rows fit the shared
+ * memory of one thread-block cluster (up to 16 CTAs; e.g. 16 384 rows of a
+ * 5-point operator) run as one launch, the whole recurrence on chip
+ * (enable != 0, the default); 0 keeps the multi-kernel solve for every size.
+ * Same recurrence and termination; the dot products sum in another order. */
+cfd_status cfd_context_set_cluster_solve(cfd_context* ctx, int32_t enable);
 cfd_status cfd_context_synchronize(cfd_context* ctx);
 cfd_status cfd_context_destroy(cfd_context* ctx);
 

@@ -252,6 +252,60 @@ def test_pcg_jacobi_c1_parity(cuda, oracle):
     assert np.linalg.norm(b - A.matvec(x)) <= 1.0000001e-8 * np.linalg.norm(b)
 
 
+@pytest.mark.parametrize("pre", ["jacobi", "none"])
+def test_cluster_solve_matches_multi_kernel_solve(cuda, oracle, pre):
+    """Small systems run CG / Jacobi-PCG as one thread-block-cluster launch:
+    the 128^2 pressure system (16 384 rows) gives the multi-kernel solve's
+    iteration count to one and its solution to 1e-10, with a single kernel
+    launch; a 256^2 system does not fit a cluster's shared memory and runs
+    the multi-kernel solve."""
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import problems as P
+    from cfdrs_b200.device import device_matrix
+    A, b = P.poisson_2d_dirichlet(128, seed=0)
+    dm = device_matrix(A)
+    pc = cf.JacobiPreconditioner(A) if pre == "jacobi" else None
+    cfgs = cf.IterativeSolverConfig(0.0, 1e-8, 5000)
+
+    def solve(cluster):
+        dm.ctx.set_cluster_solve(cluster)
+        x = np.zeros_like(b)
+        rep = cf.cg_preconditioned(A, b, pc, x, cfgs) if pc is not None else cf.cg(A, b, x, cfgs)
+        return x, rep, dm.ctx.kernel_stats()["launches"]
+    try:
+        x1, r1, l1 = solve(True)
+        x2, r2, l2 = solve(False)
+    finally:
+        dm.ctx.set_cluster_solve(True)
+    assert r1.termination == r2.termination == cf.Termination.CONVERGED
+    assert abs(r1.iterations - r2.iterations) <= 1 and l1 == 1 and l2 > 3 * r2.iterations
+    assert rel(x1, x2) < 1e-10
+    assert abs(r1.initial_residual_norm - r2.initial_residual_norm) <= 1e-13 * r2.initial_residual_norm
+    opre = oracle.PRE_JACOBI if pre == "jacobi" else oracle.PRE_NONE
+    xo, ro = _oracle_solve(oracle, A, b, opre)
+    assert abs(r1.iterations - ro.iterations) <= 1 and rel(x1, xo) < 1e-10
+    B, bb = P.poisson_2d_dirichlet(256, seed=0)
+    xb = np.zeros_like(bb)
+    rb = cf.cg_preconditioned(B, bb, cf.JacobiPreconditioner(B), xb, cfgs)
+    assert rb.termination == cf.Termination.CONVERGED and device_matrix(B).ctx.kernel_stats()["launches"] > 3
+
+
+def test_cluster_solve_edge_cases(cuda):
+    """Fewer rows than the cluster's CTAs could hold (17 rows over two CTAs,
+    an odd split), a warm start at the solution, and the iteration budget."""
+    import cfdrs_b200 as cf
+    A = tridiag(17, lo=-1.0, d=2.5, hi=-1.0)
+    b = np.random.default_rng(4).uniform(-1, 1, 17)
+    x = np.zeros(17)
+    rep = cf.cg_preconditioned(A, b, cf.JacobiPreconditioner(A), x, cf.IterativeSolverConfig(0.0, 1e-12, 100))
+    assert rep.termination == cf.Termination.CONVERGED
+    np.testing.assert_allclose(A.matvec(x), b, atol=1e-10)
+    rep = cf.cg_preconditioned(A, b, cf.JacobiPreconditioner(A), x.copy(), cf.IterativeSolverConfig(1e-6, 0.0, 100))
+    assert rep.termination == cf.Termination.INITIAL_RESIDUAL and rep.iterations == 0
+    rep = cf.cg(A, b, np.zeros(17), cf.IterativeSolverConfig(0.0, 1e-14, 3))
+    assert rep.termination == cf.Termination.MAX_ITERATIONS and rep.iterations == 3
+
+
 def test_amg_pcg_parity(cuda, oracle):
     """3-D Poisson (constant k), AMG-PCG V(1,1) Jacobi w=2/3, dense coarsest, to 1e-8."""
     import cfdrs_b200 as cf
