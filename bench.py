@@ -622,14 +622,21 @@ def run_plain(args, world, rank, local):
             "config": config,
             "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": N * 8},
             "gpu_launches": int(launches * args.steps),
-            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
-                         "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "SpMV FP64 of the operator, timed alone ("
-                                   + ("diagonal pipeline; achieved counts the stored diagonals, x and y"
-                                      if diagonal else "achieved counts CSR bytes") + ")"
-                                   + (" (L2-resident: the HBM fraction does not bound it)"
-                                      if args.workload == "c1" else ""),
-                         "bytes_per_launch": spmv_bytes},
+            "roofline": ({"bound": "latency", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+                          "traffic": None, "peak_kind": peak_kind,
+                          "kernel": "k_cluster_pcg: the whole Jacobi-PCG solve in one thread-block cluster "
+                                    f"launch, {1e3 * ms / max(rep.iterations, 1):.2f} us per iteration (three "
+                                    "cluster barriers and two cluster reductions each; the system, 1.3 MB, "
+                                    "lives in distributed shared memory)"}
+                         if args.workload == "c1" and launches <= 2 else
+                         {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                          "traffic": None, "peak_kind": peak_kind,
+                          "kernel": "SpMV FP64 of the operator, timed alone ("
+                                    + ("diagonal pipeline; achieved counts the stored diagonals, x and y"
+                                       if diagonal else "achieved counts CSR bytes") + ")"
+                                    + (" (L2-resident: the HBM fraction does not bound it)"
+                                       if args.workload == "c1" else ""),
+                          "bytes_per_launch": spmv_bytes}),
             "iterations": rep.iterations, "true_rel_residual": true_rel, "clocks": clk.summary(),
         }
         line.update(extra)
