@@ -84,7 +84,8 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (arrival time, line)
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
@@ -93,16 +94,27 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the timed region starts once nvidia-smi is producing samples
+            deadline = time.perf_counter() + 5.0
+            while not self.lines and time.perf_counter() < deadline:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
+        self.t0 = time.perf_counter()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
 
     def __exit__(self, *a):
+        self.t1 = time.perf_counter()
         if self.proc:
+            # one sample after the region, for regions shorter than the sampling period
+            n = len(self.lines)
+            deadline = time.perf_counter() + 0.5
+            while len(self.lines) == n and time.perf_counter() < deadline:
+                time.sleep(0.005)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -112,7 +124,14 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        inside = [ln for t, ln in self.lines if self.t0 is not None and self.t0 <= t <= self.t1]
+        bracket = False
+        if not inside and self.t0 is not None:
+            # a region shorter than the 50 ms period: the last sample before it and the first after it
+            before = [ln for t, ln in self.lines if t < self.t0][-1:]
+            after = [ln for t, ln in self.lines if t > self.t1][:1]
+            inside, bracket = before + after, True
+        for ln in inside:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -126,8 +145,10 @@ class ClockSampler:
                     reasons.add(nm)
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        if bracket:
+            out["note"] = "timed region shorter than the 50 ms sampling period: the samples just before and after it"
+        return out
 
 
 def measured_peak():
