@@ -54,7 +54,8 @@ namespace {
 constexpr int kAsmThreads = 256;
 
 // bad[0]: smallest edge with a rejected conductance; bad[1]: bit 0 a
-// non-finite matrix entry, bit 1 a non-finite right-hand side.
+// non-finite matrix entry, bit 1 a non-finite right-hand side, bit 2 a finite
+// entry beyond the FP32 range (its FP32 copy is infinite: FP64 solves only).
 __global__ void k_network_assemble(NetworkView V, int64_t edges, int64_t nnz, int64_t rows,
                                    const double* __restrict__ g, const double* __restrict__ q, double* v64,
                                    float* v32, double* b, int* bad) {
@@ -65,8 +66,12 @@ __global__ void k_network_assemble(NetworkView V, int64_t edges, int64_t nnz, in
   for (int64_t k = t0; k < nnz; k += stride) {
     const double v = net_slot_value(V, k, g);
     v64[k] = v;
-    v32[k] = (float)v;
-    if (!isfinite(v)) atomicOr(bad + 1, 1);
+    const float f = (float)v;
+    v32[k] = f;
+    if (!isfinite(v))
+      atomicOr(bad + 1, 1);
+    else if (!isfinite(f))
+      atomicOr(bad + 1, 4);
   }
   for (int64_t r = t0; r < rows; r += stride) {
     const double br = net_rhs_value(V, r, g, q);
@@ -324,7 +329,9 @@ cfd_status cfd_batch_assemble(cfd_batch* bt, const double* conductance, const do
         CFD_TRY_CUDA(cudaMemcpy(&ge, conductance + e, sizeof(double), cudaMemcpyDeviceToHost));
       return bad_conductance("cfd_batch_assemble", e, ge);
     }
-    if (d->h_bad[1]) return nonfinite_system("cfd_batch_assemble", d->h_bad[1]);
+    if (d->h_bad[1] & 3) return nonfinite_system("cfd_batch_assemble", d->h_bad[1] & 3);
+    // FP32 solves of this batch are refused while an entry exceeds the FP32 range
+    bt->f32_out_of_range = (d->h_bad[1] & 4) != 0;
     bt->values_valid = true;
     bt->rhs_resident = true;
     return CFD_OK;

@@ -495,7 +495,9 @@ cfd_status cfd_batch_create_networks(cfd_context* ctx, int32_t num_systems, cons
  * non-finite assembled entry or right-hand side (a source or fixed pressure
  * that is not finite, an overflowing sum) is CFD_ERR_NONFINITE, as
  * validate_linear_system rejects it (solver_detection.rs:66-93). After either
- * the batch holds no valid matrix until a successful assembly. */
+ * the batch holds no valid matrix until a successful assembly. A finite entry
+ * beyond the FP32 range assembles (FP64 is exact), and FP32_REFINE solves of
+ * the batch return CFD_ERR_NONFINITE until an assembly without one. */
 cfd_status cfd_batch_assemble(cfd_batch* batch, const double* conductance, const double* neumann,
                               int32_t memory);
 /* Copies the batch's current values (nnz) and right-hand sides (total rows)

@@ -183,3 +183,25 @@ def test_nonfinite_system_rejected_on_device(cuda, nets):
     nb.assemble(pk.conductance)
     _, rep = nb.solve(None, config=cf.IterativeSolverConfig(0.0, 1e-10, 20000))
     assert rep.converged_systems == rep.num_systems
+
+
+def test_entry_beyond_fp32_range_blocks_fp32_solves(cuda, nets):
+    """A finite conductance above the FP32 range assembles (the FP64 values are
+    exact) and the FP64 solve runs; the FP32 copy would be infinite, so an
+    FP32 + refinement solve is refused until an assembly without such an entry."""
+    import cfdrs_b200 as cf
+    from cfdrs_b200.batch import NetworkBatch
+    from cfdrs_b200.krylov import SolveError
+    nb = NetworkBatch.from_networks(nets[:3])
+    pk = nb.packed
+    g = pk.conductance.copy()
+    g[0] = 1e39  # finite in FP64, above FLT_MAX
+    nb.assemble(g)
+    cfg = cf.IterativeSolverConfig(0.0, 1e-10, 20000)
+    _, rep = nb.solve(None, config=cfg)
+    assert rep.num_systems == 3
+    with pytest.raises(SolveError, match="FP32 range"):
+        nb.solve(None, config=cfg, precision=cf.Precision.FP32_REFINE)
+    nb.assemble(pk.conductance)
+    _, rep = nb.solve(None, config=cfg, precision=cf.Precision.FP32_REFINE)
+    assert rep.converged_systems == rep.num_systems
