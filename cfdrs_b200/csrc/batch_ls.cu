@@ -692,44 +692,24 @@ __device__ __forceinline__ void fast_load(double (*dst)[kFld], const double* __r
   }
 }
 
-// C = A B for a 64 x 64 tile from shared memory (c < kb, rows and columns of
-// A and B past kb zero) on the FP64 tensor path: mma.sync m8n8k4 f64, each of
-// the eight warps a 16 x 32 block of C (2 x 4 tiles of 8 x 8), per k-step of 4
-// two A and four B fragments for eight products. Thread (lane = 4 g + t) holds
-// C[wr 16 + 8 mi + g][wc 32 + 8 ni + 2 t + e] in acc[mi][ni][e].
-struct MmaTile {
-  int r0, c0, g, t;
-  __device__ MmaTile() {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    r0 = (w >> 1) * 16;
-    c0 = (w & 1) * 32;
-    g = lane >> 2;
-    t = lane & 3;
-  }
-  __device__ int row(int mi) const { return r0 + 8 * mi + g; }
-  __device__ int col(int ni, int e) const { return c0 + 8 * ni + 2 * t + e; }
-};
-
+// acc[a][q] = sum_c A[ty + 16 a][c] B[c][tx + 16 q], c < kb.
 __device__ __forceinline__ void fast_mm(const double (*A)[kFld], const double (*B)[kFld], int kb,
-                                        double (&acc)[2][4][2]) {
-  const MmaTile T;
+                                        double (&acc)[4][4]) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
 #pragma unroll
-  for (int mi = 0; mi < 2; ++mi)
+  for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int ni = 0; ni < 4; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
-  for (int k = 0; k < kb; k += 4) {
-    double a[2], b[4];
+    for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
+  for (int c = 0; c < kb; ++c) {
+    double lv[4], uv[4];
 #pragma unroll
-    for (int mi = 0; mi < 2; ++mi) a[mi] = A[T.r0 + 8 * mi + T.g][k + T.t];
+    for (int a = 0; a < 4; ++a) lv[a] = A[ty + 16 * a][c];
 #pragma unroll
-    for (int ni = 0; ni < 4; ++ni) b[ni] = B[k + T.t][T.c0 + 8 * ni + T.g];
+    for (int q = 0; q < 4; ++q) uv[q] = B[c][tx + 16 * q];
 #pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni)
-        asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%5};\n"
-                     : "=d"(acc[mi][ni][0]), "=d"(acc[mi][ni][1])
-                     : "d"(a[mi]), "d"(b[ni]), "d"(acc[mi][ni][0]), "d"(acc[mi][ni][1]));
+      for (int q = 0; q < 4; ++q) acc[a][q] += lv[a] * uv[q];
   }
 }
 
@@ -744,7 +724,7 @@ __device__ bool lu_solve_fast(double* __restrict__ M, double* __restrict__ Uinv_
   double(*At)[kFld] = Ui + kFb;
   double(*Bt)[kFld] = At + kFb;
   const int tid = threadIdx.x, nt = blockDim.x;
-  const MmaTile T;
+  const int tx = tid & 15, ty = tid >> 4;
   const size_t ld = (size_t)n + 1;
   if (tid == 0) *s_bad = 0;
   __syncthreads();
@@ -797,21 +777,18 @@ __device__ bool lu_solve_fast(double* __restrict__ M, double* __restrict__ Uinv_
       const int rows = min(kFb, n - rt);
       fast_load(At, M, ld, rt, k0, rows, kb);
       __syncthreads();
-      double acc[2][4][2];
+      double acc[4][4];
       fast_mm(At, Ui, kb, acc);
 #pragma unroll
-      for (int mi = 0; mi < 2; ++mi)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int r = T.row(mi), c = T.col(ni, e);
-            const double l = acc[mi][ni][e];
-            if (r < rows && c < kb) {
-              if (fabs(l) > 1.0 + kPivotSlack || !isfinite(l)) *s_bad = 1;
-              M[(size_t)(rt + r) * ld + k0 + c] = l;
-            }
+        for (int q = 0; q < 4; ++q) {
+          const int r = ty + 16 * a, c = tx + 16 * q;
+          if (r < rows && c < kb) {
+            if (fabs(acc[a][q]) > 1.0 + kPivotSlack || !isfinite(acc[a][q])) *s_bad = 1;
+            M[(size_t)(rt + r) * ld + k0 + c] = acc[a][q];
           }
+        }
       __syncthreads();
     }
     if (*s_bad) return false;
@@ -820,17 +797,15 @@ __device__ bool lu_solve_fast(double* __restrict__ M, double* __restrict__ Uinv_
       const int cols = min(kFb, n + 1 - ct);
       fast_load(Bt, M, ld, k0, ct, kb, cols);
       __syncthreads();
-      double acc[2][4][2];
+      double acc[4][4];
       fast_mm(Li, Bt, kb, acc);
 #pragma unroll
-      for (int mi = 0; mi < 2; ++mi)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int r = T.row(mi), c = T.col(ni, e);
-            if (r < kb && c < cols) M[(size_t)(k0 + r) * ld + ct + c] = acc[mi][ni][e];
-          }
+        for (int q = 0; q < 4; ++q) {
+          const int r = ty + 16 * a, c = tx + 16 * q;
+          if (r < kb && c < cols) M[(size_t)(k0 + r) * ld + ct + c] = acc[a][q];
+        }
       __syncthreads();
     }
     // A22 -= L21 U12 (columns through the right-hand side)
@@ -843,27 +818,23 @@ __device__ bool lu_solve_fast(double* __restrict__ M, double* __restrict__ Uinv_
         __syncthreads();
         // this thread's C entries are loaded before the product, so their
         // latency overlaps it
-        double cv[2][4][2];
+        double cv[4][4];
 #pragma unroll
-        for (int mi = 0; mi < 2; ++mi)
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              const int r = T.row(mi), c = T.col(ni, e);
-              cv[mi][ni][e] = (r < rows && c < cols) ? M[(size_t)(rt + r) * ld + ct + c] : 0.0;
-            }
-        double acc[2][4][2];
+          for (int q = 0; q < 4; ++q) {
+            const int r = ty + 16 * a, c = tx + 16 * q;
+            cv[a][q] = (r < rows && c < cols) ? M[(size_t)(rt + r) * ld + ct + c] : 0.0;
+          }
+        double acc[4][4];
         fast_mm(At, Bt, kb, acc);
 #pragma unroll
-        for (int mi = 0; mi < 2; ++mi)
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              const int r = T.row(mi), c = T.col(ni, e);
-              if (r < rows && c < cols) M[(size_t)(rt + r) * ld + ct + c] = cv[mi][ni][e] - acc[mi][ni][e];
-            }
+          for (int q = 0; q < 4; ++q) {
+            const int r = ty + 16 * a, c = tx + 16 * q;
+            if (r < rows && c < cols) M[(size_t)(rt + r) * ld + ct + c] = cv[a][q] - acc[a][q];
+          }
         __syncthreads();
       }
     }
