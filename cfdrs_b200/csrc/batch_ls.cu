@@ -713,56 +713,6 @@ __device__ __forceinline__ void fast_mm(const double (*A)[kFld], const double (*
   }
 }
 
-// Trailing update A22 -= L21 U12 by 128 x 128 blocks of C: L21 rows in a
-// 128 x kb tile (row stride kFld), U12 columns in a kb x 128 tile (row stride
-// kWld), each thread an 8 x 8 block of C (rows ty + 16 a, columns tx + 16 q),
-// so a k-step reads 16 operands from shared memory for 64 products. The tiles
-// overlay the panel buffers, which are free by then.
-constexpr int kWb = 2 * kFb;   // 128
-constexpr int kWld = kWb + 1;  // 129
-static_assert((size_t)kWb * kFld * sizeof(double) + (size_t)kFb * kWld * sizeof(double) <= kFastSmem,
-              "the 128 x 128 update tiles overlay the panel buffers");
-
-// dst[r * dld + c] = M[(r0 + r) ld + c0 + c] for r < rows, c < cols, else 0,
-// for an R x Cc tile; every thread issues its loads before its stores.
-template <int R, int Cc>
-__device__ __forceinline__ void tile_load(double* dst, int dld, const double* __restrict__ M, size_t ld, int r0,
-                                          int c0, int rows, int cols) {
-  constexpr int kPer = R * Cc / kLsThreads;
-  double v[kPer];
-#pragma unroll
-  for (int t = 0; t < kPer; ++t) {
-    const int q = threadIdx.x + t * kLsThreads, r = q / Cc, c = q % Cc;
-    v[t] = (r < rows && c < cols) ? M[(size_t)(r0 + r) * ld + c0 + c] : 0.0;
-  }
-#pragma unroll
-  for (int t = 0; t < kPer; ++t) {
-    const int q = threadIdx.x + t * kLsThreads;
-    dst[(q / Cc) * dld + q % Cc] = v[t];
-  }
-}
-
-// acc[a][q] = sum_c A[ty + 16 a][c] B[c][tx + 16 q], c < kb (A 128 x kFld, B kb x kWld).
-__device__ __forceinline__ void fast_mm8(const double* __restrict__ A, const double* __restrict__ B, int kb,
-                                         double (&acc)[8][8]) {
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-#pragma unroll
-  for (int a = 0; a < 8; ++a)
-#pragma unroll
-    for (int q = 0; q < 8; ++q) acc[a][q] = 0.0;
-  for (int c = 0; c < kb; ++c) {
-    double lv[8], uv[8];
-#pragma unroll
-    for (int a = 0; a < 8; ++a) lv[a] = A[(ty + 16 * a) * kFld + c];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) uv[q] = B[c * kWld + tx + 16 * q];
-#pragma unroll
-    for (int a = 0; a < 8; ++a)
-#pragma unroll
-      for (int q = 0; q < 8; ++q) acc[a][q] += lv[a] * uv[q];
-  }
-}
-
 // Factor and solve the n x n system in M (row stride n + 1, right-hand side in
 // column n); on success column n holds x. Returns false (uniformly) when the
 // pivot guard stops the fast path.
@@ -858,34 +808,33 @@ __device__ bool lu_solve_fast(double* __restrict__ M, double* __restrict__ Uinv_
         }
       __syncthreads();
     }
-    // A22 -= L21 U12 (columns through the right-hand side), 128 x 128 blocks
-    double* Wa = reinterpret_cast<double*>(smem);  // 128 x kFld
-    double* Wb = Wa + (size_t)kWb * kFld;          // kFb x kWld
-    __syncthreads();  // the panel buffers are overlaid from here
-    for (int rt = m0; rt < n; rt += kWb) {
-      const int rows = min(kWb, n - rt);
-      tile_load<kWb, kFb>(Wa, kFld, M, ld, rt, k0, rows, kb);
-      for (int ct = m0; ct <= n; ct += kWb) {
-        const int cols = min(kWb, n + 1 - ct);
-        tile_load<kFb, kWb>(Wb, kWld, M, ld, k0, ct, kb, cols);
+    // A22 -= L21 U12 (columns through the right-hand side)
+    for (int rt = m0; rt < n; rt += kFb) {
+      const int rows = min(kFb, n - rt);
+      fast_load(At, M, ld, rt, k0, rows, kb);
+      for (int ct = m0; ct <= n; ct += kFb) {
+        const int cols = min(kFb, n + 1 - ct);
+        fast_load(Bt, M, ld, k0, ct, kb, cols);
         __syncthreads();
-        double acc[8][8];
-        fast_mm8(Wa, Wb, kb, acc);
+        // this thread's C entries are loaded before the product, so their
+        // latency overlaps it
+        double cv[4][4];
 #pragma unroll
-        for (int a = 0; a < 8; ++a) {
-          const int r = ty + 16 * a;
-          double cv[8];
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int c = tx + 16 * q;
-            cv[q] = (r < rows && c < cols) ? M[(size_t)(rt + r) * ld + ct + c] : 0.0;
+          for (int q = 0; q < 4; ++q) {
+            const int r = ty + 16 * a, c = tx + 16 * q;
+            cv[a][q] = (r < rows && c < cols) ? M[(size_t)(rt + r) * ld + ct + c] : 0.0;
           }
+        double acc[4][4];
+        fast_mm(At, Bt, kb, acc);
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int c = tx + 16 * q;
-            if (r < rows && c < cols) M[(size_t)(rt + r) * ld + ct + c] = cv[q] - acc[a][q];
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int r = ty + 16 * a, c = tx + 16 * q;
+            if (r < rows && c < cols) M[(size_t)(rt + r) * ld + ct + c] = cv[a][q] - acc[a][q];
           }
-        }
         __syncthreads();
       }
     }
