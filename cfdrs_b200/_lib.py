@@ -28,7 +28,7 @@ EXPORTS = [
     "cfd_amg_level", "cfd_amg_set_path", "cfd_amg_destroy", "cfd_amg_setup_host", "cfd_selftest_wait_timeout",
     "cfd_saddle_setup", "cfd_simple_apply", "cfd_block_diagonal_apply", "cfd_simple_apply_host",
     "cfd_block_diagonal_host", "cfd_component_block_setup", "cfd_component_block_apply",
-    "cfd_darcy2d_assemble", "cfd_darcy2d_theta_grad", "cfd_context_set_cluster_solve",
+    "cfd_darcy2d_assemble", "cfd_darcy2d_theta_grad", "cfd_context_set_cluster_solve", "cfd_adjoint",
     "cfd_solve_options_default", "cfd_solve", "cfd_last_kernel_stats",
     "cfd_pattern_outer", "cfd_csr_set_values_device",
     "cfd_batch_create", "cfd_batch_update_values", "cfd_batch_solve", "cfd_batch_autotune", "cfd_batch_config",
@@ -160,6 +160,7 @@ def load():
         "cfd_component_block_apply": (C.c_int, [P, P, P]),
         "cfd_darcy2d_assemble": (C.c_int, [P, C.c_int64, P, P, P]),
         "cfd_context_set_cluster_solve": (C.c_int, [P, I32]),
+        "cfd_adjoint": (C.c_int, [P, P, P, P, P, P, P, I32, P, P]),
         "cfd_darcy2d_theta_grad": (C.c_int, [P, C.c_int64, P, P, P, P]),
         "cfd_block_diagonal_host": (C.c_int, [C.c_int64, P, P, P, C.c_int64, P]),
         "cfd_simple_apply_host": (C.c_int, [C.c_int64, P, P, P, C.c_int64, P, P]),

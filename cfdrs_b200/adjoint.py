@@ -25,7 +25,8 @@ import torch
 
 from . import _lib
 from .device import device_matrix, mark_synced
-from .krylov import IterativeSolverConfig, Precision, SolveError, Termination, cg_preconditioned
+from .krylov import (IterativeSolverConfig, Precision, SolveError, SolveReport, Termination, bicgstab_preconditioned,
+                     cg_preconditioned)
 from .multigrid import AlgebraicMultigrid, AMGConfig, JacobiPreconditioner
 from .sparse import CsrMatrix
 
@@ -44,11 +45,14 @@ class SparseSolver:
 
     def __init__(self, pattern: CsrMatrix, preconditioner: str = "amg", amg_config: AMGConfig | None = None,
                  precision: Precision = Precision.FP32_REFINE,
-                 config: IterativeSolverConfig | None = None):
+                 config: IterativeSolverConfig | None = None, solver: str = "cg"):
         self.pattern = CsrMatrix(pattern.row_ptr, pattern.col, pattern.val.copy(), pattern.shape)
         if self.pattern.nrows != self.pattern.ncols:
             raise SolveError("SparseSolver needs a square matrix")
         self.dm = device_matrix(self.pattern)
+        if solver not in ("cg", "bicgstab"):
+            raise SolveError(f"solver must be 'cg' or 'bicgstab', got {solver!r}")
+        self.solver = solver
         self.kind = preconditioner
         if amg_config is None:
             # values change at every call, and with them (by the Galerkin
@@ -103,12 +107,46 @@ class SparseSolver:
               config: IterativeSolverConfig | None = None) -> torch.Tensor:
         x = torch.zeros_like(b, dtype=torch.float64)
         pre = self.amg if self.kind == "amg" else JacobiPreconditioner(self.dm)
-        rep = cg_preconditioned(self.dm, b.to(torch.float64).contiguous(), pre, x, config or self.config,
-                                precision=self.precision if precision is None else precision)
+        fn = cg_preconditioned if self.solver == "cg" else bicgstab_preconditioned
+        rep = fn(self.dm, b.to(torch.float64).contiguous(), pre, x, config or self.config,
+                 precision=self.precision if precision is None else precision)
         if rep.termination not in (Termination.CONVERGED, Termination.INITIAL_RESIDUAL):
             raise SolveError(f"sparse solve did not converge: {rep}")
         self.last_report = rep
         return x
+
+    def adjoint(self, g: torch.Tensor, x: torch.Tensor, values: bool = True):
+        """The backward of x = A^-1 b for g = dL/dx (``cfd_adjoint``): lambda =
+        A^-T g, solved on A when A is symmetric (the forward's preconditioner)
+        and on A's transpose otherwise (Jacobi preconditioner), and, with
+        ``values``, dL/dA on A's pattern. Returns (lambda, dL/dA or None)."""
+        g = g.to(torch.float64).contiguous()
+        x = x.to(torch.float64).contiguous()
+        lam = torch.empty_like(g)
+        gv = torch.empty(self.pattern.nnz, dtype=torch.float64, device=g.device) if values else None
+        transpose = not self.symmetric
+        use_amg = self.kind == "amg" and not transpose
+        opt = _lib.SolveOptionsC(0 if self.solver == "cg" else 1, 2 if use_amg else 1, int(self.precision), 1,
+                                 1e-4, 20, 0, 30)
+        cfg = self.config.to_c()
+        rep = _lib.SolveReportC()
+        self.dm.ctx.set_stream(torch.cuda.current_stream(g.device).cuda_stream)
+        try:
+            st = _lib.load().cfd_adjoint(self.dm.h, C.byref(opt), self.amg.h if use_amg else None,
+                                         C.c_void_p(x.data_ptr()), C.c_void_p(g.data_ptr()),
+                                         C.c_void_p(lam.data_ptr()), C.c_void_p(gv.data_ptr()) if values else None,
+                                         1 if transpose else 0, C.byref(cfg), C.byref(rep))
+        finally:
+            self.dm.ctx.set_stream(None)
+        if st != _lib.CFD_OK:
+            raise SolveError(f"adjoint solve failed: {_lib.STATUS_NAMES.get(st, st)}: "
+                             f"{_lib.load().cfd_last_error().decode()}")
+        report = SolveReport(Termination(rep.termination), rep.iterations, rep.initial_residual,
+                             rep.final_residual, rep.threshold, rep.outer_iterations, rep.device_ms)
+        if report.termination not in (Termination.CONVERGED, Termination.INITIAL_RESIDUAL):
+            raise SolveError(f"adjoint solve did not converge: {report}")
+        self.last_report = report
+        return lam, gv
 
     def pattern_outer(self, lam: torch.Tensor, x: torch.Tensor, scale: float = 1.0) -> torch.Tensor:
         """g_e = -scale * lam[row(e)] * x[col(e)] on A's pattern (device)."""
@@ -139,10 +177,7 @@ class SparseSolveFunction(torch.autograd.Function):
     def backward(ctx, gx):
         solver: SparseSolver = ctx.solver
         (x,) = ctx.saved_tensors
-        if not solver.symmetric:
-            raise SolveError("the adjoint solve reuses A and its preconditioner, so A must be symmetric")
-        lam = solver.solve(gx.contiguous())  # A^T lambda = dL/dx with A^T = A
-        gvals = solver.pattern_outer(lam, x)
+        lam, gvals = solver.adjoint(gx, x)  # A^T lambda = dL/dx; dL/dA = -lambda x^T on the pattern
         return gvals, lam, None, None
 
 
@@ -232,9 +267,7 @@ class DarcySolveFunction(torch.autograd.Function):
     def backward(ctx, gx):
         solver: SparseSolver = ctx.solver
         theta, x = ctx.saved_tensors
-        if not solver.symmetric:
-            raise SolveError("the adjoint solve reuses A and its preconditioner, so A must be symmetric")
-        lam = solver.solve(gx.contiguous())
+        lam, _ = solver.adjoint(gx, x, values=False)
         n = theta.shape[0]
         g = torch.empty_like(theta)
         solver.dm.ctx.set_stream(torch.cuda.current_stream(theta.device).cuda_stream)

@@ -127,6 +127,17 @@ __global__ void k_cast64to32(int64_t n, const double* __restrict__ s, float* __r
 }
 
 }  // namespace
+
+cfd_status pattern_outer_launch(cfd_csr* a, const double* lambda, const double* x, double scale, double* g) {
+  const int64_t n = a->dev.nrows;
+  if (n == 0) return CFD_OK;
+  const int grid = (int)std::min<int64_t>((n + kThreads - 1) / kThreads, (int64_t)a->ctx->num_sms * 8);
+  k_pattern_outer<<<grid, kThreads, 0, a->ctx->stream>>>(n, a->dev.rp, a->dev.col, lambda, x, scale, g);
+  a->ctx->stats.launches++;
+  CFD_TRY_CUDA(cudaGetLastError());
+  return CFD_OK;
+}
+
 }  // namespace cfd
 
 using namespace cfd;
@@ -140,12 +151,7 @@ cfd_status cfd_pattern_outer(cfd_csr* a, const double* lambda, const double* x, 
   }
   std::lock_guard<std::mutex> lk(a->ctx->mu);
   CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
-  const int64_t n = a->dev.nrows;
-  if (n == 0) return CFD_OK;
-  const int grid = (int)std::min<int64_t>((n + kThreads - 1) / kThreads, (int64_t)a->ctx->num_sms * 8);
-  k_pattern_outer<<<grid, kThreads, 0, a->ctx->stream>>>(n, a->dev.rp, a->dev.col, lambda, x, scale, g);
-  CFD_TRY_CUDA(cudaGetLastError());
-  return CFD_OK;
+  return pattern_outer_launch(a, lambda, x, scale, g);
 }
 
 cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev) {
@@ -168,6 +174,7 @@ cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev) {
   // The host copy feeds AMG setup (the Galerkin recompute reads the device values).
   CFD_TRY_CUDA(cudaMemcpyAsync(a->host.v.data(), val_dev, nnz * sizeof(double), cudaMemcpyDeviceToHost, s));
   CFD_TRY_CUDA(cudaStreamSynchronize(s));
+  a->values_version++;
   a->simple_stale = a->simple_nv >= 0;
   a->cblock_stale = a->cblock_nv >= 0;
   if (a->diag64) {

@@ -647,6 +647,7 @@ cfd_status cfd_csr_update_values(cfd_csr* a, const double* val) {
     // only once the device copy and the FP32 cast have succeeded.
     CFD_TRY(devmat_update_values(a->dev, val, a->host.nnz(), false, a->ctx->stream));
     std::copy(val, val + a->host.nnz(), a->host.v.begin());
+    a->values_version++;
     a->simple_stale = a->simple_nv >= 0;
     a->cblock_stale = a->cblock_nv >= 0;
     dfree(a->diag64);
@@ -766,6 +767,7 @@ cfd_status cfd_csr_destroy(cfd_csr* a) {
   dfree(a->jinv32);
   simple_free(a->simple);
   component_free(a->cblock);
+  cfd_csr_destroy(a->tr);
   delete a;
   return CFD_OK;
 }
@@ -1006,6 +1008,119 @@ void cfd_solve_options_default(cfd_solve_options* o) {
   o->restart = 30;
 }
 
+// The solve arguments cfd_solve and cfd_adjoint share.
+static cfd_status validate_solve(const cfd_csr* a, const cfd_solve_options* opt, const cfd_solver_config* cfg) {
+  // convergence_policy (krylov.rs:123-139) rejects non-finite or negative
+  // tolerances and a zero iteration budget at construction.
+  if (!(cfg->tolerance >= 0.0) || !(cfg->relative_tolerance >= 0.0) || !std::isfinite(cfg->tolerance) ||
+      !std::isfinite(cfg->relative_tolerance) || cfg->max_iterations <= 0) {
+    set_error("invalid iterative solver configuration: tolerance %g, relative %g, max_iterations %lld",
+              cfg->tolerance, cfg->relative_tolerance, (long long)cfg->max_iterations);
+    return CFD_ERR_CONFIG;
+  }
+  if (opt->solver < 0 || opt->solver > 2 || opt->precond < 0 || opt->precond > 5 || opt->precision < 0 ||
+      opt->precision > 1 || opt->memory < 0 || opt->memory > 1 || (opt->solver == CFD_SOLVER_GMRES && opt->restart < 1)) {
+    set_error("invalid solve options");
+    return CFD_ERR_CONFIG;
+  }
+  if (a->host.nrows != a->host.ncols) {
+    set_error("Krylov solve needs a square matrix (%lld x %lld)", (long long)a->host.nrows,
+              (long long)a->host.ncols);
+    return CFD_ERR_DIM;
+  }
+  return CFD_OK;
+}
+
+// A's transpose as a matrix of its own context, formed on the host from A's
+// current values (columns of each row ascending) and uploaded; its values are
+// refreshed after A's change. Called with the context's lock held.
+static cfd_status csr_transposed(cfd_csr* a, cfd_csr** out) {
+  if (a->tr && a->tr_version == a->values_version) {
+    *out = a->tr;
+    return CFD_OK;
+  }
+  const HostCsr& h = a->host;
+  HostCsr T;
+  T.nrows = h.ncols;
+  T.ncols = h.nrows;
+  T.rp.assign(T.nrows + 1, 0);
+  for (int64_t k = 0; k < h.nnz(); ++k) T.rp[h.ci[k] + 1]++;
+  for (int64_t i = 0; i < T.nrows; ++i) T.rp[i + 1] += T.rp[i];
+  T.ci.resize(h.nnz());
+  T.v.resize(h.nnz());
+  std::vector<int64_t> next(T.rp.begin(), T.rp.end() - 1);
+  for (int64_t r = 0; r < h.nrows; ++r)
+    for (int64_t k = h.rp[r]; k < h.rp[r + 1]; ++k) {
+      const int64_t q = next[h.ci[k]]++;
+      T.ci[q] = (int32_t)r;
+      T.v[q] = h.v[k];
+    }
+  if (a->tr) {
+    CFD_TRY(devmat_update_values(a->tr->dev, T.v.data(), T.nnz(), false, a->ctx->stream));
+    a->tr->host.v = T.v;
+    a->tr->values_version++;
+    dfree(a->tr->diag64);
+    dfree(a->tr->diag32);
+    dfree(a->tr->jinv64);
+    dfree(a->tr->jinv32);
+    a->tr->jacobi_status = -1;
+  } else {
+    cfd_csr* t = new cfd_csr;
+    t->ctx = a->ctx;
+    t->host = std::move(T);
+    cfd_status st = devmat_upload(t->dev, t->host, false, a->ctx->stream);
+    if (st == CFD_OK) st = ensure_partials(a->ctx, t->dev.nblk);
+    if (st != CFD_OK) {
+      devmat_free(t->dev);
+      delete t;
+      return st;
+    }
+    a->tr = t;
+  }
+  a->tr_version = a->values_version;
+  *out = a->tr;
+  return CFD_OK;
+}
+
+cfd_status cfd_adjoint(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, const double* x, const double* g,
+                       double* lambda, double* gvals, int32_t transpose, const cfd_solver_config* cfg,
+                       cfd_solve_report* rep) {
+  return guarded("cfd_adjoint", [&]() -> cfd_status {
+    if (!a || !opt || !x || !g || !lambda || !cfg || !rep) {
+      set_error("null argument to cfd_adjoint");
+      return CFD_ERR_STATE;
+    }
+    CFD_TRY(validate_solve(a, opt, cfg));
+    if (transpose && opt->precond != CFD_PRECOND_NONE && opt->precond != CFD_PRECOND_JACOBI) {
+      set_error("cfd_adjoint: the transposed solve takes the Jacobi preconditioner or none (the AMG and "
+                "saddle-point preconditioners were built for A)");
+      return CFD_ERR_CONFIG;
+    }
+    cfd_solve_options o = *opt;
+    o.memory = CFD_MEMORY_DEVICE;
+    std::lock_guard<std::mutex> lk(a->ctx->mu);
+    CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
+    cfd_csr* target = a;
+    if (transpose) CFD_TRY(csr_transposed(a, &target));
+    CFD_TRY(check_precond(target, o, amg));
+    a->ctx->stats.reset();
+    std::memset(rep, 0, sizeof(*rep));
+    const int64_t n = a->host.nrows;
+    if (n == 0) {
+      rep->termination = CFD_TERM_INITIAL_RESIDUAL;
+      return CFD_OK;
+    }
+    CFD_TRY_CUDA(cudaMemsetAsync(lambda, 0, n * sizeof(double), a->ctx->stream));
+    if (o.precision == CFD_PRECISION_FP32_REFINE)
+      CFD_TRY(solve_refine(target, o, amg, g, lambda, *cfg, *rep));
+    else
+      CFD_TRY(solve_fp64(target, o, amg, g, lambda, *cfg, *rep));
+    if (gvals) CFD_TRY(pattern_outer_launch(a, lambda, x, 1.0, gvals));
+    CFD_TRY_CUDA(cudaStreamSynchronize(a->ctx->stream));
+    return check_device_flag(a->ctx);
+  });
+}
+
 cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, const double* b, double* x,
                      const cfd_solver_config* cfg, cfd_solve_report* rep) {
   return guarded("cfd_solve", [&]() -> cfd_status {
@@ -1013,24 +1128,7 @@ cfd_status cfd_solve(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, con
       set_error("null argument to cfd_solve");
       return CFD_ERR_STATE;
     }
-    // convergence_policy (krylov.rs:123-139) rejects non-finite or negative
-    // tolerances and a zero iteration budget at construction.
-    if (!(cfg->tolerance >= 0.0) || !(cfg->relative_tolerance >= 0.0) || !std::isfinite(cfg->tolerance) ||
-        !std::isfinite(cfg->relative_tolerance) || cfg->max_iterations <= 0) {
-      set_error("invalid iterative solver configuration: tolerance %g, relative %g, max_iterations %lld",
-                cfg->tolerance, cfg->relative_tolerance, (long long)cfg->max_iterations);
-      return CFD_ERR_CONFIG;
-    }
-    if (opt->solver < 0 || opt->solver > 2 || opt->precond < 0 || opt->precond > 5 || opt->precision < 0 ||
-        opt->precision > 1 || opt->memory < 0 || opt->memory > 1 || (opt->solver == CFD_SOLVER_GMRES && opt->restart < 1)) {
-      set_error("invalid solve options");
-      return CFD_ERR_CONFIG;
-    }
-    if (a->host.nrows != a->host.ncols) {
-      set_error("Krylov solve needs a square matrix (%lld x %lld)", (long long)a->host.nrows,
-                (long long)a->host.ncols);
-      return CFD_ERR_DIM;
-    }
+    CFD_TRY(validate_solve(a, opt, cfg));
     std::lock_guard<std::mutex> g(a->ctx->mu);
     CFD_TRY_CUDA(cudaSetDevice(a->ctx->device));
     CFD_TRY(check_precond(a, *opt, amg));

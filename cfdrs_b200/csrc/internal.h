@@ -342,6 +342,11 @@ struct cfd_csr {
   // Grid size n of the 2-D Darcy pattern the matrix was checked against
   // (cfd_darcy2d_*), -1 before the first check.
   int64_t darcy_n = -1;
+  // Value updates so far, and the transpose (cfd_adjoint with transpose != 0),
+  // formed from the values of update tr_version.
+  uint64_t values_version = 0;
+  cfd_csr* tr = nullptr;
+  uint64_t tr_version = 0;
 };
 
 namespace cfd {
@@ -350,6 +355,8 @@ cfd_status ensure_partials(cfd_context* ctx, int blocks);
 // as CFD_ERR_TIMEOUT and the flag and reduction ticket are reset.
 cfd_status check_device_flag(cfd_context* ctx);
 cfd_status ensure_diagonals(cfd_csr* a);
+// g_e = -scale * lambda[row(e)] * x[col(e)] over A's pattern, on the context stream.
+cfd_status pattern_outer_launch(cfd_csr* a, const double* lambda, const double* x, double scale, double* g);
 // Whole CG / Jacobi-PCG solve in one thread-block cluster (cluster_pcg.cu):
 // *ok = false (nothing launched) when the system does not fit.
 cfd_status cluster_pcg_solve(cfd_context* ctx, const DevMat& m, const double* jinv, const double* b, double* x,

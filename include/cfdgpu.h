@@ -311,6 +311,17 @@ cfd_status cfd_pattern_outer(cfd_csr* a, const double* lambda_dev, const double*
 /* Replace A's values from device memory (same pattern); the host copy used by
  * AMG setup is refreshed too (cfd_amg_recompute reads the device values). */
 cfd_status cfd_csr_set_values_device(cfd_csr* a, const double* val_dev);
+/* The backward of x = A^-1 b for an upstream gradient g = dL/dx (device arrays
+ * of n): lambda = A^-T g (dL/db), solved with opt (memory forced to device;
+ * lambda starts from 0) on A when transpose == 0 (A symmetric: the forward's
+ * preconditioner, AMG included, serves) or on A's transpose when transpose !=
+ * 0 (formed from A's current values and kept until they change; Jacobi or no
+ * preconditioner, e.g. BiCGSTAB for a non-symmetric A); then, when gvals is
+ * not NULL, dL/da_ij = -lambda_i x_j on A's pattern into gvals (nnz). The
+ * report is the transposed solve's. */
+cfd_status cfd_adjoint(cfd_csr* a, const cfd_solve_options* opt, cfd_amg* amg, const double* x_dev,
+                       const double* g_dev, double* lambda_dev, double* gvals_dev, int32_t transpose,
+                       const cfd_solver_config* cfg, cfd_solve_report* rep);
 /* The 2-D Darcy workload's assembly and its chain rule on the device, on the
  * context's stream. a holds the pattern of an n x n cell grid (row i + n j;
  * per row south, west, diagonal, east, north as present; checked once):

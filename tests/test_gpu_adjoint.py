@@ -204,3 +204,46 @@ def test_darcy_512_fused_gradient(cuda):
     fd = AC.central_fd_lowrank(theta, col, cells, h=1e-6)
     ga = np.array([g[j, i] for j, i in cells])
     assert np.abs(ga - fd).max() <= 1e-4 * np.abs(g_cpu).max()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_refine"])
+def test_nonsymmetric_adjoint_is_a_transposed_solve(cuda, precision):
+    """A non-symmetric operator (diffusion plus first-order upwind convection
+    on 24 x 24 cells): the backward solves A^T lambda = dL/dx on A's
+    transpose (cfd_adjoint, BiCGSTAB with Jacobi), so dL/db = A^-T w and
+    dL/dA = -lambda x^T on the pattern match the direct solves to 1e-8; a
+    value update re-forms the transpose."""
+    torch = cuda
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    import cfdrs_b200 as cf
+    from cfdrs_b200.adjoint import SparseSolver, sparse_solve
+    from cfdrs_b200.sparse import CsrMatrix
+    n = 24
+    e = np.ones(n)
+    T = sp.diags([-e[:-1], 2 * e, -e[:-1]], [-1, 0, 1])
+    U = sp.diags([-e[:-1], e], [-1, 0])  # upwind first difference
+    I = sp.identity(n)
+    S = (sp.kron(I, T) + sp.kron(T, I) + 0.8 * sp.kron(I, U)).tocsr()
+    S.sort_indices()
+    A = CsrMatrix(S.indptr.astype(np.int64), S.indices.astype(np.int64), S.data.copy(), S.shape)
+    prec = cf.Precision.FP64 if precision == "fp64" else cf.Precision.FP32_REFINE
+    s = SparseSolver(A, preconditioner="jacobi", solver="bicgstab", precision=prec,
+                     config=cf.IterativeSolverConfig(0.0, 1e-13 if precision == "fp64" else 1e-11, 5000))
+    rng = np.random.default_rng(5)
+    b = rng.standard_normal(n * n)
+    w = torch.as_tensor(rng.standard_normal(n * n), device="cuda")
+    rows = np.repeat(np.arange(n * n), np.diff(A.row_ptr))
+    for scale in (1.0, 1.7):
+        vals = torch.as_tensor(scale * A.val, device="cuda").requires_grad_(True)
+        bt = torch.as_tensor(b, device="cuda").requires_grad_(True)
+        x = sparse_solve(vals, bt, s)
+        assert s.symmetric is False
+        (x * w).sum().backward()
+        Sc = (scale * S).tocsc()
+        xs = spla.spsolve(Sc, b)
+        lam = spla.spsolve(Sc.T.tocsc(), w.cpu().numpy())
+        tol = 1e-8 if precision == "fp64" else 1e-7
+        assert np.linalg.norm(bt.grad.cpu().numpy() - lam) <= tol * np.linalg.norm(lam)
+        gv = -lam[rows] * xs[A.col]
+        assert np.linalg.norm(vals.grad.cpu().numpy() - gv) <= tol * np.linalg.norm(gv)
