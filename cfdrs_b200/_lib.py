@@ -32,6 +32,7 @@ EXPORTS = [
     "cfd_solve_options_default", "cfd_solve", "cfd_last_kernel_stats",
     "cfd_pattern_outer", "cfd_csr_set_values_device",
     "cfd_batch_create", "cfd_batch_update_values", "cfd_batch_solve", "cfd_batch_autotune", "cfd_batch_config",
+    "cfd_batch_groups", "cfd_batch_set_config",
     "cfd_batch_create_networks", "cfd_batch_assemble", "cfd_batch_values", "cfd_network_assemble_host",
     "cfd_batch_destroy", "cfd_ls_options_default", "cfd_batch_linear_system_solve",
     "cfd_residual_norm_noalloc",
@@ -172,6 +173,8 @@ def load():
         "cfd_batch_solve": (C.c_int, [P, P, P, P, P, P, P, P, P]),
         "cfd_batch_autotune": (C.c_int, [P, I32, I32]),
         "cfd_batch_config": (C.c_int, [P, I32, P, P, P]),
+        "cfd_batch_groups": (C.c_int, [P, I32, P]),
+        "cfd_batch_set_config": (C.c_int, [P, I32, P, P]),
         "cfd_batch_destroy": (C.c_int, [P]),
         "cfd_ls_options_default": (None, [P]),
         "cfd_batch_linear_system_solve": (C.c_int, [P, P, P, P, P, P]),

@@ -323,12 +323,24 @@ class NetworkBatch:
         _lib.check(_lib.load().cfd_batch_autotune(self.h, int(precision), sample_iterations))
         return self.config(precision)
 
+    def set_config(self, threads, systems_per_cta, precision: Precision = Precision.FP64) -> None:
+        """Fix the Jacobi-PCG kernel's threads per system and systems per CTA
+        for each of the 4 size buckets (in place of :meth:`autotune`)."""
+        thr = np.ascontiguousarray(threads, dtype=np.int32)
+        grp = np.ascontiguousarray(systems_per_cta, dtype=np.int32)
+        if thr.shape != (4,) or grp.shape != (4,):
+            raise ValueError("threads and systems_per_cta take one entry per bucket (4)")
+        _lib.check(_lib.load().cfd_batch_set_config(self.h, int(precision), _p(thr), _p(grp)))
+
     def config(self, precision: Precision = Precision.FP64) -> dict:
         rows = np.zeros(4, np.int32)
         thr = np.zeros(4, np.int32)
         sysn = np.zeros(4, np.int32)
+        grp = np.zeros(4, np.int32)
         _lib.check(_lib.load().cfd_batch_config(self.h, int(precision), _p(rows), _p(thr), _p(sysn)))
-        return {"bucket_rows": rows.tolist(), "threads": thr.tolist(), "systems": sysn.tolist()}
+        _lib.check(_lib.load().cfd_batch_groups(self.h, int(precision), _p(grp)))
+        return {"bucket_rows": rows.tolist(), "threads": thr.tolist(), "systems_per_cta": grp.tolist(),
+                "systems": sysn.tolist()}
 
     def __del__(self):
         h = getattr(self, "h", None)

@@ -33,7 +33,8 @@
 namespace cfd {
 namespace {
 
-constexpr int kCandidates[] = {32, 64, 128, 256, 512};
+constexpr int kCandidates[] = {32, 64, 128, 256, 512};  // threads per system
+constexpr int kGroupCandidates[] = {1, 2, 4};             // systems per CTA
 
 struct BatchSys {
   const int* __restrict__ sys_row;   // first global row of each system (nsys + 1)
@@ -72,14 +73,37 @@ __host__ __device__ constexpr size_t batch_smem(int nmax, int zmax) {
   return batch_vec_off<T>(nmax, zmax) + 6 * round16((size_t)nmax * sizeof(T));
 }
 
-// Sum over the CTA, result in every thread. `slot` alternates between calls so
-// one barrier suffices between consecutive reductions.
-__device__ __forceinline__ double cta_sum(double v, double* buf) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+// A CTA runs G independent system groups of blockDim / G threads (G = 1, 2 or
+// 4; a group is a whole number of warps). A group synchronises on its own
+// named barrier (1 + group; the CTA-wide barrier 0 when G = 1; the warp
+// barrier when the group is one warp), so groups that run systems of
+// different lengths never wait for one another.
+constexpr int kMaxGroups = 4;
+struct Group {
+  int g, gsz, t;  // group, threads per group, thread within the group
+  __device__ Group(int groups) {
+    gsz = (int)blockDim.x / groups;
+    g = (int)threadIdx.x / gsz;
+    t = (int)threadIdx.x - g * gsz;
+  }
+  __device__ __forceinline__ void sync(int groups) const {
+    if (groups == 1)
+      __syncthreads();
+    else if (gsz == 32)
+      __syncwarp();
+    else
+      asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(gsz) : "memory");
+  }
+};
+
+// Sum over the group, result in every thread. `slot` alternates between calls
+// so one barrier suffices between consecutive reductions.
+__device__ __forceinline__ double group_sum(double v, double* buf, const Group& G, int groups) {
+  const int lane = G.t & 31, w = G.t >> 5, nw = G.gsz >> 5;
   v = warp_sum(v);
   if (nw == 1) return __shfl_sync(0xffffffffu, v, 0);
   if (lane == 0) buf[w] = v;
-  __syncthreads();
+  G.sync(groups);
   double t = lane < nw ? buf[lane] : 0.0;
   t = warp_sum(t);
   t = __shfl_sync(0xffffffffu, t, 0);
@@ -88,8 +112,10 @@ __device__ __forceinline__ double cta_sum(double v, double* buf) {
 
 template <typename T, bool REFINE>
 __global__ void k_batch_pcg(BatchSys S, BatchOut O, const int* __restrict__ order, int count, unsigned* queue,
-                            const BatchParams* __restrict__ prm, int nmax, int zmax) {
-  extern __shared__ __align__(16) unsigned char sm[];
+                            const BatchParams* __restrict__ prm, int nmax, int zmax, int groups) {
+  extern __shared__ __align__(16) unsigned char smem_all[];
+  const Group G(groups);
+  unsigned char* sm = smem_all + (size_t)G.g * round16(batch_smem<T>(nmax, zmax));
   T* sv = reinterpret_cast<T*>(sm);
   unsigned short* sc = reinterpret_cast<unsigned short*>(sm + batch_col_off<T>(zmax));
   int* srp = reinterpret_cast<int*>(sm + batch_rp_off<T>(zmax));
@@ -101,16 +127,19 @@ __global__ void k_batch_pcg(BatchSys S, BatchOut O, const int* __restrict__ orde
   T* vq = reinterpret_cast<T*>(vbase + 3 * vstride);
   T* vj = reinterpret_cast<T*>(vbase + 4 * vstride);  // 1 / a_ii (identity where |a_ii| <= eps)
   T* vs = reinterpret_cast<T*>(vbase + 5 * vstride);  // equilibration scale 1 / max_j |a_ij|
-  __shared__ double red[2][32];
-  __shared__ int s_k;
-  const int tid = threadIdx.x, nt = blockDim.x;
+  __shared__ double reds[kMaxGroups][2][32];
+  __shared__ int s_ks[kMaxGroups];
+  double(*red)[32] = reds[G.g];
+  int& s_k = s_ks[G.g];
+  const int tid = G.t, nt = G.gsz;
   const BatchParams P = *prm;
+  auto gsync = [&]() { G.sync(groups); };
 
   for (;;) {
     if (tid == 0) s_k = (int)atomicAdd(queue, 1u);
-    __syncthreads();
+    gsync();
     const int k = s_k;
-    __syncthreads();
+    gsync();
     if (k >= count) break;
     const int sys = order[k];
     const int r0 = S.sys_row[sys], n = S.sys_row[sys + 1] - r0;
@@ -121,7 +150,7 @@ __global__ void k_batch_pcg(BatchSys S, BatchOut O, const int* __restrict__ orde
       sv[e] = REFINE ? (T)S.v32[k0 + e] : (T)S.v64[k0 + e];
       sc[e] = (unsigned short)S.col[k0 + e];
     }
-    __syncthreads();
+    gsync();
     for (int i = tid; i < n; i += nt) {
       double d = 0.0, mx = 0.0;
       for (int e = srp[i]; e < srp[i + 1]; ++e) {
@@ -132,12 +161,12 @@ __global__ void k_batch_pcg(BatchSys S, BatchOut O, const int* __restrict__ orde
       vj[i] = (T)(fabs(d) <= DBL_EPSILON ? 1.0 : 1.0 / d);
       vs[i] = (T)((mx > DBL_EPSILON && isfinite(mx)) ? 1.0 / mx : 1.0);
     }
-    __syncthreads();
+    gsync();
     int term = CFD_TERM_MAX_ITERATIONS, it_total = 0;
     double e_rel = 0.0;
     int slot = 0;
     auto sum = [&](double v) {
-      const double t = cta_sum(v, red[slot]);
+      const double t = group_sum(v, red[slot], G, groups);
       slot ^= 1;
       return t;
     };
@@ -167,7 +196,7 @@ __global__ void k_batch_pcg(BatchSys S, BatchOut O, const int* __restrict__ orde
         term_out = CFD_TERM_INITIAL_RESIDUAL;
         return 0;
       }
-      __syncthreads();
+      gsync();
       for (int it = 1; it <= max_it; ++it) {
         double pq = 0.0;
         for (int i = tid; i < n; i += nt) {
@@ -211,7 +240,7 @@ __global__ void k_batch_pcg(BatchSys S, BatchOut O, const int* __restrict__ orde
         const T beta = (T)(rz / rho);
         rho = rz;
         for (int i = tid; i < n; i += nt) vp[i] = vr[i] * vj[i] + beta * vp[i];
-        __syncthreads();
+        gsync();
       }
       term_out = CFD_TERM_MAX_ITERATIONS;
       return max_it;
@@ -220,17 +249,17 @@ __global__ void k_batch_pcg(BatchSys S, BatchOut O, const int* __restrict__ orde
     if (!REFINE) {
       // r = b - A x0 in shared memory.
       for (int i = tid; i < n; i += nt) vx[i] = (T)O.x[r0 + i];
-      __syncthreads();
+      gsync();
       for (int i = tid; i < n; i += nt) {
         T s = T(0);
         for (int e = srp[i]; e < srp[i + 1]; ++e) s += sv[e] * vx[sc[e]];
         vr[i] = (T)O.b[r0 + i] - s;
       }
-      __syncthreads();
+      gsync();
       double e0, e;
       it_total = pcg(P.tol_rel, P.max_iter, e0, e, term, true, P.tol_abs);
       e_rel = e0 > 0.0 ? e / e0 : 0.0;
-      __syncthreads();
+      gsync();
       for (int i = tid; i < n; i += nt) O.x[r0 + i] = (double)vx[i];
     } else {
       // Outer FP64 residual and update from global memory, inner FP32 PCG.
@@ -264,21 +293,21 @@ __global__ void k_batch_pcg(BatchSys S, BatchOut O, const int* __restrict__ orde
         }
         if (outer == P.max_outer || it_total >= P.max_iter) break;
         const double scale = 1.0 / rn;
-        __syncthreads();
+        gsync();
         for (int i = tid; i < n; i += nt) {
           double s = 0.0;
           for (int e2i = srp[i]; e2i < srp[i + 1]; ++e2i) s += S.v64[k0 + e2i] * O.x[r0 + sc[e2i]];
           vr[i] = (T)((O.b[r0 + i] - s) * scale);
           vx[i] = T(0);
         }
-        __syncthreads();
+        gsync();
         double ie0, ie;
         int iterm = CFD_TERM_MAX_ITERATIONS;
         const int its = pcg(P.inner_tol, P.max_iter - it_total, ie0, ie, iterm, false, 0.0);
         it_total += its;
-        __syncthreads();
+        gsync();
         for (int i = tid; i < n; i += nt) O.x[r0 + i] += (double)vx[i] / scale;
-        __syncthreads();
+        gsync();
         if (iterm == CFD_TERM_BREAKDOWN || iterm == CFD_TERM_NON_POSITIVE_CURVATURE) {
           term = iterm;
           break;
@@ -290,7 +319,7 @@ __global__ void k_batch_pcg(BatchSys S, BatchOut O, const int* __restrict__ orde
       O.iters[sys] = it_total;
       O.resid[sys] = e_rel;
     }
-    __syncthreads();
+    gsync();
   }
 }
 
@@ -312,13 +341,15 @@ cfd_status dalloc(T** p, int64_t n) {
 }
 
 // Shared-memory size, attribute and persistent grid of bucket k at `threads`.
+// `threads` per system, `groups` systems per CTA.
 template <bool REFINE>
-cfd_status prepare_bucket(cfd_batch* bt, int bkt, int threads, int* grid, size_t* smem_out) {
+cfd_status prepare_bucket(cfd_batch* bt, int bkt, int threads, int groups, int* grid, size_t* smem_out) {
   using T = typename std::conditional<REFINE, float, double>::type;
   const int count = bt->bucket_begin[bkt + 1] - bt->bucket_begin[bkt];
   *grid = 0;
   if (count == 0) return CFD_OK;
-  const size_t smem = batch_smem<T>(bt->bucket_nmax[bkt], bt->bucket_zmax[bkt]);
+  const size_t smem = (size_t)groups * round16(batch_smem<T>(bt->bucket_nmax[bkt], bt->bucket_zmax[bkt]));
+  threads *= groups;
   auto kern = k_batch_pcg<T, REFINE>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
     cudaGetLastError();
@@ -331,31 +362,31 @@ cfd_status prepare_bucket(cfd_batch* bt, int bkt, int threads, int* grid, size_t
     set_error("batch bucket %d: %zu bytes of shared memory at %d threads do not fit", bkt, smem, threads);
     return CFD_ERR_CONFIG;
   }
-  *grid = std::min(count, bt->ctx->num_sms * occ);
+  *grid = std::min((count + groups - 1) / groups, bt->ctx->num_sms * occ);
   *smem_out = smem;
   return CFD_OK;
 }
 
 template <bool REFINE>
-cfd_status launch_bucket(cfd_batch* bt, int bkt, int threads, int grid, size_t smem, cudaStream_t s) {
+cfd_status launch_bucket(cfd_batch* bt, int bkt, int threads, int groups, int grid, size_t smem, cudaStream_t s) {
   using T = typename std::conditional<REFINE, float, double>::type;
   const int count = bt->bucket_begin[bkt + 1] - bt->bucket_begin[bkt];
   if (count == 0 || grid == 0) return CFD_OK;
   BatchSys S{bt->sys_row, bt->rp, bt->col, bt->v64, bt->v32};
   BatchOut O{bt->x, bt->b, bt->term, bt->iters, bt->resid};
-  k_batch_pcg<T, REFINE><<<grid, threads, smem, s>>>(S, O, bt->order + bt->bucket_begin[bkt], count,
-                                                      bt->queues + bkt, bt->params, bt->bucket_nmax[bkt],
-                                                      bt->bucket_zmax[bkt]);
+  k_batch_pcg<T, REFINE><<<grid, threads * groups, smem, s>>>(S, O, bt->order + bt->bucket_begin[bkt], count,
+                                                               bt->queues + bkt, bt->params, bt->bucket_nmax[bkt],
+                                                               bt->bucket_zmax[bkt], groups);
   CFD_TRY_CUDA(cudaGetLastError());
   return CFD_OK;
 }
 
 template <bool REFINE>
-cfd_status run_bucket(cfd_batch* bt, int bkt, int threads, cudaStream_t s) {
+cfd_status run_bucket(cfd_batch* bt, int bkt, int threads, int groups, cudaStream_t s) {
   int grid = 0;
   size_t smem = 0;
-  CFD_TRY(prepare_bucket<REFINE>(bt, bkt, threads, &grid, &smem));
-  return launch_bucket<REFINE>(bt, bkt, threads, grid, smem, s);
+  CFD_TRY(prepare_bucket<REFINE>(bt, bkt, threads, groups, &grid, &smem));
+  return launch_bucket<REFINE>(bt, bkt, threads, groups, grid, smem, s);
 }
 
 // The device part of one batched solve: reset the queues, one persistent
@@ -364,9 +395,9 @@ cfd_status enqueue_solve(cfd_batch* bt, int prec, const int* grid, const size_t*
   CFD_TRY_CUDA(cudaMemsetAsync(bt->queues, 0, kBuckets * sizeof(unsigned), s));
   for (int k = kBuckets - 1; k >= 0; --k) {
     if (prec)
-      CFD_TRY(launch_bucket<true>(bt, k, bt->threads[prec][k], grid[k], smem[k], s));
+      CFD_TRY(launch_bucket<true>(bt, k, bt->threads[prec][k], bt->groups[prec][k], grid[k], smem[k], s));
     else
-      CFD_TRY(launch_bucket<false>(bt, k, bt->threads[prec][k], grid[k], smem[k], s));
+      CFD_TRY(launch_bucket<false>(bt, k, bt->threads[prec][k], bt->groups[prec][k], grid[k], smem[k], s));
   }
   return CFD_OK;
 }
@@ -381,9 +412,25 @@ cfd_status capture_graph(cfd_batch* bt, int prec) {
   size_t smem[kBuckets] = {};
   for (int k = 0; k < kBuckets; ++k) {
     if (prec)
-      CFD_TRY(prepare_bucket<true>(bt, k, bt->threads[prec][k], &grid[k], &smem[k]));
+      CFD_TRY(prepare_bucket<true>(bt, k, bt->threads[prec][k], bt->groups[prec][k], &grid[k], &smem[k]));
     else
-      CFD_TRY(prepare_bucket<false>(bt, k, bt->threads[prec][k], &grid[k], &smem[k]));
+      CFD_TRY(prepare_bucket<false>(bt, k, bt->threads[prec][k], bt->groups[prec][k], &grid[k], &smem[k]));
+  }
+  // The buckets share one kernel per precision: its shared-memory limit must
+  // cover the largest of them (with several systems per CTA a small-row
+  // bucket can need more than a larger one).
+  const size_t smem_max = *std::max_element(smem, smem + kBuckets);
+  if (smem_max > 0) {
+    const cudaError_t ea =
+        prec ? cudaFuncSetAttribute(k_batch_pcg<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_max)
+             : cudaFuncSetAttribute(k_batch_pcg<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_max);
+    if (ea != cudaSuccess) {
+      cudaGetLastError();
+      set_error("batch: %zu bytes of shared memory are not available", smem_max);
+      return CFD_ERR_CONFIG;
+    }
   }
   cudaGraph_t g = nullptr;
   CFD_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -704,29 +751,32 @@ cfd_status cfd_batch_autotune(cfd_batch* bt, int32_t precision, int32_t sample_i
     for (int k = 0; k < kBuckets; ++k) {
       if (bt->bucket_begin[k + 1] == bt->bucket_begin[k]) continue;
       float best = 1e30f;
-      int best_t = bt->threads[precision][k];
-      for (int t : kCandidates) {
-        if (t > 2 * std::max(32, bt->bucket_nmax[k])) continue;
-        float ms_min = 1e30f;
-        for (int rep = 0; rep < 2; ++rep) {
-          CFD_TRY_CUDA(cudaMemsetAsync(bt->x, 0, bt->rows * sizeof(double), s));
-          CFD_TRY_CUDA(cudaMemsetAsync(bt->queues + k, 0, sizeof(unsigned), s));
-          CFD_TRY_CUDA(cudaEventRecord(ctx->ev0, s));
-          cfd_status st = precision ? run_bucket<true>(bt, k, t, s) : run_bucket<false>(bt, k, t, s);
-          if (st == CFD_ERR_CONFIG) break;  // does not fit at this width
-          CFD_TRY(st);
-          CFD_TRY_CUDA(cudaEventRecord(ctx->ev1, s));
-          CFD_TRY_CUDA(cudaStreamSynchronize(s));
-          float ms = 0.f;
-          CFD_TRY_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-          ms_min = std::min(ms_min, ms);
+      int best_t = bt->threads[precision][k], best_g = bt->groups[precision][k];
+      for (int t : kCandidates)
+        for (int gr : kGroupCandidates) {
+          if (t > 2 * std::max(32, bt->bucket_nmax[k]) || (gr > 1 && t * gr > 512)) continue;
+          float ms_min = 1e30f;
+          for (int rep = 0; rep < 2; ++rep) {
+            CFD_TRY_CUDA(cudaMemsetAsync(bt->x, 0, bt->rows * sizeof(double), s));
+            CFD_TRY_CUDA(cudaMemsetAsync(bt->queues + k, 0, sizeof(unsigned), s));
+            CFD_TRY_CUDA(cudaEventRecord(ctx->ev0, s));
+            cfd_status st = precision ? run_bucket<true>(bt, k, t, gr, s) : run_bucket<false>(bt, k, t, gr, s);
+            if (st == CFD_ERR_CONFIG) break;  // does not fit at this width
+            CFD_TRY(st);
+            CFD_TRY_CUDA(cudaEventRecord(ctx->ev1, s));
+            CFD_TRY_CUDA(cudaStreamSynchronize(s));
+            float ms = 0.f;
+            CFD_TRY_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+            ms_min = std::min(ms_min, ms);
+          }
+          if (ms_min < best) {
+            best = ms_min;
+            best_t = t;
+            best_g = gr;
+          }
         }
-        if (ms_min < best) {
-          best = ms_min;
-          best_t = t;
-        }
-      }
       bt->threads[precision][k] = best_t;
+      bt->groups[precision][k] = best_g;
     }
     bt->tuned[precision] = true;
     drop_graphs(bt);
@@ -742,6 +792,35 @@ cfd_status cfd_batch_config(const cfd_batch* bt, int32_t precision, int32_t* buc
     if (threads) threads[k] = bt->threads[precision][k];
     if (systems) systems[k] = bt->bucket_begin[k + 1] - bt->bucket_begin[k];
   }
+  return CFD_OK;
+}
+
+cfd_status cfd_batch_set_config(cfd_batch* bt, int32_t precision, const int32_t* threads, const int32_t* groups) {
+  return guarded("cfd_batch_set_config", [&]() -> cfd_status {
+    if (!bt || precision < 0 || precision > 1 || !threads || !groups) return CFD_ERR_CONFIG;
+    for (int k = 0; k < kBuckets; ++k) {
+      const bool tok = std::find(std::begin(kCandidates), std::end(kCandidates), threads[k]) != std::end(kCandidates);
+      const bool gok = std::find(std::begin(kGroupCandidates), std::end(kGroupCandidates), groups[k]) !=
+                       std::end(kGroupCandidates);
+      if (!tok || !gok || threads[k] * groups[k] > 1024) {
+        set_error("cfd_batch_set_config: bucket %d: %d threads per system x %d systems per CTA is not a candidate",
+                  k, threads[k], groups[k]);
+        return CFD_ERR_CONFIG;
+      }
+    }
+    std::lock_guard<std::mutex> g(bt->ctx->mu);
+    for (int k = 0; k < kBuckets; ++k) {
+      bt->threads[precision][k] = threads[k];
+      bt->groups[precision][k] = groups[k];
+    }
+    drop_graphs(bt);
+    return CFD_OK;
+  });
+}
+
+cfd_status cfd_batch_groups(const cfd_batch* bt, int32_t precision, int32_t* groups) {
+  if (!bt || precision < 0 || precision > 1 || !groups) return CFD_ERR_STATE;
+  for (int k = 0; k < kBuckets; ++k) groups[k] = bt->groups[precision][k];
   return CFD_OK;
 }
 

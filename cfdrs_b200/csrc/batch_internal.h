@@ -53,7 +53,8 @@ struct cfd_batch {
   int* order = nullptr;  // systems of each bucket, largest first, bucket after bucket
   int bucket_begin[cfd::kBuckets + 1] = {};
   int bucket_nmax[cfd::kBuckets] = {}, bucket_zmax[cfd::kBuckets] = {};
-  int threads[2][cfd::kBuckets] = {{32, 64, 128, 256}, {32, 64, 128, 256}};  // [precision][bucket]
+  int threads[2][cfd::kBuckets] = {{32, 64, 128, 256}, {32, 64, 128, 256}};  // [precision][bucket], per system
+  int groups[2][cfd::kBuckets] = {{1, 1, 1, 1}, {1, 1, 1, 1}};  // systems per CTA of the Jacobi-PCG kernel
   bool tuned[2] = {false, false};
   unsigned* queues = nullptr;  // one ticket per bucket
   cfd::BatchParams* params = nullptr;

@@ -971,6 +971,26 @@ struct DiaXPlain {
   __device__ void store1(int, VT) const {}
 };
 
+// Asks the bulk-copy engine to bring the next span of each diagonal (and of
+// the lane masks) into L2 while this span's loads are served: one thread per
+// stream, in-bounds sizes only (the arrays are ld long; ld and span are
+// multiples of 16 bytes' worth of entries).
+template <typename VT, int TPR>
+__device__ __forceinline__ void dia_prefetch_next(const DiaView<VT>& D, int64_t s0, int64_t span) {
+  const int64_t sn = s0 + (int64_t)gridDim.x * span;
+  const int t = threadIdx.x;
+  if (sn >= D.nrows || t > D.n) return;
+  const int64_t cnt = min(span, D.ld - sn);
+  if (t < D.n) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(D.val + (int64_t)t * D.ld + sn),
+                 "r"((unsigned)(cnt * (int64_t)sizeof(VT)))
+                 : "memory");
+  } else if (TPR > 1) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(D.mask + sn), "r"((unsigned)(cnt * 4))
+                 : "memory");
+  }
+}
+
 template <typename VT, bool OFFDIAG, int NS>
 __device__ __forceinline__ void dia_sum(const VT (&v)[NS], const VT (&xv)[NS], int nd, int main, VT& sum,
                                         VT& diag) {
@@ -1001,6 +1021,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, XS xs, Epi
   const int omin = D.off[0], omax = D.off[nd - 1];
   const int lane = threadIdx.x & 31;
   for (int64_t s0 = (int64_t)blockIdx.x * span; s0 < D.nrows; s0 += (int64_t)gridDim.x * span) {
+    dia_prefetch_next<VT, 1>(D, s0, span);
     const bool interior = s0 + omin >= 0 && s0 + span + omax <= D.nrows && s0 + span <= D.nrows;
     typename Epi::Pre pre[V];
     VT v[V][NS], xv[V][NS];
@@ -1177,6 +1198,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia_gen(DiaView<VT> D, XS xs,
   const int64_t span = (int64_t)kThreads * V;
   const int omin = D.off[0], omax = D.off[nd - 1];
   for (int64_t s0 = (int64_t)blockIdx.x * span; s0 < D.nrows; s0 += (int64_t)gridDim.x * span) {
+    dia_prefetch_next<VT, TPR>(D, s0, span);
     const bool interior = s0 + omin >= 0 && s0 + span + omax <= D.nrows && s0 + span <= D.nrows;
     typename Epi::Pre pre[V];
     VT s[V][TPR], diag[V];

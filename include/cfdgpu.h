@@ -472,12 +472,22 @@ typedef struct {
 void cfd_ls_options_default(cfd_ls_options* opt);
 cfd_status cfd_batch_linear_system_solve(cfd_batch* batch, const cfd_ls_options* opt, const double* b, double* x,
                                          cfd_ls_result* results, cfd_batch_report* rep);
-/* Time each CTA width (32..512 threads) per size bucket on this batch with a
- * fixed iteration budget and keep the fastest (per precision). */
+/* Time each pair (threads per system 32..512, systems per CTA 1, 2 or 4) per
+ * size bucket on this batch with a fixed iteration budget and keep the fastest
+ * (per precision). Several systems per CTA each run on their own named barrier
+ * (a warp-wide one for 32-thread systems). */
 cfd_status cfd_batch_autotune(cfd_batch* batch, int32_t precision, int32_t sample_iterations);
-/* Bucket row limits, chosen CTA widths and systems per bucket (4 entries each). */
+/* Bucket row limits, chosen threads per system and systems per bucket (4
+ * entries each). */
 cfd_status cfd_batch_config(const cfd_batch* batch, int32_t precision, int32_t* bucket_rows,
                             int32_t* threads, int32_t* systems);
+/* Chosen systems per CTA of the Jacobi-PCG kernel per bucket (4 entries). */
+cfd_status cfd_batch_groups(const cfd_batch* batch, int32_t precision, int32_t* groups);
+/* Set threads per system (32, 64, 128, 256 or 512) and systems per CTA (1, 2
+ * or 4; at most 1024 threads per CTA) per bucket, in place of the autotuner's
+ * choice. A bucket whose shared memory does not fit at that choice fails at
+ * the next solve with CFD_ERR_CONFIG. */
+cfd_status cfd_batch_set_config(cfd_batch* batch, int32_t precision, const int32_t* threads, const int32_t* groups);
 cfd_status cfd_batch_destroy(cfd_batch* batch);
 
 /* ---- network assembly on the device --------------------------------------

@@ -36,7 +36,7 @@ def test_sparse_solve_gradients(cuda):
     A, b = P.darcy_2d(theta)
     s = SparseSolver(A, preconditioner="jacobi", precision=cf.Precision.FP64,
                      config=cf.IterativeSolverConfig(0.0, 1e-13, 5000))
-    vals = torch.as_tensor(A.val, device="cuda").requires_grad_(True)
+    vals = torch.as_tensor(np.array(A.val), device="cuda").requires_grad_(True)
     bt = torch.as_tensor(b, device="cuda").requires_grad_(True)
     w = torch.as_tensor(np.random.default_rng(2).standard_normal(A.nrows), device="cuda")
     x = sparse_solve(vals, bt, s)

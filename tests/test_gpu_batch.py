@@ -73,6 +73,7 @@ def test_batch_autotune_and_initial_guess(batch):
     nb, mats, b = batch
     cfg = nb.autotune(cf.Precision.FP64, sample_iterations=32)
     assert all(t in (32, 64, 128, 256, 512) for t in cfg["threads"])
+    assert all(g in (1, 2, 4) for g in cfg["systems_per_cta"])
     assert sum(cfg["systems"]) == len(mats)
     x, rep = nb.solve(b, config=cf.IterativeSolverConfig(0.0, 1e-10, 20000))
     assert rep.converged_systems == rep.num_systems
@@ -100,3 +101,42 @@ def test_batch_rejects_oversized_system(cuda):
     from cfdrs_b200 import _lib
     with pytest.raises(_lib.CfdError, match="at most"):
         NetworkBatch([A])
+
+
+@pytest.mark.parametrize("precision", ["FP64", "FP32_REFINE"])
+def test_batch_systems_per_cta_bit_identical(batch, precision):
+    """Several systems per CTA (each on its own named barrier, or the warp
+    barrier at 32 threads) give the results of one system per CTA at the same
+    threads per system bit for bit."""
+    import cfdrs_b200 as cf
+    nb, mats, b = batch
+    prec = cf.Precision[precision]
+    cfg = cf.IterativeSolverConfig(0.0, 1e-10, 40000)
+    saved = nb.config(prec)
+    try:
+        for thr in ([32, 32, 32, 32], [64, 64, 128, 128]):
+            nb.set_config(thr, [1, 1, 1, 1], prec)
+            x1, r1 = nb.solve(b, config=cfg, precision=prec)
+            # the two large buckets' systems take more than half the shared
+            # memory of an SM in FP64, so they stay at one per CTA
+            for grp in ([2, 2, 1, 1], [4, 4, 1, 1], [2, 4, 2, 1]) if precision == "FP32_REFINE" else \
+                    ([2, 2, 1, 1], [4, 4, 1, 1]):
+                nb.set_config(thr, grp, prec)
+                xg, rg = nb.solve(b, config=cfg, precision=prec)
+                assert np.array_equal(x1.view(np.int64), xg.view(np.int64)), (thr, grp)
+                assert np.array_equal(r1.iterations, rg.iterations)
+                assert rg.converged_systems == rg.num_systems
+    finally:
+        nb.set_config(saved["threads"], saved["systems_per_cta"], prec)
+
+
+def test_batch_set_config_rejects_bad_widths(batch):
+    import cfdrs_b200 as cf
+    from cfdrs_b200 import _lib
+    nb, _, _ = batch
+    with pytest.raises(_lib.CfdError):
+        nb.set_config([48, 64, 64, 64], [1, 1, 1, 1])
+    with pytest.raises(_lib.CfdError):
+        nb.set_config([512, 64, 64, 64], [4, 1, 1, 1])
+    with pytest.raises(_lib.CfdError):
+        nb.set_config([64, 64, 64, 64], [3, 1, 1, 1])
