@@ -175,6 +175,31 @@ struct EpiStore {
   __device__ void finish(const double*) const {}
 };
 
+// y = A x, and x0 = the first damped-Jacobi sweep from zero on y (w y / a_ii,
+// smooth0_value) for the level whose right-hand side y is: the restriction
+// hands the coarse level its pre-smoothed start, so that level needs no
+// separate pass over b. Bit for bit what the separate pass computes.
+template <typename XT>
+struct EpiStoreSmooth {
+  static constexpr int NRED = 0;
+  using Pre = XT;  // a_ii of the row of y
+  XT* __restrict__ y;
+  XT* __restrict__ x0;
+  const XT* __restrict__ d;
+  XT omega;
+  const int* done;
+  Red red;
+  __device__ bool skip() const { return flag_set(done); }
+  __device__ Pre load(int i) const { return d[i]; }
+  template <typename S>
+  __device__ void row(int i, S s, S, const Pre& di, double*) const {
+    const XT yi = (XT)s;
+    y[i] = yi;
+    x0[i] = smooth0_value<XT>(yi, di, omega);
+  }
+  __device__ void finish(const double*) const {}
+};
+
 // y = base + A x (prolongation with correction, amg.rs:475-489; y may alias base)
 template <typename XT>
 struct EpiAddTo {
@@ -971,26 +996,6 @@ struct DiaXPlain {
   __device__ void store1(int, VT) const {}
 };
 
-// Asks the bulk-copy engine to bring the next span of each diagonal (and of
-// the lane masks) into L2 while this span's loads are served: one thread per
-// stream, in-bounds sizes only (the arrays are ld long; ld and span are
-// multiples of 16 bytes' worth of entries).
-template <typename VT, int TPR>
-__device__ __forceinline__ void dia_prefetch_next(const DiaView<VT>& D, int64_t s0, int64_t span) {
-  const int64_t sn = s0 + (int64_t)gridDim.x * span;
-  const int t = threadIdx.x;
-  if (sn >= D.nrows || t > D.n) return;
-  const int64_t cnt = min(span, D.ld - sn);
-  if (t < D.n) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(D.val + (int64_t)t * D.ld + sn),
-                 "r"((unsigned)(cnt * (int64_t)sizeof(VT)))
-                 : "memory");
-  } else if (TPR > 1) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(D.mask + sn), "r"((unsigned)(cnt * 4))
-                 : "memory");
-  }
-}
-
 template <typename VT, bool OFFDIAG, int NS>
 __device__ __forceinline__ void dia_sum(const VT (&v)[NS], const VT (&xv)[NS], int nd, int main, VT& sum,
                                         VT& diag) {
@@ -1021,7 +1026,6 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, XS xs, Epi
   const int omin = D.off[0], omax = D.off[nd - 1];
   const int lane = threadIdx.x & 31;
   for (int64_t s0 = (int64_t)blockIdx.x * span; s0 < D.nrows; s0 += (int64_t)gridDim.x * span) {
-    dia_prefetch_next<VT, 1>(D, s0, span);
     const bool interior = s0 + omin >= 0 && s0 + span + omax <= D.nrows && s0 + span <= D.nrows;
     typename Epi::Pre pre[V];
     VT v[V][NS], xv[V][NS];
@@ -1198,7 +1202,6 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia_gen(DiaView<VT> D, XS xs,
   const int64_t span = (int64_t)kThreads * V;
   const int omin = D.off[0], omax = D.off[nd - 1];
   for (int64_t s0 = (int64_t)blockIdx.x * span; s0 < D.nrows; s0 += (int64_t)gridDim.x * span) {
-    dia_prefetch_next<VT, TPR>(D, s0, span);
     const bool interior = s0 + omin >= 0 && s0 + span + omax <= D.nrows && s0 + span <= D.nrows;
     typename Epi::Pre pre[V];
     VT s[V][TPR], diag[V];

@@ -91,10 +91,13 @@ __global__ void __launch_bounds__(kThreads) k_dense_gemv(int n, const double* __
 // PCG: x += alpha p; r -= alpha q; ||r||; with Jacobi also rho_new = r.(D^-1 r).
 // The last CTA applies the termination tests (converged / non-finite / budget)
 // and, for Jacobi or no preconditioner, beta = rho_new / rho.
+// With AMG, x0 != NULL also writes the V-cycle's first pre-smoothing sweep on
+// the new r (x0 = w r / a_ii, smooth0_value with the fine level's diagonal d0).
 template <typename XT, int PRE>
 __global__ void __launch_bounds__(kThreads) k_cg_update(int64_t n, XT* __restrict__ x, const XT* __restrict__ p,
                                                         XT* __restrict__ r, const XT* __restrict__ q,
-                                                        const XT* __restrict__ jinv, DevState* st, Red red) {
+                                                        const XT* __restrict__ jinv, DevState* st, Red red,
+                                                        XT* __restrict__ x0, const XT* __restrict__ d0, XT omega) {
   if (st->done) return;
   const XT a = (XT)st->alpha;
   double acc[2] = {0.0, 0.0};
@@ -104,6 +107,7 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(int64_t n, XT* __restric
     r[i] = ri;
     acc[0] += (double)ri * (double)ri;
     if (PRE == kPreJacobi) acc[1] += (double)ri * (double)(ri * jinv[i]);
+    if (PRE == kPreAmg && x0) x0[i] = smooth0_value<XT>(ri, d0[i], omega);
   })
   double tot[2];
   if (grid_reduce<2>(acc, red, tot) && threadIdx.x == 0) {
@@ -841,9 +845,18 @@ static cfd_status jacobi_sweep(Launcher& lc, const DevLevel& L, const XT* xo, XT
   }
 }
 
+// Whether level l's first pre-smoothing sweep can be written by the kernel
+// that produces its right-hand side (into the level's vecs().xa).
+template <typename XT>
+static bool smooth0_fusable(const cfd_amg* amg, size_t l) {
+  return l + 1 < amg->dev.size() && amg->cfg.pre_smooth >= 1;
+}
+
+// x0_ready: the producer of b already wrote the first pre-smoothing sweep
+// (smooth0_value) into this level's vecs().xa.
 template <typename XT>
 static cfd_status vcycle(Launcher& lc, cfd_amg* amg, size_t l, const XT* b, XT* out, int dot, DevState* st,
-                         const int* done) {
+                         const int* done, bool x0_ready = false) {
   DevLevel& L = amg->dev[l];
   LevelVecs<XT>& V = vecs<XT>(L);
   const int64_t n = L.A.nrows;
@@ -882,7 +895,7 @@ static cfd_status vcycle(Launcher& lc, cfd_amg* amg, size_t l, const XT* b, XT* 
   XT* x = V.xa;
   XT* y = V.xb;
   if (c.pre_smooth >= 1) {
-    CFD_TRY(lc.vec(n, k_smooth0<XT>, b, diag_of<XT>(L), omega, x, done));
+    if (!x0_ready) CFD_TRY(lc.vec(n, k_smooth0<XT>, b, diag_of<XT>(L), omega, x, done));
     for (int s = 1; s < c.pre_smooth; ++s) {
       CFD_TRY(jacobi_sweep<XT>(lc, L, x, y, b, omega, 0, st, done));
       std::swap(x, y);
@@ -895,9 +908,14 @@ static cfd_status vcycle(Launcher& lc, cfd_amg* amg, size_t l, const XT* b, XT* 
   // 3. restriction to the next level's right-hand side
   DevLevel& Lc = amg->dev[l + 1];
   LevelVecs<XT>& Vc = vecs<XT>(Lc);
-  CFD_TRY(lc.spmv<XT, XT, false>(L.R, V.r, EpiStore<XT>{Vc.b, done, {}}));
+  const bool fuse = smooth0_fusable<XT>(amg, l + 1);
+  if (fuse)
+    CFD_TRY(lc.spmv<XT, XT, false>(L.R, V.r,
+                                   EpiStoreSmooth<XT>{Vc.b, Vc.xa, diag_of<XT>(Lc), omega, done, {}}));
+  else
+    CFD_TRY(lc.spmv<XT, XT, false>(L.R, V.r, EpiStore<XT>{Vc.b, done, {}}));
   // 4. coarse solve from zero
-  CFD_TRY(vcycle<XT>(lc, amg, l + 1, Vc.b, Vc.e, 0, st, done));
+  CFD_TRY(vcycle<XT>(lc, amg, l + 1, Vc.b, Vc.e, 0, st, done, fuse));
   // 5-6. x += P e_c
   CFD_TRY(lc.spmv<XT, XT, false>(L.P, Vc.e, EpiAddTo<XT>{x, x, done, {}}));
   // 7. post-smoothing
@@ -997,11 +1015,21 @@ static cfd_status pcg_loop(Launcher& lc, cfd_csr* a, cfd_amg* amg, KrylovBufs<XT
   const int64_t max_launch = std::max<int64_t>(1, st ? (int64_t)1 << 40 : 1);
   (void)max_launch;
   int64_t launched = 0;
+  // the V-cycle's first sweep on the fine level comes from k_cg_update
+  XT* x0 = nullptr;
+  const XT* d0 = nullptr;
+  XT omega = XT(0);
+  if (PRE == kPreAmg && smooth0_fusable<XT>(amg, 0)) {
+    x0 = vecs<XT>(amg->dev[0]).xa;
+    d0 = diag_of<XT>(amg->dev[0]);
+    omega = (XT)amg->cfg.relaxation;
+  }
   for (;;) {
     for (int k = 0; k < pl.chunk; ++k) {
       CFD_TRY(lc.spmv<XT, XT, false>(a->dev, B.p, EpiCgDot<XT>{B.q, B.p, st, {}}));
-      CFD_TRY(lc.vec(n, k_cg_update<XT, PRE>, B.x, (const XT*)B.p, B.r, (const XT*)B.q, jinv, st, lc.red()));
-      if (PRE == kPreAmg) CFD_TRY(vcycle<XT>(lc, amg, 0, B.r, B.z, 2, st, done));
+      CFD_TRY(lc.vec(n, k_cg_update<XT, PRE>, B.x, (const XT*)B.p, B.r, (const XT*)B.q, jinv, st, lc.red(), x0,
+                     d0, omega));
+      if (PRE == kPreAmg) CFD_TRY(vcycle<XT>(lc, amg, 0, B.r, B.z, 2, st, done, x0 != nullptr));
       CFD_TRY(lc.vec(n, k_p_update<XT, PRE>, B.p, (const XT*)B.r, (const XT*)B.z, jinv, (const DevState*)st));
       ++launched;
     }
