@@ -981,6 +981,29 @@ struct DiaVec<double> {
   }
 };
 
+// N consecutive entries by one vector load (N * sizeof(VT) = 8 or 16 bytes).
+template <typename VT, int N>
+struct DiaVecN;
+template <>
+struct DiaVecN<float, 4> : DiaVec<float> {};
+template <>
+struct DiaVecN<double, 2> : DiaVec<double> {};
+template <typename VT>
+struct DiaVecN<VT, 1> {
+  using type = VT;
+  static constexpr int V = 1;
+  __device__ static void unpack(const VT& a, VT (&o)[1]) { o[0] = a; }
+};
+template <>
+struct DiaVecN<float, 2> {
+  using type = float2;
+  static constexpr int V = 2;
+  __device__ static void unpack(const float2& a, float (&o)[2]) {
+    o[0] = a.x;
+    o[1] = a.y;
+  }
+};
+
 // x operand of the diagonal kernels (a stored vector; the kernels take it as
 // a source object so a fused producer of x can take its place).
 template <typename VT>
@@ -991,6 +1014,11 @@ struct DiaXPlain {
   __device__ VT one(int j) const { return __ldg(x + j); }
   __device__ void vec(int j, VT (&o)[Vec::V]) const {
     Vec::unpack(__ldg(reinterpret_cast<const typename Vec::type*>(x + j)), o);
+  }
+  template <int N>
+  __device__ void vecn(int j, VT (&o)[N]) const {
+    using W = DiaVecN<VT, N>;
+    W::unpack(__ldg(reinterpret_cast<const typename W::type*>(x + j)), o);
   }
   __device__ void store(int, const VT (&)[Vec::V]) const {}
   __device__ void store1(int, VT) const {}
@@ -1185,16 +1213,16 @@ __device__ __forceinline__ void dia_add(VT v, VT xv, int d, int main, uint32_t l
 // Any number of diagonals up to kDiaMax: the diagonals are streamed in order,
 // each adding into the rows' partial sums (unrolled by eight so the loads of
 // several diagonals are in flight). Interior spans with aligned x: V
-// consecutive rows per thread, one 16-byte value load per diagonal, x by one
-// 16-byte load where the offset is a multiple of V and entry by entry
-// otherwise (lanes 16 bytes apart: the entries of four loads share their
-// cache lines). Other spans: V rows kThreads apart, predicated loads.
-template <typename VT, bool OFFDIAG, class Epi, int TPR, class XS>
+// consecutive rows per thread (V = 2: 32 registers, eight CTAs per SM), one
+// V-entry vector load of values per diagonal, x by one vector load where the
+// offset is a multiple of V and entry by entry otherwise (the entries of a
+// warp's loads share their cache lines). Other spans: V rows kThreads apart,
+// predicated loads.
+template <typename VT, bool OFFDIAG, class Epi, int TPR, class XS, int V>
 __global__ void __launch_bounds__(kThreads) k_spmv_dia_gen(DiaView<VT> D, XS xs, Epi epi) {
   static_assert(TPR == 1 || TPR == 2, "row groups of one or two threads");
   if (epi.skip()) return;
-  using Vec = DiaVec<VT>;
-  constexpr int V = Vec::V;
+  using Vec = DiaVecN<VT, V>;
   double red[Epi::NRED > 0 ? Epi::NRED : 1];
 #pragma unroll
   for (int q = 0; q < (Epi::NRED > 0 ? Epi::NRED : 1); ++q) red[q] = 0.0;
@@ -1226,7 +1254,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_dia_gen(DiaView<VT> D, XS xs,
         VT vd[V], xd[V];
         Vec::unpack(__ldcs(reinterpret_cast<const typename Vec::type*>(D.val + (int64_t)d * D.ld + r0)), vd);
         if ((o & (V - 1)) == 0) {
-          xs.vec(r0 + o, xd);
+          xs.template vecn<V>(r0 + o, xd);
         } else {
 #pragma unroll
           for (int q = 0; q < V; ++q) xd[q] = xs.one(r0 + o + q);

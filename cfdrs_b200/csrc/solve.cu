@@ -627,6 +627,10 @@ struct Launcher {
     m.dia_stale = false;
     return CFD_OK;
   }
+  // Rows per thread of the streaming diagonal kernel: FP32 two (8-byte value
+  // loads, half the scalar x loads of four rows per thread), FP64 two.
+  template <typename VT>
+  static constexpr int kDiaGenRows = 2;
   template <typename VT, bool OFF, class Epi>
   cfd_status dia_launch(const DevMat& m, const VT* x, Epi epi) {
     return dia_launch_xs<VT, OFF, Epi>(m, DiaXPlain<VT>{x}, ((uintptr_t)x & 15) == 0, epi);
@@ -634,13 +638,17 @@ struct Launcher {
   // xvec: every array the x source reads (and stores) is 16-byte aligned.
   template <typename VT, bool OFF, class Epi, class XS>
   cfd_status dia_launch_xs(const DevMat& m, XS xs, bool xvec, Epi epi) {
-    if (m.tpr == 1 && m.dia_n == 7) return dia_launch_k<VT, Epi>(m, k_spmv_dia<VT, OFF, Epi, 7, XS>, xs, xvec, epi);
-    if (m.tpr == 1 && m.dia_n == 5) return dia_launch_k<VT, Epi>(m, k_spmv_dia<VT, OFF, Epi, 5, XS>, xs, xvec, epi);
-    if (m.tpr == 1) return dia_launch_k<VT, Epi>(m, k_spmv_dia_gen<VT, OFF, Epi, 1, XS>, xs, xvec, epi);
-    return dia_launch_k<VT, Epi>(m, k_spmv_dia_gen<VT, OFF, Epi, 2, XS>, xs, xvec, epi);
+    constexpr int V = DiaVec<VT>::V, VG = kDiaGenRows<VT>;
+    if (m.tpr == 1 && m.dia_n == 7)
+      return dia_launch_k<VT, Epi, V>(m, k_spmv_dia<VT, OFF, Epi, 7, XS>, xs, xvec, epi);
+    if (m.tpr == 1 && m.dia_n == 5)
+      return dia_launch_k<VT, Epi, V>(m, k_spmv_dia<VT, OFF, Epi, 5, XS>, xs, xvec, epi);
+    if (m.tpr == 1) return dia_launch_k<VT, Epi, VG>(m, k_spmv_dia_gen<VT, OFF, Epi, 1, XS, VG>, xs, xvec, epi);
+    return dia_launch_k<VT, Epi, VG>(m, k_spmv_dia_gen<VT, OFF, Epi, 2, XS, VG>, xs, xvec, epi);
   }
-  // One launch of a diagonal kernel (its occupancy looked up once per device).
-  template <typename VT, class Epi, class XS>
+  // One launch of a diagonal kernel of V rows per thread and span (its
+  // occupancy looked up once per device).
+  template <typename VT, class Epi, int V, class XS>
   cfd_status dia_launch_k(const DevMat& m, void (*kern)(DiaView<VT>, XS, Epi), XS xs, bool xvec, Epi epi) {
     CFD_TRY(dia_refresh(m));
     static std::mutex occ_mu;
@@ -659,7 +667,7 @@ struct Launcher {
       }
       occ = o;
     }
-    const int64_t span = (int64_t)kThreads * DiaVec<VT>::V;
+    const int64_t span = (int64_t)kThreads * V;
     const int64_t spans = (m.nrows + span - 1) / span;
     // at most one reduction slot per CTA (the context's partials)
     const int grid = (int)std::max<int64_t>(
