@@ -152,6 +152,16 @@ __device__ __forceinline__ XT smooth0_value(XT b, XT d, XT omega) {
   return diag_ok<XT>(d) ? omega * sweep_div<XT>(b, d) : XT(0);
 }
 
+// Programmatic dependent launch. The solve's kernels are launched with
+// programmatic stream serialization, so the next kernel of the stream can be
+// scheduled while this one drains. Every such kernel first waits for the
+// stream's preceding grid to complete and its memory to be visible
+// (griddepcontrol.wait; it returns at once for a launch without the
+// attribute), then lets its own successor be scheduled.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Epilogues. load(i) fetches the row's own operands (issued before the x
 // gathers so the latencies overlap); row(i, sum, diag, pre, acc) finishes it.
@@ -583,6 +593,7 @@ struct PipeLayout {
 template <typename VT, typename XT, bool OFFDIAG, class Epi, bool CODES>
 __global__ void __launch_bounds__(kPipeThreads, PipeLayout<VT, CODES>::kMinBlocks) k_spmv_pipe(MatView<VT> A, int nblk, const XT* __restrict__ x,
                                                                 Epi epi, int* err) {
+  pdl_enter();
   if (epi.skip()) return;
   using L = PipeLayout<VT, CODES>;
   constexpr int kStages = L::kStages;
@@ -860,6 +871,7 @@ constexpr int kSlBatch = 8;
 
 template <typename XT, bool OFFDIAG, class Epi>
 __global__ void __launch_bounds__(kThreads) k_spmv_sl(SlView S, const XT* __restrict__ x, Epi epi) {
+  pdl_enter();
   if (epi.skip()) return;
   __shared__ int sdict[256];
   double red[Epi::NRED > 0 ? Epi::NRED : 1];
@@ -1041,6 +1053,7 @@ __device__ __forceinline__ void dia_sum(const VT (&v)[NS], const VT (&xv)[NS], i
 
 template <typename VT, bool OFFDIAG, class Epi, int ND, class XS>
 __global__ void __launch_bounds__(kThreads) k_spmv_dia(DiaView<VT> D, XS xs, Epi epi) {
+  pdl_enter();
   static_assert(ND > 0 && ND <= 8, "k_spmv_dia holds every diagonal of a row in registers");
   if (epi.skip()) return;
   using Vec = DiaVec<VT>;
@@ -1220,6 +1233,7 @@ __device__ __forceinline__ void dia_add(VT v, VT xv, int d, int main, uint32_t l
 // predicated loads.
 template <typename VT, bool OFFDIAG, class Epi, int TPR, class XS, int V>
 __global__ void __launch_bounds__(kThreads) k_spmv_dia_gen(DiaView<VT> D, XS xs, Epi epi) {
+  pdl_enter();
   static_assert(TPR == 1 || TPR == 2, "row groups of one or two threads");
   if (epi.skip()) return;
   using Vec = DiaVecN<VT, V>;
@@ -1415,6 +1429,7 @@ __device__ __forceinline__ void rows_from_stage_xs(const Epi& epi, const uint16_
 template <typename VT, bool OFFDIAG, class Epi>
 __global__ void __launch_bounds__(kXsThreads, 1) k_spmv_xs(MatView<VT> A, XsView X, int nblk,
                                                             const VT* __restrict__ x, Epi epi, int* err) {
+  pdl_enter();
   if (epi.skip()) return;
   using L = XsLayout<VT>;
   constexpr int kStages = L::kStages;

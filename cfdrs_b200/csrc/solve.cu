@@ -55,6 +55,7 @@ inline int vec_grid(int64_t n) {
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_smooth0(int64_t n, const XT* __restrict__ b, const XT* __restrict__ d,
                                                       XT omega, XT* __restrict__ x, const int* done) {
+  pdl_enter();
   if (flag_set(done)) return;
   GRID_STRIDE_U4(i, n, {
     x[i] = smooth0_value<XT>(b[i], d[i], omega);
@@ -63,12 +64,14 @@ __global__ void __launch_bounds__(kThreads) k_smooth0(int64_t n, const XT* __res
 
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_fill(int64_t n, XT* __restrict__ x, XT v, const int* done) {
+  pdl_enter();
   if (flag_set(done)) return;
   GRID_STRIDE_U4(i, n, x[i] = v;)
 }
 
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_copy(int64_t n, const XT* __restrict__ s, XT* __restrict__ d, const int* done) {
+  pdl_enter();
   if (flag_set(done)) return;
   GRID_STRIDE_U4(i, n, d[i] = s[i];)
 }
@@ -77,6 +80,7 @@ __global__ void __launch_bounds__(kThreads) k_copy(int64_t n, const XT* __restri
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_dense_gemv(int n, const double* __restrict__ inv, const XT* __restrict__ b,
                                                          XT* __restrict__ x, const int* done) {
+  pdl_enter();
   if (flag_set(done)) return;
   const int lane = threadIdx.x & 31;
   const int row = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
@@ -98,6 +102,7 @@ __global__ void __launch_bounds__(kThreads) k_cg_update(int64_t n, XT* __restric
                                                         XT* __restrict__ r, const XT* __restrict__ q,
                                                         const XT* __restrict__ jinv, DevState* st, Red red,
                                                         XT* __restrict__ x0, const XT* __restrict__ d0, XT omega) {
+  pdl_enter();
   if (st->done) return;
   const XT a = (XT)st->alpha;
   double acc[2] = {0.0, 0.0};
@@ -137,6 +142,7 @@ template <typename XT, int PRE>
 __global__ void __launch_bounds__(kThreads) k_pcg_init(int64_t n, XT* __restrict__ p, const XT* __restrict__ r,
                                                        const XT* __restrict__ z, const XT* __restrict__ jinv,
                                                        DevState* st, Red red) {
+  pdl_enter();
   if (st->done) return;
   double acc[1] = {0.0};
   GRID_STRIDE_U4(i, n, {
@@ -154,6 +160,7 @@ template <typename XT, int PRE>
 __global__ void __launch_bounds__(kThreads) k_p_update(int64_t n, XT* __restrict__ p, const XT* __restrict__ r,
                                                        const XT* __restrict__ z, const XT* __restrict__ jinv,
                                                        const DevState* st) {
+  pdl_enter();
   if (st->done) return;
   const XT beta = (XT)st->beta;
   GRID_STRIDE_U4(i, n, {
@@ -166,6 +173,7 @@ __global__ void __launch_bounds__(kThreads) k_p_update(int64_t n, XT* __restrict
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_rz(int64_t n, const XT* __restrict__ r, const XT* __restrict__ z,
                                                  DevState* st, int mode, Red red) {
+  pdl_enter();
   if (st->done) return;
   double acc[1] = {0.0};
   GRID_STRIDE_U4(i, n, acc[0] += (double)r[i] * (double)z[i];)
@@ -183,6 +191,7 @@ __global__ void __launch_bounds__(kThreads) k_rz(int64_t n, const XT* __restrict
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_bicg_rho(int64_t n, const XT* __restrict__ rhat, const XT* __restrict__ r,
                                                        DevState* st, Red red) {
+  pdl_enter();
   if (st->done) return;
   double acc[1] = {0.0};
   GRID_STRIDE_U4(i, n, acc[0] += (double)rhat[i] * (double)r[i];)
@@ -204,6 +213,7 @@ template <typename XT, int PRE>
 __global__ void __launch_bounds__(kThreads) k_bicg_p(int64_t n, XT* __restrict__ p, XT* __restrict__ ph,
                                                      const XT* __restrict__ r, const XT* __restrict__ v,
                                                      const XT* __restrict__ jinv, const DevState* st, int first) {
+  pdl_enter();
   if (st->done) return;
   const XT beta = (XT)st->beta, om = (XT)st->omega;
   GRID_STRIDE_U4(i, n, {
@@ -220,6 +230,7 @@ template <typename XT, int PRE>
 __global__ void __launch_bounds__(kThreads) k_bicg_s(int64_t n, XT* __restrict__ s, XT* __restrict__ sh,
                                                      const XT* __restrict__ r, const XT* __restrict__ v,
                                                      const XT* __restrict__ jinv, DevState* st, Red red) {
+  pdl_enter();
   if (st->done) return;
   const XT a = (XT)st->alpha;
   double acc[1] = {0.0};
@@ -249,6 +260,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_x(int64_t n, XT* __restrict__
                                                      const XT* __restrict__ ph, const XT* __restrict__ sh,
                                                      const XT* __restrict__ s, const XT* __restrict__ t,
                                                      DevState* st, Red red) {
+  pdl_enter();
   if (st->done) return;
   const XT a = (XT)st->alpha, om = (XT)st->omega;
   double acc[1] = {0.0};
@@ -281,6 +293,7 @@ __global__ void __launch_bounds__(kThreads) k_bicg_x(int64_t n, XT* __restrict__
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_axpy_state(int64_t n, XT* __restrict__ x, const XT* __restrict__ y,
                                                          const DevState* st) {
+  pdl_enter();
   const XT a = (XT)st->alpha;
   GRID_STRIDE_U4(i, n, x[i] = x[i] + a * y[i];)
 }
@@ -346,6 +359,7 @@ template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_gemv_sub(int64_t n, const XT* __restrict__ V, int64_t ldv, int nv,
                                                        const double* __restrict__ h, XT* __restrict__ w,
                                                        const int* skip) {
+  pdl_enter();
   if (flag_set(skip)) return;
   GRID_STRIDE(i, n) {
     double s = 0.0;
@@ -359,6 +373,7 @@ template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_gemv_cols(int64_t n, const XT* __restrict__ V, int64_t ldv,
                                                         const int* __restrict__ cols, const double* __restrict__ y,
                                                         XT* __restrict__ u, const int* skip) {
+  pdl_enter();
   if (flag_set(skip)) return;
   const int nc = *cols;
   GRID_STRIDE(i, n) {
@@ -372,6 +387,7 @@ __global__ void __launch_bounds__(kThreads) k_gemv_cols(int64_t n, const XT* __r
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_scale_div(int64_t n, const XT* src, XT* dst,
                                                         const double* __restrict__ div, const int* skip) {
+  pdl_enter();
   if (flag_set(skip)) return;
   const double d = *div;
   if (d == 0.0) return;
@@ -382,6 +398,7 @@ template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_jacobi_apply(int64_t n, const XT* __restrict__ r,
                                                            const XT* __restrict__ jinv, XT* __restrict__ z,
                                                            const int* skip) {
+  pdl_enter();
   if (flag_set(skip)) return;
   GRID_STRIDE_U4(i, n, z[i] = r[i] * jinv[i];)
 }
@@ -389,6 +406,7 @@ __global__ void __launch_bounds__(kThreads) k_jacobi_apply(int64_t n, const XT* 
 template <typename XT>
 __global__ void __launch_bounds__(kThreads) k_add(int64_t n, XT* __restrict__ x, const XT* __restrict__ z,
                                                   const int* skip) {
+  pdl_enter();
   if (flag_set(skip)) return;
   GRID_STRIDE_U4(i, n, x[i] = x[i] + z[i];)
 }
@@ -468,6 +486,7 @@ __global__ void k_gmres_check(DevState* st) {
 __global__ void __launch_bounds__(kThreads) k_refine_start(int64_t n, const double* __restrict__ r64,
                                                            float* __restrict__ r32, float* __restrict__ x32,
                                                            const DevState* outer, DevState* inner, Red red) {
+  pdl_enter();
   const double sc = 1.0 / outer->rnorm;
   double acc[1] = {0.0};
   GRID_STRIDE_U4(i, n, {
@@ -499,6 +518,7 @@ __global__ void __launch_bounds__(kThreads) k_refine_start(int64_t n, const doub
 // x64 += ||r64|| * d32 (the FP64 solution accumulation).
 __global__ void __launch_bounds__(kThreads) k_refine_accumulate(int64_t n, double* __restrict__ x64,
                                                                 const float* __restrict__ d32, const DevState* outer) {
+  pdl_enter();
   const double sc = outer->rnorm;
   GRID_STRIDE_U4(i, n, x64[i] += sc * (double)d32[i];)
 }
@@ -530,7 +550,7 @@ struct Launcher {
       occ[ctx->device] = std::max(1, o);
     }
     const int grid = std::min(m.nblk, ctx->num_sms * occ[ctx->device]);
-    kern<<<grid, kPipeThreads, smem, s>>>(mat_view<VT>(m), m.nblk, x, epi, ctx->err);
+    launch(kern, grid, kPipeThreads, smem, mat_view<VT>(m), m.nblk, x, epi, ctx->err);
     return CFD_OK;
   }
   // x-staged pipeline: one CTA per SM.
@@ -549,7 +569,7 @@ struct Launcher {
     }
     const int grid = std::min(m.nblk, ctx->num_sms);
     const XsView xv{m.xdesc, m.xwin, m.rec, (int)m.ncols};
-    kern<<<grid, kXsThreads, smem, s>>>(mat_view<VT>(m), xv, m.nblk, x, epi, ctx->err);
+    launch(kern, grid, kXsThreads, smem, mat_view<VT>(m), xv, m.nblk, x, epi, ctx->err);
     ctx->stats.xs_launches++;
     return CFD_OK;
   }
@@ -591,7 +611,7 @@ struct Launcher {
         1, std::min<int64_t>({chunks, (int64_t)ctx->num_sms * occ[ctx->device], (int64_t)ctx->partial_capacity}));
     const SlView sv{m.sl_off, m.sl_code, m.sl_dict, m.sl_doff, m.sl_v32, (unsigned long long)m.base_mult,
                     (int)m.sl_slices, (int)m.nrows};
-    kern<<<grid, kThreads, 0, s>>>(sv, x, epi);
+    launch(kern, grid, kThreads, 0, sv, x, epi);
     return CFD_OK;
   }
   // Diagonal pipeline: refills the diagonal-major values first when the CSR
@@ -674,7 +694,7 @@ struct Launcher {
         1, std::min<int64_t>({spans, (int64_t)ctx->num_sms * occ, (int64_t)ctx->partial_capacity}));
     DiaView<VT> D = dia_view<VT>(m);
     D.xvec = xvec ? 1 : 0;
-    kern<<<grid, kThreads, 0, s>>>(D, xs, epi);
+    launch(kern, grid, kThreads, 0, D, xs, epi);
     return CFD_OK;
   }
   // The diagonal pipeline runs when the values of this precision are there
@@ -803,11 +823,27 @@ struct Launcher {
     }
     return CFD_OK;
   }
-  template <typename K, typename... Args>
-  cfd_status vec(int64_t n, K kernel, Args... args) {
-    kernel<<<vec_grid(n), kThreads, 0, s>>>(n, args...);
+  template <typename... KArgs, typename... Args>
+  cfd_status vec(int64_t n, void (*kernel)(KArgs...), Args... args) {
+    launch(kernel, vec_grid(n), kThreads, 0, n, args...);
     ctx->stats.launches++;
     return check();
+  }
+  // Launch with programmatic stream serialization (the kernel begins with
+  // pdl_enter, which waits for the stream's preceding grid on the device).
+  template <typename... KArgs, typename... Args>
+  void launch(void (*kernel)(KArgs...), int grid, int block, size_t smem, Args... args) const {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
   }
 };
 
@@ -873,7 +909,8 @@ static cfd_status vcycle(Launcher& lc, cfd_amg* amg, size_t l, const XT* b, XT* 
   const bool coarsest = (l + 1 == amg->dev.size());
   if (coarsest) {
     if (c.coarse_solve == CFD_COARSE_DENSE && amg->coarse_inv) {
-      k_dense_gemv<XT><<<(int)((n + 7) / 8), kThreads, 0, lc.s>>>((int)n, amg->coarse_inv, b, out, done);
+      lc.launch(k_dense_gemv<XT>, (int)((n + 7) / 8), kThreads, 0, (int)n, (const double*)amg->coarse_inv, b, out,
+                done);
       lc.ctx->stats.launches++;
       CFD_TRY(lc.check());
       if (dot) CFD_TRY(lc.vec(n, k_rz<XT>, b, (const XT*)out, st, dot, lc.red()));
@@ -982,6 +1019,11 @@ struct Poller {
     }
     const DevState& h = *host;
     int c = std::min(2 * chunk, 64);
+    if (last_rn == 0.0 && h.iter >= 3 && h.rnorm0 > 0.0) {
+      // first look after a predicted chunk: measure from the start
+      last_iter = 0;
+      last_rn = h.rnorm0;
+    }
     if (h.iter > last_iter && last_rn > 0.0 && h.rnorm > 0.0 && h.rnorm < last_rn) {
       const double rate = std::pow(h.rnorm / last_rn, 1.0 / (double)(h.iter - last_iter));
       if (rate < 1.0 && rate > 0.0) {
@@ -1396,6 +1438,7 @@ cfd_status solve_refine(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg, 
   double rn = hs[0].rnorm;
   int64_t inner_iters = 0;
   int outer_steps = 0;
+  double inner_rate = 0.0;
   const int max_outer = opt.max_outer > 0 ? opt.max_outer : 20;
   while (!hs[0].done) {
     if (outer_steps >= max_outer || inner_iters >= cfg.max_iterations) {
@@ -1409,11 +1452,20 @@ cfd_status solve_refine(cfd_csr* a, const cfd_solve_options& opt, cfd_amg* amg, 
     CFD_TRY(lc.vec(n, k_refine_start, (const double*)r64, B.r, B.x, (const DevState*)outer, inner, lc.red()));
     Poller pl{ctx, inner, hs + 1};
     pl.fixed = opt.check_every;
-    pl.poll();
+    // The previous inner solve's contraction rate predicts this one's length:
+    // its first chunk stops one iteration short of the prediction, so the
+    // host's first look at the state comes near the end instead of after one
+    // iteration (no look at all before the first chunk).
+    if (inner_rate > 0.0 && inner_rate < 1.0 && opt.solver == CFD_SOLVER_CG) {
+      const double k = std::log(icfg.relative_tolerance) / std::log(inner_rate);
+      pl.chunk = (int)std::max(1.0, std::min(64.0, std::floor(k) - 1.0));
+    }
     if (opt.solver == CFD_SOLVER_GMRES) CFD_TRY(lc.vec(n, k_copy<float>, (const float*)B.r, B.b, (const int*)nullptr));
     CFD_TRY(krylov_loop<float>(lc, opt.solver, opt.precond, a, amg, B, inner, pl, opt.restart));
     inner_iters += hs[1].iter;
     ++outer_steps;
+    if (hs[1].iter > 0 && hs[1].rnorm0 > 0.0 && hs[1].rnorm > 0.0)
+      inner_rate = std::pow(hs[1].rnorm / hs[1].rnorm0, 1.0 / (double)hs[1].iter);
     const int iterm = hs[1].term;
     CFD_TRY(lc.vec(n, k_refine_accumulate, x64, (const float*)B.x, (const DevState*)outer));
     // outer FP64 residual and convergence test
