@@ -43,6 +43,7 @@ struct cfd_amg {
   std::vector<cfd::HostLevel> host;
   std::vector<cfd::DevLevel> dev;
   double* coarse_inv = nullptr;  // dense FP64 inverse of the coarsest operator (CFD_COARSE_DENSE)
+  float* coarse_inv32 = nullptr;  // its FP32 rounding, applied by the FP32 (inner) V-cycle
   int64_t coarse_n = 0;
   bool have32 = false;
   bool host_values_stale = false;  // level A values re-formed on the device (cfd_amg_recompute)

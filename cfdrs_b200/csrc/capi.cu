@@ -364,6 +364,7 @@ void amg_free_device(cfd_amg* amg) {
   }
   amg->dev.clear();
   dfree(amg->coarse_inv);
+  dfree(amg->coarse_inv32);
   amg->have32 = false;
 }
 
@@ -429,6 +430,11 @@ cfd_status amg_ensure32(cfd_amg* amg) {
       CFD_TRY(devmat_ensure32(D.R, s));
     }
     CFD_TRY(alloc_level_vecs(D.v32, D.A.nrows));
+  }
+  if (amg->coarse_inv) {
+    const int64_t nn = std::max<int64_t>(amg->coarse_n * amg->coarse_n, 1);
+    CFD_TRY(dmalloc(&amg->coarse_inv32, nn));
+    CFD_TRY(cast_to_f32(amg->coarse_inv, amg->coarse_inv32, nn, s));
   }
   CFD_TRY_CUDA(cudaStreamSynchronize(s));
   amg->have32 = true;

@@ -488,6 +488,11 @@ cfd_status amg_recompute_device(cfd_amg* amg, const cfd_csr* a) {
     if (amg->coarse_inv) cudaFree(amg->coarse_inv);
     amg->coarse_inv = inv;
     amg->coarse_n = Ac.nrows;
+    if (amg->coarse_inv32) {
+      const int64_t nn = Ac.nrows * Ac.nrows;
+      k_cast32<<<grid_for(amg->ctx, nn, 256), 256, 0, s>>>(nn, inv, amg->coarse_inv32);
+      CFD_TRY_CUDA(cudaGetLastError());
+    }
   }
   CFD_TRY_CUDA(cudaStreamSynchronize(s));
   return CFD_OK;

@@ -76,18 +76,19 @@ __global__ void __launch_bounds__(kThreads) k_copy(int64_t n, const XT* __restri
   GRID_STRIDE_U4(i, n, d[i] = s[i];)
 }
 
-// Dense coarsest-level solve x = A_c^{-1} b with the FP64 inverse; one warp per row.
-template <typename XT>
-__global__ void __launch_bounds__(kThreads) k_dense_gemv(int n, const double* __restrict__ inv, const XT* __restrict__ b,
+// Dense coarsest-level solve x = A_c^{-1} b with the inverse (FP64, or its FP32
+// rounding in the FP32 V-cycle), FP64 sums; one warp per row.
+template <typename XT, typename IT>
+__global__ void __launch_bounds__(kThreads) k_dense_gemv(int n, const IT* __restrict__ inv, const XT* __restrict__ b,
                                                          XT* __restrict__ x, const int* done) {
   pdl_enter();
   if (flag_set(done)) return;
   const int lane = threadIdx.x & 31;
   const int row = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
   if (row >= n) return;
-  const double* a = inv + (size_t)row * n;
+  const IT* a = inv + (size_t)row * n;
   double s = 0.0;
-  for (int k = lane; k < n; k += 32) s += a[k] * (double)b[k];
+  for (int k = lane; k < n; k += 32) s += (double)a[k] * (double)b[k];
   s = warp_sum(s);
   if (lane == 0) x[row] = (XT)s;
 }
@@ -909,8 +910,12 @@ static cfd_status vcycle(Launcher& lc, cfd_amg* amg, size_t l, const XT* b, XT* 
   const bool coarsest = (l + 1 == amg->dev.size());
   if (coarsest) {
     if (c.coarse_solve == CFD_COARSE_DENSE && amg->coarse_inv) {
-      lc.launch(k_dense_gemv<XT>, (int)((n + 7) / 8), kThreads, 0, (int)n, (const double*)amg->coarse_inv, b, out,
-                done);
+      if (sizeof(XT) == 4 && amg->coarse_inv32)
+        lc.launch(k_dense_gemv<XT, float>, (int)((n + 7) / 8), kThreads, 0, (int)n,
+                  (const float*)amg->coarse_inv32, b, out, done);
+      else
+        lc.launch(k_dense_gemv<XT, double>, (int)((n + 7) / 8), kThreads, 0, (int)n,
+                  (const double*)amg->coarse_inv, b, out, done);
       lc.ctx->stats.launches++;
       CFD_TRY(lc.check());
       if (dot) CFD_TRY(lc.vec(n, k_rz<XT>, b, (const XT*)out, st, dot, lc.red()));
