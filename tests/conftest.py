@@ -39,11 +39,11 @@ def cuda():
 # Under `pytest -x` the first failure ends the run, so the suites of the solve
 # path itself (parity, GMRES, batch, adjoint, recompute) run before the
 # components added on top of them (device network assembly, the saddle-point
-# tiers, the pressure dispatch), and the suites that must come last (the no-alloc and wait-timeout
-# checks) keep their place at the end.
+# tiers, the pressure dispatch), then the wait-timeout check, and the no-alloc
+# entry point's test runs last of all.
 _FILE_ORDER = ["test_gpu_parity", "test_gpu_configs", "test_gpu_gmres", "test_gpu_batch", "test_gpu_network_cascade", "test_gpu_adjoint", "test_gpu_recompute",
-               "test_gpu_network_assembly", "test_gpu_simple", "test_gpu_component", "test_gpu_pressure", "test_zz_no_alloc",
-               "test_zz_wait_timeout"]
+               "test_gpu_network_assembly", "test_gpu_simple", "test_gpu_component", "test_gpu_pressure",
+               "test_zy_wait_timeout", "test_zz_no_alloc"]
 
 
 def pytest_collection_modifyitems(session, config, items):
