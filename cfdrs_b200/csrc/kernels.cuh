@@ -282,27 +282,30 @@ __device__ __forceinline__ void pcg_rho_update(DevState* st, double rho_new) {
 //   xn_i = xo_i + w ((b_i - sum_{j != i} a_ij xo_j) / a_ii - xo_i),  xn_i = xo_i if |a_ii| <= 1e-15.
 // DOT 1: also accumulate b.xn and store it as rho (PCG start, z = M r).
 // DOT 2: b.xn is rho_new of the PCG recurrence: breakdown test, beta, rho.
+// a_ii comes from the level's diagonal array (the value of the row's diagonal
+// entry), not from the SpMV's diagonal argument.
 template <typename XT, int DOT>
 struct EpiJacobi {
   static constexpr int NRED = DOT ? 1 : 0;
   struct Pre {
-    XT xo, b;
+    XT xo, b, d;
   };
   XT* __restrict__ xn;
   const XT* __restrict__ xo;
   const XT* __restrict__ b;
+  const XT* __restrict__ dg;
   XT omega;
   DevState* st;
   const int* done;
   Red red;
   __device__ bool skip() const { return flag_set(done); }
-  __device__ Pre load(int i) const { return {xo[i], b[i]}; }
+  __device__ Pre load(int i) const { return {xo[i], b[i], dg[i]}; }
   template <typename S>
-  __device__ void row(int i, S s, S d, const Pre& p, double* acc) const {
+  __device__ void row(int i, S s, S, const Pre& p, double* acc) const {
     XT out = p.xo;
-    if (diag_ok<XT>((XT)d)) {
+    if (diag_ok<XT>(p.d)) {
       // FP32 (inner) sweeps: the fast single-precision division (within 2 ulp)
-      const XT nv = sweep_div<XT>(p.b - (XT)s, (XT)d);
+      const XT nv = sweep_div<XT>(p.b - (XT)s, p.d);
       out = p.xo + omega * (nv - p.xo);
     }
     xn[i] = out;
@@ -507,25 +510,24 @@ __device__ __forceinline__ void rows_from_stage(const Epi& epi, const Rp& srp, c
         const int c = sc.at(k, rb[q]);
         const VT v = sv[k];
         // The gather is issued for the diagonal entry too (a valid, cached
-        // address) and the diagonal test selects instead of branching; the
-        // row sum sees the same terms in the same order.
+        // address). With OFFDIAG the diagonal entry enters the row sum as
+        // 0 * x_i: the sum starts at +0, so it is never -0, and adding the
+        // product (+-0) leaves it unchanged for finite x_i, so the row sum
+        // equals the off-diagonal sum bit for bit. a_ii itself is not kept
+        // here: the sweep's epilogue reads it from the level's diagonal
+        // array (keeping it in the loop made the FP64 sweeps take 1.8x their
+        // residual's time).
         const VT xv = (VT)__ldg(x + c);
-        if constexpr (OFFDIAG) {
-          const bool isd = (c == row[q]);
-          diag[q] = isd ? v : diag[q];
-          sum[q] = isd ? sum[q] : sum[q] + v * xv;
-        } else {
+        if constexpr (OFFDIAG)
+          sum[q] += (c == row[q] ? VT(0) : v) * xv;
+        else
           sum[q] += v * xv;
-        }
       }
     }
   }
 #pragma unroll
   for (int q = 0; q < kRowsPerThread; ++q) {
-    for (int o = step >> 1; o > 0; o >>= 1) {
-      sum[q] += __shfl_xor_sync(0xffffffffu, sum[q], o);
-      if (OFFDIAG) diag[q] += __shfl_xor_sync(0xffffffffu, diag[q], o);
-    }
+    for (int o = step >> 1; o > 0; o >>= 1) sum[q] += __shfl_xor_sync(0xffffffffu, sum[q], o);
     if (row[q] < r1 && lane == 0) epi.row(row[q], sum[q], diag[q], pre[q], red);
   }
 }

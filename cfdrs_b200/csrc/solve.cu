@@ -884,9 +884,10 @@ static cfd_status jacobi_sweep(Launcher& lc, const DevLevel& L, const XT* xo, XT
     if (dot == 2) return lc.spmv<float, float, false>(L.A, xo, EpiJacobiR<float, 2>{xn, xo, b, d, omega, st, done, {}});
     return lc.spmv<float, float, false>(L.A, xo, EpiJacobiR<float, 0>{xn, xo, b, d, omega, st, done, {}});
   } else {
-    if (dot == 1) return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 1>{xn, xo, b, omega, st, done, {}});
-    if (dot == 2) return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 2>{xn, xo, b, omega, st, done, {}});
-    return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 0>{xn, xo, b, omega, st, done, {}});
+    const XT* d = diag_of<XT>(L);
+    if (dot == 1) return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 1>{xn, xo, b, d, omega, st, done, {}});
+    if (dot == 2) return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 2>{xn, xo, b, d, omega, st, done, {}});
+    return lc.spmv<XT, XT, true>(L.A, xo, EpiJacobi<XT, 0>{xn, xo, b, d, omega, st, done, {}});
   }
 }
 
