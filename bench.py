@@ -744,6 +744,10 @@ def run_batch(args, world, rank, local):
             "max_residual": rep.max_residual,
             "fp32_refine_ms": rep32.device_ms,
             "jacobi_pcg_ms": min(pcg), "jacobi_pcg_total_iterations": prep.total_iterations,
+            "jacobi_pcg_max_iterations": prep.max_iterations,
+            # the longest system's CTA ran for at most the whole call, so the call's
+            # device time over its iterations bounds one iteration on the critical path
+            "jacobi_pcg_us_per_iteration_bound": 1e3 * min(pcg) / max(prep.max_iterations, 1),
             "jacobi_pcg_fp32_refine_ms": prep32.device_ms,
             "autotuned": tuned, "clocks": clk.summary(),
         }

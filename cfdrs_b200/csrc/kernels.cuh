@@ -446,8 +446,9 @@ struct EpiBicgT {
 // kRowsPerThread rows of the block (g and g + 256 >> tl, ...); the groups read
 // strided shares of both rows in one interleaved loop so their x gathers are in
 // flight together, then reduce with a butterfly. OFFDIAG=true forms
-// sum_{j != i} a_ij x_j and returns a_ii separately (the Jacobi smoother's
-// split, smoothers.rs:177-186). srp/sc/sv index rows and nonzeros directly.
+// sum_{j != i} a_ij x_j for the Jacobi smoother's split form
+// (smoothers.rs:177-186), whose epilogue reads a_ii from the level's diagonal
+// array. srp/sc/sv index rows and nonzeros directly.
 // Column of staged entry k: int32 as stored, or base(row) + dict[code[k]]
 // with base(row) = (row * mult) >> 20, mult = (ncols << 20) / nrows (row
 // itself for square matrices), computed identically by the host encoder.
@@ -485,7 +486,7 @@ __device__ __forceinline__ void rows_from_stage(const Epi& epi, const Rp& srp, c
   const int ngroups = kThreads >> tl;
   int row[kRowsPerThread], ra[kRowsPerThread], re[kRowsPerThread], rb[kRowsPerThread];
   typename Epi::Pre pre[kRowsPerThread];
-  VT sum[kRowsPerThread], diag[kRowsPerThread];
+  VT sum[kRowsPerThread];
 #pragma unroll
   for (int q = 0; q < kRowsPerThread; ++q) {
     row[q] = r0 + g + q * ngroups;
@@ -496,7 +497,6 @@ __device__ __forceinline__ void rows_from_stage(const Epi& epi, const Rp& srp, c
     pre[q] = typename Epi::Pre{};
     if (live && lane == 0) pre[q] = epi.load(row[q]);
     sum[q] = VT(0);
-    diag[q] = VT(0);
   }
   int len = 0;
 #pragma unroll
@@ -528,7 +528,7 @@ __device__ __forceinline__ void rows_from_stage(const Epi& epi, const Rp& srp, c
 #pragma unroll
   for (int q = 0; q < kRowsPerThread; ++q) {
     for (int o = step >> 1; o > 0; o >>= 1) sum[q] += __shfl_xor_sync(0xffffffffu, sum[q], o);
-    if (row[q] < r1 && lane == 0) epi.row(row[q], sum[q], diag[q], pre[q], red);
+    if (row[q] < r1 && lane == 0) epi.row(row[q], sum[q], VT(0), pre[q], red);
   }
 }
 
@@ -1397,7 +1397,7 @@ __device__ __forceinline__ void rows_from_stage_xs(const Epi& epi, const uint16_
     xr += (int)(((unsigned long long)row * mult) >> 20) - b0;
     if (lane == 0) pre = epi.load(row);
   }
-  VT sum = VT(0), diag = VT(0);
+  VT sum = VT(0);
   for (int kb = ka; kb < ke; kb += kBatch * step) {
     unsigned c[kBatch];
     VT v[kBatch];
@@ -1411,21 +1411,15 @@ __device__ __forceinline__ void rows_from_stage_xs(const Epi& epi, const uint16_
     for (int u = 0; u < kBatch; ++u) {
       if (kb + u * step < ke) {
         const VT xv = xr[se[c[u]]];
-        if constexpr (OFFDIAG) {
-          const bool isd = ((int)c[u] == zq);
-          diag = isd ? v[u] : diag;
-          sum = isd ? sum : sum + v[u] * xv;
-        } else {
+        if constexpr (OFFDIAG)
+          sum += ((int)c[u] == zq ? VT(0) : v[u]) * xv;  // the diagonal as a zero product
+        else
           sum += v[u] * xv;
-        }
       }
     }
   }
-  for (int o = step >> 1; o > 0; o >>= 1) {
-    sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    if (OFFDIAG) diag += __shfl_xor_sync(0xffffffffu, diag, o);
-  }
-  if (live && lane == 0) epi.row(row, sum, diag, pre, red);
+  for (int o = step >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if (live && lane == 0) epi.row(row, sum, VT(0), pre, red);
 }
 
 template <typename VT, bool OFFDIAG, class Epi>
