@@ -87,7 +87,7 @@ def test_reference_arm_adjoint():
 
 
 def test_reference_arm_two_ranks():
-    """As the driver launches N > 1: one rank per process over gloo; rank 0
+    """Launched with torchrun for N > 1: one rank per process over gloo; rank 0
     alone measures and prints, the other rank exits 0 without work."""
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(free_port()),
